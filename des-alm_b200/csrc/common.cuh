@@ -1,0 +1,64 @@
+// common.cuh -- shared device types and helpers of the B200 DES-ALM path.
+//
+// Layout in HBM: one structure-of-arrays block per multigrid level.  Every
+// field is a contiguous array of im*jm*km values, i fastest, then j, then k
+// (the reference's Fortran order, src/init.F90:917-937, without concatenating
+// the levels).  Node (i, j, k) with 0-based indices lives at
+// i + im*(j + jm*k); interior nodes are 1..im-2 etc.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define DESALM_DEV __device__ __forceinline__
+
+namespace desalm {
+
+// Per-level device view passed by value to the kernels.  T is the storage and
+// arithmetic type of the level's state (double; float for coarse levels in
+// MIXED mode), W the type of the DAF work arrays (line sweeps).
+template <class T, class W>
+struct Lv {
+  int im, jm, km;
+  int N;           // im*jm*km
+  int sj, sk;      // strides of j and k (im, im*jm)
+  T dc, de, dz;    // inverse spacings dc(n) (src/init.F90:1117-1121)
+  // state
+  T* q[5];
+  T* qn[5];
+  T* qnm1[5];
+  T* qold[5];
+  T* rh[4];        // raw residual (restriction input), boundary nodes stay 0
+  T* pk[4];        // FAS forcing
+  T* nut;
+  T* dtau;
+  T* diss1;        // diss(1) of the first residual pass (reused by the recalc)
+  // geometry
+  const T* csi[3];
+  const T* eta[3];
+  const T* zet[3];
+  const T* aj;
+  // DAF work: transformed residual, forward-elimination scratch
+  W* wk[4];
+  W* sd[3];        // eliminated diagonal: systems (1,2), 3, 4
+  W* su[3];        // super-diagonal: systems (1,2), 3, 4
+  W* bi;           // i-face boundary vectors: [2][4][jm*km]
+  W* bj;           // j-face: [4][4][im*km]  (rows 2, 3, jm-1, jm-2 after the i sweep)
+  W* bk;           // k-face: [4][4][im*jm]
+  int* flags;      // [0] pivot-would-swap count, [1] zero pivot count
+};
+
+// Scalar parameters of the case used by kernels (constant per context).
+struct Par {
+  double ren, beta, delti, es;   // es = e_source
+  double cfl1, vnn1, pdiss;
+  double ep1[3], ep2[3];
+  double sa[4][6], sb[4][6];     // src/init.F90:482-509
+  int btype[6];
+  int fine;                      // 1 when the level is the finest
+};
+
+template <class T> DESALM_DEV T dabs(T x) { return x < T(0) ? -x : x; }
+template <class T> DESALM_DEV T dmin(T a, T b) { return a < b ? a : b; }
+template <class T> DESALM_DEV T dmax(T a, T b) { return a > b ? a : b; }
+
+}  // namespace desalm

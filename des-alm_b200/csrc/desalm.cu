@@ -1,0 +1,984 @@
+// desalm.cu -- host runtime and C ABI of the B200 DES-ALM pseudo-time iteration.
+//
+// The context owns every device array (allocated once per level at init),
+// the CUDA stream all work is ordered on, and the host-side mirror of the
+// reference's mg_driver control flow (src/mg_driver.F90:2-323).  Each public
+// function in include/desalm.h maps to one reference subroutine; kernels are
+// in resid.cuh (K_R), sweep.cuh (K_I/K_J/K_K), mg.cuh (transfers, boundary
+// conditions, norm, metrics) and sa.cuh (Spalart-Allmaras).
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <cmath>
+#include <string>
+#include <vector>
+#include <algorithm>
+
+#include "desalm.h"
+#include "common.cuh"
+#include "resid.cuh"
+#include "sweep.cuh"
+#include "mg.cuh"
+#include "sa.cuh"
+
+using namespace desalm;
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+// One level: storage type chosen at runtime (FP64 or FP32 state, FP64 or
+// FP32 sweep work); exactly one of the typed views is active.
+struct Level {
+  int im = 0, jm = 0, km = 0;
+  long N = 0;
+  double dc = 1, de = 1, dz = 1;
+  int tbytes = 8, wbytes = 8;  // state / work element sizes
+  std::vector<void*> allocs;
+  Lv<double, double> dd{};
+  Lv<double, float> df{};
+  Lv<float, float> ff{};
+  void* dq[4] = {nullptr, nullptr, nullptr, nullptr};  // prolongation correction
+  double* fac[3] = {nullptr, nullptr, nullptr};         // rsmooth multipliers
+  double* dpr[3] = {nullptr, nullptr, nullptr};         // rsmooth eliminated diagonal
+  bool dtau_valid = false;
+};
+
+}  // namespace
+
+struct desalm_ctx {
+  desalm_case c{};
+  int ng = 0;
+  std::vector<Level> L;
+  cudaStream_t stream = nullptr;
+  Par par{};
+  std::string err;
+  bool have_grid = false, have_state = false;
+  // fine-level extras (always FP64)
+  double *x = nullptr, *y = nullptr, *z = nullptr, *wd = nullptr, *dtev = nullptr;
+  double* cov[9] = {};
+  double* rat = nullptr;
+  int ratdim = 0;
+  double* pfix = nullptr;     // device scalar (type of the fine level: double)
+  double* part = nullptr;     // norm partials
+  int part_blocks = 0;
+  double* norm = nullptr;     // device [5]
+  double* h_norm = nullptr;   // pinned host [5]
+  int* flags = nullptr;       // device [2]
+  SaWork sa{};
+  // driver state
+  int itc = 0;
+  double init_resd[5] = {0, 0, 0, 0, 0};
+  std::vector<void*> allocs;
+};
+
+namespace {
+
+#define CK(call)                                                                 \
+  do {                                                                           \
+    cudaError_t e__ = (call);                                                    \
+    if (e__ != cudaSuccess) {                                                    \
+      ctx->err = std::string(#call) + ": " + cudaGetErrorString(e__);            \
+      return DESALM_ECUDA;                                                       \
+    }                                                                            \
+  } while (0)
+
+#define CKL()                                                                    \
+  do {                                                                           \
+    cudaError_t e__ = cudaGetLastError();                                        \
+    if (e__ != cudaSuccess) {                                                    \
+      ctx->err = std::string("kernel launch: ") + cudaGetErrorString(e__);       \
+      return DESALM_ECUDA;                                                       \
+    }                                                                            \
+  } while (0)
+
+#define RET(x)            \
+  do {                    \
+    int r__ = (x);        \
+    if (r__) return r__;  \
+  } while (0)
+
+inline unsigned cdiv(long a, long b) { return (unsigned)((a + b - 1) / b); }
+
+int dalloc(desalm_ctx* ctx, std::vector<void*>& owner, void** p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    ctx->err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+    return DESALM_ENOMEM;
+  }
+  owner.push_back(*p);
+  e = cudaMemsetAsync(*p, 0, bytes, ctx->stream);
+  if (e != cudaSuccess) {
+    ctx->err = std::string("cudaMemsetAsync: ") + cudaGetErrorString(e);
+    return DESALM_ECUDA;
+  }
+  return 0;
+}
+
+template <class T, class W>
+int alloc_level(desalm_ctx* ctx, Level& G, Lv<T, W>& L) {
+  const long N = G.N;
+  L.im = G.im; L.jm = G.jm; L.km = G.km;
+  L.N = (int)N;
+  L.sj = G.im; L.sk = G.im * G.jm;
+  L.dc = T(G.dc); L.de = T(G.de); L.dz = T(G.dz);
+  auto A = [&](T** p) { return dalloc(ctx, G.allocs, (void**)p, N * sizeof(T)); };
+  auto AW = [&](W** p) { return dalloc(ctx, G.allocs, (void**)p, N * sizeof(W)); };
+  for (int m = 0; m < 5; ++m) { RET(A(&L.q[m])); RET(A(&L.qn[m])); RET(A(&L.qnm1[m])); RET(A(&L.qold[m])); }
+  for (int m = 0; m < 4; ++m) { RET(A(&L.rh[m])); RET(A(&L.pk[m])); }
+  RET(A(&L.nut)); RET(A(&L.dtau)); RET(A(&L.diss1));
+  for (int d = 0; d < 3; ++d) {
+    RET(A((T**)&L.csi[d])); RET(A((T**)&L.eta[d])); RET(A((T**)&L.zet[d]));
+  }
+  RET(A((T**)&L.aj));
+  for (int m = 0; m < 4; ++m) RET(AW(&L.wk[m]));
+  for (int m = 0; m < 3; ++m) { RET(AW(&L.sd[m])); RET(AW(&L.su[m])); }
+  RET(dalloc(ctx, G.allocs, (void**)&L.bi, sizeof(W) * 8L * G.jm * G.km));
+  RET(dalloc(ctx, G.allocs, (void**)&L.bj, sizeof(W) * 16L * G.im * G.km));
+  RET(dalloc(ctx, G.allocs, (void**)&L.bk, sizeof(W) * 16L * G.im * G.jm));
+  L.flags = ctx->flags;
+  return 0;
+}
+
+int check_case(desalm_ctx* ctx, const desalm_case& c) {
+  auto bad = [&](const char* why) { ctx->err = why; return DESALM_EINVAL; };
+  if (c.ng < 1 || c.ng > 4) return bad("ng must be 1..4");
+  if (c.im < 5 || c.jm < 5 || c.km < 5) return bad("each extent must be >= 5");
+  if ((c.icrs != 0 && c.icrs != 1) || (c.jcrs != 0 && c.jcrs != 1) || (c.kcrs != 0 && c.kcrs != 1))
+    return bad("icrs/jcrs/kcrs must be 0 or 1");
+  for (int b = 0; b < 6; ++b)
+    if (c.btype[b] == 5) return bad("btype 5 (characteristics outlet) is not supported");
+  if (c.precision_mode != DESALM_FP64 && c.precision_mode != DESALM_MIXED) return bad("unknown precision_mode");
+  if (c.predictor != DESALM_PRED_QN && c.predictor != DESALM_PRED_LINEAR) return bad("unknown predictor");
+  if (c.ifix < 1 || c.ifix > c.im || c.jfix < 1 || c.jfix > c.jm || c.kfix < 1 || c.kfix > c.km)
+    return bad("pressure reference node outside the grid");
+  // vertex-centred coarsening (ii = 2i - 1) needs odd extents on every level
+  int im = c.im, jm = c.jm, km = c.km;
+  for (int n = 1; n < c.ng; ++n) {
+    if ((c.icrs && im % 2 == 0) || (c.jcrs && jm % 2 == 0) || (c.kcrs && km % 2 == 0))
+      return bad("full coarsening needs odd extents on every level above the coarsest");
+    im = (im + c.icrs) >> c.icrs; jm = (jm + c.jcrs) >> c.jcrs; km = (km + c.kcrs) >> c.kcrs;
+    if (im < 5 || jm < 5 || km < 5) return bad("coarsest level must keep >= 5 nodes per direction");
+  }
+  if ((long)c.im * c.jm * c.km * 4 >= (1L << 31)) return bad("grid too large for 32-bit indexing");
+  return 0;
+}
+
+void fill_par(desalm_ctx* ctx) {
+  const desalm_case& c = ctx->c;
+  Par& P = ctx->par;
+  P.ren = c.ren; P.beta = c.beta; P.delti = c.delti; P.es = c.unsteady ? 1.0 : 0.0;
+  P.cfl1 = c.cfl1; P.vnn1 = c.vnn1; P.pdiss = c.pdiss_coef;
+  for (int d = 0; d < 3; ++d) { P.ep1[d] = c.ep[0][d]; P.ep2[d] = c.ep[1][d]; }
+  // src/init.F90:482-509
+  for (int m = 0; m < 4; ++m)
+    for (int b = 0; b < 6; ++b) { P.sa[m][b] = 4.0 / 3.0; P.sb[m][b] = -(1.0 / 3.0); }
+  for (int b = 0; b < 6; ++b) {
+    P.btype[b] = c.btype[b];
+    if (c.btype[b] == 1) for (int m = 1; m < 4; ++m) { P.sa[m][b] = 0; P.sb[m][b] = 0; }
+    if (c.btype[b] == 2) {
+      int m = c.bdir[b];
+      if (m >= 1 && m <= 3) { P.sa[m][b] = 0; P.sb[m][b] = 0; }
+    }
+  }
+  P.fine = 0;
+}
+
+// rsmooth factors for a line of n interior nodes: SGTSV's elimination of
+// (-e, 1+2e, -e) in its own order (src/sgtsv.f:163-176).
+void rs_factors(int n, double e, std::vector<double>& fac, std::vector<double>& dpr) {
+  fac.assign(std::max(n - 1, 1), 0.0);
+  dpr.assign(n, 0.0);
+  const double dl = -e, du = -e, dg = 1.0 + 2.0 * e;
+  dpr[0] = dg;
+  for (int p = 0; p + 1 < n; ++p) {
+    double f = dl / dpr[p];
+    fac[p] = f;
+    dpr[p + 1] = dg - f * du;
+  }
+}
+
+// launch helpers --------------------------------------------------------------
+dim3 blk3() { return dim3(32, 4, 1); }
+template <class T, class W>
+dim3 grid_interior(const Lv<T, W>& L) { return dim3(cdiv(L.im - 2, 32), cdiv(L.jm - 2, 4), L.km - 2); }
+
+template <class T, class W>
+int launch_daf(desalm_ctx* ctx, Lv<T, W>& L, Level& G, int n, int recalc, int itr) {
+  Par P = ctx->par;
+  P.fine = (n == 0);
+  const desalm_case& c = ctx->c;
+  cudaStream_t s = ctx->stream;
+  if (!G.dtau_valid) {
+    k_dtau<T, W><<<cdiv(L.N, 256), 256, 0, s>>>(L, P);
+    CKL();
+    G.dtau_valid = true;
+  }
+  const int fine = (n == 0);
+  const int upwind = fine ? 2 : 1;
+  const int bback = fine && c.btype[0] != 5;
+  k_resid<T, W, 0><<<grid_interior(L), blk3(), 0, s>>>(L, P, upwind, itr == 1 ? 1 : 0, n > 0 ? 1 : 0, bback);
+  CKL();
+  const int TB = 64;
+  k_sweep<T, W, 0><<<dim3(cdiv(L.jm - 2, TB), L.km - 2), TB, 0, s>>>(L, P, bback, 0);
+  CKL();
+  k_sweep<T, W, 1><<<dim3(cdiv(L.im - 2, TB), L.km - 2), TB, 0, s>>>(L, P, fine && c.btype[2] != 5, fine && c.btype[3] != 5);
+  CKL();
+  k_sweep<T, W, 2><<<dim3(cdiv(L.im - 2, TB), L.jm - 2), TB, 0, s>>>(L, P, fine && c.btype[4] != 5,
+                                                                      fine && c.btype[5] != 5 && c.btype[5] != 6);
+  CKL();
+  return 0;
+}
+
+template <class T, class W>
+int launch_recalc(desalm_ctx* ctx, Lv<T, W>& L, int n) {
+  Par P = ctx->par;
+  P.fine = (n == 0);
+  k_resid<T, W, 1><<<grid_interior(L), blk3(), 0, ctx->stream>>>(L, P, n == 0 ? 2 : 1, 0, n > 0 ? 1 : 0, 0);
+  CKL();
+  return 0;
+}
+
+template <class T, class W>
+int launch_bcond(desalm_ctx* ctx, Lv<T, W>& L) {
+  Par P = ctx->par;
+  P.fine = 1;
+  cudaStream_t s = ctx->stream;
+  const T* rat = (const T*)ctx->rat;
+  k_bcond<T, W, 0><<<dim3(cdiv(L.jm, 64), L.km), 64, 0, s>>>(L, P, rat, ctx->ratdim);
+  CKL();
+  k_bcond<T, W, 1><<<dim3(cdiv(L.im, 64), L.km), 64, 0, s>>>(L, P, rat, ctx->ratdim);
+  CKL();
+  k_bcond<T, W, 2><<<dim3(cdiv(L.im, 64), L.jm), 64, 0, s>>>(L, P, rat, ctx->ratdim);
+  CKL();
+  const desalm_case& c = ctx->c;
+  int lfix = (c.ifix - 1) + L.sj * (c.jfix - 1) + L.sk * (c.kfix - 1);
+  k_pfix_read<T, W><<<1, 1, 0, s>>>(L, lfix, (T*)ctx->pfix);
+  CKL();
+  k_pfix_sub<T, W><<<cdiv(L.N, 256), 256, 0, s>>>(L, (const T*)ctx->pfix);
+  CKL();
+  return 0;
+}
+
+template <class TF, class WF, class TC, class WC>
+int launch_nlevel(desalm_ctx* ctx, Lv<TF, WF>& F, Lv<TC, WC>& C) {
+  const desalm_case& c = ctx->c;
+  k_nlevel<TF, WF, TC, WC><<<dim3(cdiv(C.im, 32), cdiv(C.jm, 4), C.km), dim3(32, 4, 1), 0, ctx->stream>>>(F, C, c.icrs, c.jcrs, c.kcrs);
+  CKL();
+  return 0;
+}
+
+template <class TF, class WF, class TC, class WC>
+int launch_prolong(desalm_ctx* ctx, Lv<TF, WF>& F, Lv<TC, WC>& C, Level& G) {
+  const desalm_case& c = ctx->c;
+  cudaStream_t s = ctx->stream;
+  TF* dq = (TF*)G.dq[0];
+  k_prolong_interp<TF, WF, TC, WC><<<grid_interior(F), blk3(), 0, s>>>(F, C, dq, c.icrs, c.jcrs, c.kcrs);
+  CKL();
+  const int TB = 64;
+  k_rsmooth<TF, WF, 0><<<dim3(cdiv(F.jm - 2, TB), F.km - 2), TB, 0, s>>>(F, dq, G.fac[0], G.dpr[0], c.ep[1][0], 0);
+  CKL();
+  k_rsmooth<TF, WF, 1><<<dim3(cdiv(F.im - 2, TB), F.km - 2), TB, 0, s>>>(F, dq, G.fac[1], G.dpr[1], c.ep[1][1], 0);
+  CKL();
+  k_rsmooth<TF, WF, 2><<<dim3(cdiv(F.im - 2, TB), F.jm - 2), TB, 0, s>>>(F, dq, G.fac[2], G.dpr[2], c.ep[1][2], 1);
+  CKL();
+  return 0;
+}
+
+template <class T, class W>
+int launch_norm(desalm_ctx* ctx, Lv<T, W>& L, int copy, double* out) {
+  cudaStream_t s = ctx->stream;
+  long total = (long)(L.im - 2) * (L.jm - 2) * (L.km - 2);
+  int nb = (int)std::min<long>(ctx->part_blocks, std::max<long>(1, cdiv(total, 256)));
+  k_norm_partial<T, W><<<nb, 256, 0, s>>>(L, ctx->part, 5, copy);
+  CKL();
+  k_norm_final<<<1, 32, 0, s>>>(ctx->part, nb, ctx->norm);
+  CKL();
+  CK(cudaMemcpyAsync(ctx->h_norm, ctx->norm, 5 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  double tnu = double((long)(L.im - 2) * (L.jm - 2) * (L.km - 2));
+  for (int m = 0; m < 5; ++m) out[m] = std::log10(ctx->h_norm[m] / tnu);
+  return 0;
+}
+
+// dispatch on the active view of a level ------------------------------------
+enum Kind { K_DD, K_DF, K_FF };
+Kind kind_of(const desalm_ctx* ctx, int n) {
+  if (ctx->c.precision_mode == DESALM_FP64) return K_DD;
+  return n == 0 ? K_DF : K_FF;
+}
+
+#define DISPATCH(ctx, n, FN, ...)                                   \
+  ([&]() -> int {                                                   \
+    Level& G__ = (ctx)->L[n];                                       \
+    switch (kind_of(ctx, n)) {                                      \
+      case K_DD: return FN((ctx), G__.dd, ##__VA_ARGS__);           \
+      case K_DF: return FN((ctx), G__.df, ##__VA_ARGS__);           \
+      default: return FN((ctx), G__.ff, ##__VA_ARGS__);             \
+    }                                                               \
+  }())
+
+int do_daf(desalm_ctx* ctx, int n, int recalc, int itr) {
+  Level& G = ctx->L[n];
+  int rc;
+  switch (kind_of(ctx, n)) {
+    case K_DD: rc = launch_daf(ctx, G.dd, G, n, recalc, itr); break;
+    case K_DF: rc = launch_daf(ctx, G.df, G, n, recalc, itr); break;
+    default: rc = launch_daf(ctx, G.ff, G, n, recalc, itr); break;
+  }
+  if (rc) return rc;
+  if (n == 0) {
+    // bcond_fm inside solver_daf (src/solver_daf.F90:421)
+    rc = kind_of(ctx, 0) == K_DD ? launch_bcond(ctx, G.dd) : launch_bcond(ctx, G.df);
+    if (rc) return rc;
+  }
+  if (recalc == 1) {
+    switch (kind_of(ctx, n)) {
+      case K_DD: rc = launch_recalc(ctx, G.dd, n); break;
+      case K_DF: rc = launch_recalc(ctx, G.df, n); break;
+      default: rc = launch_recalc(ctx, G.ff, n); break;
+    }
+  }
+  return rc;
+}
+
+int do_bcond(desalm_ctx* ctx) {
+  Level& G = ctx->L[0];
+  return kind_of(ctx, 0) == K_DD ? launch_bcond(ctx, G.dd) : launch_bcond(ctx, G.df);
+}
+
+int do_nlevel(desalm_ctx* ctx, int n) {  // n = coarse level index (>= 1)
+  Level& F = ctx->L[n - 1];
+  Level& C = ctx->L[n];
+  C.dtau_valid = false;
+  Kind kf = kind_of(ctx, n - 1), kc = kind_of(ctx, n);
+  if (kf == K_DD) return launch_nlevel(ctx, F.dd, C.dd);
+  if (kf == K_DF) return launch_nlevel(ctx, F.df, C.ff);
+  (void)kc;
+  return launch_nlevel(ctx, F.ff, C.ff);
+}
+
+int do_prolong(desalm_ctx* ctx, int n) {  // fine level index n, coarse n+1
+  Level& F = ctx->L[n];
+  Level& C = ctx->L[n + 1];
+  Kind kf = kind_of(ctx, n);
+  if (kf == K_DD) return launch_prolong(ctx, F.dd, C.dd, F);
+  if (kf == K_DF) return launch_prolong(ctx, F.df, C.ff, F);
+  return launch_prolong(ctx, F.ff, C.ff, F);
+}
+
+int do_norm(desalm_ctx* ctx, int n, int copy, double* out) {
+  Level& G = ctx->L[n];
+  switch (kind_of(ctx, n)) {
+    case K_DD: return launch_norm(ctx, G.dd, copy, out);
+    case K_DF: return launch_norm(ctx, G.df, copy, out);
+    default: return launch_norm(ctx, G.ff, copy, out);
+  }
+}
+
+// pointer to one SoA field of a level and its element size
+int field_ptr(desalm_ctx* ctx, int n, int f, void** p, int* esz) {
+  Level& G = ctx->L[n];
+  Kind k = kind_of(ctx, n);
+  *esz = (k == K_FF) ? 4 : 8;
+  auto pick = [&](auto& L) -> int {
+    if (f >= DESALM_F_Q && f < DESALM_F_Q + 5) { *p = L.q[f - DESALM_F_Q]; return 0; }
+    if (f >= DESALM_F_QN && f < DESALM_F_QN + 5) { *p = L.qn[f - DESALM_F_QN]; return 0; }
+    if (f >= DESALM_F_QNM1 && f < DESALM_F_QNM1 + 5) { *p = L.qnm1[f - DESALM_F_QNM1]; return 0; }
+    if (f >= DESALM_F_QOLD && f < DESALM_F_QOLD + 5) { *p = L.qold[f - DESALM_F_QOLD]; return 0; }
+    if (f >= DESALM_F_RH && f < DESALM_F_RH + 4) { *p = L.rh[f - DESALM_F_RH]; return 0; }
+    if (f >= DESALM_F_PK && f < DESALM_F_PK + 4) { *p = L.pk[f - DESALM_F_PK]; return 0; }
+    if (f >= DESALM_F_CSI && f < DESALM_F_CSI + 3) { *p = (void*)L.csi[f - DESALM_F_CSI]; return 0; }
+    if (f >= DESALM_F_ETA && f < DESALM_F_ETA + 3) { *p = (void*)L.eta[f - DESALM_F_ETA]; return 0; }
+    if (f >= DESALM_F_ZET && f < DESALM_F_ZET + 3) { *p = (void*)L.zet[f - DESALM_F_ZET]; return 0; }
+    if (f == DESALM_F_AJ) { *p = (void*)L.aj; return 0; }
+    if (f == DESALM_F_NUT) { *p = L.nut; return 0; }
+    if (f == DESALM_F_DTAU) { *p = L.dtau; return 0; }
+    if (n == 0 && f == DESALM_F_DTEV) { *p = ctx->dtev; *esz = 8; return 0; }
+    if (n == 0 && f == DESALM_F_WD) { *p = ctx->wd; *esz = 8; return 0; }
+    if (n == 0 && f == DESALM_F_X) { *p = ctx->x; *esz = 8; return 0; }
+    if (n == 0 && f == DESALM_F_Y) { *p = ctx->y; *esz = 8; return 0; }
+    if (n == 0 && f == DESALM_F_Z) { *p = ctx->z; *esz = 8; return 0; }
+    ctx->err = "unknown field id for this level";
+    return DESALM_EINVAL;
+  };
+  if (k == K_DD) return pick(G.dd);
+  if (k == K_DF) return pick(G.df);
+  return pick(G.ff);
+}
+
+// Inflow extrapolation ratios on the host from the fine grid
+// (src/init.F90:2750-2891).  The k faces' guard in the reference
+// ('btype == 4 .and. btype == 5') is never true, so rat(:,:,5:6) are never
+// assigned there; they stay zero here.
+void outlet_ratios(const desalm_case& c, const double* x, const double* y, const double* z, std::vector<double>& rat, int rd) {
+  rat.assign((size_t)6 * rd * rd, 0.0);
+  const int im = c.im, jm = c.jm, km = c.km;
+  auto id = [&](int i, int j, int k) { return (long)(i - 1) + (long)im * ((j - 1) + (long)jm * (k - 1)); };
+  for (int b = 0; b < 4; ++b) {
+    if (!(c.btype[b] == 4 || c.btype[b] == 5)) continue;
+    int dir = c.bdir[b];
+    if (dir < 1 || dir > 3) continue;
+    const double* v = dir == 1 ? x : (dir == 2 ? y : z);
+    if (b < 2) {
+      for (int k = 1; k <= km; ++k)
+        for (int j = 1; j <= jm; ++j) {
+          double r;
+          if (b == 0) r = (v[id(2, j, k)] - v[id(1, j, k)]) / (v[id(3, j, k)] - v[id(2, j, k)]);
+          else r = (v[id(im, j, k)] - v[id(im - 1, j, k)]) / (v[id(im - 1, j, k)] - v[id(im - 2, j, k)]);
+          rat[(size_t)b * rd * rd + (j - 1) + (size_t)rd * (k - 1)] = r;
+        }
+    } else {
+      for (int k = 1; k <= km; ++k)
+        for (int i = 1; i <= im; ++i) {
+          double r;
+          if (b == 2) r = (v[id(i, 2, k)] - v[id(i, 1, k)]) / (v[id(i, 3, k)] - v[id(i, 2, k)]);
+          else r = (v[id(i, jm, k)] - v[id(i, jm - 1, k)]) / (v[id(i, jm - 1, k)] - v[id(i, jm - 2, k)]);
+          rat[(size_t)b * rd * rd + (i - 1) + (size_t)rd * (k - 1)] = r;
+        }
+    }
+  }
+}
+
+int pseudo_iter(desalm_ctx* ctx, desalm_step_report* rep);
+int sa_des_eddy(desalm_ctx* ctx);
+int sa_conservation(desalm_ctx* ctx);
+
+}  // namespace
+
+// =============================================================== C ABI
+extern "C" {
+
+const char* desalm_last_error(const desalm_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+void desalm_destroy(desalm_ctx* ctx) {
+  if (!ctx) return;
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto& G : ctx->L)
+    for (void* p : G.allocs) cudaFree(p);
+  for (void* p : ctx->allocs) cudaFree(p);
+  if (ctx->h_norm) cudaFreeHost(ctx->h_norm);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+int desalm_init(const desalm_case* c, desalm_ctx** out) {
+  if (!c || !out) return DESALM_EINVAL;
+  *out = nullptr;
+  desalm_ctx* ctx = new desalm_ctx();
+  int rc = check_case(ctx, *c);
+  if (rc) {
+    // keep the message reachable: return the context so desalm_last_error works
+    *out = ctx;
+    return rc;
+  }
+  ctx->c = *c;
+  ctx->ng = c->ng;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    ctx->err = std::string("no CUDA device: ") + cudaGetErrorString(e);
+    *out = ctx;
+    return DESALM_ECUDA;
+  }
+  e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    ctx->err = std::string("cudaStreamCreate: ") + cudaGetErrorString(e);
+    *out = ctx;
+    return DESALM_ECUDA;
+  }
+  fill_par(ctx);
+  ctx->L.resize(ctx->ng);
+  ctx->L[0].im = c->im; ctx->L[0].jm = c->jm; ctx->L[0].km = c->km;
+  for (int n = 1; n < ctx->ng; ++n) {
+    ctx->L[n].im = (ctx->L[n - 1].im + c->icrs) >> c->icrs;
+    ctx->L[n].jm = (ctx->L[n - 1].jm + c->jcrs) >> c->jcrs;
+    ctx->L[n].km = (ctx->L[n - 1].km + c->kcrs) >> c->kcrs;
+  }
+  rc = dalloc(ctx, ctx->allocs, (void**)&ctx->flags, 2 * sizeof(int));
+  if (rc) { *out = ctx; return rc; }
+  for (int n = 0; n < ctx->ng; ++n) {
+    Level& G = ctx->L[n];
+    G.N = (long)G.im * G.jm * G.km;
+    G.dc = 1.0 / std::pow(2.0, double(n * c->icrs));
+    G.de = 1.0 / std::pow(2.0, double(n * c->jcrs));
+    G.dz = 1.0 / std::pow(2.0, double(n * c->kcrs));
+    Kind k = kind_of(ctx, n);
+    if (k == K_DD) rc = alloc_level(ctx, G, G.dd);
+    else if (k == K_DF) rc = alloc_level(ctx, G, G.df);
+    else rc = alloc_level(ctx, G, G.ff);
+    if (rc) { *out = ctx; return rc; }
+    G.tbytes = k == K_FF ? 4 : 8;
+    G.wbytes = k == K_DD ? 8 : 4;
+    if (n + 1 < ctx->ng) {
+      rc = dalloc(ctx, G.allocs, &G.dq[0], (size_t)4 * G.N * G.tbytes);
+      if (rc) { *out = ctx; return rc; }
+      const int ext[3] = {G.im, G.jm, G.km};
+      for (int d = 0; d < 3; ++d) {
+        std::vector<double> fac, dpr;
+        rs_factors(ext[d] - 2, c->ep[1][d], fac, dpr);
+        rc = dalloc(ctx, G.allocs, (void**)&G.fac[d], fac.size() * sizeof(double));
+        if (!rc) rc = dalloc(ctx, G.allocs, (void**)&G.dpr[d], dpr.size() * sizeof(double));
+        if (rc) { *out = ctx; return rc; }
+        cudaMemcpyAsync(G.fac[d], fac.data(), fac.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+        cudaMemcpyAsync(G.dpr[d], dpr.data(), dpr.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+      }
+    }
+  }
+  const long NF = ctx->L[0].N;
+  auto A = [&](double** p, long n) { return dalloc(ctx, ctx->allocs, (void**)p, n * sizeof(double)); };
+  rc = A(&ctx->x, NF); if (!rc) rc = A(&ctx->y, NF); if (!rc) rc = A(&ctx->z, NF);
+  if (!rc) rc = A(&ctx->wd, NF);
+  if (!rc) rc = A(&ctx->dtev, NF);
+  for (int t = 0; t < 9 && !rc; ++t) rc = A(&ctx->cov[t], NF);
+  ctx->ratdim = std::max(c->im, std::max(c->jm, c->km));
+  if (!rc) rc = A(&ctx->rat, 6L * ctx->ratdim * ctx->ratdim);
+  if (!rc) rc = A(&ctx->pfix, 1);
+  ctx->part_blocks = 148 * 8;
+  if (!rc) rc = A(&ctx->part, 5L * ctx->part_blocks);
+  if (!rc) rc = A(&ctx->norm, 5);
+  if (!rc && c->turbulence)
+    for (int t = 0; t < SaWork::NARR && !rc; ++t) rc = A(&ctx->sa.a[t], NF);
+  if (rc) { *out = ctx; return rc; }
+  if (cudaMallocHost((void**)&ctx->h_norm, 5 * sizeof(double)) != cudaSuccess) {
+    ctx->err = "cudaMallocHost failed";
+    *out = ctx;
+    return DESALM_ENOMEM;
+  }
+  e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) {
+    ctx->err = std::string("init: ") + cudaGetErrorString(e);
+    *out = ctx;
+    return DESALM_ECUDA;
+  }
+  *out = ctx;
+  return 0;
+}
+
+int desalm_level_dims(const desalm_ctx* ctx, int n, int dims[3]) {
+  if (!ctx || n < 1 || n > ctx->ng) return DESALM_EINVAL;
+  dims[0] = ctx->L[n - 1].im; dims[1] = ctx->L[n - 1].jm; dims[2] = ctx->L[n - 1].km;
+  return 0;
+}
+
+int desalm_set_grid(desalm_ctx* ctx, const double* x, const double* y, const double* z, const double* wd) {
+  if (!ctx || !x || !y || !z) return DESALM_EINVAL;
+  if (ctx->L.empty()) return DESALM_ENOTREADY;
+  const desalm_case& c = ctx->c;
+  cudaStream_t s = ctx->stream;
+  const long NF = ctx->L[0].N;
+  CK(cudaMemcpyAsync(ctx->x, x, NF * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(ctx->y, y, NF * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(ctx->z, z, NF * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (wd) CK(cudaMemcpyAsync(ctx->wd, wd, NF * sizeof(double), cudaMemcpyHostToDevice, s));
+  else CK(cudaMemsetAsync(ctx->wd, 0, NF * sizeof(double), s));
+  // coordinates of every level (injection), metrics per level in FP64
+  double* xs[3] = {ctx->x, ctx->y, ctx->z};
+  std::vector<double*> lvl_xyz(3 * ctx->ng, nullptr);
+  for (int t = 0; t < 3; ++t) lvl_xyz[t] = xs[t];
+  std::vector<void*> tmp;
+  auto cleanup = [&]() { for (void* p : tmp) cudaFree(p); };
+  for (int n = 1; n < ctx->ng; ++n) {
+    Level& C = ctx->L[n];
+    Level& F = ctx->L[n - 1];
+    for (int t = 0; t < 3; ++t) {
+      double* p = nullptr;
+      if (cudaMalloc((void**)&p, C.N * sizeof(double)) != cudaSuccess) { cleanup(); ctx->err = "cudaMalloc"; return DESALM_ENOMEM; }
+      tmp.push_back(p);
+      k_inject<double, double><<<dim3(cdiv(C.im, 64), C.jm, C.km), 64, 0, s>>>(p, lvl_xyz[3 * (n - 1) + t], C.im, C.jm, C.km, F.im, F.jm,
+                                                                              c.icrs, c.jcrs, c.kcrs);
+      lvl_xyz[3 * n + t] = p;
+    }
+  }
+  for (int n = 0; n < ctx->ng; ++n) {
+    Level& G = ctx->L[n];
+    double* cov[9];
+    double* met[9];
+    double* aj = nullptr;
+    for (int t = 0; t < 9; ++t) {
+      if (n == 0) cov[t] = ctx->cov[t];
+      else {
+        if (cudaMalloc((void**)&cov[t], G.N * sizeof(double)) != cudaSuccess) { cleanup(); ctx->err = "cudaMalloc"; return DESALM_ENOMEM; }
+        tmp.push_back(cov[t]);
+      }
+    }
+    // metrics are computed in FP64; FP32 levels receive a converted copy
+    for (int t = 0; t < 10; ++t) {
+      double* p = nullptr;
+      if (cudaMalloc((void**)&p, G.N * sizeof(double)) != cudaSuccess) { cleanup(); ctx->err = "cudaMalloc"; return DESALM_ENOMEM; }
+      tmp.push_back(p);
+      if (t < 9) met[t] = p; else aj = p;
+    }
+    double** dcov = nullptr;
+    double** dmet = nullptr;
+    if (cudaMalloc((void**)&dcov, 9 * sizeof(double*)) != cudaSuccess || cudaMalloc((void**)&dmet, 9 * sizeof(double*)) != cudaSuccess) {
+      cleanup(); ctx->err = "cudaMalloc"; return DESALM_ENOMEM;
+    }
+    tmp.push_back(dcov); tmp.push_back(dmet);
+    CK(cudaMemcpyAsync(dcov, cov, 9 * sizeof(double*), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(dmet, met, 9 * sizeof(double*), cudaMemcpyHostToDevice, s));
+    k_metrics<<<dim3(cdiv(G.im, 64), G.jm, G.km), 64, 0, s>>>(lvl_xyz[3 * n], lvl_xyz[3 * n + 1], lvl_xyz[3 * n + 2], G.im, G.jm, G.km,
+                                                             G.dc, G.de, G.dz, dcov, dmet, aj);
+    CKL();
+    // copy into the level's typed arrays
+    void* dst[10];
+    int esz;
+    for (int d = 0; d < 3; ++d) {
+      RET(field_ptr(ctx, n, DESALM_F_CSI + d, &dst[d], &esz));
+      RET(field_ptr(ctx, n, DESALM_F_ETA + d, &dst[3 + d], &esz));
+      RET(field_ptr(ctx, n, DESALM_F_ZET + d, &dst[6 + d], &esz));
+    }
+    RET(field_ptr(ctx, n, DESALM_F_AJ, &dst[9], &esz));
+    for (int t = 0; t < 10; ++t) {
+      const double* src = t < 9 ? met[t] : aj;
+      if (esz == 8) CK(cudaMemcpyAsync(dst[t], src, G.N * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      else k_copy<float, double><<<cdiv(G.N, 256), 256, 0, s>>>((float*)dst[t], src, G.N);
+    }
+    CKL();
+    if (n == 0)
+      k_dtev<<<cdiv(G.N, 256), 256, 0, s>>>(dcov, ctx->dtev, G.N, c.cfl2, c.vnn2, c.ren, c.delti, c.unsteady);
+    CKL();
+    G.dtau_valid = false;
+    // the temporaries above are freed after the stream drains
+  }
+  std::vector<double> rat;
+  outlet_ratios(c, x, y, z, rat, ctx->ratdim);
+  CK(cudaMemcpyAsync(ctx->rat, rat.data(), rat.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  cudaError_t e = cudaStreamSynchronize(s);
+  cleanup();
+  if (e != cudaSuccess) {
+    ctx->err = std::string("set_grid: ") + cudaGetErrorString(e);
+    return DESALM_ECUDA;
+  }
+  ctx->have_grid = true;
+  return 0;
+}
+
+int desalm_set_state(desalm_ctx* ctx, const double* q, const double* qn, const double* qnm1, const double* nut) {
+  if (!ctx || !q) return DESALM_EINVAL;
+  cudaStream_t s = ctx->stream;
+  Level& G = ctx->L[0];
+  const long N = G.N;
+  double* h = nullptr;
+  double* d = nullptr;
+  CK(cudaMalloc((void**)&d, 5 * N * sizeof(double)));
+  const double* srcs[3] = {q, qn, qnm1};
+  const int fb[3] = {DESALM_F_Q, DESALM_F_QN, DESALM_F_QNM1};
+  int rc = 0;
+  for (int a = 0; a < 3 && !rc; ++a) {
+    void* dst[5];
+    int esz = 8;
+    for (int m = 0; m < 5; ++m) rc |= field_ptr(ctx, 0, fb[a] + m, &dst[m], &esz);
+    if (rc) break;
+    if (!srcs[a]) {
+      for (int m = 0; m < 5; ++m) cudaMemsetAsync(dst[m], 0, N * sizeof(double), s);
+      continue;
+    }
+    cudaMemcpyAsync(d, srcs[a], 5 * N * sizeof(double), cudaMemcpyHostToDevice, s);
+    double** dp = nullptr;
+    cudaMalloc((void**)&dp, 5 * sizeof(double*));
+    cudaMemcpyAsync(dp, dst, 5 * sizeof(double*), cudaMemcpyHostToDevice, s);
+    k_aos_to_soa<double><<<cdiv(N, 256), 256, 0, s>>>(dp, d, 5, N);
+    cudaStreamSynchronize(s);
+    cudaFree(dp);
+  }
+  void* dn;
+  int esz;
+  rc |= field_ptr(ctx, 0, DESALM_F_NUT, &dn, &esz);
+  if (!rc) {
+    if (nut) cudaMemcpyAsync(dn, nut, N * sizeof(double), cudaMemcpyHostToDevice, s);
+    else cudaMemsetAsync(dn, 0, N * sizeof(double), s);
+  }
+  (void)h;
+  cudaError_t e = cudaStreamSynchronize(s);
+  cudaFree(d);
+  if (rc) return rc;
+  if (e != cudaSuccess) {
+    ctx->err = std::string("set_state: ") + cudaGetErrorString(e);
+    return DESALM_ECUDA;
+  }
+  for (auto& L : ctx->L) L.dtau_valid = false;
+  ctx->have_state = true;
+  return 0;
+}
+
+int desalm_get_state(desalm_ctx* ctx, double* q, double* qn, double* qnm1, double* nut) {
+  if (!ctx) return DESALM_EINVAL;
+  cudaStream_t s = ctx->stream;
+  const long N = ctx->L[0].N;
+  double* d = nullptr;
+  CK(cudaMalloc((void**)&d, 5 * N * sizeof(double)));
+  double* dsts[3] = {q, qn, qnm1};
+  const int fb[3] = {DESALM_F_Q, DESALM_F_QN, DESALM_F_QNM1};
+  int rc = 0;
+  for (int a = 0; a < 3 && !rc; ++a) {
+    if (!dsts[a]) continue;
+    void* src[5];
+    int esz;
+    for (int m = 0; m < 5; ++m) rc |= field_ptr(ctx, 0, fb[a] + m, &src[m], &esz);
+    if (rc) break;
+    double** dp = nullptr;
+    cudaMalloc((void**)&dp, 5 * sizeof(double*));
+    cudaMemcpyAsync(dp, src, 5 * sizeof(double*), cudaMemcpyHostToDevice, s);
+    k_soa_to_aos<double><<<cdiv(N, 256), 256, 0, s>>>(d, dp, 5, N);
+    cudaMemcpyAsync(dsts[a], d, 5 * N * sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    cudaFree(dp);
+  }
+  if (nut && !rc) {
+    void* dn;
+    int esz;
+    rc = field_ptr(ctx, 0, DESALM_F_NUT, &dn, &esz);
+    if (!rc) cudaMemcpyAsync(nut, dn, N * sizeof(double), cudaMemcpyDeviceToHost, s);
+  }
+  cudaError_t e = cudaStreamSynchronize(s);
+  cudaFree(d);
+  if (rc) return rc;
+  if (e != cudaSuccess) {
+    ctx->err = std::string("get_state: ") + cudaGetErrorString(e);
+    return DESALM_ECUDA;
+  }
+  return 0;
+}
+
+int desalm_get_field(desalm_ctx* ctx, int n, int f, double* out) {
+  if (!ctx || !out || n < 1 || n > ctx->ng) return DESALM_EINVAL;
+  void* p;
+  int esz;
+  RET(field_ptr(ctx, n - 1, f, &p, &esz));
+  const long N = ctx->L[n - 1].N;
+  cudaStream_t s = ctx->stream;
+  if (esz == 8) {
+    CK(cudaMemcpyAsync(out, p, N * sizeof(double), cudaMemcpyDeviceToHost, s));
+  } else {
+    double* d = nullptr;
+    CK(cudaMalloc((void**)&d, N * sizeof(double)));
+    k_copy<double, float><<<cdiv(N, 256), 256, 0, s>>>(d, (const float*)p, N);
+    cudaMemcpyAsync(out, d, N * sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    cudaFree(d);
+  }
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+int desalm_set_field(desalm_ctx* ctx, int n, int f, const double* in) {
+  if (!ctx || !in || n < 1 || n > ctx->ng) return DESALM_EINVAL;
+  void* p;
+  int esz;
+  RET(field_ptr(ctx, n - 1, f, &p, &esz));
+  const long N = ctx->L[n - 1].N;
+  cudaStream_t s = ctx->stream;
+  if (esz == 8) {
+    CK(cudaMemcpyAsync(p, in, N * sizeof(double), cudaMemcpyHostToDevice, s));
+  } else {
+    double* d = nullptr;
+    CK(cudaMalloc((void**)&d, N * sizeof(double)));
+    cudaMemcpyAsync(d, in, N * sizeof(double), cudaMemcpyHostToDevice, s);
+    k_copy<float, double><<<cdiv(N, 256), 256, 0, s>>>((float*)p, d, N);
+    cudaStreamSynchronize(s);
+    cudaFree(d);
+  }
+  CK(cudaStreamSynchronize(s));
+  if (f == DESALM_F_NUT || (f >= DESALM_F_CSI && f <= DESALM_F_AJ)) ctx->L[n - 1].dtau_valid = false;
+  return 0;
+}
+
+int desalm_solver_daf(desalm_ctx* ctx, int n, int recalc, int itr) {
+  if (!ctx || n < 1 || n > ctx->ng) return DESALM_EINVAL;
+  if (!ctx->have_grid) { ctx->err = "grid not set"; return DESALM_ENOTREADY; }
+  RET(do_daf(ctx, n - 1, recalc, itr));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+int desalm_mg_nlevel(desalm_ctx* ctx, int n) {
+  if (!ctx || n < 2 || n > ctx->ng) return DESALM_EINVAL;
+  RET(do_nlevel(ctx, n - 1));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+int desalm_mg_prolong(desalm_ctx* ctx, int n) {
+  if (!ctx || n < 1 || n >= ctx->ng) return DESALM_EINVAL;
+  RET(do_prolong(ctx, n - 1));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+int desalm_mg_residual(desalm_ctx* ctx, int n, double res[5]) {
+  if (!ctx || !res || n < 1 || n > ctx->ng) return DESALM_EINVAL;
+  return do_norm(ctx, n - 1, 0, res);
+}
+
+int desalm_bcond_fm(desalm_ctx* ctx) {
+  if (!ctx) return DESALM_EINVAL;
+  RET(do_bcond(ctx));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+int desalm_des_eddy(desalm_ctx* ctx) {
+  if (!ctx) return DESALM_EINVAL;
+  if (!ctx->c.turbulence) { ctx->err = "des_eddy needs turbulence = 1"; return DESALM_EINVAL; }
+  RET(sa_des_eddy(ctx));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+int desalm_conservation(desalm_ctx* ctx) {
+  if (!ctx) return DESALM_EINVAL;
+  RET(sa_conservation(ctx));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+int desalm_save_qold(desalm_ctx* ctx) {
+  if (!ctx) return DESALM_EINVAL;
+  Level& G = ctx->L[0];
+  for (int m = 0; m < 5; ++m) {
+    void *src, *dst;
+    int esz;
+    RET(field_ptr(ctx, 0, DESALM_F_Q + m, &src, &esz));
+    RET(field_ptr(ctx, 0, DESALM_F_QOLD + m, &dst, &esz));
+    CK(cudaMemcpyAsync(dst, src, G.N * esz, cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+int desalm_begin_step(desalm_ctx* ctx) {
+  if (!ctx) return DESALM_EINVAL;
+  if (!ctx->have_grid || !ctx->have_state) { ctx->err = "grid or state not set"; return DESALM_ENOTREADY; }
+  const desalm_case& c = ctx->c;
+  cudaStream_t s = ctx->stream;
+  Level& F = ctx->L[0];
+  // qnm1 <- qn; qn <- q (src/mg_driver.F90:48-51)
+  for (int m = 0; m < 5; ++m) {
+    void *q, *qn, *qnm1;
+    int esz;
+    RET(field_ptr(ctx, 0, DESALM_F_Q + m, &q, &esz));
+    RET(field_ptr(ctx, 0, DESALM_F_QN + m, &qn, &esz));
+    RET(field_ptr(ctx, 0, DESALM_F_QNM1 + m, &qnm1, &esz));
+    CK(cudaMemcpyAsync(qnm1, qn, F.N * esz, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(qn, q, F.N * esz, cudaMemcpyDeviceToDevice, s));
+    if (c.predictor == DESALM_PRED_LINEAR)
+      k_extrapolate<double><<<cdiv(F.N, 256), 256, 0, s>>>((double*)q, (const double*)qn, (const double*)qnm1, F.N);
+  }
+  CKL();
+  // inject qn, qnm1 to the coarse levels (src/mg_driver.F90:55-58)
+  for (int n = 1; n < ctx->ng; ++n) {
+    Level& C = ctx->L[n];
+    Level& P = ctx->L[n - 1];
+    for (int a = 0; a < 2; ++a)
+      for (int m = 0; m < 5; ++m) {
+        int f = (a == 0 ? DESALM_F_QN : DESALM_F_QNM1) + m;
+        void *pf, *pc;
+        int ef, ec;
+        RET(field_ptr(ctx, n - 1, f, &pf, &ef));
+        RET(field_ptr(ctx, n, f, &pc, &ec));
+        dim3 g(cdiv(C.im, 64), C.jm, C.km);
+        if (ef == 8 && ec == 8)
+          k_inject<double, double><<<g, 64, 0, s>>>((double*)pc, (const double*)pf, C.im, C.jm, C.km, P.im, P.jm, c.icrs, c.jcrs, c.kcrs);
+        else if (ef == 8)
+          k_inject<double, float><<<g, 64, 0, s>>>((float*)pc, (const double*)pf, C.im, C.jm, C.km, P.im, P.jm, c.icrs, c.jcrs, c.kcrs);
+        else
+          k_inject<float, float><<<g, 64, 0, s>>>((float*)pc, (const float*)pf, C.im, C.jm, C.km, P.im, P.jm, c.icrs, c.jcrs, c.kcrs);
+      }
+  }
+  CKL();
+  if (c.conservation) RET(sa_conservation(ctx));
+  ctx->itc = 0;
+  RET(desalm_save_qold(ctx));
+  return 0;
+}
+
+int desalm_pseudo_iteration(desalm_ctx* ctx, desalm_step_report* rep) {
+  if (!ctx) return DESALM_EINVAL;
+  return pseudo_iter(ctx, rep);
+}
+
+int desalm_mg_driver(desalm_ctx* ctx, desalm_step_report* rep) {
+  if (!ctx) return DESALM_EINVAL;
+  RET(desalm_begin_step(ctx));
+  desalm_step_report r{};
+  int piv = 0;
+  for (int it = 1; it <= ctx->c.itmax; ++it) {
+    RET(pseudo_iter(ctx, &r));
+    piv += r.pivots;
+    if (r.converged) break;
+  }
+  r.pivots = piv;
+  if (rep) *rep = r;
+  return 0;
+}
+
+int desalm_sync(desalm_ctx* ctx) {
+  if (!ctx) return DESALM_EINVAL;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+}  // extern "C"
+
+namespace {
+
+// One pseudo-time iteration (src/mg_driver.F90:81-316).  qold_mg of the fine
+// level holds q at the start of the iteration (set by desalm_begin_step for
+// the first one and by the norm kernel of the previous one).
+int pseudo_iter(desalm_ctx* ctx, desalm_step_report* rep) {
+  const desalm_case& c = ctx->c;
+  ctx->itc++;
+  CK(cudaMemsetAsync(ctx->flags, 0, 2 * sizeof(int), ctx->stream));
+  int recalc = 0;
+  for (int n = 0; n < ctx->ng; ++n) {
+    if (n > 0) RET(do_nlevel(ctx, n));
+    for (int itr = 1; itr <= c.iter[n]; ++itr) {
+      // decide_recalc_rh keeps its last value on the coarsest level (Q5)
+      if (n != ctx->ng - 1) recalc = (itr != c.iter[n]) ? 0 : 1;
+      if (c.turbulence && n == 0) RET(sa_des_eddy(ctx));
+      // the recalculated residual on the coarsest level feeds nothing
+      int rc_eff = (n == ctx->ng - 1) ? 0 : recalc;
+      RET(do_daf(ctx, n, rc_eff, itr));
+    }
+  }
+  for (int n = ctx->ng - 2; n >= 0; --n) RET(do_prolong(ctx, n));
+  RET(do_bcond(ctx));
+  double res[5];
+  RET(do_norm(ctx, 0, 1, res));
+  int hflags[2] = {0, 0};
+  CK(cudaMemcpy(hflags, ctx->flags, 2 * sizeof(int), cudaMemcpyDeviceToHost));
+  if (ctx->itc == 1)
+    for (int m = 0; m < 5; ++m) ctx->init_resd[m] = res[m];
+  // mg_ck_conver (src/mg_driver.F90:372-398)
+  double eomax = std::max(res[1], std::max(res[2], res[3]));
+  double ermax = std::max(res[1] - ctx->init_resd[1], std::max(res[2] - ctx->init_resd[2], res[3] - ctx->init_resd[3]));
+  bool conv = false;
+  if (ctx->itc > c.it_min && ermax < c.er_min) conv = true;
+  if (ctx->itc > c.it_min && eomax < c.eo_min) conv = true;
+  if (rep) {
+    rep->iterations = ctx->itc;
+    rep->converged = conv ? 1 : 0;
+    for (int m = 0; m < 5; ++m) { rep->residual[m] = res[m]; rep->init_residual[m] = ctx->init_resd[m]; }
+    rep->pivots = hflags[0];
+  }
+  for (int m = 1; m < 4; ++m)
+    if (!std::isfinite(res[m])) { ctx->err = "non-finite convergence norm"; return DESALM_ENONFINITE; }
+  return 0;
+}
+
+}  // namespace
+
+namespace {
+int sa_des_eddy(desalm_ctx* ctx) {
+  ctx->err = "Spalart-Allmaras path not built yet";
+  return DESALM_EINVAL;
+}
+int sa_conservation(desalm_ctx* ctx) {
+  ctx->err = "conservation not built yet";
+  return DESALM_EINVAL;
+}
+}  // namespace

@@ -1,0 +1,269 @@
+// resid.cuh -- K_R: the momentum/continuity residual of one level, fused.
+//
+// One thread per interior node computes, in registers:
+//   U/J at the neighbours            src/rhs_contra_j.F90:14-29
+//   viscous face fluxes and visc     src/rhs_viscous.F90:103-329
+//   pressure dissipation diss(1)     src/rhs_diss_p.F90:33-203   (first pass)
+//   pressure gradient + divergence   src/rhs_flux_sans_convec.F90:44-136
+//   QUICK / first-order convection   src/rhs_convec_quick.F90:53-425
+//   BDF2 + assembly                  src/rhs_unst_visc_diss.F90:35-50
+//   FAS forcing (coarse levels)      src/rhs_pk.F90:35-67
+// and then either stores the raw residual (recalculation pass,
+// src/solver_daf.F90:432-477) or applies r = S (-dtau J rh) and r <- Ma^-1 r
+// (src/rhs_diag_solver.F90:53-122) and stores the transformed residual for
+// the line sweeps.  Nothing is staged through intermediate full-size arrays.
+#pragma once
+#include "modal.cuh"
+
+namespace desalm {
+
+// U/J of direction d at node l
+template <class T, class W>
+DESALM_DEV T ucn(const Lv<T, W>& L, int d, int l) {
+  const T* const* m = d == 0 ? L.csi : (d == 1 ? L.eta : L.zet);
+  T tmp = T(1) / L.aj[l];
+  return tmp * (m[0][l] * L.q[1][l] + m[1][l] * L.q[2][l] + m[2][l] * L.q[3][l]);
+}
+
+// Viscous flux through the face between l0 and l0 + st[dir]
+// (src/rhs_viscous.F90:112-163 for dir 0, :189-240 dir 1, :263-313 dir 2).
+template <class T, class W>
+DESALM_DEV void visc_face(const Lv<T, W>& L, int dir, int l0, T rei, T out[3]) {
+  const int sj = L.sj, sk = L.sk;
+  const T dc = L.dc, de = L.de, dz = L.dz;
+  const T q4 = T(0.25);
+  int l1;
+  T U[3], E[3], Z[3];
+  if (dir == 0) {
+    l1 = l0 + 1;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      const T* v = L.q[m + 1];
+      U[m] = dc * (v[l1] - v[l0]);
+      E[m] = (q4 * de) * (v[l1 + sj] - v[l1 - sj] + v[l0 + sj] - v[l0 - sj]);
+      Z[m] = (q4 * dz) * (v[l1 + sk] - v[l1 - sk] + v[l0 + sk] - v[l0 - sk]);
+    }
+  } else if (dir == 1) {
+    l1 = l0 + sj;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      const T* v = L.q[m + 1];
+      U[m] = (q4 * dc) * (v[l1 + 1] - v[l1 - 1] + v[l0 + 1] - v[l0 - 1]);
+      E[m] = de * (v[l1] - v[l0]);
+      Z[m] = (q4 * dz) * (v[l1 + sk] - v[l1 - sk] + v[l0 + sk] - v[l0 - sk]);
+    }
+  } else {
+    l1 = l0 + sk;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      const T* v = L.q[m + 1];
+      U[m] = (q4 * dc) * (v[l1 + 1] - v[l1 - 1] + v[l0 + 1] - v[l0 - 1]);
+      E[m] = (q4 * de) * (v[l1 + sj] - v[l1 - sj] + v[l0 + sj] - v[l0 - sj]);
+      Z[m] = dz * (v[l1] - v[l0]);
+    }
+  }
+  T a1 = L.csi[0][l1] + L.csi[0][l0], a2 = L.csi[1][l1] + L.csi[1][l0], a3 = L.csi[2][l1] + L.csi[2][l0];
+  T b1 = L.eta[0][l1] + L.eta[0][l0], b2 = L.eta[1][l1] + L.eta[1][l0], b3 = L.eta[2][l1] + L.eta[2][l0];
+  T c1 = L.zet[0][l1] + L.zet[0][l0], c2 = L.zet[1][l1] + L.zet[1][l0], c3 = L.zet[2][l1] + L.zet[2][l0];
+  T uu1 = a1 * U[0] + b1 * E[0] + c1 * Z[0], vv1 = a1 * U[1] + b1 * E[1] + c1 * Z[1], ww1 = a1 * U[2] + b1 * E[2] + c1 * Z[2];
+  T uu2 = a2 * U[0] + b2 * E[0] + c2 * Z[0], vv2 = a2 * U[1] + b2 * E[1] + c2 * Z[1], ww2 = a2 * U[2] + b2 * E[2] + c2 * Z[2];
+  T uu3 = a3 * U[0] + b3 * E[0] + c3 * Z[0], vv3 = a3 * U[1] + b3 * E[1] + c3 * Z[1], ww3 = a3 * U[2] + b3 * E[2] + c3 * Z[2];
+  T n1, n2, n3, k1, k2, k3;
+  if (dir == 0) {
+    n1 = a1; n2 = a2; n3 = a3;
+    k1 = a1 * a1 + a2 * a2 + a3 * a3; k2 = a1 * b1 + a2 * b2 + a3 * b3; k3 = a1 * c1 + a2 * c2 + a3 * c3;
+  } else if (dir == 1) {
+    n1 = b1; n2 = b2; n3 = b3;
+    k1 = b1 * a1 + b2 * a2 + b3 * a3; k2 = b1 * b1 + b2 * b2 + b3 * b3; k3 = b1 * c1 + b2 * c2 + b3 * c3;
+  } else {
+    n1 = c1; n2 = c2; n3 = c3;
+    k1 = c1 * a1 + c2 * a2 + c3 * a3; k2 = c1 * b1 + c2 * b2 + c3 * b3; k3 = c1 * c1 + c2 * c2 + c3 * c3;
+  }
+  T vtj = T(0.25) * ((rei + L.nut[l1]) + (rei + L.nut[l0])) / (L.aj[l1] + L.aj[l0]);
+  out[0] = vtj * (n1 * uu1 + n2 * vv1 + n3 * ww1 + k1 * U[0] + k2 * E[0] + k3 * Z[0]);
+  out[1] = vtj * (n1 * uu2 + n2 * vv2 + n3 * ww2 + k1 * U[1] + k2 * E[1] + k3 * Z[1]);
+  out[2] = vtj * (n1 * uu3 + n2 * vv3 + n3 * ww3 + k1 * U[2] + k2 * E[2] + k3 * Z[2]);
+}
+
+// Second difference of the pressure scaled by g_dd dtau / J at node l
+// (src/rhs_diss_p.F90:58-117).
+template <class T, class W>
+DESALM_DEV T diss_fv(const Lv<T, W>& L, int dir, int l, int st, T dsq) {
+  const T* const* m = dir == 0 ? L.csi : (dir == 1 ? L.eta : L.zet);
+  T g = m[0][l] * m[0][l] + m[1][l] * m[1][l] + m[2][l] * m[2][l];
+  T tmp1 = g * L.dtau[l] / L.aj[l];
+  const T* p = L.q[0];
+  T tmp2 = dsq * (p[l + st] - T(2) * p[l] + p[l - st]);
+  return tmp1 * tmp2;
+}
+
+// MODE 0: first pass of a DAF step; MODE 1: recalculation for restriction.
+template <class T, class W, int MODE>
+__global__ void __launch_bounds__(128) k_resid(Lv<T, W> L, Par P, int upwind, int calc_pk, int coarse, int bback) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int k = blockIdx.z + 1;
+  if (i > L.im - 2 || j > L.jm - 2) return;
+  const int sj = L.sj, sk = L.sk;
+  const int l = i + sj * j + sk * k;
+  const T rei = T(1) / T(P.ren);
+  const T dsp[3] = {L.dc, L.de, L.dz};
+  const int st[3] = {1, sj, sk};
+  const int pos[3] = {i, j, k};
+  const int ext[3] = {L.im, L.jm, L.km};
+
+  // ---- viscous terms
+  T visc[3];
+  {
+    T fp[3], fm[3];
+    visc_face(L, 0, l, rei, fp);
+    visc_face(L, 0, l - 1, rei, fm);
+#pragma unroll
+    for (int m = 0; m < 3; ++m) visc[m] = L.dc * (fp[m] - fm[m]);
+    visc_face(L, 1, l, rei, fp);
+    visc_face(L, 1, l - sj, rei, fm);
+#pragma unroll
+    for (int m = 0; m < 3; ++m) visc[m] = visc[m] + L.de * (fp[m] - fm[m]);
+    visc_face(L, 2, l, rei, fp);
+    visc_face(L, 2, l - sk, rei, fm);
+#pragma unroll
+    for (int m = 0; m < 3; ++m) visc[m] = visc[m] + L.dz * (fp[m] - fm[m]);
+  }
+
+  // ---- pressure dissipation (first pass only; the recalculation reuses it)
+  T diss1;
+  if (MODE == 0) {
+    T acc[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const T dsq = dsp[d] * dsp[d];
+      const int s = st[d];
+      // boundary copies fv(1) = fv(2), fv(m) = fv(m-1) (src/rhs_diss_p.F90:124-129)
+      T f0 = diss_fv(L, d, l, s, dsq);
+      T fmi = pos[d] - 1 == 0 ? f0 : diss_fv(L, d, l - s, s, dsq);
+      T fpl = pos[d] + 1 == ext[d] - 1 ? f0 : diss_fv(L, d, l + s, s, dsq);
+      acc[d] = fpl - T(2) * f0 + fmi;
+    }
+    diss1 = T(P.pdiss) * (acc[0] + acc[1] + acc[2]);
+    L.diss1[l] = diss1;
+  } else {
+    diss1 = L.diss1[l];
+  }
+
+  // ---- pressure gradient and divergence
+  T rh[4];
+  {
+    const T* p = L.q[0];
+    const T dh[3] = {T(0.5) * L.dc, T(0.5) * L.de, T(0.5) * L.dz};
+    const T* const* mt[3] = {L.csi, L.eta, L.zet};
+    T pp[3], pm[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      pp[d] = p[l + st[d]] / L.aj[l + st[d]];
+      pm[d] = p[l - st[d]] / L.aj[l - st[d]];
+    }
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+      T v = dh[0] * (pp[0] * mt[0][x][l + 1] - pm[0] * mt[0][x][l - 1]);
+      v = v + dh[1] * (pp[1] * mt[1][x][l + sj] - pm[1] * mt[1][x][l - sj]);
+      v = v + dh[2] * (pp[2] * mt[2][x][l + sk] - pm[2] * mt[2][x][l - sk]);
+      rh[x + 1] = v;
+    }
+    T dudx = dh[0] * (ucn(L, 0, l + 1) - ucn(L, 0, l - 1));
+    T dvdy = dh[1] * (ucn(L, 1, l + sj) - ucn(L, 1, l - sj));
+    T dwdz = dh[2] * (ucn(L, 2, l + sk) - ucn(L, 2, l - sk));
+    rh[0] = dudx + dvdy + dwdz;
+  }
+
+  // ---- convection
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int s = st[d];
+    const T h = dsp[d];
+    T ucon = T(0.5) * ucn(L, d, l);
+    T up = ucon + dabs(ucon), um = ucon - dabs(ucon);
+    bool first = (upwind == 1) || pos[d] == 1 || pos[d] == ext[d] - 2;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      const T* v = L.q[m + 1];
+      T f;
+      if (first) {
+        f = h * (up * (v[l] - v[l - s]) + um * (v[l + s] - v[l]));
+      } else {
+        f = T(0.125) * h * (up * (T(3) * v[l + s] + T(3) * v[l] - T(7) * v[l - s] + v[l - 2 * s]) +
+                            um * (-T(3) * v[l - s] - T(3) * v[l] + T(7) * v[l + s] - v[l + 2 * s]));
+      }
+      rh[m + 1] = rh[m + 1] + f;
+    }
+  }
+
+  // ---- unsteady terms, viscous and dissipation
+  {
+    T dtaj = T(2) * T(P.delti) * L.aj[l];
+    rh[0] = rh[0] + diss1;
+#pragma unroll
+    for (int m = 1; m < 4; ++m) {
+      T dq = T(P.es) * (T(3) * L.q[m][l] - T(4) * L.qn[m][l] + L.qnm1[m][l]) / dtaj;
+      rh[m] = rh[m] + T(0) + dq - visc[m - 1];
+    }
+  }
+
+  // ---- FAS forcing on coarse levels
+  if (coarse) {
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      T pk = L.pk[m][l];
+      if (MODE == 0 && calc_pk) {
+        pk = pk - rh[m];
+        L.pk[m][l] = pk;
+      }
+      rh[m] = rh[m] + pk;
+    }
+  }
+
+  if (MODE == 1) {
+#pragma unroll
+    for (int m = 0; m < 4; ++m) L.rh[m][l] = rh[m];
+    return;
+  }
+
+  // ---- r = S (-dtau rh J), then Ma^-1 r
+  const T dtau = L.dtau[l];
+  T alpha = T(1) + (T(P.es) * T(1.5) / T(P.delti)) * dtau;
+  T s[4] = {T(P.beta), T(1) / alpha, T(1) / alpha, T(1) / alpha};
+  T r[4];
+#pragma unroll
+  for (int m = 0; m < 4; ++m) r[m] = s[m] * (-dtau * rh[m] * L.aj[l]);
+  if (bback && (i == 1 || i == 2)) {
+    W* b = L.bi + (i - 1) * 4 * (L.jm * L.km);
+    const int o = j + L.jm * k;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) b[m * (L.jm * L.km) + o] = W(r[m]);
+  }
+  M4<T> A;
+  mat_mai(L, P, l, A);
+  T rp[4];
+  mv4(A, r, rp);
+#pragma unroll
+  for (int m = 0; m < 4; ++m) L.wk[m][l] = W(rp[m]);
+}
+
+// dtau on every node (src/rhs_daf_dtau.F90:85-117)
+template <class T, class W>
+__global__ void k_dtau(Lv<T, W> L, Par P) {
+  int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= L.N) return;
+  const T cfl = T(P.cfl1), vnn = T(P.vnn1), rei = T(1) / T(P.ren);
+  const T dcsq = L.dc * L.dc, desq = L.de * L.de, dzsq = L.dz * L.dz;
+  T g1 = L.csi[0][l] * L.csi[0][l] + L.csi[1][l] * L.csi[1][l] + L.csi[2][l] * L.csi[2][l];
+  T g2 = L.eta[0][l] * L.eta[0][l] + L.eta[1][l] * L.eta[1][l] + L.eta[2][l] * L.eta[2][l];
+  T g3 = L.zet[0][l] * L.zet[0][l] + L.zet[1][l] * L.zet[1][l] + L.zet[2][l] * L.zet[2][l];
+  T dti1 = cfl / sqrt(g1) / L.dc, dti2 = cfl / sqrt(g2) / L.de, dti3 = cfl / sqrt(g3) / L.dz;
+  T ret = rei + L.nut[l];
+  T dtv1 = vnn / ret / dcsq / g1, dtv2 = vnn / ret / desq / g2, dtv3 = vnn / ret / dzsq / g3;
+  T m = dti1;
+  m = dmin(m, dti2); m = dmin(m, dti3); m = dmin(m, dtv1); m = dmin(m, dtv2); m = dmin(m, dtv3);
+  L.dtau[l] = m;
+}
+
+}  // namespace desalm

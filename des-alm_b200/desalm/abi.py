@@ -1,0 +1,97 @@
+"""ctypes mirror of include/desalm.h (structs, constants, field ids).
+
+The C ABI is the product boundary; this module only describes it for Python
+callers (tests, bench, examples).  Field layouts follow the reference's
+Fortran arrays: q(1:5, i, j, k) with the component fastest, then i, j, k.
+"""
+import ctypes as C
+
+DESALM_OK = 0
+DESALM_EINVAL = -1
+DESALM_ENOMEM = -2
+DESALM_ECUDA = -3
+DESALM_ENONFINITE = -4
+DESALM_ESINGULAR = -5
+DESALM_ETIMEOUT = -6
+DESALM_ENOTREADY = -7
+
+FP64 = 0
+MIXED = 1
+PRED_QN = 0
+PRED_LINEAR = 1
+
+BC_INTERFACE, BC_WALL, BC_SYMMETRY, BC_FREESTREAM, BC_INFLOW, BC_PERIODIC = 0, 1, 2, 3, 4, 6
+
+F_Q, F_QN, F_QNM1, F_QOLD, F_RH, F_PK = 0, 8, 16, 24, 32, 40
+F_CSI, F_ETA, F_ZET, F_AJ, F_NUT, F_DTAU, F_DTEV, F_WD = 48, 52, 56, 60, 61, 62, 63, 64
+F_X, F_Y, F_Z = 65, 66, 67
+
+
+class Case(C.Structure):
+    _fields_ = [
+        ("im", C.c_int), ("jm", C.c_int), ("km", C.c_int),
+        ("ng", C.c_int),
+        ("icrs", C.c_int), ("jcrs", C.c_int), ("kcrs", C.c_int),
+        ("iter", C.c_int * 4),
+        ("itmax", C.c_int),
+        ("it_min", C.c_int),
+        ("er_min", C.c_double), ("eo_min", C.c_double),
+        ("delti", C.c_double),
+        ("ren", C.c_double), ("beta", C.c_double),
+        ("cfl1", C.c_double), ("vnn1", C.c_double),
+        ("cfl2", C.c_double), ("vnn2", C.c_double),
+        ("itk", C.c_int),
+        ("ep", (C.c_double * 3) * 2),
+        ("pdiss_coef", C.c_double),
+        ("btype", C.c_int * 6), ("bdir", C.c_int * 6),
+        ("ifix", C.c_int), ("jfix", C.c_int), ("kfix", C.c_int),
+        ("turbulence", C.c_int),
+        ("unsteady", C.c_int),
+        ("conservation", C.c_int),
+        ("precision_mode", C.c_int),
+        ("predictor", C.c_int),
+        ("use_graph", C.c_int),
+        ("reserved", C.c_int * 6),
+    ]
+
+    def copy(self):
+        c = Case()
+        C.pointer(c)[0] = self
+        return c
+
+    def as_dict(self):
+        d = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            if name == "ep":
+                v = [[v[a][b] for b in range(3)] for a in range(2)]
+            elif hasattr(v, "__len__"):
+                v = list(v)
+            d[name] = v
+        return d
+
+
+class StepReport(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int),
+        ("converged", C.c_int),
+        ("residual", C.c_double * 5),
+        ("init_residual", C.c_double * 5),
+        ("pivots", C.c_int),
+        ("reserved", C.c_int * 7),
+    ]
+
+    def as_dict(self):
+        return {"iterations": self.iterations, "converged": bool(self.converged),
+                "residual": list(self.residual), "init_residual": list(self.init_residual),
+                "pivots": self.pivots}
+
+
+def level_dims(case, n):
+    """Extents of level n (1-based): src/init.F90:257-263."""
+    im, jm, km = case.im, case.jm, case.km
+    for _ in range(1, n):
+        im = (im + case.icrs) // (2 ** case.icrs)
+        jm = (jm + case.jcrs) // (2 ** case.jcrs)
+        km = (km + case.kcrs) // (2 ** case.kcrs)
+    return im, jm, km

@@ -1,0 +1,232 @@
+"""Seeded synthetic cases with the shapes of the reference workloads.
+
+The reference ships no grids or solutions ('grid', 'solu' files are read at
+src/init.F90:2226-2243,2392-2411 but none are included), so every workload is
+generated here from numpy's default_rng(seed).  Each builder returns
+(case, grid, state) where grid = dict(x, y, z, wd) with arrays x(i,j,k)
+(i fastest, Fortran order) and state = dict(q, qn, qnm1, nut) with q(1:5,i,j,k).
+
+Presets
+  cavity   laminar lid-driven cavity, Re = 1000, unit cube with interior nodes
+           displaced by a seeded sinusoid of amplitude 0.02 h, 3-level FAS.
+  channel  SA RANS channel at Re_tau = 395: tanh wall-normal stretching (first
+           cell y+ ~ 1), nu_tilde = 3 nu, periodic i/k faces.
+  ogrid    O-grid around a circular cylinder (radial geometric stretching to
+           20 D, span pi D), SA, Re = 3900, delti = 0.005.
+"""
+import numpy as np
+
+from .abi import Case, BC_WALL, BC_INFLOW, BC_PERIODIC, BC_FREESTREAM, FP64, PRED_QN
+
+
+def _base_case(im, jm, km):
+    c = Case()
+    c.im, c.jm, c.km = im, jm, km
+    c.ng = 3
+    c.icrs = c.jcrs = c.kcrs = 1
+    for n, v in enumerate((1, 2, 3, 3)):
+        c.iter[n] = v
+    c.itmax = 200
+    c.it_min = 7
+    c.er_min = -6.0
+    c.eo_min = -14.0
+    c.delti = 0.05
+    c.ren = 1000.0
+    c.beta = 1.0
+    c.cfl1, c.vnn1 = 1.0, 0.1
+    c.cfl2, c.vnn2 = 0.5, 0.05
+    c.itk = 2
+    for d, v in enumerate((1.0, 2.5, 2.5)):
+        c.ep[0][d] = v
+    for d, v in enumerate((0.1, 0.2, 0.2)):
+        c.ep[1][d] = v
+    c.pdiss_coef = 0.1
+    for b in range(6):
+        c.btype[b] = BC_WALL
+    for b, v in enumerate((1, 1, 2, 2, 3, 3)):
+        c.bdir[b] = v
+    c.ifix = c.jfix = c.kfix = 1
+    c.turbulence = 0
+    c.unsteady = 1
+    c.conservation = 0
+    c.precision_mode = FP64
+    c.predictor = PRED_QN
+    c.use_graph = 0
+    return c
+
+
+def _mesh(xs, ys, zs):
+    """Fortran-order (i fastest) flattened coordinate arrays of a product grid."""
+    X = np.empty((len(zs), len(ys), len(xs)))
+    Y = np.empty_like(X)
+    Z = np.empty_like(X)
+    X[:] = xs[None, None, :]
+    Y[:] = ys[None, :, None]
+    Z[:] = zs[:, None, None]
+    return X, Y, Z
+
+
+def _flat(a):
+    return np.ascontiguousarray(a.reshape(-1), dtype=np.float64)
+
+
+def cavity(n=65, seed=0, re=1000.0, amp=0.02, ng=3, itmax=200):
+    """Lid-driven cavity on a perturbed unit cube (wall faces, lid at j = jm).
+
+    The lid is a btype-4 face holding u = 1 (bcond_fm only re-extrapolates the
+    pressure there, src/bcond_fm.F90:221-229); the other five faces are
+    no-slip walls.  Interior nodes move by amp * h * s(x,y,z) with s a product
+    of sines with seeded phases that vanishes on every face.
+    """
+    rng = np.random.default_rng(seed)
+    c = _base_case(n, n, n)
+    c.ng = ng
+    c.ren = re
+    c.itmax = itmax
+    c.btype[3] = BC_INFLOW
+    h = 1.0 / (n - 1)
+    s = np.linspace(0.0, 1.0, n)
+    X, Y, Z = _mesh(s, s, s)
+    bump = np.sin(np.pi * X) * np.sin(np.pi * Y) * np.sin(np.pi * Z)
+    ph = rng.uniform(0, 2 * np.pi, size=(3, 3))
+    wv = rng.integers(1, 4, size=(3, 3))
+    disp = []
+    for a in range(3):
+        w = (np.sin(wv[a, 0] * 2 * np.pi * X + ph[a, 0]) *
+             np.sin(wv[a, 1] * 2 * np.pi * Y + ph[a, 1]) *
+             np.sin(wv[a, 2] * 2 * np.pi * Z + ph[a, 2]))
+        disp.append(amp * h * bump * w)
+    X = X + disp[0]
+    Y = Y + disp[1]
+    Z = Z + disp[2]
+    grid = dict(x=_flat(X), y=_flat(Y), z=_flat(Z), wd=None)
+    N = n ** 3
+    q = np.zeros((N, 5))
+    q[:, 1:4] = rng.normal(0.0, 1e-3, size=(N, 3))
+    q = q.reshape(n, n, n, 5)          # [k][j][i][m]
+    # walls: zero velocity; lid (j = jm): u = 1, v = w = 0
+    for sl in [(slice(None), slice(None), 0), (slice(None), slice(None), -1),
+               (slice(None), 0, slice(None)), (0, slice(None), slice(None)),
+               (-1, slice(None), slice(None))]:
+        q[sl + (slice(1, 4),)] = 0.0
+    q[:, -1, :, 1] = 1.0
+    q[:, -1, :, 2:4] = 0.0
+    q = q.reshape(-1)
+    state = dict(q=q.copy(), qn=q.copy(), qnm1=q.copy(), nut=np.zeros(N))
+    return c, grid, state
+
+
+def _tanh_stretch(jm, first, length=2.0):
+    """Symmetric tanh clustering on [0, length] with first spacing ~ first."""
+    eta = np.linspace(0.0, 1.0, jm)
+
+    def ys(g):
+        return 0.5 * length * (1.0 - np.tanh(g * (1.0 - 2.0 * eta)) / np.tanh(g))
+
+    lo, hi = 1e-3, 10.0
+    for _ in range(200):
+        g = 0.5 * (lo + hi)
+        if ys(g)[1] > first:
+            lo = g
+        else:
+            hi = g
+    return ys(0.5 * (lo + hi))
+
+
+def _sa_fv1(nut_tilde, ren):
+    chi = nut_tilde * ren
+    chic = chi ** 3
+    return nut_tilde * chic / (chic + 357.911)
+
+
+def channel(im=129, jm=97, km=65, seed=0, re_tau=395.0, itmax=400):
+    """SA channel: i streamwise (2 pi), j wall-normal (walls at j = 1, jm),
+    k spanwise (pi); half height 1, bulk velocity ~ 1.  Re based on the half
+    height and bulk velocity (6875 for Re_tau = 395, Dean's correlation)."""
+    rng = np.random.default_rng(seed)
+    c = _base_case(im, jm, km)
+    re_b = 2.0 * (re_tau / 0.09) ** (1.0 / 0.88)   # Re_bulk on 2 delta
+    c.ren = 0.5 * re_b
+    c.turbulence = 1
+    c.itmax = itmax
+    c.delti = 0.02
+    c.btype[0] = c.btype[1] = BC_PERIODIC
+    c.btype[2] = c.btype[3] = BC_WALL
+    c.btype[4] = c.btype[5] = BC_PERIODIC
+    c.ifix, c.jfix, c.kfix = im // 2, jm // 2, km // 2
+    xs = np.linspace(0.0, 2 * np.pi, im)
+    zs = np.linspace(0.0, np.pi, km)
+    ys = _tanh_stretch(jm, 1.0 / re_tau)
+    X, Y, Z = _mesh(xs, ys, zs)
+    wd = np.minimum(Y, 2.0 - Y)
+    grid = dict(x=_flat(X), y=_flat(Y), z=_flat(Z), wd=_flat(wd))
+    N = im * jm * km
+    # mean profile: 1/7 power law with bulk ~ 1, plus seeded noise
+    u = (8.0 / 7.0) * np.clip(wd, 0.0, 1.0) ** (1.0 / 7.0)
+    q = np.zeros((km, jm, im, 5))
+    q[..., 1] = u
+    q[..., 1:4] += rng.normal(0.0, 1e-3, size=(km, jm, im, 3)) * (wd > 0)[..., None]
+    q[:, 0, :, 1:4] = 0.0
+    q[:, -1, :, 1:4] = 0.0
+    nu = 1.0 / c.ren
+    q[..., 4] = 3.0 * nu
+    q[:, 0, :, 4] = 1e-7
+    q[:, -1, :, 4] = 1e-7
+    q = q.reshape(-1)
+    nut = _sa_fv1(q[4::5], c.ren)
+    state = dict(q=q.copy(), qn=q.copy(), qnm1=q.copy(), nut=nut)
+    return c, grid, state
+
+
+def ogrid(im=257, jm=129, km=65, seed=0, re=3900.0, rfar=20.0, itmax=400):
+    """O-grid around a unit-diameter cylinder: i azimuthal (periodic faces),
+    j radial from the wall (j = 1) to a free-stream face at rfar diameters,
+    k spanwise over pi D; SA with nu_tilde = 3 nu; uniform free stream plus
+    seeded noise."""
+    rng = np.random.default_rng(seed)
+    c = _base_case(im, jm, km)
+    c.ren = re
+    c.turbulence = 1
+    c.itmax = itmax
+    c.delti = 0.005
+    c.btype[0] = c.btype[1] = BC_PERIODIC
+    c.btype[2] = BC_WALL
+    c.btype[3] = BC_FREESTREAM
+    c.btype[4] = c.btype[5] = BC_PERIODIC
+    c.ifix, c.jfix, c.kfix = 1, jm, 1
+    th = np.linspace(0.0, 2 * np.pi, im)
+    r0 = 0.5
+    first = 0.5 / np.sqrt(re) / 10.0
+    lo, hi = 1.0 + 1e-9, 2.0
+    for _ in range(200):  # geometric ratio with r(jm) = rfar
+        g = 0.5 * (lo + hi)
+        rend = r0 + first * (g ** (jm - 1) - 1.0) / (g - 1.0)
+        if rend > rfar:
+            hi = g
+        else:
+            lo = g
+    g = 0.5 * (lo + hi)
+    r = r0 + first * (g ** np.arange(jm) - 1.0) / (g - 1.0)
+    zs = np.linspace(0.0, np.pi, km)
+    TH = np.broadcast_to(th[None, None, :], (km, jm, im))
+    RR = np.broadcast_to(r[None, :, None], (km, jm, im))
+    ZZ = np.broadcast_to(zs[:, None, None], (km, jm, im))
+    X = RR * np.cos(TH)
+    Y = -RR * np.sin(TH)
+    wd = RR - r0
+    grid = dict(x=_flat(X), y=_flat(Y), z=_flat(ZZ), wd=_flat(wd))
+    N = im * jm * km
+    q = np.zeros((km, jm, im, 5))
+    ramp = np.clip((RR - r0) / 1.0, 0.0, 1.0)
+    q[..., 1] = ramp
+    q[..., 1:4] += rng.normal(0.0, 1e-3, size=(km, jm, im, 3)) * (ramp > 0)[..., None]
+    q[:, 0, :, 1:4] = 0.0
+    q[..., 4] = 3.0 / c.ren
+    q[:, 0, :, 4] = 1e-7
+    q = q.reshape(-1)
+    nut = _sa_fv1(q[4::5], c.ren)
+    state = dict(q=q.copy(), qn=q.copy(), qnm1=q.copy(), nut=nut)
+    return c, grid, state
+
+
+PRESETS = {"cavity": cavity, "channel": channel, "ogrid": ogrid}

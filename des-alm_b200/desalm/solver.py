@@ -1,0 +1,174 @@
+"""ctypes binding of libdesalm.so (the CUDA implementation of include/desalm.h).
+
+Solver mirrors the reference's subroutine chain (solver_daf, mg_nlevel,
+mg_prolong, mg_residual, bcond_fm, des_eddy, conservation, mg_driver) one
+method per C entry point.  There is no CPU fallback: constructing a Solver
+fails loudly when the library or a CUDA device is missing.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from .abi import Case, StepReport, level_dims
+
+PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_ROOT, "libdesalm.so")
+_LIB = None
+
+
+class DesalmError(RuntimeError):
+    pass
+
+
+def build(force=False):
+    """Compile libdesalm.so for sm_100a in place (make -C csrc)."""
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-s", "-C", os.path.join(PKG_ROOT, "csrc")], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise DesalmError("libdesalm.so is not built (run make -C des-alm_b200/csrc)")
+        L = C.CDLL(LIB_PATH)
+        vp, ip, dp = C.c_void_p, C.c_int, C.POINTER(C.c_double)
+        L.desalm_init.argtypes = [C.POINTER(Case), C.POINTER(vp)]
+        L.desalm_init.restype = C.c_int
+        L.desalm_destroy.argtypes = [vp]
+        L.desalm_destroy.restype = None
+        L.desalm_last_error.argtypes = [vp]
+        L.desalm_last_error.restype = C.c_char_p
+        for name, args in [
+            ("level_dims", [vp, ip, C.POINTER(C.c_int)]),
+            ("set_grid", [vp, dp, dp, dp, dp]),
+            ("set_state", [vp, dp, dp, dp, dp]),
+            ("get_state", [vp, dp, dp, dp, dp]),
+            ("get_field", [vp, ip, ip, dp]),
+            ("set_field", [vp, ip, ip, dp]),
+            ("solver_daf", [vp, ip, ip, ip]),
+            ("mg_nlevel", [vp, ip]),
+            ("mg_prolong", [vp, ip]),
+            ("mg_residual", [vp, ip, dp]),
+            ("bcond_fm", [vp]),
+            ("des_eddy", [vp]),
+            ("conservation", [vp]),
+            ("save_qold", [vp]),
+            ("begin_step", [vp]),
+            ("pseudo_iteration", [vp, C.POINTER(StepReport)]),
+            ("mg_driver", [vp, C.POINTER(StepReport)]),
+            ("sync", [vp]),
+        ]:
+            f = getattr(L, "desalm_" + name)
+            f.argtypes = args
+            f.restype = C.c_int
+        _LIB = L
+    return _LIB
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _f64(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Solver:
+    """One device context (one block, one GPU) of the pseudo-time iteration."""
+
+    def __init__(self, case):
+        self.case = case.copy()
+        self.L = lib()
+        self.ctx = C.c_void_p()
+        rc = self.L.desalm_init(C.byref(self.case), C.byref(self.ctx))
+        if rc:
+            msg = self.L.desalm_last_error(self.ctx).decode() if self.ctx.value else ""
+            if self.ctx.value:
+                self.L.desalm_destroy(self.ctx)
+                self.ctx = C.c_void_p()
+            raise DesalmError("desalm_init failed (%d): %s" % (rc, msg))
+
+    def close(self):
+        if getattr(self, "ctx", None) is not None and self.ctx.value:
+            self.L.desalm_destroy(self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+    def _ck(self, rc, what):
+        if rc:
+            raise DesalmError("%s failed (%d): %s" % (what, rc, self.L.desalm_last_error(self.ctx).decode()))
+
+    def dims(self, n):
+        return level_dims(self.case, n)
+
+    def set_grid(self, x, y, z, wd=None):
+        x, y, z, wd = map(_f64, (x, y, z, wd))
+        self._ck(self.L.desalm_set_grid(self.ctx, _p(x), _p(y), _p(z), _p(wd)), "set_grid")
+
+    def set_state(self, q, qn=None, qnm1=None, nut=None):
+        q, qn, qnm1, nut = map(_f64, (q, qn, qnm1, nut))
+        self._ck(self.L.desalm_set_state(self.ctx, _p(q), _p(qn), _p(qnm1), _p(nut)), "set_state")
+
+    def get_state(self):
+        N = self.case.im * self.case.jm * self.case.km
+        q, qn, qnm1, nut = (np.zeros(5 * N), np.zeros(5 * N), np.zeros(5 * N), np.zeros(N))
+        self._ck(self.L.desalm_get_state(self.ctx, _p(q), _p(qn), _p(qnm1), _p(nut)), "get_state")
+        return dict(q=q, qn=qn, qnm1=qnm1, nut=nut)
+
+    def get_field(self, n, f):
+        im, jm, km = self.dims(n)
+        out = np.zeros(im * jm * km)
+        self._ck(self.L.desalm_get_field(self.ctx, n, f, _p(out)), "get_field")
+        return out
+
+    def set_field(self, n, f, v):
+        v = _f64(v)
+        self._ck(self.L.desalm_set_field(self.ctx, n, f, _p(v)), "set_field")
+
+    def solver_daf(self, n, recalc, itr):
+        self._ck(self.L.desalm_solver_daf(self.ctx, n, recalc, itr), "solver_daf")
+
+    def mg_nlevel(self, n):
+        self._ck(self.L.desalm_mg_nlevel(self.ctx, n), "mg_nlevel")
+
+    def mg_prolong(self, n):
+        self._ck(self.L.desalm_mg_prolong(self.ctx, n), "mg_prolong")
+
+    def mg_residual(self, n):
+        r = np.zeros(5)
+        self._ck(self.L.desalm_mg_residual(self.ctx, n, _p(r)), "mg_residual")
+        return r
+
+    def bcond_fm(self):
+        self._ck(self.L.desalm_bcond_fm(self.ctx), "bcond_fm")
+
+    def des_eddy(self):
+        self._ck(self.L.desalm_des_eddy(self.ctx), "des_eddy")
+
+    def conservation(self):
+        self._ck(self.L.desalm_conservation(self.ctx), "conservation")
+
+    def save_qold(self):
+        self._ck(self.L.desalm_save_qold(self.ctx), "save_qold")
+
+    def begin_step(self):
+        self._ck(self.L.desalm_begin_step(self.ctx), "begin_step")
+
+    def pseudo_iteration(self):
+        rep = StepReport()
+        self._ck(self.L.desalm_pseudo_iteration(self.ctx, C.byref(rep)), "pseudo_iteration")
+        return rep.as_dict()
+
+    def mg_driver(self):
+        rep = StepReport()
+        self._ck(self.L.desalm_mg_driver(self.ctx, C.byref(rep)), "mg_driver")
+        return rep.as_dict()
+
+    def sync(self):
+        self._ck(self.L.desalm_sync(self.ctx), "sync")

@@ -1,0 +1,183 @@
+/*
+ * desalm.h -- C ABI of the B200 pseudo-time iteration (RHS residual, diagonal
+ * approximate-factorisation smoother, FAS multigrid V-cycle, Spalart-Allmaras
+ * sub-iterations) of the DES-ALM artificial-compressibility solver.
+ *
+ * Every entry point replaces one subroutine of the reference's mg_driver call
+ * chain (src/mg_driver.F90).  The reference passes Fortran explicit-shape
+ * arrays q(1:me, il:iu, jl:ju, kl:ku) (component fastest, then i, j, k); the
+ * host arrays of this ABI use exactly that layout, so a Fortran caller passes
+ * its own arrays through ISO_C_BINDING without a copy.  On the device the
+ * library keeps one structure-of-arrays block per multigrid level.
+ *
+ * All functions return 0 on success or a negative DESALM_E* status.  Calls on
+ * one context are ordered on the context's CUDA stream and are not thread safe;
+ * independent contexts are.  desalm_last_error() returns a message for the last
+ * failure on a context.
+ *
+ * The same symbols with the prefix desalm_oracle_ are exported by the CPU
+ * restatement used as the test oracle (oracle/); it is not part of the product.
+ */
+#ifndef DESALM_H
+#define DESALM_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DESALM_ABI_VERSION 1
+
+/* status codes */
+#define DESALM_OK          0
+#define DESALM_EINVAL     -1   /* bad argument or unsupported case setting      */
+#define DESALM_ENOMEM     -2   /* device or host allocation failed              */
+#define DESALM_ECUDA      -3   /* CUDA runtime error                            */
+#define DESALM_ENONFINITE -4   /* NaN/Inf in the convergence norm               */
+#define DESALM_ESINGULAR  -5   /* zero pivot in a line solve                    */
+#define DESALM_ETIMEOUT   -6   /* bounded device wait gave up                   */
+#define DESALM_ENOTREADY  -7   /* grid or state not bound yet                   */
+
+/* precision_mode */
+#define DESALM_FP64   0        /* everything in FP64                            */
+#define DESALM_MIXED  1        /* FP64 residual/update, FP32 DAF sweeps and
+                                  FP32 coarse-grid levels                       */
+/* predictor: initial guess of q^{n+1} for the pseudo-time loop */
+#define DESALM_PRED_QN      0  /* q^n, as src/mg_driver.F90:50-51              */
+#define DESALM_PRED_LINEAR  1  /* 2 q^n - q^{n-1}                               */
+
+/* boundary types, as documented at the end of ind3dmg.dat (nbtype) */
+#define DESALM_BC_INTERFACE 0
+#define DESALM_BC_WALL      1
+#define DESALM_BC_SYMMETRY  2
+#define DESALM_BC_FREESTREAM 3
+#define DESALM_BC_INFLOW    4
+#define DESALM_BC_PERIODIC  6
+
+/* Case description: the part of ind3dmg.dat (read in src/init.F90:176-236)
+ * and of the compile-time switches (src/global.F90, src/global_param.F90)
+ * that the pseudo-time iteration uses.  Sizes are node counts including the
+ * boundary nodes (one block, one rank: no ghost layers). */
+typedef struct desalm_case {
+    int    im, jm, km;      /* fine-grid nodes: img(1), jmg(1), kmg(1)         */
+    int    ng;              /* multigrid levels, 1..4 (ng in src/global.F90)    */
+    int    icrs, jcrs, kcrs;/* 1 = full coarsening in that direction, 0 = none  */
+    int    iter[4];         /* smoothing iterations per level: iter(n)          */
+    int    itmax;           /* itm(1): pseudo-iterations per physical step      */
+    int    it_min;          /* minimum pseudo-iterations before convergence     */
+    double er_min, eo_min;  /* log10 drop / absolute tolerances                 */
+    double delti;           /* physical time step                               */
+    double ren, beta;       /* Reynolds number, artificial compressibility      */
+    double cfl1, vnn1;      /* local pseudo-time step limits (mean flow)        */
+    double cfl2, vnn2;      /* local pseudo-time step limits (turbulence)       */
+    int    itk;             /* SA sub-iterations per call                       */
+    double ep[2][3];        /* ep(1,:) DAF implicit smoothing, ep(2,:) prolongation smoothing */
+    double pdiss_coef;      /* pressure dissipation coefficient                 */
+    int    btype[6], bdir[6];
+    int    ifix, jfix, kfix;/* 1-based pressure reference node                  */
+    int    turbulence;      /* 0: laminar (nu_t = 0); 1: Spalart-Allmaras       */
+    int    unsteady;        /* e_source = 1 (BDF2 physical time terms) or 0     */
+    int    conservation;    /* 1: outlet mass-flux fix once per physical step   */
+    int    precision_mode;  /* DESALM_FP64 or DESALM_MIXED                      */
+    int    predictor;       /* DESALM_PRED_*                                    */
+    int    use_graph;       /* 1: replay each pseudo-iteration as a CUDA graph  */
+    int    reserved[6];
+} desalm_case;
+
+/* Outcome of one physical time step (desalm_mg_driver). */
+typedef struct desalm_step_report {
+    int    iterations;      /* pseudo-iterations taken (itc)                    */
+    int    converged;       /* 1 if the mg_ck_conver test passed                */
+    double residual[5];     /* last log10 mean |q - q_old| per field            */
+    double init_residual[5];/* first-iteration values (init_resd)               */
+    int    pivots;          /* line-solve rows where partial pivoting would swap */
+    int    reserved[7];
+} desalm_step_report;
+
+/* fields for desalm_get_field / desalm_set_field (SoA, one level) */
+enum desalm_field {
+    DESALM_F_Q = 0,        /* +m, m = 0..4 (p, u, v, w, nu_tilde)               */
+    DESALM_F_QN = 8,       /* +m                                               */
+    DESALM_F_QNM1 = 16,    /* +m                                               */
+    DESALM_F_QOLD = 24,    /* +m  (qold_mg)                                    */
+    DESALM_F_RH = 32,      /* +m, m = 0..3                                     */
+    DESALM_F_PK = 40,      /* +m, m = 0..3                                     */
+    DESALM_F_CSI = 48,     /* +d, d = 0..2                                     */
+    DESALM_F_ETA = 52,
+    DESALM_F_ZET = 56,
+    DESALM_F_AJ = 60,
+    DESALM_F_NUT = 61,
+    DESALM_F_DTAU = 62,
+    DESALM_F_DTEV = 63,
+    DESALM_F_WD = 64,
+    DESALM_F_X = 65, DESALM_F_Y = 66, DESALM_F_Z = 67
+};
+
+typedef struct desalm_ctx desalm_ctx;
+
+/* Context life cycle.  Replaces init_mg / init_daf_bc (src/init.F90:1025,439):
+ * validates the case and allocates every level's device arrays once. */
+int  desalm_init(const desalm_case* c, desalm_ctx** out);
+void desalm_destroy(desalm_ctx* ctx);
+const char* desalm_last_error(const desalm_ctx* ctx);
+/* Level extents (1-based level n): writes im, jm, km. */
+int  desalm_level_dims(const desalm_ctx* ctx, int n, int dims[3]);
+
+/* Fine-grid coordinates x(i,j,k), y, z (i fastest) and the wall distance
+ * (nullable; needed for SA).  Injects the grid to the coarse levels
+ * (src/mg_inject.F90:26-62), computes metrics and Jacobians on every level
+ * (src/mg_metrics.F90:56-250), the SA pseudo-time step dtev
+ * (src/mg_metrics.F90:262-282) and the inflow extrapolation ratios rat
+ * (src/init.F90:2750-2891). */
+int  desalm_set_grid(desalm_ctx* ctx, const double* x, const double* y,
+                     const double* z, const double* wd);
+
+/* Fine-level state in the reference's layout q(1:5, i, j, k) (src/global.F90:62);
+ * nut is xnut(i,j,k).  qn/qnm1/nut may be NULL (then zero).  Replaces the
+ * 'solu' reader (src/init.F90:2392-2411). */
+int  desalm_set_state(desalm_ctx* ctx, const double* q, const double* qn,
+                      const double* qnm1, const double* nut);
+int  desalm_get_state(desalm_ctx* ctx, double* q, double* qn, double* qnm1,
+                      double* nut);
+
+/* One SoA field of one level (values converted to/from double). */
+int  desalm_get_field(desalm_ctx* ctx, int n, int field, double* out);
+int  desalm_set_field(desalm_ctx* ctx, int n, int field, const double* in);
+
+/* One DAF smoother step on level n: src/solver_daf.F90:2-488
+ * (solver_daf(me, n, decide_recalc_rh, itr, ...)). */
+int  desalm_solver_daf(desalm_ctx* ctx, int n, int recalc, int itr);
+/* FAS restriction + injection to level n, then mg_zero_pk_boundary:
+ * src/mg_nlevel.F90:2-146 and src/mg_driver.F90:134,407-466. */
+int  desalm_mg_nlevel(desalm_ctx* ctx, int n);
+/* Coarse-grid correction from level n+1 to level n: src/mg_prolong.F90:2-277
+ * with src/rsmooth.F90:7-95 and src/rs_sweep.F90:111-291. */
+int  desalm_mg_prolong(desalm_ctx* ctx, int n);
+/* log10 of mean |q - qold_mg| per field over interior nodes of level n:
+ * src/mg_residual.F90:2-84. */
+int  desalm_mg_residual(desalm_ctx* ctx, int n, double res[5]);
+/* Fine-grid boundary conditions and pressure fix: src/bcond_fm.F90:2-322. */
+int  desalm_bcond_fm(desalm_ctx* ctx);
+/* Spalart-Allmaras sub-iterations on the fine level: src/des_eddy.F90:2-297. */
+int  desalm_des_eddy(desalm_ctx* ctx);
+/* Outlet mass-flux correction: src/conservation.F90:2-162. */
+int  desalm_conservation(desalm_ctx* ctx);
+/* qold_mg <- q on the fine level (src/mg_driver.F90:98-100). */
+int  desalm_save_qold(desalm_ctx* ctx);
+/* Start of a physical time step (src/mg_driver.F90:42-75): qnm1 <- qn,
+ * qn <- q, the predictor's initial guess, injection of qn/qnm1 to the coarse
+ * levels, the optional mass-flux fix, and qold_mg <- q. */
+int  desalm_begin_step(desalm_ctx* ctx);
+/* One physical time step: src/mg_driver.F90:2-323 (history shift, coarse
+ * injection of qn/qnm1, predictor, optional conservation, pseudo-time loop
+ * with down-leg V-cycle, prolongation, bcond_fm and mg_ck_conver). */
+int  desalm_mg_driver(desalm_ctx* ctx, desalm_step_report* rep);
+/* One pseudo-time iteration of the loop above (for callers that drive the
+ * loop themselves); rep->residual receives the iteration's residual. */
+int  desalm_pseudo_iteration(desalm_ctx* ctx, desalm_step_report* rep);
+/* Wait for all work on the context's stream. */
+int  desalm_sync(desalm_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DESALM_H */
