@@ -1,0 +1,359 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 pseudo-time iteration: wall-seconds per physical time
+step (dual time stepping to a 1e-6 drop of the pseudo-time update, capped at
+the case's itmax), one replica per GPU.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--case channel|cavity]
+                  [--impl ours|reference]
+
+ours:       value = device-timed seconds per physical step of the product
+            configuration (MIXED precision: FP64 residual/update, FP32 line
+            sweeps and coarse levels; linear-extrapolation initial guess),
+            state resident in HBM.  e2e = the same step through the C ABI with
+            the state copied from pinned host memory and back every step.
+            The plain FP64 path (q^n guess, as the reference) is timed too.
+reference:  the CPU oracle (C++ restatement of the reference, FP32 like the
+            reference's own build, one thread) on the same case; a bounded
+            sample of pseudo-iterations scaled to one physical step.
+
+Under torchrun each rank runs an independent replica on its own GPU
+(the path does not shard: no collective in the data path); times are the max
+over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "des-alm_b200"))
+
+from desalm import abi, cases  # noqa: E402
+
+METRIC = "wall-s per physical step to 1e-6 residual drop: learned+mixed vs plain FP64 GPU"
+UNIT = "s/step"
+
+# Algorithmic bytes per interior node of each kernel class: every distinct
+# array element the kernel must read or write once, at its stored precision
+# (T = state bytes, W = line-sweep work bytes).  Halo re-reads and the
+# line-solve scratch are not algorithmic.
+def alg_bytes(kind, T, W, coarse):
+    pk = 4 * T if coarse else 0
+    return {
+        "resid": 23 * T + 4 * W + pk,     # q4 qn3 qnm1-3 metrics9 aj nut dtau | wk4 diss1
+        "recalc": 26 * T + pk,            # q4 qn3 qnm1-3 metrics9 aj nut diss1 | rh4
+        "sweep_i": 8 * W + 7 * T,         # wk4 in/out, dtau, csi3, eta3
+        "sweep_j": 8 * W + 7 * T,         # wk4 in/out, dtau, eta3, zet3
+        "sweep_k": 4 * W + 12 * T,        # wk4, dtau, zet3, q4 in/out
+        "dtau": 11 * T,                   # metrics9 nut | dtau
+        "norm": 15 * T,                   # q5 qold5 | qold5
+        "rsmooth": 8 * T,                 # dq4 in/out (last one: q4 in/out instead)
+        "prolong": 4 * T,                 # dq4 out (coarse reads amortised)
+        "sa_rhs": 18 * 8,                 # q2..5, qn5 qnm1-5, metrics9, aj, wd, dtev | rh
+        "sa_sweep": 10 * 8,               # rh in/out, q5, u v w (U/J), metrics3, aj, dtev
+    }.get(kind)
+
+
+def build_case(name, precision, predictor):
+    if name == "cavity":
+        case, grid, state = cases.cavity(n=65, itmax=200)
+        desc = "laminar lid-driven cavity Re=1000, 65^3 perturbed cube, 3-level FAS, 200 pseudo-iterations/step"
+    elif name == "channel":
+        case, grid, state = cases.channel()
+        desc = "SA RANS channel Re_tau=395, 129x97x65 tanh-stretched, periodic i/k, 3-level FAS"
+    else:
+        raise SystemExit("unknown case " + name)
+    case.precision_mode = precision
+    case.predictor = predictor
+    return case, grid, state, desc
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        out, _ = self.p.communicate(timeout=10)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def run_ours(args, rank, world, dist):
+    import torch
+    from desalm.solver import Solver
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    torch.cuda.init()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def timed_steps(S, K, body):
+        """K calls of body(), bracketed by barrier + synchronize, CUDA events
+        on the library's stream; returns seconds per call (max over ranks)."""
+        stream = torch.cuda.ExternalStream(S.stream())
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        S.sync()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        reps = []
+        for _ in range(K):
+            reps.append(body())
+        e1.record(stream)
+        S.sync()
+        torch.cuda.synchronize()
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1) / 1e3 / K), reps
+
+    # ---- product configuration: MIXED + linear extrapolation
+    case, grid, state, desc = build_case(args.case, abi.MIXED, abi.PRED_LINEAR)
+    nint = (case.im - 2) * (case.jm - 2) * (case.km - 2)
+    S = Solver(case)
+    S.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
+    S.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
+    for _ in range(args.warmup):
+        S.mg_driver()
+    clk = Clocks(dev)
+    clk.start()
+    S.profile(False)
+    S.profile(False)  # resets the launch counter
+    sec, reps = timed_steps(S, args.steps, S.mg_driver)
+    clocks = clk.stop()
+    _, launches = S.kernel_stats()
+    iters = [r["iterations"] for r in reps]
+    conv = [r["converged"] for r in reps]
+
+    # ---- e2e through the C ABI with host buffers (pinned), H2D + D2H per step
+    N = case.im * case.jm * case.km
+    pin = lambda n: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    hq, hqn, hqnm1, hnut = pin(5 * N), pin(5 * N), pin(5 * N), pin(N)
+    st = S.get_state()
+    hq[:], hqn[:], hqnm1[:], hnut[:] = st["q"], st["qn"], st["qnm1"], st["nut"]
+    import ctypes as C
+    L = S.L
+    P = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+
+    def e2e_step():
+        S._ck(L.desalm_set_state(S.ctx, P(hq), P(hqn), P(hqnm1), P(hnut)), "set_state")
+        r = S.mg_driver()
+        S._ck(L.desalm_get_state(S.ctx, P(hq), P(hqn), P(hqnm1), P(hnut)), "get_state")
+        return r
+
+    e2e_sec, _ = timed_steps(S, args.steps, e2e_step)
+    h2d = (3 * 5 * N + N) * 8
+    d2h = (3 * 5 * N + N) * 8
+
+    # ---- per-kernel CUDA-event timing over the same workload (roofline)
+    S.profile(True)
+    for _ in range(args.steps):
+        S.mg_driver()
+    stats, _ = S.kernel_stats()
+    S.profile(False)
+    T = {1: 8, 2: 4, 3: 4, 4: 4}
+    W = {1: 4, 2: 4, 3: 4, 4: 4}
+    best = None
+    for kind, per in stats.items():
+        ms = sum(v[0] for v in per.values())
+        if best is None or ms > best[1]:
+            best = (kind, ms, per)
+    kind, ms_tot, per = best
+    byts, nlaunch, ms_sum = 0.0, 0, 0.0
+    for lvl, (ms, nl, nodes) in per.items():
+        b = alg_bytes(kind, T[lvl], W[lvl], lvl > 1)
+        byts += (b or 0) * nodes
+        nlaunch += nl
+        ms_sum += ms
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = byts / (ms_sum / 1e3) / 1e9 if ms_sum > 0 else 0.0
+    share = {k: round(sum(v[0] for v in p.values()) / max(1e-9, sum(sum(w[0] for w in q.values()) for q in stats.values())), 4)
+             for k, p in stats.items()}
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tfile):
+        tt = json.load(open(tfile)).get(args.case, {}).get(kind)
+        traffic = tt
+    del S
+
+    # ---- plain FP64 GPU path (q^n guess, as the reference's mg_driver)
+    case64, grid, state, _ = build_case(args.case, abi.FP64, abi.PRED_QN)
+    S64 = Solver(case64)
+    S64.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
+    S64.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
+    for _ in range(args.warmup):
+        S64.mg_driver()
+    sec64, reps64 = timed_steps(S64, args.steps, S64.mg_driver)
+    iters64 = [r["iterations"] for r in reps64]
+    del S64
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(args.case, max(1, int(np.mean(iters64))))
+
+    cell_updates = nint * float(np.mean(iters)) / sec
+    out = {
+        "metric": METRIC, "value": sec, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
+        "data": "synthetic (seeded numpy generator; the reference ships no grids or solutions)",
+        "impl": "ours",
+        "config": {"workload": desc, "case": args.case, "grid": [case.im, case.jm, case.km],
+                   "interior_nodes": nint, "precision": "mixed (FP64 residual/update, FP32 sweeps + coarse levels)",
+                   "predictor": "linear extrapolation", "learned_predictor": "not built",
+                   "pseudo_iterations_per_step": iters, "converged": conv,
+                   "l2": "working set of every level > 126 MB L2 for the channel; no flush between steps",
+                   "parallelism": "replicas only (%d independent replicas)" % world},
+        "fp64_plain": {"value": sec64, "unit": UNIT, "pseudo_iterations_per_step": iters64,
+                       "speedup_mixed_vs_fp64": sec64 / sec},
+        "cell_updates_per_s": sum_over_ranks(cell_updates),
+        "e2e": {"value": e2e_sec, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": kind, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "alg_bytes_per_launch": byts / max(1, nlaunch), "launches": nlaunch,
+                     "avg_launch_ms": ms_sum / max(1, nlaunch),
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s"},
+        "kernel_time_share": share,
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    return out
+
+
+def cpu_baseline(case_name, iters_per_step, budget_s=20.0):
+    """The CPU oracle in FP32 (the reference's precision), one thread: a
+    bounded sample of pseudo-iterations, scaled to one physical step."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    case, grid, state, _ = build_case(case_name, abi.FP64, abi.PRED_QN)
+    o = oracle.OracleSolver(case, 4)
+    o.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
+    o.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
+    o.begin_step()
+    t0 = time.perf_counter()
+    k = 0
+    while True:
+        o.pseudo_iteration()
+        k += 1
+        if time.perf_counter() - t0 > budget_s or k >= iters_per_step:
+            break
+    per_it = (time.perf_counter() - t0) / k
+    return {"value": per_it * iters_per_step, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": "%d pseudo-iterations of the first physical step (%.2f s each, FP32 oracle, 1 thread), "
+                      "scaled by the %d pseudo-iterations the FP64 GPU path needed per step" % (k, per_it, iters_per_step)}
+
+
+def run_reference(args):
+    """--impl reference: the oracle (CPU port of the reference) on this case."""
+    iters = {"cavity": 200}.get(args.case)
+    if iters is None:
+        iters = REF_ITERS.get(args.case, 200)
+    vals = []
+    for _ in range(args.warmup + args.steps):
+        cb = cpu_baseline(args.case, iters, budget_s=max(5.0, 60.0 / max(1, args.steps + args.warmup)))
+        vals.append(cb)
+    v = float(np.mean([c["value"] for c in vals[args.warmup:]]))
+    cb = vals[-1]
+    cb["value"] = v
+    _, _, _, desc = build_case(args.case, abi.FP64, abi.PRED_QN)
+    return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": desc, "case": args.case},
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+# pseudo-iterations per physical step of the FP64 path (q^n guess) on each
+# case, as measured on the GPU path whose iterates follow the oracle's
+# (used only to scale the reference arm's bounded CPU sample)
+REF_ITERS = {"cavity": 200, "channel": 400}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--case", default="cavity", choices=["cavity", "channel"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)))
+        return
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as td
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist = td
+    out = run_ours(args, rank, world, dist)
+    if rank == 0:
+        print(json.dumps(out))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -69,6 +69,12 @@ struct desalm_ctx {
   double* h_norm = nullptr;   // pinned host [5]
   int* flags = nullptr;       // device [2]
   SaWork sa{};
+  // per-kernel CUDA-event timing (desalm_profile) and launch counter
+  struct ProfRec { int cls, lvl; double nodes; cudaEvent_t a, b; };
+  bool prof_on = false;
+  std::vector<ProfRec> prof;
+  size_t prof_used = 0;
+  long launches = 0;
   // driver state
   int itc = 0;
   double init_resd[5] = {0, 0, 0, 0, 0};
@@ -102,6 +108,25 @@ namespace {
   } while (0)
 
 inline unsigned cdiv(long a, long b) { return (unsigned)((a + b - 1) / b); }
+
+// kernel classes for desalm_kernel_stats
+enum KClass { KC_DTAU = 0, KC_RESID, KC_SWEEP_I, KC_SWEEP_J, KC_SWEEP_K, KC_RECALC, KC_BCOND, KC_PFIX,
+              KC_NLEVEL, KC_PROLONG, KC_RSMOOTH, KC_NORM, KC_SA_RHS, KC_SA_SWEEP, KC_SA_BC, KC_MISC, KC_COUNT };
+
+struct ProfScope {
+  desalm_ctx* ctx;
+  size_t slot;
+  bool on;
+  ProfScope(desalm_ctx* c, int cls, int lvl, double nodes);
+  ~ProfScope();
+};
+
+// Launch one kernel: count it and, when profiling, bracket it with events.
+#define LAUNCH(CLS, LVL, NODES, ...)                 \
+  do {                                               \
+    ProfScope ps__(ctx, (CLS), (LVL), (NODES));      \
+    __VA_ARGS__;                                     \
+  } while (0)
 
 int dalloc(desalm_ctx* ctx, std::vector<void*>& owner, void** p, size_t bytes) {
   cudaError_t e = cudaMalloc(p, bytes);
@@ -213,22 +238,23 @@ int launch_daf(desalm_ctx* ctx, Lv<T, W>& L, Level& G, int n, int recalc, int it
   const desalm_case& c = ctx->c;
   cudaStream_t s = ctx->stream;
   if (!G.dtau_valid) {
-    k_dtau<T, W><<<cdiv(L.N, 256), 256, 0, s>>>(L, P);
+    LAUNCH(KC_DTAU, n, L.N, k_dtau<T, W><<<cdiv(L.N, 256), 256, 0, s>>>(L, P));
     CKL();
     G.dtau_valid = true;
   }
   const int fine = (n == 0);
   const int upwind = fine ? 2 : 1;
   const int bback = fine && c.btype[0] != 5;
-  k_resid<T, W, 0><<<grid_interior(L), blk3(), 0, s>>>(L, P, upwind, itr == 1 ? 1 : 0, n > 0 ? 1 : 0, bback);
+  const double nin = double(L.im - 2) * (L.jm - 2) * (L.km - 2);
+  LAUNCH(KC_RESID, n, nin, k_resid<T, W, 0><<<grid_interior(L), blk3(), 0, s>>>(L, P, upwind, itr == 1 ? 1 : 0, n > 0 ? 1 : 0, bback));
   CKL();
   const int TB = 64;
-  k_sweep<T, W, 0><<<dim3(cdiv(L.jm - 2, TB), L.km - 2), TB, 0, s>>>(L, P, bback, 0);
+  LAUNCH(KC_SWEEP_I, n, nin, k_sweep<T, W, 0><<<dim3(cdiv(L.jm - 2, TB), L.km - 2), TB, 0, s>>>(L, P, bback, 0));
   CKL();
-  k_sweep<T, W, 1><<<dim3(cdiv(L.im - 2, TB), L.km - 2), TB, 0, s>>>(L, P, fine && c.btype[2] != 5, fine && c.btype[3] != 5);
+  LAUNCH(KC_SWEEP_J, n, nin, k_sweep<T, W, 1><<<dim3(cdiv(L.im - 2, TB), L.km - 2), TB, 0, s>>>(L, P, fine && c.btype[2] != 5, fine && c.btype[3] != 5));
   CKL();
-  k_sweep<T, W, 2><<<dim3(cdiv(L.im - 2, TB), L.jm - 2), TB, 0, s>>>(L, P, fine && c.btype[4] != 5,
-                                                                      fine && c.btype[5] != 5 && c.btype[5] != 6);
+  LAUNCH(KC_SWEEP_K, n, nin, k_sweep<T, W, 2><<<dim3(cdiv(L.im - 2, TB), L.jm - 2), TB, 0, s>>>(L, P, fine && c.btype[4] != 5,
+                                                                      fine && c.btype[5] != 5 && c.btype[5] != 6));
   CKL();
   return 0;
 }
@@ -237,7 +263,7 @@ template <class T, class W>
 int launch_recalc(desalm_ctx* ctx, Lv<T, W>& L, int n) {
   Par P = ctx->par;
   P.fine = (n == 0);
-  k_resid<T, W, 1><<<grid_interior(L), blk3(), 0, ctx->stream>>>(L, P, n == 0 ? 2 : 1, 0, n > 0 ? 1 : 0, 0);
+  LAUNCH(KC_RECALC, n, double(L.im - 2) * (L.jm - 2) * (L.km - 2), k_resid<T, W, 1><<<grid_interior(L), blk3(), 0, ctx->stream>>>(L, P, n == 0 ? 2 : 1, 0, n > 0 ? 1 : 0, 0));
   CKL();
   return 0;
 }
@@ -248,17 +274,17 @@ int launch_bcond(desalm_ctx* ctx, Lv<T, W>& L) {
   P.fine = 1;
   cudaStream_t s = ctx->stream;
   const T* rat = (const T*)ctx->rat;
-  k_bcond<T, W, 0><<<dim3(cdiv(L.jm, 64), L.km), 64, 0, s>>>(L, P, rat, ctx->ratdim);
+  LAUNCH(KC_BCOND, 0, 2.0 * L.jm * L.km, k_bcond<T, W, 0><<<dim3(cdiv(L.jm, 64), L.km), 64, 0, s>>>(L, P, rat, ctx->ratdim));
   CKL();
-  k_bcond<T, W, 1><<<dim3(cdiv(L.im, 64), L.km), 64, 0, s>>>(L, P, rat, ctx->ratdim);
+  LAUNCH(KC_BCOND, 0, 2.0 * L.im * L.km, k_bcond<T, W, 1><<<dim3(cdiv(L.im, 64), L.km), 64, 0, s>>>(L, P, rat, ctx->ratdim));
   CKL();
-  k_bcond<T, W, 2><<<dim3(cdiv(L.im, 64), L.jm), 64, 0, s>>>(L, P, rat, ctx->ratdim);
+  LAUNCH(KC_BCOND, 0, 2.0 * L.im * L.jm, k_bcond<T, W, 2><<<dim3(cdiv(L.im, 64), L.jm), 64, 0, s>>>(L, P, rat, ctx->ratdim));
   CKL();
   const desalm_case& c = ctx->c;
   int lfix = (c.ifix - 1) + L.sj * (c.jfix - 1) + L.sk * (c.kfix - 1);
-  k_pfix_read<T, W><<<1, 1, 0, s>>>(L, lfix, (T*)ctx->pfix);
+  LAUNCH(KC_PFIX, 0, 1, k_pfix_read<T, W><<<1, 1, 0, s>>>(L, lfix, (T*)ctx->pfix));
   CKL();
-  k_pfix_sub<T, W><<<cdiv(L.N, 256), 256, 0, s>>>(L, (const T*)ctx->pfix);
+  LAUNCH(KC_PFIX, 0, L.N, k_pfix_sub<T, W><<<cdiv(L.N, 256), 256, 0, s>>>(L, (const T*)ctx->pfix));
   CKL();
   return 0;
 }
@@ -266,7 +292,7 @@ int launch_bcond(desalm_ctx* ctx, Lv<T, W>& L) {
 template <class TF, class WF, class TC, class WC>
 int launch_nlevel(desalm_ctx* ctx, Lv<TF, WF>& F, Lv<TC, WC>& C) {
   const desalm_case& c = ctx->c;
-  k_nlevel<TF, WF, TC, WC><<<dim3(cdiv(C.im, 32), cdiv(C.jm, 4), C.km), dim3(32, 4, 1), 0, ctx->stream>>>(F, C, c.icrs, c.jcrs, c.kcrs);
+  LAUNCH(KC_NLEVEL, 0, double(C.N), k_nlevel<TF, WF, TC, WC><<<dim3(cdiv(C.im, 32), cdiv(C.jm, 4), C.km), dim3(32, 4, 1), 0, ctx->stream>>>(F, C, c.icrs, c.jcrs, c.kcrs));
   CKL();
   return 0;
 }
@@ -276,14 +302,15 @@ int launch_prolong(desalm_ctx* ctx, Lv<TF, WF>& F, Lv<TC, WC>& C, Level& G) {
   const desalm_case& c = ctx->c;
   cudaStream_t s = ctx->stream;
   TF* dq = (TF*)G.dq[0];
-  k_prolong_interp<TF, WF, TC, WC><<<grid_interior(F), blk3(), 0, s>>>(F, C, dq, c.icrs, c.jcrs, c.kcrs);
+  const double nin = double(F.im - 2) * (F.jm - 2) * (F.km - 2);
+  LAUNCH(KC_PROLONG, 0, nin, k_prolong_interp<TF, WF, TC, WC><<<grid_interior(F), blk3(), 0, s>>>(F, C, dq, c.icrs, c.jcrs, c.kcrs));
   CKL();
   const int TB = 64;
-  k_rsmooth<TF, WF, 0><<<dim3(cdiv(F.jm - 2, TB), F.km - 2), TB, 0, s>>>(F, dq, G.fac[0], G.dpr[0], c.ep[1][0], 0);
+  LAUNCH(KC_RSMOOTH, 0, nin, k_rsmooth<TF, WF, 0><<<dim3(cdiv(F.jm - 2, TB), F.km - 2), TB, 0, s>>>(F, dq, G.fac[0], G.dpr[0], c.ep[1][0], 0));
   CKL();
-  k_rsmooth<TF, WF, 1><<<dim3(cdiv(F.im - 2, TB), F.km - 2), TB, 0, s>>>(F, dq, G.fac[1], G.dpr[1], c.ep[1][1], 0);
+  LAUNCH(KC_RSMOOTH, 0, nin, k_rsmooth<TF, WF, 1><<<dim3(cdiv(F.im - 2, TB), F.km - 2), TB, 0, s>>>(F, dq, G.fac[1], G.dpr[1], c.ep[1][1], 0));
   CKL();
-  k_rsmooth<TF, WF, 2><<<dim3(cdiv(F.im - 2, TB), F.jm - 2), TB, 0, s>>>(F, dq, G.fac[2], G.dpr[2], c.ep[1][2], 1);
+  LAUNCH(KC_RSMOOTH, 0, nin, k_rsmooth<TF, WF, 2><<<dim3(cdiv(F.im - 2, TB), F.jm - 2), TB, 0, s>>>(F, dq, G.fac[2], G.dpr[2], c.ep[1][2], 1));
   CKL();
   return 0;
 }
@@ -293,9 +320,9 @@ int launch_norm(desalm_ctx* ctx, Lv<T, W>& L, int copy, double* out) {
   cudaStream_t s = ctx->stream;
   long total = (long)(L.im - 2) * (L.jm - 2) * (L.km - 2);
   int nb = (int)std::min<long>(ctx->part_blocks, std::max<long>(1, cdiv(total, 256)));
-  k_norm_partial<T, W><<<nb, 256, 0, s>>>(L, ctx->part, 5, copy);
+  LAUNCH(KC_NORM, 0, double(total), k_norm_partial<T, W><<<nb, 256, 0, s>>>(L, ctx->part, 5, copy));
   CKL();
-  k_norm_final<<<1, 32, 0, s>>>(ctx->part, nb, ctx->norm);
+  LAUNCH(KC_NORM, 0, 0, k_norm_final<<<1, 32, 0, s>>>(ctx->part, nb, ctx->norm));
   CKL();
   CK(cudaMemcpyAsync(ctx->h_norm, ctx->norm, 5 * sizeof(double), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
@@ -460,6 +487,7 @@ void desalm_destroy(desalm_ctx* ctx) {
   for (auto& G : ctx->L)
     for (void* p : G.allocs) cudaFree(p);
   for (void* p : ctx->allocs) cudaFree(p);
+  for (auto& r : ctx->prof) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
   if (ctx->h_norm) cudaFreeHost(ctx->h_norm);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -662,7 +690,6 @@ int desalm_set_state(desalm_ctx* ctx, const double* q, const double* qn, const d
   cudaStream_t s = ctx->stream;
   Level& G = ctx->L[0];
   const long N = G.N;
-  double* h = nullptr;
   double* d = nullptr;
   CK(cudaMalloc((void**)&d, 5 * N * sizeof(double)));
   const double* srcs[3] = {q, qn, qnm1};
@@ -681,7 +708,7 @@ int desalm_set_state(desalm_ctx* ctx, const double* q, const double* qn, const d
     double** dp = nullptr;
     cudaMalloc((void**)&dp, 5 * sizeof(double*));
     cudaMemcpyAsync(dp, dst, 5 * sizeof(double*), cudaMemcpyHostToDevice, s);
-    k_aos_to_soa<double><<<cdiv(N, 256), 256, 0, s>>>(dp, d, 5, N);
+    LAUNCH(KC_MISC, 0, N, k_aos_to_soa<double><<<cdiv(N, 256), 256, 0, s>>>(dp, d, 5, N));
     cudaStreamSynchronize(s);
     cudaFree(dp);
   }
@@ -692,7 +719,6 @@ int desalm_set_state(desalm_ctx* ctx, const double* q, const double* qn, const d
     if (nut) cudaMemcpyAsync(dn, nut, N * sizeof(double), cudaMemcpyHostToDevice, s);
     else cudaMemsetAsync(dn, 0, N * sizeof(double), s);
   }
-  (void)h;
   cudaError_t e = cudaStreamSynchronize(s);
   cudaFree(d);
   if (rc) return rc;
@@ -723,7 +749,7 @@ int desalm_get_state(desalm_ctx* ctx, double* q, double* qn, double* qnm1, doubl
     double** dp = nullptr;
     cudaMalloc((void**)&dp, 5 * sizeof(double*));
     cudaMemcpyAsync(dp, src, 5 * sizeof(double*), cudaMemcpyHostToDevice, s);
-    k_soa_to_aos<double><<<cdiv(N, 256), 256, 0, s>>>(d, dp, 5, N);
+    LAUNCH(KC_MISC, 0, N, k_soa_to_aos<double><<<cdiv(N, 256), 256, 0, s>>>(d, dp, 5, N));
     cudaMemcpyAsync(dsts[a], d, 5 * N * sizeof(double), cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
     cudaFree(dp);
@@ -866,7 +892,7 @@ int desalm_begin_step(desalm_ctx* ctx) {
     CK(cudaMemcpyAsync(qnm1, qn, F.N * esz, cudaMemcpyDeviceToDevice, s));
     CK(cudaMemcpyAsync(qn, q, F.N * esz, cudaMemcpyDeviceToDevice, s));
     if (c.predictor == DESALM_PRED_LINEAR)
-      k_extrapolate<double><<<cdiv(F.N, 256), 256, 0, s>>>((double*)q, (const double*)qn, (const double*)qnm1, F.N);
+      LAUNCH(KC_MISC, 0, F.N, k_extrapolate<double><<<cdiv(F.N, 256), 256, 0, s>>>((double*)q, (const double*)qn, (const double*)qnm1, F.N));
   }
   CKL();
   // inject qn, qnm1 to the coarse levels (src/mg_driver.F90:55-58)
@@ -882,11 +908,11 @@ int desalm_begin_step(desalm_ctx* ctx) {
         RET(field_ptr(ctx, n, f, &pc, &ec));
         dim3 g(cdiv(C.im, 64), C.jm, C.km);
         if (ef == 8 && ec == 8)
-          k_inject<double, double><<<g, 64, 0, s>>>((double*)pc, (const double*)pf, C.im, C.jm, C.km, P.im, P.jm, c.icrs, c.jcrs, c.kcrs);
+          LAUNCH(KC_MISC, n, C.N, k_inject<double, double><<<g, 64, 0, s>>>((double*)pc, (const double*)pf, C.im, C.jm, C.km, P.im, P.jm, c.icrs, c.jcrs, c.kcrs));
         else if (ef == 8)
-          k_inject<double, float><<<g, 64, 0, s>>>((float*)pc, (const double*)pf, C.im, C.jm, C.km, P.im, P.jm, c.icrs, c.jcrs, c.kcrs);
+          LAUNCH(KC_MISC, n, C.N, k_inject<double, float><<<g, 64, 0, s>>>((float*)pc, (const double*)pf, C.im, C.jm, C.km, P.im, P.jm, c.icrs, c.jcrs, c.kcrs));
         else
-          k_inject<float, float><<<g, 64, 0, s>>>((float*)pc, (const float*)pf, C.im, C.jm, C.km, P.im, P.jm, c.icrs, c.jcrs, c.kcrs);
+          LAUNCH(KC_MISC, n, C.N, k_inject<float, float><<<g, 64, 0, s>>>((float*)pc, (const float*)pf, C.im, C.jm, C.km, P.im, P.jm, c.icrs, c.jcrs, c.kcrs));
       }
   }
   CKL();
@@ -971,6 +997,59 @@ int pseudo_iter(desalm_ctx* ctx, desalm_step_report* rep) {
 }
 
 }  // namespace
+
+namespace {
+ProfScope::ProfScope(desalm_ctx* c, int cls, int lvl, double nodes) : ctx(c), slot(0), on(c->prof_on) {
+  ctx->launches++;
+  if (!on) return;
+  if (ctx->prof_used == ctx->prof.size()) {
+    desalm_ctx::ProfRec r{};
+    cudaEventCreate(&r.a);
+    cudaEventCreate(&r.b);
+    ctx->prof.push_back(r);
+  }
+  slot = ctx->prof_used++;
+  desalm_ctx::ProfRec& r = ctx->prof[slot];
+  r.cls = cls; r.lvl = lvl; r.nodes = nodes;
+  cudaEventRecord(r.a, ctx->stream);
+}
+ProfScope::~ProfScope() {
+  if (on) cudaEventRecord(ctx->prof[slot].b, ctx->stream);
+}
+}  // namespace
+
+extern "C" {
+// Enable/disable per-kernel event timing; resets the statistics and the
+// launch counter.
+int desalm_profile(desalm_ctx* ctx, int enable) {
+  if (!ctx) return DESALM_EINVAL;
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->prof_on = enable != 0;
+  ctx->prof_used = 0;
+  ctx->launches = 0;
+  return 0;
+}
+// Per kernel class and level (KC_COUNT x 4 entries, index cls*4 + level):
+// total milliseconds, launches and nodes processed since desalm_profile.
+int desalm_kernel_stats(desalm_ctx* ctx, double* ms, long* launches, double* nodes, long* total_launches) {
+  if (!ctx) return DESALM_EINVAL;
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (int t = 0; t < KC_COUNT * 4; ++t) { ms[t] = 0; launches[t] = 0; nodes[t] = 0; }
+  for (size_t i = 0; i < ctx->prof_used; ++i) {
+    desalm_ctx::ProfRec& r = ctx->prof[i];
+    float e = 0.f;
+    cudaEventElapsedTime(&e, r.a, r.b);
+    int t = r.cls * 4 + std::min(r.lvl, 3);
+    ms[t] += e; launches[t] += 1; nodes[t] += r.nodes;
+  }
+  if (total_launches) *total_launches = ctx->launches;
+  return 0;
+}
+int desalm_kernel_class_count(void) { return KC_COUNT; }
+// The CUDA stream of the context (cudaStream_t), for callers that order
+// their own work or events with the library's.
+void* desalm_stream(desalm_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+}  // extern "C"
 
 namespace {
 int sa_des_eddy(desalm_ctx* ctx) {

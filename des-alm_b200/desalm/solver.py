@@ -61,12 +61,23 @@ def lib():
             ("pseudo_iteration", [vp, C.POINTER(StepReport)]),
             ("mg_driver", [vp, C.POINTER(StepReport)]),
             ("sync", [vp]),
+            ("profile", [vp, ip]),
+            ("kernel_stats", [vp, dp, C.POINTER(C.c_long), dp, C.POINTER(C.c_long)]),
         ]:
             f = getattr(L, "desalm_" + name)
             f.argtypes = args
             f.restype = C.c_int
+        L.desalm_stream.argtypes = [vp]
+        L.desalm_stream.restype = C.c_void_p
+        L.desalm_kernel_class_count.argtypes = []
+        L.desalm_kernel_class_count.restype = C.c_int
         _LIB = L
     return _LIB
+
+
+# kernel classes reported by desalm_kernel_stats (order of the C enum)
+KERNEL_CLASSES = ["dtau", "resid", "sweep_i", "sweep_j", "sweep_k", "recalc", "bcond", "pfix",
+                  "nlevel", "prolong", "rsmooth", "norm", "sa_rhs", "sa_sweep", "sa_bc", "misc"]
 
 
 def _p(a):
@@ -172,3 +183,27 @@ class Solver:
 
     def sync(self):
         self._ck(self.L.desalm_sync(self.ctx), "sync")
+
+    def stream(self):
+        """The context's cudaStream_t as an integer handle."""
+        return self.L.desalm_stream(self.ctx)
+
+    def profile(self, enable=True):
+        self._ck(self.L.desalm_profile(self.ctx, 1 if enable else 0), "profile")
+
+    def kernel_stats(self):
+        """{class: {level: (ms, launches, nodes)}} since the last profile() call,
+        and the total number of kernel launches."""
+        n = self.L.desalm_kernel_class_count() * 4
+        ms = np.zeros(n)
+        la = (C.c_long * n)()
+        nodes = np.zeros(n)
+        tot = C.c_long(0)
+        self._ck(self.L.desalm_kernel_stats(self.ctx, _p(ms), la, _p(nodes), C.byref(tot)), "kernel_stats")
+        out = {}
+        for c, name in enumerate(KERNEL_CLASSES):
+            for lvl in range(4):
+                t = c * 4 + lvl
+                if la[t]:
+                    out.setdefault(name, {})[lvl + 1] = (float(ms[t]), int(la[t]), float(nodes[t]))
+        return out, int(tot.value)

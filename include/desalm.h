@@ -176,6 +176,20 @@ int  desalm_mg_driver(desalm_ctx* ctx, desalm_step_report* rep);
 int  desalm_pseudo_iteration(desalm_ctx* ctx, desalm_step_report* rep);
 /* Wait for all work on the context's stream. */
 int  desalm_sync(desalm_ctx* ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that order their
+ * own work or timing events with the library's. */
+void* desalm_stream(desalm_ctx* ctx);
+
+/* Instrumentation.  desalm_profile(ctx, 1) brackets every kernel launch with
+ * CUDA events on the context stream and resets the statistics and the launch
+ * counter; desalm_kernel_stats() returns, per kernel class and level
+ * (desalm_kernel_class_count() x 4 entries, index class*4 + level-1), the
+ * accumulated milliseconds, launches and nodes processed, plus the total
+ * number of kernels launched since the reset. */
+int  desalm_profile(desalm_ctx* ctx, int enable);
+int  desalm_kernel_stats(desalm_ctx* ctx, double* ms, long* launches,
+                         double* nodes, long* total_launches);
+int  desalm_kernel_class_count(void);
 
 #ifdef __cplusplus
 }
