@@ -60,6 +60,7 @@ struct desalm_ctx {
   // fine-level extras (always FP64)
   double *x = nullptr, *y = nullptr, *z = nullptr, *wd = nullptr, *dtev = nullptr;
   double* cov[9] = {};
+  double** dcov = nullptr;    // device copy of cov[]
   double* rat = nullptr;
   int ratdim = 0;
   double* pfix = nullptr;     // device scalar (type of the fine level: double)
@@ -562,6 +563,8 @@ int desalm_init(const desalm_case* c, desalm_ctx** out) {
   if (!rc) rc = A(&ctx->wd, NF);
   if (!rc) rc = A(&ctx->dtev, NF);
   for (int t = 0; t < 9 && !rc; ++t) rc = A(&ctx->cov[t], NF);
+  if (!rc) rc = dalloc(ctx, ctx->allocs, (void**)&ctx->dcov, 9 * sizeof(double*));
+  if (!rc) cudaMemcpyAsync(ctx->dcov, ctx->cov, 9 * sizeof(double*), cudaMemcpyHostToDevice, ctx->stream);
   ctx->ratdim = std::max(c->im, std::max(c->jm, c->km));
   if (!rc) rc = A(&ctx->rat, 6L * ctx->ratdim * ctx->ratdim);
   if (!rc) rc = A(&ctx->pfix, 1);
@@ -1052,12 +1055,64 @@ void* desalm_stream(desalm_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr
 }  // extern "C"
 
 namespace {
+
+// SA view of the fine level (FP64 in every precision mode)
+template <class W>
+Sa make_sa(desalm_ctx* ctx, Lv<double, W>& L) {
+  Sa S{};
+  S.im = L.im; S.jm = L.jm; S.km = L.km; S.N = L.N; S.sj = L.sj; S.sk = L.sk;
+  for (int m = 0; m < 5; ++m) S.q[m] = L.q[m];
+  S.qn5 = L.qn[4]; S.qnm1_5 = L.qnm1[4];
+  for (int d = 0; d < 3; ++d) { S.csi[d] = L.csi[d]; S.eta[d] = L.eta[d]; S.zet[d] = L.zet[d]; }
+  S.aj = L.aj; S.wd = ctx->wd; S.dtev = ctx->dtev; S.nut = L.nut;
+  S.wo = ctx->sa.a[0]; S.rh = ctx->sa.a[1]; S.sd = ctx->sa.a[2]; S.su = ctx->sa.a[3];
+  S.flags = ctx->flags;
+  S.ren = ctx->c.ren; S.delti = ctx->c.delti; S.es = ctx->c.unsteady ? 1.0 : 0.0;
+  for (int b = 0; b < 6; ++b) { S.sa1[b] = ctx->par.sa[0][b]; S.sb1[b] = ctx->par.sb[0][b]; S.btype[b] = ctx->c.btype[b]; }
+  return S;
+}
+
+template <class W>
+int sa_run(desalm_ctx* ctx, Lv<double, W>& L) {
+  Sa S = make_sa(ctx, L);
+  cudaStream_t s = ctx->stream;
+  const double nin = double(L.im - 2) * (L.jm - 2) * (L.km - 2);
+  const dim3 gi(cdiv(L.im - 2, 32), cdiv(L.jm - 2, 4), L.km - 2);
+  LAUNCH(KC_SA_RHS, 0, nin, k_sa_source<<<gi, blk3(), 0, s>>>(S));
+  const int TB = 64;
+  for (int it = 0; it < ctx->c.itk; ++it) {
+    LAUNCH(KC_SA_RHS, 0, nin, k_sa_rhs<<<gi, blk3(), 0, s>>>(S));
+    LAUNCH(KC_SA_SWEEP, 0, nin, k_sa_sweep<0><<<dim3(cdiv(L.jm - 2, TB), L.km - 2), TB, 0, s>>>(S));
+    LAUNCH(KC_SA_SWEEP, 0, nin, k_sa_sweep<1><<<dim3(cdiv(L.im - 2, TB), L.km - 2), TB, 0, s>>>(S));
+    LAUNCH(KC_SA_SWEEP, 0, nin, k_sa_sweep<2><<<dim3(cdiv(L.im - 2, TB), L.jm - 2), TB, 0, s>>>(S));
+    LAUNCH(KC_SA_BC, 0, 2.0 * L.jm * L.km, k_sa_bc<0><<<dim3(cdiv(L.jm, 64), L.km), 64, 0, s>>>(S));
+    LAUNCH(KC_SA_BC, 0, 2.0 * L.im * L.km, k_sa_bc<1><<<dim3(cdiv(L.im, 64), L.km), 64, 0, s>>>(S));
+    LAUNCH(KC_SA_BC, 0, 2.0 * L.im * L.jm, k_sa_bc<2><<<dim3(cdiv(L.im, 64), L.jm), 64, 0, s>>>(S));
+    LAUNCH(KC_SA_BC, 0, L.N, k_sa_clamp<<<cdiv(L.N, 256), 256, 0, s>>>(S));
+  }
+  CKL();
+  ctx->L[0].dtau_valid = false;  // nu_t changed
+  return 0;
+}
+
+template <class W>
+int cons_run(desalm_ctx* ctx, Lv<double, W>& L) {
+  Sa S = make_sa(ctx, L);
+  cudaStream_t s = ctx->stream;
+  double* acc = ctx->part;
+  LAUNCH(KC_MISC, 0, 2.0 * L.jm * L.km, k_cons_sum<<<1, 256, 0, s>>>(S, acc));
+  LAUNCH(KC_MISC, 0, 1.0 * L.jm * L.km, k_cons_apply<<<cdiv(L.jm * L.km, 128), 128, 0, s>>>(S, acc, ctx->dcov));
+  CKL();
+  return 0;
+}
+
 int sa_des_eddy(desalm_ctx* ctx) {
-  ctx->err = "Spalart-Allmaras path not built yet";
-  return DESALM_EINVAL;
+  if (!ctx->c.turbulence) return 0;
+  return kind_of(ctx, 0) == K_DD ? sa_run(ctx, ctx->L[0].dd) : sa_run(ctx, ctx->L[0].df);
 }
+
 int sa_conservation(desalm_ctx* ctx) {
-  ctx->err = "conservation not built yet";
-  return DESALM_EINVAL;
+  return kind_of(ctx, 0) == K_DD ? cons_run(ctx, ctx->L[0].dd) : cons_run(ctx, ctx->L[0].df);
 }
+
 }  // namespace

@@ -1,4 +1,7 @@
-// sa.cuh -- Spalart-Allmaras sub-iterations on the fine level (des_eddy).
+// sa.cuh -- Spalart-Allmaras sub-iterations on the fine level (des_eddy,
+// src/des_eddy.F90:109-297) and the outlet mass-flux fix (conservation,
+// src/conservation.F90:64-160).  The fine level is FP64 in every precision
+// mode, so these kernels are FP64 only.
 #pragma once
 #include "common.cuh"
 
@@ -6,8 +9,332 @@ namespace desalm {
 
 // fine-level FP64 work arrays of the SA model
 struct SaWork {
-  static const int NARR = 12;
-  double* a[NARR];
+  static const int NARR = 4;
+  double* a[NARR];  // wo, rh5, sd, su
 };
+
+struct Sa {
+  int im, jm, km, N, sj, sk;
+  double* q[5];
+  const double* qn5;
+  const double* qnm1_5;
+  const double* csi[3];
+  const double* eta[3];
+  const double* zet[3];
+  const double* aj;
+  const double* wd;
+  const double* dtev;
+  double* nut;
+  double* wo;
+  double* rh;
+  double* sd;
+  double* su;
+  int* flags;
+  double ren, delti, es;
+  double sa1[6], sb1[6];  // pressure-row extrapolation coefficients, sa(1,b), sb(1,b)
+  int btype[6];
+};
+
+DESALM_DEV double sa_ucn(const Sa& S, int d, int l) {
+  const double* const* m = d == 0 ? S.csi : (d == 1 ? S.eta : S.zet);
+  double tmp = 1.0 / S.aj[l];
+  return tmp * (m[0][l] * S.q[1][l] + m[1][l] * S.q[2][l] + m[2][l] * S.q[3][l]);
+}
+
+// vorticity magnitude wo = 2 |W|^2 on interior nodes (src/rhs_sa_source.F90:44-93)
+__global__ void k_sa_source(Sa S) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int k = blockIdx.z + 1;
+  if (i > S.im - 2 || j > S.jm - 2) return;
+  const int l = i + S.sj * j + S.sk * k;
+  double g[3][3];
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {
+    const double* v = S.q[m + 1];
+    g[m][0] = 0.5 * (v[l + 1] - v[l - 1]);
+    g[m][1] = 0.5 * (v[l + S.sj] - v[l - S.sj]);
+    g[m][2] = 0.5 * (v[l + S.sk] - v[l - S.sk]);
+  }
+  double d[3][3];
+#pragma unroll
+  for (int m = 0; m < 3; ++m)
+#pragma unroll
+    for (int x = 0; x < 3; ++x) d[m][x] = g[m][0] * S.csi[x][l] + g[m][1] * S.eta[x][l] + g[m][2] * S.zet[x][l];
+  double w12 = 0.5 * (d[0][1] - d[1][0]);
+  double w13 = 0.5 * (d[0][2] - d[2][0]);
+  double w23 = 0.5 * (d[1][2] - d[2][1]);
+  S.wo[l] = 2.0 * (w12 * w12 + w13 * w13 + w23 * w23);
+}
+
+// viscous flux of nu_tilde through the face l0 -> l0 + st[dir]
+// (src/rhs_sa_viscous.F90:58-175)
+DESALM_DEV double sa_visc_face(const Sa& S, int dir, int l0, double rei, double sig) {
+  const int sj = S.sj, sk = S.sk;
+  const double* v = S.q[4];
+  int l1;
+  double vcs, vet, vze;
+  if (dir == 0) {
+    l1 = l0 + 1;
+    vcs = v[l1] - v[l0];
+    vet = 0.25 * (v[l1 + sj] - v[l1 - sj] + v[l0 + sj] - v[l0 - sj]);
+    vze = 0.25 * (v[l1 + sk] - v[l1 - sk] + v[l0 + sk] - v[l0 - sk]);
+  } else if (dir == 1) {
+    l1 = l0 + sj;
+    vcs = 0.25 * (v[l1 + 1] - v[l1 - 1] + v[l0 + 1] - v[l0 - 1]);
+    vet = v[l1] - v[l0];
+    vze = 0.25 * (v[l1 + sk] - v[l1 - sk] + v[l0 + sk] - v[l0 - sk]);
+  } else {
+    l1 = l0 + sk;
+    vcs = 0.25 * (v[l1 + 1] - v[l1 - 1] + v[l0 + 1] - v[l0 - 1]);
+    vet = 0.25 * (v[l1 + sj] - v[l1 - sj] + v[l0 + sj] - v[l0 - sj]);
+    vze = v[l1] - v[l0];
+  }
+  double a1 = S.csi[0][l1] + S.csi[0][l0], a2 = S.csi[1][l1] + S.csi[1][l0], a3 = S.csi[2][l1] + S.csi[2][l0];
+  double b1 = S.eta[0][l1] + S.eta[0][l0], b2 = S.eta[1][l1] + S.eta[1][l0], b3 = S.eta[2][l1] + S.eta[2][l0];
+  double c1 = S.zet[0][l1] + S.zet[0][l0], c2 = S.zet[1][l1] + S.zet[1][l0], c3 = S.zet[2][l1] + S.zet[2][l0];
+  double k1, k2, k3;
+  if (dir == 0) { k1 = a1 * a1 + a2 * a2 + a3 * a3; k2 = a1 * b1 + a2 * b2 + a3 * b3; k3 = a1 * c1 + a2 * c2 + a3 * c3; }
+  else if (dir == 1) { k1 = b1 * a1 + b2 * a2 + b3 * a3; k2 = b1 * b1 + b2 * b2 + b3 * b3; k3 = b1 * c1 + b2 * c2 + b3 * c3; }
+  else { k1 = c1 * a1 + c2 * a2 + c3 * a3; k2 = c1 * b1 + c2 * b2 + c3 * b3; k3 = c1 * c1 + c2 * c2 + c3 * c3; }
+  double vtj = 0.25 * ((rei + v[l1]) / sig + (rei + v[l0]) / sig) / (S.aj[l1] + S.aj[l0]);
+  return vtj * (k1 * vcs + k2 * vet + k3 * vze);
+}
+
+// first-order flux-difference upwind flux of nu_tilde through the face
+// l0 -> l0 + st (src/rhs_sa_flux.F90:32-109)
+DESALM_DEV double sa_conv_face(const Sa& S, int dir, int l0, int st) {
+  const int l1 = l0 + st;
+  const double u1 = sa_ucn(S, dir, l1), u0 = sa_ucn(S, dir, l0);
+  const double* v = S.q[4];
+  double eigh = 0.5 * fabs(u1 + u0);
+  return 0.5 * (v[l1] * u1 + v[l0] * u0 - eigh * (v[l1] - v[l0]));
+}
+
+// One fused pass of rhs_sa_grdnu, rhs_sa_prod, rhs_sa_viscous, rhs_sa_flux,
+// rhs_sa_unst_visc and rhs_sa_implicit_source on interior nodes
+// (src/des_eddy.F90:164-223); boundary values of rh stay zero.
+__global__ void __launch_bounds__(128) k_sa_rhs(Sa S) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int k = blockIdx.z + 1;
+  if (i > S.im - 2 || j > S.jm - 2) return;
+  const int sj = S.sj, sk = S.sk;
+  const int l = i + sj * j + sk * k;
+  const double cb1 = 0.1355, cb2 = 0.622, sig = 2.0 / 3.0, capa = 0.41;
+  const double cw1 = 3.23906782, cw2 = 0.3, cw3h = 64.0, cv1c = 357.911, cv2 = 5.0;
+  const double rei = 1.0 / S.ren;
+  const double* q5 = S.q[4];
+  const int st[3] = {1, sj, sk};
+  const double* const* mt[3] = {S.csi, S.eta, S.zet};
+  // gradient of nu_tilde (src/rhs_sa_grdnu.F90:22-60)
+  double dn[3];
+  {
+    double qp[3], qm[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      qp[d] = q5[l + st[d]] / S.aj[l + st[d]];
+      qm[d] = q5[l - st[d]] / S.aj[l - st[d]];
+    }
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+      double v = 0.5 * (qp[0] * mt[0][x][l + 1] - qm[0] * mt[0][x][l - 1]);
+      v = v + 0.5 * (qp[1] * mt[1][x][l + sj] - qm[1] * mt[1][x][l - sj]);
+      v = v + 0.5 * (qp[2] * mt[2][x][l + sk] - qm[2] * mt[2][x][l - sk]);
+      dn[x] = v;
+    }
+  }
+  double aj2 = S.aj[l] * S.aj[l];
+  double dnu = aj2 * (dn[0] * dn[0] + dn[1] * dn[1] + dn[2] * dn[2]);
+  // production, destruction, diffusion (src/rhs_sa_prod.F90:32-100)
+  double psa;
+  const double w = S.wd[l];
+  if (w == 0.0) {
+    psa = 0.0;
+  } else {
+    double nt = q5[l];
+    double chi = nt / rei;
+    double chic = chi * chi * chi;
+    double fv1 = chic / (chic + cv1c);
+    double t = 1.0 + chi / cv2;
+    double fv2 = 1.0 / (t * t * t);
+    double fv3 = ((1.0 + chi * fv1) * (1.0 - fv2)) / chi;
+    double vtcm = sqrt(2.0 * S.wo[l]);
+    double cawd = capa * capa * w * w;
+    double vtc = fv3 * vtcm + nt * fv2 / cawd;
+    vtc = vtc > 0.00001 ? vtc : 0.00001;
+    double p = cb1 * vtc * nt;
+    double rr = nt / (vtc * cawd);
+    double rr6 = rr * rr * rr * rr * rr * rr;
+    double grr = rr + cw2 * (rr6 - rr);
+    grr = grr > 0.0 ? grr : 0.0;
+    double grr6 = grr * grr * grr * grr * grr * grr;
+    double fw = grr * pow((1.0 + cw3h) / (grr6 + cw3h), 1.0 / 6.0);
+    double vwd = nt / w;
+    p = p - cw1 * fw * vwd * vwd;
+    p = p + cb2 * dnu / sig;
+    psa = p;
+  }
+  // viscous terms
+  double visc = sa_visc_face(S, 0, l, rei, sig) - sa_visc_face(S, 0, l - 1, rei, sig);
+  visc = visc + sa_visc_face(S, 1, l, rei, sig) - sa_visc_face(S, 1, l - sj, rei, sig);
+  visc = visc + sa_visc_face(S, 2, l, rei, sig) - sa_visc_face(S, 2, l - sk, rei, sig);
+  // convective flux
+  double rh = sa_conv_face(S, 0, l, 1) - sa_conv_face(S, 0, l - 1, 1);
+  rh = rh + sa_conv_face(S, 1, l, sj) - sa_conv_face(S, 1, l - sj, sj);
+  rh = rh + sa_conv_face(S, 2, l, sk) - sa_conv_face(S, 2, l - sk, sk);
+  // unsteady term and implicit source scaling
+  double dtj = 2.0 * S.delti * S.aj[l];
+  double dq5dt = S.es * (3.0 * q5[l] - 4.0 * S.qn5[l] + S.qnm1_5[l]) / dtj;
+  double r = rh + dq5dt - visc - psa / S.aj[l];
+  S.rh[l] = -S.dtev[l] * S.aj[l] * r;
+}
+
+// Scalar ADI sweep of nu_tilde along one direction
+// (src/rhs_sa_adi_solver.F90:50-244): SGTSV no-interchange elimination in
+// SGTSV's order, a would-swap row counted in flags[0].  The k sweep ends
+// with the update nu <- nu + (-nu + (nu_old + dnu)) / (1 + 1.5 dtev / dt)
+// (src/des_eddy.F90:260-272).
+template <int DIR>
+__global__ void __launch_bounds__(128) k_sa_sweep(Sa S) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int b = blockIdx.y + 1;
+  int amax, n, st, lb;
+  if (DIR == 0) { amax = S.jm - 2; n = S.im - 2; st = 1; lb = S.sj * a + S.sk * b; }
+  else if (DIR == 1) { amax = S.im - 2; n = S.jm - 2; st = S.sj; lb = a + S.sk * b; }
+  else { amax = S.im - 2; n = S.km - 2; st = S.sk; lb = a + S.sj * b; }
+  if (a > amax) return;
+  const double* const* mt = DIR == 0 ? S.csi : (DIR == 1 ? S.eta : S.zet);
+  const double sig = 2.0 / 3.0, rei = 1.0 / S.ren;
+  const double* q5 = S.q[4];
+  auto face = [&](int l0) {
+    const int l1 = l0 + st;
+    double gx = mt[0][l1] + mt[0][l0], gy = mt[1][l1] + mt[1][l0], gz = mt[2][l1] + mt[2][l0];
+    double ev = (rei + 0.5 * (q5[l1] + q5[l0])) / sig;
+    double ucna = 0.5 * fabs(sa_ucn(S, DIR, l1) + sa_ucn(S, DIR, l0));
+    return ucna + ev * (gx * gx + gy * gy + gz * gz) / (S.aj[l1] + S.aj[l0]);
+  };
+  double avw = face(lb);                 // face between the boundary node and row 0
+  double uw = sa_ucn(S, DIR, lb);        // U/J of the node before the current row
+  double u0 = sa_ucn(S, DIR, lb + st);
+  double dprev = 0, duprev = 0, bprev = 0;
+  int npiv = 0;
+  for (int p = 0; p < n; ++p) {
+    const int l = lb + (p + 1) * st;
+    double ave = face(l);
+    double ue = sa_ucn(S, DIR, l + st);
+    double dtj = 0.5 * S.dtev[l] * S.aj[l];
+    double aw = -dtj * (uw + avw);
+    double ap = 1.0 + dtj * (avw + ave);
+    double ae = dtj * (ue - ave);
+    double r = S.rh[l];
+    double d;
+    if (p == 0) {
+      d = ap;
+      bprev = r;
+    } else {
+      npiv += fabs(dprev) < fabs(aw);
+      double f = aw / dprev;
+      d = ap - f * duprev;
+      bprev = r - f * bprev;
+    }
+    S.sd[l] = d;
+    S.su[l] = ae;
+    S.rh[l] = bprev;
+    dprev = d; duprev = ae;
+    avw = ave; uw = u0; u0 = ue;
+  }
+  if (npiv) atomicAdd(&S.flags[0], npiv);
+  double x = 0;
+  const double dmul = 1.5 * S.es;
+  for (int p = n - 1; p >= 0; --p) {
+    const int l = lb + (p + 1) * st;
+    double bb = S.rh[l];
+    x = (p == n - 1) ? bb / S.sd[l] : (bb - S.su[l] * x) / S.sd[l];
+    if (DIR == 2) {
+      double nt = S.q[4][l];
+      double qe5 = nt + x;
+      double dum = 1.0 + dmul * S.dtev[l] / S.delti;
+      S.q[4][l] = nt + (-nt + qe5) / dum;
+    } else {
+      S.rh[l] = x;
+    }
+  }
+}
+
+// boundary values of nu_tilde (src/rhs_sa_bcond.F90:40-269): one kernel per
+// face pair in the order i, j, k; full transverse ranges.
+template <int DIR>
+__global__ void k_sa_bc(Sa S) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = blockIdx.y;
+  int amax, n, st, lb;
+  if (DIR == 0) { amax = S.jm; n = S.im; st = 1; lb = S.sj * a + S.sk * b; }
+  else if (DIR == 1) { amax = S.im; n = S.jm; st = S.sj; lb = a + S.sk * b; }
+  else { amax = S.im; n = S.km; st = S.sk; lb = a + S.sj * b; }
+  if (a >= amax) return;
+  double* q5 = S.q[4];
+#pragma unroll
+  for (int side = 0; side < 2; ++side) {
+    const int bi = 2 * DIR + side;
+    const int bt = S.btype[bi];
+    const int l = side == 0 ? lb : lb + (n - 1) * st;
+    const int s = side == 0 ? st : -st;
+    if (bt == 1) q5[l] = 0.0;
+    else if (bt == 2 || bt == 3) q5[l] = S.sa1[bi] * q5[l + s] + S.sb1[bi] * q5[l + 2 * s];
+    else if (bt == 6) q5[l] = side == 0 ? q5[lb + (n - 2) * st] : q5[lb + st];
+    else if (bt == 8 && DIR == 0 && side == 1) q5[l] = q5[l - 1];
+  }
+}
+
+// nu_tilde >= 1e-7 and nu_t = nu_tilde f_v1 on every node (src/rhs_sa_bcond.F90:279-291)
+__global__ void k_sa_clamp(Sa S) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= S.N) return;
+  double v = S.q[4][l];
+  v = v > 1.0E-07 ? v : 1.0E-07;
+  S.q[4][l] = v;
+  double chi = v / (1.0 / S.ren);
+  double chic = chi * chi * chi;
+  S.nut[l] = v * (chic / (chic + 357.911));
+}
+
+// ---------------------------------------------------------------- conservation
+// Sums of U/J over the first and last i planes (all j, k), into acc[0..1].
+__global__ void k_cons_sum(Sa S, double* acc) {
+  __shared__ double sh[2][256];
+  double a0 = 0, a1 = 0;
+  const int P = S.jm * S.km;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < P; t += gridDim.x * blockDim.x) {
+    const int j = t % S.jm, k = t / S.jm;
+    a0 += sa_ucn(S, 0, S.sj * j + S.sk * k);
+    a1 += sa_ucn(S, 0, (S.im - 1) + S.sj * j + S.sk * k);
+  }
+  sh[0][threadIdx.x] = a0;
+  sh[1][threadIdx.x] = a1;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) { sh[0][threadIdx.x] += sh[0][threadIdx.x + s]; sh[1][threadIdx.x] += sh[1][threadIdx.x + s]; }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) { acc[0] = sh[0][0]; acc[1] = sh[1][0]; }
+}
+
+// Rescale the outlet plane's U/J by fin/fout and return to Cartesian
+// velocities with the covariant metrics (src/conservation.F90:137-157).
+__global__ void k_cons_apply(Sa S, const double* acc, double* const* cov) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= S.jm * S.km) return;
+  const int j = t % S.jm, k = t / S.jm;
+  const int l = (S.im - 1) + S.sj * j + S.sk * k;
+  const double fin = acc[0], fout = acc[1];
+  const double delta_e = fin - fout;
+  double u1 = sa_ucn(S, 0, l), u2 = sa_ucn(S, 1, l), u3 = sa_ucn(S, 2, l);
+  u1 = u1 + delta_e * u1 / fout;
+  const double a = S.aj[l];
+  S.q[1][l] = a * (u1 * cov[0][l] + u2 * cov[1][l] + u3 * cov[2][l]);
+  S.q[2][l] = a * (u1 * cov[3][l] + u2 * cov[4][l] + u3 * cov[5][l]);
+  S.q[3][l] = a * (u1 * cov[6][l] + u2 * cov[7][l] + u3 * cov[8][l]);
+}
 
 }  // namespace desalm

@@ -180,3 +180,45 @@ def test_mixed_precision_step(oracle_mod):
     for m in range(4):
         err = rel_l2(g.get_field(1, abi.F_Q + m), o.get_field(1, abi.F_Q + m))
         assert err <= 2e-5, (m, err)
+
+
+def _small_channel(seed=61):
+    case, grid, state = cases.channel(im=17, jm=17, km=17, seed=seed)
+    return case, grid, state
+
+
+def test_des_eddy(oracle_mod):
+    case, grid, state = _small_channel()
+    case.itk = 2
+    g, o = make_pair(case, grid, state, oracle_mod)
+    for s in (g, o):
+        s.des_eddy()
+    check_fields(g, o, 1, [abi.F_Q + 4, abi.F_NUT], TOL64, "des_eddy")
+
+
+def test_conservation(oracle_mod):
+    case, grid, state = _reshape_cavity((17, 17, 17), seed=71)
+    case.btype[0] = abi.BC_INFLOW
+    case.btype[1] = abi.BC_FREESTREAM
+    rng = np.random.default_rng(72)
+    q = state["q"].reshape(-1, 5)
+    q[:, 1] = 1.0 + 0.05 * rng.normal(size=q.shape[0])
+    state["q"] = q.reshape(-1)
+    g, o = make_pair(case, grid, state, oracle_mod)
+    for s in (g, o):
+        s.conservation()
+    check_fields(g, o, 1, Q4, TOL64, "conservation")
+
+
+@pytest.mark.parametrize("precision", [abi.FP64, abi.MIXED])
+def test_pseudo_iterations_channel_sa(precision, oracle_mod):
+    case, grid, state = _small_channel(seed=81)
+    case.precision_mode = precision
+    g, o = make_pair(case, grid, state, oracle_mod)
+    g.begin_step()
+    o.begin_step()
+    tol = 1e-10 if precision == abi.FP64 else 5e-5
+    for it in range(4):
+        g.pseudo_iteration()
+        o.pseudo_iteration()
+    check_fields(g, o, 1, Q4 + [abi.F_Q + 4, abi.F_NUT], tol, "SA pseudo-iterations")
