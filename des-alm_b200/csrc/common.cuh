@@ -39,8 +39,12 @@ struct Lv {
   const T* aj;
   // DAF work: transformed residual, forward-elimination scratch
   W* wk[4];
-  W* sd[3];        // eliminated diagonal: systems (1,2), 3, 4
-  W* su[3];        // super-diagonal: systems (1,2), 3, 4
+  W* sd[4];        // eliminated diagonal, one array per system
+  W* su[3];        // super-diagonal: systems (1,2), 3, 4 (first-generation sweep)
+  W* tc[3];        // per direction: tmp = dtau ep spr dsq (diagonal part of each row)
+  W* hc[3];        // per direction: dtau (dxi/2) spr (neighbour coupling of the
+                   // characteristic rows); also set on the boundary nodes that
+                   // precede/follow the interior lines
   W* bi;           // i-face boundary vectors: [2][4][jm*km]
   W* bj;           // j-face: [4][4][im*km]  (rows 2, 3, jm-1, jm-2 after the i sweep)
   W* bk;           // k-face: [4][4][im*jm]

@@ -161,7 +161,8 @@ int alloc_level(desalm_ctx* ctx, Level& G, Lv<T, W>& L) {
   }
   RET(A((T**)&L.aj));
   for (int m = 0; m < 4; ++m) RET(AW(&L.wk[m]));
-  for (int m = 0; m < 3; ++m) { RET(AW(&L.sd[m])); RET(AW(&L.su[m])); }
+  for (int m = 0; m < 4; ++m) RET(AW(&L.sd[m]));
+  for (int m = 0; m < 3; ++m) { RET(AW(&L.su[m])); RET(AW(&L.tc[m])); RET(AW(&L.hc[m])); }
   RET(dalloc(ctx, G.allocs, (void**)&L.bi, sizeof(W) * 8L * G.jm * G.km));
   RET(dalloc(ctx, G.allocs, (void**)&L.bj, sizeof(W) * 16L * G.im * G.km));
   RET(dalloc(ctx, G.allocs, (void**)&L.bk, sizeof(W) * 16L * G.im * G.jm));
@@ -249,12 +250,11 @@ int launch_daf(desalm_ctx* ctx, Lv<T, W>& L, Level& G, int n, int recalc, int it
   const double nin = double(L.im - 2) * (L.jm - 2) * (L.km - 2);
   LAUNCH(KC_RESID, n, nin, k_resid<T, W, 0><<<grid_interior(L), blk3(), 0, s>>>(L, P, upwind, itr == 1 ? 1 : 0, n > 0 ? 1 : 0, bback));
   CKL();
-  const int TB = 64;
-  LAUNCH(KC_SWEEP_I, n, nin, k_sweep<T, W, 0><<<dim3(cdiv(L.jm - 2, TB), L.km - 2), TB, 0, s>>>(L, P, bback, 0));
+  LAUNCH(KC_SWEEP_I, n, nin, k_sweep2<T, W, 0><<<dim3(cdiv(L.jm - 2, 32), L.km - 2), 128, 0, s>>>(L, P, bback, 0));
   CKL();
-  LAUNCH(KC_SWEEP_J, n, nin, k_sweep<T, W, 1><<<dim3(cdiv(L.im - 2, TB), L.km - 2), TB, 0, s>>>(L, P, fine && c.btype[2] != 5, fine && c.btype[3] != 5));
+  LAUNCH(KC_SWEEP_J, n, nin, k_sweep2<T, W, 1><<<dim3(cdiv(L.im - 2, 32), L.km - 2), 128, 0, s>>>(L, P, fine && c.btype[2] != 5, fine && c.btype[3] != 5));
   CKL();
-  LAUNCH(KC_SWEEP_K, n, nin, k_sweep<T, W, 2><<<dim3(cdiv(L.im - 2, TB), L.jm - 2), TB, 0, s>>>(L, P, fine && c.btype[4] != 5,
+  LAUNCH(KC_SWEEP_K, n, nin, k_sweep2<T, W, 2><<<dim3(cdiv(L.im - 2, 32), L.jm - 2), 128, 0, s>>>(L, P, fine && c.btype[4] != 5,
                                                                       fine && c.btype[5] != 5 && c.btype[5] != 6));
   CKL();
   return 0;
@@ -306,12 +306,11 @@ int launch_prolong(desalm_ctx* ctx, Lv<TF, WF>& F, Lv<TC, WC>& C, Level& G) {
   const double nin = double(F.im - 2) * (F.jm - 2) * (F.km - 2);
   LAUNCH(KC_PROLONG, 0, nin, k_prolong_interp<TF, WF, TC, WC><<<grid_interior(F), blk3(), 0, s>>>(F, C, dq, c.icrs, c.jcrs, c.kcrs));
   CKL();
-  const int TB = 64;
-  LAUNCH(KC_RSMOOTH, 0, nin, k_rsmooth<TF, WF, 0><<<dim3(cdiv(F.jm - 2, TB), F.km - 2), TB, 0, s>>>(F, dq, G.fac[0], G.dpr[0], c.ep[1][0], 0));
+  LAUNCH(KC_RSMOOTH, 0, nin, k_rsmooth2<TF, WF, 0><<<dim3(cdiv(F.jm - 2, 32), F.km - 2), 128, 0, s>>>(F, dq, G.fac[0], G.dpr[0], c.ep[1][0], 0));
   CKL();
-  LAUNCH(KC_RSMOOTH, 0, nin, k_rsmooth<TF, WF, 1><<<dim3(cdiv(F.im - 2, TB), F.km - 2), TB, 0, s>>>(F, dq, G.fac[1], G.dpr[1], c.ep[1][1], 0));
+  LAUNCH(KC_RSMOOTH, 0, nin, k_rsmooth2<TF, WF, 1><<<dim3(cdiv(F.im - 2, 32), F.km - 2), 128, 0, s>>>(F, dq, G.fac[1], G.dpr[1], c.ep[1][1], 0));
   CKL();
-  LAUNCH(KC_RSMOOTH, 0, nin, k_rsmooth<TF, WF, 2><<<dim3(cdiv(F.im - 2, TB), F.jm - 2), TB, 0, s>>>(F, dq, G.fac[2], G.dpr[2], c.ep[1][2], 1));
+  LAUNCH(KC_RSMOOTH, 0, nin, k_rsmooth2<TF, WF, 2><<<dim3(cdiv(F.im - 2, 32), F.jm - 2), 128, 0, s>>>(F, dq, G.fac[2], G.dpr[2], c.ep[1][2], 1));
   CKL();
   return 0;
 }

@@ -335,3 +335,41 @@ __global__ void k_dtev(double* const* cov, double* dtev, long n, double cfl2, do
 }
 
 }  // namespace desalm
+
+namespace desalm {
+
+// Second-generation constant-coefficient smoothing: one thread per (line,
+// component); warp m handles component m of 32 lines (coalesced for j and
+// k lines).  Same arithmetic as k_rsmooth.
+template <class TF, class WF, int DIR>
+__global__ void __launch_bounds__(128) k_rsmooth2(Lv<TF, WF> F, TF* dq, const double* fac, const double* dpr, double e, int last) {
+  const int lane = threadIdx.x & 31, m = threadIdx.x >> 5;
+  const int a = blockIdx.x * 32 + lane + 1;
+  const int b = blockIdx.y + 1;
+  int amax, n, st, lb;
+  if (DIR == 0) { amax = F.jm - 2; n = F.im - 2; st = 1; lb = F.sj * a + F.sk * b; }
+  else if (DIR == 1) { amax = F.im - 2; n = F.jm - 2; st = F.sj; lb = a + F.sk * b; }
+  else { amax = F.im - 2; n = F.km - 2; st = F.sk; lb = a + F.sj * b; }
+  if (a > amax) return;
+  TF* v = dq + (long)m * F.N;
+  const TF du = TF(-e);
+  TF bp = 0;
+  for (int p = 0; p < n; ++p) {
+    const int l = lb + (p + 1) * st;
+    TF x = v[l];
+    if (p > 0) x = x - TF(fac[p - 1]) * bp;
+    bp = x;
+    v[l] = x;
+  }
+  TF x = 0;
+  for (int p = n - 1; p >= 0; --p) {
+    const int l = lb + (p + 1) * st;
+    const TF d = TF(dpr[p]);
+    const TF bb = v[l];
+    x = (p == n - 1) ? bb / d : (bb - du * x) / d;
+    if (last) F.q[m][l] = F.q[m][l] + x;
+    else v[l] = x;
+  }
+}
+
+}  // namespace desalm

@@ -240,12 +240,37 @@ __global__ void __launch_bounds__(128) k_resid(Lv<T, W> L, Par P, int upwind, in
 #pragma unroll
     for (int m = 0; m < 4; ++m) b[m * (L.jm * L.km) + o] = W(r[m]);
   }
+  T sg, th;
+  sigma_theta(dtau, P, sg, th);
   M4<T> A;
-  mat_mai(L, P, l, A);
+  modal_inv(L.csi[0][l], L.csi[1][l], L.csi[2][l], sg, A);
   T rp[4];
   mv4(A, r, rp);
 #pragma unroll
   for (int m = 0; m < 4; ++m) L.wk[m][l] = W(rp[m]);
+
+  // ---- line-sweep coefficients of every direction (src/rhs_diag_solver.F90:
+  // 159-181): tmp = dtau ep spr dsq for the node's own row, and
+  // h = dtau (dxi/2) spr, which the neighbouring rows multiply by lambda.
+  // The boundary nodes before/after each line get their h too.
+  const T* const* mt[3] = {L.csi, L.eta, L.zet};
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const T* const* m3 = mt[d];
+    T g = m3[0][l] * m3[0][l] + m3[1][l] * m3[1][l] + m3[2][l] * m3[2][l];
+    T spr = th * sqrt(g);
+    T dq = dsp[d] * dsp[d];
+    T dh = T(0.5) * dsp[d];
+    L.tc[d][l] = W(dtau * T(P.ep1[d]) * spr * dq);
+    L.hc[d][l] = W(dtau * dh * spr);
+    if (pos[d] == 1 || pos[d] == ext[d] - 2) {
+      const int lb = pos[d] == 1 ? l - st[d] : l + st[d];
+      T s2, t2;
+      sigma_theta(L.dtau[lb], P, s2, t2);
+      T g2 = m3[0][lb] * m3[0][lb] + m3[1][lb] * m3[1][lb] + m3[2][lb] * m3[2][lb];
+      L.hc[d][lb] = W(L.dtau[lb] * dh * (t2 * sqrt(g2)));
+    }
+  }
 }
 
 // dtau on every node (src/rhs_daf_dtau.F90:85-117)

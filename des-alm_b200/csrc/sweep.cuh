@@ -189,3 +189,175 @@ __global__ void __launch_bounds__(128) k_sweep(Lv<T, W> L, Par P, int blo, int b
 }
 
 }  // namespace desalm
+
+namespace desalm {
+
+// ---------------------------------------------------------------------------
+// Second-generation sweep: one thread per (line, system).  A CTA owns 32
+// lines; warp m solves system m of all 32 lines, so for j and k lines every
+// row access is coalesced across the warp.  The row coefficients come from
+// the per-node tc/hc arrays written by K_R (no spectral radii recomputed
+// here).  The forward elimination keeps SGTSV's no-interchange order and
+// writes the eliminated right-hand side in place and the eliminated diagonal
+// to sd[m]; the back substitution leaves x in wk.  After a barrier, phase 2
+// walks the CTA's nodes with coalesced indexing and applies the next modal
+// transform (N1^-1, N2^-1) or Mc and the update q <- q + dq.
+// ---------------------------------------------------------------------------
+template <class T, class W, int DIR>
+__global__ void __launch_bounds__(128) k_sweep2(Lv<T, W> L, Par P, int blo, int bhi) {
+  __shared__ W sbw[32][4], sbe[32][4];
+  const int lane = threadIdx.x & 31, m = threadIdx.x >> 5;
+  const int a0 = blockIdx.x * 32 + 1;
+  const int a = a0 + lane;
+  const int b = blockIdx.y + 1;
+  int amax, n, st, sa;  // sa: stride between consecutive lines of the CTA
+  if (DIR == 0) { amax = L.jm - 2; n = L.im - 2; st = 1; sa = L.sj; }
+  else if (DIR == 1) { amax = L.im - 2; n = L.jm - 2; st = L.sj; sa = 1; }
+  else { amax = L.im - 2; n = L.km - 2; st = L.sk; sa = 1; }
+  const int base = (DIR == 0) ? L.sk * b : (DIR == 1 ? L.sk * b : L.sj * b);  // line a = 0 at row -1
+  const bool act = a <= amax;
+  const int lb = base + a * sa;  // boundary node before the line
+
+  // ---- phase 0: semi-explicit boundary vectors (fine level)
+  if (m == 0) {
+    T bw[4] = {0, 0, 0, 0}, be[4] = {0, 0, 0, 0};
+    if (act) {
+      if (DIR == 0) {
+        if (blo) {
+          const int S = L.jm * L.km, o = a + L.jm * b;
+          face_vec<T, W, 0>(L, P, lb, 0, L.bi + o, L.bi + 4 * S + o, S, bw);
+        }
+      } else if (DIR == 1) {
+        const int S = L.im * L.km, o = a + L.im * b;
+        if (blo) face_vec<T, W, 1>(L, P, lb, 2, L.bj + o, L.bj + 4 * S + o, S, bw);
+        if (bhi) face_vec<T, W, 1>(L, P, lb + (n + 1) * st, 3, L.bj + 8 * S + o, L.bj + 12 * S + o, S, be);
+      } else {
+        const int S = L.im * L.jm, o = a + L.im * b;
+        if (blo) face_vec<T, W, 2>(L, P, lb, 4, L.bk + o, L.bk + 4 * S + o, S, bw);
+        if (bhi) face_vec<T, W, 2>(L, P, lb + (n + 1) * st, 5, L.bk + 8 * S + o, L.bk + 12 * S + o, S, be);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) { sbw[lane][q] = W(bw[q]); sbe[lane][q] = W(be[q]); }
+  }
+  __syncthreads();
+
+  // ---- phase 1: scalar tridiagonal solve of system m along the line
+  if (act) {
+    const W bwm = sbw[lane][m], bem = sbe[lane][m];
+    const W* tc = L.tc[DIR];
+    const W* hc = L.hc[DIR];
+    W* r = L.wk[m];
+    W* sd = L.sd[m];
+    W hw = hc[lb];
+    W dprev = 0, duprev = 0, bprev = 0;
+    int npiv = 0, nzero = 0;
+    for (int p = 0; p < n; ++p) {
+      const int l = lb + (p + 1) * st;
+      const W t = tc[l];
+      const W he = hc[l + st];
+      const W hcur = hc[l];
+      const W dw = t != W(0) ? hw : W(0);
+      const W de = t != W(0) ? he : W(0);
+      W aw, ae;
+      if (m < 2) { aw = -t; ae = -t; }
+      else if (m == 2) { aw = -dw - t; ae = de - t; }
+      else { aw = dw - t; ae = -de - t; }
+      const W ap = W(1) + W(2) * t;
+      W rr = r[l];
+      if (p == 0) rr = rr - aw * bwm;
+      if (p == n - 1) rr = rr - ae * bem;
+      W d;
+      if (p == 0) {
+        d = ap;
+        bprev = rr;
+      } else {
+        npiv += dabs(dprev) < dabs(aw);
+        nzero += dprev == W(0);
+        const W f = aw / dprev;
+        d = ap - f * duprev;
+        bprev = rr - f * bprev;
+      }
+      sd[l] = d;
+      r[l] = bprev;
+      dprev = d;
+      duprev = ae;
+      hw = hcur;
+    }
+    nzero += dprev == W(0);
+    if (npiv) atomicAdd(&L.flags[0], npiv);
+    if (nzero) atomicAdd(&L.flags[1], nzero);
+    W x = 0;
+    for (int p = n - 1; p >= 0; --p) {
+      const int l = lb + (p + 1) * st;
+      const W bb = r[l];
+      if (p == n - 1) {
+        x = bb / sd[l];
+      } else {
+        const W t = tc[l];
+        const W he = hc[l + st];
+        const W de = t != W(0) ? he : W(0);
+        W ae;
+        if (m < 2) ae = -t;
+        else if (m == 2) ae = de - t;
+        else ae = -de - t;
+        x = (bb - ae * x) / sd[l];
+      }
+      r[l] = x;
+    }
+  }
+  __syncthreads();
+
+  // ---- phase 2: per-node transform of the CTA's lines
+  const int nl = min(32, amax - a0 + 1);
+  const int total = nl * n;
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    int li, p;
+    if (DIR == 0) { li = t / n; p = t - li * n; }  // consecutive threads walk along i
+    else { p = t / nl; li = t - p * nl; }          // consecutive threads walk across lines (i)
+    const int aa = a0 + li;
+    const int l = base + aa * sa + (p + 1) * st;
+    T xv[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) xv[q] = T(L.wk[q][l]);
+    if (DIR == 0) {
+      // rows j = 2, 3, jm-1, jm-2 (1-based) feed the j-face boundary vectors
+      const int S = L.im * L.km, o = (p + 1) + L.im * b;
+      const int tgt[4] = {1, 2, L.jm - 2, L.jm - 3};
+#pragma unroll
+      for (int s = 0; s < 4; ++s)
+        if (aa == tgt[s])
+#pragma unroll
+          for (int q = 0; q < 4; ++q) L.bj[(s * 4 + q) * S + o] = W(xv[q]);
+      M4<T> A;
+      mat_n1i(L, P, l, A);
+      T y[4];
+      mv4(A, xv, y);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) L.wk[q][l] = W(y[q]);
+    } else if (DIR == 1) {
+      const int S = L.im * L.jm, o = aa + L.im * (p + 1);
+      const int tgt[4] = {1, 2, L.km - 2, L.km - 3};
+#pragma unroll
+      for (int s = 0; s < 4; ++s)
+        if (b == tgt[s])
+#pragma unroll
+          for (int q = 0; q < 4; ++q) L.bk[(s * 4 + q) * S + o] = W(xv[q]);
+      M4<T> A;
+      mat_n2i(L, P, l, A);
+      T y[4];
+      mv4(A, xv, y);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) L.wk[q][l] = W(y[q]);
+    } else {
+      M4<T> A;
+      mat_mc(L, P, l, A);
+      T y[4];
+      mv4(A, xv, y);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) L.q[q][l] = L.q[q][l] + y[q];
+    }
+  }
+}
+
+}  // namespace desalm
