@@ -44,11 +44,11 @@ UNIT = "s/step"
 def alg_bytes(kind, T, W, coarse):
     pk = 4 * T if coarse else 0
     return {
-        "resid": 23 * T + 4 * W + pk,     # q4 qn3 qnm1-3 metrics9 aj nut dtau | wk4 diss1
+        "resid": 23 * T + 10 * W + pk,    # q4 qn3 qnm1-3 metrics9 aj nut dtau | wk4 diss1 tc3 hc3
         "recalc": 26 * T + pk,            # q4 qn3 qnm1-3 metrics9 aj nut diss1 | rh4
-        "sweep_i": 8 * W + 7 * T,         # wk4 in/out, dtau, csi3, eta3
-        "sweep_j": 8 * W + 7 * T,         # wk4 in/out, dtau, eta3, zet3
-        "sweep_k": 4 * W + 12 * T,        # wk4, dtau, zet3, q4 in/out
+        "sweep_i": 10 * W + 7 * T,        # wk4 in/out, tc, hc, dtau, csi3, eta3
+        "sweep_j": 10 * W + 7 * T,        # wk4 in/out, tc, hc, dtau, eta3, zet3
+        "sweep_k": 6 * W + 12 * T,        # wk4, tc, hc, dtau, zet3, q4 in/out
         "dtau": 11 * T,                   # metrics9 nut | dtau
         "norm": 15 * T,                   # q5 qold5 | qold5
         "rsmooth": 8 * T,                 # dq4 in/out (last one: q4 in/out instead)
@@ -69,6 +69,7 @@ def build_case(name, precision, predictor):
         raise SystemExit("unknown case " + name)
     case.precision_mode = precision
     case.predictor = predictor
+    case.use_graph = 1      # each physical step replays one CUDA graph (device-side while loop)
     return case, grid, state, desc
 
 
@@ -202,8 +203,8 @@ def run_ours(args, rank, world, dist):
         S.mg_driver()
     stats, _ = S.kernel_stats()
     S.profile(False)
-    T = {1: 8, 2: 4, 3: 4, 4: 4}
-    W = {1: 4, 2: 4, 3: 4, 4: 4}
+    T = {1: 8, 2: 8, 3: 8, 4: 8}      # MIXED: FP64 state on every level
+    W = {1: 4, 2: 4, 3: 4, 4: 4}      # FP32 line-sweep work
     best = None
     for kind, per in stats.items():
         ms = sum(v[0] for v in per.values())

@@ -25,6 +25,45 @@ using namespace desalm;
 
 namespace {
 
+// Convergence state of the device-side pseudo-time loop.
+struct DevConv {
+  int itc, converged, pivots, nonfinite;
+  double res[5], init[5];
+};
+
+struct ConvPar {
+  int it_min, itmax;
+  double er_min, eo_min, tnu;
+};
+
+// mg_residual + mg_ck_conver on the device (src/mg_residual.F90:77-84,
+// src/mg_driver.F90:372-398): sums the norm partials, updates the loop
+// state and sets the while-node condition of the graph.
+__global__ void k_conv(const double* part, int nblk, DevConv* st, const int* flags, ConvPar cp,
+                       cudaGraphConditionalHandle h) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double res[5];
+  for (int m = 0; m < 5; ++m) {
+    double sum = 0;
+    for (int b = 0; b < nblk; ++b) sum += part[b * 5 + m];
+    res[m] = log10(sum / cp.tnu);
+    st->res[m] = res[m];
+  }
+  st->itc += 1;
+  st->pivots += flags[0];
+  if (st->itc == 1)
+    for (int m = 0; m < 5; ++m) st->init[m] = res[m];
+  double eomax = fmax(res[1], fmax(res[2], res[3]));
+  double ermax = fmax(res[1] - st->init[1], fmax(res[2] - st->init[2], res[3] - st->init[3]));
+  int conv = 0;
+  if (st->itc > cp.it_min && ermax < cp.er_min) conv = 1;
+  if (st->itc > cp.it_min && eomax < cp.eo_min) conv = 1;
+  int finite = isfinite(res[1]) && isfinite(res[2]) && isfinite(res[3]);
+  st->converged = conv;
+  st->nonfinite = !finite;
+  cudaGraphSetConditional(h, (!conv && finite && st->itc < cp.itmax) ? 1u : 0u);
+}
+
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
@@ -76,6 +115,12 @@ struct desalm_ctx {
   std::vector<ProfRec> prof;
   size_t prof_used = 0;
   long launches = 0;
+  // CUDA graph of a physical step's pseudo-time loop (use_graph = 1)
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  long graph_kernels = 0;     // kernels per pseudo-iteration in the graph body
+  DevConv* dconv = nullptr;   // device-side convergence state
+  DevConv* hconv = nullptr;   // pinned host copy
   // driver state
   int itc = 0;
   double init_resd[5] = {0, 0, 0, 0, 0};
@@ -332,10 +377,16 @@ int launch_norm(desalm_ctx* ctx, Lv<T, W>& L, int copy, double* out) {
 }
 
 // dispatch on the active view of a level ------------------------------------
+// FP64 mode: FP64 state and sweeps on every level.  MIXED: FP64 state on
+// every level (residual, metrics, update, restriction, coarse corrections
+// q_c - qold_c, which FP32 storage would lose to cancellation) and FP32
+// line-sweep work (LHS coefficients, eliminated rows, transformed residual).
+// The FP32-state view (K_FF) is kept for experiments only.
 enum Kind { K_DD, K_DF, K_FF };
 Kind kind_of(const desalm_ctx* ctx, int n) {
+  (void)n;
   if (ctx->c.precision_mode == DESALM_FP64) return K_DD;
-  return n == 0 ? K_DF : K_FF;
+  return K_DF;
 }
 
 #define DISPATCH(ctx, n, FN, ...)                                   \
@@ -383,8 +434,8 @@ int do_nlevel(desalm_ctx* ctx, int n) {  // n = coarse level index (>= 1)
   C.dtau_valid = false;
   Kind kf = kind_of(ctx, n - 1), kc = kind_of(ctx, n);
   if (kf == K_DD) return launch_nlevel(ctx, F.dd, C.dd);
+  if (kf == K_DF && kc == K_DF) return launch_nlevel(ctx, F.df, C.df);
   if (kf == K_DF) return launch_nlevel(ctx, F.df, C.ff);
-  (void)kc;
   return launch_nlevel(ctx, F.ff, C.ff);
 }
 
@@ -393,6 +444,8 @@ int do_prolong(desalm_ctx* ctx, int n) {  // fine level index n, coarse n+1
   Level& C = ctx->L[n + 1];
   Kind kf = kind_of(ctx, n);
   if (kf == K_DD) return launch_prolong(ctx, F.dd, C.dd, F);
+  Kind kc = kind_of(ctx, n + 1);
+  if (kf == K_DF && kc == K_DF) return launch_prolong(ctx, F.df, C.df, F);
   if (kf == K_DF) return launch_prolong(ctx, F.df, C.ff, F);
   return launch_prolong(ctx, F.ff, C.ff, F);
 }
@@ -471,6 +524,8 @@ void outlet_ratios(const desalm_case& c, const double* x, const double* y, const
 }
 
 int pseudo_iter(desalm_ctx* ctx, desalm_step_report* rep);
+int enqueue_iteration(desalm_ctx* ctx);
+int graph_step(desalm_ctx* ctx, desalm_step_report* rep);
 int sa_des_eddy(desalm_ctx* ctx);
 int sa_conservation(desalm_ctx* ctx);
 
@@ -488,6 +543,9 @@ void desalm_destroy(desalm_ctx* ctx) {
     for (void* p : G.allocs) cudaFree(p);
   for (void* p : ctx->allocs) cudaFree(p);
   for (auto& r : ctx->prof) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+  if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+  if (ctx->graph) cudaGraphDestroy(ctx->graph);
+  if (ctx->hconv) cudaFreeHost(ctx->hconv);
   if (ctx->h_norm) cudaFreeHost(ctx->h_norm);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -932,6 +990,7 @@ int desalm_pseudo_iteration(desalm_ctx* ctx, desalm_step_report* rep) {
 int desalm_mg_driver(desalm_ctx* ctx, desalm_step_report* rep) {
   if (!ctx) return DESALM_EINVAL;
   RET(desalm_begin_step(ctx));
+  if (ctx->c.use_graph && !ctx->prof_on) return graph_step(ctx, rep);
   desalm_step_report r{};
   int piv = 0;
   for (int it = 1; it <= ctx->c.itmax; ++it) {
@@ -957,9 +1016,11 @@ namespace {
 // One pseudo-time iteration (src/mg_driver.F90:81-316).  qold_mg of the fine
 // level holds q at the start of the iteration (set by desalm_begin_step for
 // the first one and by the norm kernel of the previous one).
-int pseudo_iter(desalm_ctx* ctx, desalm_step_report* rep) {
+// The kernels of one pseudo-time iteration up to bcond_fm
+// (src/mg_driver.F90:98-304), enqueued on the context stream; used eagerly
+// and under stream capture.
+int enqueue_iteration(desalm_ctx* ctx) {
   const desalm_case& c = ctx->c;
-  ctx->itc++;
   CK(cudaMemsetAsync(ctx->flags, 0, 2 * sizeof(int), ctx->stream));
   int recalc = 0;
   for (int n = 0; n < ctx->ng; ++n) {
@@ -975,6 +1036,13 @@ int pseudo_iter(desalm_ctx* ctx, desalm_step_report* rep) {
   }
   for (int n = ctx->ng - 2; n >= 0; --n) RET(do_prolong(ctx, n));
   RET(do_bcond(ctx));
+  return 0;
+}
+
+int pseudo_iter(desalm_ctx* ctx, desalm_step_report* rep) {
+  const desalm_case& c = ctx->c;
+  ctx->itc++;
+  RET(enqueue_iteration(ctx));
   double res[5];
   RET(do_norm(ctx, 0, 1, res));
   int hflags[2] = {0, 0};
@@ -1112,6 +1180,96 @@ int sa_des_eddy(desalm_ctx* ctx) {
 
 int sa_conservation(desalm_ctx* ctx) {
   return kind_of(ctx, 0) == K_DD ? cons_run(ctx, ctx->L[0].dd) : cons_run(ctx, ctx->L[0].df);
+}
+
+}  // namespace
+
+namespace {
+
+// Build (once) the graph of a physical step's pseudo-time loop: a while
+// conditional node whose body is one pseudo-iteration followed by the norm
+// and k_conv, which decides on the device whether to run another iteration
+// (no host round trip per pseudo-iteration).
+int build_graph(desalm_ctx* ctx) {
+  cudaStream_t s = ctx->stream;
+  // laminar fine-level dtau never changes: make it valid outside the graph
+  if (!ctx->c.turbulence && !ctx->L[0].dtau_valid) {
+    Level& G = ctx->L[0];
+    Par P = ctx->par;
+    P.fine = 1;
+    if (kind_of(ctx, 0) == K_DD) LAUNCH(KC_DTAU, 0, G.N, k_dtau<double, double><<<cdiv(G.N, 256), 256, 0, s>>>(G.dd, P));
+    else LAUNCH(KC_DTAU, 0, G.N, k_dtau<double, float><<<cdiv(G.N, 256), 256, 0, s>>>(G.df, P));
+    CKL();
+    G.dtau_valid = true;
+  }
+  if (!ctx->dconv) {
+    RET(dalloc(ctx, ctx->allocs, (void**)&ctx->dconv, sizeof(DevConv)));
+    if (cudaMallocHost((void**)&ctx->hconv, sizeof(DevConv)) != cudaSuccess) { ctx->err = "cudaMallocHost"; return DESALM_ENOMEM; }
+  }
+  CK(cudaStreamSynchronize(s));
+  cudaGraph_t g = nullptr;
+  CK(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle h;
+  CK(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  CK(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  long l0 = ctx->launches;
+  CK(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  int rc = enqueue_iteration(ctx);
+  Level& G = ctx->L[0];
+  const int nb = ctx->part_blocks;
+  const long total = (long)(G.im - 2) * (G.jm - 2) * (G.km - 2);
+  ConvPar cv{ctx->c.it_min, ctx->c.itmax, ctx->c.er_min, ctx->c.eo_min, double(total)};
+  if (!rc) {
+    int nbu = (int)std::min<long>(nb, std::max<long>(1, cdiv(total, 256)));
+    if (kind_of(ctx, 0) == K_DD) LAUNCH(KC_NORM, 0, double(total), k_norm_partial<double, double><<<nbu, 256, 0, s>>>(G.dd, ctx->part, 5, 1));
+    else LAUNCH(KC_NORM, 0, double(total), k_norm_partial<double, float><<<nbu, 256, 0, s>>>(G.df, ctx->part, 5, 1));
+    LAUNCH(KC_NORM, 0, 0, k_conv<<<1, 32, 0, s>>>(ctx->part, nbu, ctx->dconv, ctx->flags, cv, h));
+  }
+  cudaGraph_t out = nullptr;
+  cudaError_t e = cudaStreamEndCapture(s, &out);
+  if (rc || e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    if (!rc) ctx->err = std::string("graph capture: ") + cudaGetErrorString(e);
+    return rc ? rc : DESALM_ECUDA;
+  }
+  ctx->graph_kernels = ctx->launches - l0;
+  ctx->launches = l0;
+  e = cudaGraphInstantiate(&ctx->gexec, g, 0);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    ctx->err = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e);
+    return DESALM_ECUDA;
+  }
+  ctx->graph = g;
+  return 0;
+}
+
+int graph_step(desalm_ctx* ctx, desalm_step_report* rep) {
+  if (!ctx->gexec) RET(build_graph(ctx));
+  cudaStream_t s = ctx->stream;
+  CK(cudaMemsetAsync(ctx->dconv, 0, sizeof(DevConv), s));
+  CK(cudaGraphLaunch(ctx->gexec, s));
+  CK(cudaMemcpyAsync(ctx->hconv, ctx->dconv, sizeof(DevConv), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  const DevConv& st = *ctx->hconv;
+  ctx->itc = st.itc;
+  for (int m = 0; m < 5; ++m) ctx->init_resd[m] = st.init[m];
+  ctx->launches += ctx->graph_kernels * st.itc;
+  if (rep) {
+    rep->iterations = st.itc;
+    rep->converged = st.converged;
+    for (int m = 0; m < 5; ++m) { rep->residual[m] = st.res[m]; rep->init_residual[m] = st.init[m]; }
+    rep->pivots = st.pivots;
+  }
+  if (st.nonfinite) { ctx->err = "non-finite convergence norm"; return DESALM_ENONFINITE; }
+  return 0;
 }
 
 }  // namespace

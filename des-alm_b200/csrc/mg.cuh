@@ -353,22 +353,46 @@ __global__ void __launch_bounds__(128) k_rsmooth2(Lv<TF, WF> F, TF* dq, const do
   if (a > amax) return;
   TF* v = dq + (long)m * F.N;
   const TF du = TF(-e);
+  constexpr int R = 8;
   TF bp = 0;
-  for (int p = 0; p < n; ++p) {
-    const int l = lb + (p + 1) * st;
-    TF x = v[l];
-    if (p > 0) x = x - TF(fac[p - 1]) * bp;
-    bp = x;
-    v[l] = x;
+  for (int p0 = 0; p0 < n; p0 += R) {
+    TF bv[R];
+#pragma unroll
+    for (int u = 0; u < R; ++u)
+      if (p0 + u < n) bv[u] = v[lb + (p0 + u + 1) * st];
+#pragma unroll
+    for (int u = 0; u < R; ++u) {
+      const int p = p0 + u;
+      if (p < n) {
+        TF x = bv[u];
+        if (p > 0) x = x - TF(fac[p - 1]) * bp;
+        bp = x;
+        v[lb + (p + 1) * st] = x;
+      }
+    }
   }
   TF x = 0;
-  for (int p = n - 1; p >= 0; --p) {
-    const int l = lb + (p + 1) * st;
-    const TF d = TF(dpr[p]);
-    const TF bb = v[l];
-    x = (p == n - 1) ? bb / d : (bb - du * x) / d;
-    if (last) F.q[m][l] = F.q[m][l] + x;
-    else v[l] = x;
+  for (int p1 = n - 1; p1 >= 0; p1 -= R) {
+    TF bv[R], bq[R];
+#pragma unroll
+    for (int u = 0; u < R; ++u) {
+      const int p = p1 - u;
+      if (p >= 0) {
+        bv[u] = v[lb + (p + 1) * st];
+        if (last) bq[u] = F.q[m][lb + (p + 1) * st];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < R; ++u) {
+      const int p = p1 - u;
+      if (p >= 0) {
+        const int l = lb + (p + 1) * st;
+        const TF d = TF(dpr[p]);
+        x = (p == n - 1) ? bv[u] / d : (bv[u] - du * x) / d;
+        if (last) F.q[m][l] = bq[u] + x;
+        else v[l] = x;
+      }
+    }
   }
 }
 

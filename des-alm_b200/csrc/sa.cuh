@@ -207,57 +207,104 @@ __global__ void __launch_bounds__(128) k_sa_sweep(Sa S) {
   const double* const* mt = DIR == 0 ? S.csi : (DIR == 1 ? S.eta : S.zet);
   const double sig = 2.0 / 3.0, rei = 1.0 / S.ren;
   const double* q5 = S.q[4];
-  auto face = [&](int l0) {
-    const int l1 = l0 + st;
-    double gx = mt[0][l1] + mt[0][l0], gy = mt[1][l1] + mt[1][l0], gz = mt[2][l1] + mt[2][l0];
-    double ev = (rei + 0.5 * (q5[l1] + q5[l0])) / sig;
-    double ucna = 0.5 * fabs(sa_ucn(S, DIR, l1) + sa_ucn(S, DIR, l0));
-    return ucna + ev * (gx * gx + gy * gy + gz * gz) / (S.aj[l1] + S.aj[l0]);
+  // per-node data along the line: metric vector of this direction, nu, J, U/J
+  struct Nd { double m0, m1, m2, nu, aj, u; };
+  auto load = [&](int l) {
+    Nd d;
+    d.m0 = mt[0][l]; d.m1 = mt[1][l]; d.m2 = mt[2][l];
+    d.nu = q5[l]; d.aj = S.aj[l];
+    const double tmp = 1.0 / d.aj;
+    d.u = tmp * (d.m0 * S.q[1][l] + d.m1 * S.q[2][l] + d.m2 * S.q[3][l]);
+    return d;
   };
-  double avw = face(lb);                 // face between the boundary node and row 0
-  double uw = sa_ucn(S, DIR, lb);        // U/J of the node before the current row
-  double u0 = sa_ucn(S, DIR, lb + st);
+  // av on the face between nodes A and B = A + st (src/rhs_sa_adi_solver.F90:53-63)
+  auto face = [&](const Nd& A, const Nd& B) {
+    double gx = B.m0 + A.m0, gy = B.m1 + A.m1, gz = B.m2 + A.m2;
+    double ev = (rei + 0.5 * (B.nu + A.nu)) / sig;
+    double ucna = 0.5 * fabs(B.u + A.u);
+    return ucna + ev * (gx * gx + gy * gy + gz * gz) / (B.aj + A.aj);
+  };
+  constexpr int R = 4;
+  Nd prev = load(lb), cur = load(lb + st);
+  double avw = face(prev, cur);
+  double uw = prev.u;
   double dprev = 0, duprev = 0, bprev = 0;
   int npiv = 0;
-  for (int p = 0; p < n; ++p) {
-    const int l = lb + (p + 1) * st;
-    double ave = face(l);
-    double ue = sa_ucn(S, DIR, l + st);
-    double dtj = 0.5 * S.dtev[l] * S.aj[l];
-    double aw = -dtj * (uw + avw);
-    double ap = 1.0 + dtj * (avw + ave);
-    double ae = dtj * (ue - ave);
-    double r = S.rh[l];
-    double d;
-    if (p == 0) {
-      d = ap;
-      bprev = r;
-    } else {
-      npiv += fabs(dprev) < fabs(aw);
-      double f = aw / dprev;
-      d = ap - f * duprev;
-      bprev = r - f * bprev;
+  for (int p0 = 0; p0 < n; p0 += R) {
+    Nd east[R];
+    double bdt[R], brh[R];
+#pragma unroll
+    for (int u = 0; u < R; ++u) {
+      const int p = p0 + u;
+      if (p < n) {
+        const int l = lb + (p + 1) * st;
+        east[u] = load(l + st);
+        bdt[u] = S.dtev[l];
+        brh[u] = S.rh[l];
+      }
     }
-    S.sd[l] = d;
-    S.su[l] = ae;
-    S.rh[l] = bprev;
-    dprev = d; duprev = ae;
-    avw = ave; uw = u0; u0 = ue;
+#pragma unroll
+    for (int u = 0; u < R; ++u) {
+      const int p = p0 + u;
+      if (p < n) {
+        const int l = lb + (p + 1) * st;
+        const double ave = face(cur, east[u]);
+        const double dtj = 0.5 * bdt[u] * cur.aj;
+        const double aw = -dtj * (uw + avw);
+        const double ap = 1.0 + dtj * (avw + ave);
+        const double ae = dtj * (east[u].u - ave);
+        double d;
+        if (p == 0) {
+          d = ap;
+          bprev = brh[u];
+        } else {
+          npiv += fabs(dprev) < fabs(aw);
+          const double f = aw / dprev;
+          d = ap - f * duprev;
+          bprev = brh[u] - f * bprev;
+        }
+        S.sd[l] = d;
+        S.su[l] = ae;
+        S.rh[l] = bprev;
+        dprev = d;
+        duprev = ae;
+        avw = ave;
+        uw = cur.u;
+        cur = east[u];
+      }
+    }
   }
   if (npiv) atomicAdd(&S.flags[0], npiv);
   double x = 0;
   const double dmul = 1.5 * S.es;
-  for (int p = n - 1; p >= 0; --p) {
-    const int l = lb + (p + 1) * st;
-    double bb = S.rh[l];
-    x = (p == n - 1) ? bb / S.sd[l] : (bb - S.su[l] * x) / S.sd[l];
-    if (DIR == 2) {
-      double nt = S.q[4][l];
-      double qe5 = nt + x;
-      double dum = 1.0 + dmul * S.dtev[l] / S.delti;
-      S.q[4][l] = nt + (-nt + qe5) / dum;
-    } else {
-      S.rh[l] = x;
+  for (int p1 = n - 1; p1 >= 0; p1 -= R) {
+    double bb[R], bd[R], bu[R], bn[R], bt[R];
+#pragma unroll
+    for (int u = 0; u < R; ++u) {
+      const int p = p1 - u;
+      if (p >= 0) {
+        const int l = lb + (p + 1) * st;
+        bb[u] = S.rh[l];
+        bd[u] = S.sd[l];
+        bu[u] = S.su[l];
+        if (DIR == 2) { bn[u] = S.q[4][l]; bt[u] = S.dtev[l]; }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < R; ++u) {
+      const int p = p1 - u;
+      if (p >= 0) {
+        const int l = lb + (p + 1) * st;
+        x = (p == n - 1) ? bb[u] / bd[u] : (bb[u] - bu[u] * x) / bd[u];
+        if (DIR == 2) {
+          const double nt = bn[u];
+          const double qe5 = nt + x;
+          const double dum = 1.0 + dmul * bt[u] / S.delti;
+          S.q[4][l] = nt + (-nt + qe5) / dum;
+        } else {
+          S.rh[l] = x;
+        }
+      }
     }
   }
 }

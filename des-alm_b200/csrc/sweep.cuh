@@ -242,68 +242,105 @@ __global__ void __launch_bounds__(128) k_sweep2(Lv<T, W> L, Par P, int blo, int 
   }
   __syncthreads();
 
-  // ---- phase 1: scalar tridiagonal solve of system m along the line
+  // ---- phase 1: scalar tridiagonal solve of system m along the line.
+  // Rows are processed in blocks of R: all loads of a block are issued
+  // before any of its stores, so R rows of memory latency overlap.
   if (act) {
+    constexpr int R = 8;
     const W bwm = sbw[lane][m], bem = sbe[lane][m];
     const W* tc = L.tc[DIR];
     const W* hc = L.hc[DIR];
     W* r = L.wk[m];
     W* sd = L.sd[m];
-    W hw = hc[lb];
+    W hw = hc[lb];            // h of the node before the current row
+    W hcur = hc[lb + st];     // h of the current row's node
     W dprev = 0, duprev = 0, bprev = 0;
     int npiv = 0, nzero = 0;
-    for (int p = 0; p < n; ++p) {
-      const int l = lb + (p + 1) * st;
-      const W t = tc[l];
-      const W he = hc[l + st];
-      const W hcur = hc[l];
-      const W dw = t != W(0) ? hw : W(0);
-      const W de = t != W(0) ? he : W(0);
-      W aw, ae;
-      if (m < 2) { aw = -t; ae = -t; }
-      else if (m == 2) { aw = -dw - t; ae = de - t; }
-      else { aw = dw - t; ae = -de - t; }
-      const W ap = W(1) + W(2) * t;
-      W rr = r[l];
-      if (p == 0) rr = rr - aw * bwm;
-      if (p == n - 1) rr = rr - ae * bem;
-      W d;
-      if (p == 0) {
-        d = ap;
-        bprev = rr;
-      } else {
-        npiv += dabs(dprev) < dabs(aw);
-        nzero += dprev == W(0);
-        const W f = aw / dprev;
-        d = ap - f * duprev;
-        bprev = rr - f * bprev;
+    for (int p0 = 0; p0 < n; p0 += R) {
+      W bt[R], bh[R], br[R];
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int p = p0 + u;
+        if (p < n) {
+          const int l = lb + (p + 1) * st;
+          bt[u] = tc[l];
+          bh[u] = hc[l + st];
+          br[u] = r[l];
+        }
       }
-      sd[l] = d;
-      r[l] = bprev;
-      dprev = d;
-      duprev = ae;
-      hw = hcur;
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int p = p0 + u;
+        if (p < n) {
+          const int l = lb + (p + 1) * st;
+          const W t = bt[u];
+          const W he = bh[u];
+          const W dw = t != W(0) ? hw : W(0);
+          const W de = t != W(0) ? he : W(0);
+          W aw, ae;
+          if (m < 2) { aw = -t; ae = -t; }
+          else if (m == 2) { aw = -dw - t; ae = de - t; }
+          else { aw = dw - t; ae = -de - t; }
+          const W ap = W(1) + W(2) * t;
+          W rr = br[u];
+          if (p == 0) rr = rr - aw * bwm;
+          if (p == n - 1) rr = rr - ae * bem;
+          W d;
+          if (p == 0) {
+            d = ap;
+            bprev = rr;
+          } else {
+            npiv += dabs(dprev) < dabs(aw);
+            nzero += dprev == W(0);
+            const W f = aw / dprev;
+            d = ap - f * duprev;
+            bprev = rr - f * bprev;
+          }
+          sd[l] = d;
+          r[l] = bprev;
+          dprev = d;
+          duprev = ae;
+          hw = hcur;
+          hcur = he;
+        }
+      }
     }
     nzero += dprev == W(0);
     if (npiv) atomicAdd(&L.flags[0], npiv);
     if (nzero) atomicAdd(&L.flags[1], nzero);
     W x = 0;
-    for (int p = n - 1; p >= 0; --p) {
-      const int l = lb + (p + 1) * st;
-      const W bb = r[l];
-      if (p == n - 1) {
-        x = bb / sd[l];
-      } else {
-        const W t = tc[l];
-        const W he = hc[l + st];
-        const W de = t != W(0) ? he : W(0);
-        W ae;
-        if (m < 2) ae = -t;
-        else if (m == 2) ae = de - t;
-        else ae = -de - t;
-        x = (bb - ae * x) / sd[l];
+    for (int p1 = n - 1; p1 >= 0; p1 -= R) {
+      W bb[R], bd[R], bt[R], bh[R];
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int p = p1 - u;
+        if (p >= 0) {
+          const int l = lb + (p + 1) * st;
+          bb[u] = r[l];
+          bd[u] = sd[l];
+          bt[u] = tc[l];
+          bh[u] = hc[l + st];
+        }
       }
-      r[l] = x;
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int p = p1 - u;
+        if (p >= 0) {
+          const int l = lb + (p + 1) * st;
+          if (p == n - 1) {
+            x = bb[u] / bd[u];
+          } else {
+            const W t = bt[u];
+            const W de = t != W(0) ? bh[u] : W(0);
+            W ae;
+            if (m < 2) ae = -t;
+            else if (m == 2) ae = de - t;
+            else ae = -de - t;
+            x = (bb[u] - ae * x) / bd[u];
+          }
+          r[l] = x;
+        }
+      }
     }
   }
   __syncthreads();

@@ -222,3 +222,31 @@ def test_pseudo_iterations_channel_sa(precision, oracle_mod):
         g.pseudo_iteration()
         o.pseudo_iteration()
     check_fields(g, o, 1, Q4 + [abi.F_Q + 4, abi.F_NUT], tol, "SA pseudo-iterations")
+
+
+@pytest.mark.parametrize("which", ["cavity", "channel"])
+def test_graph_step_matches_eager(which, oracle_mod):
+    """use_graph = 1 replays the pseudo-time loop as one CUDA graph with a
+    device-side while node; it must reproduce the eager driver exactly."""
+    from desalm.solver import Solver
+    if which == "cavity":
+        case, grid, state = cases.cavity(n=17, seed=91, itmax=9)
+    else:
+        case, grid, state = _small_channel(seed=92)
+        case.itmax = 7
+    case.it_min = 3
+    case.er_min = -0.5       # converges inside the cap on some steps
+    out = []
+    for graph in (0, 1):
+        c = case.copy()
+        c.use_graph = graph
+        s = Solver(c)
+        s.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
+        s.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
+        reps = [s.mg_driver() for _ in range(3)]
+        out.append((reps, s.get_state()))
+    (r0, s0), (r1, s1) = out
+    for a, b in zip(r0, r1):
+        assert a["iterations"] == b["iterations"] and a["converged"] == b["converged"]
+        assert np.allclose(a["residual"][:4], b["residual"][:4], rtol=0, atol=1e-12)
+    assert np.array_equal(s0["q"], s1["q"])
