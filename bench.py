@@ -114,6 +114,17 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def over_ranks(x, op, dist, device="cuda"):
+    """Reduce one timing over the replicas (op = "max" or "sum"); the only
+    cross-rank step of the benchmark (the data path has no collective)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def run_ours(args, rank, world, dist):
     import torch
     from desalm.solver import Solver
@@ -127,18 +138,10 @@ def run_ours(args, rank, world, dist):
             dist.barrier()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return over_ranks(x, "max", dist)
 
     def sum_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+        return over_ranks(x, "sum", dist)
 
     def timed_steps(S, K, body):
         """K calls of body(), bracketed by barrier + synchronize, CUDA events

@@ -397,3 +397,121 @@ __global__ void __launch_bounds__(128) k_rsmooth2(Lv<TF, WF> F, TF* dq, const do
 }
 
 }  // namespace desalm
+
+namespace desalm {
+
+// Two-ended constant-coefficient smoothing: warps 0-3 eliminate the upper
+// half of component m top-down, warps 4-7 the lower half bottom-up (the
+// matrix is symmetric Toeplitz, so the bottom-up eliminated diagonal and
+// multipliers are the top-down ones mirrored); the halves meet in a 2x2
+// solve and back-substitute.  Same operator as k_rsmooth2, twice the threads.
+template <class TF, class WF, int DIR>
+__global__ void __launch_bounds__(256) k_rsmooth3(Lv<TF, WF> F, TF* dq, const double* fac, const double* dpr, double e, int last) {
+  __shared__ TF s_top[32][4][2], s_bot[32][4][2];  // (eliminated b, nothing) of the middle rows
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int m = w & 3, half = w >> 2;
+  const int a = blockIdx.x * 32 + lane + 1;
+  const int b = blockIdx.y + 1;
+  int amax, n, st, lb;
+  if (DIR == 0) { amax = F.jm - 2; n = F.im - 2; st = 1; lb = F.sj * a + F.sk * b; }
+  else if (DIR == 1) { amax = F.im - 2; n = F.jm - 2; st = F.sj; lb = a + F.sk * b; }
+  else { amax = F.im - 2; n = F.km - 2; st = F.sk; lb = a + F.sj * b; }
+  const bool act = a <= amax;
+  TF* v = dq + (long)m * F.N;
+  const TF off = TF(-e);
+  const int h = n / 2;
+  constexpr int R = 8;
+  if (act && half == 0) {
+    TF bp = 0;
+    for (int p0 = 0; p0 < h; p0 += R) {
+      TF bv[R];
+#pragma unroll
+      for (int u = 0; u < R; ++u)
+        if (p0 + u < h) bv[u] = v[lb + (p0 + u + 1) * st];
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int p = p0 + u;
+        if (p < h) {
+          TF x = bv[u];
+          if (p > 0) x = x - TF(fac[p - 1]) * bp;
+          bp = x;
+          v[lb + (p + 1) * st] = x;
+        }
+      }
+    }
+    s_top[lane][m][0] = bp;
+  } else if (act && half == 1) {
+    TF bp = 0;
+    for (int p0 = n - 1; p0 >= h; p0 -= R) {
+      TF bv[R];
+#pragma unroll
+      for (int u = 0; u < R; ++u)
+        if (p0 - u >= h) bv[u] = v[lb + (p0 - u + 1) * st];
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int p = p0 - u;
+        if (p >= h) {
+          TF x = bv[u];
+          if (p < n - 1) x = x - TF(fac[n - 2 - p]) * bp;
+          bp = x;
+          v[lb + (p + 1) * st] = x;
+        }
+      }
+    }
+    s_bot[lane][m][0] = bp;
+  }
+  __syncthreads();
+  if (!act) return;
+  const TF d1 = TF(dpr[h - 1]), d2 = TF(dpr[n - 1 - h]);
+  const TF b1 = s_top[lane][m][0], b2 = s_bot[lane][m][0];
+  const TF det = d1 * d2 - off * off;
+  const TF x1 = (b1 * d2 - off * b2) / det;
+  const TF x2 = (d1 * b2 - off * b1) / det;
+  if (half == 0) {
+    TF x = x1;
+    {
+      const int l = lb + h * st;
+      if (last) F.q[m][l] = F.q[m][l] + x1; else v[l] = x1;
+    }
+    for (int p1 = h - 2; p1 >= 0; p1 -= R) {
+      TF bv[R], bq[R];
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int p = p1 - u;
+        if (p >= 0) { bv[u] = v[lb + (p + 1) * st]; if (last) bq[u] = F.q[m][lb + (p + 1) * st]; }
+      }
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int p = p1 - u;
+        if (p >= 0) {
+          x = (bv[u] - off * x) / TF(dpr[p]);
+          if (last) F.q[m][lb + (p + 1) * st] = bq[u] + x; else v[lb + (p + 1) * st] = x;
+        }
+      }
+    }
+  } else {
+    TF x = x2;
+    {
+      const int l = lb + (h + 1) * st;
+      if (last) F.q[m][l] = F.q[m][l] + x2; else v[l] = x2;
+    }
+    for (int p0 = h + 1; p0 < n; p0 += R) {
+      TF bv[R], bq[R];
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int p = p0 + u;
+        if (p < n) { bv[u] = v[lb + (p + 1) * st]; if (last) bq[u] = F.q[m][lb + (p + 1) * st]; }
+      }
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int p = p0 + u;
+        if (p < n) {
+          x = (bv[u] - off * x) / TF(dpr[n - 1 - p]);
+          if (last) F.q[m][lb + (p + 1) * st] = bq[u] + x; else v[lb + (p + 1) * st] = x;
+        }
+      }
+    }
+  }
+}
+
+}  // namespace desalm

@@ -97,9 +97,15 @@ DESALM_DEV T diss_fv(const Lv<T, W>& L, int dir, int l, int st, T dsq) {
   return tmp1 * tmp2;
 }
 
+// Minimum resident CTAs per SM requested from the register allocator for
+// K_R (128 threads each); a build-time tuning knob.
+#ifndef DESALM_KR_MINBLOCKS
+#define DESALM_KR_MINBLOCKS 3
+#endif
+
 // MODE 0: first pass of a DAF step; MODE 1: recalculation for restriction.
 template <class T, class W, int MODE>
-__global__ void __launch_bounds__(128) k_resid(Lv<T, W> L, Par P, int upwind, int calc_pk, int coarse, int bback) {
+__global__ void __launch_bounds__(128, DESALM_KR_MINBLOCKS) k_resid(Lv<T, W> L, Par P, int upwind, int calc_pk, int coarse, int bback) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int k = blockIdx.z + 1;

@@ -14,7 +14,8 @@ import numpy as np
 from .abi import Case, StepReport, level_dims
 
 PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-LIB_PATH = os.path.join(PKG_ROOT, "libdesalm.so")
+# DESALM_LIBRARY selects another build of the same library (tuning variants)
+LIB_PATH = os.environ.get("DESALM_LIBRARY") or os.path.join(PKG_ROOT, "libdesalm.so")
 _LIB = None
 
 
