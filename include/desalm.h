@@ -191,6 +191,22 @@ int  desalm_kernel_stats(desalm_ctx* ctx, double* ms, long* launches,
                          double* nodes, long* total_launches);
 int  desalm_kernel_class_count(void);
 
+/* No counterpart in the reference.  desalm_mg_residual for callers that
+ * cannot allocate device memory (code running under CUDA stream capture,
+ * hosts whose device memory belongs to another allocator): the same five
+ * log10 mean |q - qold| values over the interior of an im x jm x km level,
+ * from caller-owned device arrays q and qold (five fields of im*jm*km
+ * doubles each, field-major, i fastest), written to the host array res.
+ * Allocates nothing: its scratch is a fixed device array of about 2.5 MiB
+ * held by every GPU that loads the library until exit.  Grids with more than
+ * 134,217,728 interior nodes do not fit it and are rejected with
+ * DESALM_ENOMEM before any work is queued.  Calls share the
+ * scratch, so calls that overlap on the GPU race; the first call on each
+ * device resolves the scratch's address and should come before any stream
+ * capture.  stream may be NULL (the legacy default stream). */
+int  desalm_mg_residual_noalloc(const double* q, const double* qold, int im,
+                                int jm, int km, double res[5], void* stream);
+
 #ifdef __cplusplus
 }
 #endif
