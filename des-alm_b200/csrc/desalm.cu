@@ -41,12 +41,12 @@ struct ConvPar {
 // state and sets the while-node condition of the graph.
 __global__ void k_conv(const double* part, int nblk, DevConv* st, const int* flags, ConvPar cp,
                        cudaGraphConditionalHandle h) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double sums[5];
+  desalm::block_sum5(part, nblk, sums);   // every thread gets the sums
+  if (threadIdx.x != 0) return;
   double res[5];
   for (int m = 0; m < 5; ++m) {
-    double sum = 0;
-    for (int b = 0; b < nblk; ++b) sum += part[b * 5 + m];
-    res[m] = log10(sum / cp.tnu);
+    res[m] = log10(sums[m] / cp.tnu);
     st->res[m] = res[m];
   }
   st->itc += 1;
@@ -295,11 +295,11 @@ int launch_daf(desalm_ctx* ctx, Lv<T, W>& L, Level& G, int n, int recalc, int it
   const double nin = double(L.im - 2) * (L.jm - 2) * (L.km - 2);
   LAUNCH(KC_RESID, n, nin, k_resid<T, W, 0><<<grid_interior(L), blk3(), 0, s>>>(L, P, upwind, itr == 1 ? 1 : 0, n > 0 ? 1 : 0, bback));
   CKL();
-  LAUNCH(KC_SWEEP_I, n, nin, k_sweep2<T, W, 0><<<dim3(cdiv(L.jm - 2, 32), L.km - 2), 128, 0, s>>>(L, P, bback, 0));
+  LAUNCH(KC_SWEEP_I, n, nin, k_sweep3<T, W, 0><<<dim3(cdiv(L.jm - 2, 32), L.km - 2), 256, 0, s>>>(L, P, bback, 0));
   CKL();
-  LAUNCH(KC_SWEEP_J, n, nin, k_sweep2<T, W, 1><<<dim3(cdiv(L.im - 2, 32), L.km - 2), 128, 0, s>>>(L, P, fine && c.btype[2] != 5, fine && c.btype[3] != 5));
+  LAUNCH(KC_SWEEP_J, n, nin, k_sweep3<T, W, 1><<<dim3(cdiv(L.im - 2, 32), L.km - 2), 256, 0, s>>>(L, P, fine && c.btype[2] != 5, fine && c.btype[3] != 5));
   CKL();
-  LAUNCH(KC_SWEEP_K, n, nin, k_sweep2<T, W, 2><<<dim3(cdiv(L.im - 2, 32), L.jm - 2), 128, 0, s>>>(L, P, fine && c.btype[4] != 5,
+  LAUNCH(KC_SWEEP_K, n, nin, k_sweep3<T, W, 2><<<dim3(cdiv(L.im - 2, 32), L.jm - 2), 256, 0, s>>>(L, P, fine && c.btype[4] != 5,
                                                                       fine && c.btype[5] != 5 && c.btype[5] != 6));
   CKL();
   return 0;
@@ -351,11 +351,11 @@ int launch_prolong(desalm_ctx* ctx, Lv<TF, WF>& F, Lv<TC, WC>& C, Level& G) {
   const double nin = double(F.im - 2) * (F.jm - 2) * (F.km - 2);
   LAUNCH(KC_PROLONG, 0, nin, k_prolong_interp<TF, WF, TC, WC><<<grid_interior(F), blk3(), 0, s>>>(F, C, dq, c.icrs, c.jcrs, c.kcrs));
   CKL();
-  LAUNCH(KC_RSMOOTH, 0, nin, k_rsmooth2<TF, WF, 0><<<dim3(cdiv(F.jm - 2, 32), F.km - 2), 128, 0, s>>>(F, dq, G.fac[0], G.dpr[0], c.ep[1][0], 0));
+  LAUNCH(KC_RSMOOTH, 0, nin, k_rsmooth3<TF, WF, 0><<<dim3(cdiv(F.jm - 2, 32), F.km - 2), 256, 0, s>>>(F, dq, G.fac[0], G.dpr[0], c.ep[1][0], 0));
   CKL();
-  LAUNCH(KC_RSMOOTH, 0, nin, k_rsmooth2<TF, WF, 1><<<dim3(cdiv(F.im - 2, 32), F.km - 2), 128, 0, s>>>(F, dq, G.fac[1], G.dpr[1], c.ep[1][1], 0));
+  LAUNCH(KC_RSMOOTH, 0, nin, k_rsmooth3<TF, WF, 1><<<dim3(cdiv(F.im - 2, 32), F.km - 2), 256, 0, s>>>(F, dq, G.fac[1], G.dpr[1], c.ep[1][1], 0));
   CKL();
-  LAUNCH(KC_RSMOOTH, 0, nin, k_rsmooth2<TF, WF, 2><<<dim3(cdiv(F.im - 2, 32), F.jm - 2), 128, 0, s>>>(F, dq, G.fac[2], G.dpr[2], c.ep[1][2], 1));
+  LAUNCH(KC_RSMOOTH, 0, nin, k_rsmooth3<TF, WF, 2><<<dim3(cdiv(F.im - 2, 32), F.jm - 2), 256, 0, s>>>(F, dq, G.fac[2], G.dpr[2], c.ep[1][2], 1));
   CKL();
   return 0;
 }
@@ -367,7 +367,7 @@ int launch_norm(desalm_ctx* ctx, Lv<T, W>& L, int copy, double* out) {
   int nb = (int)std::min<long>(ctx->part_blocks, std::max<long>(1, cdiv(total, 256)));
   LAUNCH(KC_NORM, 0, double(total), k_norm_partial<T, W><<<nb, 256, 0, s>>>(L, ctx->part, 5, copy));
   CKL();
-  LAUNCH(KC_NORM, 0, 0, k_norm_final<<<1, 32, 0, s>>>(ctx->part, nb, ctx->norm));
+  LAUNCH(KC_NORM, 0, 0, k_norm_final<<<1, 256, 0, s>>>(ctx->part, nb, ctx->norm));
   CKL();
   CK(cudaMemcpyAsync(ctx->h_norm, ctx->norm, 5 * sizeof(double), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
@@ -1146,12 +1146,11 @@ int sa_run(desalm_ctx* ctx, Lv<double, W>& L) {
   const double nin = double(L.im - 2) * (L.jm - 2) * (L.km - 2);
   const dim3 gi(cdiv(L.im - 2, 32), cdiv(L.jm - 2, 4), L.km - 2);
   LAUNCH(KC_SA_RHS, 0, nin, k_sa_source<<<gi, blk3(), 0, s>>>(S));
-  const int TB = 64;
   for (int it = 0; it < ctx->c.itk; ++it) {
     LAUNCH(KC_SA_RHS, 0, nin, k_sa_rhs<<<gi, blk3(), 0, s>>>(S));
-    LAUNCH(KC_SA_SWEEP, 0, nin, k_sa_sweep<0><<<dim3(cdiv(L.jm - 2, TB), L.km - 2), TB, 0, s>>>(S));
-    LAUNCH(KC_SA_SWEEP, 0, nin, k_sa_sweep<1><<<dim3(cdiv(L.im - 2, TB), L.km - 2), TB, 0, s>>>(S));
-    LAUNCH(KC_SA_SWEEP, 0, nin, k_sa_sweep<2><<<dim3(cdiv(L.im - 2, TB), L.jm - 2), TB, 0, s>>>(S));
+    LAUNCH(KC_SA_SWEEP, 0, nin, k_sa_sweep2<0><<<dim3(cdiv(L.jm - 2, 64), L.km - 2), 128, 0, s>>>(S));
+    LAUNCH(KC_SA_SWEEP, 0, nin, k_sa_sweep2<1><<<dim3(cdiv(L.im - 2, 64), L.km - 2), 128, 0, s>>>(S));
+    LAUNCH(KC_SA_SWEEP, 0, nin, k_sa_sweep2<2><<<dim3(cdiv(L.im - 2, 64), L.jm - 2), 128, 0, s>>>(S));
     LAUNCH(KC_SA_BC, 0, 2.0 * L.jm * L.km, k_sa_bc<0><<<dim3(cdiv(L.jm, 64), L.km), 64, 0, s>>>(S));
     LAUNCH(KC_SA_BC, 0, 2.0 * L.im * L.km, k_sa_bc<1><<<dim3(cdiv(L.im, 64), L.km), 64, 0, s>>>(S));
     LAUNCH(KC_SA_BC, 0, 2.0 * L.im * L.jm, k_sa_bc<2><<<dim3(cdiv(L.im, 64), L.jm), 64, 0, s>>>(S));
@@ -1230,7 +1229,7 @@ int build_graph(desalm_ctx* ctx) {
     int nbu = (int)std::min<long>(nb, std::max<long>(1, cdiv(total, 256)));
     if (kind_of(ctx, 0) == K_DD) LAUNCH(KC_NORM, 0, double(total), k_norm_partial<double, double><<<nbu, 256, 0, s>>>(G.dd, ctx->part, 5, 1));
     else LAUNCH(KC_NORM, 0, double(total), k_norm_partial<double, float><<<nbu, 256, 0, s>>>(G.df, ctx->part, 5, 1));
-    LAUNCH(KC_NORM, 0, 0, k_conv<<<1, 32, 0, s>>>(ctx->part, nbu, ctx->dconv, ctx->flags, cv, h));
+    LAUNCH(KC_NORM, 0, 0, k_conv<<<1, 256, 0, s>>>(ctx->part, nbu, ctx->dconv, ctx->flags, cv, h));
   }
   cudaGraph_t out = nullptr;
   cudaError_t e = cudaStreamEndCapture(s, &out);

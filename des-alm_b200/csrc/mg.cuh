@@ -230,13 +230,28 @@ __global__ void __launch_bounds__(256) k_norm_partial(Lv<T, W> L, double* part, 
     for (int m = 0; m < 5; ++m) part[blockIdx.x * 5 + m] = sh[m][0];
 }
 
-__global__ void k_norm_final(const double* part, int nblk, double* out) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  for (int m = 0; m < 5; ++m) {
-    double s = 0;
-    for (int b = 0; b < nblk; ++b) s += part[b * 5 + m];
-    out[m] = s;
+// Deterministic sum of nblk x 5 partials by one 256-thread block: strided
+// per-thread sums, then a fixed tree; every thread receives the five sums.
+DESALM_DEV void block_sum5(const double* part, int nblk, double out[5]) {
+  __shared__ double sh[5][256];
+  double acc[5] = {0, 0, 0, 0, 0};
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x)
+    for (int m = 0; m < 5; ++m) acc[m] += part[b * 5 + m];
+  for (int m = 0; m < 5; ++m) sh[m][threadIdx.x] = acc[m];
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s)
+      for (int m = 0; m < 5; ++m) sh[m][threadIdx.x] += sh[m][threadIdx.x + s];
+    __syncthreads();
   }
+  for (int m = 0; m < 5; ++m) out[m] = sh[m][0];
+}
+
+__global__ void __launch_bounds__(256) k_norm_final(const double* part, int nblk, double* out) {
+  double sums[5];
+  block_sum5(part, nblk, sums);
+  if (threadIdx.x == 0)
+    for (int m = 0; m < 5; ++m) out[m] = sums[m];
 }
 
 // ---------------------------------------------------------------- helpers

@@ -309,6 +309,199 @@ __global__ void __launch_bounds__(128) k_sa_sweep(Sa S) {
   }
 }
 
+// Two-ended form of k_sa_sweep: a CTA owns 64 lines; threads 0-63 eliminate
+// the upper half of each line top-down (SGTSV's no-interchange order),
+// threads 64-127 the lower half bottom-up; the halves meet in a 2x2 solve.
+// Same system as k_sa_sweep, twice the threads, half the dependent chain.
+template <int DIR>
+__global__ void __launch_bounds__(128) k_sa_sweep2(Sa S) {
+  __shared__ double m_d[64], m_c[64], m_b[64], n_d[64], n_c[64], n_b[64];
+  const int lane = threadIdx.x & 63, half = threadIdx.x >> 6;
+  const int a = blockIdx.x * 64 + lane + 1;
+  const int b = blockIdx.y + 1;
+  int amax, n, st, lb;
+  if (DIR == 0) { amax = S.jm - 2; n = S.im - 2; st = 1; lb = S.sj * a + S.sk * b; }
+  else if (DIR == 1) { amax = S.im - 2; n = S.jm - 2; st = S.sj; lb = a + S.sk * b; }
+  else { amax = S.im - 2; n = S.km - 2; st = S.sk; lb = a + S.sj * b; }
+  const bool act = a <= amax;
+  const double* const* mt = DIR == 0 ? S.csi : (DIR == 1 ? S.eta : S.zet);
+  const double sig = 2.0 / 3.0, rei = 1.0 / S.ren;
+  const double* q5 = S.q[4];
+  struct Nd { double m0, m1, m2, nu, aj, u; };
+  auto load = [&](int l) {
+    Nd d;
+    d.m0 = mt[0][l]; d.m1 = mt[1][l]; d.m2 = mt[2][l];
+    d.nu = q5[l]; d.aj = S.aj[l];
+    const double tmp = 1.0 / d.aj;
+    d.u = tmp * (d.m0 * S.q[1][l] + d.m1 * S.q[2][l] + d.m2 * S.q[3][l]);
+    return d;
+  };
+  auto face = [&](const Nd& A, const Nd& B) {  // B = A + st
+    double gx = B.m0 + A.m0, gy = B.m1 + A.m1, gz = B.m2 + A.m2;
+    double ev = (rei + 0.5 * (B.nu + A.nu)) / sig;
+    double ucna = 0.5 * fabs(B.u + A.u);
+    return ucna + ev * (gx * gx + gy * gy + gz * gz) / (B.aj + A.aj);
+  };
+  constexpr int R = 4;
+  const int h = n / 2;
+  int npiv = 0;
+  if (act && half == 0) {
+    Nd prev = load(lb), cur = load(lb + st);
+    double avw = face(prev, cur);
+    double uw = prev.u;
+    double dprev = 0, duprev = 0, bprev = 0;
+    for (int p0 = 0; p0 < h; p0 += R) {
+      Nd east[R];
+      double bdt[R], brh[R];
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int p = p0 + u;
+        if (p < h) {
+          const int l = lb + (p + 1) * st;
+          east[u] = load(l + st);
+          bdt[u] = S.dtev[l];
+          brh[u] = S.rh[l];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int p = p0 + u;
+        if (p < h) {
+          const int l = lb + (p + 1) * st;
+          const double ave = face(cur, east[u]);
+          const double dtj = 0.5 * bdt[u] * cur.aj;
+          const double aw = -dtj * (uw + avw);
+          const double ap = 1.0 + dtj * (avw + ave);
+          const double ae = dtj * (east[u].u - ave);
+          double d;
+          if (p == 0) { d = ap; bprev = brh[u]; }
+          else {
+            npiv += fabs(dprev) < fabs(aw);
+            const double f = aw / dprev;
+            d = ap - f * duprev;
+            bprev = brh[u] - f * bprev;
+          }
+          S.sd[l] = d; S.su[l] = ae; S.rh[l] = bprev;
+          dprev = d; duprev = ae;
+          avw = ave; uw = cur.u; cur = east[u];
+        }
+      }
+    }
+    m_d[lane] = dprev; m_c[lane] = duprev; m_b[lane] = bprev;
+  } else if (act && half == 1) {
+    Nd east = load(lb + (n + 1) * st), cur = load(lb + n * st);
+    double ave = face(cur, east);
+    double dprev = 0, awprev = 0, bprev = 0;
+    for (int p0 = n - 1; p0 >= h; p0 -= R) {
+      Nd west[R];
+      double bdt[R], brh[R];
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int p = p0 - u;
+        if (p >= h) {
+          const int l = lb + (p + 1) * st;
+          west[u] = load(l - st);
+          bdt[u] = S.dtev[l];
+          brh[u] = S.rh[l];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int p = p0 - u;
+        if (p >= h) {
+          const int l = lb + (p + 1) * st;
+          const double avw = face(west[u], cur);
+          const double dtj = 0.5 * bdt[u] * cur.aj;
+          const double aw = -dtj * (west[u].u + avw);
+          const double ap = 1.0 + dtj * (avw + ave);
+          const double ae = dtj * (east.u - ave);
+          double d;
+          if (p == n - 1) { d = ap; bprev = brh[u]; }
+          else {
+            npiv += fabs(dprev) < fabs(ae);
+            const double f = ae / dprev;
+            d = ap - f * awprev;
+            bprev = brh[u] - f * bprev;
+          }
+          S.sd[l] = d; S.su[l] = aw; S.rh[l] = bprev;
+          dprev = d; awprev = aw;
+          ave = avw; east = cur; cur = west[u];
+        }
+      }
+    }
+    n_d[lane] = dprev; n_c[lane] = awprev; n_b[lane] = bprev;
+  }
+  if (npiv) atomicAdd(&S.flags[0], npiv);
+  __syncthreads();
+  if (!act) return;
+  const double d1 = m_d[lane], u1 = m_c[lane], b1 = m_b[lane];
+  const double d2 = n_d[lane], l2 = n_c[lane], b2 = n_b[lane];
+  const double det = d1 * d2 - u1 * l2;
+  const double dmul = 1.5 * S.es;
+  auto put = [&](int l, double x, double nt, double dt) {
+    if (DIR == 2) {
+      const double qe5 = nt + x;
+      const double dum = 1.0 + dmul * dt / S.delti;
+      S.q[4][l] = nt + (-nt + qe5) / dum;
+    } else {
+      S.rh[l] = x;
+    }
+  };
+  if (half == 0) {
+    double x = (b1 * d2 - u1 * b2) / det;
+    {
+      const int l = lb + h * st;
+      put(l, x, DIR == 2 ? S.q[4][l] : 0.0, DIR == 2 ? S.dtev[l] : 0.0);
+    }
+    for (int p1 = h - 2; p1 >= 0; p1 -= R) {
+      double bb[R], bd[R], bu[R], bn[R], bt[R];
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int p = p1 - u;
+        if (p >= 0) {
+          const int l = lb + (p + 1) * st;
+          bb[u] = S.rh[l]; bd[u] = S.sd[l]; bu[u] = S.su[l];
+          if (DIR == 2) { bn[u] = S.q[4][l]; bt[u] = S.dtev[l]; }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int p = p1 - u;
+        if (p >= 0) {
+          x = (bb[u] - bu[u] * x) / bd[u];
+          put(lb + (p + 1) * st, x, DIR == 2 ? bn[u] : 0.0, DIR == 2 ? bt[u] : 0.0);
+        }
+      }
+    }
+  } else {
+    double x = (d1 * b2 - l2 * b1) / det;
+    {
+      const int l = lb + (h + 1) * st;
+      put(l, x, DIR == 2 ? S.q[4][l] : 0.0, DIR == 2 ? S.dtev[l] : 0.0);
+    }
+    for (int p0 = h + 1; p0 < n; p0 += R) {
+      double bb[R], bd[R], bu[R], bn[R], bt[R];
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int p = p0 + u;
+        if (p < n) {
+          const int l = lb + (p + 1) * st;
+          bb[u] = S.rh[l]; bd[u] = S.sd[l]; bu[u] = S.su[l];
+          if (DIR == 2) { bn[u] = S.q[4][l]; bt[u] = S.dtev[l]; }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int p = p0 + u;
+        if (p < n) {
+          x = (bb[u] - bu[u] * x) / bd[u];
+          put(lb + (p + 1) * st, x, DIR == 2 ? bn[u] : 0.0, DIR == 2 ? bt[u] : 0.0);
+        }
+      }
+    }
+  }
+}
+
 // boundary values of nu_tilde (src/rhs_sa_bcond.F90:40-269): one kernel per
 // face pair in the order i, j, k; full transverse ranges.
 template <int DIR>
