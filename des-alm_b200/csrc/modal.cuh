@@ -139,4 +139,40 @@ DESALM_DEV void mat_mc(const Lv<T, W>& L, const Par& P, int l, M4<T>& A) {
   modal_fwd(L.zet[0][l], L.zet[1][l], L.zet[2][l], s, A);
 }
 
+// The same matrices evaluated in precision C (metrics and dtau read in the
+// level's state precision and rounded to C): the line-sweep precision in
+// MIXED mode, where the transforms belong to the FP32 preconditioner.
+template <class C, class T, class W>
+DESALM_DEV void sigma_c(const Lv<T, W>& L, const Par& P, int l, C& sigma) {
+  T s, t;
+  sigma_theta(L.dtau[l], P, s, t);
+  sigma = C(s);
+}
+template <class C, class T, class W>
+DESALM_DEV void mat_mai_c(const Lv<T, W>& L, const Par& P, int l, M4<C>& A) {
+  C s; sigma_c(L, P, l, s);
+  modal_inv(C(L.csi[0][l]), C(L.csi[1][l]), C(L.csi[2][l]), s, A);
+}
+template <class C, class T, class W>
+DESALM_DEV void mat_n1i_c(const Lv<T, W>& L, const Par& P, int l, M4<C>& A) {
+  C s; sigma_c(L, P, l, s);
+  M4<C> ma, mbi;
+  modal_fwd(C(L.csi[0][l]), C(L.csi[1][l]), C(L.csi[2][l]), s, ma);
+  modal_inv(C(L.eta[0][l]), C(L.eta[1][l]), C(L.eta[2][l]), s, mbi);
+  mm4(mbi, ma, A);
+}
+template <class C, class T, class W>
+DESALM_DEV void mat_n2i_c(const Lv<T, W>& L, const Par& P, int l, M4<C>& A) {
+  C s; sigma_c(L, P, l, s);
+  M4<C> mb, mci;
+  modal_fwd(C(L.eta[0][l]), C(L.eta[1][l]), C(L.eta[2][l]), s, mb);
+  modal_inv(C(L.zet[0][l]), C(L.zet[1][l]), C(L.zet[2][l]), s, mci);
+  mm4(mci, mb, A);
+}
+template <class C, class T, class W>
+DESALM_DEV void mat_mc_c(const Lv<T, W>& L, const Par& P, int l, M4<C>& A) {
+  C s; sigma_c(L, P, l, s);
+  modal_fwd(C(L.zet[0][l]), C(L.zet[1][l]), C(L.zet[2][l]), s, A);
+}
+
 }  // namespace desalm

@@ -248,12 +248,16 @@ __global__ void __launch_bounds__(128, DESALM_KR_MINBLOCKS) k_resid(Lv<T, W> L, 
   }
   T sg, th;
   sigma_theta(dtau, P, sg, th);
-  M4<T> A;
-  modal_inv(L.csi[0][l], L.csi[1][l], L.csi[2][l], sg, A);
-  T rp[4];
-  mv4(A, r, rp);
+  {
+    // Ma^-1 in the sweep precision W (the preconditioner's precision)
+    M4<W> A;
+    modal_inv(W(L.csi[0][l]), W(L.csi[1][l]), W(L.csi[2][l]), W(sg), A);
+    W rw[4] = {W(r[0]), W(r[1]), W(r[2]), W(r[3])};
+    W rp[4];
+    mv4(A, rw, rp);
 #pragma unroll
-  for (int m = 0; m < 4; ++m) L.wk[m][l] = W(rp[m]);
+    for (int m = 0; m < 4; ++m) L.wk[m][l] = rp[m];
+  }
 
   // ---- line-sweep coefficients of every direction (src/rhs_diag_solver.F90:
   // 159-181): tmp = dtau ep spr dsq for the node's own row, and

@@ -599,7 +599,8 @@ __global__ void __launch_bounds__(256) k_sweep3(Lv<T, W> L, Par P, int blo, int 
   }
   __syncthreads();
 
-  // ---- phase 2: per-node transform of the CTA's lines
+  // ---- phase 2: per-node transform of the CTA's lines, in the sweep
+  // precision W (FP64 in FP64 mode, FP32 in MIXED mode)
   const int nl = min(32, amax - a0 + 1);
   const int total = nl * n;
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
@@ -608,9 +609,9 @@ __global__ void __launch_bounds__(256) k_sweep3(Lv<T, W> L, Par P, int blo, int 
     else { p = t / nl; li = t - p * nl; }
     const int aa = a0 + li;
     const int l = base + aa * sa + (p + 1) * st;
-    T xv[4];
+    W xv[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) xv[q] = T(L.wk[q][l]);
+    for (int q = 0; q < 4; ++q) xv[q] = L.wk[q][l];
     if (DIR == 0) {
       const int S = L.im * L.km, o = (p + 1) + L.im * b;
       const int tgt[4] = {1, 2, L.jm - 2, L.jm - 3};
@@ -618,13 +619,13 @@ __global__ void __launch_bounds__(256) k_sweep3(Lv<T, W> L, Par P, int blo, int 
       for (int s = 0; s < 4; ++s)
         if (aa == tgt[s])
 #pragma unroll
-          for (int q = 0; q < 4; ++q) L.bj[(s * 4 + q) * S + o] = W(xv[q]);
-      M4<T> A;
-      mat_n1i(L, P, l, A);
-      T y[4];
+          for (int q = 0; q < 4; ++q) L.bj[(s * 4 + q) * S + o] = xv[q];
+      M4<W> A;
+      mat_n1i_c<W>(L, P, l, A);
+      W y[4];
       mv4(A, xv, y);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) L.wk[q][l] = W(y[q]);
+      for (int q = 0; q < 4; ++q) L.wk[q][l] = y[q];
     } else if (DIR == 1) {
       const int S = L.im * L.jm, o = aa + L.im * (p + 1);
       const int tgt[4] = {1, 2, L.km - 2, L.km - 3};
@@ -632,20 +633,20 @@ __global__ void __launch_bounds__(256) k_sweep3(Lv<T, W> L, Par P, int blo, int 
       for (int s = 0; s < 4; ++s)
         if (b == tgt[s])
 #pragma unroll
-          for (int q = 0; q < 4; ++q) L.bk[(s * 4 + q) * S + o] = W(xv[q]);
-      M4<T> A;
-      mat_n2i(L, P, l, A);
-      T y[4];
+          for (int q = 0; q < 4; ++q) L.bk[(s * 4 + q) * S + o] = xv[q];
+      M4<W> A;
+      mat_n2i_c<W>(L, P, l, A);
+      W y[4];
       mv4(A, xv, y);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) L.wk[q][l] = W(y[q]);
+      for (int q = 0; q < 4; ++q) L.wk[q][l] = y[q];
     } else {
-      M4<T> A;
-      mat_mc(L, P, l, A);
-      T y[4];
+      M4<W> A;
+      mat_mc_c<W>(L, P, l, A);
+      W y[4];
       mv4(A, xv, y);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) L.q[q][l] = L.q[q][l] + y[q];
+      for (int q = 0; q < 4; ++q) L.q[q][l] = L.q[q][l] + T(y[q]);
     }
   }
 }
