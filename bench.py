@@ -328,6 +328,22 @@ def run_reference(args):
 REF_ITERS = {"cavity": 200, "channel": 400}
 
 
+def ncu_workload(case_name, precision):
+    """A short, eager run for Nsight Compute captures: the case's setup, the
+    start of a physical step and one pseudo-iteration, without CUDA graphs
+    (so every kernel is a separate, capturable launch)."""
+    from desalm.solver import Solver
+    case, grid, state, _ = build_case(case_name, precision, abi.PRED_LINEAR)
+    case.use_graph = 0
+    S = Solver(case)
+    S.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
+    S.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
+    S.begin_step()
+    S.pseudo_iteration()
+    S.sync()
+    print(json.dumps({"ncu_workload": case_name, "precision": precision}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -336,7 +352,13 @@ def main():
     ap.add_argument("--case", default="cavity", choices=["cavity", "channel"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ncu-workload", action="store_true",
+                    help="run one eager pseudo-iteration of --case for an ncu capture and exit")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     args = ap.parse_args()
+    if args.ncu_workload:
+        ncu_workload(args.case, abi.MIXED if args.precision == "mixed" else abi.FP64)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":
