@@ -1123,16 +1123,18 @@ void* desalm_stream(desalm_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr
 
 namespace {
 
-// SA view of the fine level (FP64 in every precision mode)
-template <class W>
-Sa make_sa(desalm_ctx* ctx, Lv<double, W>& L) {
-  Sa S{};
+// SA view of the fine level: nu_tilde, nu_t and the residual terms in FP64;
+// the ADI work in W (FP32 in MIXED mode).
+template <class SW, class W>
+SaT<SW> make_sa(desalm_ctx* ctx, Lv<double, W>& L) {
+  SaT<SW> S{};
   S.im = L.im; S.jm = L.jm; S.km = L.km; S.N = L.N; S.sj = L.sj; S.sk = L.sk;
   for (int m = 0; m < 5; ++m) S.q[m] = L.q[m];
   S.qn5 = L.qn[4]; S.qnm1_5 = L.qnm1[4];
   for (int d = 0; d < 3; ++d) { S.csi[d] = L.csi[d]; S.eta[d] = L.eta[d]; S.zet[d] = L.zet[d]; }
   S.aj = L.aj; S.wd = ctx->wd; S.dtev = ctx->dtev; S.nut = L.nut;
-  S.wo = ctx->sa.a[0]; S.rh = ctx->sa.a[1]; S.sd = ctx->sa.a[2]; S.su = ctx->sa.a[3];
+  S.wo = ctx->sa.a[0];
+  S.rh = (SW*)ctx->sa.a[1]; S.sd = (SW*)ctx->sa.a[2]; S.su = (SW*)ctx->sa.a[3];
   S.flags = ctx->flags;
   S.ren = ctx->c.ren; S.delti = ctx->c.delti; S.es = ctx->c.unsteady ? 1.0 : 0.0;
   for (int b = 0; b < 6; ++b) { S.sa1[b] = ctx->par.sa[0][b]; S.sb1[b] = ctx->par.sb[0][b]; S.btype[b] = ctx->c.btype[b]; }
@@ -1141,20 +1143,20 @@ Sa make_sa(desalm_ctx* ctx, Lv<double, W>& L) {
 
 template <class W>
 int sa_run(desalm_ctx* ctx, Lv<double, W>& L) {
-  Sa S = make_sa(ctx, L);
+  SaT<W> S = make_sa<W>(ctx, L);
   cudaStream_t s = ctx->stream;
   const double nin = double(L.im - 2) * (L.jm - 2) * (L.km - 2);
   const dim3 gi(cdiv(L.im - 2, 32), cdiv(L.jm - 2, 4), L.km - 2);
-  LAUNCH(KC_SA_RHS, 0, nin, k_sa_source<<<gi, blk3(), 0, s>>>(S));
+  LAUNCH(KC_SA_RHS, 0, nin, k_sa_source<W><<<gi, blk3(), 0, s>>>(S));
   for (int it = 0; it < ctx->c.itk; ++it) {
-    LAUNCH(KC_SA_RHS, 0, nin, k_sa_rhs<<<gi, blk3(), 0, s>>>(S));
-    LAUNCH(KC_SA_SWEEP, 0, nin, k_sa_sweep2<0><<<dim3(cdiv(L.jm - 2, 64), L.km - 2), 128, 0, s>>>(S));
-    LAUNCH(KC_SA_SWEEP, 0, nin, k_sa_sweep2<1><<<dim3(cdiv(L.im - 2, 64), L.km - 2), 128, 0, s>>>(S));
-    LAUNCH(KC_SA_SWEEP, 0, nin, k_sa_sweep2<2><<<dim3(cdiv(L.im - 2, 64), L.jm - 2), 128, 0, s>>>(S));
-    LAUNCH(KC_SA_BC, 0, 2.0 * L.jm * L.km, k_sa_bc<0><<<dim3(cdiv(L.jm, 64), L.km), 64, 0, s>>>(S));
-    LAUNCH(KC_SA_BC, 0, 2.0 * L.im * L.km, k_sa_bc<1><<<dim3(cdiv(L.im, 64), L.km), 64, 0, s>>>(S));
-    LAUNCH(KC_SA_BC, 0, 2.0 * L.im * L.jm, k_sa_bc<2><<<dim3(cdiv(L.im, 64), L.jm), 64, 0, s>>>(S));
-    LAUNCH(KC_SA_BC, 0, L.N, k_sa_clamp<<<cdiv(L.N, 256), 256, 0, s>>>(S));
+    LAUNCH(KC_SA_RHS, 0, nin, k_sa_rhs<W><<<gi, blk3(), 0, s>>>(S));
+    LAUNCH(KC_SA_SWEEP, 0, nin, k_sa_sweep2<W, 0><<<dim3(cdiv(L.jm - 2, 64), L.km - 2), 128, 0, s>>>(S));
+    LAUNCH(KC_SA_SWEEP, 0, nin, k_sa_sweep2<W, 1><<<dim3(cdiv(L.im - 2, 64), L.km - 2), 128, 0, s>>>(S));
+    LAUNCH(KC_SA_SWEEP, 0, nin, k_sa_sweep2<W, 2><<<dim3(cdiv(L.im - 2, 64), L.jm - 2), 128, 0, s>>>(S));
+    LAUNCH(KC_SA_BC, 0, 2.0 * L.jm * L.km, k_sa_bc<W, 0><<<dim3(cdiv(L.jm, 64), L.km), 64, 0, s>>>(S));
+    LAUNCH(KC_SA_BC, 0, 2.0 * L.im * L.km, k_sa_bc<W, 1><<<dim3(cdiv(L.im, 64), L.km), 64, 0, s>>>(S));
+    LAUNCH(KC_SA_BC, 0, 2.0 * L.im * L.jm, k_sa_bc<W, 2><<<dim3(cdiv(L.im, 64), L.jm), 64, 0, s>>>(S));
+    LAUNCH(KC_SA_BC, 0, L.N, k_sa_clamp<W><<<cdiv(L.N, 256), 256, 0, s>>>(S));
   }
   CKL();
   ctx->L[0].dtau_valid = false;  // nu_t changed
@@ -1163,7 +1165,7 @@ int sa_run(desalm_ctx* ctx, Lv<double, W>& L) {
 
 template <class W>
 int cons_run(desalm_ctx* ctx, Lv<double, W>& L) {
-  Sa S = make_sa(ctx, L);
+  Sa S = make_sa<double>(ctx, L);
   cudaStream_t s = ctx->stream;
   double* acc = ctx->part;
   LAUNCH(KC_MISC, 0, 2.0 * L.jm * L.km, k_cons_sum<<<1, 256, 0, s>>>(S, acc));

@@ -159,44 +159,11 @@ __global__ void k_prolong_interp(Lv<TF, WF> F, Lv<TC, WC> C, TF* dq, int icrs, i
 }
 
 // Constant-coefficient implicit smoothing (-e, 1+2e, -e) along one direction
-// (src/rs_sweep.F90:163-284), NRHS = 4.  The system never pivots; fac/dpr
-// hold SGTSV's multipliers and eliminated diagonal for the line length, built
-// on the host in SGTSV's order.  The last direction (k) adds dq to q on the
-// interior (src/mg_prolong.F90:218-277: dq is zero on the boundary).
-template <class TF, class WF, int DIR>
-__global__ void k_rsmooth(Lv<TF, WF> F, TF* dq, const double* fac, const double* dpr, double e, int last) {
-  const int a = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int b = blockIdx.y + 1;
-  int amax, n, st, lb;
-  if (DIR == 0) { amax = F.jm - 2; n = F.im - 2; st = 1; lb = F.sj * a + F.sk * b; }
-  else if (DIR == 1) { amax = F.im - 2; n = F.jm - 2; st = F.sj; lb = a + F.sk * b; }
-  else { amax = F.im - 2; n = F.km - 2; st = F.sk; lb = a + F.sj * b; }
-  if (a > amax) return;
-  const TF du = TF(-e);
-  TF bp[4];
-  for (int p = 0; p < n; ++p) {
-    const int l = lb + (p + 1) * st;
-#pragma unroll
-    for (int m = 0; m < 4; ++m) {
-      TF v = dq[m * F.N + l];
-      if (p > 0) v = v - TF(fac[p - 1]) * bp[m];
-      bp[m] = v;
-      dq[m * F.N + l] = v;
-    }
-  }
-  TF x[4];
-  for (int p = n - 1; p >= 0; --p) {
-    const int l = lb + (p + 1) * st;
-    const TF d = TF(dpr[p]);
-#pragma unroll
-    for (int m = 0; m < 4; ++m) {
-      TF v = dq[m * F.N + l];
-      x[m] = (p == n - 1) ? v / d : (v - du * x[m]) / d;
-      if (last) F.q[m][l] = F.q[m][l] + x[m];
-      else dq[m * F.N + l] = x[m];
-    }
-  }
-}
+// (src/rs_sweep.F90:163-284), NRHS = 4: see k_rsmooth3 below.  The system
+// never pivots; fac/dpr hold SGTSV's multipliers and eliminated diagonal for
+// the line length, built on the host in SGTSV's order.  The last direction
+// (k) adds dq to q on the interior (src/mg_prolong.F90:218-277: dq is zero on
+// the boundary).
 
 // ---------------------------------------------------------------- norm
 // Per-block partial sums of |q - qold| over interior nodes, 5 fields
@@ -353,73 +320,12 @@ __global__ void k_dtev(double* const* cov, double* dtev, long n, double cfl2, do
 
 namespace desalm {
 
-// Second-generation constant-coefficient smoothing: one thread per (line,
-// component); warp m handles component m of 32 lines (coalesced for j and
-// k lines).  Same arithmetic as k_rsmooth.
-template <class TF, class WF, int DIR>
-__global__ void __launch_bounds__(128) k_rsmooth2(Lv<TF, WF> F, TF* dq, const double* fac, const double* dpr, double e, int last) {
-  const int lane = threadIdx.x & 31, m = threadIdx.x >> 5;
-  const int a = blockIdx.x * 32 + lane + 1;
-  const int b = blockIdx.y + 1;
-  int amax, n, st, lb;
-  if (DIR == 0) { amax = F.jm - 2; n = F.im - 2; st = 1; lb = F.sj * a + F.sk * b; }
-  else if (DIR == 1) { amax = F.im - 2; n = F.jm - 2; st = F.sj; lb = a + F.sk * b; }
-  else { amax = F.im - 2; n = F.km - 2; st = F.sk; lb = a + F.sj * b; }
-  if (a > amax) return;
-  TF* v = dq + (long)m * F.N;
-  const TF du = TF(-e);
-  constexpr int R = 8;
-  TF bp = 0;
-  for (int p0 = 0; p0 < n; p0 += R) {
-    TF bv[R];
-#pragma unroll
-    for (int u = 0; u < R; ++u)
-      if (p0 + u < n) bv[u] = v[lb + (p0 + u + 1) * st];
-#pragma unroll
-    for (int u = 0; u < R; ++u) {
-      const int p = p0 + u;
-      if (p < n) {
-        TF x = bv[u];
-        if (p > 0) x = x - TF(fac[p - 1]) * bp;
-        bp = x;
-        v[lb + (p + 1) * st] = x;
-      }
-    }
-  }
-  TF x = 0;
-  for (int p1 = n - 1; p1 >= 0; p1 -= R) {
-    TF bv[R], bq[R];
-#pragma unroll
-    for (int u = 0; u < R; ++u) {
-      const int p = p1 - u;
-      if (p >= 0) {
-        bv[u] = v[lb + (p + 1) * st];
-        if (last) bq[u] = F.q[m][lb + (p + 1) * st];
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < R; ++u) {
-      const int p = p1 - u;
-      if (p >= 0) {
-        const int l = lb + (p + 1) * st;
-        const TF d = TF(dpr[p]);
-        x = (p == n - 1) ? bv[u] / d : (bv[u] - du * x) / d;
-        if (last) F.q[m][l] = bq[u] + x;
-        else v[l] = x;
-      }
-    }
-  }
-}
-
-}  // namespace desalm
-
-namespace desalm {
-
-// Two-ended constant-coefficient smoothing: warps 0-3 eliminate the upper
+// Two-ended constant-coefficient smoothing, one thread per (line, component,
+// half): warps 0-3 eliminate the upper
 // half of component m top-down, warps 4-7 the lower half bottom-up (the
 // matrix is symmetric Toeplitz, so the bottom-up eliminated diagonal and
 // multipliers are the top-down ones mirrored); the halves meet in a 2x2
-// solve and back-substitute.  Same operator as k_rsmooth2, twice the threads.
+// solve and back-substitute.
 template <class TF, class WF, int DIR>
 __global__ void __launch_bounds__(256) k_rsmooth3(Lv<TF, WF> F, TF* dq, const double* fac, const double* dpr, double e, int last) {
   __shared__ TF s_top[32][4][2], s_bot[32][4][2];  // (eliminated b, nothing) of the middle rows

@@ -13,7 +13,11 @@ struct SaWork {
   double* a[NARR];  // wo, rh5, sd, su
 };
 
-struct Sa {
+// SW: type of the ADI work arrays and arithmetic (double in FP64 mode,
+// float in MIXED mode, where the ADI is the FP32 preconditioner of an FP64
+// residual); nu_tilde, nu_t and the residual terms stay FP64.
+template <class SW>
+struct SaT {
   int im, jm, km, N, sj, sk;
   double* q[5];
   const double* qn5;
@@ -26,23 +30,27 @@ struct Sa {
   const double* dtev;
   double* nut;
   double* wo;
-  double* rh;
-  double* sd;
-  double* su;
+  SW* rh;
+  SW* sd;
+  SW* su;
   int* flags;
   double ren, delti, es;
   double sa1[6], sb1[6];  // pressure-row extrapolation coefficients, sa(1,b), sb(1,b)
   int btype[6];
 };
 
-DESALM_DEV double sa_ucn(const Sa& S, int d, int l) {
+using Sa = SaT<double>;
+
+template <class SW>
+DESALM_DEV double sa_ucn(const SaT<SW>& S, int d, int l) {
   const double* const* m = d == 0 ? S.csi : (d == 1 ? S.eta : S.zet);
   double tmp = 1.0 / S.aj[l];
   return tmp * (m[0][l] * S.q[1][l] + m[1][l] * S.q[2][l] + m[2][l] * S.q[3][l]);
 }
 
 // vorticity magnitude wo = 2 |W|^2 on interior nodes (src/rhs_sa_source.F90:44-93)
-__global__ void k_sa_source(Sa S) {
+template <class SW>
+__global__ void k_sa_source(SaT<SW> S) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int k = blockIdx.z + 1;
@@ -69,7 +77,8 @@ __global__ void k_sa_source(Sa S) {
 
 // viscous flux of nu_tilde through the face l0 -> l0 + st[dir]
 // (src/rhs_sa_viscous.F90:58-175)
-DESALM_DEV double sa_visc_face(const Sa& S, int dir, int l0, double rei, double sig) {
+template <class SW>
+DESALM_DEV double sa_visc_face(const SaT<SW>& S, int dir, int l0, double rei, double sig) {
   const int sj = S.sj, sk = S.sk;
   const double* v = S.q[4];
   int l1;
@@ -103,7 +112,8 @@ DESALM_DEV double sa_visc_face(const Sa& S, int dir, int l0, double rei, double 
 
 // first-order flux-difference upwind flux of nu_tilde through the face
 // l0 -> l0 + st (src/rhs_sa_flux.F90:32-109)
-DESALM_DEV double sa_conv_face(const Sa& S, int dir, int l0, int st) {
+template <class SW>
+DESALM_DEV double sa_conv_face(const SaT<SW>& S, int dir, int l0, int st) {
   const int l1 = l0 + st;
   const double u1 = sa_ucn(S, dir, l1), u0 = sa_ucn(S, dir, l0);
   const double* v = S.q[4];
@@ -114,7 +124,8 @@ DESALM_DEV double sa_conv_face(const Sa& S, int dir, int l0, int st) {
 // One fused pass of rhs_sa_grdnu, rhs_sa_prod, rhs_sa_viscous, rhs_sa_flux,
 // rhs_sa_unst_visc and rhs_sa_implicit_source on interior nodes
 // (src/des_eddy.F90:164-223); boundary values of rh stay zero.
-__global__ void __launch_bounds__(128) k_sa_rhs(Sa S) {
+template <class SW>
+__global__ void __launch_bounds__(128) k_sa_rhs(SaT<SW> S) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int k = blockIdx.z + 1;
@@ -187,135 +198,20 @@ __global__ void __launch_bounds__(128) k_sa_rhs(Sa S) {
   double dtj = 2.0 * S.delti * S.aj[l];
   double dq5dt = S.es * (3.0 * q5[l] - 4.0 * S.qn5[l] + S.qnm1_5[l]) / dtj;
   double r = rh + dq5dt - visc - psa / S.aj[l];
-  S.rh[l] = -S.dtev[l] * S.aj[l] * r;
+  S.rh[l] = SW(-S.dtev[l] * S.aj[l] * r);
 }
 
 // Scalar ADI sweep of nu_tilde along one direction
-// (src/rhs_sa_adi_solver.F90:50-244): SGTSV no-interchange elimination in
-// SGTSV's order, a would-swap row counted in flags[0].  The k sweep ends
-// with the update nu <- nu + (-nu + (nu_old + dnu)) / (1 + 1.5 dtev / dt)
+// (src/rhs_sa_adi_solver.F90:50-244), two-ended: a CTA owns 64 lines;
+// threads 0-63 eliminate the upper half of each line top-down (SGTSV's
+// no-interchange order; a would-swap row is counted in flags[0]), threads
+// 64-127 the lower half bottom-up; the halves meet in a 2x2 solve and
+// back-substitute.  The k sweep ends with the update
+// nu <- nu + (-nu + (nu_old + dnu)) / (1 + 1.5 dtev / dt)
 // (src/des_eddy.F90:260-272).
-template <int DIR>
-__global__ void __launch_bounds__(128) k_sa_sweep(Sa S) {
-  const int a = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int b = blockIdx.y + 1;
-  int amax, n, st, lb;
-  if (DIR == 0) { amax = S.jm - 2; n = S.im - 2; st = 1; lb = S.sj * a + S.sk * b; }
-  else if (DIR == 1) { amax = S.im - 2; n = S.jm - 2; st = S.sj; lb = a + S.sk * b; }
-  else { amax = S.im - 2; n = S.km - 2; st = S.sk; lb = a + S.sj * b; }
-  if (a > amax) return;
-  const double* const* mt = DIR == 0 ? S.csi : (DIR == 1 ? S.eta : S.zet);
-  const double sig = 2.0 / 3.0, rei = 1.0 / S.ren;
-  const double* q5 = S.q[4];
-  // per-node data along the line: metric vector of this direction, nu, J, U/J
-  struct Nd { double m0, m1, m2, nu, aj, u; };
-  auto load = [&](int l) {
-    Nd d;
-    d.m0 = mt[0][l]; d.m1 = mt[1][l]; d.m2 = mt[2][l];
-    d.nu = q5[l]; d.aj = S.aj[l];
-    const double tmp = 1.0 / d.aj;
-    d.u = tmp * (d.m0 * S.q[1][l] + d.m1 * S.q[2][l] + d.m2 * S.q[3][l]);
-    return d;
-  };
-  // av on the face between nodes A and B = A + st (src/rhs_sa_adi_solver.F90:53-63)
-  auto face = [&](const Nd& A, const Nd& B) {
-    double gx = B.m0 + A.m0, gy = B.m1 + A.m1, gz = B.m2 + A.m2;
-    double ev = (rei + 0.5 * (B.nu + A.nu)) / sig;
-    double ucna = 0.5 * fabs(B.u + A.u);
-    return ucna + ev * (gx * gx + gy * gy + gz * gz) / (B.aj + A.aj);
-  };
-  constexpr int R = 4;
-  Nd prev = load(lb), cur = load(lb + st);
-  double avw = face(prev, cur);
-  double uw = prev.u;
-  double dprev = 0, duprev = 0, bprev = 0;
-  int npiv = 0;
-  for (int p0 = 0; p0 < n; p0 += R) {
-    Nd east[R];
-    double bdt[R], brh[R];
-#pragma unroll
-    for (int u = 0; u < R; ++u) {
-      const int p = p0 + u;
-      if (p < n) {
-        const int l = lb + (p + 1) * st;
-        east[u] = load(l + st);
-        bdt[u] = S.dtev[l];
-        brh[u] = S.rh[l];
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < R; ++u) {
-      const int p = p0 + u;
-      if (p < n) {
-        const int l = lb + (p + 1) * st;
-        const double ave = face(cur, east[u]);
-        const double dtj = 0.5 * bdt[u] * cur.aj;
-        const double aw = -dtj * (uw + avw);
-        const double ap = 1.0 + dtj * (avw + ave);
-        const double ae = dtj * (east[u].u - ave);
-        double d;
-        if (p == 0) {
-          d = ap;
-          bprev = brh[u];
-        } else {
-          npiv += fabs(dprev) < fabs(aw);
-          const double f = aw / dprev;
-          d = ap - f * duprev;
-          bprev = brh[u] - f * bprev;
-        }
-        S.sd[l] = d;
-        S.su[l] = ae;
-        S.rh[l] = bprev;
-        dprev = d;
-        duprev = ae;
-        avw = ave;
-        uw = cur.u;
-        cur = east[u];
-      }
-    }
-  }
-  if (npiv) atomicAdd(&S.flags[0], npiv);
-  double x = 0;
-  const double dmul = 1.5 * S.es;
-  for (int p1 = n - 1; p1 >= 0; p1 -= R) {
-    double bb[R], bd[R], bu[R], bn[R], bt[R];
-#pragma unroll
-    for (int u = 0; u < R; ++u) {
-      const int p = p1 - u;
-      if (p >= 0) {
-        const int l = lb + (p + 1) * st;
-        bb[u] = S.rh[l];
-        bd[u] = S.sd[l];
-        bu[u] = S.su[l];
-        if (DIR == 2) { bn[u] = S.q[4][l]; bt[u] = S.dtev[l]; }
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < R; ++u) {
-      const int p = p1 - u;
-      if (p >= 0) {
-        const int l = lb + (p + 1) * st;
-        x = (p == n - 1) ? bb[u] / bd[u] : (bb[u] - bu[u] * x) / bd[u];
-        if (DIR == 2) {
-          const double nt = bn[u];
-          const double qe5 = nt + x;
-          const double dum = 1.0 + dmul * bt[u] / S.delti;
-          S.q[4][l] = nt + (-nt + qe5) / dum;
-        } else {
-          S.rh[l] = x;
-        }
-      }
-    }
-  }
-}
-
-// Two-ended form of k_sa_sweep: a CTA owns 64 lines; threads 0-63 eliminate
-// the upper half of each line top-down (SGTSV's no-interchange order),
-// threads 64-127 the lower half bottom-up; the halves meet in a 2x2 solve.
-// Same system as k_sa_sweep, twice the threads, half the dependent chain.
-template <int DIR>
-__global__ void __launch_bounds__(128) k_sa_sweep2(Sa S) {
-  __shared__ double m_d[64], m_c[64], m_b[64], n_d[64], n_c[64], n_b[64];
+template <class SW, int DIR>
+__global__ void __launch_bounds__(128) k_sa_sweep2(SaT<SW> S) {
+  __shared__ SW m_d[64], m_c[64], m_b[64], n_d[64], n_c[64], n_b[64];
   const int lane = threadIdx.x & 63, half = threadIdx.x >> 6;
   const int a = blockIdx.x * 64 + lane + 1;
   const int b = blockIdx.y + 1;
@@ -325,21 +221,21 @@ __global__ void __launch_bounds__(128) k_sa_sweep2(Sa S) {
   else { amax = S.im - 2; n = S.km - 2; st = S.sk; lb = a + S.sj * b; }
   const bool act = a <= amax;
   const double* const* mt = DIR == 0 ? S.csi : (DIR == 1 ? S.eta : S.zet);
-  const double sig = 2.0 / 3.0, rei = 1.0 / S.ren;
+  const SW sig = SW(2.0 / 3.0), rei = SW(1.0 / S.ren), half_ = SW(0.5);
   const double* q5 = S.q[4];
-  struct Nd { double m0, m1, m2, nu, aj, u; };
+  struct Nd { SW m0, m1, m2, nu, aj, u; };
   auto load = [&](int l) {
     Nd d;
-    d.m0 = mt[0][l]; d.m1 = mt[1][l]; d.m2 = mt[2][l];
-    d.nu = q5[l]; d.aj = S.aj[l];
-    const double tmp = 1.0 / d.aj;
-    d.u = tmp * (d.m0 * S.q[1][l] + d.m1 * S.q[2][l] + d.m2 * S.q[3][l]);
+    d.m0 = SW(mt[0][l]); d.m1 = SW(mt[1][l]); d.m2 = SW(mt[2][l]);
+    d.nu = SW(q5[l]); d.aj = SW(S.aj[l]);
+    const SW tmp = SW(1) / d.aj;
+    d.u = tmp * (d.m0 * SW(S.q[1][l]) + d.m1 * SW(S.q[2][l]) + d.m2 * SW(S.q[3][l]));
     return d;
   };
   auto face = [&](const Nd& A, const Nd& B) {  // B = A + st
-    double gx = B.m0 + A.m0, gy = B.m1 + A.m1, gz = B.m2 + A.m2;
-    double ev = (rei + 0.5 * (B.nu + A.nu)) / sig;
-    double ucna = 0.5 * fabs(B.u + A.u);
+    SW gx = B.m0 + A.m0, gy = B.m1 + A.m1, gz = B.m2 + A.m2;
+    SW ev = (rei + half_ * (B.nu + A.nu)) / sig;
+    SW ucna = half_ * dabs(B.u + A.u);
     return ucna + ev * (gx * gx + gy * gy + gz * gz) / (B.aj + A.aj);
   };
   constexpr int R = 4;
@@ -347,19 +243,19 @@ __global__ void __launch_bounds__(128) k_sa_sweep2(Sa S) {
   int npiv = 0;
   if (act && half == 0) {
     Nd prev = load(lb), cur = load(lb + st);
-    double avw = face(prev, cur);
-    double uw = prev.u;
-    double dprev = 0, duprev = 0, bprev = 0;
+    SW avw = face(prev, cur);
+    SW uw = prev.u;
+    SW dprev = 0, duprev = 0, bprev = 0;
     for (int p0 = 0; p0 < h; p0 += R) {
       Nd east[R];
-      double bdt[R], brh[R];
+      SW bdt[R], brh[R];
 #pragma unroll
       for (int u = 0; u < R; ++u) {
         const int p = p0 + u;
         if (p < h) {
           const int l = lb + (p + 1) * st;
           east[u] = load(l + st);
-          bdt[u] = S.dtev[l];
+          bdt[u] = SW(S.dtev[l]);
           brh[u] = S.rh[l];
         }
       }
@@ -368,16 +264,16 @@ __global__ void __launch_bounds__(128) k_sa_sweep2(Sa S) {
         const int p = p0 + u;
         if (p < h) {
           const int l = lb + (p + 1) * st;
-          const double ave = face(cur, east[u]);
-          const double dtj = 0.5 * bdt[u] * cur.aj;
-          const double aw = -dtj * (uw + avw);
-          const double ap = 1.0 + dtj * (avw + ave);
-          const double ae = dtj * (east[u].u - ave);
-          double d;
+          const SW ave = face(cur, east[u]);
+          const SW dtj = half_ * bdt[u] * cur.aj;
+          const SW aw = -dtj * (uw + avw);
+          const SW ap = SW(1) + dtj * (avw + ave);
+          const SW ae = dtj * (east[u].u - ave);
+          SW d;
           if (p == 0) { d = ap; bprev = brh[u]; }
           else {
-            npiv += fabs(dprev) < fabs(aw);
-            const double f = aw / dprev;
+            npiv += dabs(dprev) < dabs(aw);
+            const SW f = aw / dprev;
             d = ap - f * duprev;
             bprev = brh[u] - f * bprev;
           }
@@ -390,18 +286,18 @@ __global__ void __launch_bounds__(128) k_sa_sweep2(Sa S) {
     m_d[lane] = dprev; m_c[lane] = duprev; m_b[lane] = bprev;
   } else if (act && half == 1) {
     Nd east = load(lb + (n + 1) * st), cur = load(lb + n * st);
-    double ave = face(cur, east);
-    double dprev = 0, awprev = 0, bprev = 0;
+    SW ave = face(cur, east);
+    SW dprev = 0, awprev = 0, bprev = 0;
     for (int p0 = n - 1; p0 >= h; p0 -= R) {
       Nd west[R];
-      double bdt[R], brh[R];
+      SW bdt[R], brh[R];
 #pragma unroll
       for (int u = 0; u < R; ++u) {
         const int p = p0 - u;
         if (p >= h) {
           const int l = lb + (p + 1) * st;
           west[u] = load(l - st);
-          bdt[u] = S.dtev[l];
+          bdt[u] = SW(S.dtev[l]);
           brh[u] = S.rh[l];
         }
       }
@@ -410,16 +306,16 @@ __global__ void __launch_bounds__(128) k_sa_sweep2(Sa S) {
         const int p = p0 - u;
         if (p >= h) {
           const int l = lb + (p + 1) * st;
-          const double avw = face(west[u], cur);
-          const double dtj = 0.5 * bdt[u] * cur.aj;
-          const double aw = -dtj * (west[u].u + avw);
-          const double ap = 1.0 + dtj * (avw + ave);
-          const double ae = dtj * (east.u - ave);
-          double d;
+          const SW avw = face(west[u], cur);
+          const SW dtj = half_ * bdt[u] * cur.aj;
+          const SW aw = -dtj * (west[u].u + avw);
+          const SW ap = SW(1) + dtj * (avw + ave);
+          const SW ae = dtj * (east.u - ave);
+          SW d;
           if (p == n - 1) { d = ap; bprev = brh[u]; }
           else {
-            npiv += fabs(dprev) < fabs(ae);
-            const double f = ae / dprev;
+            npiv += dabs(dprev) < dabs(ae);
+            const SW f = ae / dprev;
             d = ap - f * awprev;
             bprev = brh[u] - f * bprev;
           }
@@ -434,13 +330,13 @@ __global__ void __launch_bounds__(128) k_sa_sweep2(Sa S) {
   if (npiv) atomicAdd(&S.flags[0], npiv);
   __syncthreads();
   if (!act) return;
-  const double d1 = m_d[lane], u1 = m_c[lane], b1 = m_b[lane];
-  const double d2 = n_d[lane], l2 = n_c[lane], b2 = n_b[lane];
-  const double det = d1 * d2 - u1 * l2;
+  const SW d1 = m_d[lane], u1 = m_c[lane], b1 = m_b[lane];
+  const SW d2 = n_d[lane], l2 = n_c[lane], b2 = n_b[lane];
+  const SW det = d1 * d2 - u1 * l2;
   const double dmul = 1.5 * S.es;
-  auto put = [&](int l, double x, double nt, double dt) {
+  auto put = [&](int l, SW x, double nt, double dt) {
     if (DIR == 2) {
-      const double qe5 = nt + x;
+      const double qe5 = nt + double(x);
       const double dum = 1.0 + dmul * dt / S.delti;
       S.q[4][l] = nt + (-nt + qe5) / dum;
     } else {
@@ -448,13 +344,14 @@ __global__ void __launch_bounds__(128) k_sa_sweep2(Sa S) {
     }
   };
   if (half == 0) {
-    double x = (b1 * d2 - u1 * b2) / det;
+    SW x = (b1 * d2 - u1 * b2) / det;
     {
       const int l = lb + h * st;
       put(l, x, DIR == 2 ? S.q[4][l] : 0.0, DIR == 2 ? S.dtev[l] : 0.0);
     }
     for (int p1 = h - 2; p1 >= 0; p1 -= R) {
-      double bb[R], bd[R], bu[R], bn[R], bt[R];
+      SW bb[R], bd[R], bu[R];
+      double bn[R], bt[R];
 #pragma unroll
       for (int u = 0; u < R; ++u) {
         const int p = p1 - u;
@@ -474,13 +371,14 @@ __global__ void __launch_bounds__(128) k_sa_sweep2(Sa S) {
       }
     }
   } else {
-    double x = (d1 * b2 - l2 * b1) / det;
+    SW x = (d1 * b2 - l2 * b1) / det;
     {
       const int l = lb + (h + 1) * st;
       put(l, x, DIR == 2 ? S.q[4][l] : 0.0, DIR == 2 ? S.dtev[l] : 0.0);
     }
     for (int p0 = h + 1; p0 < n; p0 += R) {
-      double bb[R], bd[R], bu[R], bn[R], bt[R];
+      SW bb[R], bd[R], bu[R];
+      double bn[R], bt[R];
 #pragma unroll
       for (int u = 0; u < R; ++u) {
         const int p = p0 + u;
@@ -504,8 +402,8 @@ __global__ void __launch_bounds__(128) k_sa_sweep2(Sa S) {
 
 // boundary values of nu_tilde (src/rhs_sa_bcond.F90:40-269): one kernel per
 // face pair in the order i, j, k; full transverse ranges.
-template <int DIR>
-__global__ void k_sa_bc(Sa S) {
+template <class SW, int DIR>
+__global__ void k_sa_bc(SaT<SW> S) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   const int b = blockIdx.y;
   int amax, n, st, lb;
@@ -528,7 +426,8 @@ __global__ void k_sa_bc(Sa S) {
 }
 
 // nu_tilde >= 1e-7 and nu_t = nu_tilde f_v1 on every node (src/rhs_sa_bcond.F90:279-291)
-__global__ void k_sa_clamp(Sa S) {
+template <class SW>
+__global__ void k_sa_clamp(SaT<SW> S) {
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= S.N) return;
   double v = S.q[4][l];
