@@ -53,8 +53,8 @@ def alg_bytes(kind, T, W, coarse):
         "norm": 15 * T,                   # q5 qold5 | qold5
         "rsmooth": 8 * T,                 # dq4 in/out (last one: q4 in/out instead)
         "prolong": 4 * T,                 # dq4 out (coarse reads amortised)
-        "sa_rhs": 18 * 8,                 # q2..5, qn5 qnm1-5, metrics9, aj, wd, dtev | rh
-        "sa_sweep": 10 * 8,               # rh in/out, q5, u v w (U/J), metrics3, aj, dtev
+        "sa_rhs": 19 * 8 + 10 * W,        # q2..5, qn5 qnm1-5, metrics9, aj, wd, wo, dtev | rh, ADI rows 9
+        "sa_sweep": 5 * W + 8,            # ADI row 3, rh in/out; k sweep: q5 in/out, dtev (1/3 each)
     }.get(kind)
 
 

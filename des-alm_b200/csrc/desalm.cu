@@ -1134,7 +1134,8 @@ SaT<SW> make_sa(desalm_ctx* ctx, Lv<double, W>& L) {
   for (int d = 0; d < 3; ++d) { S.csi[d] = L.csi[d]; S.eta[d] = L.eta[d]; S.zet[d] = L.zet[d]; }
   S.aj = L.aj; S.wd = ctx->wd; S.dtev = ctx->dtev; S.nut = L.nut;
   S.wo = ctx->sa.a[0];
-  S.rh = (SW*)ctx->sa.a[1]; S.sd = (SW*)ctx->sa.a[2]; S.su = (SW*)ctx->sa.a[3];
+  S.rh = (SW*)ctx->sa.a[1]; S.sd = (SW*)ctx->sa.a[2];
+  for (int t = 0; t < 9; ++t) S.co[t] = (SW*)ctx->sa.a[3 + t];
   S.flags = ctx->flags;
   S.ren = ctx->c.ren; S.delti = ctx->c.delti; S.es = ctx->c.unsteady ? 1.0 : 0.0;
   for (int b = 0; b < 6; ++b) { S.sa1[b] = ctx->par.sa[0][b]; S.sb1[b] = ctx->par.sb[0][b]; S.btype[b] = ctx->c.btype[b]; }
@@ -1150,9 +1151,9 @@ int sa_run(desalm_ctx* ctx, Lv<double, W>& L) {
   LAUNCH(KC_SA_RHS, 0, nin, k_sa_source<W><<<gi, blk3(), 0, s>>>(S));
   for (int it = 0; it < ctx->c.itk; ++it) {
     LAUNCH(KC_SA_RHS, 0, nin, k_sa_rhs<W><<<gi, blk3(), 0, s>>>(S));
-    LAUNCH(KC_SA_SWEEP, 0, nin, k_sa_sweep2<W, 0><<<dim3(cdiv(L.jm - 2, 64), L.km - 2), 128, 0, s>>>(S));
-    LAUNCH(KC_SA_SWEEP, 0, nin, k_sa_sweep2<W, 1><<<dim3(cdiv(L.im - 2, 64), L.km - 2), 128, 0, s>>>(S));
-    LAUNCH(KC_SA_SWEEP, 0, nin, k_sa_sweep2<W, 2><<<dim3(cdiv(L.im - 2, 64), L.jm - 2), 128, 0, s>>>(S));
+    LAUNCH(KC_SA_SWEEP, 0, nin, k_sa_sweep3<W, 0><<<dim3(cdiv(L.jm - 2, 64), L.km - 2), 128, 0, s>>>(S));
+    LAUNCH(KC_SA_SWEEP, 0, nin, k_sa_sweep3<W, 1><<<dim3(cdiv(L.im - 2, 64), L.km - 2), 128, 0, s>>>(S));
+    LAUNCH(KC_SA_SWEEP, 0, nin, k_sa_sweep3<W, 2><<<dim3(cdiv(L.im - 2, 64), L.jm - 2), 128, 0, s>>>(S));
     LAUNCH(KC_SA_BC, 0, 2.0 * L.jm * L.km, k_sa_bc<W, 0><<<dim3(cdiv(L.jm, 64), L.km), 64, 0, s>>>(S));
     LAUNCH(KC_SA_BC, 0, 2.0 * L.im * L.km, k_sa_bc<W, 1><<<dim3(cdiv(L.im, 64), L.km), 64, 0, s>>>(S));
     LAUNCH(KC_SA_BC, 0, 2.0 * L.im * L.jm, k_sa_bc<W, 2><<<dim3(cdiv(L.im, 64), L.jm), 64, 0, s>>>(S));

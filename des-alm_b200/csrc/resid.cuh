@@ -151,7 +151,6 @@ __global__ void __launch_bounds__(128, DESALM_KR_MINBLOCKS) k_resid(Lv<T, W> L, 
       acc[d] = fpl - T(2) * f0 + fmi;
     }
     diss1 = T(P.pdiss) * (acc[0] + acc[1] + acc[2]);
-    L.diss1[l] = diss1;
   } else {
     diss1 = L.diss1[l];
   }
@@ -215,14 +214,13 @@ __global__ void __launch_bounds__(128, DESALM_KR_MINBLOCKS) k_resid(Lv<T, W> L, 
   }
 
   // ---- FAS forcing on coarse levels
+  T pkn[4];
   if (coarse) {
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
       T pk = L.pk[m][l];
-      if (MODE == 0 && calc_pk) {
-        pk = pk - rh[m];
-        L.pk[m][l] = pk;
-      }
+      if (MODE == 0 && calc_pk) pk = pk - rh[m];
+      pkn[m] = pk;
       rh[m] = rh[m] + pk;
     }
   }
@@ -232,6 +230,8 @@ __global__ void __launch_bounds__(128, DESALM_KR_MINBLOCKS) k_resid(Lv<T, W> L, 
     for (int m = 0; m < 4; ++m) L.rh[m][l] = rh[m];
     return;
   }
+  // Every store of the first pass is issued after the last load, so that no
+  // store can force a metric or state value to be read again.
 
   // ---- r = S (-dtau rh J), then Ma^-1 r
   const T dtau = L.dtau[l];
@@ -240,23 +240,15 @@ __global__ void __launch_bounds__(128, DESALM_KR_MINBLOCKS) k_resid(Lv<T, W> L, 
   T r[4];
 #pragma unroll
   for (int m = 0; m < 4; ++m) r[m] = s[m] * (-dtau * rh[m] * L.aj[l]);
-  if (bback && (i == 1 || i == 2)) {
-    W* b = L.bi + (i - 1) * 4 * (L.jm * L.km);
-    const int o = j + L.jm * k;
-#pragma unroll
-    for (int m = 0; m < 4; ++m) b[m * (L.jm * L.km) + o] = W(r[m]);
-  }
   T sg, th;
   sigma_theta(dtau, P, sg, th);
+  W rp[4];
   {
     // Ma^-1 in the sweep precision W (the preconditioner's precision)
     M4<W> A;
     modal_inv(W(L.csi[0][l]), W(L.csi[1][l]), W(L.csi[2][l]), W(sg), A);
     W rw[4] = {W(r[0]), W(r[1]), W(r[2]), W(r[3])};
-    W rp[4];
     mv4(A, rw, rp);
-#pragma unroll
-    for (int m = 0; m < 4; ++m) L.wk[m][l] = rp[m];
   }
 
   // ---- line-sweep coefficients of every direction (src/rhs_diag_solver.F90:
@@ -264,6 +256,7 @@ __global__ void __launch_bounds__(128, DESALM_KR_MINBLOCKS) k_resid(Lv<T, W> L, 
   // h = dtau (dxi/2) spr, which the neighbouring rows multiply by lambda.
   // The boundary nodes before/after each line get their h too.
   const T* const* mt[3] = {L.csi, L.eta, L.zet};
+  W tcv[3], hcv[3], hcb[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     const T* const* m3 = mt[d];
@@ -271,15 +264,37 @@ __global__ void __launch_bounds__(128, DESALM_KR_MINBLOCKS) k_resid(Lv<T, W> L, 
     T spr = th * sqrt(g);
     T dq = dsp[d] * dsp[d];
     T dh = T(0.5) * dsp[d];
-    L.tc[d][l] = W(dtau * T(P.ep1[d]) * spr * dq);
-    L.hc[d][l] = W(dtau * dh * spr);
+    tcv[d] = W(dtau * T(P.ep1[d]) * spr * dq);
+    hcv[d] = W(dtau * dh * spr);
+    hcb[d] = W(0);
     if (pos[d] == 1 || pos[d] == ext[d] - 2) {
       const int lb = pos[d] == 1 ? l - st[d] : l + st[d];
       T s2, t2;
       sigma_theta(L.dtau[lb], P, s2, t2);
       T g2 = m3[0][lb] * m3[0][lb] + m3[1][lb] * m3[1][lb] + m3[2][lb] * m3[2][lb];
-      L.hc[d][lb] = W(L.dtau[lb] * dh * (t2 * sqrt(g2)));
+      hcb[d] = W(L.dtau[lb] * dh * (t2 * sqrt(g2)));
     }
+  }
+
+  // ---- stores
+  if (MODE == 0) L.diss1[l] = diss1;
+  if (coarse && calc_pk) {
+#pragma unroll
+    for (int m = 0; m < 4; ++m) L.pk[m][l] = pkn[m];
+  }
+  if (bback && (i == 1 || i == 2)) {
+    W* b = L.bi + (i - 1) * 4 * (L.jm * L.km);
+    const int o = j + L.jm * k;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) b[m * (L.jm * L.km) + o] = W(r[m]);
+  }
+#pragma unroll
+  for (int m = 0; m < 4; ++m) L.wk[m][l] = rp[m];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    L.tc[d][l] = tcv[d];
+    L.hc[d][l] = hcv[d];
+    if (pos[d] == 1 || pos[d] == ext[d] - 2) L.hc[d][pos[d] == 1 ? l - st[d] : l + st[d]] = hcb[d];
   }
 }
 

@@ -9,8 +9,8 @@ namespace desalm {
 
 // fine-level FP64 work arrays of the SA model
 struct SaWork {
-  static const int NARR = 4;
-  double* a[NARR];  // wo, rh5, sd, su
+  static const int NARR = 12;
+  double* a[NARR];  // wo, rh5, sd, then the ADI coefficients aw, ap, ae of the i, j, k lines
 };
 
 // SW: type of the ADI work arrays and arithmetic (double in FP64 mode,
@@ -32,7 +32,7 @@ struct SaT {
   double* wo;
   SW* rh;
   SW* sd;
-  SW* su;
+  SW* co[9];  // co[3 d + 0..2] = aw, ap, ae of the direction-d line through each interior node
   int* flags;
   double ren, delti, es;
   double sa1[6], sb1[6];  // pressure-row extrapolation coefficients, sa(1,b), sb(1,b)
@@ -121,9 +121,44 @@ DESALM_DEV double sa_conv_face(const SaT<SW>& S, int dir, int l0, int st) {
   return 0.5 * (v[l1] * u1 + v[l0] * u0 - eigh * (v[l1] - v[l0]));
 }
 
+// Tridiagonal row (aw, ap, ae) of the scalar ADI for nu_tilde at interior
+// node l along direction DIR (src/rhs_sa_adi_solver.F90:50-244): first-order
+// upwind convection plus the face diffusivity, scaled by dtev J / 2.  It is
+// evaluated in SW from the nodal values rounded to SW, and stored per node so
+// that the three sweeps read three coefficients instead of rebuilding them
+// from eight state and metric arrays.
+template <class SW, int DIR>
+DESALM_DEV void sa_adi_row(const SaT<SW>& S, int l) {
+  const int st = DIR == 0 ? 1 : (DIR == 1 ? S.sj : S.sk);
+  const double* const* mt = DIR == 0 ? S.csi : (DIR == 1 ? S.eta : S.zet);
+  const SW sig = SW(2.0 / 3.0), rei = SW(1.0 / S.ren), half_ = SW(0.5);
+  SW m0[3], m1[3], m2[3], nu[3], aj[3], u[3];
+#pragma unroll
+  for (int t = 0; t < 3; ++t) {
+    const int n = l + (t - 1) * st;
+    m0[t] = SW(mt[0][n]); m1[t] = SW(mt[1][n]); m2[t] = SW(mt[2][n]);
+    nu[t] = SW(S.q[4][n]); aj[t] = SW(S.aj[n]);
+    const SW tmp = SW(1) / aj[t];
+    u[t] = tmp * (m0[t] * SW(S.q[1][n]) + m1[t] * SW(S.q[2][n]) + m2[t] * SW(S.q[3][n]));
+  }
+  SW av[2];
+#pragma unroll
+  for (int f = 0; f < 2; ++f) {  // faces (l - st, l) and (l, l + st)
+    const SW gx = m0[f + 1] + m0[f], gy = m1[f + 1] + m1[f], gz = m2[f + 1] + m2[f];
+    const SW ev = (rei + half_ * (nu[f + 1] + nu[f])) / sig;
+    const SW ucna = half_ * dabs(u[f + 1] + u[f]);
+    av[f] = ucna + ev * (gx * gx + gy * gy + gz * gz) / (aj[f + 1] + aj[f]);
+  }
+  const SW dtj = half_ * SW(S.dtev[l]) * aj[1];
+  S.co[3 * DIR + 0][l] = -dtj * (u[0] + av[0]);
+  S.co[3 * DIR + 1][l] = SW(1) + dtj * (av[0] + av[1]);
+  S.co[3 * DIR + 2][l] = dtj * (u[2] - av[1]);
+}
+
 // One fused pass of rhs_sa_grdnu, rhs_sa_prod, rhs_sa_viscous, rhs_sa_flux,
 // rhs_sa_unst_visc and rhs_sa_implicit_source on interior nodes
-// (src/des_eddy.F90:164-223); boundary values of rh stay zero.
+// (src/des_eddy.F90:164-223), plus the ADI rows; boundary values of rh stay
+// zero.
 template <class SW>
 __global__ void __launch_bounds__(128) k_sa_rhs(SaT<SW> S) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -199,18 +234,24 @@ __global__ void __launch_bounds__(128) k_sa_rhs(SaT<SW> S) {
   double dq5dt = S.es * (3.0 * q5[l] - 4.0 * S.qn5[l] + S.qnm1_5[l]) / dtj;
   double r = rh + dq5dt - visc - psa / S.aj[l];
   S.rh[l] = SW(-S.dtev[l] * S.aj[l] * r);
+  // ADI rows of the three directions for this nu_tilde (its values change
+  // only at the end of the k sweep)
+  sa_adi_row<SW, 0>(S, l);
+  sa_adi_row<SW, 1>(S, l);
+  sa_adi_row<SW, 2>(S, l);
 }
 
 // Scalar ADI sweep of nu_tilde along one direction
-// (src/rhs_sa_adi_solver.F90:50-244), two-ended: a CTA owns 64 lines;
-// threads 0-63 eliminate the upper half of each line top-down (SGTSV's
-// no-interchange order; a would-swap row is counted in flags[0]), threads
-// 64-127 the lower half bottom-up; the halves meet in a 2x2 solve and
-// back-substitute.  The k sweep ends with the update
+// (src/rhs_sa_adi_solver.F90:50-244) on the stored rows, two-ended: a CTA
+// owns 64 lines; threads 0-63 eliminate the upper half of each line top-down
+// (SGTSV's no-interchange order; a would-swap row is counted in flags[0]),
+// threads 64-127 the lower half bottom-up; the halves meet in a 2x2 solve
+// and back-substitute.  Rows are read R nodes at a time so that R loads are
+// in flight per thread.  The k sweep ends with the update
 // nu <- nu + (-nu + (nu_old + dnu)) / (1 + 1.5 dtev / dt)
 // (src/des_eddy.F90:260-272).
 template <class SW, int DIR>
-__global__ void __launch_bounds__(128) k_sa_sweep2(SaT<SW> S) {
+__global__ void __launch_bounds__(128) k_sa_sweep3(SaT<SW> S) {
   __shared__ SW m_d[64], m_c[64], m_b[64], n_d[64], n_c[64], n_b[64];
   const int lane = threadIdx.x & 63, half = threadIdx.x >> 6;
   const int a = blockIdx.x * 64 + lane + 1;
@@ -220,43 +261,22 @@ __global__ void __launch_bounds__(128) k_sa_sweep2(SaT<SW> S) {
   else if (DIR == 1) { amax = S.im - 2; n = S.jm - 2; st = S.sj; lb = a + S.sk * b; }
   else { amax = S.im - 2; n = S.km - 2; st = S.sk; lb = a + S.sj * b; }
   const bool act = a <= amax;
-  const double* const* mt = DIR == 0 ? S.csi : (DIR == 1 ? S.eta : S.zet);
-  const SW sig = SW(2.0 / 3.0), rei = SW(1.0 / S.ren), half_ = SW(0.5);
-  const double* q5 = S.q[4];
-  struct Nd { SW m0, m1, m2, nu, aj, u; };
-  auto load = [&](int l) {
-    Nd d;
-    d.m0 = SW(mt[0][l]); d.m1 = SW(mt[1][l]); d.m2 = SW(mt[2][l]);
-    d.nu = SW(q5[l]); d.aj = SW(S.aj[l]);
-    const SW tmp = SW(1) / d.aj;
-    d.u = tmp * (d.m0 * SW(S.q[1][l]) + d.m1 * SW(S.q[2][l]) + d.m2 * SW(S.q[3][l]));
-    return d;
-  };
-  auto face = [&](const Nd& A, const Nd& B) {  // B = A + st
-    SW gx = B.m0 + A.m0, gy = B.m1 + A.m1, gz = B.m2 + A.m2;
-    SW ev = (rei + half_ * (B.nu + A.nu)) / sig;
-    SW ucna = half_ * dabs(B.u + A.u);
-    return ucna + ev * (gx * gx + gy * gy + gz * gz) / (B.aj + A.aj);
-  };
-  constexpr int R = 4;
+  const SW* __restrict__ caw = S.co[3 * DIR + 0];
+  const SW* __restrict__ cap = S.co[3 * DIR + 1];
+  const SW* __restrict__ cae = S.co[3 * DIR + 2];
+  constexpr int R = 8;
   const int h = n / 2;
   int npiv = 0;
   if (act && half == 0) {
-    Nd prev = load(lb), cur = load(lb + st);
-    SW avw = face(prev, cur);
-    SW uw = prev.u;
     SW dprev = 0, duprev = 0, bprev = 0;
     for (int p0 = 0; p0 < h; p0 += R) {
-      Nd east[R];
-      SW bdt[R], brh[R];
+      SW raw[R], rap[R], rae[R], rrh[R];
 #pragma unroll
       for (int u = 0; u < R; ++u) {
         const int p = p0 + u;
         if (p < h) {
           const int l = lb + (p + 1) * st;
-          east[u] = load(l + st);
-          bdt[u] = SW(S.dtev[l]);
-          brh[u] = S.rh[l];
+          raw[u] = caw[l]; rap[u] = cap[l]; rae[u] = cae[l]; rrh[u] = S.rh[l];
         }
       }
 #pragma unroll
@@ -264,41 +284,30 @@ __global__ void __launch_bounds__(128) k_sa_sweep2(SaT<SW> S) {
         const int p = p0 + u;
         if (p < h) {
           const int l = lb + (p + 1) * st;
-          const SW ave = face(cur, east[u]);
-          const SW dtj = half_ * bdt[u] * cur.aj;
-          const SW aw = -dtj * (uw + avw);
-          const SW ap = SW(1) + dtj * (avw + ave);
-          const SW ae = dtj * (east[u].u - ave);
           SW d;
-          if (p == 0) { d = ap; bprev = brh[u]; }
+          if (p == 0) { d = rap[u]; bprev = rrh[u]; }
           else {
-            npiv += dabs(dprev) < dabs(aw);
-            const SW f = aw / dprev;
-            d = ap - f * duprev;
-            bprev = brh[u] - f * bprev;
+            npiv += dabs(dprev) < dabs(raw[u]);
+            const SW f = raw[u] / dprev;
+            d = rap[u] - f * duprev;
+            bprev = rrh[u] - f * bprev;
           }
-          S.sd[l] = d; S.su[l] = ae; S.rh[l] = bprev;
-          dprev = d; duprev = ae;
-          avw = ave; uw = cur.u; cur = east[u];
+          S.sd[l] = d; S.rh[l] = bprev;
+          dprev = d; duprev = rae[u];
         }
       }
     }
     m_d[lane] = dprev; m_c[lane] = duprev; m_b[lane] = bprev;
   } else if (act && half == 1) {
-    Nd east = load(lb + (n + 1) * st), cur = load(lb + n * st);
-    SW ave = face(cur, east);
     SW dprev = 0, awprev = 0, bprev = 0;
     for (int p0 = n - 1; p0 >= h; p0 -= R) {
-      Nd west[R];
-      SW bdt[R], brh[R];
+      SW raw[R], rap[R], rae[R], rrh[R];
 #pragma unroll
       for (int u = 0; u < R; ++u) {
         const int p = p0 - u;
         if (p >= h) {
           const int l = lb + (p + 1) * st;
-          west[u] = load(l - st);
-          bdt[u] = SW(S.dtev[l]);
-          brh[u] = S.rh[l];
+          raw[u] = caw[l]; rap[u] = cap[l]; rae[u] = cae[l]; rrh[u] = S.rh[l];
         }
       }
 #pragma unroll
@@ -306,22 +315,16 @@ __global__ void __launch_bounds__(128) k_sa_sweep2(SaT<SW> S) {
         const int p = p0 - u;
         if (p >= h) {
           const int l = lb + (p + 1) * st;
-          const SW avw = face(west[u], cur);
-          const SW dtj = half_ * bdt[u] * cur.aj;
-          const SW aw = -dtj * (west[u].u + avw);
-          const SW ap = SW(1) + dtj * (avw + ave);
-          const SW ae = dtj * (east.u - ave);
           SW d;
-          if (p == n - 1) { d = ap; bprev = brh[u]; }
+          if (p == n - 1) { d = rap[u]; bprev = rrh[u]; }
           else {
-            npiv += dabs(dprev) < dabs(ae);
-            const SW f = ae / dprev;
-            d = ap - f * awprev;
-            bprev = brh[u] - f * bprev;
+            npiv += dabs(dprev) < dabs(rae[u]);
+            const SW f = rae[u] / dprev;
+            d = rap[u] - f * awprev;
+            bprev = rrh[u] - f * bprev;
           }
-          S.sd[l] = d; S.su[l] = aw; S.rh[l] = bprev;
-          dprev = d; awprev = aw;
-          ave = avw; east = cur; cur = west[u];
+          S.sd[l] = d; S.rh[l] = bprev;
+          dprev = d; awprev = raw[u];
         }
       }
     }
@@ -343,58 +346,33 @@ __global__ void __launch_bounds__(128) k_sa_sweep2(SaT<SW> S) {
       S.rh[l] = x;
     }
   };
-  if (half == 0) {
-    SW x = (b1 * d2 - u1 * b2) / det;
-    {
-      const int l = lb + h * st;
-      put(l, x, DIR == 2 ? S.q[4][l] : 0.0, DIR == 2 ? S.dtev[l] : 0.0);
-    }
-    for (int p1 = h - 2; p1 >= 0; p1 -= R) {
-      SW bb[R], bd[R], bu[R];
-      double bn[R], bt[R];
+  // half 0 runs back from node h-1 with the ae couplings, half 1 forward
+  // from node h with the aw couplings
+  const SW* __restrict__ cup = half == 0 ? cae : caw;
+  SW x = half == 0 ? (b1 * d2 - u1 * b2) / det : (d1 * b2 - l2 * b1) / det;
+  {
+    const int l = lb + (half == 0 ? h : h + 1) * st;
+    put(l, x, DIR == 2 ? S.q[4][l] : 0.0, DIR == 2 ? S.dtev[l] : 0.0);
+  }
+  const int cnt = half == 0 ? h - 1 : n - h - 1;  // nodes left to back-substitute
+  const int pstart = half == 0 ? h - 2 : h + 1;
+  const int dp = half == 0 ? -1 : 1;
+  for (int t0 = 0; t0 < cnt; t0 += R) {
+    SW bb[R], bd[R], bu[R];
+    double bn[R], bt[R];
 #pragma unroll
-      for (int u = 0; u < R; ++u) {
-        const int p = p1 - u;
-        if (p >= 0) {
-          const int l = lb + (p + 1) * st;
-          bb[u] = S.rh[l]; bd[u] = S.sd[l]; bu[u] = S.su[l];
-          if (DIR == 2) { bn[u] = S.q[4][l]; bt[u] = S.dtev[l]; }
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < R; ++u) {
-        const int p = p1 - u;
-        if (p >= 0) {
-          x = (bb[u] - bu[u] * x) / bd[u];
-          put(lb + (p + 1) * st, x, DIR == 2 ? bn[u] : 0.0, DIR == 2 ? bt[u] : 0.0);
-        }
+    for (int u = 0; u < R; ++u) {
+      if (t0 + u < cnt) {
+        const int l = lb + (pstart + dp * (t0 + u) + 1) * st;
+        bb[u] = S.rh[l]; bd[u] = S.sd[l]; bu[u] = cup[l];
+        if (DIR == 2) { bn[u] = S.q[4][l]; bt[u] = S.dtev[l]; }
       }
     }
-  } else {
-    SW x = (d1 * b2 - l2 * b1) / det;
-    {
-      const int l = lb + (h + 1) * st;
-      put(l, x, DIR == 2 ? S.q[4][l] : 0.0, DIR == 2 ? S.dtev[l] : 0.0);
-    }
-    for (int p0 = h + 1; p0 < n; p0 += R) {
-      SW bb[R], bd[R], bu[R];
-      double bn[R], bt[R];
 #pragma unroll
-      for (int u = 0; u < R; ++u) {
-        const int p = p0 + u;
-        if (p < n) {
-          const int l = lb + (p + 1) * st;
-          bb[u] = S.rh[l]; bd[u] = S.sd[l]; bu[u] = S.su[l];
-          if (DIR == 2) { bn[u] = S.q[4][l]; bt[u] = S.dtev[l]; }
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < R; ++u) {
-        const int p = p0 + u;
-        if (p < n) {
-          x = (bb[u] - bu[u] * x) / bd[u];
-          put(lb + (p + 1) * st, x, DIR == 2 ? bn[u] : 0.0, DIR == 2 ? bt[u] : 0.0);
-        }
+    for (int u = 0; u < R; ++u) {
+      if (t0 + u < cnt) {
+        x = (bb[u] - bu[u] * x) / bd[u];
+        put(lb + (pstart + dp * (t0 + u) + 1) * st, x, DIR == 2 ? bn[u] : 0.0, DIR == 2 ? bt[u] : 0.0);
       }
     }
   }
