@@ -10,6 +10,7 @@
 #include <stdint.h>
 
 #define DESALM_DEV __device__ __forceinline__
+#define DESALM_HD __host__ __device__
 
 namespace desalm {
 
@@ -37,10 +38,9 @@ struct Lv {
   const T* eta[3];
   const T* zet[3];
   const T* aj;
-  // DAF work: transformed residual, forward-elimination scratch
+  // DAF work: transformed residual and row coefficients
   W* wk[4];
-  W* sd[4];        // eliminated diagonal, one array per system
-  W* su[3];        // super-diagonal: systems (1,2), 3, 4 (first-generation sweep)
+  W* sig;          // sigma = sqrt(beta alpha) of each interior node, from the first residual pass
   W* tc[3];        // per direction: tmp = dtau ep spr dsq (diagonal part of each row)
   W* hc[3];        // per direction: dtau (dxi/2) spr (neighbour coupling of the
                    // characteristic rows); also set on the boundary nodes that

@@ -27,7 +27,7 @@ namespace {
 
 // Convergence state of the device-side pseudo-time loop.
 struct DevConv {
-  int itc, converged, pivots, nonfinite;
+  int itc, converged, pivots, nonfinite, zero_pivots, pad_;
   double res[5], init[5];
 };
 
@@ -51,6 +51,7 @@ __global__ void k_conv(const double* part, int nblk, DevConv* st, const int* fla
   }
   st->itc += 1;
   st->pivots += flags[0];
+  st->zero_pivots += flags[1];
   if (st->itc == 1)
     for (int m = 0; m < 5; ++m) st->init[m] = res[m];
   double eomax = fmax(res[1], fmax(res[2], res[3]));
@@ -61,7 +62,7 @@ __global__ void k_conv(const double* part, int nblk, DevConv* st, const int* fla
   int finite = isfinite(res[1]) && isfinite(res[2]) && isfinite(res[3]);
   st->converged = conv;
   st->nonfinite = !finite;
-  cudaGraphSetConditional(h, (!conv && finite && st->itc < cp.itmax) ? 1u : 0u);
+  cudaGraphSetConditional(h, (!conv && finite && st->zero_pivots == 0 && st->itc < cp.itmax) ? 1u : 0u);
 }
 
 struct DevBuf {
@@ -79,7 +80,6 @@ struct Level {
   std::vector<void*> allocs;
   Lv<double, double> dd{};
   Lv<double, float> df{};
-  Lv<float, float> ff{};
   void* dq[4] = {nullptr, nullptr, nullptr, nullptr};  // prolongation correction
   double* fac[3] = {nullptr, nullptr, nullptr};         // rsmooth multipliers
   double* dpr[3] = {nullptr, nullptr, nullptr};         // rsmooth eliminated diagonal
@@ -206,8 +206,8 @@ int alloc_level(desalm_ctx* ctx, Level& G, Lv<T, W>& L) {
   }
   RET(A((T**)&L.aj));
   for (int m = 0; m < 4; ++m) RET(AW(&L.wk[m]));
-  for (int m = 0; m < 4; ++m) RET(AW(&L.sd[m]));
-  for (int m = 0; m < 3; ++m) { RET(AW(&L.su[m])); RET(AW(&L.tc[m])); RET(AW(&L.hc[m])); }
+  RET(AW(&L.sig));
+  for (int m = 0; m < 3; ++m) { RET(AW(&L.tc[m])); RET(AW(&L.hc[m])); }
   RET(dalloc(ctx, G.allocs, (void**)&L.bi, sizeof(W) * 8L * G.jm * G.km));
   RET(dalloc(ctx, G.allocs, (void**)&L.bj, sizeof(W) * 16L * G.im * G.km));
   RET(dalloc(ctx, G.allocs, (void**)&L.bk, sizeof(W) * 16L * G.im * G.jm));
@@ -278,6 +278,59 @@ dim3 blk3() { return dim3(32, 4, 1); }
 template <class T, class W>
 dim3 grid_interior(const Lv<T, W>& L) { return dim3(cdiv(L.im - 2, 32), cdiv(L.jm - 2, 4), L.km - 2); }
 
+// One DAF line sweep as k_sweep4 with the widest slab (lines per CTA) whose
+// shared memory leaves room for two CTAs per SM, else the widest that fits
+// one CTA per SM.
+constexpr size_t kSlabTwoPerSm = 110 * 1024;
+constexpr size_t kSlabMax = 220 * 1024;  // below the 227 KB opt-in less the kernels' static shared memory
+template <class W>
+size_t slab_bytes(int n, int nl) { return (size_t)10 * slab_fs(n + 2, nl + 1) * sizeof(W); }
+
+template <class T, class W, int DIR, int NL>
+int sweep4_nl(desalm_ctx* ctx, Lv<T, W>& L, const Par& P, int lvl, int blo, int bhi) {
+  int amax, n, nb;
+  if (DIR == 0) { amax = L.jm - 2; n = L.im - 2; nb = L.km - 2; }
+  else if (DIR == 1) { amax = L.im - 2; n = L.jm - 2; nb = L.km - 2; }
+  else { amax = L.im - 2; n = L.km - 2; nb = L.jm - 2; }
+  const size_t bytes = slab_bytes<W>(n, NL);
+  const int cls = DIR == 0 ? KC_SWEEP_I : (DIR == 1 ? KC_SWEEP_J : KC_SWEEP_K);
+  const double nin = double(amax) * n * nb;
+  cudaStream_t s = ctx->stream;
+  LAUNCH(cls, lvl, nin, k_sweep4<T, W, DIR, NL><<<dim3(cdiv(amax, NL), nb), 8 * NL, bytes, s>>>(L, P, blo, bhi));
+  CKL();
+  return 0;
+}
+
+// Shared-memory opt-in of every slab-sweep instantiation on the current
+// device (done when a context is created, outside any stream capture).
+template <class T, class W>
+cudaError_t slab_attrs() {
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  auto set = [&](const void* f) {
+    cudaFuncAttributes fa;
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, f);
+    if (e != cudaSuccess) return;
+    const int mx = (int)std::min<size_t>(kSlabMax, (size_t)optin - fa.sharedSizeBytes);
+    e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  };
+  set((const void*)k_sweep4<T, W, 0, 16>); set((const void*)k_sweep4<T, W, 0, 8>); set((const void*)k_sweep4<T, W, 0, 4>);
+  set((const void*)k_sweep4<T, W, 1, 16>); set((const void*)k_sweep4<T, W, 1, 8>); set((const void*)k_sweep4<T, W, 1, 4>);
+  set((const void*)k_sweep4<T, W, 2, 16>); set((const void*)k_sweep4<T, W, 2, 8>); set((const void*)k_sweep4<T, W, 2, 4>);
+  return e;
+}
+
+template <class T, class W, int DIR>
+int launch_sweep(desalm_ctx* ctx, Lv<T, W>& L, const Par& P, int lvl, int blo, int bhi) {
+  const int n = DIR == 0 ? L.im - 2 : (DIR == 1 ? L.jm - 2 : L.km - 2);
+  if (slab_bytes<W>(n, 16) <= kSlabTwoPerSm) return sweep4_nl<T, W, DIR, 16>(ctx, L, P, lvl, blo, bhi);
+  if (slab_bytes<W>(n, 8) <= kSlabTwoPerSm) return sweep4_nl<T, W, DIR, 8>(ctx, L, P, lvl, blo, bhi);
+  if (slab_bytes<W>(n, 4) <= kSlabMax) return sweep4_nl<T, W, DIR, 4>(ctx, L, P, lvl, blo, bhi);
+  ctx->err = "grid line too long for the shared-memory line sweep";
+  return DESALM_EINVAL;
+}
+
 template <class T, class W>
 int launch_daf(desalm_ctx* ctx, Lv<T, W>& L, Level& G, int n, int recalc, int itr) {
   Par P = ctx->par;
@@ -295,13 +348,9 @@ int launch_daf(desalm_ctx* ctx, Lv<T, W>& L, Level& G, int n, int recalc, int it
   const double nin = double(L.im - 2) * (L.jm - 2) * (L.km - 2);
   LAUNCH(KC_RESID, n, nin, k_resid<T, W, 0><<<grid_interior(L), blk3(), 0, s>>>(L, P, upwind, itr == 1 ? 1 : 0, n > 0 ? 1 : 0, bback));
   CKL();
-  LAUNCH(KC_SWEEP_I, n, nin, k_sweep3<T, W, 0><<<dim3(cdiv(L.jm - 2, 32), L.km - 2), 256, 0, s>>>(L, P, bback, 0));
-  CKL();
-  LAUNCH(KC_SWEEP_J, n, nin, k_sweep3<T, W, 1><<<dim3(cdiv(L.im - 2, 32), L.km - 2), 256, 0, s>>>(L, P, fine && c.btype[2] != 5, fine && c.btype[3] != 5));
-  CKL();
-  LAUNCH(KC_SWEEP_K, n, nin, k_sweep3<T, W, 2><<<dim3(cdiv(L.im - 2, 32), L.jm - 2), 256, 0, s>>>(L, P, fine && c.btype[4] != 5,
-                                                                      fine && c.btype[5] != 5 && c.btype[5] != 6));
-  CKL();
+  RET((launch_sweep<T, W, 0>(ctx, L, P, n, bback, 0)));
+  RET((launch_sweep<T, W, 1>(ctx, L, P, n, fine && c.btype[2] != 5, fine && c.btype[3] != 5)));
+  RET((launch_sweep<T, W, 2>(ctx, L, P, n, fine && c.btype[4] != 5, fine && c.btype[5] != 5 && c.btype[5] != 6)));
   return 0;
 }
 
@@ -381,8 +430,7 @@ int launch_norm(desalm_ctx* ctx, Lv<T, W>& L, int copy, double* out) {
 // every level (residual, metrics, update, restriction, coarse corrections
 // q_c - qold_c, which FP32 storage would lose to cancellation) and FP32
 // line-sweep work (LHS coefficients, eliminated rows, transformed residual).
-// The FP32-state view (K_FF) is kept for experiments only.
-enum Kind { K_DD, K_DF, K_FF };
+enum Kind { K_DD, K_DF };
 Kind kind_of(const desalm_ctx* ctx, int n) {
   (void)n;
   if (ctx->c.precision_mode == DESALM_FP64) return K_DD;
@@ -394,8 +442,7 @@ Kind kind_of(const desalm_ctx* ctx, int n) {
     Level& G__ = (ctx)->L[n];                                       \
     switch (kind_of(ctx, n)) {                                      \
       case K_DD: return FN((ctx), G__.dd, ##__VA_ARGS__);           \
-      case K_DF: return FN((ctx), G__.df, ##__VA_ARGS__);           \
-      default: return FN((ctx), G__.ff, ##__VA_ARGS__);             \
+      default: return FN((ctx), G__.df, ##__VA_ARGS__);             \
     }                                                               \
   }())
 
@@ -404,8 +451,7 @@ int do_daf(desalm_ctx* ctx, int n, int recalc, int itr) {
   int rc;
   switch (kind_of(ctx, n)) {
     case K_DD: rc = launch_daf(ctx, G.dd, G, n, recalc, itr); break;
-    case K_DF: rc = launch_daf(ctx, G.df, G, n, recalc, itr); break;
-    default: rc = launch_daf(ctx, G.ff, G, n, recalc, itr); break;
+    default: rc = launch_daf(ctx, G.df, G, n, recalc, itr); break;
   }
   if (rc) return rc;
   if (n == 0) {
@@ -416,8 +462,7 @@ int do_daf(desalm_ctx* ctx, int n, int recalc, int itr) {
   if (recalc == 1) {
     switch (kind_of(ctx, n)) {
       case K_DD: rc = launch_recalc(ctx, G.dd, n); break;
-      case K_DF: rc = launch_recalc(ctx, G.df, n); break;
-      default: rc = launch_recalc(ctx, G.ff, n); break;
+      default: rc = launch_recalc(ctx, G.df, n); break;
     }
   }
   return rc;
@@ -432,30 +477,22 @@ int do_nlevel(desalm_ctx* ctx, int n) {  // n = coarse level index (>= 1)
   Level& F = ctx->L[n - 1];
   Level& C = ctx->L[n];
   C.dtau_valid = false;
-  Kind kf = kind_of(ctx, n - 1), kc = kind_of(ctx, n);
-  if (kf == K_DD) return launch_nlevel(ctx, F.dd, C.dd);
-  if (kf == K_DF && kc == K_DF) return launch_nlevel(ctx, F.df, C.df);
-  if (kf == K_DF) return launch_nlevel(ctx, F.df, C.ff);
-  return launch_nlevel(ctx, F.ff, C.ff);
+  if (kind_of(ctx, n - 1) == K_DD) return launch_nlevel(ctx, F.dd, C.dd);
+  return launch_nlevel(ctx, F.df, C.df);
 }
 
 int do_prolong(desalm_ctx* ctx, int n) {  // fine level index n, coarse n+1
   Level& F = ctx->L[n];
   Level& C = ctx->L[n + 1];
-  Kind kf = kind_of(ctx, n);
-  if (kf == K_DD) return launch_prolong(ctx, F.dd, C.dd, F);
-  Kind kc = kind_of(ctx, n + 1);
-  if (kf == K_DF && kc == K_DF) return launch_prolong(ctx, F.df, C.df, F);
-  if (kf == K_DF) return launch_prolong(ctx, F.df, C.ff, F);
-  return launch_prolong(ctx, F.ff, C.ff, F);
+  if (kind_of(ctx, n) == K_DD) return launch_prolong(ctx, F.dd, C.dd, F);
+  return launch_prolong(ctx, F.df, C.df, F);
 }
 
 int do_norm(desalm_ctx* ctx, int n, int copy, double* out) {
   Level& G = ctx->L[n];
   switch (kind_of(ctx, n)) {
     case K_DD: return launch_norm(ctx, G.dd, copy, out);
-    case K_DF: return launch_norm(ctx, G.df, copy, out);
-    default: return launch_norm(ctx, G.ff, copy, out);
+    default: return launch_norm(ctx, G.df, copy, out);
   }
 }
 
@@ -463,7 +500,7 @@ int do_norm(desalm_ctx* ctx, int n, int copy, double* out) {
 int field_ptr(desalm_ctx* ctx, int n, int f, void** p, int* esz) {
   Level& G = ctx->L[n];
   Kind k = kind_of(ctx, n);
-  *esz = (k == K_FF) ? 4 : 8;
+  *esz = 8;
   auto pick = [&](auto& L) -> int {
     if (f >= DESALM_F_Q && f < DESALM_F_Q + 5) { *p = L.q[f - DESALM_F_Q]; return 0; }
     if (f >= DESALM_F_QN && f < DESALM_F_QN + 5) { *p = L.qn[f - DESALM_F_QN]; return 0; }
@@ -486,8 +523,7 @@ int field_ptr(desalm_ctx* ctx, int n, int f, void** p, int* esz) {
     return DESALM_EINVAL;
   };
   if (k == K_DD) return pick(G.dd);
-  if (k == K_DF) return pick(G.df);
-  return pick(G.ff);
+  return pick(G.df);
 }
 
 // Inflow extrapolation ratios on the host from the fine grid
@@ -594,10 +630,9 @@ int desalm_init(const desalm_case* c, desalm_ctx** out) {
     G.dz = 1.0 / std::pow(2.0, double(n * c->kcrs));
     Kind k = kind_of(ctx, n);
     if (k == K_DD) rc = alloc_level(ctx, G, G.dd);
-    else if (k == K_DF) rc = alloc_level(ctx, G, G.df);
-    else rc = alloc_level(ctx, G, G.ff);
+    else rc = alloc_level(ctx, G, G.df);
     if (rc) { *out = ctx; return rc; }
-    G.tbytes = k == K_FF ? 4 : 8;
+    G.tbytes = 8;
     G.wbytes = k == K_DD ? 8 : 4;
     if (n + 1 < ctx->ng) {
       rc = dalloc(ctx, G.allocs, &G.dq[0], (size_t)4 * G.N * G.tbytes);
@@ -636,7 +671,8 @@ int desalm_init(const desalm_case* c, desalm_ctx** out) {
     *out = ctx;
     return DESALM_ENOMEM;
   }
-  e = cudaStreamSynchronize(ctx->stream);
+  e = kind_of(ctx, 0) == K_DD ? slab_attrs<double, double>() : slab_attrs<double, float>();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) {
     ctx->err = std::string("init: ") + cudaGetErrorString(e);
     *out = ctx;
@@ -1061,6 +1097,7 @@ int pseudo_iter(desalm_ctx* ctx, desalm_step_report* rep) {
     for (int m = 0; m < 5; ++m) { rep->residual[m] = res[m]; rep->init_residual[m] = ctx->init_resd[m]; }
     rep->pivots = hflags[0];
   }
+  if (hflags[1]) { ctx->err = "zero pivot in a line solve"; return DESALM_ESINGULAR; }
   for (int m = 1; m < 4; ++m)
     if (!std::isfinite(res[m])) { ctx->err = "non-finite convergence norm"; return DESALM_ENONFINITE; }
   return 0;
@@ -1270,6 +1307,7 @@ int graph_step(desalm_ctx* ctx, desalm_step_report* rep) {
     for (int m = 0; m < 5; ++m) { rep->residual[m] = st.res[m]; rep->init_residual[m] = st.init[m]; }
     rep->pivots = st.pivots;
   }
+  if (st.zero_pivots) { ctx->err = "zero pivot in a line solve"; return DESALM_ESINGULAR; }
   if (st.nonfinite) { ctx->err = "non-finite convergence norm"; return DESALM_ENONFINITE; }
   return 0;
 }

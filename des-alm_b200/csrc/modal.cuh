@@ -139,40 +139,46 @@ DESALM_DEV void mat_mc(const Lv<T, W>& L, const Par& P, int l, M4<T>& A) {
   modal_fwd(L.zet[0][l], L.zet[1][l], L.zet[2][l], s, A);
 }
 
-// The same matrices evaluated in precision C (metrics and dtau read in the
-// level's state precision and rounded to C): the line-sweep precision in
-// MIXED mode, where the transforms belong to the FP32 preconditioner.
-template <class C, class T, class W>
-DESALM_DEV void sigma_c(const Lv<T, W>& L, const Par& P, int l, C& sigma) {
-  T s, t;
-  sigma_theta(L.dtau[l], P, s, t);
-  sigma = C(s);
+// Application of M and M^-1 to a vector in precision C, using the structure
+// of the closed forms above: row 0 of M is (0, 0, sigma, sigma) and its last
+// two columns are opposite; row 0 of M^-1 repeats its last entry and rows 2
+// and 3 share all but the sign of their last three entries; every entry is a
+// polynomial in (c1, c2, c3) times one of 1/s, 1/sqrt(g), 1/(s sqrt(g)) or
+// 1/dm.  With those factors formed once, M x costs two square roots, two
+// divisions and about twenty multiplies instead of the 4x4 matrix's twelve
+// divisions and sixteen multiplies; the result equals mv4 of the matrix up to
+// rounding.
+template <class C>
+DESALM_DEV void mfwd_apply(C c1, C c2, C c3, C sigma, const C x[4], C y[4]) {
+  const C g = c1 * c1 + c2 * c2 + c3 * c3;
+  const C rsg = C(1) / sqrt(g);
+  const C dd = c2 - c3;
+  const C ris = C(1) / sqrt(C(2) * g + dd * dd);
+  const C risg = ris * rsg;
+  const C xd = x[2] - x[3];
+  const C x0s = ris * x[0], x1s = risg * x[1], xds = rsg * xd;
+  y[0] = sigma * (x[2] + x[3]);
+  y[1] = -(c2 + c3) * x0s + c1 * (c3 - c2) * x1s + c1 * xds;
+  y[2] = c1 * x0s + (g + c2 * (c3 - c2)) * x1s + c2 * xds;
+  y[3] = c1 * x0s - (g - c3 * (c3 - c2)) * x1s + c3 * xds;
 }
-template <class C, class T, class W>
-DESALM_DEV void mat_mai_c(const Lv<T, W>& L, const Par& P, int l, M4<C>& A) {
-  C s; sigma_c(L, P, l, s);
-  modal_inv(C(L.csi[0][l]), C(L.csi[1][l]), C(L.csi[2][l]), s, A);
-}
-template <class C, class T, class W>
-DESALM_DEV void mat_n1i_c(const Lv<T, W>& L, const Par& P, int l, M4<C>& A) {
-  C s; sigma_c(L, P, l, s);
-  M4<C> ma, mbi;
-  modal_fwd(C(L.csi[0][l]), C(L.csi[1][l]), C(L.csi[2][l]), s, ma);
-  modal_inv(C(L.eta[0][l]), C(L.eta[1][l]), C(L.eta[2][l]), s, mbi);
-  mm4(mbi, ma, A);
-}
-template <class C, class T, class W>
-DESALM_DEV void mat_n2i_c(const Lv<T, W>& L, const Par& P, int l, M4<C>& A) {
-  C s; sigma_c(L, P, l, s);
-  M4<C> mb, mci;
-  modal_fwd(C(L.eta[0][l]), C(L.eta[1][l]), C(L.eta[2][l]), s, mb);
-  modal_inv(C(L.zet[0][l]), C(L.zet[1][l]), C(L.zet[2][l]), s, mci);
-  mm4(mci, mb, A);
-}
-template <class C, class T, class W>
-DESALM_DEV void mat_mc_c(const Lv<T, W>& L, const Par& P, int l, M4<C>& A) {
-  C s; sigma_c(L, P, l, s);
-  modal_fwd(C(L.zet[0][l]), C(L.zet[1][l]), C(L.zet[2][l]), s, A);
+template <class C>
+DESALM_DEV void minv_apply(C c1, C c2, C c3, C sigma, const C x[4], C y[4]) {
+  const C c1s = c1 * c1, c2s = c2 * c2, c3s = c3 * c3;
+  const C g = c1s + c2s + c3s;
+  const C rsg = C(1) / sqrt(g);
+  const C dd = c2 - c3;
+  const C s = sqrt(C(2) * g + dd * dd);
+  const C rdm = C(1) / (g + C(2) * c2 * c3 + c1s);
+  const C ssgd = s * rsg * rdm, sgd2 = C(0.5) * rsg * rdm;
+  const C r1 = c2 + c3, r2 = c2 - c3, r3 = c2s - c3s;
+  y[0] = s * rdm * (-(c2 + c3) * x[1] + c1 * (x[2] + x[3]));
+  y[1] = ssgd * (c1 * (c3 - c2) * x[1] + (c2 * c3 + c1s + c3s) * x[2] - (c2 * c3 + c1s + c2s) * x[3]);
+  const C e = sgd2 * (c1 * (C(2) * g + C(2) * c2 * c3 - c2s - c3s) * x[1] + (g * r1 + c1s * r2 + c3 * r3) * x[2] +
+                      (g * r1 - c1s * r2 - c2 * r3) * x[3]);
+  const C h0 = C(0.5) / sigma * x[0];
+  y[2] = h0 + e;
+  y[3] = h0 - e;
 }
 
 }  // namespace desalm

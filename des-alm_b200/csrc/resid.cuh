@@ -11,7 +11,7 @@
 // and then either stores the raw residual (recalculation pass,
 // src/solver_daf.F90:432-477) or applies r = S (-dtau J rh) and r <- Ma^-1 r
 // (src/rhs_diag_solver.F90:53-122) and stores the transformed residual for
-// the line sweeps.  Nothing is staged through intermediate full-size arrays.
+// the line sweeps, with sigma and the row coefficients of every direction.
 #pragma once
 #include "modal.cuh"
 
@@ -245,10 +245,8 @@ __global__ void __launch_bounds__(128, DESALM_KR_MINBLOCKS) k_resid(Lv<T, W> L, 
   W rp[4];
   {
     // Ma^-1 in the sweep precision W (the preconditioner's precision)
-    M4<W> A;
-    modal_inv(W(L.csi[0][l]), W(L.csi[1][l]), W(L.csi[2][l]), W(sg), A);
     W rw[4] = {W(r[0]), W(r[1]), W(r[2]), W(r[3])};
-    mv4(A, rw, rp);
+    minv_apply<W>(W(L.csi[0][l]), W(L.csi[1][l]), W(L.csi[2][l]), W(sg), rw, rp);
   }
 
   // ---- line-sweep coefficients of every direction (src/rhs_diag_solver.F90:
@@ -290,6 +288,7 @@ __global__ void __launch_bounds__(128, DESALM_KR_MINBLOCKS) k_resid(Lv<T, W> L, 
   }
 #pragma unroll
   for (int m = 0; m < 4; ++m) L.wk[m][l] = rp[m];
+  L.sig[l] = W(sg);
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     L.tc[d][l] = tcv[d];

@@ -6,7 +6,9 @@
 // K_R; the semi-explicit boundary rows (brh) are applied to the first/last
 // interior rows; the elimination follows LAPACK SGTSV's no-interchange
 // branch (src/sgtsv.f:107-121, 232-243), and a row where SGTSV would swap
-// rows (|d_i| < |dl_i|) is counted in flags[0], a zero pivot in flags[1].
+// rows (|d_i| < |dl_i|) is counted in flags[0], a zero pivot (where SGTSV
+// returns INFO > 0, src/sgtsv.f:112-119) or a singular middle 2x2 block in
+// flags[1].
 // After the solve each node gets the next modal transform (N1^-1 after the i
 // sweep, N2^-1 after the j sweep) or, after the k sweep, Mc and the update
 // q <- q + dq (src/solver_daf.F90:409-418).
@@ -33,37 +35,95 @@ DESALM_DEV void face_vec(const Lv<T, W>& L, const Par& P, int lb, int b, const W
 namespace desalm {
 
 // ---------------------------------------------------------------------------
-// Two-ended line sweep.  A CTA owns 32 lines and
-// has 8 warps: warp m (< 4) eliminates the upper half of system m top-down
-// (SGTSV's no-interchange order), warp 4 + m eliminates the lower half
-// bottom-up; the two meet in a 2x2 solve at the middle rows, then each warp
-// back-substitutes its own half: twice the threads of a one-ended solve and
-// half the dependent chain per line; the result differs from one top-down
-// pass by round-off only.  Phase 2 walks the CTA's nodes with coalesced
-// indexing and applies the modal transform (or the update).
+// Shared-memory slab sweep.  A CTA owns NL lines of one plane (consecutive in
+// the transverse index that is contiguous in memory, or, for the i sweep,
+// NL rows of contiguous i lines) and 8 NL threads.
+//   phase 0  tc, hc and the four transformed residuals of the slab are read
+//            once, with loads coalesced along the fastest global index, into
+//            shared memory laid out [node][line] (line stride NL + 1, so that
+//            the transposed i-sweep stores are free of bank conflicts);
+//   phase 1  thread (line, system m, half) eliminates its half-line in shared
+//            memory exactly as the two-ended sweep does (same operations,
+//            same order); the halves meet in the 2x2 middle solve and
+//            back-substitute; the eliminated diagonal never leaves the SM;
+//   phase 2  every node of the slab gets the next modal transform (or the
+//            update) from the solved values in shared memory and writes its
+//            four results once.
+// Shared memory: 10 fields (tc, hc, r[4], d[4]) of slab_fs(n + 2, NL + 1)
+// elements of W.
 // ---------------------------------------------------------------------------
-template <class T, class W, int DIR>
-__global__ void __launch_bounds__(256) k_sweep3(Lv<T, W> L, Par P, int blo, int bhi) {
-  __shared__ W sbw[32][4], sbe[32][4];
-  __shared__ W mt_d[32][4], mt_u[32][4], mt_b[32][4];   // top half's last eliminated row
-  __shared__ W mb_d[32][4], mb_l[32][4], mb_b[32][4];   // bottom half's last eliminated row
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int m = w & 3, half = w >> 2;
-  const int a0 = blockIdx.x * 32 + 1;
-  const int a = a0 + lane;
+DESALM_HD inline int slab_fs(int np, int nlp) { return ((np * nlp + 31) / 32) * 32 + 16; }
+
+template <class T, class W, int DIR, int NL>
+__global__ void __launch_bounds__(8 * NL) k_sweep4(Lv<T, W> L, Par P, int blo, int bhi) {
+  constexpr int NT = 8 * NL, NLP = NL + 1;
+  extern __shared__ __align__(16) unsigned char sweep_slab[];
+  __shared__ W sbw[NL][4], sbe[NL][4];
+  __shared__ W mt_d[NL][4], mt_u[NL][4], mt_b[NL][4];   // top half's last eliminated row
+  __shared__ W mb_d[NL][4], mb_l[NL][4], mb_b[NL][4];   // bottom half's last eliminated row
+  const int tid = threadIdx.x;
+  const int a0 = blockIdx.x * NL + 1;
   const int b = blockIdx.y + 1;
   int amax, n, st, sa;
   if (DIR == 0) { amax = L.jm - 2; n = L.im - 2; st = 1; sa = L.sj; }
   else if (DIR == 1) { amax = L.im - 2; n = L.jm - 2; st = L.sj; sa = 1; }
   else { amax = L.im - 2; n = L.km - 2; st = L.sk; sa = 1; }
   const int base = (DIR == 2) ? L.sj * b : L.sk * b;
-  const bool act = a <= amax;
-  const int lb = base + a * sa;
-  const int h = n / 2;  // rows 0..h-1 top, h..n-1 bottom (n >= 3)
+  const int nl = min(NL, amax - a0 + 1);
+  const int np = n + 2;
+  const int fs = slab_fs(np, NLP);
+  W* s_tc = reinterpret_cast<W*>(sweep_slab);
+  W* s_hc = s_tc + fs;
+  W* s_r = s_tc + 2 * fs;  // system q at s_r + q fs
+  W* s_d = s_tc + 6 * fs;
 
-  if (w == 0) {
+  // ---- phase 0: slab -> shared memory
+  {
+    const W* tc = L.tc[DIR];
+    const W* hc = L.hc[DIR];
+    const int total = nl * np;
+    constexpr int U = 4;
+    for (int t0 = tid; t0 < total; t0 += NT * U) {
+      W v[U][6];
+      int so[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int t = t0 + u * NT;
+        so[u] = -1;
+        if (t < total) {
+          int li, p;
+          if (DIR == 0) { li = t / np; p = t - li * np; }
+          else { p = t / nl; li = t - p * nl; }
+          const int l = base + (a0 + li) * sa + p * st;
+          so[u] = p * NLP + li;
+          v[u][1] = hc[l];
+          if (p >= 1 && p <= n) {
+            v[u][0] = tc[l];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) v[u][2 + q] = L.wk[q][l];
+          } else {
+#pragma unroll
+            for (int q = 0; q < 6; ++q) if (q != 1) v[u][q] = W(0);
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (so[u] >= 0) {
+          s_tc[so[u]] = v[u][0];
+          s_hc[so[u]] = v[u][1];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) s_r[q * fs + so[u]] = v[u][2 + q];
+        }
+      }
+    }
+  }
+  // semi-explicit boundary rows of each line
+  if (tid < NL) {
     T bw[4] = {0, 0, 0, 0}, be[4] = {0, 0, 0, 0};
-    if (act) {
+    if (tid < nl) {
+      const int a = a0 + tid;
+      const int lb = base + a * sa;
       if (DIR == 0) {
         if (blo) {
           const int S = L.jm * L.km, o = a + L.jm * b;
@@ -80,15 +140,19 @@ __global__ void __launch_bounds__(256) k_sweep3(Lv<T, W> L, Par P, int blo, int 
       }
     }
 #pragma unroll
-    for (int q = 0; q < 4; ++q) { sbw[lane][q] = W(bw[q]); sbe[lane][q] = W(be[q]); }
+    for (int q = 0; q < 4; ++q) { sbw[tid][q] = W(bw[q]); sbe[tid][q] = W(be[q]); }
   }
   __syncthreads();
 
-  const W* tc = L.tc[DIR];
-  const W* hc = L.hc[DIR];
-  W* r = L.wk[m];
-  W* sd = L.sd[m];
-  // row coefficients of system m: aw uses h of the west node, ae of the east
+  // ---- phase 1: two-ended elimination in shared memory
+  const int li = tid % NL, combo = tid / NL;
+  const int m = combo & 3, half = combo >> 2;
+  const bool act = li < nl;
+  W* __restrict__ r = s_r + m * fs;
+  W* __restrict__ sd = s_d + m * fs;
+  const W* __restrict__ ctc = s_tc;
+  const W* __restrict__ chc = s_hc;
+  auto at = [&](int p) { return p * NLP + li; };
   auto coef = [&](W t, W hw_, W he_, W& aw, W& ae) {
     const W dw = t != W(0) ? hw_ : W(0);
     const W de = t != W(0) ? he_ : W(0);
@@ -96,154 +160,104 @@ __global__ void __launch_bounds__(256) k_sweep3(Lv<T, W> L, Par P, int blo, int 
     else if (m == 2) { aw = -dw - t; ae = de - t; }
     else { aw = dw - t; ae = -de - t; }
   };
-  constexpr int R = 8;
-  int npiv = 0;
+  const int h = n / 2;  // rows 0..h-1 top (nodes 1..h), h..n-1 bottom (nodes h+1..n)
+  int npiv = 0, nzero = 0;
   if (act && half == 0) {
-    // ---- top half, top-down
-    const W bwm = sbw[lane][m];
-    W hw = hc[lb], hcur = hc[lb + st];
+    const W bwm = sbw[li][m];
+    W hw = chc[at(0)], hcur = chc[at(1)];
     W dprev = 0, duprev = 0, bprev = 0;
-    for (int p0 = 0; p0 < h; p0 += R) {
-      W bt[R], bh[R], br[R];
-#pragma unroll
-      for (int u = 0; u < R; ++u) {
-        const int p = p0 + u;
-        if (p < h) { const int l = lb + (p + 1) * st; bt[u] = tc[l]; bh[u] = hc[l + st]; br[u] = r[l]; }
+    for (int p = 1; p <= h; ++p) {
+      const W t = ctc[at(p)], hn = chc[at(p + 1)];
+      W aw, ae;
+      coef(t, hw, hn, aw, ae);
+      const W ap = W(1) + W(2) * t;
+      W rr = r[at(p)];
+      W d;
+      if (p == 1) { rr = rr - aw * bwm; d = ap; bprev = rr; }
+      else {
+        npiv += dabs(dprev) < dabs(aw);
+        const W f = aw / dprev;
+        d = ap - f * duprev;
+        bprev = rr - f * bprev;
       }
-#pragma unroll
-      for (int u = 0; u < R; ++u) {
-        const int p = p0 + u;
-        if (p < h) {
-          const int l = lb + (p + 1) * st;
-          W aw, ae;
-          coef(bt[u], hw, bh[u], aw, ae);
-          const W ap = W(1) + W(2) * bt[u];
-          W rr = br[u];
-          if (p == 0) rr = rr - aw * bwm;
-          W d;
-          if (p == 0) { d = ap; bprev = rr; }
-          else {
-            npiv += dabs(dprev) < dabs(aw);
-            const W f = aw / dprev;
-            d = ap - f * duprev;
-            bprev = rr - f * bprev;
-          }
-          sd[l] = d;
-          r[l] = bprev;
-          dprev = d; duprev = ae;
-          hw = hcur; hcur = bh[u];
-        }
-      }
+      nzero += d == W(0);
+      sd[at(p)] = d;
+      r[at(p)] = bprev;
+      dprev = d; duprev = ae;
+      hw = hcur; hcur = hn;
     }
-    mt_d[lane][m] = dprev; mt_u[lane][m] = duprev; mt_b[lane][m] = bprev;
+    mt_d[li][m] = dprev; mt_u[li][m] = duprev; mt_b[li][m] = bprev;
   } else if (act && half == 1) {
-    // ---- bottom half, bottom-up: eliminate the super-diagonal
-    const W bem = sbe[lane][m];
-    W he = hc[lb + (n + 1) * st];           // h of the node after the line
-    W hcur = hc[lb + n * st];               // h of row n-1's node
-    W dprev = 0, awprev = 0, bprev = 0;     // row p+1 after elimination, and its aw
-    for (int p0 = n - 1; p0 >= h; p0 -= R) {
-      W bt[R], bh[R], br[R];
-#pragma unroll
-      for (int u = 0; u < R; ++u) {
-        const int p = p0 - u;
-        if (p >= h) { const int l = lb + (p + 1) * st; bt[u] = tc[l]; bh[u] = hc[l - st]; br[u] = r[l]; }
+    const W bem = sbe[li][m];
+    W he = chc[at(n + 1)], hcur = chc[at(n)];
+    W dprev = 0, awprev = 0, bprev = 0;
+    for (int p = n; p > h; --p) {
+      const W t = ctc[at(p)], hwv = chc[at(p - 1)];
+      W aw, ae;
+      coef(t, hwv, he, aw, ae);
+      const W ap = W(1) + W(2) * t;
+      W rr = r[at(p)];
+      W d;
+      if (p == n) { rr = rr - ae * bem; d = ap; bprev = rr; }
+      else {
+        npiv += dabs(dprev) < dabs(ae);
+        const W f = ae / dprev;
+        d = ap - f * awprev;
+        bprev = rr - f * bprev;
       }
-#pragma unroll
-      for (int u = 0; u < R; ++u) {
-        const int p = p0 - u;
-        if (p >= h) {
-          const int l = lb + (p + 1) * st;
-          W aw, ae;
-          coef(bt[u], bh[u], he, aw, ae);
-          const W ap = W(1) + W(2) * bt[u];
-          W rr = br[u];
-          if (p == n - 1) rr = rr - ae * bem;
-          W d;
-          if (p == n - 1) { d = ap; bprev = rr; }
-          else {
-            npiv += dabs(dprev) < dabs(ae);
-            const W f = ae / dprev;
-            d = ap - f * awprev;
-            bprev = rr - f * bprev;
-          }
-          sd[l] = d;
-          r[l] = bprev;
-          dprev = d; awprev = aw;
-          he = hcur; hcur = bh[u];
-        }
-      }
+      nzero += d == W(0);
+      sd[at(p)] = d;
+      r[at(p)] = bprev;
+      dprev = d; awprev = aw;
+      he = hcur; hcur = hwv;
     }
-    mb_d[lane][m] = dprev; mb_l[lane][m] = awprev; mb_b[lane][m] = bprev;
+    mb_d[li][m] = dprev; mb_l[li][m] = awprev; mb_b[li][m] = bprev;
   }
   if (npiv) atomicAdd(&L.flags[0], npiv);
   __syncthreads();
   if (act) {
-    // ---- the two middle rows: d1 x1 + u1 x2 = b1 (row h-1), l2 x1 + d2 x2 = b2 (row h)
-    const W d1 = mt_d[lane][m], u1 = mt_u[lane][m], b1 = mt_b[lane][m];
-    const W d2 = mb_d[lane][m], l2 = mb_l[lane][m], b2 = mb_b[lane][m];
+    // the two middle rows: d1 x1 + u1 x2 = b1 (row h-1), l2 x1 + d2 x2 = b2 (row h)
+    const W d1 = mt_d[li][m], u1 = mt_u[li][m], b1 = mt_b[li][m];
+    const W d2 = mb_d[li][m], l2 = mb_l[li][m], b2 = mb_b[li][m];
     const W det = d1 * d2 - u1 * l2;
-    const W x1 = (b1 * d2 - u1 * b2) / det;
-    const W x2 = (d1 * b2 - l2 * b1) / det;
+    nzero += half == 0 && det == W(0);
+    if (nzero) atomicAdd(&L.flags[1], nzero);
     if (half == 0) {
-      W x = x1;
-      r[lb + h * st] = x1;
-      for (int p1 = h - 2; p1 >= 0; p1 -= R) {
-        W bb[R], bd[R], bt[R], bh[R];
-#pragma unroll
-        for (int u = 0; u < R; ++u) {
-          const int p = p1 - u;
-          if (p >= 0) { const int l = lb + (p + 1) * st; bb[u] = r[l]; bd[u] = sd[l]; bt[u] = tc[l]; bh[u] = hc[l + st]; }
-        }
-#pragma unroll
-        for (int u = 0; u < R; ++u) {
-          const int p = p1 - u;
-          if (p >= 0) {
-            W aw, ae;
-            coef(bt[u], W(0), bh[u], aw, ae);
-            x = (bb[u] - ae * x) / bd[u];
-            r[lb + (p + 1) * st] = x;
-          }
-        }
+      W x = (b1 * d2 - u1 * b2) / det;
+      r[at(h)] = x;
+      for (int p = h - 1; p >= 1; --p) {
+        W aw, ae;
+        coef(ctc[at(p)], W(0), chc[at(p + 1)], aw, ae);
+        x = (r[at(p)] - ae * x) / sd[at(p)];
+        r[at(p)] = x;
       }
     } else {
-      W x = x2;
-      r[lb + (h + 1) * st] = x2;
-      for (int p0 = h + 1; p0 < n; p0 += R) {
-        W bb[R], bd[R], bt[R], bh[R];
-#pragma unroll
-        for (int u = 0; u < R; ++u) {
-          const int p = p0 + u;
-          if (p < n) { const int l = lb + (p + 1) * st; bb[u] = r[l]; bd[u] = sd[l]; bt[u] = tc[l]; bh[u] = hc[l - st]; }
-        }
-#pragma unroll
-        for (int u = 0; u < R; ++u) {
-          const int p = p0 + u;
-          if (p < n) {
-            W aw, ae;
-            coef(bt[u], bh[u], W(0), aw, ae);
-            x = (bb[u] - aw * x) / bd[u];
-            r[lb + (p + 1) * st] = x;
-          }
-        }
+      W x = (d1 * b2 - l2 * b1) / det;
+      r[at(h + 1)] = x;
+      for (int p = h + 2; p <= n; ++p) {
+        W aw, ae;
+        coef(ctc[at(p)], chc[at(p - 1)], W(0), aw, ae);
+        x = (r[at(p)] - aw * x) / sd[at(p)];
+        r[at(p)] = x;
       }
     }
   }
   __syncthreads();
 
-  // ---- phase 2: per-node transform of the CTA's lines, in the sweep
-  // precision W (FP64 in FP64 mode, FP32 in MIXED mode)
-  const int nl = min(32, amax - a0 + 1);
+  // ---- phase 2: per-node transform in the sweep precision W
   const int total = nl * n;
-  for (int t = threadIdx.x; t < total; t += blockDim.x) {
-    int li, p;
-    if (DIR == 0) { li = t / n; p = t - li * n; }
-    else { p = t / nl; li = t - p * nl; }
-    const int aa = a0 + li;
+  for (int t = tid; t < total; t += NT) {
+    int lq, p;
+    if (DIR == 0) { lq = t / n; p = t - lq * n; }
+    else { p = t / nl; lq = t - p * nl; }
+    const int aa = a0 + lq;
     const int l = base + aa * sa + (p + 1) * st;
+    const int so = (p + 1) * NLP + lq;
     W xv[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) xv[q] = L.wk[q][l];
+    for (int q = 0; q < 4; ++q) xv[q] = s_r[q * fs + so];
+    const W sg = L.sig[l];
+    W y[4], z[4];
     if (DIR == 0) {
       const int S = L.im * L.km, o = (p + 1) + L.im * b;
       const int tgt[4] = {1, 2, L.jm - 2, L.jm - 3};
@@ -252,12 +266,11 @@ __global__ void __launch_bounds__(256) k_sweep3(Lv<T, W> L, Par P, int blo, int 
         if (aa == tgt[s])
 #pragma unroll
           for (int q = 0; q < 4; ++q) L.bj[(s * 4 + q) * S + o] = xv[q];
-      M4<W> A;
-      mat_n1i_c<W>(L, P, l, A);
-      W y[4];
-      mv4(A, xv, y);
+      // N1^-1 x = Mb^-1 (Ma x)
+      mfwd_apply<W>(W(L.csi[0][l]), W(L.csi[1][l]), W(L.csi[2][l]), sg, xv, y);
+      minv_apply<W>(W(L.eta[0][l]), W(L.eta[1][l]), W(L.eta[2][l]), sg, y, z);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) L.wk[q][l] = y[q];
+      for (int q = 0; q < 4; ++q) L.wk[q][l] = z[q];
     } else if (DIR == 1) {
       const int S = L.im * L.jm, o = aa + L.im * (p + 1);
       const int tgt[4] = {1, 2, L.km - 2, L.km - 3};
@@ -266,17 +279,13 @@ __global__ void __launch_bounds__(256) k_sweep3(Lv<T, W> L, Par P, int blo, int 
         if (b == tgt[s])
 #pragma unroll
           for (int q = 0; q < 4; ++q) L.bk[(s * 4 + q) * S + o] = xv[q];
-      M4<W> A;
-      mat_n2i_c<W>(L, P, l, A);
-      W y[4];
-      mv4(A, xv, y);
+      // N2^-1 x = Mc^-1 (Mb x)
+      mfwd_apply<W>(W(L.eta[0][l]), W(L.eta[1][l]), W(L.eta[2][l]), sg, xv, y);
+      minv_apply<W>(W(L.zet[0][l]), W(L.zet[1][l]), W(L.zet[2][l]), sg, y, z);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) L.wk[q][l] = y[q];
+      for (int q = 0; q < 4; ++q) L.wk[q][l] = z[q];
     } else {
-      M4<W> A;
-      mat_mc_c<W>(L, P, l, A);
-      W y[4];
-      mv4(A, xv, y);
+      mfwd_apply<W>(W(L.zet[0][l]), W(L.zet[1][l]), W(L.zet[2][l]), sg, xv, y);
 #pragma unroll
       for (int q = 0; q < 4; ++q) L.q[q][l] = L.q[q][l] + T(y[q]);
     }
