@@ -44,16 +44,16 @@ UNIT = "s/step"
 def alg_bytes(kind, T, W, coarse):
     pk = 4 * T if coarse else 0
     return {
-        "resid": 23 * T + 10 * W + pk,    # q4 qn3 qnm1-3 metrics9 aj nut dtau | wk4 diss1 tc3 hc3
-        "recalc": 26 * T + pk,            # q4 qn3 qnm1-3 metrics9 aj nut diss1 | rh4
-        "sweep_i": 10 * W + 7 * T,        # wk4 in/out, tc, hc, dtau, csi3, eta3
-        "sweep_j": 10 * W + 7 * T,        # wk4 in/out, tc, hc, dtau, eta3, zet3
-        "sweep_k": 6 * W + 12 * T,        # wk4, tc, hc, dtau, zet3, q4 in/out
+        "resid": 24 * T + 11 * W + pk,    # q4 qn3 qnm1-3 metrics9 aj 1/aj nut dtau | wk4 sigma tc3 hc3, diss1
+        "recalc": 26 * T + pk,            # q4 qn3 qnm1-3 metrics9 aj 1/aj nut diss1 | rh4
+        "sweep_i": 11 * W + 6 * T,        # wk4 in/out, tc, hc, sigma, csi3, eta3
+        "sweep_j": 11 * W + 6 * T,        # wk4 in/out, tc, hc, sigma, eta3, zet3
+        "sweep_k": 7 * W + 11 * T,        # wk4, tc, hc, sigma, zet3, q4 in/out
         "dtau": 11 * T,                   # metrics9 nut | dtau
         "norm": 15 * T,                   # q5 qold5 | qold5
         "rsmooth": 8 * T,                 # dq4 in/out (last one: q4 in/out instead)
         "prolong": 4 * T,                 # dq4 out (coarse reads amortised)
-        "sa_rhs": 19 * 8 + 10 * W,        # q2..5, qn5 qnm1-5, metrics9, aj, wd, wo, dtev | rh, ADI rows 9
+        "sa_rhs": 22 * 8 + 10 * W,        # q5 qn5 qnm1-5, U/J 3, metrics9, aj, 1/aj, wd, wo, dtev | rh, ADI rows 9
         "sa_sweep": 5 * W + 8,            # ADI row 3, rh in/out; k sweep: q5 in/out, dtev (1/3 each)
     }.get(kind)
 
@@ -256,7 +256,7 @@ def run_ours(args, rank, world, dist):
         "data": "synthetic (seeded numpy generator; the reference ships no grids or solutions)",
         "impl": "ours",
         "config": {"workload": desc, "case": args.case, "grid": [case.im, case.jm, case.km],
-                   "interior_nodes": nint, "precision": "mixed (FP64 residual/update, FP32 sweeps + coarse levels)",
+                   "interior_nodes": nint, "precision": "mixed (FP64 state, residual, restriction, update and norm on every level; FP32 line-sweep work, modal transforms and SA ADI)",
                    "predictor": "linear extrapolation", "learned_predictor": "not built",
                    "pseudo_iterations_per_step": iters, "converged": conv,
                    "l2": "working set of every level > 126 MB L2 for the channel; no flush between steps",
@@ -349,7 +349,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--case", default="cavity", choices=["cavity", "channel"])
+    ap.add_argument("--case", default="channel", choices=["cavity", "channel"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ncu-workload", action="store_true",

@@ -38,6 +38,7 @@ struct Lv {
   const T* eta[3];
   const T* zet[3];
   const T* aj;
+  const T* rj;      // 1/aj, formed once whenever aj is set
   // DAF work: transformed residual and row coefficients
   W* wk[4];
   W* sig;          // sigma = sqrt(beta alpha) of each interior node, from the first residual pass
@@ -62,6 +63,17 @@ struct Par {
 };
 
 template <class T> DESALM_DEV T dabs(T x) { return x < T(0) ? -x : x; }
+
+// Asynchronous global -> shared copy of one 4- or 8-byte element
+// (cp.async, cached in L1); completion by cp_async_wait_all().
+template <class E>
+DESALM_DEV void cp_async_elem(E* smem, const E* gmem) {
+  static_assert(sizeof(E) == 4 || sizeof(E) == 8, "cp.async element size");
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  if (sizeof(E) == 4) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+DESALM_DEV void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 template <class T> DESALM_DEV T dmin(T a, T b) { return a < b ? a : b; }
 template <class T> DESALM_DEV T dmax(T a, T b) { return a > b ? a : b; }
 

@@ -205,6 +205,7 @@ int alloc_level(desalm_ctx* ctx, Level& G, Lv<T, W>& L) {
     RET(A((T**)&L.csi[d])); RET(A((T**)&L.eta[d])); RET(A((T**)&L.zet[d]));
   }
   RET(A((T**)&L.aj));
+  RET(A((T**)&L.rj));
   for (int m = 0; m < 4; ++m) RET(AW(&L.wk[m]));
   RET(AW(&L.sig));
   for (int m = 0; m < 3; ++m) { RET(AW(&L.tc[m])); RET(AW(&L.hc[m])); }
@@ -301,8 +302,9 @@ int sweep4_nl(desalm_ctx* ctx, Lv<T, W>& L, const Par& P, int lvl, int blo, int 
   return 0;
 }
 
-// Shared-memory opt-in of every slab-sweep instantiation on the current
-// device (done when a context is created, outside any stream capture).
+// Shared-memory opt-in of every slab-sweep and SA slab-sweep instantiation
+// on the current device (done when a context is created, outside any stream
+// capture).
 template <class T, class W>
 cudaError_t slab_attrs() {
   int dev = 0, optin = 0;
@@ -318,6 +320,9 @@ cudaError_t slab_attrs() {
   set((const void*)k_sweep4<T, W, 0, 16>); set((const void*)k_sweep4<T, W, 0, 8>); set((const void*)k_sweep4<T, W, 0, 4>);
   set((const void*)k_sweep4<T, W, 1, 16>); set((const void*)k_sweep4<T, W, 1, 8>); set((const void*)k_sweep4<T, W, 1, 4>);
   set((const void*)k_sweep4<T, W, 2, 16>); set((const void*)k_sweep4<T, W, 2, 8>); set((const void*)k_sweep4<T, W, 2, 4>);
+  set((const void*)k_sa_sweep4<W, 0, 32>); set((const void*)k_sa_sweep4<W, 0, 16>); set((const void*)k_sa_sweep4<W, 0, 8>);
+  set((const void*)k_sa_sweep4<W, 1, 32>); set((const void*)k_sa_sweep4<W, 1, 16>); set((const void*)k_sa_sweep4<W, 1, 8>);
+  set((const void*)k_sa_sweep4<W, 2, 32>); set((const void*)k_sa_sweep4<W, 2, 16>); set((const void*)k_sa_sweep4<W, 2, 8>);
   return e;
 }
 
@@ -494,6 +499,16 @@ int do_norm(desalm_ctx* ctx, int n, int copy, double* out) {
     case K_DD: return launch_norm(ctx, G.dd, copy, out);
     default: return launch_norm(ctx, G.df, copy, out);
   }
+}
+
+// 1/aj of level n, after aj has been set
+int refresh_rj(desalm_ctx* ctx, int n) {
+  Level& G = ctx->L[n];
+  cudaStream_t s = ctx->stream;
+  if (kind_of(ctx, n) == K_DD) k_recip<double><<<cdiv(G.N, 256), 256, 0, s>>>((double*)G.dd.rj, G.dd.aj, G.N);
+  else k_recip<double><<<cdiv(G.N, 256), 256, 0, s>>>((double*)G.df.rj, G.df.aj, G.N);
+  CKL();
+  return 0;
 }
 
 // pointer to one SoA field of a level and its element size
@@ -762,6 +777,7 @@ int desalm_set_grid(desalm_ctx* ctx, const double* x, const double* y, const dou
       else k_copy<float, double><<<cdiv(G.N, 256), 256, 0, s>>>((float*)dst[t], src, G.N);
     }
     CKL();
+    RET(refresh_rj(ctx, n));
     if (n == 0)
       k_dtev<<<cdiv(G.N, 256), 256, 0, s>>>(dcov, ctx->dtev, G.N, c.cfl2, c.vnn2, c.ren, c.delti, c.unsteady);
     CKL();
@@ -904,6 +920,7 @@ int desalm_set_field(desalm_ctx* ctx, int n, int f, const double* in) {
     cudaStreamSynchronize(s);
     cudaFree(d);
   }
+  if (f == DESALM_F_AJ) RET(refresh_rj(ctx, n - 1));
   CK(cudaStreamSynchronize(s));
   if (f == DESALM_F_NUT || (f >= DESALM_F_CSI && f <= DESALM_F_AJ)) ctx->L[n - 1].dtau_valid = false;
   return 0;
@@ -1169,14 +1186,35 @@ SaT<SW> make_sa(desalm_ctx* ctx, Lv<double, W>& L) {
   for (int m = 0; m < 5; ++m) S.q[m] = L.q[m];
   S.qn5 = L.qn[4]; S.qnm1_5 = L.qnm1[4];
   for (int d = 0; d < 3; ++d) { S.csi[d] = L.csi[d]; S.eta[d] = L.eta[d]; S.zet[d] = L.zet[d]; }
-  S.aj = L.aj; S.wd = ctx->wd; S.dtev = ctx->dtev; S.nut = L.nut;
+  S.aj = L.aj; S.rj = L.rj; S.wd = ctx->wd; S.dtev = ctx->dtev; S.nut = L.nut;
   S.wo = ctx->sa.a[0];
-  S.rh = (SW*)ctx->sa.a[1]; S.sd = (SW*)ctx->sa.a[2];
-  for (int t = 0; t < 9; ++t) S.co[t] = (SW*)ctx->sa.a[3 + t];
+  S.rh = (SW*)ctx->sa.a[1];
+  for (int t = 0; t < 9; ++t) S.co[t] = (SW*)ctx->sa.a[2 + t];
+  for (int d = 0; d < 3; ++d) S.uc[d] = ctx->sa.a[11 + d];
   S.flags = ctx->flags;
   S.ren = ctx->c.ren; S.delti = ctx->c.delti; S.es = ctx->c.unsteady ? 1.0 : 0.0;
   for (int b = 0; b < 6; ++b) { S.sa1[b] = ctx->par.sa[0][b]; S.sb1[b] = ctx->par.sb[0][b]; S.btype[b] = ctx->c.btype[b]; }
   return S;
+}
+
+// One SA ADI sweep as k_sa_sweep4 with the widest slab whose shared memory
+// leaves room for two CTAs per SM (amax lines of n nodes in each of nb planes).
+template <class SW>
+size_t sa_slab_bytes(int n, int nl) { return (size_t)4 * slab_fs(n, nl + 1) * sizeof(SW); }
+template <class SW, int DIR, int NL>
+int sa_sweep_nl(desalm_ctx* ctx, SaT<SW>& S, int amax, int n, int nb, double nin) {
+  cudaStream_t s = ctx->stream;
+  LAUNCH(KC_SA_SWEEP, 0, nin, k_sa_sweep4<SW, DIR, NL><<<dim3(cdiv(amax, NL), nb), 2 * NL, sa_slab_bytes<SW>(n, NL), s>>>(S));
+  CKL();
+  return 0;
+}
+template <class SW, int DIR>
+int sa_sweep(desalm_ctx* ctx, SaT<SW>& S, int amax, int n, int nb, double nin) {
+  if (sa_slab_bytes<SW>(n, 32) <= kSlabTwoPerSm) return sa_sweep_nl<SW, DIR, 32>(ctx, S, amax, n, nb, nin);
+  if (sa_slab_bytes<SW>(n, 16) <= kSlabTwoPerSm) return sa_sweep_nl<SW, DIR, 16>(ctx, S, amax, n, nb, nin);
+  if (sa_slab_bytes<SW>(n, 8) <= kSlabMax) return sa_sweep_nl<SW, DIR, 8>(ctx, S, amax, n, nb, nin);
+  ctx->err = "grid line too long for the shared-memory SA sweep";
+  return DESALM_EINVAL;
 }
 
 template <class W>
@@ -1186,11 +1224,12 @@ int sa_run(desalm_ctx* ctx, Lv<double, W>& L) {
   const double nin = double(L.im - 2) * (L.jm - 2) * (L.km - 2);
   const dim3 gi(cdiv(L.im - 2, 32), cdiv(L.jm - 2, 4), L.km - 2);
   LAUNCH(KC_SA_RHS, 0, nin, k_sa_source<W><<<gi, blk3(), 0, s>>>(S));
+  LAUNCH(KC_SA_RHS, 0, L.N, k_sa_ucn<W><<<cdiv(L.N, 256), 256, 0, s>>>(S));
   for (int it = 0; it < ctx->c.itk; ++it) {
     LAUNCH(KC_SA_RHS, 0, nin, k_sa_rhs<W><<<gi, blk3(), 0, s>>>(S));
-    LAUNCH(KC_SA_SWEEP, 0, nin, k_sa_sweep3<W, 0><<<dim3(cdiv(L.jm - 2, 64), L.km - 2), 128, 0, s>>>(S));
-    LAUNCH(KC_SA_SWEEP, 0, nin, k_sa_sweep3<W, 1><<<dim3(cdiv(L.im - 2, 64), L.km - 2), 128, 0, s>>>(S));
-    LAUNCH(KC_SA_SWEEP, 0, nin, k_sa_sweep3<W, 2><<<dim3(cdiv(L.im - 2, 64), L.jm - 2), 128, 0, s>>>(S));
+    RET((sa_sweep<W, 0>(ctx, S, L.jm - 2, L.im - 2, L.km - 2, nin)));
+    RET((sa_sweep<W, 1>(ctx, S, L.im - 2, L.jm - 2, L.km - 2, nin)));
+    RET((sa_sweep<W, 2>(ctx, S, L.im - 2, L.km - 2, L.jm - 2, nin)));
     LAUNCH(KC_SA_BC, 0, 2.0 * L.jm * L.km, k_sa_bc<W, 0><<<dim3(cdiv(L.jm, 64), L.km), 64, 0, s>>>(S));
     LAUNCH(KC_SA_BC, 0, 2.0 * L.im * L.km, k_sa_bc<W, 1><<<dim3(cdiv(L.im, 64), L.km), 64, 0, s>>>(S));
     LAUNCH(KC_SA_BC, 0, 2.0 * L.im * L.jm, k_sa_bc<W, 2><<<dim3(cdiv(L.im, 64), L.jm), 64, 0, s>>>(S));

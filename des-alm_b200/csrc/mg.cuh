@@ -263,6 +263,13 @@ __global__ void k_inject(TC* c, const TF* f, int cim, int cjm, int ckm, int fim,
   c[i + cim * (j + cjm * k)] = TC(f[ii + fim * (jj + fjm * kk)]);
 }
 
+// r = 1 / a element-wise (the reciprocal Jacobian of a level)
+template <class T>
+__global__ void k_recip(T* r, const T* a, long n) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) r[t] = T(1) / a[t];
+}
+
 // Covariant metrics, Jacobian and contravariant metrics of one level
 // (src/mg_metrics.F90:56-250).  cov[9] = xc, xe, xz, yc, ye, yz, zc, ze, zz.
 __global__ void k_metrics(const double* x, const double* y, const double* z, int im, int jm, int km,

@@ -12,6 +12,9 @@
 // src/solver_daf.F90:432-477) or applies r = S (-dtau J rh) and r <- Ma^-1 r
 // (src/rhs_diag_solver.F90:53-122) and stores the transformed residual for
 // the line sweeps, with sigma and the row coefficients of every direction.
+// Divisions by J are multiplications by the stored 1/J, and the BDF2 and
+// alpha denominators are inverted once per node; the results equal the
+// reference's expressions up to rounding.
 #pragma once
 #include "modal.cuh"
 
@@ -21,7 +24,7 @@ namespace desalm {
 template <class T, class W>
 DESALM_DEV T ucn(const Lv<T, W>& L, int d, int l) {
   const T* const* m = d == 0 ? L.csi : (d == 1 ? L.eta : L.zet);
-  T tmp = T(1) / L.aj[l];
+  T tmp = L.rj[l];
   return tmp * (m[0][l] * L.q[1][l] + m[1][l] * L.q[2][l] + m[2][l] * L.q[3][l]);
 }
 
@@ -91,7 +94,7 @@ template <class T, class W>
 DESALM_DEV T diss_fv(const Lv<T, W>& L, int dir, int l, int st, T dsq) {
   const T* const* m = dir == 0 ? L.csi : (dir == 1 ? L.eta : L.zet);
   T g = m[0][l] * m[0][l] + m[1][l] * m[1][l] + m[2][l] * m[2][l];
-  T tmp1 = g * L.dtau[l] / L.aj[l];
+  T tmp1 = g * L.dtau[l] * L.rj[l];
   const T* p = L.q[0];
   T tmp2 = dsq * (p[l + st] - T(2) * p[l] + p[l - st]);
   return tmp1 * tmp2;
@@ -164,8 +167,8 @@ __global__ void __launch_bounds__(128, DESALM_KR_MINBLOCKS) k_resid(Lv<T, W> L, 
     T pp[3], pm[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      pp[d] = p[l + st[d]] / L.aj[l + st[d]];
-      pm[d] = p[l - st[d]] / L.aj[l - st[d]];
+      pp[d] = p[l + st[d]] * L.rj[l + st[d]];
+      pm[d] = p[l - st[d]] * L.rj[l - st[d]];
     }
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
@@ -204,11 +207,11 @@ __global__ void __launch_bounds__(128, DESALM_KR_MINBLOCKS) k_resid(Lv<T, W> L, 
 
   // ---- unsteady terms, viscous and dissipation
   {
-    T dtaj = T(2) * T(P.delti) * L.aj[l];
+    const T rdtaj = T(1) / (T(2) * T(P.delti) * L.aj[l]);
     rh[0] = rh[0] + diss1;
 #pragma unroll
     for (int m = 1; m < 4; ++m) {
-      T dq = T(P.es) * (T(3) * L.q[m][l] - T(4) * L.qn[m][l] + L.qnm1[m][l]) / dtaj;
+      T dq = T(P.es) * (T(3) * L.q[m][l] - T(4) * L.qn[m][l] + L.qnm1[m][l]) * rdtaj;
       rh[m] = rh[m] + T(0) + dq - visc[m - 1];
     }
   }
@@ -235,13 +238,14 @@ __global__ void __launch_bounds__(128, DESALM_KR_MINBLOCKS) k_resid(Lv<T, W> L, 
 
   // ---- r = S (-dtau rh J), then Ma^-1 r
   const T dtau = L.dtau[l];
-  T alpha = T(1) + (T(P.es) * T(1.5) / T(P.delti)) * dtau;
-  T s[4] = {T(P.beta), T(1) / alpha, T(1) / alpha, T(1) / alpha};
+  // sigma and theta of src/rhs_modal_matrices.F90:82-84 with one division
+  const T alpha = T(1) + (T(P.es) * T(1.5) / T(P.delti)) * dtau;
+  const T ra = T(1) / alpha;
+  const T sg = sqrt(T(P.beta) * alpha), th = sqrt(T(P.beta) * ra);
+  T s[4] = {T(P.beta), ra, ra, ra};
   T r[4];
 #pragma unroll
   for (int m = 0; m < 4; ++m) r[m] = s[m] * (-dtau * rh[m] * L.aj[l]);
-  T sg, th;
-  sigma_theta(dtau, P, sg, th);
   W rp[4];
   {
     // Ma^-1 in the sweep precision W (the preconditioner's precision)

@@ -1,16 +1,18 @@
 // sa.cuh -- Spalart-Allmaras sub-iterations on the fine level (des_eddy,
 // src/des_eddy.F90:109-297) and the outlet mass-flux fix (conservation,
-// src/conservation.F90:64-160).  The fine level is FP64 in every precision
-// mode, so these kernels are FP64 only.
+// src/conservation.F90:64-160).  nu_tilde, nu_t and the residual terms are
+// FP64 in every precision mode; the ADI rows and line solves run in the
+// sweep precision SW (FP32 in MIXED mode).
 #pragma once
 #include "common.cuh"
+#include "sweep.cuh"
 
 namespace desalm {
 
 // fine-level FP64 work arrays of the SA model
 struct SaWork {
-  static const int NARR = 12;
-  double* a[NARR];  // wo, rh5, sd, then the ADI coefficients aw, ap, ae of the i, j, k lines
+  static const int NARR = 14;
+  double* a[NARR];  // wo, rh5, the ADI coefficients aw, ap, ae of the i, j, k lines, U/J V/J W/J
 };
 
 // SW: type of the ADI work arrays and arithmetic (double in FP64 mode,
@@ -26,13 +28,14 @@ struct SaT {
   const double* eta[3];
   const double* zet[3];
   const double* aj;
+  const double* rj;  // 1/aj
   const double* wd;
   const double* dtev;
   double* nut;
   double* wo;
   SW* rh;
-  SW* sd;
-  SW* co[9];  // co[3 d + 0..2] = aw, ap, ae of the direction-d line through each interior node
+  SW* co[9];
+  double* uc[3];  // contravariant U/J of each direction on every node, for the current velocities  // co[3 d + 0..2] = aw, ap, ae of the direction-d line through each interior node
   int* flags;
   double ren, delti, es;
   double sa1[6], sb1[6];  // pressure-row extrapolation coefficients, sa(1,b), sb(1,b)
@@ -44,8 +47,19 @@ using Sa = SaT<double>;
 template <class SW>
 DESALM_DEV double sa_ucn(const SaT<SW>& S, int d, int l) {
   const double* const* m = d == 0 ? S.csi : (d == 1 ? S.eta : S.zet);
-  double tmp = 1.0 / S.aj[l];
+  double tmp = S.rj[l];
   return tmp * (m[0][l] * S.q[1][l] + m[1][l] * S.q[2][l] + m[2][l] * S.q[3][l]);
+}
+
+// U/J of the three directions on every node (src/rhs_contra_j.F90:14-29), once
+// per pseudo-iteration: the velocities do not change during the SA
+// sub-iterations.
+template <class SW>
+__global__ void k_sa_ucn(SaT<SW> S) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= S.N) return;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) S.uc[d][l] = sa_ucn(S, d, l);
 }
 
 // vorticity magnitude wo = 2 |W|^2 on interior nodes (src/rhs_sa_source.F90:44-93)
@@ -78,7 +92,7 @@ __global__ void k_sa_source(SaT<SW> S) {
 // viscous flux of nu_tilde through the face l0 -> l0 + st[dir]
 // (src/rhs_sa_viscous.F90:58-175)
 template <class SW>
-DESALM_DEV double sa_visc_face(const SaT<SW>& S, int dir, int l0, double rei, double sig) {
+DESALM_DEV double sa_visc_face(const SaT<SW>& S, int dir, int l0, double rei, double rsig) {
   const int sj = S.sj, sk = S.sk;
   const double* v = S.q[4];
   int l1;
@@ -106,7 +120,7 @@ DESALM_DEV double sa_visc_face(const SaT<SW>& S, int dir, int l0, double rei, do
   if (dir == 0) { k1 = a1 * a1 + a2 * a2 + a3 * a3; k2 = a1 * b1 + a2 * b2 + a3 * b3; k3 = a1 * c1 + a2 * c2 + a3 * c3; }
   else if (dir == 1) { k1 = b1 * a1 + b2 * a2 + b3 * a3; k2 = b1 * b1 + b2 * b2 + b3 * b3; k3 = b1 * c1 + b2 * c2 + b3 * c3; }
   else { k1 = c1 * a1 + c2 * a2 + c3 * a3; k2 = c1 * b1 + c2 * b2 + c3 * b3; k3 = c1 * c1 + c2 * c2 + c3 * c3; }
-  double vtj = 0.25 * ((rei + v[l1]) / sig + (rei + v[l0]) / sig) / (S.aj[l1] + S.aj[l0]);
+  double vtj = 0.25 * ((rei + v[l1]) * rsig + (rei + v[l0]) * rsig) / (S.aj[l1] + S.aj[l0]);
   return vtj * (k1 * vcs + k2 * vet + k3 * vze);
 }
 
@@ -115,7 +129,7 @@ DESALM_DEV double sa_visc_face(const SaT<SW>& S, int dir, int l0, double rei, do
 template <class SW>
 DESALM_DEV double sa_conv_face(const SaT<SW>& S, int dir, int l0, int st) {
   const int l1 = l0 + st;
-  const double u1 = sa_ucn(S, dir, l1), u0 = sa_ucn(S, dir, l0);
+  const double u1 = S.uc[dir][l1], u0 = S.uc[dir][l0];
   const double* v = S.q[4];
   double eigh = 0.5 * fabs(u1 + u0);
   return 0.5 * (v[l1] * u1 + v[l0] * u0 - eigh * (v[l1] - v[l0]));
@@ -131,21 +145,20 @@ template <class SW, int DIR>
 DESALM_DEV void sa_adi_row(const SaT<SW>& S, int l) {
   const int st = DIR == 0 ? 1 : (DIR == 1 ? S.sj : S.sk);
   const double* const* mt = DIR == 0 ? S.csi : (DIR == 1 ? S.eta : S.zet);
-  const SW sig = SW(2.0 / 3.0), rei = SW(1.0 / S.ren), half_ = SW(0.5);
+  const SW rsig = SW(1.5), rei = SW(1.0 / S.ren), half_ = SW(0.5);  // rsig = 1 / sigma_SA
   SW m0[3], m1[3], m2[3], nu[3], aj[3], u[3];
 #pragma unroll
   for (int t = 0; t < 3; ++t) {
     const int n = l + (t - 1) * st;
     m0[t] = SW(mt[0][n]); m1[t] = SW(mt[1][n]); m2[t] = SW(mt[2][n]);
     nu[t] = SW(S.q[4][n]); aj[t] = SW(S.aj[n]);
-    const SW tmp = SW(1) / aj[t];
-    u[t] = tmp * (m0[t] * SW(S.q[1][n]) + m1[t] * SW(S.q[2][n]) + m2[t] * SW(S.q[3][n]));
+    u[t] = SW(S.uc[DIR][n]);
   }
   SW av[2];
 #pragma unroll
   for (int f = 0; f < 2; ++f) {  // faces (l - st, l) and (l, l + st)
     const SW gx = m0[f + 1] + m0[f], gy = m1[f + 1] + m1[f], gz = m2[f + 1] + m2[f];
-    const SW ev = (rei + half_ * (nu[f + 1] + nu[f])) / sig;
+    const SW ev = (rei + half_ * (nu[f + 1] + nu[f])) * rsig;
     const SW ucna = half_ * dabs(u[f + 1] + u[f]);
     av[f] = ucna + ev * (gx * gx + gy * gy + gz * gz) / (aj[f + 1] + aj[f]);
   }
@@ -158,7 +171,9 @@ DESALM_DEV void sa_adi_row(const SaT<SW>& S, int l) {
 // One fused pass of rhs_sa_grdnu, rhs_sa_prod, rhs_sa_viscous, rhs_sa_flux,
 // rhs_sa_unst_visc and rhs_sa_implicit_source on interior nodes
 // (src/des_eddy.F90:164-223), plus the ADI rows; boundary values of rh stay
-// zero.
+// zero.  Divisions by J and by sigma_SA are multiplications by 1/J and 1.5,
+// U/J comes from k_sa_ucn, and f_w's sixth root is cbrt(sqrt(x)); the results
+// equal the reference's expressions up to rounding.
 template <class SW>
 __global__ void __launch_bounds__(128) k_sa_rhs(SaT<SW> S) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -167,7 +182,7 @@ __global__ void __launch_bounds__(128) k_sa_rhs(SaT<SW> S) {
   if (i > S.im - 2 || j > S.jm - 2) return;
   const int sj = S.sj, sk = S.sk;
   const int l = i + sj * j + sk * k;
-  const double cb1 = 0.1355, cb2 = 0.622, sig = 2.0 / 3.0, capa = 0.41;
+  const double cb1 = 0.1355, cb2 = 0.622, rsig = 1.5, capa = 0.41;  // rsig = 1 / sigma_SA
   const double cw1 = 3.23906782, cw2 = 0.3, cw3h = 64.0, cv1c = 357.911, cv2 = 5.0;
   const double rei = 1.0 / S.ren;
   const double* q5 = S.q[4];
@@ -179,8 +194,8 @@ __global__ void __launch_bounds__(128) k_sa_rhs(SaT<SW> S) {
     double qp[3], qm[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      qp[d] = q5[l + st[d]] / S.aj[l + st[d]];
-      qm[d] = q5[l - st[d]] / S.aj[l - st[d]];
+      qp[d] = q5[l + st[d]] * S.rj[l + st[d]];
+      qm[d] = q5[l - st[d]] * S.rj[l - st[d]];
     }
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
@@ -199,7 +214,7 @@ __global__ void __launch_bounds__(128) k_sa_rhs(SaT<SW> S) {
     psa = 0.0;
   } else {
     double nt = q5[l];
-    double chi = nt / rei;
+    double chi = nt * S.ren;
     double chic = chi * chi * chi;
     double fv1 = chic / (chic + cv1c);
     double t = 1.0 + chi / cv2;
@@ -215,24 +230,24 @@ __global__ void __launch_bounds__(128) k_sa_rhs(SaT<SW> S) {
     double grr = rr + cw2 * (rr6 - rr);
     grr = grr > 0.0 ? grr : 0.0;
     double grr6 = grr * grr * grr * grr * grr * grr;
-    double fw = grr * pow((1.0 + cw3h) / (grr6 + cw3h), 1.0 / 6.0);
+    double fw = grr * cbrt(sqrt((1.0 + cw3h) / (grr6 + cw3h)));  // x^(1/6)
     double vwd = nt / w;
     p = p - cw1 * fw * vwd * vwd;
-    p = p + cb2 * dnu / sig;
+    p = p + cb2 * dnu * rsig;
     psa = p;
   }
   // viscous terms
-  double visc = sa_visc_face(S, 0, l, rei, sig) - sa_visc_face(S, 0, l - 1, rei, sig);
-  visc = visc + sa_visc_face(S, 1, l, rei, sig) - sa_visc_face(S, 1, l - sj, rei, sig);
-  visc = visc + sa_visc_face(S, 2, l, rei, sig) - sa_visc_face(S, 2, l - sk, rei, sig);
+  double visc = sa_visc_face(S, 0, l, rei, rsig) - sa_visc_face(S, 0, l - 1, rei, rsig);
+  visc = visc + sa_visc_face(S, 1, l, rei, rsig) - sa_visc_face(S, 1, l - sj, rei, rsig);
+  visc = visc + sa_visc_face(S, 2, l, rei, rsig) - sa_visc_face(S, 2, l - sk, rei, rsig);
   // convective flux
   double rh = sa_conv_face(S, 0, l, 1) - sa_conv_face(S, 0, l - 1, 1);
   rh = rh + sa_conv_face(S, 1, l, sj) - sa_conv_face(S, 1, l - sj, sj);
   rh = rh + sa_conv_face(S, 2, l, sk) - sa_conv_face(S, 2, l - sk, sk);
   // unsteady term and implicit source scaling
-  double dtj = 2.0 * S.delti * S.aj[l];
-  double dq5dt = S.es * (3.0 * q5[l] - 4.0 * S.qn5[l] + S.qnm1_5[l]) / dtj;
-  double r = rh + dq5dt - visc - psa / S.aj[l];
+  double rdtj = 1.0 / (2.0 * S.delti * S.aj[l]);
+  double dq5dt = S.es * (3.0 * q5[l] - 4.0 * S.qn5[l] + S.qnm1_5[l]) * rdtj;
+  double r = rh + dq5dt - visc - psa * S.rj[l];
   S.rh[l] = SW(-S.dtev[l] * S.aj[l] * r);
   // ADI rows of the three directions for this nu_tilde (its values change
   // only at the end of the k sweep)
@@ -242,137 +257,153 @@ __global__ void __launch_bounds__(128) k_sa_rhs(SaT<SW> S) {
 }
 
 // Scalar ADI sweep of nu_tilde along one direction
-// (src/rhs_sa_adi_solver.F90:50-244) on the stored rows, two-ended: a CTA
-// owns 64 lines; threads 0-63 eliminate the upper half of each line top-down
-// (SGTSV's no-interchange order; a would-swap row is counted in flags[0]),
-// threads 64-127 the lower half bottom-up; the halves meet in a 2x2 solve
-// and back-substitute.  Rows are read R nodes at a time so that R loads are
-// in flight per thread.  The k sweep ends with the update
-// nu <- nu + (-nu + (nu_old + dnu)) / (1 + 1.5 dtev / dt)
-// (src/des_eddy.F90:260-272).
-template <class SW, int DIR>
-__global__ void __launch_bounds__(128) k_sa_sweep3(SaT<SW> S) {
-  __shared__ SW m_d[64], m_c[64], m_b[64], n_d[64], n_c[64], n_b[64];
-  const int lane = threadIdx.x & 63, half = threadIdx.x >> 6;
-  const int a = blockIdx.x * 64 + lane + 1;
+// (src/rhs_sa_adi_solver.F90:50-244) on the stored rows, as a shared-memory
+// slab: a CTA owns NL lines of one plane and 2 NL threads.
+//   phase 0  the rows (aw, ap, ae) and the right-hand side of the slab are
+//            copied into shared memory (cp.async, all in flight, coalesced
+//            along the fastest global index), laid out [node][line];
+//   phase 1  thread (line, half) eliminates the upper half of its line
+//            top-down (SGTSV's no-interchange order; a would-swap row is
+//            counted in flags[0]) or the lower half bottom-up, the eliminated
+//            diagonal replacing ap; the halves meet in a 2x2 solve and
+//            back-substitute;
+//   phase 2  the solution goes back to rh, or, after the k sweep, into the
+//            update nu <- nu + (-nu + (nu_old + dnu)) / (1 + 1.5 dtev / dt)
+//            (src/des_eddy.F90:260-272).
+// Shared memory: 4 fields of slab_fs(n, NL + 1) elements of SW.
+template <class SW, int DIR, int NL>
+__global__ void __launch_bounds__(2 * NL) k_sa_sweep4(SaT<SW> S) {
+  constexpr int NT = 2 * NL, NLP = NL + 1;
+  extern __shared__ __align__(16) unsigned char sa_slab[];
+  __shared__ SW m_d[NL], m_c[NL], m_b[NL], n_d[NL], n_c[NL], n_b[NL];
+  const int tid = threadIdx.x;
+  const int a0 = blockIdx.x * NL + 1;
   const int b = blockIdx.y + 1;
-  int amax, n, st, lb;
-  if (DIR == 0) { amax = S.jm - 2; n = S.im - 2; st = 1; lb = S.sj * a + S.sk * b; }
-  else if (DIR == 1) { amax = S.im - 2; n = S.jm - 2; st = S.sj; lb = a + S.sk * b; }
-  else { amax = S.im - 2; n = S.km - 2; st = S.sk; lb = a + S.sj * b; }
-  const bool act = a <= amax;
-  const SW* __restrict__ caw = S.co[3 * DIR + 0];
-  const SW* __restrict__ cap = S.co[3 * DIR + 1];
-  const SW* __restrict__ cae = S.co[3 * DIR + 2];
-  constexpr int R = 8;
+  int amax, n, st, sa, base;
+  if (DIR == 0) { amax = S.jm - 2; n = S.im - 2; st = 1; sa = S.sj; base = S.sk * b; }
+  else if (DIR == 1) { amax = S.im - 2; n = S.jm - 2; st = S.sj; sa = 1; base = S.sk * b; }
+  else { amax = S.im - 2; n = S.km - 2; st = S.sk; sa = 1; base = S.sj * b; }
+  const int nl = min(NL, amax - a0 + 1);
+  const int fs = slab_fs(n, NLP);  // row p (node p + 1) at p * NLP + line
+  SW* s_aw = reinterpret_cast<SW*>(sa_slab);
+  SW* s_ap = s_aw + fs;
+  SW* s_ae = s_aw + 2 * fs;
+  SW* s_rh = s_aw + 3 * fs;
+  const int total = nl * n;
+  auto node = [&](int t, int& li, int& p) {
+    if (DIR == 0) { li = t / n; p = t - li * n; }
+    else { p = t / nl; li = t - p * nl; }
+    return base + (a0 + li) * sa + (p + 1) * st;
+  };
+
+  // ---- phase 0
+  for (int t = tid; t < total; t += NT) {
+    int li, p;
+    const int l = node(t, li, p);
+    const int so = p * NLP + li;
+    cp_async_elem(s_aw + so, S.co[3 * DIR + 0] + l);
+    cp_async_elem(s_ap + so, S.co[3 * DIR + 1] + l);
+    cp_async_elem(s_ae + so, S.co[3 * DIR + 2] + l);
+    cp_async_elem(s_rh + so, S.rh + l);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+
+  // ---- phase 1
+  const int li = tid % NL, half = tid / NL;
+  const bool act = li < nl;
   const int h = n / 2;
+  auto at = [&](int p) { return p * NLP + li; };
   int npiv = 0;
   if (act && half == 0) {
     SW dprev = 0, duprev = 0, bprev = 0;
-    for (int p0 = 0; p0 < h; p0 += R) {
-      SW raw[R], rap[R], rae[R], rrh[R];
-#pragma unroll
-      for (int u = 0; u < R; ++u) {
-        const int p = p0 + u;
-        if (p < h) {
-          const int l = lb + (p + 1) * st;
-          raw[u] = caw[l]; rap[u] = cap[l]; rae[u] = cae[l]; rrh[u] = S.rh[l];
-        }
+    for (int p = 0; p < h; ++p) {
+      const SW aw = s_aw[at(p)], ap = s_ap[at(p)], ae = s_ae[at(p)], rr = s_rh[at(p)];
+      SW d;
+      if (p == 0) { d = ap; bprev = rr; }
+      else {
+        npiv += dabs(dprev) < dabs(aw);
+        const SW f = aw / dprev;
+        d = ap - f * duprev;
+        bprev = rr - f * bprev;
       }
-#pragma unroll
-      for (int u = 0; u < R; ++u) {
-        const int p = p0 + u;
-        if (p < h) {
-          const int l = lb + (p + 1) * st;
-          SW d;
-          if (p == 0) { d = rap[u]; bprev = rrh[u]; }
-          else {
-            npiv += dabs(dprev) < dabs(raw[u]);
-            const SW f = raw[u] / dprev;
-            d = rap[u] - f * duprev;
-            bprev = rrh[u] - f * bprev;
-          }
-          S.sd[l] = d; S.rh[l] = bprev;
-          dprev = d; duprev = rae[u];
-        }
-      }
+      s_ap[at(p)] = d; s_rh[at(p)] = bprev;
+      dprev = d; duprev = ae;
     }
-    m_d[lane] = dprev; m_c[lane] = duprev; m_b[lane] = bprev;
+    m_d[li] = dprev; m_c[li] = duprev; m_b[li] = bprev;
   } else if (act && half == 1) {
     SW dprev = 0, awprev = 0, bprev = 0;
-    for (int p0 = n - 1; p0 >= h; p0 -= R) {
-      SW raw[R], rap[R], rae[R], rrh[R];
-#pragma unroll
-      for (int u = 0; u < R; ++u) {
-        const int p = p0 - u;
-        if (p >= h) {
-          const int l = lb + (p + 1) * st;
-          raw[u] = caw[l]; rap[u] = cap[l]; rae[u] = cae[l]; rrh[u] = S.rh[l];
-        }
+    for (int p = n - 1; p >= h; --p) {
+      const SW aw = s_aw[at(p)], ap = s_ap[at(p)], ae = s_ae[at(p)], rr = s_rh[at(p)];
+      SW d;
+      if (p == n - 1) { d = ap; bprev = rr; }
+      else {
+        npiv += dabs(dprev) < dabs(ae);
+        const SW f = ae / dprev;
+        d = ap - f * awprev;
+        bprev = rr - f * bprev;
       }
-#pragma unroll
-      for (int u = 0; u < R; ++u) {
-        const int p = p0 - u;
-        if (p >= h) {
-          const int l = lb + (p + 1) * st;
-          SW d;
-          if (p == n - 1) { d = rap[u]; bprev = rrh[u]; }
-          else {
-            npiv += dabs(dprev) < dabs(rae[u]);
-            const SW f = rae[u] / dprev;
-            d = rap[u] - f * awprev;
-            bprev = rrh[u] - f * bprev;
-          }
-          S.sd[l] = d; S.rh[l] = bprev;
-          dprev = d; awprev = raw[u];
-        }
-      }
+      s_ap[at(p)] = d; s_rh[at(p)] = bprev;
+      dprev = d; awprev = aw;
     }
-    n_d[lane] = dprev; n_c[lane] = awprev; n_b[lane] = bprev;
+    n_d[li] = dprev; n_c[li] = awprev; n_b[li] = bprev;
   }
   if (npiv) atomicAdd(&S.flags[0], npiv);
   __syncthreads();
-  if (!act) return;
-  const SW d1 = m_d[lane], u1 = m_c[lane], b1 = m_b[lane];
-  const SW d2 = n_d[lane], l2 = n_c[lane], b2 = n_b[lane];
-  const SW det = d1 * d2 - u1 * l2;
-  const double dmul = 1.5 * S.es;
-  auto put = [&](int l, SW x, double nt, double dt) {
-    if (DIR == 2) {
-      const double qe5 = nt + double(x);
-      const double dum = 1.0 + dmul * dt / S.delti;
-      S.q[4][l] = nt + (-nt + qe5) / dum;
+  if (act) {
+    const SW d1 = m_d[li], u1 = m_c[li], b1 = m_b[li];
+    const SW d2 = n_d[li], l2 = n_c[li], b2 = n_b[li];
+    const SW det = d1 * d2 - u1 * l2;
+    if (half == 0) {
+      SW x = (b1 * d2 - u1 * b2) / det;
+      s_rh[at(h - 1)] = x;
+      for (int p = h - 2; p >= 0; --p) {
+        x = (s_rh[at(p)] - s_ae[at(p)] * x) / s_ap[at(p)];
+        s_rh[at(p)] = x;
+      }
     } else {
-      S.rh[l] = x;
-    }
-  };
-  // half 0 runs back from node h-1 with the ae couplings, half 1 forward
-  // from node h with the aw couplings
-  const SW* __restrict__ cup = half == 0 ? cae : caw;
-  SW x = half == 0 ? (b1 * d2 - u1 * b2) / det : (d1 * b2 - l2 * b1) / det;
-  {
-    const int l = lb + (half == 0 ? h : h + 1) * st;
-    put(l, x, DIR == 2 ? S.q[4][l] : 0.0, DIR == 2 ? S.dtev[l] : 0.0);
-  }
-  const int cnt = half == 0 ? h - 1 : n - h - 1;  // nodes left to back-substitute
-  const int pstart = half == 0 ? h - 2 : h + 1;
-  const int dp = half == 0 ? -1 : 1;
-  for (int t0 = 0; t0 < cnt; t0 += R) {
-    SW bb[R], bd[R], bu[R];
-    double bn[R], bt[R];
-#pragma unroll
-    for (int u = 0; u < R; ++u) {
-      if (t0 + u < cnt) {
-        const int l = lb + (pstart + dp * (t0 + u) + 1) * st;
-        bb[u] = S.rh[l]; bd[u] = S.sd[l]; bu[u] = cup[l];
-        if (DIR == 2) { bn[u] = S.q[4][l]; bt[u] = S.dtev[l]; }
+      SW x = (d1 * b2 - l2 * b1) / det;
+      s_rh[at(h)] = x;
+      for (int p = h + 1; p < n; ++p) {
+        x = (s_rh[at(p)] - s_aw[at(p)] * x) / s_ap[at(p)];
+        s_rh[at(p)] = x;
       }
     }
+  }
+  __syncthreads();
+
+  // ---- phase 2
+  if (DIR < 2) {
+    for (int t = tid; t < total; t += NT) {
+      int lq, p;
+      const int l = node(t, lq, p);
+      S.rh[l] = s_rh[p * NLP + lq];
+    }
+  } else {
+    const double dmul = 1.5 * S.es;
+    constexpr int U = 4;
+    for (int t0 = tid; t0 < total; t0 += NT * U) {
+      int ln[U], so[U];
+      double nt[U], dt[U];
 #pragma unroll
-    for (int u = 0; u < R; ++u) {
-      if (t0 + u < cnt) {
-        x = (bb[u] - bu[u] * x) / bd[u];
-        put(lb + (pstart + dp * (t0 + u) + 1) * st, x, DIR == 2 ? bn[u] : 0.0, DIR == 2 ? bt[u] : 0.0);
+      for (int u = 0; u < U; ++u) {
+        const int t = t0 + u * NT;
+        ln[u] = -1;
+        so[u] = 0;
+        if (t < total) {
+          int lq, p;
+          ln[u] = node(t, lq, p);
+          so[u] = p * NLP + lq;
+          nt[u] = S.q[4][ln[u]];
+          dt[u] = __ldg(S.dtev + ln[u]);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (ln[u] < 0) continue;
+        const double qe5 = nt[u] + double(s_rh[so[u]]);
+        const double dum = 1.0 + dmul * dt[u] / S.delti;
+        S.q[4][ln[u]] = nt[u] + (-nt[u] + qe5) / dum;
       }
     }
   }

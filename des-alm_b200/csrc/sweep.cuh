@@ -38,10 +38,11 @@ namespace desalm {
 // Shared-memory slab sweep.  A CTA owns NL lines of one plane (consecutive in
 // the transverse index that is contiguous in memory, or, for the i sweep,
 // NL rows of contiguous i lines) and 8 NL threads.
-//   phase 0  tc, hc and the four transformed residuals of the slab are read
-//            once, with loads coalesced along the fastest global index, into
-//            shared memory laid out [node][line] (line stride NL + 1, so that
-//            the transposed i-sweep stores are free of bank conflicts);
+//   phase 0  tc, hc and the four transformed residuals of the slab are copied
+//            once (cp.async, all copies in flight, coalesced along the fastest
+//            global index) into shared memory laid out [node][line] (line
+//            stride NL + 1, so that the transposed i-sweep stores are free of
+//            bank conflicts);
 //   phase 1  thread (line, system m, half) eliminates its half-line in shared
 //            memory exactly as the two-ended sweep does (same operations,
 //            same order); the halves meet in the 2x2 middle solve and
@@ -77,44 +78,22 @@ __global__ void __launch_bounds__(8 * NL) k_sweep4(Lv<T, W> L, Par P, int blo, i
   W* s_r = s_tc + 2 * fs;  // system q at s_r + q fs
   W* s_d = s_tc + 6 * fs;
 
-  // ---- phase 0: slab -> shared memory
+  // ---- phase 0: slab -> shared memory, every copy in flight at once
   {
     const W* tc = L.tc[DIR];
     const W* hc = L.hc[DIR];
     const int total = nl * np;
-    constexpr int U = 4;
-    for (int t0 = tid; t0 < total; t0 += NT * U) {
-      W v[U][6];
-      int so[U];
+    for (int t = tid; t < total; t += NT) {
+      int li, p;
+      if (DIR == 0) { li = t / np; p = t - li * np; }
+      else { p = t / nl; li = t - p * nl; }
+      const int l = base + (a0 + li) * sa + p * st;
+      const int so = p * NLP + li;
+      cp_async_elem(s_hc + so, hc + l);
+      if (p >= 1 && p <= n) {
+        cp_async_elem(s_tc + so, tc + l);
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int t = t0 + u * NT;
-        so[u] = -1;
-        if (t < total) {
-          int li, p;
-          if (DIR == 0) { li = t / np; p = t - li * np; }
-          else { p = t / nl; li = t - p * nl; }
-          const int l = base + (a0 + li) * sa + p * st;
-          so[u] = p * NLP + li;
-          v[u][1] = hc[l];
-          if (p >= 1 && p <= n) {
-            v[u][0] = tc[l];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) v[u][2 + q] = L.wk[q][l];
-          } else {
-#pragma unroll
-            for (int q = 0; q < 6; ++q) if (q != 1) v[u][q] = W(0);
-          }
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        if (so[u] >= 0) {
-          s_tc[so[u]] = v[u][0];
-          s_hc[so[u]] = v[u][1];
-#pragma unroll
-          for (int q = 0; q < 4; ++q) s_r[q * fs + so[u]] = v[u][2 + q];
-        }
+        for (int q = 0; q < 4; ++q) cp_async_elem(s_r + q * fs + so, L.wk[q] + l);
       }
     }
   }
@@ -142,6 +121,7 @@ __global__ void __launch_bounds__(8 * NL) k_sweep4(Lv<T, W> L, Par P, int blo, i
 #pragma unroll
     for (int q = 0; q < 4; ++q) { sbw[tid][q] = W(bw[q]); sbe[tid][q] = W(be[q]); }
   }
+  cp_async_wait_all();
   __syncthreads();
 
   // ---- phase 1: two-ended elimination in shared memory
@@ -244,50 +224,84 @@ __global__ void __launch_bounds__(8 * NL) k_sweep4(Lv<T, W> L, Par P, int blo, i
   }
   __syncthreads();
 
-  // ---- phase 2: per-node transform in the sweep precision W
+  // ---- phase 2: per-node transform in the sweep precision W, U nodes per
+  // thread at a time: all their global reads are issued before any store
   const int total = nl * n;
-  for (int t = tid; t < total; t += NT) {
-    int lq, p;
-    if (DIR == 0) { lq = t / n; p = t - lq * n; }
-    else { p = t / nl; lq = t - p * nl; }
-    const int aa = a0 + lq;
-    const int l = base + aa * sa + (p + 1) * st;
-    const int so = (p + 1) * NLP + lq;
-    W xv[4];
+  constexpr int U = 4;
+  const T* const* m1 = DIR == 0 ? L.csi : (DIR == 1 ? L.eta : L.zet);  // forward matrix metrics
+  const T* const* m2 = DIR == 0 ? L.eta : L.zet;                       // inverse matrix metrics
+  for (int t0 = tid; t0 < total; t0 += NT * U) {
+    int lnode[U], aan[U], pn[U];
+    W a1[U][3], a2[U][3], sgv[U];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) xv[q] = s_r[q * fs + so];
-    const W sg = L.sig[l];
-    W y[4], z[4];
-    if (DIR == 0) {
-      const int S = L.im * L.km, o = (p + 1) + L.im * b;
-      const int tgt[4] = {1, 2, L.jm - 2, L.jm - 3};
+    for (int u = 0; u < U; ++u) {
+      const int t = t0 + u * NT;
+      lnode[u] = -1;
+      aan[u] = a0; pn[u] = 0;
+      if (t < total) {
+        int lq, p;
+        if (DIR == 0) { lq = t / n; p = t - lq * n; }
+        else { p = t / nl; lq = t - p * nl; }
+        aan[u] = a0 + lq;
+        pn[u] = p;
+        const int l = base + aan[u] * sa + (p + 1) * st;
+        lnode[u] = l;
+        sgv[u] = __ldg(L.sig + l);
 #pragma unroll
-      for (int s = 0; s < 4; ++s)
-        if (aa == tgt[s])
+        for (int x = 0; x < 3; ++x) a1[u][x] = W(__ldg(m1[x] + l));
+        if (DIR < 2)
 #pragma unroll
-          for (int q = 0; q < 4; ++q) L.bj[(s * 4 + q) * S + o] = xv[q];
-      // N1^-1 x = Mb^-1 (Ma x)
-      mfwd_apply<W>(W(L.csi[0][l]), W(L.csi[1][l]), W(L.csi[2][l]), sg, xv, y);
-      minv_apply<W>(W(L.eta[0][l]), W(L.eta[1][l]), W(L.eta[2][l]), sg, y, z);
+          for (int x = 0; x < 3; ++x) a2[u][x] = W(__ldg(m2[x] + l));
+      }
+    }
+    T qv[U][4];
+    if (DIR == 2) {
 #pragma unroll
-      for (int q = 0; q < 4; ++q) L.wk[q][l] = z[q];
-    } else if (DIR == 1) {
-      const int S = L.im * L.jm, o = aa + L.im * (p + 1);
-      const int tgt[4] = {1, 2, L.km - 2, L.km - 3};
+      for (int u = 0; u < U; ++u)
+        if (lnode[u] >= 0)
 #pragma unroll
-      for (int s = 0; s < 4; ++s)
-        if (b == tgt[s])
+          for (int q = 0; q < 4; ++q) qv[u][q] = L.q[q][lnode[u]];
+    }
 #pragma unroll
-          for (int q = 0; q < 4; ++q) L.bk[(s * 4 + q) * S + o] = xv[q];
-      // N2^-1 x = Mc^-1 (Mb x)
-      mfwd_apply<W>(W(L.eta[0][l]), W(L.eta[1][l]), W(L.eta[2][l]), sg, xv, y);
-      minv_apply<W>(W(L.zet[0][l]), W(L.zet[1][l]), W(L.zet[2][l]), sg, y, z);
+    for (int u = 0; u < U; ++u) {
+      if (lnode[u] < 0) continue;
+      const int l = lnode[u], p = pn[u], aa = aan[u];
+      const int so = (p + 1) * NLP + (aa - a0);
+      W xv[4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) L.wk[q][l] = z[q];
-    } else {
-      mfwd_apply<W>(W(L.zet[0][l]), W(L.zet[1][l]), W(L.zet[2][l]), sg, xv, y);
+      for (int q = 0; q < 4; ++q) xv[q] = s_r[q * fs + so];
+      W y[4], z[4];
+      if (DIR == 0) {
+        const int S = L.im * L.km, o = (p + 1) + L.im * b;
+        const int tgt[4] = {1, 2, L.jm - 2, L.jm - 3};
 #pragma unroll
-      for (int q = 0; q < 4; ++q) L.q[q][l] = L.q[q][l] + T(y[q]);
+        for (int s = 0; s < 4; ++s)
+          if (aa == tgt[s])
+#pragma unroll
+            for (int q = 0; q < 4; ++q) L.bj[(s * 4 + q) * S + o] = xv[q];
+        // N1^-1 x = Mb^-1 (Ma x)
+        mfwd_apply<W>(a1[u][0], a1[u][1], a1[u][2], sgv[u], xv, y);
+        minv_apply<W>(a2[u][0], a2[u][1], a2[u][2], sgv[u], y, z);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) L.wk[q][l] = z[q];
+      } else if (DIR == 1) {
+        const int S = L.im * L.jm, o = aa + L.im * (p + 1);
+        const int tgt[4] = {1, 2, L.km - 2, L.km - 3};
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+          if (b == tgt[s])
+#pragma unroll
+            for (int q = 0; q < 4; ++q) L.bk[(s * 4 + q) * S + o] = xv[q];
+        // N2^-1 x = Mc^-1 (Mb x)
+        mfwd_apply<W>(a1[u][0], a1[u][1], a1[u][2], sgv[u], xv, y);
+        minv_apply<W>(a2[u][0], a2[u][1], a2[u][2], sgv[u], y, z);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) L.wk[q][l] = z[q];
+      } else {
+        mfwd_apply<W>(a1[u][0], a1[u][1], a1[u][2], sgv[u], xv, y);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) L.q[q][l] = qv[u][q] + T(y[q]);
+      }
     }
   }
 }
