@@ -46,9 +46,12 @@ def alg_bytes(kind, T, W, coarse):
     return {
         "resid": 24 * T + 11 * W + pk,    # q4 qn3 qnm1-3 metrics9 aj 1/aj nut dtau | wk4 sigma tc3 hc3, diss1
         "recalc": 26 * T + pk,            # q4 qn3 qnm1-3 metrics9 aj 1/aj nut diss1 | rh4
-        "sweep_i": 11 * W + 6 * T,        # wk4 in/out, tc, hc, sigma, csi3, eta3
-        "sweep_j": 11 * W + 6 * T,        # wk4 in/out, tc, hc, sigma, eta3, zet3
-        "sweep_k": 7 * W + 11 * T,        # wk4, tc, hc, sigma, zet3, q4 in/out
+        "sweep_i": 10 * W,                # line solve: wk4 in/out, tc, hc
+        "sweep_j": 10 * W,
+        "sweep_k": 10 * W,
+        "xform_i": 9 * W + 6 * T,         # wk4 in/out, sigma, csi3, eta3 (j-face rows: not counted)
+        "xform_j": 9 * W + 6 * T,         # wk4 in/out, sigma, eta3, zet3
+        "xform_k": 5 * W + 11 * T,        # wk4, sigma, zet3, q4 in/out
         "dtau": 11 * T,                   # metrics9 nut | dtau
         "norm": 15 * T,                   # q5 qold5 | qold5
         "rsmooth": 8 * T,                 # dq4 in/out (last one: q4 in/out instead)

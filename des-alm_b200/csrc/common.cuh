@@ -62,7 +62,18 @@ struct Par {
   int fine;                      // 1 when the level is the finest
 };
 
+// Elements of one field of a shared-memory line slab: np nodes of nlp-strided
+// lines, rounded up to a multiple of 32 plus 16, so that consecutive fields
+// start on different banks.
+DESALM_HD inline int slab_fs(int np, int nlp) { return ((np * nlp + 31) / 32) * 32 + 16; }
+
 template <class T> DESALM_DEV T dabs(T x) { return x < T(0) ? -x : x; }
+
+// Reciprocal used by the line eliminations: in FP32 (the sweeps of MIXED mode,
+// a preconditioner) the hardware approximation __fdividef (2 ulp), in FP64 the
+// correctly rounded division.
+DESALM_DEV float sweep_rcp(float x) { return __fdividef(1.0f, x); }
+DESALM_DEV double sweep_rcp(double x) { return 1.0 / x; }
 
 // Asynchronous global -> shared copy of one 4- or 8-byte element
 // (cp.async, cached in L1); completion by cp_async_wait_all().

@@ -82,7 +82,7 @@ struct Level {
   Lv<double, float> df{};
   void* dq[4] = {nullptr, nullptr, nullptr, nullptr};  // prolongation correction
   double* fac[3] = {nullptr, nullptr, nullptr};         // rsmooth multipliers
-  double* dpr[3] = {nullptr, nullptr, nullptr};         // rsmooth eliminated diagonal
+  double* dpr[3] = {nullptr, nullptr, nullptr};         // rsmooth eliminated diagonal [n], then its reciprocals [n]
   bool dtau_valid = false;
 };
 
@@ -157,7 +157,8 @@ inline unsigned cdiv(long a, long b) { return (unsigned)((a + b - 1) / b); }
 
 // kernel classes for desalm_kernel_stats
 enum KClass { KC_DTAU = 0, KC_RESID, KC_SWEEP_I, KC_SWEEP_J, KC_SWEEP_K, KC_RECALC, KC_BCOND, KC_PFIX,
-              KC_NLEVEL, KC_PROLONG, KC_RSMOOTH, KC_NORM, KC_SA_RHS, KC_SA_SWEEP, KC_SA_BC, KC_MISC, KC_COUNT };
+              KC_NLEVEL, KC_PROLONG, KC_RSMOOTH, KC_NORM, KC_SA_RHS, KC_SA_SWEEP, KC_SA_BC,
+              KC_XFORM_I, KC_XFORM_J, KC_XFORM_K, KC_SA_AUX, KC_MISC, KC_COUNT };
 
 struct ProfScope {
   desalm_ctx* ctx;
@@ -299,12 +300,15 @@ int sweep4_nl(desalm_ctx* ctx, Lv<T, W>& L, const Par& P, int lvl, int blo, int 
   cudaStream_t s = ctx->stream;
   LAUNCH(cls, lvl, nin, k_sweep4<T, W, DIR, NL><<<dim3(cdiv(amax, NL), nb), 8 * NL, bytes, s>>>(L, P, blo, bhi));
   CKL();
+  const int xcls = DIR == 0 ? KC_XFORM_I : (DIR == 1 ? KC_XFORM_J : KC_XFORM_K);
+  LAUNCH(xcls, lvl, nin, k_xform<T, W, DIR><<<grid_interior(L), blk3(), 0, s>>>(L));
+  CKL();
   return 0;
 }
 
-// Shared-memory opt-in of every slab-sweep and SA slab-sweep instantiation
-// on the current device (done when a context is created, outside any stream
-// capture).
+// Shared-memory opt-in of every slab kernel (line sweeps, SA sweeps,
+// rsmooth) on the current device (done when a context is created, outside any
+// stream capture).
 template <class T, class W>
 cudaError_t slab_attrs() {
   int dev = 0, optin = 0;
@@ -323,6 +327,9 @@ cudaError_t slab_attrs() {
   set((const void*)k_sa_sweep4<W, 0, 32>); set((const void*)k_sa_sweep4<W, 0, 16>); set((const void*)k_sa_sweep4<W, 0, 8>);
   set((const void*)k_sa_sweep4<W, 1, 32>); set((const void*)k_sa_sweep4<W, 1, 16>); set((const void*)k_sa_sweep4<W, 1, 8>);
   set((const void*)k_sa_sweep4<W, 2, 32>); set((const void*)k_sa_sweep4<W, 2, 16>); set((const void*)k_sa_sweep4<W, 2, 8>);
+  set((const void*)k_rsmooth4<T, W, 0, 16>); set((const void*)k_rsmooth4<T, W, 0, 8>); set((const void*)k_rsmooth4<T, W, 0, 4>);
+  set((const void*)k_rsmooth4<T, W, 1, 16>); set((const void*)k_rsmooth4<T, W, 1, 8>); set((const void*)k_rsmooth4<T, W, 1, 4>);
+  set((const void*)k_rsmooth4<T, W, 2, 16>); set((const void*)k_rsmooth4<T, W, 2, 8>); set((const void*)k_rsmooth4<T, W, 2, 4>);
   return e;
 }
 
@@ -397,6 +404,30 @@ int launch_nlevel(desalm_ctx* ctx, Lv<TF, WF>& F, Lv<TC, WC>& C) {
   return 0;
 }
 
+// One direction of rsmooth as k_rsmooth4 with the widest slab that leaves
+// room for two CTAs per SM.
+template <class TF>
+size_t rs_slab_bytes(int n, int nl) { return (size_t)4 * slab_fs(n, nl + 1) * sizeof(TF); }
+template <class TF, class WF, int DIR, int NL>
+int rsmooth_nl(desalm_ctx* ctx, Lv<TF, WF>& F, TF* dq, Level& G, double e, int last, double nin) {
+  const int amax = DIR == 0 ? F.jm - 2 : F.im - 2;
+  const int n = DIR == 0 ? F.im - 2 : (DIR == 1 ? F.jm - 2 : F.km - 2);
+  const int nb = DIR == 2 ? F.jm - 2 : F.km - 2;
+  LAUNCH(KC_RSMOOTH, 0, nin, k_rsmooth4<TF, WF, DIR, NL><<<dim3(cdiv(amax, NL), nb), 8 * NL, rs_slab_bytes<TF>(n, NL), ctx->stream>>>(
+                                 F, dq, G.fac[DIR], G.dpr[DIR], e, last));
+  CKL();
+  return 0;
+}
+template <class TF, class WF, int DIR>
+int rsmooth(desalm_ctx* ctx, Lv<TF, WF>& F, TF* dq, Level& G, double e, int last, double nin) {
+  const int n = DIR == 0 ? F.im - 2 : (DIR == 1 ? F.jm - 2 : F.km - 2);
+  if (rs_slab_bytes<TF>(n, 16) <= kSlabTwoPerSm) return rsmooth_nl<TF, WF, DIR, 16>(ctx, F, dq, G, e, last, nin);
+  if (rs_slab_bytes<TF>(n, 8) <= kSlabTwoPerSm) return rsmooth_nl<TF, WF, DIR, 8>(ctx, F, dq, G, e, last, nin);
+  if (rs_slab_bytes<TF>(n, 4) <= kSlabMax) return rsmooth_nl<TF, WF, DIR, 4>(ctx, F, dq, G, e, last, nin);
+  ctx->err = "grid line too long for the shared-memory rsmooth";
+  return DESALM_EINVAL;
+}
+
 template <class TF, class WF, class TC, class WC>
 int launch_prolong(desalm_ctx* ctx, Lv<TF, WF>& F, Lv<TC, WC>& C, Level& G) {
   const desalm_case& c = ctx->c;
@@ -405,12 +436,9 @@ int launch_prolong(desalm_ctx* ctx, Lv<TF, WF>& F, Lv<TC, WC>& C, Level& G) {
   const double nin = double(F.im - 2) * (F.jm - 2) * (F.km - 2);
   LAUNCH(KC_PROLONG, 0, nin, k_prolong_interp<TF, WF, TC, WC><<<grid_interior(F), blk3(), 0, s>>>(F, C, dq, c.icrs, c.jcrs, c.kcrs));
   CKL();
-  LAUNCH(KC_RSMOOTH, 0, nin, k_rsmooth3<TF, WF, 0><<<dim3(cdiv(F.jm - 2, 32), F.km - 2), 256, 0, s>>>(F, dq, G.fac[0], G.dpr[0], c.ep[1][0], 0));
-  CKL();
-  LAUNCH(KC_RSMOOTH, 0, nin, k_rsmooth3<TF, WF, 1><<<dim3(cdiv(F.im - 2, 32), F.km - 2), 256, 0, s>>>(F, dq, G.fac[1], G.dpr[1], c.ep[1][1], 0));
-  CKL();
-  LAUNCH(KC_RSMOOTH, 0, nin, k_rsmooth3<TF, WF, 2><<<dim3(cdiv(F.im - 2, 32), F.jm - 2), 256, 0, s>>>(F, dq, G.fac[2], G.dpr[2], c.ep[1][2], 1));
-  CKL();
+  RET((rsmooth<TF, WF, 0>(ctx, F, dq, G, c.ep[1][0], 0, nin)));
+  RET((rsmooth<TF, WF, 1>(ctx, F, dq, G, c.ep[1][1], 0, nin)));
+  RET((rsmooth<TF, WF, 2>(ctx, F, dq, G, c.ep[1][2], 1, nin)));
   return 0;
 }
 
@@ -656,6 +684,9 @@ int desalm_init(const desalm_case* c, desalm_ctx** out) {
       for (int d = 0; d < 3; ++d) {
         std::vector<double> fac, dpr;
         rs_factors(ext[d] - 2, c->ep[1][d], fac, dpr);
+        const size_t nd = dpr.size();
+        dpr.resize(2 * nd);
+        for (size_t p = 0; p < nd; ++p) dpr[nd + p] = 1.0 / dpr[p];
         rc = dalloc(ctx, G.allocs, (void**)&G.fac[d], fac.size() * sizeof(double));
         if (!rc) rc = dalloc(ctx, G.allocs, (void**)&G.dpr[d], dpr.size() * sizeof(double));
         if (rc) { *out = ctx; return rc; }
@@ -1223,8 +1254,8 @@ int sa_run(desalm_ctx* ctx, Lv<double, W>& L) {
   cudaStream_t s = ctx->stream;
   const double nin = double(L.im - 2) * (L.jm - 2) * (L.km - 2);
   const dim3 gi(cdiv(L.im - 2, 32), cdiv(L.jm - 2, 4), L.km - 2);
-  LAUNCH(KC_SA_RHS, 0, nin, k_sa_source<W><<<gi, blk3(), 0, s>>>(S));
-  LAUNCH(KC_SA_RHS, 0, L.N, k_sa_ucn<W><<<cdiv(L.N, 256), 256, 0, s>>>(S));
+  LAUNCH(KC_SA_AUX, 0, nin, k_sa_source<W><<<gi, blk3(), 0, s>>>(S));
+  LAUNCH(KC_SA_AUX, 0, L.N, k_sa_ucn<W><<<cdiv(L.N, 256), 256, 0, s>>>(S));
   for (int it = 0; it < ctx->c.itk; ++it) {
     LAUNCH(KC_SA_RHS, 0, nin, k_sa_rhs<W><<<gi, blk3(), 0, s>>>(S));
     RET((sa_sweep<W, 0>(ctx, S, L.jm - 2, L.im - 2, L.km - 2, nin)));

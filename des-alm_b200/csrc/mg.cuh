@@ -158,13 +158,6 @@ __global__ void k_prolong_interp(Lv<TF, WF> F, Lv<TC, WC> C, TF* dq, int icrs, i
   for (int m = 0; m < 4; ++m) dq[m * F.N + l] = I.fi(i, j, k, m);
 }
 
-// Constant-coefficient implicit smoothing (-e, 1+2e, -e) along one direction
-// (src/rs_sweep.F90:163-284), NRHS = 4: see k_rsmooth3 below.  The system
-// never pivots; fac/dpr hold SGTSV's multipliers and eliminated diagonal for
-// the line length, built on the host in SGTSV's order.  The last direction
-// (k) adds dq to q on the interior (src/mg_prolong.F90:218-277: dq is zero on
-// the boundary).
-
 // ---------------------------------------------------------------- norm
 // Per-block partial sums of |q - qold| over interior nodes, 5 fields
 // (src/mg_residual.F90:58-67); optionally qold <- q for the next iteration.
@@ -327,117 +320,117 @@ __global__ void k_dtev(double* const* cov, double* dtev, long n, double cfl2, do
 
 namespace desalm {
 
-// Two-ended constant-coefficient smoothing, one thread per (line, component,
-// half): warps 0-3 eliminate the upper
-// half of component m top-down, warps 4-7 the lower half bottom-up (the
-// matrix is symmetric Toeplitz, so the bottom-up eliminated diagonal and
-// multipliers are the top-down ones mirrored); the halves meet in a 2x2
-// solve and back-substitute.
-template <class TF, class WF, int DIR>
-__global__ void __launch_bounds__(256) k_rsmooth3(Lv<TF, WF> F, TF* dq, const double* fac, const double* dpr, double e, int last) {
-  __shared__ TF s_top[32][4][2], s_bot[32][4][2];  // (eliminated b, nothing) of the middle rows
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int m = w & 3, half = w >> 2;
-  const int a = blockIdx.x * 32 + lane + 1;
+// Constant-coefficient implicit smoothing (-e, 1+2e, -e) of the four
+// correction components along one direction (src/rs_sweep.F90:163-284), as a
+// shared-memory slab: a CTA owns NL lines of one plane and 8 NL threads.
+//   phase 0  the slab of dq is copied into shared memory (cp.async);
+//   phase 1  thread (line, component m, half) eliminates the upper half of
+//            its line top-down or the lower half bottom-up with SGTSV's
+//            multipliers fac and eliminated diagonal dpr for this line length
+//            (built on the host in SGTSV's order, with 1/dpr after dpr; the
+//            matrix is symmetric Toeplitz, so the bottom-up factors are the
+//            top-down ones mirrored); the halves meet in a 2x2 solve and
+//            back-substitute, multiplying by 1/dpr;
+//   phase 2  dq gets the smoothed values, or, after the last direction (k),
+//            q += dq on the interior (src/mg_prolong.F90:218-277: dq is zero
+//            on the boundary).
+// Shared memory: 4 components of slab_fs(n, NL + 1) elements of TF.
+template <class TF, class WF, int DIR, int NL>
+__global__ void __launch_bounds__(8 * NL) k_rsmooth4(Lv<TF, WF> F, TF* dq, const double* fac, const double* dpr, double e, int last) {
+  constexpr int NT = 8 * NL, NLP = NL + 1;
+  extern __shared__ __align__(16) unsigned char rs_slab[];
+  __shared__ TF s_top[NL][4], s_bot[NL][4];  // eliminated b of the two middle rows
+  const int tid = threadIdx.x;
+  const int a0 = blockIdx.x * NL + 1;
   const int b = blockIdx.y + 1;
-  int amax, n, st, lb;
-  if (DIR == 0) { amax = F.jm - 2; n = F.im - 2; st = 1; lb = F.sj * a + F.sk * b; }
-  else if (DIR == 1) { amax = F.im - 2; n = F.jm - 2; st = F.sj; lb = a + F.sk * b; }
-  else { amax = F.im - 2; n = F.km - 2; st = F.sk; lb = a + F.sj * b; }
-  const bool act = a <= amax;
-  TF* v = dq + (long)m * F.N;
+  int amax, n, st, sa, base;
+  if (DIR == 0) { amax = F.jm - 2; n = F.im - 2; st = 1; sa = F.sj; base = F.sk * b; }
+  else if (DIR == 1) { amax = F.im - 2; n = F.jm - 2; st = F.sj; sa = 1; base = F.sk * b; }
+  else { amax = F.im - 2; n = F.km - 2; st = F.sk; sa = 1; base = F.sj * b; }
+  const int nl = min(NL, amax - a0 + 1);
+  const int fs = slab_fs(n, NLP);  // row p (node p + 1) of component m at m fs + p NLP + line
+  TF* sv = reinterpret_cast<TF*>(rs_slab);
+  const int total = nl * n;
+  auto node = [&](int t, int& li, int& p) {
+    if (DIR == 0) { li = t / n; p = t - li * n; }
+    else { p = t / nl; li = t - p * nl; }
+    return base + (a0 + li) * sa + (p + 1) * st;
+  };
+
+  // ---- phase 0
+  for (int t = tid; t < total; t += NT) {
+    int li, p;
+    const int l = node(t, li, p);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) cp_async_elem(sv + m * fs + p * NLP + li, dq + (long)m * F.N + l);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+
+  // ---- phase 1
+  const int li = tid % NL, combo = tid / NL;
+  const int m = combo & 3, half = combo >> 2;
+  const bool act = li < nl;
+  TF* v = sv + m * fs + li;
   const TF off = TF(-e);
   const int h = n / 2;
-  constexpr int R = 8;
+  const double* rdpr = dpr + n;  // 1 / dpr
   if (act && half == 0) {
     TF bp = 0;
-    for (int p0 = 0; p0 < h; p0 += R) {
-      TF bv[R];
-#pragma unroll
-      for (int u = 0; u < R; ++u)
-        if (p0 + u < h) bv[u] = v[lb + (p0 + u + 1) * st];
-#pragma unroll
-      for (int u = 0; u < R; ++u) {
-        const int p = p0 + u;
-        if (p < h) {
-          TF x = bv[u];
-          if (p > 0) x = x - TF(fac[p - 1]) * bp;
-          bp = x;
-          v[lb + (p + 1) * st] = x;
-        }
-      }
+    for (int p = 0; p < h; ++p) {
+      TF x = v[p * NLP];
+      if (p > 0) x = x - TF(__ldg(fac + p - 1)) * bp;
+      bp = x;
+      v[p * NLP] = x;
     }
-    s_top[lane][m][0] = bp;
+    s_top[li][m] = bp;
   } else if (act && half == 1) {
     TF bp = 0;
-    for (int p0 = n - 1; p0 >= h; p0 -= R) {
-      TF bv[R];
-#pragma unroll
-      for (int u = 0; u < R; ++u)
-        if (p0 - u >= h) bv[u] = v[lb + (p0 - u + 1) * st];
-#pragma unroll
-      for (int u = 0; u < R; ++u) {
-        const int p = p0 - u;
-        if (p >= h) {
-          TF x = bv[u];
-          if (p < n - 1) x = x - TF(fac[n - 2 - p]) * bp;
-          bp = x;
-          v[lb + (p + 1) * st] = x;
-        }
-      }
+    for (int p = n - 1; p >= h; --p) {
+      TF x = v[p * NLP];
+      if (p < n - 1) x = x - TF(__ldg(fac + n - 2 - p)) * bp;
+      bp = x;
+      v[p * NLP] = x;
     }
-    s_bot[lane][m][0] = bp;
+    s_bot[li][m] = bp;
   }
   __syncthreads();
-  if (!act) return;
-  const TF d1 = TF(dpr[h - 1]), d2 = TF(dpr[n - 1 - h]);
-  const TF b1 = s_top[lane][m][0], b2 = s_bot[lane][m][0];
-  const TF det = d1 * d2 - off * off;
-  const TF x1 = (b1 * d2 - off * b2) / det;
-  const TF x2 = (d1 * b2 - off * b1) / det;
-  if (half == 0) {
-    TF x = x1;
-    {
-      const int l = lb + h * st;
-      if (last) F.q[m][l] = F.q[m][l] + x1; else v[l] = x1;
-    }
-    for (int p1 = h - 2; p1 >= 0; p1 -= R) {
-      TF bv[R], bq[R];
-#pragma unroll
-      for (int u = 0; u < R; ++u) {
-        const int p = p1 - u;
-        if (p >= 0) { bv[u] = v[lb + (p + 1) * st]; if (last) bq[u] = F.q[m][lb + (p + 1) * st]; }
+  if (act) {
+    const TF d1 = TF(__ldg(dpr + h - 1)), d2 = TF(__ldg(dpr + n - 1 - h));
+    const TF b1 = s_top[li][m], b2 = s_bot[li][m];
+    const TF det = d1 * d2 - off * off;
+    if (half == 0) {
+      TF x = (b1 * d2 - off * b2) / det;
+      v[(h - 1) * NLP] = x;
+      for (int p = h - 2; p >= 0; --p) {
+        x = (v[p * NLP] - off * x) * TF(__ldg(rdpr + p));
+        v[p * NLP] = x;
       }
-#pragma unroll
-      for (int u = 0; u < R; ++u) {
-        const int p = p1 - u;
-        if (p >= 0) {
-          x = (bv[u] - off * x) / TF(dpr[p]);
-          if (last) F.q[m][lb + (p + 1) * st] = bq[u] + x; else v[lb + (p + 1) * st] = x;
-        }
+    } else {
+      TF x = (d1 * b2 - off * b1) / det;
+      v[h * NLP] = x;
+      for (int p = h + 1; p < n; ++p) {
+        x = (v[p * NLP] - off * x) * TF(__ldg(rdpr + n - 1 - p));
+        v[p * NLP] = x;
       }
     }
-  } else {
-    TF x = x2;
-    {
-      const int l = lb + (h + 1) * st;
-      if (last) F.q[m][l] = F.q[m][l] + x2; else v[l] = x2;
-    }
-    for (int p0 = h + 1; p0 < n; p0 += R) {
-      TF bv[R], bq[R];
+  }
+  __syncthreads();
+
+  // ---- phase 2
+  for (int t = tid; t < total; t += NT) {
+    int lq, p;
+    const int l = node(t, lq, p);
+    const int so = p * NLP + lq;
+    if (last) {
+      TF qv[4];
 #pragma unroll
-      for (int u = 0; u < R; ++u) {
-        const int p = p0 + u;
-        if (p < n) { bv[u] = v[lb + (p + 1) * st]; if (last) bq[u] = F.q[m][lb + (p + 1) * st]; }
-      }
+      for (int mm = 0; mm < 4; ++mm) qv[mm] = F.q[mm][l];
 #pragma unroll
-      for (int u = 0; u < R; ++u) {
-        const int p = p0 + u;
-        if (p < n) {
-          x = (bv[u] - off * x) / TF(dpr[n - 1 - p]);
-          if (last) F.q[m][lb + (p + 1) * st] = bq[u] + x; else v[lb + (p + 1) * st] = x;
-        }
-      }
+      for (int mm = 0; mm < 4; ++mm) F.q[mm][l] = qv[mm] + sv[mm * fs + so];
+    } else {
+#pragma unroll
+      for (int mm = 0; mm < 4; ++mm) dq[(long)mm * F.N + l] = sv[mm * fs + so];
     }
   }
 }

@@ -301,22 +301,28 @@ __global__ void __launch_bounds__(128, DESALM_KR_MINBLOCKS) k_resid(Lv<T, W> L, 
   }
 }
 
-// dtau on every node (src/rhs_daf_dtau.F90:85-117)
+// dtau on every node (src/rhs_daf_dtau.F90:85-117): the smallest of the
+// convective limits cfl / (|grad xi_d| dxi_d) and the viscous limits
+// vnn / ((1/Re + nu_t) dxi_d^2 g_dd), formed as 1 / (the largest of their
+// reciprocals) so that a node costs one division; equal to the reference's
+// minimum up to rounding.
 template <class T, class W>
 __global__ void k_dtau(Lv<T, W> L, Par P) {
   int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= L.N) return;
-  const T cfl = T(P.cfl1), vnn = T(P.vnn1), rei = T(1) / T(P.ren);
+  const T rcfl = T(1) / T(P.cfl1), rvnn = T(1) / T(P.vnn1), rei = T(1) / T(P.ren);
   const T dcsq = L.dc * L.dc, desq = L.de * L.de, dzsq = L.dz * L.dz;
   T g1 = L.csi[0][l] * L.csi[0][l] + L.csi[1][l] * L.csi[1][l] + L.csi[2][l] * L.csi[2][l];
   T g2 = L.eta[0][l] * L.eta[0][l] + L.eta[1][l] * L.eta[1][l] + L.eta[2][l] * L.eta[2][l];
   T g3 = L.zet[0][l] * L.zet[0][l] + L.zet[1][l] * L.zet[1][l] + L.zet[2][l] * L.zet[2][l];
-  T dti1 = cfl / sqrt(g1) / L.dc, dti2 = cfl / sqrt(g2) / L.de, dti3 = cfl / sqrt(g3) / L.dz;
   T ret = rei + L.nut[l];
-  T dtv1 = vnn / ret / dcsq / g1, dtv2 = vnn / ret / desq / g2, dtv3 = vnn / ret / dzsq / g3;
-  T m = dti1;
-  m = dmin(m, dti2); m = dmin(m, dti3); m = dmin(m, dtv1); m = dmin(m, dtv2); m = dmin(m, dtv3);
-  L.dtau[l] = m;
+  T m = sqrt(g1) * L.dc * rcfl;
+  m = dmax(m, sqrt(g2) * L.de * rcfl);
+  m = dmax(m, sqrt(g3) * L.dz * rcfl);
+  m = dmax(m, ret * dcsq * g1 * rvnn);
+  m = dmax(m, ret * desq * g2 * rvnn);
+  m = dmax(m, ret * dzsq * g3 * rvnn);
+  L.dtau[l] = T(1) / m;
 }
 
 }  // namespace desalm

@@ -264,9 +264,9 @@ __global__ void __launch_bounds__(128) k_sa_rhs(SaT<SW> S) {
 //            along the fastest global index), laid out [node][line];
 //   phase 1  thread (line, half) eliminates the upper half of its line
 //            top-down (SGTSV's no-interchange order; a would-swap row is
-//            counted in flags[0]) or the lower half bottom-up, the eliminated
-//            diagonal replacing ap; the halves meet in a 2x2 solve and
-//            back-substitute;
+//            counted in flags[0]) or the lower half bottom-up, the reciprocal
+//            of the eliminated diagonal replacing ap; the halves meet in a 2x2
+//            solve and back-substitute;
 //   phase 2  the solution goes back to rh, or, after the k sweep, into the
 //            update nu <- nu + (-nu + (nu_old + dnu)) / (1 + 1.5 dtev / dt)
 //            (src/des_eddy.F90:260-272).
@@ -309,42 +309,63 @@ __global__ void __launch_bounds__(2 * NL) k_sa_sweep4(SaT<SW> S) {
   cp_async_wait_all();
   __syncthreads();
 
-  // ---- phase 1
+  // ---- phase 1 (1/d replaces ap, so that back-substitution multiplies)
   const int li = tid % NL, half = tid / NL;
   const bool act = li < nl;
   const int h = n / 2;
   auto at = [&](int p) { return p * NLP + li; };
+  constexpr int R = 4;  // rows read ahead of the elimination chain
   int npiv = 0;
   if (act && half == 0) {
-    SW dprev = 0, duprev = 0, bprev = 0;
-    for (int p = 0; p < h; ++p) {
-      const SW aw = s_aw[at(p)], ap = s_ap[at(p)], ae = s_ae[at(p)], rr = s_rh[at(p)];
-      SW d;
-      if (p == 0) { d = ap; bprev = rr; }
-      else {
-        npiv += dabs(dprev) < dabs(aw);
-        const SW f = aw / dprev;
-        d = ap - f * duprev;
-        bprev = rr - f * bprev;
+    SW dprev = 0, rdprev = 0, duprev = 0, bprev = 0;
+    for (int p0 = 0; p0 < h; p0 += R) {
+      SW baw[R], bap[R], bae[R], brr[R];
+#pragma unroll
+      for (int u = 0; u < R; ++u)
+        if (p0 + u < h) { baw[u] = s_aw[at(p0 + u)]; bap[u] = s_ap[at(p0 + u)]; bae[u] = s_ae[at(p0 + u)]; brr[u] = s_rh[at(p0 + u)]; }
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int p = p0 + u;
+        if (p < h) {
+          SW d;
+          if (p == 0) { d = bap[u]; bprev = brr[u]; }
+          else {
+            npiv += dabs(dprev) < dabs(baw[u]);
+            const SW f = baw[u] * rdprev;
+            d = bap[u] - f * duprev;
+            bprev = brr[u] - f * bprev;
+          }
+          rdprev = sweep_rcp(d);
+          s_ap[at(p)] = rdprev; s_rh[at(p)] = bprev;
+          dprev = d; duprev = bae[u];
+        }
       }
-      s_ap[at(p)] = d; s_rh[at(p)] = bprev;
-      dprev = d; duprev = ae;
     }
     m_d[li] = dprev; m_c[li] = duprev; m_b[li] = bprev;
   } else if (act && half == 1) {
-    SW dprev = 0, awprev = 0, bprev = 0;
-    for (int p = n - 1; p >= h; --p) {
-      const SW aw = s_aw[at(p)], ap = s_ap[at(p)], ae = s_ae[at(p)], rr = s_rh[at(p)];
-      SW d;
-      if (p == n - 1) { d = ap; bprev = rr; }
-      else {
-        npiv += dabs(dprev) < dabs(ae);
-        const SW f = ae / dprev;
-        d = ap - f * awprev;
-        bprev = rr - f * bprev;
+    SW dprev = 0, rdprev = 0, awprev = 0, bprev = 0;
+    for (int p0 = n - 1; p0 >= h; p0 -= R) {
+      SW baw[R], bap[R], bae[R], brr[R];
+#pragma unroll
+      for (int u = 0; u < R; ++u)
+        if (p0 - u >= h) { baw[u] = s_aw[at(p0 - u)]; bap[u] = s_ap[at(p0 - u)]; bae[u] = s_ae[at(p0 - u)]; brr[u] = s_rh[at(p0 - u)]; }
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int p = p0 - u;
+        if (p >= h) {
+          SW d;
+          if (p == n - 1) { d = bap[u]; bprev = brr[u]; }
+          else {
+            npiv += dabs(dprev) < dabs(bae[u]);
+            const SW f = bae[u] * rdprev;
+            d = bap[u] - f * awprev;
+            bprev = brr[u] - f * bprev;
+          }
+          rdprev = sweep_rcp(d);
+          s_ap[at(p)] = rdprev; s_rh[at(p)] = bprev;
+          dprev = d; awprev = baw[u];
+        }
       }
-      s_ap[at(p)] = d; s_rh[at(p)] = bprev;
-      dprev = d; awprev = aw;
     }
     n_d[li] = dprev; n_c[li] = awprev; n_b[li] = bprev;
   }
@@ -357,16 +378,26 @@ __global__ void __launch_bounds__(2 * NL) k_sa_sweep4(SaT<SW> S) {
     if (half == 0) {
       SW x = (b1 * d2 - u1 * b2) / det;
       s_rh[at(h - 1)] = x;
-      for (int p = h - 2; p >= 0; --p) {
-        x = (s_rh[at(p)] - s_ae[at(p)] * x) / s_ap[at(p)];
-        s_rh[at(p)] = x;
+      for (int p0 = h - 2; p0 >= 0; p0 -= R) {
+        SW bae[R], brr[R], brd[R];
+#pragma unroll
+        for (int u = 0; u < R; ++u)
+          if (p0 - u >= 0) { bae[u] = s_ae[at(p0 - u)]; brr[u] = s_rh[at(p0 - u)]; brd[u] = s_ap[at(p0 - u)]; }
+#pragma unroll
+        for (int u = 0; u < R; ++u)
+          if (p0 - u >= 0) { x = (brr[u] - bae[u] * x) * brd[u]; s_rh[at(p0 - u)] = x; }
       }
     } else {
       SW x = (d1 * b2 - l2 * b1) / det;
       s_rh[at(h)] = x;
-      for (int p = h + 1; p < n; ++p) {
-        x = (s_rh[at(p)] - s_aw[at(p)] * x) / s_ap[at(p)];
-        s_rh[at(p)] = x;
+      for (int p0 = h + 1; p0 < n; p0 += R) {
+        SW baw[R], brr[R], brd[R];
+#pragma unroll
+        for (int u = 0; u < R; ++u)
+          if (p0 + u < n) { baw[u] = s_aw[at(p0 + u)]; brr[u] = s_rh[at(p0 + u)]; brd[u] = s_ap[at(p0 + u)]; }
+#pragma unroll
+        for (int u = 0; u < R; ++u)
+          if (p0 + u < n) { x = (brr[u] - baw[u] * x) * brd[u]; s_rh[at(p0 + u)] = x; }
       }
     }
   }

@@ -47,13 +47,11 @@ namespace desalm {
 //            memory exactly as the two-ended sweep does (same operations,
 //            same order); the halves meet in the 2x2 middle solve and
 //            back-substitute; the eliminated diagonal never leaves the SM;
-//   phase 2  every node of the slab gets the next modal transform (or the
-//            update) from the solved values in shared memory and writes its
-//            four results once.
+//   phase 2  the solved values go back to wk; k_xform then applies the next
+//            modal transform (or the update) per node at full occupancy.
 // Shared memory: 10 fields (tc, hc, r[4], d[4]) of slab_fs(n + 2, NL + 1)
 // elements of W.
 // ---------------------------------------------------------------------------
-DESALM_HD inline int slab_fs(int np, int nlp) { return ((np * nlp + 31) / 32) * 32 + 16; }
 
 template <class T, class W, int DIR, int NL>
 __global__ void __launch_bounds__(8 * NL) k_sweep4(Lv<T, W> L, Par P, int blo, int bhi) {
@@ -142,54 +140,76 @@ __global__ void __launch_bounds__(8 * NL) k_sweep4(Lv<T, W> L, Par P, int blo, i
   };
   const int h = n / 2;  // rows 0..h-1 top (nodes 1..h), h..n-1 bottom (nodes h+1..n)
   int npiv = 0, nzero = 0;
+  constexpr int R = 4;  // rows whose shared-memory operands are read ahead of the elimination chain
+  // sd holds 1/d of every eliminated row, so that back-substitution multiplies
   if (act && half == 0) {
     const W bwm = sbw[li][m];
     W hw = chc[at(0)], hcur = chc[at(1)];
-    W dprev = 0, duprev = 0, bprev = 0;
-    for (int p = 1; p <= h; ++p) {
-      const W t = ctc[at(p)], hn = chc[at(p + 1)];
-      W aw, ae;
-      coef(t, hw, hn, aw, ae);
-      const W ap = W(1) + W(2) * t;
-      W rr = r[at(p)];
-      W d;
-      if (p == 1) { rr = rr - aw * bwm; d = ap; bprev = rr; }
-      else {
-        npiv += dabs(dprev) < dabs(aw);
-        const W f = aw / dprev;
-        d = ap - f * duprev;
-        bprev = rr - f * bprev;
+    W dprev = 0, rdprev = 0, duprev = 0, bprev = 0;
+    for (int p0 = 1; p0 <= h; p0 += R) {
+      W bt[R], bh[R], br[R];
+#pragma unroll
+      for (int u = 0; u < R; ++u)
+        if (p0 + u <= h) { bt[u] = ctc[at(p0 + u)]; bh[u] = chc[at(p0 + u + 1)]; br[u] = r[at(p0 + u)]; }
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int p = p0 + u;
+        if (p <= h) {
+          W aw, ae;
+          coef(bt[u], hw, bh[u], aw, ae);
+          const W ap = W(1) + W(2) * bt[u];
+          W rr = br[u];
+          W d;
+          if (p == 1) { rr = rr - aw * bwm; d = ap; bprev = rr; }
+          else {
+            npiv += dabs(dprev) < dabs(aw);
+            const W f = aw * rdprev;
+            d = ap - f * duprev;
+            bprev = rr - f * bprev;
+          }
+          nzero += d == W(0);
+          rdprev = sweep_rcp(d);
+          sd[at(p)] = rdprev;
+          r[at(p)] = bprev;
+          dprev = d; duprev = ae;
+          hw = hcur; hcur = bh[u];
+        }
       }
-      nzero += d == W(0);
-      sd[at(p)] = d;
-      r[at(p)] = bprev;
-      dprev = d; duprev = ae;
-      hw = hcur; hcur = hn;
     }
     mt_d[li][m] = dprev; mt_u[li][m] = duprev; mt_b[li][m] = bprev;
   } else if (act && half == 1) {
     const W bem = sbe[li][m];
     W he = chc[at(n + 1)], hcur = chc[at(n)];
-    W dprev = 0, awprev = 0, bprev = 0;
-    for (int p = n; p > h; --p) {
-      const W t = ctc[at(p)], hwv = chc[at(p - 1)];
-      W aw, ae;
-      coef(t, hwv, he, aw, ae);
-      const W ap = W(1) + W(2) * t;
-      W rr = r[at(p)];
-      W d;
-      if (p == n) { rr = rr - ae * bem; d = ap; bprev = rr; }
-      else {
-        npiv += dabs(dprev) < dabs(ae);
-        const W f = ae / dprev;
-        d = ap - f * awprev;
-        bprev = rr - f * bprev;
+    W dprev = 0, rdprev = 0, awprev = 0, bprev = 0;
+    for (int p0 = n; p0 > h; p0 -= R) {
+      W bt[R], bh[R], br[R];
+#pragma unroll
+      for (int u = 0; u < R; ++u)
+        if (p0 - u > h) { bt[u] = ctc[at(p0 - u)]; bh[u] = chc[at(p0 - u - 1)]; br[u] = r[at(p0 - u)]; }
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int p = p0 - u;
+        if (p > h) {
+          W aw, ae;
+          coef(bt[u], bh[u], he, aw, ae);
+          const W ap = W(1) + W(2) * bt[u];
+          W rr = br[u];
+          W d;
+          if (p == n) { rr = rr - ae * bem; d = ap; bprev = rr; }
+          else {
+            npiv += dabs(dprev) < dabs(ae);
+            const W f = ae * rdprev;
+            d = ap - f * awprev;
+            bprev = rr - f * bprev;
+          }
+          nzero += d == W(0);
+          rdprev = sweep_rcp(d);
+          sd[at(p)] = rdprev;
+          r[at(p)] = bprev;
+          dprev = d; awprev = aw;
+          he = hcur; hcur = bh[u];
+        }
       }
-      nzero += d == W(0);
-      sd[at(p)] = d;
-      r[at(p)] = bprev;
-      dprev = d; awprev = aw;
-      he = hcur; hcur = hwv;
     }
     mb_d[li][m] = dprev; mb_l[li][m] = awprev; mb_b[li][m] = bprev;
   }
@@ -205,104 +225,103 @@ __global__ void __launch_bounds__(8 * NL) k_sweep4(Lv<T, W> L, Par P, int blo, i
     if (half == 0) {
       W x = (b1 * d2 - u1 * b2) / det;
       r[at(h)] = x;
-      for (int p = h - 1; p >= 1; --p) {
-        W aw, ae;
-        coef(ctc[at(p)], W(0), chc[at(p + 1)], aw, ae);
-        x = (r[at(p)] - ae * x) / sd[at(p)];
-        r[at(p)] = x;
+      for (int p0 = h - 1; p0 >= 1; p0 -= R) {
+        W bt[R], bh[R], br[R], bd[R];
+#pragma unroll
+        for (int u = 0; u < R; ++u)
+          if (p0 - u >= 1) { bt[u] = ctc[at(p0 - u)]; bh[u] = chc[at(p0 - u + 1)]; br[u] = r[at(p0 - u)]; bd[u] = sd[at(p0 - u)]; }
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+          if (p0 - u >= 1) {
+            W aw, ae;
+            coef(bt[u], W(0), bh[u], aw, ae);
+            x = (br[u] - ae * x) * bd[u];
+            r[at(p0 - u)] = x;
+          }
+        }
       }
     } else {
       W x = (d1 * b2 - l2 * b1) / det;
       r[at(h + 1)] = x;
-      for (int p = h + 2; p <= n; ++p) {
-        W aw, ae;
-        coef(ctc[at(p)], chc[at(p - 1)], W(0), aw, ae);
-        x = (r[at(p)] - aw * x) / sd[at(p)];
-        r[at(p)] = x;
+      for (int p0 = h + 2; p0 <= n; p0 += R) {
+        W bt[R], bh[R], br[R], bd[R];
+#pragma unroll
+        for (int u = 0; u < R; ++u)
+          if (p0 + u <= n) { bt[u] = ctc[at(p0 + u)]; bh[u] = chc[at(p0 + u - 1)]; br[u] = r[at(p0 + u)]; bd[u] = sd[at(p0 + u)]; }
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+          if (p0 + u <= n) {
+            W aw, ae;
+            coef(bt[u], bh[u], W(0), aw, ae);
+            x = (br[u] - aw * x) * bd[u];
+            r[at(p0 + u)] = x;
+          }
+        }
       }
     }
   }
   __syncthreads();
 
-  // ---- phase 2: per-node transform in the sweep precision W, U nodes per
-  // thread at a time: all their global reads are issued before any store
+  // ---- phase 2: the solved values back to wk (the modal transform follows
+  // in k_xform, at full occupancy)
   const int total = nl * n;
-  constexpr int U = 4;
-  const T* const* m1 = DIR == 0 ? L.csi : (DIR == 1 ? L.eta : L.zet);  // forward matrix metrics
-  const T* const* m2 = DIR == 0 ? L.eta : L.zet;                       // inverse matrix metrics
-  for (int t0 = tid; t0 < total; t0 += NT * U) {
-    int lnode[U], aan[U], pn[U];
-    W a1[U][3], a2[U][3], sgv[U];
+  for (int t = tid; t < total; t += NT) {
+    int lq, p;
+    if (DIR == 0) { lq = t / n; p = t - lq * n; }
+    else { p = t / nl; lq = t - p * nl; }
+    const int l = base + (a0 + lq) * sa + (p + 1) * st;
+    const int so = (p + 1) * NLP + lq;
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int t = t0 + u * NT;
-      lnode[u] = -1;
-      aan[u] = a0; pn[u] = 0;
-      if (t < total) {
-        int lq, p;
-        if (DIR == 0) { lq = t / n; p = t - lq * n; }
-        else { p = t / nl; lq = t - p * nl; }
-        aan[u] = a0 + lq;
-        pn[u] = p;
-        const int l = base + aan[u] * sa + (p + 1) * st;
-        lnode[u] = l;
-        sgv[u] = __ldg(L.sig + l);
+    for (int q = 0; q < 4; ++q) L.wk[q][l] = s_r[q * fs + so];
+  }
+}
+
+// Per-node step after a line sweep, in the sweep precision W, one thread per
+// interior node: after the i sweep the semi-explicit rows of the j faces are
+// copied out (rows 2, 3, jm-1, jm-2) and wk <- N1^-1 wk = Mb^-1 (Ma wk);
+// after the j sweep the k-face rows are copied and wk <- N2^-1 wk =
+// Mc^-1 (Mb wk); after the k sweep q <- q + Mc wk (src/rhs_diag_solver.F90:
+// 240-258, 416-434, 600-633; src/solver_daf.F90:409-418).
+template <class T, class W, int DIR>
+__global__ void __launch_bounds__(128) k_xform(Lv<T, W> L) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int k = blockIdx.z + 1;
+  if (i > L.im - 2 || j > L.jm - 2) return;
+  const int l = i + L.sj * j + L.sk * k;
+  W xv[4];
 #pragma unroll
-        for (int x = 0; x < 3; ++x) a1[u][x] = W(__ldg(m1[x] + l));
-        if (DIR < 2)
+  for (int q = 0; q < 4; ++q) xv[q] = L.wk[q][l];
+  const W sg = L.sig[l];
+  W y[4], z[4];
+  if (DIR == 0) {
+    const int S = L.im * L.km, o = i + L.im * k;
+    const int tgt[4] = {1, 2, L.jm - 2, L.jm - 3};
 #pragma unroll
-          for (int x = 0; x < 3; ++x) a2[u][x] = W(__ldg(m2[x] + l));
-      }
-    }
-    T qv[U][4];
-    if (DIR == 2) {
+    for (int s = 0; s < 4; ++s)
+      if (j == tgt[s])
 #pragma unroll
-      for (int u = 0; u < U; ++u)
-        if (lnode[u] >= 0)
+        for (int q = 0; q < 4; ++q) L.bj[(s * 4 + q) * S + o] = xv[q];
+    mfwd_apply<W>(W(L.csi[0][l]), W(L.csi[1][l]), W(L.csi[2][l]), sg, xv, y);
+    minv_apply<W>(W(L.eta[0][l]), W(L.eta[1][l]), W(L.eta[2][l]), sg, y, z);
 #pragma unroll
-          for (int q = 0; q < 4; ++q) qv[u][q] = L.q[q][lnode[u]];
-    }
+    for (int q = 0; q < 4; ++q) L.wk[q][l] = z[q];
+  } else if (DIR == 1) {
+    const int S = L.im * L.jm, o = i + L.im * j;
+    const int tgt[4] = {1, 2, L.km - 2, L.km - 3};
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      if (lnode[u] < 0) continue;
-      const int l = lnode[u], p = pn[u], aa = aan[u];
-      const int so = (p + 1) * NLP + (aa - a0);
-      W xv[4];
+    for (int s = 0; s < 4; ++s)
+      if (k == tgt[s])
 #pragma unroll
-      for (int q = 0; q < 4; ++q) xv[q] = s_r[q * fs + so];
-      W y[4], z[4];
-      if (DIR == 0) {
-        const int S = L.im * L.km, o = (p + 1) + L.im * b;
-        const int tgt[4] = {1, 2, L.jm - 2, L.jm - 3};
+        for (int q = 0; q < 4; ++q) L.bk[(s * 4 + q) * S + o] = xv[q];
+    mfwd_apply<W>(W(L.eta[0][l]), W(L.eta[1][l]), W(L.eta[2][l]), sg, xv, y);
+    minv_apply<W>(W(L.zet[0][l]), W(L.zet[1][l]), W(L.zet[2][l]), sg, y, z);
 #pragma unroll
-        for (int s = 0; s < 4; ++s)
-          if (aa == tgt[s])
+    for (int q = 0; q < 4; ++q) L.wk[q][l] = z[q];
+  } else {
+    mfwd_apply<W>(W(L.zet[0][l]), W(L.zet[1][l]), W(L.zet[2][l]), sg, xv, y);
 #pragma unroll
-            for (int q = 0; q < 4; ++q) L.bj[(s * 4 + q) * S + o] = xv[q];
-        // N1^-1 x = Mb^-1 (Ma x)
-        mfwd_apply<W>(a1[u][0], a1[u][1], a1[u][2], sgv[u], xv, y);
-        minv_apply<W>(a2[u][0], a2[u][1], a2[u][2], sgv[u], y, z);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) L.wk[q][l] = z[q];
-      } else if (DIR == 1) {
-        const int S = L.im * L.jm, o = aa + L.im * (p + 1);
-        const int tgt[4] = {1, 2, L.km - 2, L.km - 3};
-#pragma unroll
-        for (int s = 0; s < 4; ++s)
-          if (b == tgt[s])
-#pragma unroll
-            for (int q = 0; q < 4; ++q) L.bk[(s * 4 + q) * S + o] = xv[q];
-        // N2^-1 x = Mc^-1 (Mb x)
-        mfwd_apply<W>(a1[u][0], a1[u][1], a1[u][2], sgv[u], xv, y);
-        minv_apply<W>(a2[u][0], a2[u][1], a2[u][2], sgv[u], y, z);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) L.wk[q][l] = z[q];
-      } else {
-        mfwd_apply<W>(a1[u][0], a1[u][1], a1[u][2], sgv[u], xv, y);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) L.q[q][l] = qv[u][q] + T(y[q]);
-      }
-    }
+    for (int q = 0; q < 4; ++q) L.q[q][l] = L.q[q][l] + T(y[q]);
   }
 }
 

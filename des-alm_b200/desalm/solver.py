@@ -78,7 +78,8 @@ def lib():
 
 # kernel classes reported by desalm_kernel_stats (order of the C enum)
 KERNEL_CLASSES = ["dtau", "resid", "sweep_i", "sweep_j", "sweep_k", "recalc", "bcond", "pfix",
-                  "nlevel", "prolong", "rsmooth", "norm", "sa_rhs", "sa_sweep", "sa_bc", "misc"]
+                  "nlevel", "prolong", "rsmooth", "norm", "sa_rhs", "sa_sweep", "sa_bc",
+                  "xform_i", "xform_j", "xform_k", "sa_aux", "misc"]
 
 
 def _p(a):
