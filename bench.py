@@ -245,7 +245,24 @@ def run_ours(args, rank, world, dist):
         S64.mg_driver()
     sec64, reps64 = timed_steps(S64, args.steps, S64.mg_driver)
     iters64 = [r["iterations"] for r in reps64]
+    st64 = S64.get_state()
     del S64
+
+    # ---- per-field error of the mixed path against the FP64 path: MIXED with
+    # the same q^n guess, the same number of physical steps from the same state
+    caseq, _, _, _ = build_case(args.case, abi.MIXED, abi.PRED_QN)
+    SQ = Solver(caseq)
+    SQ.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
+    SQ.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
+    for _ in range(args.warmup + args.steps):
+        SQ.mg_driver()
+    stq = SQ.get_state()
+    del SQ
+    a = np.asarray(stq["q"]).reshape(-1, 5)
+    b = np.asarray(st64["q"]).reshape(-1, 5)
+    names = ["p", "u", "v", "w", "nu_tilde"] if case.turbulence else ["p", "u", "v", "w"]
+    field_err = {nm: float(np.linalg.norm(a[:, m] - b[:, m]) / max(1e-300, np.linalg.norm(b[:, m])))
+                 for m, nm in enumerate(names)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -266,6 +283,9 @@ def run_ours(args, rank, world, dist):
                    "parallelism": "replicas only (%d independent replicas)" % world},
         "fp64_plain": {"value": sec64, "unit": UNIT, "pseudo_iterations_per_step": iters64,
                        "speedup_mixed_vs_fp64": sec64 / sec},
+        "mixed_vs_fp64_rel_l2": {"fields": field_err,
+                                 "how": "relative L2 over all nodes of the state after %d physical steps from the same "
+                                        "initial state, both with the q^n guess" % (args.warmup + args.steps)},
         "cell_updates_per_s": sum_over_ranks(cell_updates),
         "e2e": {"value": e2e_sec, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),

@@ -67,6 +67,15 @@ struct Par {
 // start on different banks.
 DESALM_HD inline int slab_fs(int np, int nlp) { return ((np * nlp + 31) / 32) * 32 + 16; }
 
+// Programmatic dependent launch: when a kernel is launched with programmatic
+// stream serialisation, pdl_wait() blocks until the grids it depends on have
+// completed and their writes are visible (it must come before the first
+// global-memory access), and pdl_trigger() lets the next grid in the stream
+// be scheduled once every CTA of this one has started.  Without that launch
+// attribute both are no-ops; every kernel of the library calls both first.
+DESALM_DEV void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+DESALM_DEV void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
 template <class T> DESALM_DEV T dabs(T x) { return x < T(0) ? -x : x; }
 
 // Reciprocal used by the line eliminations: in FP32 (the sweeps of MIXED mode,

@@ -13,6 +13,7 @@
 #include <string>
 #include <vector>
 #include <algorithm>
+#include <utility>
 
 #include "desalm.h"
 #include "common.cuh"
@@ -22,6 +23,28 @@
 #include "sa.cuh"
 
 using namespace desalm;
+
+// Kernel launch through cudaLaunchKernelEx.  Every kernel calls pdl_wait()
+// before its first global-memory access, so any of them may be launched with
+// programmatic stream serialisation (its launch overlapping the tail of the
+// grid before it); on the channel workload that measured about 3% slower per
+// physical step than plain stream order (0.511 against 0.497 s), so it is off.
+// Failures are reported by the next cudaGetLastError().
+constexpr int kProgrammaticLaunch = 0;
+template <typename... KArgs, typename... Args>
+cudaError_t launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = kProgrammaticLaunch;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 namespace {
 
@@ -41,6 +64,8 @@ struct ConvPar {
 // state and sets the while-node condition of the graph.
 __global__ void k_conv(const double* part, int nblk, DevConv* st, const int* flags, ConvPar cp,
                        cudaGraphConditionalHandle h) {
+  pdl_wait();
+  pdl_trigger();
   double sums[5];
   desalm::block_sum5(part, nblk, sums);   // every thread gets the sums
   if (threadIdx.x != 0) return;
@@ -107,6 +132,8 @@ struct desalm_ctx {
   int part_blocks = 0;
   double* norm = nullptr;     // device [5]
   double* h_norm = nullptr;   // pinned host [5]
+  double* stage = nullptr;    // device staging of one host state array, 5 N (component-fastest)
+  double** ftab = nullptr;    // device table of the fine level's q[5], qn[5], qnm1[5] field pointers
   int* flags = nullptr;       // device [2]
   SaWork sa{};
   // per-kernel CUDA-event timing (desalm_profile) and launch counter
@@ -217,6 +244,13 @@ int alloc_level(desalm_ctx* ctx, Level& G, Lv<T, W>& L) {
   return 0;
 }
 
+// Shared memory of the slab kernels (line sweeps, SA sweeps, rsmooth): the
+// widest slab that leaves room for two CTAs per SM is used, else the widest
+// that fits one (below the 227 KB opt-in less the kernels' static shared
+// memory).
+constexpr size_t kSlabTwoPerSm = 110 * 1024;
+constexpr size_t kSlabMax = 220 * 1024;
+
 int check_case(desalm_ctx* ctx, const desalm_case& c) {
   auto bad = [&](const char* why) { ctx->err = why; return DESALM_EINVAL; };
   if (c.ng < 1 || c.ng > 4) return bad("ng must be 1..4");
@@ -238,6 +272,14 @@ int check_case(desalm_ctx* ctx, const desalm_case& c) {
     if (im < 5 || jm < 5 || km < 5) return bad("coarsest level must keep >= 5 nodes per direction");
   }
   if ((long)c.im * c.jm * c.km * 4 >= (1L << 31)) return bad("grid too large for 32-bit indexing");
+  // the narrowest slab of every line solve must fit: DAF sweep 4 lines of
+  // 10 W-fields, rsmooth 4 lines of 4 FP64 fields, SA sweep 8 lines of 4 W-fields
+  const size_t wb = c.precision_mode == DESALM_FP64 ? 8 : 4;
+  for (int n : {c.im - 2, c.jm - 2, c.km - 2})
+    if ((size_t)10 * slab_fs(n + 2, 5) * wb > kSlabMax || (size_t)4 * slab_fs(n, 5) * 8 > kSlabMax ||
+        (size_t)4 * slab_fs(n, 9) * wb > kSlabMax)
+      return bad("a grid line is too long for the shared-memory line solves (at most 554 interior nodes in "
+                 "FP64 mode, 1118 in MIXED mode)");
   return 0;
 }
 
@@ -283,8 +325,6 @@ dim3 grid_interior(const Lv<T, W>& L) { return dim3(cdiv(L.im - 2, 32), cdiv(L.j
 // One DAF line sweep as k_sweep4 with the widest slab (lines per CTA) whose
 // shared memory leaves room for two CTAs per SM, else the widest that fits
 // one CTA per SM.
-constexpr size_t kSlabTwoPerSm = 110 * 1024;
-constexpr size_t kSlabMax = 220 * 1024;  // below the 227 KB opt-in less the kernels' static shared memory
 template <class W>
 size_t slab_bytes(int n, int nl) { return (size_t)10 * slab_fs(n + 2, nl + 1) * sizeof(W); }
 
@@ -298,10 +338,10 @@ int sweep4_nl(desalm_ctx* ctx, Lv<T, W>& L, const Par& P, int lvl, int blo, int 
   const int cls = DIR == 0 ? KC_SWEEP_I : (DIR == 1 ? KC_SWEEP_J : KC_SWEEP_K);
   const double nin = double(amax) * n * nb;
   cudaStream_t s = ctx->stream;
-  LAUNCH(cls, lvl, nin, k_sweep4<T, W, DIR, NL><<<dim3(cdiv(amax, NL), nb), 8 * NL, bytes, s>>>(L, P, blo, bhi));
+  LAUNCH(cls, lvl, nin, launch_k(k_sweep4<T, W, DIR, NL>, dim3(cdiv(amax, NL), nb), 8 * NL, bytes, s, L, P, blo, bhi));
   CKL();
   const int xcls = DIR == 0 ? KC_XFORM_I : (DIR == 1 ? KC_XFORM_J : KC_XFORM_K);
-  LAUNCH(xcls, lvl, nin, k_xform<T, W, DIR><<<grid_interior(L), blk3(), 0, s>>>(L));
+  LAUNCH(xcls, lvl, nin, launch_k(k_xform<T, W, DIR>, grid_interior(L), blk3(), 0, s, L));
   CKL();
   return 0;
 }
@@ -350,7 +390,7 @@ int launch_daf(desalm_ctx* ctx, Lv<T, W>& L, Level& G, int n, int recalc, int it
   const desalm_case& c = ctx->c;
   cudaStream_t s = ctx->stream;
   if (!G.dtau_valid) {
-    LAUNCH(KC_DTAU, n, L.N, k_dtau<T, W><<<cdiv(L.N, 256), 256, 0, s>>>(L, P));
+    LAUNCH(KC_DTAU, n, L.N, launch_k(k_dtau<T, W>, cdiv(L.N, 256), 256, 0, s, L, P));
     CKL();
     G.dtau_valid = true;
   }
@@ -358,7 +398,7 @@ int launch_daf(desalm_ctx* ctx, Lv<T, W>& L, Level& G, int n, int recalc, int it
   const int upwind = fine ? 2 : 1;
   const int bback = fine && c.btype[0] != 5;
   const double nin = double(L.im - 2) * (L.jm - 2) * (L.km - 2);
-  LAUNCH(KC_RESID, n, nin, k_resid<T, W, 0><<<grid_interior(L), blk3(), 0, s>>>(L, P, upwind, itr == 1 ? 1 : 0, n > 0 ? 1 : 0, bback));
+  LAUNCH(KC_RESID, n, nin, launch_k(k_resid<T, W, 0>, grid_interior(L), blk3(), 0, s, L, P, upwind, itr == 1 ? 1 : 0, n > 0 ? 1 : 0, bback));
   CKL();
   RET((launch_sweep<T, W, 0>(ctx, L, P, n, bback, 0)));
   RET((launch_sweep<T, W, 1>(ctx, L, P, n, fine && c.btype[2] != 5, fine && c.btype[3] != 5)));
@@ -370,7 +410,7 @@ template <class T, class W>
 int launch_recalc(desalm_ctx* ctx, Lv<T, W>& L, int n) {
   Par P = ctx->par;
   P.fine = (n == 0);
-  LAUNCH(KC_RECALC, n, double(L.im - 2) * (L.jm - 2) * (L.km - 2), k_resid<T, W, 1><<<grid_interior(L), blk3(), 0, ctx->stream>>>(L, P, n == 0 ? 2 : 1, 0, n > 0 ? 1 : 0, 0));
+  LAUNCH(KC_RECALC, n, double(L.im - 2) * (L.jm - 2) * (L.km - 2), launch_k(k_resid<T, W, 1>, grid_interior(L), blk3(), 0, ctx->stream, L, P, n == 0 ? 2 : 1, 0, n > 0 ? 1 : 0, 0));
   CKL();
   return 0;
 }
@@ -381,17 +421,17 @@ int launch_bcond(desalm_ctx* ctx, Lv<T, W>& L) {
   P.fine = 1;
   cudaStream_t s = ctx->stream;
   const T* rat = (const T*)ctx->rat;
-  LAUNCH(KC_BCOND, 0, 2.0 * L.jm * L.km, k_bcond<T, W, 0><<<dim3(cdiv(L.jm, 64), L.km), 64, 0, s>>>(L, P, rat, ctx->ratdim));
+  LAUNCH(KC_BCOND, 0, 2.0 * L.jm * L.km, launch_k(k_bcond<T, W, 0>, dim3(cdiv(L.jm, 64), L.km), 64, 0, s, L, P, rat, ctx->ratdim));
   CKL();
-  LAUNCH(KC_BCOND, 0, 2.0 * L.im * L.km, k_bcond<T, W, 1><<<dim3(cdiv(L.im, 64), L.km), 64, 0, s>>>(L, P, rat, ctx->ratdim));
+  LAUNCH(KC_BCOND, 0, 2.0 * L.im * L.km, launch_k(k_bcond<T, W, 1>, dim3(cdiv(L.im, 64), L.km), 64, 0, s, L, P, rat, ctx->ratdim));
   CKL();
-  LAUNCH(KC_BCOND, 0, 2.0 * L.im * L.jm, k_bcond<T, W, 2><<<dim3(cdiv(L.im, 64), L.jm), 64, 0, s>>>(L, P, rat, ctx->ratdim));
+  LAUNCH(KC_BCOND, 0, 2.0 * L.im * L.jm, launch_k(k_bcond<T, W, 2>, dim3(cdiv(L.im, 64), L.jm), 64, 0, s, L, P, rat, ctx->ratdim));
   CKL();
   const desalm_case& c = ctx->c;
   int lfix = (c.ifix - 1) + L.sj * (c.jfix - 1) + L.sk * (c.kfix - 1);
-  LAUNCH(KC_PFIX, 0, 1, k_pfix_read<T, W><<<1, 1, 0, s>>>(L, lfix, (T*)ctx->pfix));
+  LAUNCH(KC_PFIX, 0, 1, launch_k(k_pfix_read<T, W>, 1, 1, 0, s, L, lfix, (T*)ctx->pfix));
   CKL();
-  LAUNCH(KC_PFIX, 0, L.N, k_pfix_sub<T, W><<<cdiv(L.N, 256), 256, 0, s>>>(L, (const T*)ctx->pfix));
+  LAUNCH(KC_PFIX, 0, L.N, launch_k(k_pfix_sub<T, W>, cdiv(L.N, 256), 256, 0, s, L, (const T*)ctx->pfix));
   CKL();
   return 0;
 }
@@ -399,7 +439,7 @@ int launch_bcond(desalm_ctx* ctx, Lv<T, W>& L) {
 template <class TF, class WF, class TC, class WC>
 int launch_nlevel(desalm_ctx* ctx, Lv<TF, WF>& F, Lv<TC, WC>& C) {
   const desalm_case& c = ctx->c;
-  LAUNCH(KC_NLEVEL, 0, double(C.N), k_nlevel<TF, WF, TC, WC><<<dim3(cdiv(C.im, 32), cdiv(C.jm, 4), C.km), dim3(32, 4, 1), 0, ctx->stream>>>(F, C, c.icrs, c.jcrs, c.kcrs));
+  LAUNCH(KC_NLEVEL, 0, double(C.N), launch_k(k_nlevel<TF, WF, TC, WC>, dim3(cdiv(C.im, 32), cdiv(C.jm, 4), C.km), dim3(32, 4, 1), 0, ctx->stream, F, C, c.icrs, c.jcrs, c.kcrs));
   CKL();
   return 0;
 }
@@ -413,7 +453,7 @@ int rsmooth_nl(desalm_ctx* ctx, Lv<TF, WF>& F, TF* dq, Level& G, double e, int l
   const int amax = DIR == 0 ? F.jm - 2 : F.im - 2;
   const int n = DIR == 0 ? F.im - 2 : (DIR == 1 ? F.jm - 2 : F.km - 2);
   const int nb = DIR == 2 ? F.jm - 2 : F.km - 2;
-  LAUNCH(KC_RSMOOTH, 0, nin, k_rsmooth4<TF, WF, DIR, NL><<<dim3(cdiv(amax, NL), nb), 8 * NL, rs_slab_bytes<TF>(n, NL), ctx->stream>>>(
+  LAUNCH(KC_RSMOOTH, 0, nin, launch_k(k_rsmooth4<TF, WF, DIR, NL>, dim3(cdiv(amax, NL), nb), 8 * NL, rs_slab_bytes<TF>(n, NL), ctx->stream, 
                                  F, dq, G.fac[DIR], G.dpr[DIR], e, last));
   CKL();
   return 0;
@@ -434,7 +474,7 @@ int launch_prolong(desalm_ctx* ctx, Lv<TF, WF>& F, Lv<TC, WC>& C, Level& G) {
   cudaStream_t s = ctx->stream;
   TF* dq = (TF*)G.dq[0];
   const double nin = double(F.im - 2) * (F.jm - 2) * (F.km - 2);
-  LAUNCH(KC_PROLONG, 0, nin, k_prolong_interp<TF, WF, TC, WC><<<grid_interior(F), blk3(), 0, s>>>(F, C, dq, c.icrs, c.jcrs, c.kcrs));
+  LAUNCH(KC_PROLONG, 0, nin, launch_k(k_prolong_interp<TF, WF, TC, WC>, grid_interior(F), blk3(), 0, s, F, C, dq, c.icrs, c.jcrs, c.kcrs));
   CKL();
   RET((rsmooth<TF, WF, 0>(ctx, F, dq, G, c.ep[1][0], 0, nin)));
   RET((rsmooth<TF, WF, 1>(ctx, F, dq, G, c.ep[1][1], 0, nin)));
@@ -447,9 +487,9 @@ int launch_norm(desalm_ctx* ctx, Lv<T, W>& L, int copy, double* out) {
   cudaStream_t s = ctx->stream;
   long total = (long)(L.im - 2) * (L.jm - 2) * (L.km - 2);
   int nb = (int)std::min<long>(ctx->part_blocks, std::max<long>(1, cdiv(total, 256)));
-  LAUNCH(KC_NORM, 0, double(total), k_norm_partial<T, W><<<nb, 256, 0, s>>>(L, ctx->part, 5, copy));
+  LAUNCH(KC_NORM, 0, double(total), launch_k(k_norm_partial<T, W>, nb, 256, 0, s, L, ctx->part, 5, copy));
   CKL();
-  LAUNCH(KC_NORM, 0, 0, k_norm_final<<<1, 256, 0, s>>>(ctx->part, nb, ctx->norm));
+  LAUNCH(KC_NORM, 0, 0, launch_k(k_norm_final, 1, 256, 0, s, ctx->part, nb, ctx->norm));
   CKL();
   CK(cudaMemcpyAsync(ctx->h_norm, ctx->norm, 5 * sizeof(double), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
@@ -533,8 +573,8 @@ int do_norm(desalm_ctx* ctx, int n, int copy, double* out) {
 int refresh_rj(desalm_ctx* ctx, int n) {
   Level& G = ctx->L[n];
   cudaStream_t s = ctx->stream;
-  if (kind_of(ctx, n) == K_DD) k_recip<double><<<cdiv(G.N, 256), 256, 0, s>>>((double*)G.dd.rj, G.dd.aj, G.N);
-  else k_recip<double><<<cdiv(G.N, 256), 256, 0, s>>>((double*)G.df.rj, G.df.aj, G.N);
+  if (kind_of(ctx, n) == K_DD) launch_k(k_recip<double>, cdiv(G.N, 256), 256, 0, s, (double*)G.dd.rj, G.dd.aj, G.N);
+  else launch_k(k_recip<double>, cdiv(G.N, 256), 256, 0, s, (double*)G.df.rj, G.df.aj, G.N);
   CKL();
   return 0;
 }
@@ -717,6 +757,18 @@ int desalm_init(const desalm_case* c, desalm_ctx** out) {
     *out = ctx;
     return DESALM_ENOMEM;
   }
+  // state transfers: one staging array and the fine level's field table
+  rc = A(&ctx->stage, 5 * NF);
+  if (!rc) rc = dalloc(ctx, ctx->allocs, (void**)&ctx->ftab, 15 * sizeof(double*));
+  if (rc) { *out = ctx; return rc; }
+  {
+    double* tab[15];
+    const int fb[3] = {DESALM_F_Q, DESALM_F_QN, DESALM_F_QNM1};
+    int esz = 8;
+    for (int a = 0; a < 3; ++a)
+      for (int m = 0; m < 5; ++m) field_ptr(ctx, 0, fb[a] + m, (void**)&tab[5 * a + m], &esz);
+    cudaMemcpyAsync(ctx->ftab, tab, sizeof(tab), cudaMemcpyHostToDevice, ctx->stream);
+  }
   e = kind_of(ctx, 0) == K_DD ? slab_attrs<double, double>() : slab_attrs<double, float>();
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) {
@@ -758,7 +810,7 @@ int desalm_set_grid(desalm_ctx* ctx, const double* x, const double* y, const dou
       double* p = nullptr;
       if (cudaMalloc((void**)&p, C.N * sizeof(double)) != cudaSuccess) { cleanup(); ctx->err = "cudaMalloc"; return DESALM_ENOMEM; }
       tmp.push_back(p);
-      k_inject<double, double><<<dim3(cdiv(C.im, 64), C.jm, C.km), 64, 0, s>>>(p, lvl_xyz[3 * (n - 1) + t], C.im, C.jm, C.km, F.im, F.jm,
+      launch_k(k_inject<double, double>, dim3(cdiv(C.im, 64), C.jm, C.km), 64, 0, s, p, lvl_xyz[3 * (n - 1) + t], C.im, C.jm, C.km, F.im, F.jm,
                                                                               c.icrs, c.jcrs, c.kcrs);
       lvl_xyz[3 * n + t] = p;
     }
@@ -790,7 +842,7 @@ int desalm_set_grid(desalm_ctx* ctx, const double* x, const double* y, const dou
     tmp.push_back(dcov); tmp.push_back(dmet);
     CK(cudaMemcpyAsync(dcov, cov, 9 * sizeof(double*), cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(dmet, met, 9 * sizeof(double*), cudaMemcpyHostToDevice, s));
-    k_metrics<<<dim3(cdiv(G.im, 64), G.jm, G.km), 64, 0, s>>>(lvl_xyz[3 * n], lvl_xyz[3 * n + 1], lvl_xyz[3 * n + 2], G.im, G.jm, G.km,
+    launch_k(k_metrics, dim3(cdiv(G.im, 64), G.jm, G.km), 64, 0, s, lvl_xyz[3 * n], lvl_xyz[3 * n + 1], lvl_xyz[3 * n + 2], G.im, G.jm, G.km,
                                                              G.dc, G.de, G.dz, dcov, dmet, aj);
     CKL();
     // copy into the level's typed arrays
@@ -805,12 +857,12 @@ int desalm_set_grid(desalm_ctx* ctx, const double* x, const double* y, const dou
     for (int t = 0; t < 10; ++t) {
       const double* src = t < 9 ? met[t] : aj;
       if (esz == 8) CK(cudaMemcpyAsync(dst[t], src, G.N * sizeof(double), cudaMemcpyDeviceToDevice, s));
-      else k_copy<float, double><<<cdiv(G.N, 256), 256, 0, s>>>((float*)dst[t], src, G.N);
+      else launch_k(k_copy<float, double>, cdiv(G.N, 256), 256, 0, s, (float*)dst[t], src, G.N);
     }
     CKL();
     RET(refresh_rj(ctx, n));
     if (n == 0)
-      k_dtev<<<cdiv(G.N, 256), 256, 0, s>>>(dcov, ctx->dtev, G.N, c.cfl2, c.vnn2, c.ren, c.delti, c.unsteady);
+      launch_k(k_dtev, cdiv(G.N, 256), 256, 0, s, dcov, ctx->dtev, G.N, c.cfl2, c.vnn2, c.ren, c.delti, c.unsteady);
     CKL();
     G.dtau_valid = false;
     // the temporaries above are freed after the stream drains
@@ -831,44 +883,31 @@ int desalm_set_grid(desalm_ctx* ctx, const double* x, const double* y, const dou
 int desalm_set_state(desalm_ctx* ctx, const double* q, const double* qn, const double* qnm1, const double* nut) {
   if (!ctx || !q) return DESALM_EINVAL;
   cudaStream_t s = ctx->stream;
-  Level& G = ctx->L[0];
-  const long N = G.N;
-  double* d = nullptr;
-  CK(cudaMalloc((void**)&d, 5 * N * sizeof(double)));
+  const long N = ctx->L[0].N;
   const double* srcs[3] = {q, qn, qnm1};
-  const int fb[3] = {DESALM_F_Q, DESALM_F_QN, DESALM_F_QNM1};
-  int rc = 0;
-  for (int a = 0; a < 3 && !rc; ++a) {
-    void* dst[5];
-    int esz = 8;
-    for (int m = 0; m < 5; ++m) rc |= field_ptr(ctx, 0, fb[a] + m, &dst[m], &esz);
-    if (rc) break;
+  for (int a = 0; a < 3; ++a) {
+    double** dst = ctx->ftab + 5 * a;
     if (!srcs[a]) {
-      for (int m = 0; m < 5; ++m) cudaMemsetAsync(dst[m], 0, N * sizeof(double), s);
+      for (int m = 0; m < 5; ++m) {
+        void* p;
+        int esz;
+        RET(field_ptr(ctx, 0, DESALM_F_Q + 8 * a + m, &p, &esz));
+        CK(cudaMemsetAsync(p, 0, N * sizeof(double), s));
+      }
       continue;
     }
-    cudaMemcpyAsync(d, srcs[a], 5 * N * sizeof(double), cudaMemcpyHostToDevice, s);
-    double** dp = nullptr;
-    cudaMalloc((void**)&dp, 5 * sizeof(double*));
-    cudaMemcpyAsync(dp, dst, 5 * sizeof(double*), cudaMemcpyHostToDevice, s);
-    LAUNCH(KC_MISC, 0, N, k_aos_to_soa<double><<<cdiv(N, 256), 256, 0, s>>>(dp, d, 5, N));
-    cudaStreamSynchronize(s);
-    cudaFree(dp);
+    // stream order keeps the next copy into the staging array behind this conversion
+    CK(cudaMemcpyAsync(ctx->stage, srcs[a], 5 * N * sizeof(double), cudaMemcpyHostToDevice, s));
+    LAUNCH(KC_MISC, 0, N, launch_k(k_aos_to_soa<double>, cdiv(N, 256), 256, 0, s, dst, ctx->stage, 5, N));
+    CKL();
   }
   void* dn;
   int esz;
-  rc |= field_ptr(ctx, 0, DESALM_F_NUT, &dn, &esz);
-  if (!rc) {
-    if (nut) cudaMemcpyAsync(dn, nut, N * sizeof(double), cudaMemcpyHostToDevice, s);
-    else cudaMemsetAsync(dn, 0, N * sizeof(double), s);
-  }
-  cudaError_t e = cudaStreamSynchronize(s);
-  cudaFree(d);
-  if (rc) return rc;
-  if (e != cudaSuccess) {
-    ctx->err = std::string("set_state: ") + cudaGetErrorString(e);
-    return DESALM_ECUDA;
-  }
+  RET(field_ptr(ctx, 0, DESALM_F_NUT, &dn, &esz));
+  if (nut) CK(cudaMemcpyAsync(dn, nut, N * sizeof(double), cudaMemcpyHostToDevice, s));
+  else CK(cudaMemsetAsync(dn, 0, N * sizeof(double), s));
+  // the caller may reuse its arrays when this returns
+  CK(cudaStreamSynchronize(s));
   for (auto& L : ctx->L) L.dtau_valid = false;
   ctx->have_state = true;
   return 0;
@@ -878,38 +917,20 @@ int desalm_get_state(desalm_ctx* ctx, double* q, double* qn, double* qnm1, doubl
   if (!ctx) return DESALM_EINVAL;
   cudaStream_t s = ctx->stream;
   const long N = ctx->L[0].N;
-  double* d = nullptr;
-  CK(cudaMalloc((void**)&d, 5 * N * sizeof(double)));
   double* dsts[3] = {q, qn, qnm1};
-  const int fb[3] = {DESALM_F_Q, DESALM_F_QN, DESALM_F_QNM1};
-  int rc = 0;
-  for (int a = 0; a < 3 && !rc; ++a) {
+  for (int a = 0; a < 3; ++a) {
     if (!dsts[a]) continue;
-    void* src[5];
-    int esz;
-    for (int m = 0; m < 5; ++m) rc |= field_ptr(ctx, 0, fb[a] + m, &src[m], &esz);
-    if (rc) break;
-    double** dp = nullptr;
-    cudaMalloc((void**)&dp, 5 * sizeof(double*));
-    cudaMemcpyAsync(dp, src, 5 * sizeof(double*), cudaMemcpyHostToDevice, s);
-    LAUNCH(KC_MISC, 0, N, k_soa_to_aos<double><<<cdiv(N, 256), 256, 0, s>>>(d, dp, 5, N));
-    cudaMemcpyAsync(dsts[a], d, 5 * N * sizeof(double), cudaMemcpyDeviceToHost, s);
-    cudaStreamSynchronize(s);
-    cudaFree(dp);
+    LAUNCH(KC_MISC, 0, N, launch_k(k_soa_to_aos<double>, cdiv(N, 256), 256, 0, s, ctx->stage, ctx->ftab + 5 * a, 5, N));
+    CKL();
+    CK(cudaMemcpyAsync(dsts[a], ctx->stage, 5 * N * sizeof(double), cudaMemcpyDeviceToHost, s));
   }
-  if (nut && !rc) {
+  if (nut) {
     void* dn;
     int esz;
-    rc = field_ptr(ctx, 0, DESALM_F_NUT, &dn, &esz);
-    if (!rc) cudaMemcpyAsync(nut, dn, N * sizeof(double), cudaMemcpyDeviceToHost, s);
+    RET(field_ptr(ctx, 0, DESALM_F_NUT, &dn, &esz));
+    CK(cudaMemcpyAsync(nut, dn, N * sizeof(double), cudaMemcpyDeviceToHost, s));
   }
-  cudaError_t e = cudaStreamSynchronize(s);
-  cudaFree(d);
-  if (rc) return rc;
-  if (e != cudaSuccess) {
-    ctx->err = std::string("get_state: ") + cudaGetErrorString(e);
-    return DESALM_ECUDA;
-  }
+  CK(cudaStreamSynchronize(s));
   return 0;
 }
 
@@ -925,7 +946,7 @@ int desalm_get_field(desalm_ctx* ctx, int n, int f, double* out) {
   } else {
     double* d = nullptr;
     CK(cudaMalloc((void**)&d, N * sizeof(double)));
-    k_copy<double, float><<<cdiv(N, 256), 256, 0, s>>>(d, (const float*)p, N);
+    launch_k(k_copy<double, float>, cdiv(N, 256), 256, 0, s, d, (const float*)p, N);
     cudaMemcpyAsync(out, d, N * sizeof(double), cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
     cudaFree(d);
@@ -947,7 +968,7 @@ int desalm_set_field(desalm_ctx* ctx, int n, int f, const double* in) {
     double* d = nullptr;
     CK(cudaMalloc((void**)&d, N * sizeof(double)));
     cudaMemcpyAsync(d, in, N * sizeof(double), cudaMemcpyHostToDevice, s);
-    k_copy<float, double><<<cdiv(N, 256), 256, 0, s>>>((float*)p, d, N);
+    launch_k(k_copy<float, double>, cdiv(N, 256), 256, 0, s, (float*)p, d, N);
     cudaStreamSynchronize(s);
     cudaFree(d);
   }
@@ -1036,7 +1057,7 @@ int desalm_begin_step(desalm_ctx* ctx) {
     CK(cudaMemcpyAsync(qnm1, qn, F.N * esz, cudaMemcpyDeviceToDevice, s));
     CK(cudaMemcpyAsync(qn, q, F.N * esz, cudaMemcpyDeviceToDevice, s));
     if (c.predictor == DESALM_PRED_LINEAR)
-      LAUNCH(KC_MISC, 0, F.N, k_extrapolate<double><<<cdiv(F.N, 256), 256, 0, s>>>((double*)q, (const double*)qn, (const double*)qnm1, F.N));
+      LAUNCH(KC_MISC, 0, F.N, launch_k(k_extrapolate<double>, cdiv(F.N, 256), 256, 0, s, (double*)q, (const double*)qn, (const double*)qnm1, F.N));
   }
   CKL();
   // inject qn, qnm1 to the coarse levels (src/mg_driver.F90:55-58)
@@ -1052,11 +1073,11 @@ int desalm_begin_step(desalm_ctx* ctx) {
         RET(field_ptr(ctx, n, f, &pc, &ec));
         dim3 g(cdiv(C.im, 64), C.jm, C.km);
         if (ef == 8 && ec == 8)
-          LAUNCH(KC_MISC, n, C.N, k_inject<double, double><<<g, 64, 0, s>>>((double*)pc, (const double*)pf, C.im, C.jm, C.km, P.im, P.jm, c.icrs, c.jcrs, c.kcrs));
+          LAUNCH(KC_MISC, n, C.N, launch_k(k_inject<double, double>, g, 64, 0, s, (double*)pc, (const double*)pf, C.im, C.jm, C.km, P.im, P.jm, c.icrs, c.jcrs, c.kcrs));
         else if (ef == 8)
-          LAUNCH(KC_MISC, n, C.N, k_inject<double, float><<<g, 64, 0, s>>>((float*)pc, (const double*)pf, C.im, C.jm, C.km, P.im, P.jm, c.icrs, c.jcrs, c.kcrs));
+          LAUNCH(KC_MISC, n, C.N, launch_k(k_inject<double, float>, g, 64, 0, s, (float*)pc, (const double*)pf, C.im, C.jm, C.km, P.im, P.jm, c.icrs, c.jcrs, c.kcrs));
         else
-          LAUNCH(KC_MISC, n, C.N, k_inject<float, float><<<g, 64, 0, s>>>((float*)pc, (const float*)pf, C.im, C.jm, C.km, P.im, P.jm, c.icrs, c.jcrs, c.kcrs));
+          LAUNCH(KC_MISC, n, C.N, launch_k(k_inject<float, float>, g, 64, 0, s, (float*)pc, (const float*)pf, C.im, C.jm, C.km, P.im, P.jm, c.icrs, c.jcrs, c.kcrs));
       }
   }
   CKL();
@@ -1235,7 +1256,7 @@ size_t sa_slab_bytes(int n, int nl) { return (size_t)4 * slab_fs(n, nl + 1) * si
 template <class SW, int DIR, int NL>
 int sa_sweep_nl(desalm_ctx* ctx, SaT<SW>& S, int amax, int n, int nb, double nin) {
   cudaStream_t s = ctx->stream;
-  LAUNCH(KC_SA_SWEEP, 0, nin, k_sa_sweep4<SW, DIR, NL><<<dim3(cdiv(amax, NL), nb), 2 * NL, sa_slab_bytes<SW>(n, NL), s>>>(S));
+  LAUNCH(KC_SA_SWEEP, 0, nin, launch_k(k_sa_sweep4<SW, DIR, NL>, dim3(cdiv(amax, NL), nb), 2 * NL, sa_slab_bytes<SW>(n, NL), s, S));
   CKL();
   return 0;
 }
@@ -1254,17 +1275,17 @@ int sa_run(desalm_ctx* ctx, Lv<double, W>& L) {
   cudaStream_t s = ctx->stream;
   const double nin = double(L.im - 2) * (L.jm - 2) * (L.km - 2);
   const dim3 gi(cdiv(L.im - 2, 32), cdiv(L.jm - 2, 4), L.km - 2);
-  LAUNCH(KC_SA_AUX, 0, nin, k_sa_source<W><<<gi, blk3(), 0, s>>>(S));
-  LAUNCH(KC_SA_AUX, 0, L.N, k_sa_ucn<W><<<cdiv(L.N, 256), 256, 0, s>>>(S));
+  LAUNCH(KC_SA_AUX, 0, nin, launch_k(k_sa_source<W>, gi, blk3(), 0, s, S));
+  LAUNCH(KC_SA_AUX, 0, L.N, launch_k(k_sa_ucn<W>, cdiv(L.N, 256), 256, 0, s, S));
   for (int it = 0; it < ctx->c.itk; ++it) {
-    LAUNCH(KC_SA_RHS, 0, nin, k_sa_rhs<W><<<gi, blk3(), 0, s>>>(S));
+    LAUNCH(KC_SA_RHS, 0, nin, launch_k(k_sa_rhs<W>, gi, blk3(), 0, s, S));
     RET((sa_sweep<W, 0>(ctx, S, L.jm - 2, L.im - 2, L.km - 2, nin)));
     RET((sa_sweep<W, 1>(ctx, S, L.im - 2, L.jm - 2, L.km - 2, nin)));
     RET((sa_sweep<W, 2>(ctx, S, L.im - 2, L.km - 2, L.jm - 2, nin)));
-    LAUNCH(KC_SA_BC, 0, 2.0 * L.jm * L.km, k_sa_bc<W, 0><<<dim3(cdiv(L.jm, 64), L.km), 64, 0, s>>>(S));
-    LAUNCH(KC_SA_BC, 0, 2.0 * L.im * L.km, k_sa_bc<W, 1><<<dim3(cdiv(L.im, 64), L.km), 64, 0, s>>>(S));
-    LAUNCH(KC_SA_BC, 0, 2.0 * L.im * L.jm, k_sa_bc<W, 2><<<dim3(cdiv(L.im, 64), L.jm), 64, 0, s>>>(S));
-    LAUNCH(KC_SA_BC, 0, L.N, k_sa_clamp<W><<<cdiv(L.N, 256), 256, 0, s>>>(S));
+    LAUNCH(KC_SA_BC, 0, 2.0 * L.jm * L.km, launch_k(k_sa_bc<W, 0>, dim3(cdiv(L.jm, 64), L.km), 64, 0, s, S));
+    LAUNCH(KC_SA_BC, 0, 2.0 * L.im * L.km, launch_k(k_sa_bc<W, 1>, dim3(cdiv(L.im, 64), L.km), 64, 0, s, S));
+    LAUNCH(KC_SA_BC, 0, 2.0 * L.im * L.jm, launch_k(k_sa_bc<W, 2>, dim3(cdiv(L.im, 64), L.jm), 64, 0, s, S));
+    LAUNCH(KC_SA_BC, 0, L.N, launch_k(k_sa_clamp<W>, cdiv(L.N, 256), 256, 0, s, S));
   }
   CKL();
   ctx->L[0].dtau_valid = false;  // nu_t changed
@@ -1276,8 +1297,8 @@ int cons_run(desalm_ctx* ctx, Lv<double, W>& L) {
   Sa S = make_sa<double>(ctx, L);
   cudaStream_t s = ctx->stream;
   double* acc = ctx->part;
-  LAUNCH(KC_MISC, 0, 2.0 * L.jm * L.km, k_cons_sum<<<1, 256, 0, s>>>(S, acc));
-  LAUNCH(KC_MISC, 0, 1.0 * L.jm * L.km, k_cons_apply<<<cdiv(L.jm * L.km, 128), 128, 0, s>>>(S, acc, ctx->dcov));
+  LAUNCH(KC_MISC, 0, 2.0 * L.jm * L.km, launch_k(k_cons_sum, 1, 256, 0, s, S, acc));
+  LAUNCH(KC_MISC, 0, 1.0 * L.jm * L.km, launch_k(k_cons_apply, cdiv(L.jm * L.km, 128), 128, 0, s, S, acc, ctx->dcov));
   CKL();
   return 0;
 }
@@ -1306,8 +1327,8 @@ int build_graph(desalm_ctx* ctx) {
     Level& G = ctx->L[0];
     Par P = ctx->par;
     P.fine = 1;
-    if (kind_of(ctx, 0) == K_DD) LAUNCH(KC_DTAU, 0, G.N, k_dtau<double, double><<<cdiv(G.N, 256), 256, 0, s>>>(G.dd, P));
-    else LAUNCH(KC_DTAU, 0, G.N, k_dtau<double, float><<<cdiv(G.N, 256), 256, 0, s>>>(G.df, P));
+    if (kind_of(ctx, 0) == K_DD) LAUNCH(KC_DTAU, 0, G.N, launch_k(k_dtau<double, double>, cdiv(G.N, 256), 256, 0, s, G.dd, P));
+    else LAUNCH(KC_DTAU, 0, G.N, launch_k(k_dtau<double, float>, cdiv(G.N, 256), 256, 0, s, G.df, P));
     CKL();
     G.dtau_valid = true;
   }
@@ -1337,9 +1358,9 @@ int build_graph(desalm_ctx* ctx) {
   ConvPar cv{ctx->c.it_min, ctx->c.itmax, ctx->c.er_min, ctx->c.eo_min, double(total)};
   if (!rc) {
     int nbu = (int)std::min<long>(nb, std::max<long>(1, cdiv(total, 256)));
-    if (kind_of(ctx, 0) == K_DD) LAUNCH(KC_NORM, 0, double(total), k_norm_partial<double, double><<<nbu, 256, 0, s>>>(G.dd, ctx->part, 5, 1));
-    else LAUNCH(KC_NORM, 0, double(total), k_norm_partial<double, float><<<nbu, 256, 0, s>>>(G.df, ctx->part, 5, 1));
-    LAUNCH(KC_NORM, 0, 0, k_conv<<<1, 256, 0, s>>>(ctx->part, nbu, ctx->dconv, ctx->flags, cv, h));
+    if (kind_of(ctx, 0) == K_DD) LAUNCH(KC_NORM, 0, double(total), launch_k(k_norm_partial<double, double>, nbu, 256, 0, s, G.dd, ctx->part, 5, 1));
+    else LAUNCH(KC_NORM, 0, double(total), launch_k(k_norm_partial<double, float>, nbu, 256, 0, s, G.df, ctx->part, 5, 1));
+    LAUNCH(KC_NORM, 0, 0, launch_k(k_conv, 1, 256, 0, s, ctx->part, nbu, ctx->dconv, ctx->flags, cv, h));
   }
   cudaGraph_t out = nullptr;
   cudaError_t e = cudaStreamEndCapture(s, &out);

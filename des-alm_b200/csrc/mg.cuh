@@ -13,6 +13,8 @@ namespace desalm {
 // covers the full transverse range (edges and corners included).
 template <class T, class W, int DIR>
 __global__ void k_bcond(Lv<T, W> L, Par P, const T* rat, int ratdim) {
+  pdl_wait();
+  pdl_trigger();
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   const int b = blockIdx.y;
   int amax, n, st, lb;
@@ -46,11 +48,15 @@ __global__ void k_bcond(Lv<T, W> L, Par P, const T* rat, int ratdim) {
 // pressure reference value after the face updates (src/bcond_fm.F90:310)
 template <class T, class W>
 __global__ void k_pfix_read(Lv<T, W> L, int lfix, T* pfix) {
+  pdl_wait();
+  pdl_trigger();
   *pfix = L.q[0][lfix];
 }
 // p <- p - pfix over the whole level (src/bcond_fm.F90:316-322)
 template <class T, class W>
 __global__ void k_pfix_sub(Lv<T, W> L, const T* pfix) {
+  pdl_wait();
+  pdl_trigger();
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= L.N) return;
   L.q[0][l] = L.q[0][l] - *pfix;
@@ -62,6 +68,8 @@ __global__ void k_pfix_sub(Lv<T, W> L, const T* pfix) {
 // the 27-point full-weighting restriction of the fine residual into pk.
 template <class TF, class WF, class TC, class WC>
 __global__ void k_nlevel(Lv<TF, WF> F, Lv<TC, WC> C, int icrs, int jcrs, int kcrs) {
+  pdl_wait();
+  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z;
@@ -148,6 +156,8 @@ struct Interp {
 
 template <class TF, class WF, class TC, class WC>
 __global__ void k_prolong_interp(Lv<TF, WF> F, Lv<TC, WC> C, TF* dq, int icrs, int jcrs, int kcrs) {
+  pdl_wait();
+  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int k = blockIdx.z + 1;
@@ -163,6 +173,8 @@ __global__ void k_prolong_interp(Lv<TF, WF> F, Lv<TC, WC> C, TF* dq, int icrs, i
 // (src/mg_residual.F90:58-67); optionally qold <- q for the next iteration.
 template <class T, class W>
 __global__ void __launch_bounds__(256) k_norm_partial(Lv<T, W> L, double* part, int nf, int copy) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ double sh[5][256];
   const int ni = L.im - 2, nj = L.jm - 2, nk = L.km - 2;
   const long total = (long)ni * nj * nk;
@@ -208,6 +220,8 @@ DESALM_DEV void block_sum5(const double* part, int nblk, double out[5]) {
 }
 
 __global__ void __launch_bounds__(256) k_norm_final(const double* part, int nblk, double* out) {
+  pdl_wait();
+  pdl_trigger();
   double sums[5];
   block_sum5(part, nblk, sums);
   if (threadIdx.x == 0)
@@ -217,29 +231,39 @@ __global__ void __launch_bounds__(256) k_norm_final(const double* part, int nblk
 // ---------------------------------------------------------------- helpers
 template <class T>
 __global__ void k_fill(T* a, T v, long n) {
+  pdl_wait();
+  pdl_trigger();
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) a[t] = v;
 }
 template <class TD, class TS>
 __global__ void k_copy(TD* d, const TS* s, long n) {
+  pdl_wait();
+  pdl_trigger();
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) d[t] = TD(s[t]);
 }
 // q^{n+1,(0)} = 2 q^n - q^{n-1}
 template <class T>
 __global__ void k_extrapolate(T* q, const T* qn, const T* qnm1, long n) {
+  pdl_wait();
+  pdl_trigger();
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) q[t] = T(2) * qn[t] - qnm1[t];
 }
 // Reference-layout AoS (me, i, j, k) <-> SoA
 template <class T>
 __global__ void k_aos_to_soa(T* const* dst, const double* src, int me, long n) {
+  pdl_wait();
+  pdl_trigger();
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   for (int m = 0; m < me; ++m) dst[m][t] = T(src[t * me + m]);
 }
 template <class T>
 __global__ void k_soa_to_aos(double* dst, T* const* src, int me, long n) {
+  pdl_wait();
+  pdl_trigger();
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   for (int m = 0; m < me; ++m) dst[t * me + m] = double(src[m][t]);
@@ -248,6 +272,8 @@ __global__ void k_soa_to_aos(double* dst, T* const* src, int me, long n) {
 // Injection of one scalar field to the next coarser level (src/mg_inject.F90:26-62)
 template <class TF, class TC>
 __global__ void k_inject(TC* c, const TF* f, int cim, int cjm, int ckm, int fim, int fjm, int icrs, int jcrs, int kcrs) {
+  pdl_wait();
+  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
   const int k = blockIdx.z;
@@ -259,6 +285,8 @@ __global__ void k_inject(TC* c, const TF* f, int cim, int cjm, int ckm, int fim,
 // r = 1 / a element-wise (the reciprocal Jacobian of a level)
 template <class T>
 __global__ void k_recip(T* r, const T* a, long n) {
+  pdl_wait();
+  pdl_trigger();
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) r[t] = T(1) / a[t];
 }
@@ -267,6 +295,8 @@ __global__ void k_recip(T* r, const T* a, long n) {
 // (src/mg_metrics.F90:56-250).  cov[9] = xc, xe, xz, yc, ye, yz, zc, ze, zz.
 __global__ void k_metrics(const double* x, const double* y, const double* z, int im, int jm, int km,
                           double dc, double de, double dz, double* const* cov, double* const* met, double* aj) {
+  pdl_wait();
+  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
   const int k = blockIdx.z;
@@ -303,6 +333,8 @@ __global__ void k_metrics(const double* x, const double* y, const double* z, int
 
 // SA pseudo-time step on the fine level (src/mg_metrics.F90:262-282)
 __global__ void k_dtev(double* const* cov, double* dtev, long n, double cfl2, double vnn2, double ren, double delti, int unsteady) {
+  pdl_wait();
+  pdl_trigger();
   long l = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= n) return;
   double xc = cov[0][l], xe = cov[1][l], xz = cov[2][l], yc = cov[3][l], ye = cov[4][l], yz = cov[5][l];
@@ -337,6 +369,8 @@ namespace desalm {
 // Shared memory: 4 components of slab_fs(n, NL + 1) elements of TF.
 template <class TF, class WF, int DIR, int NL>
 __global__ void __launch_bounds__(8 * NL) k_rsmooth4(Lv<TF, WF> F, TF* dq, const double* fac, const double* dpr, double e, int last) {
+  pdl_wait();
+  pdl_trigger();
   constexpr int NT = 8 * NL, NLP = NL + 1;
   extern __shared__ __align__(16) unsigned char rs_slab[];
   __shared__ TF s_top[NL][4], s_bot[NL][4];  // eliminated b of the two middle rows

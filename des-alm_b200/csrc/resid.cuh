@@ -109,6 +109,8 @@ DESALM_DEV T diss_fv(const Lv<T, W>& L, int dir, int l, int st, T dsq) {
 // MODE 0: first pass of a DAF step; MODE 1: recalculation for restriction.
 template <class T, class W, int MODE>
 __global__ void __launch_bounds__(128, DESALM_KR_MINBLOCKS) k_resid(Lv<T, W> L, Par P, int upwind, int calc_pk, int coarse, int bback) {
+  pdl_wait();
+  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int k = blockIdx.z + 1;
@@ -308,6 +310,8 @@ __global__ void __launch_bounds__(128, DESALM_KR_MINBLOCKS) k_resid(Lv<T, W> L, 
 // minimum up to rounding.
 template <class T, class W>
 __global__ void k_dtau(Lv<T, W> L, Par P) {
+  pdl_wait();
+  pdl_trigger();
   int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= L.N) return;
   const T rcfl = T(1) / T(P.cfl1), rvnn = T(1) / T(P.vnn1), rei = T(1) / T(P.ren);

@@ -56,6 +56,8 @@ DESALM_DEV double sa_ucn(const SaT<SW>& S, int d, int l) {
 // sub-iterations.
 template <class SW>
 __global__ void k_sa_ucn(SaT<SW> S) {
+  pdl_wait();
+  pdl_trigger();
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= S.N) return;
 #pragma unroll
@@ -65,6 +67,8 @@ __global__ void k_sa_ucn(SaT<SW> S) {
 // vorticity magnitude wo = 2 |W|^2 on interior nodes (src/rhs_sa_source.F90:44-93)
 template <class SW>
 __global__ void k_sa_source(SaT<SW> S) {
+  pdl_wait();
+  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int k = blockIdx.z + 1;
@@ -176,6 +180,8 @@ DESALM_DEV void sa_adi_row(const SaT<SW>& S, int l) {
 // equal the reference's expressions up to rounding.
 template <class SW>
 __global__ void __launch_bounds__(128) k_sa_rhs(SaT<SW> S) {
+  pdl_wait();
+  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int k = blockIdx.z + 1;
@@ -273,6 +279,8 @@ __global__ void __launch_bounds__(128) k_sa_rhs(SaT<SW> S) {
 // Shared memory: 4 fields of slab_fs(n, NL + 1) elements of SW.
 template <class SW, int DIR, int NL>
 __global__ void __launch_bounds__(2 * NL) k_sa_sweep4(SaT<SW> S) {
+  pdl_wait();
+  pdl_trigger();
   constexpr int NT = 2 * NL, NLP = NL + 1;
   extern __shared__ __align__(16) unsigned char sa_slab[];
   __shared__ SW m_d[NL], m_c[NL], m_b[NL], n_d[NL], n_c[NL], n_b[NL];
@@ -444,6 +452,8 @@ __global__ void __launch_bounds__(2 * NL) k_sa_sweep4(SaT<SW> S) {
 // face pair in the order i, j, k; full transverse ranges.
 template <class SW, int DIR>
 __global__ void k_sa_bc(SaT<SW> S) {
+  pdl_wait();
+  pdl_trigger();
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   const int b = blockIdx.y;
   int amax, n, st, lb;
@@ -468,6 +478,8 @@ __global__ void k_sa_bc(SaT<SW> S) {
 // nu_tilde >= 1e-7 and nu_t = nu_tilde f_v1 on every node (src/rhs_sa_bcond.F90:279-291)
 template <class SW>
 __global__ void k_sa_clamp(SaT<SW> S) {
+  pdl_wait();
+  pdl_trigger();
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= S.N) return;
   double v = S.q[4][l];
@@ -481,6 +493,8 @@ __global__ void k_sa_clamp(SaT<SW> S) {
 // ---------------------------------------------------------------- conservation
 // Sums of U/J over the first and last i planes (all j, k), into acc[0..1].
 __global__ void k_cons_sum(Sa S, double* acc) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ double sh[2][256];
   double a0 = 0, a1 = 0;
   const int P = S.jm * S.km;
@@ -502,6 +516,8 @@ __global__ void k_cons_sum(Sa S, double* acc) {
 // Rescale the outlet plane's U/J by fin/fout and return to Cartesian
 // velocities with the covariant metrics (src/conservation.F90:137-157).
 __global__ void k_cons_apply(Sa S, const double* acc, double* const* cov) {
+  pdl_wait();
+  pdl_trigger();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= S.jm * S.km) return;
   const int j = t % S.jm, k = t / S.jm;

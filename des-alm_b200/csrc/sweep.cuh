@@ -55,6 +55,8 @@ namespace desalm {
 
 template <class T, class W, int DIR, int NL>
 __global__ void __launch_bounds__(8 * NL) k_sweep4(Lv<T, W> L, Par P, int blo, int bhi) {
+  pdl_wait();
+  pdl_trigger();
   constexpr int NT = 8 * NL, NLP = NL + 1;
   extern __shared__ __align__(16) unsigned char sweep_slab[];
   __shared__ W sbw[NL][4], sbe[NL][4];
@@ -284,6 +286,8 @@ __global__ void __launch_bounds__(8 * NL) k_sweep4(Lv<T, W> L, Par P, int blo, i
 // 240-258, 416-434, 600-633; src/solver_daf.F90:409-418).
 template <class T, class W, int DIR>
 __global__ void __launch_bounds__(128) k_xform(Lv<T, W> L) {
+  pdl_wait();
+  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int k = blockIdx.z + 1;
