@@ -67,6 +67,10 @@ struct Par {
 // start on different banks.
 DESALM_HD inline int slab_fs(int np, int nlp) { return ((np * nlp + 31) / 32) * 32 + 16; }
 
+// Threads of a slab CTA: all of them copy the slab in and out, the first
+// 8 NL (DAF sweeps, rsmooth) or 2 NL (SA sweeps) solve the lines.
+constexpr int kSlabThreads = 256;
+
 // Programmatic dependent launch: when a kernel is launched with programmatic
 // stream serialisation, pdl_wait() blocks until the grids it depends on have
 // completed and their writes are visible (it must come before the first

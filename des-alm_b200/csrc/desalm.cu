@@ -273,10 +273,10 @@ int check_case(desalm_ctx* ctx, const desalm_case& c) {
   }
   if ((long)c.im * c.jm * c.km * 4 >= (1L << 31)) return bad("grid too large for 32-bit indexing");
   // the narrowest slab of every line solve must fit: DAF sweep 4 lines of
-  // 10 W-fields, rsmooth 4 lines of 4 FP64 fields, SA sweep 8 lines of 4 W-fields
+  // 10 W-fields, rsmooth 4 lines of 4 W-fields, SA sweep 8 lines of 4 W-fields
   const size_t wb = c.precision_mode == DESALM_FP64 ? 8 : 4;
   for (int n : {c.im - 2, c.jm - 2, c.km - 2})
-    if ((size_t)10 * slab_fs(n + 2, 5) * wb > kSlabMax || (size_t)4 * slab_fs(n, 5) * 8 > kSlabMax ||
+    if ((size_t)10 * slab_fs(n + 2, 5) * wb > kSlabMax || (size_t)4 * slab_fs(n, 5) * wb > kSlabMax ||
         (size_t)4 * slab_fs(n, 9) * wb > kSlabMax)
       return bad("a grid line is too long for the shared-memory line solves (at most 554 interior nodes in "
                  "FP64 mode, 1118 in MIXED mode)");
@@ -328,6 +328,11 @@ dim3 grid_interior(const Lv<T, W>& L) { return dim3(cdiv(L.im - 2, 32), cdiv(L.j
 template <class W>
 size_t slab_bytes(int n, int nl) { return (size_t)10 * slab_fs(n + 2, nl + 1) * sizeof(W); }
 
+// A slab of at most 48 KB (four or more CTAs per SM) runs with its 8 NL
+// solver threads only; a larger one with kSlabThreads, the extra threads
+// sharing the copies.  Both variants have the shared-memory opt-in, since the
+// static arrays come on top of the slab.
+constexpr size_t kSlabFourPerSm = 48 * 1024;
 template <class T, class W, int DIR, int NL>
 int sweep4_nl(desalm_ctx* ctx, Lv<T, W>& L, const Par& P, int lvl, int blo, int bhi) {
   int amax, n, nb;
@@ -338,7 +343,10 @@ int sweep4_nl(desalm_ctx* ctx, Lv<T, W>& L, const Par& P, int lvl, int blo, int 
   const int cls = DIR == 0 ? KC_SWEEP_I : (DIR == 1 ? KC_SWEEP_J : KC_SWEEP_K);
   const double nin = double(amax) * n * nb;
   cudaStream_t s = ctx->stream;
-  LAUNCH(cls, lvl, nin, launch_k(k_sweep4<T, W, DIR, NL>, dim3(cdiv(amax, NL), nb), 8 * NL, bytes, s, L, P, blo, bhi));
+  if (bytes <= kSlabFourPerSm)
+    LAUNCH(cls, lvl, nin, launch_k(k_sweep4<T, W, DIR, NL, 8 * NL>, dim3(cdiv(amax, NL), nb), 8 * NL, bytes, s, L, P, blo, bhi));
+  else
+    LAUNCH(cls, lvl, nin, launch_k(k_sweep4<T, W, DIR, NL, kSlabThreads>, dim3(cdiv(amax, NL), nb), kSlabThreads, bytes, s, L, P, blo, bhi));
   CKL();
   const int xcls = DIR == 0 ? KC_XFORM_I : (DIR == 1 ? KC_XFORM_J : KC_XFORM_K);
   LAUNCH(xcls, lvl, nin, launch_k(k_xform<T, W, DIR>, grid_interior(L), blk3(), 0, s, L));
@@ -361,9 +369,18 @@ cudaError_t slab_attrs() {
     const int mx = (int)std::min<size_t>(kSlabMax, (size_t)optin - fa.sharedSizeBytes);
     e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
   };
-  set((const void*)k_sweep4<T, W, 0, 16>); set((const void*)k_sweep4<T, W, 0, 8>); set((const void*)k_sweep4<T, W, 0, 4>);
-  set((const void*)k_sweep4<T, W, 1, 16>); set((const void*)k_sweep4<T, W, 1, 8>); set((const void*)k_sweep4<T, W, 1, 4>);
-  set((const void*)k_sweep4<T, W, 2, 16>); set((const void*)k_sweep4<T, W, 2, 8>); set((const void*)k_sweep4<T, W, 2, 4>);
+  set((const void*)k_sweep4<T, W, 0, 16, kSlabThreads>); set((const void*)k_sweep4<T, W, 0, 8, kSlabThreads>);
+  set((const void*)k_sweep4<T, W, 0, 4, kSlabThreads>);
+  set((const void*)k_sweep4<T, W, 1, 16, kSlabThreads>); set((const void*)k_sweep4<T, W, 1, 8, kSlabThreads>);
+  set((const void*)k_sweep4<T, W, 1, 4, kSlabThreads>);
+  set((const void*)k_sweep4<T, W, 2, 16, kSlabThreads>); set((const void*)k_sweep4<T, W, 2, 8, kSlabThreads>);
+  set((const void*)k_sweep4<T, W, 2, 4, kSlabThreads>);
+  set((const void*)k_sweep4<T, W, 0, 16, 128>); set((const void*)k_sweep4<T, W, 0, 8, 64>);
+  set((const void*)k_sweep4<T, W, 0, 4, 32>);
+  set((const void*)k_sweep4<T, W, 1, 16, 128>); set((const void*)k_sweep4<T, W, 1, 8, 64>);
+  set((const void*)k_sweep4<T, W, 1, 4, 32>);
+  set((const void*)k_sweep4<T, W, 2, 16, 128>); set((const void*)k_sweep4<T, W, 2, 8, 64>);
+  set((const void*)k_sweep4<T, W, 2, 4, 32>);
   set((const void*)k_sa_sweep4<W, 0, 32>); set((const void*)k_sa_sweep4<W, 0, 16>); set((const void*)k_sa_sweep4<W, 0, 8>);
   set((const void*)k_sa_sweep4<W, 1, 32>); set((const void*)k_sa_sweep4<W, 1, 16>); set((const void*)k_sa_sweep4<W, 1, 8>);
   set((const void*)k_sa_sweep4<W, 2, 32>); set((const void*)k_sa_sweep4<W, 2, 16>); set((const void*)k_sa_sweep4<W, 2, 8>);
@@ -446,24 +463,24 @@ int launch_nlevel(desalm_ctx* ctx, Lv<TF, WF>& F, Lv<TC, WC>& C) {
 
 // One direction of rsmooth as k_rsmooth4 with the widest slab that leaves
 // room for two CTAs per SM.
-template <class TF>
-size_t rs_slab_bytes(int n, int nl) { return (size_t)4 * slab_fs(n, nl + 1) * sizeof(TF); }
+template <class WF>
+size_t rs_slab_bytes(int n, int nl) { return (size_t)4 * slab_fs(n, nl + 1) * sizeof(WF); }
 template <class TF, class WF, int DIR, int NL>
-int rsmooth_nl(desalm_ctx* ctx, Lv<TF, WF>& F, TF* dq, Level& G, double e, int last, double nin) {
+int rsmooth_nl(desalm_ctx* ctx, Lv<TF, WF>& F, WF* dq, Level& G, double e, int last, double nin) {
   const int amax = DIR == 0 ? F.jm - 2 : F.im - 2;
   const int n = DIR == 0 ? F.im - 2 : (DIR == 1 ? F.jm - 2 : F.km - 2);
   const int nb = DIR == 2 ? F.jm - 2 : F.km - 2;
-  LAUNCH(KC_RSMOOTH, 0, nin, launch_k(k_rsmooth4<TF, WF, DIR, NL>, dim3(cdiv(amax, NL), nb), 8 * NL, rs_slab_bytes<TF>(n, NL), ctx->stream, 
+  LAUNCH(KC_RSMOOTH, 0, nin, launch_k(k_rsmooth4<TF, WF, DIR, NL>, dim3(cdiv(amax, NL), nb), kSlabThreads, rs_slab_bytes<WF>(n, NL), ctx->stream, 
                                  F, dq, G.fac[DIR], G.dpr[DIR], e, last));
   CKL();
   return 0;
 }
 template <class TF, class WF, int DIR>
-int rsmooth(desalm_ctx* ctx, Lv<TF, WF>& F, TF* dq, Level& G, double e, int last, double nin) {
+int rsmooth(desalm_ctx* ctx, Lv<TF, WF>& F, WF* dq, Level& G, double e, int last, double nin) {
   const int n = DIR == 0 ? F.im - 2 : (DIR == 1 ? F.jm - 2 : F.km - 2);
-  if (rs_slab_bytes<TF>(n, 16) <= kSlabTwoPerSm) return rsmooth_nl<TF, WF, DIR, 16>(ctx, F, dq, G, e, last, nin);
-  if (rs_slab_bytes<TF>(n, 8) <= kSlabTwoPerSm) return rsmooth_nl<TF, WF, DIR, 8>(ctx, F, dq, G, e, last, nin);
-  if (rs_slab_bytes<TF>(n, 4) <= kSlabMax) return rsmooth_nl<TF, WF, DIR, 4>(ctx, F, dq, G, e, last, nin);
+  if (rs_slab_bytes<WF>(n, 16) <= kSlabTwoPerSm) return rsmooth_nl<TF, WF, DIR, 16>(ctx, F, dq, G, e, last, nin);
+  if (rs_slab_bytes<WF>(n, 8) <= kSlabTwoPerSm) return rsmooth_nl<TF, WF, DIR, 8>(ctx, F, dq, G, e, last, nin);
+  if (rs_slab_bytes<WF>(n, 4) <= kSlabMax) return rsmooth_nl<TF, WF, DIR, 4>(ctx, F, dq, G, e, last, nin);
   ctx->err = "grid line too long for the shared-memory rsmooth";
   return DESALM_EINVAL;
 }
@@ -472,7 +489,7 @@ template <class TF, class WF, class TC, class WC>
 int launch_prolong(desalm_ctx* ctx, Lv<TF, WF>& F, Lv<TC, WC>& C, Level& G) {
   const desalm_case& c = ctx->c;
   cudaStream_t s = ctx->stream;
-  TF* dq = (TF*)G.dq[0];
+  WF* dq = (WF*)G.dq[0];  // the prolongation correction, in the sweep precision
   const double nin = double(F.im - 2) * (F.jm - 2) * (F.km - 2);
   LAUNCH(KC_PROLONG, 0, nin, launch_k(k_prolong_interp<TF, WF, TC, WC>, grid_interior(F), blk3(), 0, s, F, C, dq, c.icrs, c.jcrs, c.kcrs));
   CKL();
@@ -718,7 +735,7 @@ int desalm_init(const desalm_case* c, desalm_ctx** out) {
     G.tbytes = 8;
     G.wbytes = k == K_DD ? 8 : 4;
     if (n + 1 < ctx->ng) {
-      rc = dalloc(ctx, G.allocs, &G.dq[0], (size_t)4 * G.N * G.tbytes);
+      rc = dalloc(ctx, G.allocs, &G.dq[0], (size_t)4 * G.N * G.wbytes);
       if (rc) { *out = ctx; return rc; }
       const int ext[3] = {G.im, G.jm, G.km};
       for (int d = 0; d < 3; ++d) {
@@ -1256,7 +1273,7 @@ size_t sa_slab_bytes(int n, int nl) { return (size_t)4 * slab_fs(n, nl + 1) * si
 template <class SW, int DIR, int NL>
 int sa_sweep_nl(desalm_ctx* ctx, SaT<SW>& S, int amax, int n, int nb, double nin) {
   cudaStream_t s = ctx->stream;
-  LAUNCH(KC_SA_SWEEP, 0, nin, launch_k(k_sa_sweep4<SW, DIR, NL>, dim3(cdiv(amax, NL), nb), 2 * NL, sa_slab_bytes<SW>(n, NL), s, S));
+  LAUNCH(KC_SA_SWEEP, 0, nin, launch_k(k_sa_sweep4<SW, DIR, NL>, dim3(cdiv(amax, NL), nb), kSlabThreads, sa_slab_bytes<SW>(n, NL), s, S));
   CKL();
   return 0;
 }

@@ -155,7 +155,7 @@ struct Interp {
 };
 
 template <class TF, class WF, class TC, class WC>
-__global__ void k_prolong_interp(Lv<TF, WF> F, Lv<TC, WC> C, TF* dq, int icrs, int jcrs, int kcrs) {
+__global__ void k_prolong_interp(Lv<TF, WF> F, Lv<TC, WC> C, WF* dq, int icrs, int jcrs, int kcrs) {
   pdl_wait();
   pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -165,7 +165,7 @@ __global__ void k_prolong_interp(Lv<TF, WF> F, Lv<TC, WC> C, TF* dq, int icrs, i
   const int l = i + F.sj * j + F.sk * k;
   Interp<TF, WF, TC, WC> I{&F, &C, icrs, jcrs, kcrs};
 #pragma unroll
-  for (int m = 0; m < 4; ++m) dq[m * F.N + l] = I.fi(i, j, k, m);
+  for (int m = 0; m < 4; ++m) dq[m * F.N + l] = WF(I.fi(i, j, k, m));
 }
 
 // ---------------------------------------------------------------- norm
@@ -354,7 +354,7 @@ namespace desalm {
 
 // Constant-coefficient implicit smoothing (-e, 1+2e, -e) of the four
 // correction components along one direction (src/rs_sweep.F90:163-284), as a
-// shared-memory slab: a CTA owns NL lines of one plane and 8 NL threads.
+// shared-memory slab: a CTA owns NL lines of one plane (kSlabThreads threads).
 //   phase 0  the slab of dq is copied into shared memory (cp.async);
 //   phase 1  thread (line, component m, half) eliminates the upper half of
 //            its line top-down or the lower half bottom-up with SGTSV's
@@ -366,14 +366,17 @@ namespace desalm {
 //   phase 2  dq gets the smoothed values, or, after the last direction (k),
 //            q += dq on the interior (src/mg_prolong.F90:218-277: dq is zero
 //            on the boundary).
-// Shared memory: 4 components of slab_fs(n, NL + 1) elements of TF.
+// The correction dq is held in the sweep precision WF (FP32 in MIXED mode: it
+// is part of the coarse-grid correction, a preconditioner) and added to the
+// FP64 state at the end.  Shared memory: 4 components of slab_fs(n, NL + 1)
+// elements of WF.
 template <class TF, class WF, int DIR, int NL>
-__global__ void __launch_bounds__(8 * NL) k_rsmooth4(Lv<TF, WF> F, TF* dq, const double* fac, const double* dpr, double e, int last) {
+__global__ void __launch_bounds__(kSlabThreads) k_rsmooth4(Lv<TF, WF> F, WF* dq, const double* fac, const double* dpr, double e, int last) {
   pdl_wait();
   pdl_trigger();
-  constexpr int NT = 8 * NL, NLP = NL + 1;
+  constexpr int NT = kSlabThreads, NLP = NL + 1;
   extern __shared__ __align__(16) unsigned char rs_slab[];
-  __shared__ TF s_top[NL][4], s_bot[NL][4];  // eliminated b of the two middle rows
+  __shared__ WF s_top[NL][4], s_bot[NL][4];  // eliminated b of the two middle rows
   const int tid = threadIdx.x;
   const int a0 = blockIdx.x * NL + 1;
   const int b = blockIdx.y + 1;
@@ -383,7 +386,7 @@ __global__ void __launch_bounds__(8 * NL) k_rsmooth4(Lv<TF, WF> F, TF* dq, const
   else { amax = F.im - 2; n = F.km - 2; st = F.sk; sa = 1; base = F.sj * b; }
   const int nl = min(NL, amax - a0 + 1);
   const int fs = slab_fs(n, NLP);  // row p (node p + 1) of component m at m fs + p NLP + line
-  TF* sv = reinterpret_cast<TF*>(rs_slab);
+  WF* sv = reinterpret_cast<WF*>(rs_slab);
   const int total = nl * n;
   auto node = [&](int t, int& li, int& p) {
     if (DIR == 0) { li = t / n; p = t - li * n; }
@@ -404,25 +407,25 @@ __global__ void __launch_bounds__(8 * NL) k_rsmooth4(Lv<TF, WF> F, TF* dq, const
   // ---- phase 1
   const int li = tid % NL, combo = tid / NL;
   const int m = combo & 3, half = combo >> 2;
-  const bool act = li < nl;
-  TF* v = sv + m * fs + li;
-  const TF off = TF(-e);
+  const bool act = tid < 8 * NL && li < nl;  // solver threads
+  WF* v = sv + m * fs + li;
+  const WF off = WF(-e);
   const int h = n / 2;
   const double* rdpr = dpr + n;  // 1 / dpr
   if (act && half == 0) {
-    TF bp = 0;
+    WF bp = 0;
     for (int p = 0; p < h; ++p) {
-      TF x = v[p * NLP];
-      if (p > 0) x = x - TF(__ldg(fac + p - 1)) * bp;
+      WF x = v[p * NLP];
+      if (p > 0) x = x - WF(__ldg(fac + p - 1)) * bp;
       bp = x;
       v[p * NLP] = x;
     }
     s_top[li][m] = bp;
   } else if (act && half == 1) {
-    TF bp = 0;
+    WF bp = 0;
     for (int p = n - 1; p >= h; --p) {
-      TF x = v[p * NLP];
-      if (p < n - 1) x = x - TF(__ldg(fac + n - 2 - p)) * bp;
+      WF x = v[p * NLP];
+      if (p < n - 1) x = x - WF(__ldg(fac + n - 2 - p)) * bp;
       bp = x;
       v[p * NLP] = x;
     }
@@ -430,21 +433,21 @@ __global__ void __launch_bounds__(8 * NL) k_rsmooth4(Lv<TF, WF> F, TF* dq, const
   }
   __syncthreads();
   if (act) {
-    const TF d1 = TF(__ldg(dpr + h - 1)), d2 = TF(__ldg(dpr + n - 1 - h));
-    const TF b1 = s_top[li][m], b2 = s_bot[li][m];
-    const TF det = d1 * d2 - off * off;
+    const WF d1 = WF(__ldg(dpr + h - 1)), d2 = WF(__ldg(dpr + n - 1 - h));
+    const WF b1 = s_top[li][m], b2 = s_bot[li][m];
+    const WF det = d1 * d2 - off * off;
     if (half == 0) {
-      TF x = (b1 * d2 - off * b2) / det;
+      WF x = (b1 * d2 - off * b2) / det;
       v[(h - 1) * NLP] = x;
       for (int p = h - 2; p >= 0; --p) {
-        x = (v[p * NLP] - off * x) * TF(__ldg(rdpr + p));
+        x = (v[p * NLP] - off * x) * WF(__ldg(rdpr + p));
         v[p * NLP] = x;
       }
     } else {
-      TF x = (d1 * b2 - off * b1) / det;
+      WF x = (d1 * b2 - off * b1) / det;
       v[h * NLP] = x;
       for (int p = h + 1; p < n; ++p) {
-        x = (v[p * NLP] - off * x) * TF(__ldg(rdpr + n - 1 - p));
+        x = (v[p * NLP] - off * x) * WF(__ldg(rdpr + n - 1 - p));
         v[p * NLP] = x;
       }
     }
@@ -461,7 +464,7 @@ __global__ void __launch_bounds__(8 * NL) k_rsmooth4(Lv<TF, WF> F, TF* dq, const
 #pragma unroll
       for (int mm = 0; mm < 4; ++mm) qv[mm] = F.q[mm][l];
 #pragma unroll
-      for (int mm = 0; mm < 4; ++mm) F.q[mm][l] = qv[mm] + sv[mm * fs + so];
+      for (int mm = 0; mm < 4; ++mm) F.q[mm][l] = qv[mm] + TF(sv[mm * fs + so]);
     } else {
 #pragma unroll
       for (int mm = 0; mm < 4; ++mm) dq[(long)mm * F.N + l] = sv[mm * fs + so];

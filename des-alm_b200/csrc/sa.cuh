@@ -264,7 +264,7 @@ __global__ void __launch_bounds__(128) k_sa_rhs(SaT<SW> S) {
 
 // Scalar ADI sweep of nu_tilde along one direction
 // (src/rhs_sa_adi_solver.F90:50-244) on the stored rows, as a shared-memory
-// slab: a CTA owns NL lines of one plane and 2 NL threads.
+// slab: a CTA owns NL lines of one plane (kSlabThreads threads).
 //   phase 0  the rows (aw, ap, ae) and the right-hand side of the slab are
 //            copied into shared memory (cp.async, all in flight, coalesced
 //            along the fastest global index), laid out [node][line];
@@ -278,10 +278,10 @@ __global__ void __launch_bounds__(128) k_sa_rhs(SaT<SW> S) {
 //            (src/des_eddy.F90:260-272).
 // Shared memory: 4 fields of slab_fs(n, NL + 1) elements of SW.
 template <class SW, int DIR, int NL>
-__global__ void __launch_bounds__(2 * NL) k_sa_sweep4(SaT<SW> S) {
+__global__ void __launch_bounds__(kSlabThreads) k_sa_sweep4(SaT<SW> S) {
   pdl_wait();
   pdl_trigger();
-  constexpr int NT = 2 * NL, NLP = NL + 1;
+  constexpr int NT = kSlabThreads, NLP = NL + 1;
   extern __shared__ __align__(16) unsigned char sa_slab[];
   __shared__ SW m_d[NL], m_c[NL], m_b[NL], n_d[NL], n_c[NL], n_b[NL];
   const int tid = threadIdx.x;
@@ -319,7 +319,7 @@ __global__ void __launch_bounds__(2 * NL) k_sa_sweep4(SaT<SW> S) {
 
   // ---- phase 1 (1/d replaces ap, so that back-substitution multiplies)
   const int li = tid % NL, half = tid / NL;
-  const bool act = li < nl;
+  const bool act = tid < 2 * NL && li < nl;  // solver threads
   const int h = n / 2;
   auto at = [&](int p) { return p * NLP + li; };
   constexpr int R = 4;  // rows read ahead of the elimination chain

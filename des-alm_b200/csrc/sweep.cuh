@@ -37,7 +37,7 @@ namespace desalm {
 // ---------------------------------------------------------------------------
 // Shared-memory slab sweep.  A CTA owns NL lines of one plane (consecutive in
 // the transverse index that is contiguous in memory, or, for the i sweep,
-// NL rows of contiguous i lines) and 8 NL threads.
+// NL rows of contiguous i lines) and NT >= 8 NL threads.
 //   phase 0  tc, hc and the four transformed residuals of the slab are copied
 //            once (cp.async, all copies in flight, coalesced along the fastest
 //            global index) into shared memory laid out [node][line] (line
@@ -53,11 +53,12 @@ namespace desalm {
 // elements of W.
 // ---------------------------------------------------------------------------
 
-template <class T, class W, int DIR, int NL>
-__global__ void __launch_bounds__(8 * NL) k_sweep4(Lv<T, W> L, Par P, int blo, int bhi) {
+template <class T, class W, int DIR, int NL, int NT>
+__global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int bhi) {
   pdl_wait();
   pdl_trigger();
-  constexpr int NT = 8 * NL, NLP = NL + 1;
+  constexpr int NLP = NL + 1;
+  static_assert(NT >= 8 * NL, "every solver thread is part of the CTA");
   extern __shared__ __align__(16) unsigned char sweep_slab[];
   __shared__ W sbw[NL][4], sbe[NL][4];
   __shared__ W mt_d[NL][4], mt_u[NL][4], mt_b[NL][4];   // top half's last eliminated row
@@ -127,7 +128,7 @@ __global__ void __launch_bounds__(8 * NL) k_sweep4(Lv<T, W> L, Par P, int blo, i
   // ---- phase 1: two-ended elimination in shared memory
   const int li = tid % NL, combo = tid / NL;
   const int m = combo & 3, half = combo >> 2;
-  const bool act = li < nl;
+  const bool act = tid < 8 * NL && li < nl;  // solver threads
   W* __restrict__ r = s_r + m * fs;
   W* __restrict__ sd = s_d + m * fs;
   const W* __restrict__ ctc = s_tc;
