@@ -71,14 +71,15 @@ DESALM_HD inline int slab_fs(int np, int nlp) { return ((np * nlp + 31) / 32) * 
 // 8 NL (DAF sweeps, rsmooth) or 2 NL (SA sweeps) solve the lines.
 constexpr int kSlabThreads = 256;
 
-// Programmatic dependent launch: when a kernel is launched with programmatic
-// stream serialisation, pdl_wait() blocks until the grids it depends on have
-// completed and their writes are visible (it must come before the first
-// global-memory access), and pdl_trigger() lets the next grid in the stream
-// be scheduled once every CTA of this one has started.  Without that launch
-// attribute both are no-ops; every kernel of the library calls both first.
+// Programmatic dependent launch: every kernel of the library is launched with
+// programmatic stream serialisation, so its launch is processed while the
+// grid before it finishes; pdl_wait() then blocks until the grids it depends
+// on have completed and their writes are visible.  Every kernel calls it
+// before its first global-memory access.  No kernel signals an early launch
+// of its dependents (griddepcontrol.launch_dependents): that lets the next
+// grid's CTAs take SM resources while this one still runs, and measured
+// slower.
 DESALM_DEV void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
-DESALM_DEV void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
 
 template <class T> DESALM_DEV T dabs(T x) { return x < T(0) ? -x : x; }
 

@@ -14,7 +14,6 @@ namespace desalm {
 template <class T, class W, int DIR>
 __global__ void k_bcond(Lv<T, W> L, Par P, const T* rat, int ratdim) {
   pdl_wait();
-  pdl_trigger();
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   const int b = blockIdx.y;
   int amax, n, st, lb;
@@ -49,14 +48,12 @@ __global__ void k_bcond(Lv<T, W> L, Par P, const T* rat, int ratdim) {
 template <class T, class W>
 __global__ void k_pfix_read(Lv<T, W> L, int lfix, T* pfix) {
   pdl_wait();
-  pdl_trigger();
   *pfix = L.q[0][lfix];
 }
 // p <- p - pfix over the whole level (src/bcond_fm.F90:316-322)
 template <class T, class W>
 __global__ void k_pfix_sub(Lv<T, W> L, const T* pfix) {
   pdl_wait();
-  pdl_trigger();
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= L.N) return;
   L.q[0][l] = L.q[0][l] - *pfix;
@@ -69,7 +66,6 @@ __global__ void k_pfix_sub(Lv<T, W> L, const T* pfix) {
 template <class TF, class WF, class TC, class WC>
 __global__ void k_nlevel(Lv<TF, WF> F, Lv<TC, WC> C, int icrs, int jcrs, int kcrs) {
   pdl_wait();
-  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z;
@@ -157,7 +153,6 @@ struct Interp {
 template <class TF, class WF, class TC, class WC>
 __global__ void k_prolong_interp(Lv<TF, WF> F, Lv<TC, WC> C, WF* dq, int icrs, int jcrs, int kcrs) {
   pdl_wait();
-  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int k = blockIdx.z + 1;
@@ -174,7 +169,6 @@ __global__ void k_prolong_interp(Lv<TF, WF> F, Lv<TC, WC> C, WF* dq, int icrs, i
 template <class T, class W>
 __global__ void __launch_bounds__(256) k_norm_partial(Lv<T, W> L, double* part, int nf, int copy) {
   pdl_wait();
-  pdl_trigger();
   __shared__ double sh[5][256];
   const int ni = L.im - 2, nj = L.jm - 2, nk = L.km - 2;
   const long total = (long)ni * nj * nk;
@@ -221,7 +215,6 @@ DESALM_DEV void block_sum5(const double* part, int nblk, double out[5]) {
 
 __global__ void __launch_bounds__(256) k_norm_final(const double* part, int nblk, double* out) {
   pdl_wait();
-  pdl_trigger();
   double sums[5];
   block_sum5(part, nblk, sums);
   if (threadIdx.x == 0)
@@ -232,14 +225,12 @@ __global__ void __launch_bounds__(256) k_norm_final(const double* part, int nblk
 template <class T>
 __global__ void k_fill(T* a, T v, long n) {
   pdl_wait();
-  pdl_trigger();
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) a[t] = v;
 }
 template <class TD, class TS>
 __global__ void k_copy(TD* d, const TS* s, long n) {
   pdl_wait();
-  pdl_trigger();
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) d[t] = TD(s[t]);
 }
@@ -247,7 +238,6 @@ __global__ void k_copy(TD* d, const TS* s, long n) {
 template <class T>
 __global__ void k_extrapolate(T* q, const T* qn, const T* qnm1, long n) {
   pdl_wait();
-  pdl_trigger();
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) q[t] = T(2) * qn[t] - qnm1[t];
 }
@@ -255,7 +245,6 @@ __global__ void k_extrapolate(T* q, const T* qn, const T* qnm1, long n) {
 template <class T>
 __global__ void k_aos_to_soa(T* const* dst, const double* src, int me, long n) {
   pdl_wait();
-  pdl_trigger();
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   for (int m = 0; m < me; ++m) dst[m][t] = T(src[t * me + m]);
@@ -263,7 +252,6 @@ __global__ void k_aos_to_soa(T* const* dst, const double* src, int me, long n) {
 template <class T>
 __global__ void k_soa_to_aos(double* dst, T* const* src, int me, long n) {
   pdl_wait();
-  pdl_trigger();
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   for (int m = 0; m < me; ++m) dst[t * me + m] = double(src[m][t]);
@@ -273,7 +261,6 @@ __global__ void k_soa_to_aos(double* dst, T* const* src, int me, long n) {
 template <class TF, class TC>
 __global__ void k_inject(TC* c, const TF* f, int cim, int cjm, int ckm, int fim, int fjm, int icrs, int jcrs, int kcrs) {
   pdl_wait();
-  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
   const int k = blockIdx.z;
@@ -286,7 +273,6 @@ __global__ void k_inject(TC* c, const TF* f, int cim, int cjm, int ckm, int fim,
 template <class T>
 __global__ void k_recip(T* r, const T* a, long n) {
   pdl_wait();
-  pdl_trigger();
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) r[t] = T(1) / a[t];
 }
@@ -296,7 +282,6 @@ __global__ void k_recip(T* r, const T* a, long n) {
 __global__ void k_metrics(const double* x, const double* y, const double* z, int im, int jm, int km,
                           double dc, double de, double dz, double* const* cov, double* const* met, double* aj) {
   pdl_wait();
-  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
   const int k = blockIdx.z;
@@ -334,7 +319,6 @@ __global__ void k_metrics(const double* x, const double* y, const double* z, int
 // SA pseudo-time step on the fine level (src/mg_metrics.F90:262-282)
 __global__ void k_dtev(double* const* cov, double* dtev, long n, double cfl2, double vnn2, double ren, double delti, int unsteady) {
   pdl_wait();
-  pdl_trigger();
   long l = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= n) return;
   double xc = cov[0][l], xe = cov[1][l], xz = cov[2][l], yc = cov[3][l], ye = cov[4][l], yz = cov[5][l];
@@ -373,7 +357,6 @@ namespace desalm {
 template <class TF, class WF, int DIR, int NL>
 __global__ void __launch_bounds__(kSlabThreads) k_rsmooth4(Lv<TF, WF> F, WF* dq, const double* fac, const double* dpr, double e, int last) {
   pdl_wait();
-  pdl_trigger();
   constexpr int NT = kSlabThreads, NLP = NL + 1;
   extern __shared__ __align__(16) unsigned char rs_slab[];
   __shared__ WF s_top[NL][4], s_bot[NL][4];  // eliminated b of the two middle rows

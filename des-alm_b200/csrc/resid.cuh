@@ -110,7 +110,6 @@ DESALM_DEV T diss_fv(const Lv<T, W>& L, int dir, int l, int st, T dsq) {
 template <class T, class W, int MODE>
 __global__ void __launch_bounds__(128, DESALM_KR_MINBLOCKS) k_resid(Lv<T, W> L, Par P, int upwind, int calc_pk, int coarse, int bback) {
   pdl_wait();
-  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int k = blockIdx.z + 1;
@@ -311,7 +310,6 @@ __global__ void __launch_bounds__(128, DESALM_KR_MINBLOCKS) k_resid(Lv<T, W> L, 
 template <class T, class W>
 __global__ void k_dtau(Lv<T, W> L, Par P) {
   pdl_wait();
-  pdl_trigger();
   int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= L.N) return;
   const T rcfl = T(1) / T(P.cfl1), rvnn = T(1) / T(P.vnn1), rei = T(1) / T(P.ren);

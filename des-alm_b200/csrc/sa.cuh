@@ -57,7 +57,6 @@ DESALM_DEV double sa_ucn(const SaT<SW>& S, int d, int l) {
 template <class SW>
 __global__ void k_sa_ucn(SaT<SW> S) {
   pdl_wait();
-  pdl_trigger();
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= S.N) return;
 #pragma unroll
@@ -68,7 +67,6 @@ __global__ void k_sa_ucn(SaT<SW> S) {
 template <class SW>
 __global__ void k_sa_source(SaT<SW> S) {
   pdl_wait();
-  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int k = blockIdx.z + 1;
@@ -181,7 +179,6 @@ DESALM_DEV void sa_adi_row(const SaT<SW>& S, int l) {
 template <class SW>
 __global__ void __launch_bounds__(128) k_sa_rhs(SaT<SW> S) {
   pdl_wait();
-  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int k = blockIdx.z + 1;
@@ -280,7 +277,6 @@ __global__ void __launch_bounds__(128) k_sa_rhs(SaT<SW> S) {
 template <class SW, int DIR, int NL>
 __global__ void __launch_bounds__(kSlabThreads) k_sa_sweep4(SaT<SW> S) {
   pdl_wait();
-  pdl_trigger();
   constexpr int NT = kSlabThreads, NLP = NL + 1;
   extern __shared__ __align__(16) unsigned char sa_slab[];
   __shared__ SW m_d[NL], m_c[NL], m_b[NL], n_d[NL], n_c[NL], n_b[NL];
@@ -453,7 +449,6 @@ __global__ void __launch_bounds__(kSlabThreads) k_sa_sweep4(SaT<SW> S) {
 template <class SW, int DIR>
 __global__ void k_sa_bc(SaT<SW> S) {
   pdl_wait();
-  pdl_trigger();
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   const int b = blockIdx.y;
   int amax, n, st, lb;
@@ -479,7 +474,6 @@ __global__ void k_sa_bc(SaT<SW> S) {
 template <class SW>
 __global__ void k_sa_clamp(SaT<SW> S) {
   pdl_wait();
-  pdl_trigger();
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= S.N) return;
   double v = S.q[4][l];
@@ -494,7 +488,6 @@ __global__ void k_sa_clamp(SaT<SW> S) {
 // Sums of U/J over the first and last i planes (all j, k), into acc[0..1].
 __global__ void k_cons_sum(Sa S, double* acc) {
   pdl_wait();
-  pdl_trigger();
   __shared__ double sh[2][256];
   double a0 = 0, a1 = 0;
   const int P = S.jm * S.km;
@@ -517,7 +510,6 @@ __global__ void k_cons_sum(Sa S, double* acc) {
 // velocities with the covariant metrics (src/conservation.F90:137-157).
 __global__ void k_cons_apply(Sa S, const double* acc, double* const* cov) {
   pdl_wait();
-  pdl_trigger();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= S.jm * S.km) return;
   const int j = t % S.jm, k = t / S.jm;

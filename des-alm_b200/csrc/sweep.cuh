@@ -56,7 +56,6 @@ namespace desalm {
 template <class T, class W, int DIR, int NL, int NT>
 __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int bhi) {
   pdl_wait();
-  pdl_trigger();
   constexpr int NLP = NL + 1;
   static_assert(NT >= 8 * NL, "every solver thread is part of the CTA");
   extern __shared__ __align__(16) unsigned char sweep_slab[];
@@ -288,7 +287,6 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
 template <class T, class W, int DIR>
 __global__ void __launch_bounds__(128) k_xform(Lv<T, W> L) {
   pdl_wait();
-  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int k = blockIdx.z + 1;
