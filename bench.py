@@ -7,14 +7,15 @@ the case's itmax), one replica per GPU.
                   [--impl ours|reference]
 
 ours:       value = device-timed seconds per physical step of the product
-            configuration (MIXED precision: FP64 residual/update, FP32 line
-            sweeps and coarse levels; linear-extrapolation initial guess),
-            state resident in HBM.  e2e = the same step through the C ABI with
-            the state copied from pinned host memory and back every step.
-            The plain FP64 path (q^n guess, as the reference) is timed too.
+            configuration (MIXED precision: FP64 state, residual and update,
+            FP32 line-sweep work; linear-extrapolation initial guess), state
+            resident in HBM.  e2e = the same step through the C ABI with the
+            state copied from pinned host memory and back every step.  The
+            plain FP64 path (q^n guess, as the reference) is timed too.
 reference:  the CPU oracle (C++ restatement of the reference, FP32 like the
-            reference's own build, one thread) on the same case; a bounded
-            sample of pseudo-iterations scaled to one physical step.
+            reference's own build, its loops on every host thread) on the same
+            case; a bounded sample of pseudo-iterations scaled to one physical
+            step.
 
 Under torchrun each rank runs an independent replica on its own GPU
 (the path does not shard: no collective in the data path); times are the max
@@ -299,8 +300,9 @@ def run_ours(args, rank, world, dist):
 
 
 def cpu_baseline(case_name, iters_per_step, budget_s=20.0):
-    """The CPU oracle in FP32 (the reference's precision), one thread: a
-    bounded sample of pseudo-iterations, scaled to one physical step."""
+    """The CPU oracle in FP32 (the reference's precision) on every host
+    thread its OpenMP loops can use: a bounded sample of pseudo-iterations,
+    scaled to one physical step."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     case, grid, state, _ = build_case(case_name, abi.FP64, abi.PRED_QN)
@@ -316,9 +318,11 @@ def cpu_baseline(case_name, iters_per_step, budget_s=20.0):
         if time.perf_counter() - t0 > budget_s or k >= iters_per_step:
             break
     per_it = (time.perf_counter() - t0) / k
-    return {"value": per_it * iters_per_step, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": "%d pseudo-iterations of the first physical step (%.2f s each, FP32 oracle, 1 thread), "
-                      "scaled by the %d pseudo-iterations the FP64 GPU path needed per step" % (k, per_it, iters_per_step)}
+    nth = oracle.threads()
+    return {"value": per_it * iters_per_step, "unit": UNIT, "cores": nth, "kind": "port",
+            "sample": "%d pseudo-iterations of the first physical step (%.2f s each, FP32 oracle, %d threads), "
+                      "scaled by the %d pseudo-iterations the FP64 GPU path needed per step"
+                      % (k, per_it, nth, iters_per_step)}
 
 
 def run_reference(args):

@@ -62,8 +62,15 @@ def lib():
         L.desalm_oracle_gtsv.restype = C.c_int
         L.desalm_oracle_modal.argtypes = [dp, dp, dp, C.c_double, dp]
         L.desalm_oracle_modal.restype = None
+        L.desalm_oracle_threads.argtypes = []
+        L.desalm_oracle_threads.restype = C.c_int
         _LIB = L
     return _LIB
+
+
+def threads():
+    """Host threads the oracle's parallel loops use."""
+    return int(lib().desalm_oracle_threads())
 
 
 def _p(a):

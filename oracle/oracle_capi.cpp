@@ -174,6 +174,10 @@ int check_case(const desalm_case* c, std::string& why) {
 
 }  // namespace
 
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
 extern "C" {
 
 int desalm_oracle_init(const desalm_case* c, int real_bytes, void** out) {
@@ -189,6 +193,14 @@ int desalm_oracle_init(const desalm_case* c, int real_bytes, void** out) {
   return 0;
 }
 void desalm_oracle_destroy(void* ctx) { delete (Base*)ctx; }
+// Host threads the oracle's parallel loops use (1 in a serial build).
+int desalm_oracle_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
 int desalm_oracle_level_dims(void* ctx, int n, int* d) { return ((Base*)ctx)->dims(n, d); }
 int desalm_oracle_set_grid(void* ctx, const double* x, const double* y, const double* z, const double* wd) {
   return ((Base*)ctx)->set_grid(x, y, z, wd);

@@ -28,6 +28,16 @@
 #include <cstring>
 #include <string>
 #include <vector>
+
+// Loop nests whose iterations write disjoint elements run on every host
+// thread when the oracle is built with OpenMP (each element is computed by
+// the same expressions in the same order, so the results do not depend on
+// the thread count); reductions stay serial.
+#ifdef _OPENMP
+#define ORC_PARFOR _Pragma("omp parallel for schedule(static)")
+#else
+#define ORC_PARFOR
+#endif
 #include <algorithm>
 #include <stdexcept>
 #include <chrono>
@@ -396,6 +406,7 @@ struct Solver {
   // ------------------------------------------------------- residual pieces
   // rhs_contra_j (src/rhs_contra_j.F90:14-29) on all nodes.
   void contra_j(const Level<R>& G, std::vector<R>* ucn) const {
+    ORC_PARFOR
     for (long l = 0; l < G.N; ++l) {
       R tmp = R(1) / G.aj[l];
       R u = G.q[1][l], v = G.q[2][l], w = G.q[3][l];
@@ -409,6 +420,7 @@ struct Solver {
   void daf_dtau(Level<R>& G) const {
     const R cfl = R(c.cfl1), vnn = R(c.vnn1), rei = R(1) / R(c.ren);
     const R dcsq = G.dc * G.dc, desq = G.de * G.de, dzsq = G.dz * G.dz;
+    ORC_PARFOR
     for (long l = 0; l < G.N; ++l) {
       R g1 = G.csi[0][l] * G.csi[0][l] + G.csi[1][l] * G.csi[1][l] + G.csi[2][l] * G.csi[2][l];
       R g2 = G.eta[0][l] * G.eta[0][l] + G.eta[1][l] * G.eta[1][l] + G.eta[2][l] * G.eta[2][l];
@@ -452,6 +464,7 @@ struct Solver {
       out[2] = vtj * (n1 * uu3 + n2 * vv3 + n3 * ww3 + k1 * wc + k2 * we + k3 * wz);
     };
     // csi faces (src/rhs_viscous.F90:112-166)
+    ORC_PARFOR
     for (int k = 2; k <= km - 1; ++k)
       for (int j = 2; j <= jm - 1; ++j)
         for (int i = 1; i <= im - 1; ++i) {
@@ -469,6 +482,7 @@ struct Solver {
           flux(0, l0, l1, U[0], U[1], U[2], E[0], E[1], E[2], Z[0], Z[1], Z[2], o);
           for (int m = 0; m < 3; ++m) fv[m][l0] = o[m];
         }
+    ORC_PARFOR
     for (int k = 2; k <= km - 1; ++k)
       for (int j = 2; j <= jm - 1; ++j)
         for (int i = 2; i <= im - 1; ++i) {
@@ -476,6 +490,7 @@ struct Solver {
           for (int m = 0; m < 3; ++m) visc[m][l] = dc * (fv[m][l] - fv[m][lm]);
         }
     // eta faces (src/rhs_viscous.F90:189-243)
+    ORC_PARFOR
     for (int k = 2; k <= km - 1; ++k)
       for (int j = 1; j <= jm - 1; ++j)
         for (int i = 2; i <= im - 1; ++i) {
@@ -493,6 +508,7 @@ struct Solver {
           flux(1, l0, l1, U[0], U[1], U[2], E[0], E[1], E[2], Z[0], Z[1], Z[2], o);
           for (int m = 0; m < 3; ++m) fv[m][l0] = o[m];
         }
+    ORC_PARFOR
     for (int k = 2; k <= km - 1; ++k)
       for (int j = 2; j <= jm - 1; ++j)
         for (int i = 2; i <= im - 1; ++i) {
@@ -500,6 +516,7 @@ struct Solver {
           for (int m = 0; m < 3; ++m) visc[m][l] = visc[m][l] + de * (fv[m][l] - fv[m][lm]);
         }
     // zeta faces (src/rhs_viscous.F90:263-316)
+    ORC_PARFOR
     for (int k = 1; k <= km - 1; ++k)
       for (int j = 2; j <= jm - 1; ++j)
         for (int i = 2; i <= im - 1; ++i) {
@@ -517,6 +534,7 @@ struct Solver {
           flux(2, l0, l1, U[0], U[1], U[2], E[0], E[1], E[2], Z[0], Z[1], Z[2], o);
           for (int m = 0; m < 3; ++m) fv[m][l0] = o[m];
         }
+    ORC_PARFOR
     for (int k = 2; k <= km - 1; ++k)
       for (int j = 2; j <= jm - 1; ++j)
         for (int i = 2; i <= im - 1; ++i) {
@@ -532,6 +550,7 @@ struct Solver {
     std::vector<R> fv[3];
     for (int m = 0; m < 3; ++m) fv[m].assign(G.N, R(0));
     const std::vector<R>& p = G.q[0];
+    ORC_PARFOR
     for (int k = 1; k <= km; ++k)
       for (int j = 1; j <= jm; ++j)
         for (int i = 2; i <= im - 1; ++i) {
@@ -541,6 +560,7 @@ struct Solver {
           R tmp2 = dcsq * (p[G.id(i + 1, j, k)] - R(2) * p[l] + p[G.id(i - 1, j, k)]);
           fv[0][l] = tmp1 * tmp2;
         }
+    ORC_PARFOR
     for (int k = 1; k <= km; ++k)
       for (int j = 2; j <= jm - 1; ++j)
         for (int i = 1; i <= im; ++i) {
@@ -550,6 +570,7 @@ struct Solver {
           R tmp2 = desq * (p[G.id(i, j + 1, k)] - R(2) * p[l] + p[G.id(i, j - 1, k)]);
           fv[1][l] = tmp1 * tmp2;
         }
+    ORC_PARFOR
     for (int k = 2; k <= km - 1; ++k)
       for (int j = 1; j <= jm; ++j)
         for (int i = 1; i <= im; ++i) {
@@ -577,6 +598,7 @@ struct Solver {
       }
     std::fill(G.diss1.begin(), G.diss1.end(), R(0));
     const R pd = R(c.pdiss_coef);
+    ORC_PARFOR
     for (int k = 2; k <= km - 1; ++k)
       for (int j = 2; j <= jm - 1; ++j)
         for (int i = 2; i <= im - 1; ++i) {
@@ -594,6 +616,7 @@ struct Solver {
     const R dc2 = R(0.5) * G.dc, de2 = R(0.5) * G.de, dz2 = R(0.5) * G.dz;
     std::vector<R> p(G.N, R(0));
     for (long l = 0; l < G.N; ++l) p[l] = G.q[0][l] / G.aj[l];
+    ORC_PARFOR
     for (int k = 2; k <= km - 1; ++k)
       for (int j = 2; j <= jm - 1; ++j)
         for (int i = 2; i <= im - 1; ++i) {
@@ -625,6 +648,7 @@ struct Solver {
     for (int dir = 0; dir < 3; ++dir) {
       const long st = dir == 0 ? 1 : (dir == 1 ? (long)im : (long)im * jm);
       const R h = dsp[dir];
+      ORC_PARFOR
       for (int k = 2; k <= km - 1; ++k)
         for (int j = 2; j <= jm - 1; ++j)
           for (int i = 2; i <= im - 1; ++i) {
@@ -652,6 +676,7 @@ struct Solver {
   // after rhs_convec_quick (src/rhs_convec_quick.F90:433).
   void unst_visc_diss(Level<R>& G, const std::vector<R>* visc) const {
     const int im = G.im, jm = G.jm, km = G.km;
+    ORC_PARFOR
     for (int k = 2; k <= km - 1; ++k)
       for (int j = 2; j <= jm - 1; ++j)
         for (int i = 2; i <= im - 1; ++i) {
@@ -737,6 +762,7 @@ struct Solver {
   }
   void spectral_radii(const Level<R>& G, std::vector<R>* spr) const {
     for (int d = 0; d < 3; ++d) spr[d].assign(G.N, R(0));
+    ORC_PARFOR
     for (long l = 0; l < G.N; ++l) {
       R s, t; sigma_theta(G, l, s, t);
       R c1 = G.csi[0][l], c2 = G.csi[1][l], c3 = G.csi[2][l];
@@ -761,6 +787,7 @@ struct Solver {
     spectral_radii(G, spr);
     // r <- S * (-dtau * rh * J) (src/rhs_diag_solver.F90:53-72)
     const R alpha_mult = es * R(1.5) / R(c.delti);
+    ORC_PARFOR
     for (int k = 2; k <= km - 1; ++k)
       for (int j = 2; j <= jm - 1; ++j)
         for (int i = 2; i <= im - 1; ++i) {
@@ -770,13 +797,14 @@ struct Solver {
           for (int m = 0; m < 4; ++m) G.rh[m][l] = s[m] * (-G.dtau[l] * G.rh[m][l] * G.aj[l]);
         }
     const bool fine = (n == 0);
-    std::vector<R> aw, ap, ae, aq, dl, du;
     // one line of one direction: ids = interior node ids along the line,
     // lprev / lnext = the boundary nodes before and after it; bw / be = the
-    // semi-explicit boundary vectors (brh) or null.
+    // semi-explicit boundary vectors (brh) or null.  Scratch is per call, so
+    // lines may be solved concurrently.
     auto sweep_line = [&](int dir, const std::vector<long>& ids, long lprev, long lnext, const R* bw, const R* be) {
       int len = (int)ids.size();
-      aw.assign(len, 0); ap.assign(len, 0); ae.assign(len, 0); aq.assign(len, 0);
+      std::vector<R> aw(len, 0), ap(len, 0), ae(len, 0), aq(len, 0), dl, du;
+      long piv = 0;
       const R epd = R(c.ep[0][dir]);
       for (int m = 0; m < 4; ++m) {
         for (int p = 0; p < len; ++p) {
@@ -797,8 +825,14 @@ struct Solver {
         if (be) aq[len - 1] = aq[len - 1] - ae[len - 1] * be[m];
         dl.assign(aw.begin() + 1, aw.end());
         du.assign(ae.begin(), ae.end() - 1);
-        gtsv(len, 1, dl.data(), ap.data(), du.data(), aq.data(), len, &pivots);
+        gtsv(len, 1, dl.data(), ap.data(), du.data(), aq.data(), len, &piv);
         for (int p = 0; p < len; ++p) G.rh[m][ids[p]] = aq[p];
+      }
+      if (piv) {
+#ifdef _OPENMP
+#pragma omp atomic
+#endif
+        pivots += piv;
       }
     };
     auto sabc = [&](int b, const R* r1, const R* r2, R* out) {
@@ -822,15 +856,17 @@ struct Solver {
             getr(G.id(2, j, k), r1); getr(G.id(3, j, k), r2);
             sabc(0, r1, r2, &brh[bo(j, k)]);
           }
+      ORC_PARFOR
       for (int k = 2; k <= km - 1; ++k)
         for (int j = 2; j <= jm - 1; ++j)
           for (int i = 2; i <= im - 1; ++i) { long l = G.id(i, j, k); xform(l, mat_mai(G, l)); }
       if (bback)
         for (int k = 2; k <= km - 1; ++k)
           for (int j = 2; j <= jm - 1; ++j) xvec(&brh[bo(j, k)], mat_mai(G, G.id(1, j, k)));
-      std::vector<long> ids(im - 2);
+ORC_PARFOR
       for (int k = 2; k <= km - 1; ++k)
         for (int j = 2; j <= jm - 1; ++j) {
+          std::vector<long> ids(im - 2);
           for (int i = 2; i <= im - 1; ++i) ids[i - 2] = G.id(i, j, k);
           sweep_line(0, ids, G.id(1, j, k), G.id(im, j, k), bback ? &brh[bo(j, k)] : nullptr, nullptr);
         }
@@ -846,6 +882,7 @@ struct Solver {
           if (bl) { getr(G.id(i, 2, k), r1); getr(G.id(i, 3, k), r2); sabc(2, r1, r2, &b1[bo(i, k)]); }
           if (br) { getr(G.id(i, jm - 1, k), r1); getr(G.id(i, jm - 2, k), r2); sabc(3, r1, r2, &b2[bo(i, k)]); }
         }
+      ORC_PARFOR
       for (int k = 2; k <= km - 1; ++k)
         for (int j = 2; j <= jm - 1; ++j)
           for (int i = 2; i <= im - 1; ++i) { long l = G.id(i, j, k); xform(l, mat_n1i(G, l)); }
@@ -854,9 +891,10 @@ struct Solver {
           if (bl) xvec(&b1[bo(i, k)], mat_n1i(G, G.id(i, 1, k)));
           if (br) xvec(&b2[bo(i, k)], mat_n1i(G, G.id(i, jm, k)));
         }
-      std::vector<long> ids(jm - 2);
+ORC_PARFOR
       for (int k = 2; k <= km - 1; ++k)
         for (int i = 2; i <= im - 1; ++i) {
+          std::vector<long> ids(jm - 2);
           for (int j = 2; j <= jm - 1; ++j) ids[j - 2] = G.id(i, j, k);
           sweep_line(1, ids, G.id(i, 1, k), G.id(i, jm, k), bl ? &b1[bo(i, k)] : nullptr, br ? &b2[bo(i, k)] : nullptr);
         }
@@ -875,6 +913,7 @@ struct Solver {
           if (bd) { getr(G.id(i, j, 2), r1); getr(G.id(i, j, 3), r2); sabc(4, r1, r2, &b1[bo(i, j)]); }
           if (bu_set) { getr(G.id(i, j, km - 1), r1); getr(G.id(i, j, km - 2), r2); sabc(5, r1, r2, &b2[bo(i, j)]); }
         }
+      ORC_PARFOR
       for (int k = 2; k <= km - 1; ++k)
         for (int j = 2; j <= jm - 1; ++j)
           for (int i = 2; i <= im - 1; ++i) { long l = G.id(i, j, k); xform(l, mat_n2i(G, l)); }
@@ -883,14 +922,16 @@ struct Solver {
           if (bd) xvec(&b1[bo(i, j)], mat_n2i(G, G.id(i, j, 1)));
           if (bu_use) xvec(&b2[bo(i, j)], mat_n2i(G, G.id(i, j, km)));
         }
-      std::vector<long> ids(km - 2);
+ORC_PARFOR
       for (int j = 2; j <= jm - 1; ++j)
         for (int i = 2; i <= im - 1; ++i) {
+          std::vector<long> ids(km - 2);
           for (int k = 2; k <= km - 1; ++k) ids[k - 2] = G.id(i, j, k);
           sweep_line(2, ids, G.id(i, j, 1), G.id(i, j, km), bd ? &b1[bo(i, j)] : nullptr, bu_use ? &b2[bo(i, j)] : nullptr);
         }
     }
     // dq = Mc * r (src/rhs_diag_solver.F90:624-633)
+    ORC_PARFOR
     for (int k = 2; k <= km - 1; ++k)
       for (int j = 2; j <= jm - 1; ++j)
         for (int i = 2; i <= im - 1; ++i) { long l = G.id(i, j, k); xform(l, mat_mc(G, l)); }
@@ -968,6 +1009,7 @@ struct Solver {
     for (int m = 0; m < 4; ++m) std::fill(G.rh[m].begin(), G.rh[m].end(), R(0));
     residual(G, n, true, itr == 1 ? 1 : 0);
     diag_solver(G, n);
+    ORC_PARFOR
     for (int k = 2; k <= km - 1; ++k)
       for (int j = 2; j <= jm - 1; ++j)
         for (int i = 2; i <= im - 1; ++i) {
@@ -997,6 +1039,7 @@ struct Solver {
     for (int m = 0; m < 4; ++m) C.qold[m] = C.q[m];
     const long ic = 1, ie = F.im, iz = (long)F.im * F.jm;
     const R p25 = R(0.25), p5 = R(0.5), two = R(2), s16 = R(1) / R(16);
+    ORC_PARFOR
     for (int k = 1; k <= C.km; ++k)
       for (int j = 1; j <= C.jm; ++j)
         for (int i = 1; i <= C.im; ++i) {
@@ -1048,6 +1091,7 @@ struct Solver {
     const int im = F.im, jm = F.jm, km = F.km;
     std::vector<R> dq[4];
     for (int m = 0; m < 4; ++m) dq[m].assign(F.N, R(0));
+    ORC_PARFOR
     for (int k = 1; k <= C.km; ++k)
       for (int j = 1; j <= C.jm; ++j)
         for (int i = 1; i <= C.im; ++i) {
@@ -1058,6 +1102,7 @@ struct Solver {
     const R cp = R(0.5), cm = R(0.5);
     const long ie = im, iz = (long)im * jm;
     if (c.kcrs == 1)
+ORC_PARFOR
       for (int k = 2; k <= km - 1; k += 2)
         for (int j = 1; j <= jm; j += (1 << c.jcrs))
           for (int i = 1; i <= im; i += (1 << c.icrs)) {
@@ -1065,6 +1110,7 @@ struct Solver {
             for (int m = 0; m < 4; ++m) dq[m][l] = cp * dq[m][l + iz] + cm * dq[m][l - iz];
           }
     if (c.jcrs == 1)
+ORC_PARFOR
       for (int k = 1; k <= km; ++k)
         for (int j = 2; j <= jm - 1; j += 2)
           for (int i = 1; i <= im; i += (1 << c.icrs)) {
@@ -1072,6 +1118,7 @@ struct Solver {
             for (int m = 0; m < 4; ++m) dq[m][l] = cp * dq[m][l + ie] + cm * dq[m][l - ie];
           }
     if (c.icrs == 1)
+ORC_PARFOR
       for (int k = 1; k <= km; ++k)
         for (int j = 1; j <= jm; ++j)
           for (int i = 2; i <= im - 1; i += 2) {
@@ -1084,10 +1131,11 @@ struct Solver {
       const R e = R(c.ep[1][dir]);
       int len = ext[dir] - 2;
       if (len <= 0) continue;
-      std::vector<R> ax(len), bx(len), cx(len), dx((long)4 * len);
       int a1 = dir == 0 ? jm : im, a2 = dir == 2 ? jm : km;
+ORC_PARFOR
       for (int q2 = 2; q2 <= a2 - 1; ++q2)
         for (int q1 = 2; q1 <= a1 - 1; ++q1) {
+          std::vector<R> ax(len), bx(len), cx(len), dx((long)4 * len);
           std::vector<long> ids(len);
           for (int p = 0; p < len; ++p) {
             int t = p + 2;
@@ -1149,6 +1197,7 @@ struct Solver {
     contra_j(G, ucn);
     auto id = [&](int i, int j, int k) { return G.id(i, j, k); };
     // rhs_sa_source (src/rhs_sa_source.F90:35-95): interior only
+    ORC_PARFOR
     for (int k = 2; k <= km - 1; ++k)
       for (int j = 2; j <= jm - 1; ++j)
         for (int i = 2; i <= im - 1; ++i) {
@@ -1172,6 +1221,7 @@ struct Solver {
       // rhs_sa_grdnu (src/rhs_sa_grdnu.F90:22-60)
       std::vector<R> q5j(G.N);
       for (long l = 0; l < G.N; ++l) q5j[l] = q5[l] / G.aj[l];
+      ORC_PARFOR
       for (int k = 2; k <= km - 1; ++k)
         for (int j = 2; j <= jm - 1; ++j)
           for (int i = 2; i <= im - 1; ++i) {
@@ -1189,6 +1239,7 @@ struct Solver {
             dnu[l] = aj2 * (dn[0] * dn[0] + dn[1] * dn[1] + dn[2] * dn[2]);
           }
       // rhs_sa_prod (src/rhs_sa_prod.F90:32-100)
+      ORC_PARFOR
       for (int k = 2; k <= km - 1; ++k)
         for (int j = 2; j <= jm - 1; ++j)
           for (int i = 2; i <= im - 1; ++i) {
@@ -1230,6 +1281,7 @@ struct Solver {
         return vtj * (k1 * vcs + k2 * vet + k3 * vze);
       };
       std::fill(fv.begin(), fv.end(), R(0));
+      ORC_PARFOR
       for (int k = 2; k <= km - 1; ++k)
         for (int j = 2; j <= jm - 1; ++j)
           for (int i = 1; i <= im - 1; ++i) {
@@ -1241,6 +1293,7 @@ struct Solver {
       for (int k = 2; k <= km - 1; ++k)
         for (int j = 2; j <= jm - 1; ++j)
           for (int i = 2; i <= im - 1; ++i) visc[id(i, j, k)] = fv[id(i, j, k)] - fv[id(i - 1, j, k)];
+      ORC_PARFOR
       for (int k = 2; k <= km - 1; ++k)
         for (int j = 1; j <= jm - 1; ++j)
           for (int i = 2; i <= im - 1; ++i) {
@@ -1252,6 +1305,7 @@ struct Solver {
       for (int k = 2; k <= km - 1; ++k)
         for (int j = 2; j <= jm - 1; ++j)
           for (int i = 2; i <= im - 1; ++i) visc[id(i, j, k)] = visc[id(i, j, k)] + fv[id(i, j, k)] - fv[id(i, j - 1, k)];
+      ORC_PARFOR
       for (int k = 1; k <= km - 1; ++k)
         for (int j = 2; j <= jm - 1; ++j)
           for (int i = 2; i <= im - 1; ++i) {
@@ -1267,6 +1321,7 @@ struct Solver {
       const long st[3] = {1, (long)im, (long)im * jm};
       for (int dir = 0; dir < 3; ++dir) {
         std::fill(fv.begin(), fv.end(), R(0));
+        ORC_PARFOR
         for (int k = (dir == 2 ? 1 : 2); k <= km - 1; ++k)
           for (int j = (dir == 1 ? 1 : 2); j <= jm - 1; ++j)
             for (int i = (dir == 0 ? 1 : 2); i <= im - 1; ++i) {
@@ -1285,6 +1340,7 @@ struct Solver {
       // rhs_sa_unst_visc (src/rhs_sa_unst_visc.F90:18-30) and
       // rhs_sa_implicit_source (src/rhs_sa_implicit_source.F90:41-53); the
       // boundary values of rh are then zeroed (src/des_eddy.F90:231-236).
+      ORC_PARFOR
       for (int k = 1; k <= km; ++k)
         for (int j = 1; j <= jm; ++j)
           for (int i = 1; i <= im; ++i) {
@@ -1301,10 +1357,11 @@ struct Solver {
       const std::vector<R>* met[3] = {G.csi, G.eta, G.zet};
       for (int dir = 0; dir < 3; ++dir) {
         int len = ext[dir] - 2;
-        std::vector<R> av(len + 1), aw(len), ap(len), ae(len), aq(len);
         int a1 = dir == 0 ? jm : im, a2 = dir == 2 ? jm : km;
+ORC_PARFOR
         for (int p2 = 2; p2 <= a2 - 1; ++p2)
           for (int p1 = 2; p1 <= a1 - 1; ++p1) {
+            std::vector<R> av(len + 1), aw(len), ap(len), ae(len), aq(len);
             auto node = [&](int t) { return dir == 0 ? id(t, p1, p2) : (dir == 1 ? id(p1, t, p2) : id(p1, p2, t)); };
             for (int t = 1; t <= ext[dir] - 1; ++t) {  // av(t) on the face t+1/2
               long l0 = node(t), l1 = node(t + 1);
@@ -1325,11 +1382,19 @@ struct Solver {
               aq[p] = rh[l];
             }
             std::vector<R> dl(aw.begin() + 1, aw.end()), du(ae.begin(), ae.end() - 1);
-            gtsv(len, 1, dl.data(), ap.data(), du.data(), aq.data(), len, &pivots);
+            long piv = 0;
+            gtsv(len, 1, dl.data(), ap.data(), du.data(), aq.data(), len, &piv);
+            if (piv) {
+#ifdef _OPENMP
+#pragma omp atomic
+#endif
+              pivots += piv;
+            }
             for (int t = 2; t <= ext[dir] - 1; ++t) rh[node(t)] = aq[t - 2];
           }
       }
       // update (src/des_eddy.F90:260-272)
+      ORC_PARFOR
       for (int k = 2; k <= km - 1; ++k)
         for (int j = 2; j <= jm - 1; ++j)
           for (int i = 2; i <= im - 1; ++i) {
