@@ -14,6 +14,7 @@
 #include <vector>
 #include <algorithm>
 #include <utility>
+#include <random>
 
 #include "desalm.h"
 #include "common.cuh"
@@ -21,6 +22,7 @@
 #include "sweep.cuh"
 #include "mg.cuh"
 #include "sa.cuh"
+#include "learn.cuh"
 
 using namespace desalm;
 
@@ -110,6 +112,30 @@ struct Level {
   bool dtau_valid = false;
 };
 
+// State of the learned initial guess (learn.cuh).
+struct LpState {
+  bool on = false;
+  long N = 0;
+  LpLayer ly[4];
+  long nparam = 0;
+  float *theta = nullptr, *grad = nullptr, *m = nullptr, *v = nullptr;  // flat parameters, gradient, Adam moments
+  bf16 *wf[4] = {}, *wd[4] = {};           // forward / data-gradient weight blocks
+  float *dW[4] = {}, *db[4] = {};          // per-layer gradient accumulators
+  bf16 *x0 = nullptr, *a[3] = {}, *dy4 = nullptr, *dya[2] = {};  // features, activations, gradients
+  float *y = nullptr, *t = nullptr;        // network output, training target [5][N]
+  float *rs = nullptr, *rs5 = nullptr, *s5 = nullptr;  // feature scales (1/RMS), output scales and their reciprocals
+  double* acc = nullptr;                   // reductions
+  double* qnm2[5] = {};                    // q^{n-2} of the fine level
+  double** tab = nullptr;                  // device table: q[5] qn[5] qnm1[5] qnm2[5]
+  bool scaled = false;
+  int shifts = 0;                          // history shifts since the state was set
+  long samples = 0, steps = 0, predictions = 0, adam_t = 0;
+  double first_loss = -1, last_loss = -1;
+  int train_steps = 8;                     // Adam steps per new sample
+  int warm = 2;                            // samples before the network's guess is used
+  float lr = 1e-3f;
+};
+
 }  // namespace
 
 struct desalm_ctx {
@@ -133,6 +159,7 @@ struct desalm_ctx {
   double* h_norm = nullptr;   // pinned host [5]
   double* stage = nullptr;    // device staging of one host state array, 5 N (component-fastest)
   double** ftab = nullptr;    // device table of the fine level's q[5], qn[5], qnm1[5] field pointers
+  LpState lp;                 // learned initial guess (predictor DESALM_PRED_LEARNED)
   int* flags = nullptr;       // device [2]
   SaWork sa{};
   // per-kernel CUDA-event timing (desalm_profile) and launch counter
@@ -184,7 +211,7 @@ inline unsigned cdiv(long a, long b) { return (unsigned)((a + b - 1) / b); }
 // kernel classes for desalm_kernel_stats
 enum KClass { KC_DTAU = 0, KC_RESID, KC_SWEEP_I, KC_SWEEP_J, KC_SWEEP_K, KC_RECALC, KC_BCOND, KC_PFIX,
               KC_NLEVEL, KC_PROLONG, KC_RSMOOTH, KC_NORM, KC_SA_RHS, KC_SA_SWEEP, KC_SA_BC,
-              KC_XFORM_I, KC_XFORM_J, KC_XFORM_K, KC_SA_AUX, KC_MISC, KC_COUNT };
+              KC_XFORM_I, KC_XFORM_J, KC_XFORM_K, KC_SA_AUX, KC_LEARN, KC_MISC, KC_COUNT };
 
 struct ProfScope {
   desalm_ctx* ctx;
@@ -259,7 +286,8 @@ int check_case(desalm_ctx* ctx, const desalm_case& c) {
   for (int b = 0; b < 6; ++b)
     if (c.btype[b] == 5) return bad("btype 5 (characteristics outlet) is not supported");
   if (c.precision_mode != DESALM_FP64 && c.precision_mode != DESALM_MIXED) return bad("unknown precision_mode");
-  if (c.predictor != DESALM_PRED_QN && c.predictor != DESALM_PRED_LINEAR) return bad("unknown predictor");
+  if (c.predictor != DESALM_PRED_QN && c.predictor != DESALM_PRED_LINEAR && c.predictor != DESALM_PRED_LEARNED)
+    return bad("unknown predictor");
   if (c.ifix < 1 || c.ifix > c.im || c.jfix < 1 || c.jfix > c.jm || c.kfix < 1 || c.kfix > c.km)
     return bad("pressure reference node outside the grid");
   // vertex-centred coarsening (ii = 2i - 1) needs odd extents on every level
@@ -670,6 +698,257 @@ int graph_step(desalm_ctx* ctx, desalm_step_report* rep);
 int sa_des_eddy(desalm_ctx* ctx);
 int sa_conservation(desalm_ctx* ctx);
 
+
+// ----------------------------------------------------------- learned guess
+template <int CIN, int COUT_PAD>
+int lp_conv(desalm_ctx* ctx, const bf16* in, const bf16* w, const float* bias, int relu, const bf16* mask, bf16* out,
+            float* out32, int cout_store) {
+  LpState& lp = ctx->lp;
+  const Level& F = ctx->L[0];
+  LpGrid G{F.im, F.jm, F.km, lp.N};
+  const long tiles = (lp.N + LP_TM - 1) / LP_TM;
+  const unsigned grid = (unsigned)std::min<long>(tiles, 148L * 2);
+  LAUNCH(KC_LEARN, 0, (double)lp.N, launch_k(k_lp_conv<CIN, COUT_PAD>, grid, 256, LpConvSmem<CIN, COUT_PAD>::total, ctx->stream,
+                                             G, in, w, bias, relu, mask, out, out32, cout_store));
+  CKL();
+  return 0;
+}
+
+template <int CIN, int COUT_PAD>
+int lp_wgrad(desalm_ctx* ctx, const bf16* X, const bf16* dY, float* dW) {
+  LpState& lp = ctx->lp;
+  const Level& F = ctx->L[0];
+  LpGrid G{F.im, F.jm, F.km, lp.N};
+  const long per = (long)LP_TM * 64;  // nodes per CTA
+  LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_wgrad<CIN, COUT_PAD>, cdiv(lp.N, per), 128, 0, ctx->stream, G, X, dY, dW, per));
+  CKL();
+  return 0;
+}
+
+cudaError_t lp_attrs() {
+  cudaError_t e = cudaFuncSetAttribute((const void*)k_lp_conv<16, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)LpConvSmem<16, 32>::total);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)k_lp_conv<32, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)LpConvSmem<32, 32>::total);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)k_lp_conv<32, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)LpConvSmem<32, 16>::total);
+  return e;
+}
+
+// Buffers and initial weights (He normal, seeded; the last layer scaled by
+// 0.1 so that the first guesses stay close to the linear extrapolation).
+int lp_alloc(desalm_ctx* ctx) {
+  LpState& lp = ctx->lp;
+  const Level& F = ctx->L[0];
+  lp.N = F.N;
+  const int cin[4] = {15, 32, 32, 32}, cout[4] = {32, 32, 32, 5};
+  const int cinp[4] = {16, 32, 32, 32}, coutp[4] = {32, 32, 32, 16};
+  long off = 0;
+  for (int l = 0; l < 4; ++l) {
+    LpLayer& y = lp.ly[l];
+    y.cin = cin[l]; y.cout = cout[l]; y.cin_pad = cinp[l]; y.cout_pad = coutp[l];
+    y.woff = off; off += (long)y.cout * y.cin * 27;
+    y.boff = off; off += y.cout;
+  }
+  lp.nparam = off;
+  auto A = [&](void** p, size_t bytes) { return dalloc(ctx, ctx->allocs, p, bytes); };
+  const long N = lp.N;
+  RET(A((void**)&lp.theta, off * sizeof(float))); RET(A((void**)&lp.grad, off * sizeof(float)));
+  RET(A((void**)&lp.m, off * sizeof(float))); RET(A((void**)&lp.v, off * sizeof(float)));
+  for (int l = 0; l < 4; ++l) {
+    const size_t wb = 27L * cinp[l] * coutp[l];
+    RET(A((void**)&lp.wf[l], wb * sizeof(bf16))); RET(A((void**)&lp.wd[l], wb * sizeof(bf16)));
+    RET(A((void**)&lp.dW[l], wb * sizeof(float))); RET(A((void**)&lp.db[l], coutp[l] * sizeof(float)));
+  }
+  RET(A((void**)&lp.x0, 16L * N * sizeof(bf16)));
+  for (int l = 0; l < 3; ++l) RET(A((void**)&lp.a[l], 32L * N * sizeof(bf16)));
+  RET(A((void**)&lp.dy4, 16L * N * sizeof(bf16)));
+  for (int l = 0; l < 2; ++l) RET(A((void**)&lp.dya[l], 32L * N * sizeof(bf16)));
+  RET(A((void**)&lp.y, 5L * N * sizeof(float))); RET(A((void**)&lp.t, 5L * N * sizeof(float)));
+  RET(A((void**)&lp.rs, 16 * sizeof(float))); RET(A((void**)&lp.rs5, 8 * sizeof(float)));
+  RET(A((void**)&lp.s5, 8 * sizeof(float))); RET(A((void**)&lp.acc, 16 * sizeof(double)));
+  for (int f = 0; f < 5; ++f) RET(A((void**)&lp.qnm2[f], N * sizeof(double)));
+  RET(A((void**)&lp.tab, 20 * sizeof(double*)));
+  cudaStream_t s = ctx->stream;
+  double* tab[20];
+  int esz = 8;
+  for (int f = 0; f < 5; ++f) {
+    RET(field_ptr(ctx, 0, DESALM_F_Q + f, (void**)&tab[f], &esz));
+    RET(field_ptr(ctx, 0, DESALM_F_QN + f, (void**)&tab[5 + f], &esz));
+    RET(field_ptr(ctx, 0, DESALM_F_QNM1 + f, (void**)&tab[10 + f], &esz));
+    tab[15 + f] = lp.qnm2[f];
+  }
+  CK(cudaMemcpyAsync(lp.tab, tab, sizeof(tab), cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(lp.dy4, 0, 16L * N * sizeof(bf16), s));
+  CK(cudaMemsetAsync(lp.m, 0, off * sizeof(float), s));
+  CK(cudaMemsetAsync(lp.v, 0, off * sizeof(float), s));
+  std::vector<float> th(off, 0.0f);
+  std::mt19937 rng(20241203u);
+  for (int l = 0; l < 4; ++l) {
+    const LpLayer& y = lp.ly[l];
+    std::normal_distribution<float> nd(0.0f, std::sqrt(2.0f / (27.0f * y.cin)) * (l == 3 ? 0.1f : 1.0f));
+    for (long e = 0; e < (long)y.cout * y.cin * 27; ++e) th[y.woff + e] = nd(rng);
+  }
+  CK(cudaMemcpyAsync(lp.theta, th.data(), off * sizeof(float), cudaMemcpyHostToDevice, s));
+  CK(cudaStreamSynchronize(s));
+  lp.on = true;
+  return 0;
+}
+
+int lp_pack(desalm_ctx* ctx) {
+  LpState& lp = ctx->lp;
+  for (int l = 0; l < 4; ++l) {
+    const long total = 27L * lp.ly[l].cin_pad * lp.ly[l].cout_pad;
+    LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_pack, cdiv(total, 256), 256, 0, ctx->stream, lp.ly[l], (const float*)lp.theta, lp.wf[l], lp.wd[l]));
+  }
+  CKL();
+  return 0;
+}
+
+// Forward pass on lp.x0: activations a[0..2], output y (FP32).
+int lp_forward(desalm_ctx* ctx) {
+  LpState& lp = ctx->lp;
+  const float* b[4];
+  for (int l = 0; l < 4; ++l) b[l] = lp.theta + lp.ly[l].boff;
+  // the bias pointers index the flat vector: each layer's bias is contiguous there
+  RET((lp_conv<16, 32>(ctx, lp.x0, lp.wf[0], b[0], 1, nullptr, lp.a[0], nullptr, 32)));
+  RET((lp_conv<32, 32>(ctx, lp.a[0], lp.wf[1], b[1], 1, nullptr, lp.a[1], nullptr, 32)));
+  RET((lp_conv<32, 32>(ctx, lp.a[1], lp.wf[2], b[2], 1, nullptr, lp.a[2], nullptr, 32)));
+  RET((lp_conv<32, 16>(ctx, lp.a[2], lp.wf[3], b[3], 0, nullptr, nullptr, lp.y, 5)));
+  return 0;
+}
+
+// Loss against lp.t and the gradient of the mean squared error in lp.grad;
+// the loss goes to *loss (host, after a synchronize).
+int lp_backward(desalm_ctx* ctx, double* loss) {
+  LpState& lp = ctx->lp;
+  cudaStream_t s = ctx->stream;
+  const long N = lp.N;
+  for (int l = 0; l < 4; ++l) {
+    CK(cudaMemsetAsync(lp.dW[l], 0, 27L * lp.ly[l].cin_pad * lp.ly[l].cout_pad * sizeof(float), s));
+    CK(cudaMemsetAsync(lp.db[l], 0, lp.ly[l].cout_pad * sizeof(float), s));
+  }
+  CK(cudaMemsetAsync(lp.acc, 0, sizeof(double), s));
+  LAUNCH(KC_LEARN, 0, (double)N, launch_k(k_lp_loss, 296, 256, 0, s, N, (const float*)lp.y, (const float*)lp.t, lp.dy4, lp.acc));
+  CKL();
+  // layer 4 (a[2] -> y)
+  RET((lp_wgrad<32, 16>(ctx, lp.a[2], lp.dy4, lp.dW[3])));
+  LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_bias_grad, dim3(64, 5), 256, 0, s, N, (const bf16*)lp.dy4, lp.db[3]));
+  RET((lp_conv<16, 32>(ctx, lp.dy4, lp.wd[3], nullptr, 0, lp.a[2], lp.dya[0], nullptr, 32)));
+  // layer 3 (a[1] -> a[2])
+  RET((lp_wgrad<32, 32>(ctx, lp.a[1], lp.dya[0], lp.dW[2])));
+  LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_bias_grad, dim3(64, 32), 256, 0, s, N, (const bf16*)lp.dya[0], lp.db[2]));
+  RET((lp_conv<32, 32>(ctx, lp.dya[0], lp.wd[2], nullptr, 0, lp.a[1], lp.dya[1], nullptr, 32)));
+  // layer 2 (a[0] -> a[1])
+  RET((lp_wgrad<32, 32>(ctx, lp.a[0], lp.dya[1], lp.dW[1])));
+  LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_bias_grad, dim3(64, 32), 256, 0, s, N, (const bf16*)lp.dya[1], lp.db[1]));
+  RET((lp_conv<32, 32>(ctx, lp.dya[1], lp.wd[1], nullptr, 0, lp.a[0], lp.dya[0], nullptr, 32)));
+  // layer 1 (x0 -> a[0])
+  RET((lp_wgrad<16, 32>(ctx, lp.x0, lp.dya[0], lp.dW[0])));
+  LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_bias_grad, dim3(64, 32), 256, 0, s, N, (const bf16*)lp.dya[0], lp.db[0]));
+  const float gscale = float(2.0 / (5.0 * double(N)));
+  for (int l = 0; l < 4; ++l) {
+    const long n = (long)lp.ly[l].cout * lp.ly[l].cin * 27 + lp.ly[l].cout;
+    LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_gather_grad, cdiv(n, 256), 256, 0, s, lp.ly[l], (const float*)lp.dW[l],
+                                      (const float*)lp.db[l], gscale, lp.grad));
+  }
+  CKL();
+  double sum = 0;
+  CK(cudaMemcpyAsync(&sum, lp.acc, sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (loss) *loss = sum / (5.0 * double(N));
+  return 0;
+}
+
+// Features of (qn, qnm1, qnm2) at table offsets (a, b, c) into lp.x0; the
+// scales are fixed from the first call.
+int lp_features(desalm_ctx* ctx, int a, int b, int c) {
+  LpState& lp = ctx->lp;
+  cudaStream_t s = ctx->stream;
+  const long N = lp.N;
+  if (!lp.scaled) {
+    CK(cudaMemsetAsync(lp.acc, 0, 16 * sizeof(double), s));
+    LAUNCH(KC_LEARN, 0, (double)N, launch_k(k_lp_sumsq, 296, 128, 0, s, N, (const double* const*)(lp.tab + a),
+                                            (const double* const*)(lp.tab + b), (const double* const*)(lp.tab + c), lp.acc));
+    CKL();
+    double h[16];
+    CK(cudaMemcpyAsync(h, lp.acc, 16 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    float rs[16] = {0}, s5[8] = {0}, rs5[8] = {0};
+    for (int ch = 0; ch < 15; ++ch) {
+      const double rms = std::sqrt(h[ch] / double(N));
+      rs[ch] = rms > 1e-30 ? float(1.0 / rms) : 1.0f;
+    }
+    for (int f = 0; f < 5; ++f) { rs5[f] = rs[3 * f + 1]; s5[f] = 1.0f / rs5[f]; }
+    CK(cudaMemcpyAsync(lp.rs, rs, sizeof(rs), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(lp.s5, s5, sizeof(s5), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(lp.rs5, rs5, sizeof(rs5), cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    lp.scaled = true;
+  }
+  LAUNCH(KC_LEARN, 0, (double)N, launch_k(k_lp_features, cdiv(N, 256), 256, 0, s, N, (const double* const*)(lp.tab + a),
+                                          (const double* const*)(lp.tab + b), (const double* const*)(lp.tab + c),
+                                          (const float*)lp.rs, lp.x0));
+  CKL();
+  return 0;
+}
+
+// One Adam step on the sample in lp.x0 / lp.t.
+int lp_train_step(desalm_ctx* ctx, double* loss) {
+  LpState& lp = ctx->lp;
+  RET(lp_pack(ctx));
+  RET(lp_forward(ctx));
+  RET(lp_backward(ctx, loss));
+  lp.adam_t += 1;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = float(1.0 / (1.0 - std::pow(double(b1), double(lp.adam_t))));
+  const float c2 = float(1.0 / (1.0 - std::pow(double(b2), double(lp.adam_t))));
+  LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_adam, cdiv(lp.nparam, 256), 256, 0, ctx->stream, lp.nparam, lp.theta,
+                                    (const float*)lp.grad, lp.m, lp.v, lp.lr, b1, b2, 1e-8f, c1, c2));
+  CKL();
+  lp.steps += 1;
+  return 0;
+}
+
+// At the start of a physical step, before the history shift: the newest
+// converged level q is the target of a sample whose features come from
+// (qn, qnm1, qnm2); train on it.
+int lp_learn(desalm_ctx* ctx) {
+  LpState& lp = ctx->lp;
+  if (lp.shifts < 1) return 0;  // q^{n-2} not known yet
+  RET(lp_features(ctx, 5, 10, 15));
+  LAUNCH(KC_LEARN, 0, (double)lp.N, launch_k(k_lp_target, cdiv(lp.N, 256), 256, 0, ctx->stream, lp.N,
+                                             (const double* const*)(lp.tab + 0), (const double* const*)(lp.tab + 5),
+                                             (const double* const*)(lp.tab + 10), (const float*)lp.rs5, lp.t));
+  CKL();
+  lp.samples += 1;
+  for (int it = 0; it < lp.train_steps; ++it) {
+    double loss = 0;
+    RET(lp_train_step(ctx, &loss));
+    if (lp.first_loss < 0) lp.first_loss = loss;
+    lp.last_loss = loss;
+  }
+  return 0;
+}
+
+// After the shift and the linear extrapolation: q <- 2 q^n - q^{n-1} + the
+// network's correction, once it has seen lp.warm samples.
+int lp_predict(desalm_ctx* ctx) {
+  LpState& lp = ctx->lp;
+  if (lp.samples < lp.warm || lp.shifts < 1) return 0;
+  RET(lp_features(ctx, 5, 10, 15));
+  RET(lp_pack(ctx));
+  RET(lp_forward(ctx));
+  LAUNCH(KC_LEARN, 0, (double)lp.N, launch_k(k_lp_apply, cdiv(lp.N, 256), 256, 0, ctx->stream, lp.N, lp.tab + 0,
+                                             (const double* const*)(lp.tab + 5), (const double* const*)(lp.tab + 10),
+                                             (const float*)lp.s5, (const float*)lp.y));
+  CKL();
+  lp.predictions += 1;
+  return 0;
+}
+
 }  // namespace
 
 // =============================================================== C ABI
@@ -792,6 +1071,7 @@ int desalm_init(const desalm_case* c, desalm_ctx** out) {
     cudaMemcpyAsync(ctx->ftab, tab, sizeof(tab), cudaMemcpyHostToDevice, ctx->stream);
   }
   e = kind_of(ctx, 0) == K_DD ? slab_attrs<double, double>() : slab_attrs<double, float>();
+  if (e == cudaSuccess && c->predictor == DESALM_PRED_LEARNED) e = lp_attrs();
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) {
     ctx->err = std::string("init: ") + cudaGetErrorString(e);
@@ -799,6 +1079,7 @@ int desalm_init(const desalm_case* c, desalm_ctx** out) {
     return DESALM_ECUDA;
   }
   *out = ctx;
+  if (c->predictor == DESALM_PRED_LEARNED) return lp_alloc(ctx);
   return 0;
 }
 
@@ -932,6 +1213,9 @@ int desalm_set_state(desalm_ctx* ctx, const double* q, const double* qn, const d
   CK(cudaStreamSynchronize(s));
   for (auto& L : ctx->L) L.dtau_valid = false;
   ctx->have_state = true;
+  // q^{n-2} of the learned guess is known after one shift when both older
+  // levels were given, after two or three otherwise
+  ctx->lp.shifts = qnm1 ? 0 : (qn ? -1 : -2);
   return 0;
 }
 
@@ -1069,6 +1353,9 @@ int desalm_begin_step(desalm_ctx* ctx) {
   const desalm_case& c = ctx->c;
   cudaStream_t s = ctx->stream;
   Level& F = ctx->L[0];
+  const bool learned = c.predictor == DESALM_PRED_LEARNED;
+  // the learned guess trains on the step just converged before the shift
+  if (learned) RET(lp_learn(ctx));
   // qnm1 <- qn; qn <- q (src/mg_driver.F90:48-51)
   for (int m = 0; m < 5; ++m) {
     void *q, *qn, *qnm1;
@@ -1076,12 +1363,17 @@ int desalm_begin_step(desalm_ctx* ctx) {
     RET(field_ptr(ctx, 0, DESALM_F_Q + m, &q, &esz));
     RET(field_ptr(ctx, 0, DESALM_F_QN + m, &qn, &esz));
     RET(field_ptr(ctx, 0, DESALM_F_QNM1 + m, &qnm1, &esz));
+    if (learned) CK(cudaMemcpyAsync(ctx->lp.qnm2[m], qnm1, F.N * esz, cudaMemcpyDeviceToDevice, s));
     CK(cudaMemcpyAsync(qnm1, qn, F.N * esz, cudaMemcpyDeviceToDevice, s));
     CK(cudaMemcpyAsync(qn, q, F.N * esz, cudaMemcpyDeviceToDevice, s));
-    if (c.predictor == DESALM_PRED_LINEAR)
+    if (c.predictor == DESALM_PRED_LINEAR || learned)
       LAUNCH(KC_MISC, 0, F.N, launch_k(k_extrapolate<double>, cdiv(F.N, 256), 256, 0, s, (double*)q, (const double*)qn, (const double*)qnm1, F.N));
   }
   CKL();
+  if (learned) {
+    ctx->lp.shifts += 1;
+    RET(lp_predict(ctx));
+  }
   // inject qn, qnm1 to the coarse levels (src/mg_driver.F90:55-58)
   for (int n = 1; n < ctx->ng; ++n) {
     Level& C = ctx->L[n];
@@ -1426,3 +1718,106 @@ int graph_step(desalm_ctx* ctx, desalm_step_report* rep) {
 }
 
 }  // namespace
+
+// ------------------------------------------------------ learned guess ABI
+extern "C" {
+
+int desalm_lp_config(desalm_ctx* ctx, int train_steps, int warm, float lr) {
+  if (!ctx) return DESALM_EINVAL;
+  if (!ctx->lp.on) { ctx->err = "the learned guess is off (predictor is not DESALM_PRED_LEARNED)"; return DESALM_EINVAL; }
+  if (train_steps > 1000 || warm > 1000000 || !(lr < 1.0f)) { ctx->err = "lp_config: value out of range"; return DESALM_EINVAL; }
+  if (train_steps >= 0) ctx->lp.train_steps = train_steps;
+  if (warm >= 0) ctx->lp.warm = warm;
+  if (lr >= 0.0f) ctx->lp.lr = lr;
+  return 0;
+}
+
+int desalm_lp_report_get(desalm_ctx* ctx, desalm_lp_report* r) {
+  if (!ctx || !r) return DESALM_EINVAL;
+  const LpState& lp = ctx->lp;
+  r->nparam = lp.nparam;
+  r->samples = lp.samples;
+  r->train_steps = lp.steps;
+  r->predictions = lp.predictions;
+  r->first_loss = lp.first_loss;
+  r->last_loss = lp.last_loss;
+  return 0;
+}
+
+int desalm_lp_get_params(desalm_ctx* ctx, float* theta) {
+  if (!ctx || !theta) return DESALM_EINVAL;
+  if (!ctx->lp.on) { ctx->err = "the learned guess is off"; return DESALM_EINVAL; }
+  CK(cudaMemcpyAsync(theta, ctx->lp.theta, ctx->lp.nparam * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+int desalm_lp_set_params(desalm_ctx* ctx, const float* theta) {
+  if (!ctx || !theta) return DESALM_EINVAL;
+  LpState& lp = ctx->lp;
+  if (!lp.on) { ctx->err = "the learned guess is off"; return DESALM_EINVAL; }
+  CK(cudaMemcpyAsync(lp.theta, theta, lp.nparam * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  // a new parameter vector restarts Adam
+  CK(cudaMemsetAsync(lp.m, 0, lp.nparam * sizeof(float), ctx->stream));
+  CK(cudaMemsetAsync(lp.v, 0, lp.nparam * sizeof(float), ctx->stream));
+  lp.adam_t = 0;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+int desalm_lp_eval(desalm_ctx* ctx, const float* x, const float* t, float* y, double* loss, float* grad) {
+  if (!ctx || !x) return DESALM_EINVAL;
+  LpState& lp = ctx->lp;
+  if (!lp.on) { ctx->err = "the learned guess is off"; return DESALM_EINVAL; }
+  cudaStream_t s = ctx->stream;
+  const long N = lp.N;
+  // the FP32 features pass through the state staging array (5 N doubles =
+  // 10 N floats), 8 channels at a time
+  float* xf = reinterpret_cast<float*>(ctx->stage);
+  for (long c0 = 0; c0 < 16; c0 += 8) {
+    const long nc = std::min<long>(8, 16 - c0);
+    CK(cudaMemcpyAsync(xf, x + c0 * N, nc * N * sizeof(float), cudaMemcpyHostToDevice, s));
+    LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_f2bf, cdiv(nc * N, 256), 256, 0, s, nc * N, (const float*)xf, lp.x0 + c0 * N));
+    CKL();
+  }
+  RET(lp_pack(ctx));
+  RET(lp_forward(ctx));
+  if (y) CK(cudaMemcpyAsync(y, lp.y, 5 * N * sizeof(float), cudaMemcpyDeviceToHost, s));
+  if (t) {
+    CK(cudaMemcpyAsync(lp.t, t, 5 * N * sizeof(float), cudaMemcpyHostToDevice, s));
+    double l = 0;
+    RET(lp_backward(ctx, &l));
+    if (loss) *loss = l;
+    if (grad) CK(cudaMemcpyAsync(grad, lp.grad, lp.nparam * sizeof(float), cudaMemcpyDeviceToHost, s));
+  }
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+int desalm_lp_get_buffer(desalm_ctx* ctx, int which, float* out) {
+  if (!ctx || !out) return DESALM_EINVAL;
+  LpState& lp = ctx->lp;
+  if (!lp.on) { ctx->err = "the learned guess is off"; return DESALM_EINVAL; }
+  cudaStream_t s = ctx->stream;
+  const long N = lp.N;
+  switch (which) {
+    case DESALM_LP_FEATURES: {
+      float* xf = reinterpret_cast<float*>(ctx->stage);
+      for (long c0 = 0; c0 < 16; c0 += 8) {
+        const long nc = std::min<long>(8, 16 - c0);
+        LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_bf2f, cdiv(nc * N, 256), 256, 0, s, nc * N, (const bf16*)(lp.x0 + c0 * N), xf));
+        CKL();
+        CK(cudaMemcpyAsync(out + c0 * N, xf, nc * N * sizeof(float), cudaMemcpyDeviceToHost, s));
+      }
+      break;
+    }
+    case DESALM_LP_TARGET: CK(cudaMemcpyAsync(out, lp.t, 5 * N * sizeof(float), cudaMemcpyDeviceToHost, s)); break;
+    case DESALM_LP_OUTPUT: CK(cudaMemcpyAsync(out, lp.y, 5 * N * sizeof(float), cudaMemcpyDeviceToHost, s)); break;
+    case DESALM_LP_SCALES: CK(cudaMemcpyAsync(out, lp.rs, 16 * sizeof(float), cudaMemcpyDeviceToHost, s)); break;
+    default: ctx->err = "lp_get_buffer: unknown buffer"; return DESALM_EINVAL;
+  }
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+}  // extern "C"

@@ -19,6 +19,9 @@ FP64 = 0
 MIXED = 1
 PRED_QN = 0
 PRED_LINEAR = 1
+PRED_LEARNED = 2
+
+LP_FEATURES, LP_TARGET, LP_OUTPUT, LP_SCALES = 0, 1, 2, 3
 
 BC_INTERFACE, BC_WALL, BC_SYMMETRY, BC_FREESTREAM, BC_INFLOW, BC_PERIODIC = 0, 1, 2, 3, 4, 6
 
@@ -85,6 +88,20 @@ class StepReport(C.Structure):
         return {"iterations": self.iterations, "converged": bool(self.converged),
                 "residual": list(self.residual), "init_residual": list(self.init_residual),
                 "pivots": self.pivots}
+
+
+class LpReport(C.Structure):
+    _fields_ = [
+        ("nparam", C.c_long),
+        ("samples", C.c_long),
+        ("train_steps", C.c_long),
+        ("predictions", C.c_long),
+        ("first_loss", C.c_double),
+        ("last_loss", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
 
 
 def level_dims(case, n):

@@ -11,7 +11,7 @@ import subprocess
 
 import numpy as np
 
-from .abi import Case, StepReport, level_dims
+from .abi import Case, LpReport, StepReport, level_dims
 
 PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 # DESALM_LIBRARY selects another build of the same library (tuning variants)
@@ -68,6 +68,18 @@ def lib():
             f = getattr(L, "desalm_" + name)
             f.argtypes = args
             f.restype = C.c_int
+        fp = C.POINTER(C.c_float)
+        for name, args in [
+            ("lp_config", [vp, ip, ip, C.c_float]),
+            ("lp_report_get", [vp, C.POINTER(LpReport)]),
+            ("lp_get_params", [vp, fp]),
+            ("lp_set_params", [vp, fp]),
+            ("lp_eval", [vp, fp, fp, fp, dp, fp]),
+            ("lp_get_buffer", [vp, ip, fp]),
+        ]:
+            f = getattr(L, "desalm_" + name)
+            f.argtypes = args
+            f.restype = C.c_int
         L.desalm_stream.argtypes = [vp]
         L.desalm_stream.restype = C.c_void_p
         L.desalm_kernel_class_count.argtypes = []
@@ -79,7 +91,7 @@ def lib():
 # kernel classes reported by desalm_kernel_stats (order of the C enum)
 KERNEL_CLASSES = ["dtau", "resid", "sweep_i", "sweep_j", "sweep_k", "recalc", "bcond", "pfix",
                   "nlevel", "prolong", "rsmooth", "norm", "sa_rhs", "sa_sweep", "sa_bc",
-                  "xform_i", "xform_j", "xform_k", "sa_aux", "misc"]
+                  "xform_i", "xform_j", "xform_k", "sa_aux", "learn", "misc"]
 
 
 def _p(a):
@@ -88,6 +100,14 @@ def _p(a):
 
 def _f64(a):
     return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _f32p(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _f32(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float32)
 
 
 class Solver:
@@ -209,3 +229,42 @@ class Solver:
                 if la[t]:
                     out.setdefault(name, {})[lvl + 1] = (float(ms[t]), int(la[t]), float(nodes[t]))
         return out, int(tot.value)
+
+    # ------------------------------------------------ learned initial guess
+    def lp_config(self, train_steps=-1, warm=-1, lr=-1.0):
+        self._ck(self.L.desalm_lp_config(self.ctx, int(train_steps), int(warm), float(lr)), "lp_config")
+
+    def lp_report(self):
+        r = LpReport()
+        self._ck(self.L.desalm_lp_report_get(self.ctx, C.byref(r)), "lp_report_get")
+        return r.as_dict()
+
+    def lp_params(self):
+        theta = np.zeros(self.lp_report()["nparam"], dtype=np.float32)
+        self._ck(self.L.desalm_lp_get_params(self.ctx, _f32p(theta)), "lp_get_params")
+        return theta
+
+    def lp_set_params(self, theta):
+        theta = _f32(theta)
+        if theta.size != self.lp_report()["nparam"]:
+            raise ValueError("expected %d parameters" % self.lp_report()["nparam"])
+        self._ck(self.L.desalm_lp_set_params(self.ctx, _f32p(theta)), "lp_set_params")
+
+    def lp_eval(self, x, t=None):
+        """Forward pass on features x [16, N]; with a target t [5, N] also the
+        loss and the parameter gradient.  Returns (y [5, N], loss, grad)."""
+        N = self.case.im * self.case.jm * self.case.km
+        x = _f32(x).reshape(16, N)
+        t = None if t is None else _f32(t).reshape(5, N)
+        y = np.zeros((5, N), dtype=np.float32)
+        loss = C.c_double(0.0)
+        grad = None if t is None else np.zeros(self.lp_report()["nparam"], dtype=np.float32)
+        self._ck(self.L.desalm_lp_eval(self.ctx, _f32p(x), _f32p(t), _f32p(y), C.byref(loss), _f32p(grad)), "lp_eval")
+        return y, (loss.value if t is not None else None), grad
+
+    def lp_buffer(self, which):
+        N = self.case.im * self.case.jm * self.case.km
+        size = {0: 16 * N, 1: 5 * N, 2: 5 * N, 3: 16}[which]
+        out = np.zeros(size, dtype=np.float32)
+        self._ck(self.L.desalm_lp_get_buffer(self.ctx, which, _f32p(out)), "lp_get_buffer")
+        return out if which == 3 else out.reshape(-1, N)

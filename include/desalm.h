@@ -44,6 +44,9 @@ extern "C" {
 /* predictor: initial guess of q^{n+1} for the pseudo-time loop */
 #define DESALM_PRED_QN      0  /* q^n, as src/mg_driver.F90:50-51              */
 #define DESALM_PRED_LINEAR  1  /* 2 q^n - q^{n-1}                               */
+#define DESALM_PRED_LEARNED 2  /* 2 q^n - q^{n-1} + a correction from a 3D conv
+                                  network trained online on the solver's own
+                                  time levels (desalm_lp_* below)               */
 
 /* boundary types, as documented at the end of ind3dmg.dat (nbtype) */
 #define DESALM_BC_INTERFACE 0
@@ -206,6 +209,53 @@ int  desalm_kernel_class_count(void);
  * capture.  stream may be NULL (the legacy default stream). */
 int  desalm_mg_residual_noalloc(const double* q, const double* qold, int im,
                                 int jm, int km, double res[5], void* stream);
+
+/* ---------------------------------------------------------------------
+ * Learned initial guess (predictor DESALM_PRED_LEARNED).  The reference
+ * starts each physical step from q^n (src/mg_driver.F90:48-51); these calls
+ * extend that step.  A 4-layer 3x3x3 convolutional network (15 -> 32 -> 32 ->
+ * 32 -> 5 channels, ReLU, zero padding, BF16 activations and weights, FP32
+ * accumulation) maps, per fine node, q^n, q^n - q^{n-1} and q^{n-1} - q^{n-2}
+ * of (p, u, v, w, nu_tilde), each divided by its RMS over the grid, to
+ * (q^{n+1} - 2 q^n + q^{n-1}) / s_f, s_f the RMS of (q^n - q^{n-1})_f.  At
+ * the start of every physical step desalm_begin_step trains it on the step
+ * just converged (train_steps Adam steps on the mean squared error) and, once
+ * it has seen warm samples, starts the pseudo-time loop from
+ * 2 q^n - q^{n-1} + s_f * output; a node whose output is not finite keeps the
+ * linear extrapolation.
+ *
+ * Flat parameter vector (FP32): for each layer W[cout][cin][27] with the
+ * stencil offset o = (dk+1)*9 + (dj+1)*3 + (di+1), then b[cout].
+ * --------------------------------------------------------------------- */
+typedef struct desalm_lp_report {
+  long nparam;        /* parameters (72,677)                              */
+  long samples;       /* time levels trained on                           */
+  long train_steps;   /* Adam steps taken                                 */
+  long predictions;   /* physical steps started from the network's guess  */
+  double first_loss;  /* loss of the first training step (-1: none yet)   */
+  double last_loss;   /* loss of the latest training step                 */
+} desalm_lp_report;
+
+/* buffers readable with desalm_lp_get_buffer */
+#define DESALM_LP_FEATURES 0   /* [16][N] scaled inputs of the latest pass (channel 15 zero) */
+#define DESALM_LP_TARGET   1   /* [5][N] latest training target                          */
+#define DESALM_LP_OUTPUT   2   /* [5][N] latest network output (FP32)                    */
+#define DESALM_LP_SCALES   3   /* [16] reciprocal RMS of the 15 input channels           */
+
+/* Training settings; a negative value keeps the current one (defaults:
+ * 8 Adam steps per sample, warm = 2 samples, lr = 1e-3). */
+int  desalm_lp_config(desalm_ctx* ctx, int train_steps, int warm, float lr);
+int  desalm_lp_report_get(desalm_ctx* ctx, desalm_lp_report* r);
+/* nparam floats in the flat layout above; set restarts the Adam moments */
+int  desalm_lp_get_params(desalm_ctx* ctx, float* theta);
+int  desalm_lp_set_params(desalm_ctx* ctx, const float* theta);
+/* One forward pass on host features x [16][N] (fine-level node order,
+ * i fastest) giving y [5][N]; with a target t [5][N] also the loss
+ * mean((y - t)^2) and its gradient with respect to the flat parameters.
+ * y, loss and grad may be NULL.  Changes no parameter. */
+int  desalm_lp_eval(desalm_ctx* ctx, const float* x, const float* t, float* y,
+                    double* loss, float* grad);
+int  desalm_lp_get_buffer(desalm_ctx* ctx, int which, float* out);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,166 @@
+"""The learned initial guess (predictor DESALM_PRED_LEARNED) on the GPU
+against the numpy restatement in oracle/lp_oracle.py, through the C ABI.
+
+Tolerances:
+- network output, loss and whole parameter gradient against the oracle
+  rounded to BF16 at the same points: relative L2 <= 2e-3 (the tensor cores
+  sum in FP32 in another order; a sum that lands on the other side of a BF16
+  rounding boundary moves one activation by one BF16 ulp); each layer's share
+  of the gradient: <= 1e-2, since those flips compound through the backward
+  chain and the first layer's gradient sums, with cancellation, over few
+  nodes on the small grid (measured on a B200: output 2.4e-4, first layer
+  3.7e-3 at 17^3 and 7.7e-4 at 41^3, the same at every stencil offset; the
+  other layers <= 4e-4);
+- against the all-FP64 oracle: relative L2 <= 3e-2 (BF16 quantisation);
+- scales and targets: relative 1e-6 (FP64 RMS sums in another order may move
+  a scale by one FP32 ulp); features given the GPU's scales: bit-identical;
+- zero network, or a network whose output is not finite: bit-identical to the
+  linear extrapolation.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from desalm import abi, cases
+
+import lp_oracle as lp
+
+pytestmark = pytest.mark.gpu
+
+
+def _solver(case, grid, state):
+    from desalm.solver import Solver
+    S = Solver(case)
+    S.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
+    S.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
+    return S
+
+
+def _cavity(n, predictor, itmax=12):
+    case, grid, state = cases.cavity(n=n, seed=5, itmax=itmax)
+    case.predictor = predictor
+    return case, grid, state
+
+
+def _soa(a):
+    """AoS q(5, i, j, k) -> [5, N]."""
+    return np.asarray(a).reshape(-1, 5).T.copy()
+
+
+@pytest.mark.parametrize("n", [17, 41])
+def test_network_forward_and_gradient_match_oracle(n):
+    """17^3: one partial tile; 41^3: 539 tiles, more than the grid, so the
+    convolution's tile loop strides and the last tile is partial."""
+    case, grid, state = _cavity(n, abi.PRED_LEARNED)
+    S = _solver(case, grid, state)
+    dims = (case.im, case.jm, case.km)
+    N = case.im * case.jm * case.km
+    rng = np.random.default_rng(n)
+    theta = lp.init_params(seed=n, last_scale=1.0)
+    theta[lp.nparam() - 5:] = rng.normal(0.0, 0.1, 5)        # output biases
+    S.lp_set_params(theta)
+    x = np.zeros((16, N), np.float32)
+    x[:15] = rng.normal(size=(15, N))
+    t = rng.normal(size=(5, N)).astype(np.float32)
+    y, loss, grad = S.lp_eval(x, t)
+    y_q, _ = lp.forward(theta, x, dims, quantize=True)
+    loss_q, grad_q = lp.loss_grad(theta, x, t, dims, quantize=True)
+    assert rel_l2(y, y_q) <= 2e-3
+    assert abs(loss - loss_q) <= 2e-3 * loss_q
+    assert rel_l2(grad, grad_q) <= 2e-3
+    # per layer too: each layer's share of the gradient is checked separately
+    off = 0
+    for ci, co in lp.LAYERS:
+        nl = co * ci * 27 + co
+        assert rel_l2(grad[off:off + nl], grad_q[off:off + nl]) <= 1e-2, (ci, co)
+        off += nl
+    y_e, _ = lp.forward(theta, x, dims, quantize=False)
+    assert rel_l2(y, y_e) <= 3e-2
+    _, grad_e = lp.loss_grad(theta, x, t, dims, quantize=False)
+    assert rel_l2(grad, grad_e) <= 3e-2
+    # the parameters are untouched by an evaluation
+    assert np.array_equal(S.lp_params(), theta)
+
+
+def _run(predictor, steps, setup=None, n=17):
+    case, grid, state = _cavity(n, predictor)
+    S = _solver(case, grid, state)
+    if setup:
+        setup(S)
+    reps = [S.mg_driver() for _ in range(steps)]
+    return S, S.get_state(), reps
+
+
+def test_zero_network_is_linear_extrapolation_bitwise():
+    def setup(S):
+        S.lp_set_params(np.zeros(lp.nparam(), np.float32))
+        S.lp_config(train_steps=2, warm=0, lr=0.0)
+    S, st, reps = _run(abi.PRED_LEARNED, 4, setup)
+    _, st_lin, reps_lin = _run(abi.PRED_LINEAR, 4)
+    for k in ("q", "qn", "qnm1", "nut"):
+        assert np.array_equal(st[k], st_lin[k]), k
+    assert [r["iterations"] for r in reps] == [r["iterations"] for r in reps_lin]
+    r = S.lp_report()
+    # step 1 cannot train (q^{n-2} unknown); steps 2..4 train on one sample each
+    assert r["samples"] == 3 and r["train_steps"] == 6 and r["predictions"] == 4
+    assert np.array_equal(S.lp_params(), np.zeros(lp.nparam(), np.float32))
+
+
+def test_non_finite_network_output_falls_back_to_linear():
+    def setup(S):
+        th = np.zeros(lp.nparam(), np.float32)
+        th[lp.nparam() - 5:] = np.nan                        # every output NaN
+        S.lp_set_params(th)
+        S.lp_config(train_steps=1, warm=0, lr=0.0)
+    S, st, _ = _run(abi.PRED_LEARNED, 3, setup)
+    _, st_lin, _ = _run(abi.PRED_LINEAR, 3)
+    for k in ("q", "qn", "qnm1"):
+        assert np.array_equal(st[k], st_lin[k]), k
+    assert np.isnan(S.lp_buffer(abi.LP_OUTPUT)).all()
+
+
+def test_features_targets_and_guess_match_oracle():
+    case, grid, state = _cavity(17, abi.PRED_LEARNED)
+    S = _solver(case, grid, state)
+    S.lp_config(train_steps=3, warm=1, lr=1e-3)
+    hist = [_soa(state["qnm1"]), _soa(state["qn"]), _soa(state["q"])]   # oldest first
+    rs = None
+    for step in range(4):
+        before = S.get_state()
+        q, qn, qnm1 = _soa(before["q"]), _soa(before["qn"]), _soa(before["qnm1"])
+        S.begin_step()
+        r = S.lp_report()
+        if step >= 1:
+            # the sample of this step: features of (q^n, q^{n-1}, q^{n-2}) as
+            # they were before the shift, target from the converged q
+            qnm2 = hist[-4]
+            if rs is None:
+                rs = lp.scales(qn, qnm1, qnm2)
+                got_rs = S.lp_buffer(abi.LP_SCALES)
+                assert np.allclose(got_rs, rs, rtol=1e-6, atol=0)
+                rs = got_rs
+            t = S.lp_buffer(abi.LP_TARGET)
+            assert np.allclose(t, lp.target(q, qn, qnm1, rs), rtol=1e-6, atol=1e-6 * np.abs(t).max())
+        if r["predictions"] > 0 and step >= 1:
+            # the guess: features of (q, q^n, q^{n-1}) after the shift
+            x = S.lp_buffer(abi.LP_FEATURES)
+            want = lp.features(q, qn, qnm1, rs)
+            assert np.array_equal(x, want)
+            y = S.lp_buffer(abi.LP_OUTPUT)
+            g = _soa(S.get_state()["q"])
+            assert np.allclose(g, lp.guess(q, qn, y, rs), rtol=0, atol=1e-12 * max(1.0, np.abs(g).max()))
+        S.pseudo_iteration()
+        hist.append(_soa(S.get_state()["q"]))
+    assert S.lp_report()["samples"] == 3
+
+
+def test_training_lowers_the_loss_on_a_sample():
+    """Two physical steps: the second trains 40 Adam steps on its one sample;
+    the loss of the last step is below that of the first."""
+    def setup(S):
+        S.lp_config(train_steps=40, warm=100, lr=1e-3)
+    S, st, _ = _run(abi.PRED_LEARNED, 2, setup)
+    r = S.lp_report()
+    assert r["samples"] == 1 and r["train_steps"] == 40 and r["predictions"] == 0
+    assert np.isfinite(r["first_loss"]) and np.isfinite(r["last_loss"])
+    assert r["last_loss"] < r["first_loss"], r
