@@ -123,17 +123,21 @@ struct LpState {
   float *dW[4] = {}, *db[4] = {};          // per-layer gradient accumulators
   bf16 *x0 = nullptr, *a[3] = {}, *dy4 = nullptr, *dya[2] = {};  // features, activations, gradients
   float *y = nullptr, *t = nullptr;        // network output, training target [5][N]
-  float *rs = nullptr, *rs5 = nullptr, *s5 = nullptr;  // feature scales (1/RMS), output scales and their reciprocals
+  float *rs = nullptr, *rs5 = nullptr, *s5 = nullptr;  // feature scales (1/RMS), target scales, output scales
   double* acc = nullptr;                   // reductions
   double* qnm2[5] = {};                    // q^{n-2} of the fine level
+  double* nut0 = nullptr;                  // nu_t at the start of a step begun from the network's guess
   double** tab = nullptr;                  // device table: q[5] qn[5] qnm1[5] qnm2[5]
-  bool scaled = false;
+  double* tab_h[20] = {};                  // the same pointers on the host
   int shifts = 0;                          // history shifts since the state was set
-  long samples = 0, steps = 0, predictions = 0, adam_t = 0;
+  bool predicted = false;                  // the current step began from the network's guess
+  long samples = 0, steps = 0, predictions = 0, fallbacks = 0, adam_t = 0;
+  long hold_until = 0;                     // no guesses before this many samples (after a fallback)
   double first_loss = -1, last_loss = -1;
   int train_steps = 8;                     // Adam steps per new sample
   int warm = 2;                            // samples before the network's guess is used
   float lr = 1e-3f;
+  float ymax = LP_YMAX;                    // limit of |output| in the guess
 };
 
 }  // namespace
@@ -695,6 +699,7 @@ void outlet_ratios(const desalm_case& c, const double* x, const double* y, const
 int pseudo_iter(desalm_ctx* ctx, desalm_step_report* rep);
 int enqueue_iteration(desalm_ctx* ctx);
 int graph_step(desalm_ctx* ctx, desalm_step_report* rep);
+int run_step(desalm_ctx* ctx, desalm_step_report* rep);
 int sa_des_eddy(desalm_ctx* ctx);
 int sa_conservation(desalm_ctx* ctx);
 
@@ -770,6 +775,7 @@ int lp_alloc(desalm_ctx* ctx) {
   RET(A((void**)&lp.rs, 16 * sizeof(float))); RET(A((void**)&lp.rs5, 8 * sizeof(float)));
   RET(A((void**)&lp.s5, 8 * sizeof(float))); RET(A((void**)&lp.acc, 16 * sizeof(double)));
   for (int f = 0; f < 5; ++f) RET(A((void**)&lp.qnm2[f], N * sizeof(double)));
+  RET(A((void**)&lp.nut0, N * sizeof(double)));
   RET(A((void**)&lp.tab, 20 * sizeof(double*)));
   cudaStream_t s = ctx->stream;
   double* tab[20];
@@ -780,6 +786,7 @@ int lp_alloc(desalm_ctx* ctx) {
     RET(field_ptr(ctx, 0, DESALM_F_QNM1 + f, (void**)&tab[10 + f], &esz));
     tab[15 + f] = lp.qnm2[f];
   }
+  for (int e = 0; e < 20; ++e) lp.tab_h[e] = tab[e];
   CK(cudaMemcpyAsync(lp.tab, tab, sizeof(tab), cudaMemcpyHostToDevice, s));
   CK(cudaMemsetAsync(lp.dy4, 0, 16L * N * sizeof(bf16), s));
   CK(cudaMemsetAsync(lp.m, 0, off * sizeof(float), s));
@@ -862,35 +869,19 @@ int lp_backward(desalm_ctx* ctx, double* loss) {
   return 0;
 }
 
-// Features of (qn, qnm1, qnm2) at table offsets (a, b, c) into lp.x0; the
-// scales are fixed from the first call.
+// Features of (qn, qnm1, qnm2) at table offsets (a, b, c) into lp.x0, with
+// the scales of these three levels (computed on the device).
 int lp_features(desalm_ctx* ctx, int a, int b, int c) {
   LpState& lp = ctx->lp;
   cudaStream_t s = ctx->stream;
   const long N = lp.N;
-  if (!lp.scaled) {
-    CK(cudaMemsetAsync(lp.acc, 0, 16 * sizeof(double), s));
-    LAUNCH(KC_LEARN, 0, (double)N, launch_k(k_lp_sumsq, 296, 128, 0, s, N, (const double* const*)(lp.tab + a),
-                                            (const double* const*)(lp.tab + b), (const double* const*)(lp.tab + c), lp.acc));
-    CKL();
-    double h[16];
-    CK(cudaMemcpyAsync(h, lp.acc, 16 * sizeof(double), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    float rs[16] = {0}, s5[8] = {0}, rs5[8] = {0};
-    for (int ch = 0; ch < 15; ++ch) {
-      const double rms = std::sqrt(h[ch] / double(N));
-      rs[ch] = rms > 1e-30 ? float(1.0 / rms) : 1.0f;
-    }
-    for (int f = 0; f < 5; ++f) { rs5[f] = rs[3 * f + 1]; s5[f] = 1.0f / rs5[f]; }
-    CK(cudaMemcpyAsync(lp.rs, rs, sizeof(rs), cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(lp.s5, s5, sizeof(s5), cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(lp.rs5, rs5, sizeof(rs5), cudaMemcpyHostToDevice, s));
-    CK(cudaStreamSynchronize(s));
-    lp.scaled = true;
-  }
-  LAUNCH(KC_LEARN, 0, (double)N, launch_k(k_lp_features, cdiv(N, 256), 256, 0, s, N, (const double* const*)(lp.tab + a),
-                                          (const double* const*)(lp.tab + b), (const double* const*)(lp.tab + c),
-                                          (const float*)lp.rs, lp.x0));
+  const double* const* A = (const double* const*)(lp.tab + a);
+  const double* const* B = (const double* const*)(lp.tab + b);
+  const double* const* C = (const double* const*)(lp.tab + c);
+  CK(cudaMemsetAsync(lp.acc, 0, 16 * sizeof(double), s));
+  LAUNCH(KC_LEARN, 0, (double)N, launch_k(k_lp_sumsq, 296, 128, 0, s, N, A, B, C, lp.acc));
+  LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_scales, 1, 32, 0, s, N, (const double*)lp.acc, lp.rs, lp.rs5, lp.s5));
+  LAUNCH(KC_LEARN, 0, (double)N, launch_k(k_lp_features, cdiv(N, 256), 256, 0, s, N, A, B, C, (const float*)lp.rs, lp.x0));
   CKL();
   return 0;
 }
@@ -934,18 +925,48 @@ int lp_learn(desalm_ctx* ctx) {
 }
 
 // After the shift and the linear extrapolation: q <- 2 q^n - q^{n-1} + the
-// network's correction, once it has seen lp.warm samples.
+// network's correction, once it has seen lp.warm samples (and, after a
+// fallback, lp.warm more).
 int lp_predict(desalm_ctx* ctx) {
   LpState& lp = ctx->lp;
-  if (lp.samples < lp.warm || lp.shifts < 1) return 0;
+  lp.predicted = false;
+  if (lp.samples < lp.warm || lp.samples < lp.hold_until || lp.shifts < 1) return 0;
   RET(lp_features(ctx, 5, 10, 15));
   RET(lp_pack(ctx));
   RET(lp_forward(ctx));
   LAUNCH(KC_LEARN, 0, (double)lp.N, launch_k(k_lp_apply, cdiv(lp.N, 256), 256, 0, ctx->stream, lp.N, lp.tab + 0,
                                              (const double* const*)(lp.tab + 5), (const double* const*)(lp.tab + 10),
-                                             (const float*)lp.s5, (const float*)lp.y));
+                                             (const float*)lp.s5, (const float*)lp.y, lp.ymax));
   CKL();
+  void* nut;
+  int esz;
+  RET(field_ptr(ctx, 0, DESALM_F_NUT, &nut, &esz));
+  CK(cudaMemcpyAsync(lp.nut0, nut, lp.N * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
   lp.predictions += 1;
+  lp.predicted = true;
+  return 0;
+}
+
+// A step begun from the network's guess that ended with a non-finite norm or
+// a zero pivot starts again from the linear extrapolation: q and nu_t as the
+// linear guess would have left them, then the rest of desalm_begin_step.
+int lp_fallback(desalm_ctx* ctx) {
+  LpState& lp = ctx->lp;
+  cudaStream_t s = ctx->stream;
+  const Level& F = ctx->L[0];
+  for (int m = 0; m < 5; ++m)
+    LAUNCH(KC_MISC, 0, F.N, launch_k(k_extrapolate<double>, cdiv(F.N, 256), 256, 0, s, lp.tab_h[m],
+                                     (const double*)lp.tab_h[5 + m], (const double*)lp.tab_h[10 + m], F.N));
+  CKL();
+  void* nut;
+  int esz;
+  RET(field_ptr(ctx, 0, DESALM_F_NUT, &nut, &esz));
+  CK(cudaMemcpyAsync(nut, lp.nut0, lp.N * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  if (ctx->c.conservation) RET(sa_conservation(ctx));
+  for (auto& L : ctx->L) L.dtau_valid = false;
+  lp.fallbacks += 1;
+  lp.predicted = false;
+  lp.hold_until = lp.samples + std::max(1, lp.warm);
   return 0;
 }
 
@@ -1409,17 +1430,14 @@ int desalm_pseudo_iteration(desalm_ctx* ctx, desalm_step_report* rep) {
 int desalm_mg_driver(desalm_ctx* ctx, desalm_step_report* rep) {
   if (!ctx) return DESALM_EINVAL;
   RET(desalm_begin_step(ctx));
-  if (ctx->c.use_graph && !ctx->prof_on) return graph_step(ctx, rep);
-  desalm_step_report r{};
-  int piv = 0;
-  for (int it = 1; it <= ctx->c.itmax; ++it) {
-    RET(pseudo_iter(ctx, &r));
-    piv += r.pivots;
-    if (r.converged) break;
+  int rc = run_step(ctx, rep);
+  if ((rc == DESALM_ENONFINITE || rc == DESALM_ESINGULAR) && ctx->lp.predicted) {
+    RET(lp_fallback(ctx));
+    ctx->itc = 0;
+    RET(desalm_save_qold(ctx));
+    rc = run_step(ctx, rep);
   }
-  r.pivots = piv;
-  if (rep) *rep = r;
-  return 0;
+  return rc;
 }
 
 int desalm_sync(desalm_ctx* ctx) {
@@ -1695,6 +1713,22 @@ int build_graph(desalm_ctx* ctx) {
   return 0;
 }
 
+// The pseudo-time loop of one physical step: the CUDA graph, or eagerly
+// (while profiling, or when use_graph is off).
+int run_step(desalm_ctx* ctx, desalm_step_report* rep) {
+  if (ctx->c.use_graph && !ctx->prof_on) return graph_step(ctx, rep);
+  desalm_step_report r{};
+  int piv = 0;
+  for (int it = 1; it <= ctx->c.itmax; ++it) {
+    RET(pseudo_iter(ctx, &r));
+    piv += r.pivots;
+    if (r.converged) break;
+  }
+  r.pivots = piv;
+  if (rep) *rep = r;
+  return 0;
+}
+
 int graph_step(desalm_ctx* ctx, desalm_step_report* rep) {
   if (!ctx->gexec) RET(build_graph(ctx));
   cudaStream_t s = ctx->stream;
@@ -1722,13 +1756,17 @@ int graph_step(desalm_ctx* ctx, desalm_step_report* rep) {
 // ------------------------------------------------------ learned guess ABI
 extern "C" {
 
-int desalm_lp_config(desalm_ctx* ctx, int train_steps, int warm, float lr) {
+int desalm_lp_config(desalm_ctx* ctx, int train_steps, int warm, float lr, float ymax) {
   if (!ctx) return DESALM_EINVAL;
   if (!ctx->lp.on) { ctx->err = "the learned guess is off (predictor is not DESALM_PRED_LEARNED)"; return DESALM_EINVAL; }
-  if (train_steps > 1000 || warm > 1000000 || !(lr < 1.0f)) { ctx->err = "lp_config: value out of range"; return DESALM_EINVAL; }
+  if (train_steps > 1000 || warm > 1000000 || !(lr < 1.0f) || std::isnan(ymax)) {
+    ctx->err = "lp_config: value out of range";
+    return DESALM_EINVAL;
+  }
   if (train_steps >= 0) ctx->lp.train_steps = train_steps;
   if (warm >= 0) ctx->lp.warm = warm;
   if (lr >= 0.0f) ctx->lp.lr = lr;
+  if (ymax >= 0.0f) ctx->lp.ymax = ymax;
   return 0;
 }
 
@@ -1739,6 +1777,7 @@ int desalm_lp_report_get(desalm_ctx* ctx, desalm_lp_report* r) {
   r->samples = lp.samples;
   r->train_steps = lp.steps;
   r->predictions = lp.predictions;
+  r->fallbacks = lp.fallbacks;
   r->first_loss = lp.first_loss;
   r->last_loss = lp.last_loss;
   return 0;

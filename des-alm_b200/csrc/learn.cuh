@@ -6,8 +6,10 @@
 // Network (4 layers, 3x3x3 kernels, zero padding at the grid's edges):
 //   15 -> 32 -> 32 -> 32 -> 5 channels, ReLU after the first three layers.
 // Inputs per node: q^n, q^n - q^{n-1}, q^{n-1} - q^{n-2} of (p, u, v, w,
-// nu_tilde), each divided by its RMS over the grid (fixed at the first sample);
-// output: (q^{n+1} - 2 q^n + q^{n-1}) / s, s = the RMS of q^n - q^{n-1}.
+// nu_tilde), each divided by its RMS over the grid at that time level;
+// output: (q^{n+1} - 2 q^n + q^{n-1}) / s, s = the RMS of q^n - q^{n-1}.  A
+// difference channel whose RMS is below 1e-12 of the field's own RMS counts
+// as still: its scale is zero, so its features, target and correction are zero.
 //
 // Activations are BF16, channel-major ([channel][node], nodes in the level's
 // i-fastest order); products accumulate in FP32 on the tensor cores (WMMA,
@@ -27,6 +29,7 @@ namespace desalm {
 using bf16 = __nv_bfloat16;
 
 constexpr int LP_TM = 128;           // nodes per tile
+constexpr float LP_YMAX = 8.0f;      // default limit of |output| (in units of s) in the guess
 constexpr int LP_LDA = LP_TM + 8;    // shared-memory row stride of a [channel][node] tile
 
 struct LpGrid {
@@ -269,6 +272,29 @@ __global__ void k_lp_sumsq(long N, const double* const* qn, const double* const*
   if (threadIdx.x < 15) atomicAdd(acc + threadIdx.x, sh[threadIdx.x][0]);
 }
 
+// Scales from the sums of squares acc[0..14] (one thread block of 32):
+// rs[c] = 1 / RMS of channel c (0 for a still or zero channel, and rs[15] = 0),
+// rs5[f] = rs[3 f + 1], s5[f] = the RMS of (q^n - q^{n-1})_f or 0.
+__global__ void k_lp_scales(long N, const double* __restrict__ acc, float* __restrict__ rs, float* __restrict__ rs5,
+                            float* __restrict__ s5) {
+  pdl_wait();
+  const int c = threadIdx.x;
+  if (c >= 16) return;
+  float r = 0.0f;
+  if (c < 15) {
+    const int f = c / 3;
+    const double rms = sqrt(acc[c] / double(N));
+    const double rq = sqrt(acc[3 * f] / double(N));
+    const double floor = c % 3 == 0 ? 1e-30 : fmax(1e-12 * rq, 1e-30);
+    r = rms > floor ? float(1.0 / rms) : 0.0f;
+    if (c % 3 == 1) {
+      rs5[f] = r;
+      s5[f] = r > 0.0f ? float(rms) : 0.0f;
+    }
+  }
+  rs[c] = r;
+}
+
 // Training target t[f][l] = (q^{n+1} - 2 q^n + q^{n-1})_f / s_f (FP32), with
 // q^{n+1} = q, q^n = qn, q^{n-1} = qnm1 and rs5[f] = 1 / s_f.
 __global__ void k_lp_target(long N, const double* const* q, const double* const* qn, const double* const* qnm1,
@@ -307,17 +333,17 @@ __global__ void k_lp_loss(long N, const float* __restrict__ y, const float* __re
   if (threadIdx.x == 0) atomicAdd(acc, sh[0]);
 }
 
-// The guess q = 2 q^n - q^{n-1} + s_f y_f; a node whose network output is
-// not finite keeps the linear extrapolation.
+// The guess q = 2 q^n - q^{n-1} + s_f min(max(y_f, -ymax), ymax); a node
+// whose network output is not finite keeps the linear extrapolation.
 __global__ void k_lp_apply(long N, double* const* q, const double* const* qn, const double* const* qnm1,
-                           const float* __restrict__ s5, const float* __restrict__ y) {
+                           const float* __restrict__ s5, const float* __restrict__ y, float ymax) {
   pdl_wait();
   const long l = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= N) return;
 #pragma unroll
   for (int f = 0; f < 5; ++f) {
     const float c = y[(long)f * N + l];
-    const double corr = isfinite(c) ? double(s5[f]) * double(c) : 0.0;
+    const double corr = isfinite(c) ? double(s5[f]) * double(fminf(fmaxf(c, -ymax), ymax)) : 0.0;
     q[f][l] = 2.0 * qn[f][l] - qnm1[f][l] + corr;
   }
 }

@@ -96,6 +96,7 @@ class LpReport(C.Structure):
         ("samples", C.c_long),
         ("train_steps", C.c_long),
         ("predictions", C.c_long),
+        ("fallbacks", C.c_long),
         ("first_loss", C.c_double),
         ("last_loss", C.c_double),
     ]

@@ -70,7 +70,7 @@ def lib():
             f.restype = C.c_int
         fp = C.POINTER(C.c_float)
         for name, args in [
-            ("lp_config", [vp, ip, ip, C.c_float]),
+            ("lp_config", [vp, ip, ip, C.c_float, C.c_float]),
             ("lp_report_get", [vp, C.POINTER(LpReport)]),
             ("lp_get_params", [vp, fp]),
             ("lp_set_params", [vp, fp]),
@@ -231,8 +231,8 @@ class Solver:
         return out, int(tot.value)
 
     # ------------------------------------------------ learned initial guess
-    def lp_config(self, train_steps=-1, warm=-1, lr=-1.0):
-        self._ck(self.L.desalm_lp_config(self.ctx, int(train_steps), int(warm), float(lr)), "lp_config")
+    def lp_config(self, train_steps=-1, warm=-1, lr=-1.0, ymax=-1.0):
+        self._ck(self.L.desalm_lp_config(self.ctx, int(train_steps), int(warm), float(lr), float(ymax)), "lp_config")
 
     def lp_report(self):
         r = LpReport()

@@ -222,7 +222,12 @@ int  desalm_mg_residual_noalloc(const double* q, const double* qold, int im,
  * just converged (train_steps Adam steps on the mean squared error) and, once
  * it has seen warm samples, starts the pseudo-time loop from
  * 2 q^n - q^{n-1} + s_f * output; a node whose output is not finite keeps the
- * linear extrapolation.
+ * linear extrapolation.  The scales are those of the time levels at hand; a
+ * difference whose RMS is below 1e-12 of its field's RMS has scale zero, so
+ * that field gets no correction.  desalm_mg_driver restarts a step begun from
+ * the network's guess from the linear guess when the step ends with a
+ * non-finite norm or a zero pivot, and then uses the network again only after
+ * warm more samples.
  *
  * Flat parameter vector (FP32): for each layer W[cout][cin][27] with the
  * stencil offset o = (dk+1)*9 + (dj+1)*3 + (di+1), then b[cout].
@@ -232,6 +237,8 @@ typedef struct desalm_lp_report {
   long samples;       /* time levels trained on                           */
   long train_steps;   /* Adam steps taken                                 */
   long predictions;   /* physical steps started from the network's guess  */
+  long fallbacks;     /* of those, restarted from the linear guess after a
+                         non-finite norm or a zero pivot                  */
   double first_loss;  /* loss of the first training step (-1: none yet)   */
   double last_loss;   /* loss of the latest training step                 */
 } desalm_lp_report;
@@ -240,11 +247,13 @@ typedef struct desalm_lp_report {
 #define DESALM_LP_FEATURES 0   /* [16][N] scaled inputs of the latest pass (channel 15 zero) */
 #define DESALM_LP_TARGET   1   /* [5][N] latest training target                          */
 #define DESALM_LP_OUTPUT   2   /* [5][N] latest network output (FP32)                    */
-#define DESALM_LP_SCALES   3   /* [16] reciprocal RMS of the 15 input channels           */
+#define DESALM_LP_SCALES   3   /* [16] reciprocal RMS of the 15 input channels (0: still) */
 
-/* Training settings; a negative value keeps the current one (defaults:
- * 8 Adam steps per sample, warm = 2 samples, lr = 1e-3). */
-int  desalm_lp_config(desalm_ctx* ctx, int train_steps, int warm, float lr);
+/* Settings; a negative value keeps the current one.  Defaults: 8 Adam steps
+ * per sample, warm = 2 samples before the first guess, lr = 1e-3, and
+ * ymax = 8: the output used in the guess is limited to [-ymax, ymax]. */
+int  desalm_lp_config(desalm_ctx* ctx, int train_steps, int warm, float lr,
+                      float ymax);
 int  desalm_lp_report_get(desalm_ctx* ctx, desalm_lp_report* r);
 /* nparam floats in the flat layout above; set restarts the Adam moments */
 int  desalm_lp_get_params(desalm_ctx* ctx, float* theta);

@@ -160,15 +160,23 @@ def loss_grad(theta, x, t, dims, quantize=True):
 
 
 def scales(qn, qnm1, qnm2):
-    """Reciprocal RMS of the 15 feature channels (1 where the RMS is zero);
-    q arrays are [5, N] FP64."""
-    rs = np.ones(16, np.float32)
+    """Scales of three time levels ([5, N] FP64 arrays each): rs[16], the
+    reciprocal RMS of the 15 feature channels, and s5[5], the RMS of
+    (q^n - q^{n-1})_f.  A difference channel whose RMS is not above
+    max(1e-12 RMS(q^n_f), 1e-30), or a field channel whose RMS is not above
+    1e-30, is still: its rs (and s5) is zero."""
+    rs = np.zeros(16, np.float32)
+    s5 = np.zeros(5, np.float32)
     for f in range(5):
+        rq = np.sqrt(np.sum(qn[f] * qn[f]) / qn[f].size)
         for c, v in enumerate((qn[f], qn[f] - qnm1[f], qnm1[f] - qnm2[f])):
             rms = np.sqrt(np.sum(v * v) / v.size)
-            rs[3 * f + c] = np.float32(1.0 / rms) if rms > 1e-30 else np.float32(1.0)
-    rs[15] = 0.0
-    return rs
+            floor = 1e-30 if c == 0 else max(1e-12 * rq, 1e-30)
+            if rms > floor:
+                rs[3 * f + c] = np.float32(1.0 / rms)
+                if c == 1:
+                    s5[f] = np.float32(rms)
+    return rs, s5
 
 
 def features(qn, qnm1, qnm2, rs):
@@ -189,10 +197,12 @@ def target(q, qn, qnm1, rs):
     return ((q - 2.0 * qn + qnm1).astype(np.float32) * rs5[:, None]).astype(np.float32)
 
 
-def guess(qn, qnm1, y, rs):
-    """2 q^n - q^{n-1} + s_f y_f, the linear extrapolation where y is not finite."""
-    s5 = np.array([np.float32(1.0) / rs[3 * f + 1] for f in range(5)], np.float32)
-    corr = np.where(np.isfinite(y), s5[:, None].astype(np.float64) * np.asarray(y, np.float64), 0.0)
+def guess(qn, qnm1, y, s5, ymax=8.0):
+    """2 q^n - q^{n-1} + s_f min(max(y_f, -ymax), ymax); the linear
+    extrapolation where y is not finite."""
+    y = np.asarray(y, np.float32)
+    yc = np.clip(y, np.float32(-ymax), np.float32(ymax)).astype(np.float64)
+    corr = np.where(np.isfinite(y), np.asarray(s5, np.float32)[:, None].astype(np.float64) * yc, 0.0)
     return 2.0 * qn - qnm1 + corr
 
 

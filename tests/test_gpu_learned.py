@@ -124,34 +124,57 @@ def test_features_targets_and_guess_match_oracle():
     S = _solver(case, grid, state)
     S.lp_config(train_steps=3, warm=1, lr=1e-3)
     hist = [_soa(state["qnm1"]), _soa(state["qn"]), _soa(state["q"])]   # oldest first
-    rs = None
-    for step in range(4):
+    checked = 0
+    for step in range(5):
         before = S.get_state()
         q, qn, qnm1 = _soa(before["q"]), _soa(before["qn"]), _soa(before["qnm1"])
         S.begin_step()
         r = S.lp_report()
         if step >= 1:
-            # the sample of this step: features of (q^n, q^{n-1}, q^{n-2}) as
-            # they were before the shift, target from the converged q
-            qnm2 = hist[-4]
-            if rs is None:
-                rs = lp.scales(qn, qnm1, qnm2)
-                got_rs = S.lp_buffer(abi.LP_SCALES)
-                assert np.allclose(got_rs, rs, rtol=1e-6, atol=0)
-                rs = got_rs
+            # this step's sample: scales of (q^n, q^{n-1}, q^{n-2}) as they
+            # were before the shift, target from the converged q
+            rs_learn, _ = lp.scales(qn, qnm1, hist[-4])
             t = S.lp_buffer(abi.LP_TARGET)
-            assert np.allclose(t, lp.target(q, qn, qnm1, rs), rtol=1e-6, atol=1e-6 * np.abs(t).max())
+            want = lp.target(q, qn, qnm1, rs_learn)
+            assert np.allclose(t, want, rtol=1e-6, atol=1e-6 * max(1e-30, np.abs(want).max()))
         if r["predictions"] > 0 and step >= 1:
-            # the guess: features of (q, q^n, q^{n-1}) after the shift
+            # the guess: scales and features of (q, q^n, q^{n-1}) after the shift
+            rs, s5 = lp.scales(q, qn, qnm1)
+            got_rs = S.lp_buffer(abi.LP_SCALES)
+            assert np.array_equal(got_rs > 0, rs > 0)
+            assert np.allclose(got_rs, rs, rtol=1e-6, atol=0)
             x = S.lp_buffer(abi.LP_FEATURES)
-            want = lp.features(q, qn, qnm1, rs)
-            assert np.array_equal(x, want)
+            assert np.array_equal(x, lp.features(q, qn, qnm1, got_rs))
             y = S.lp_buffer(abi.LP_OUTPUT)
+            s5_gpu = np.array([np.float32(1.0) / got_rs[3 * f + 1] if got_rs[3 * f + 1] > 0 else 0.0
+                               for f in range(5)], np.float32)
+            assert np.allclose(s5_gpu, s5, rtol=1e-6, atol=0)
             g = _soa(S.get_state()["q"])
-            assert np.allclose(g, lp.guess(q, qn, y, rs), rtol=0, atol=1e-12 * max(1.0, np.abs(g).max()))
+            assert np.allclose(g, lp.guess(q, qn, y, s5), rtol=0, atol=1e-6 * max(1.0, np.abs(g).max()))
+            checked += 1
         S.pseudo_iteration()
         hist.append(_soa(S.get_state()["q"]))
-    assert S.lp_report()["samples"] == 3
+    assert S.lp_report()["samples"] == 4 and checked == 4
+
+
+def test_blown_up_learned_step_restarts_from_linear_guess():
+    """A network whose output is huge but finite (no output limit): the step
+    begun from its guess ends with a non-finite norm, desalm_mg_driver starts
+    it again from the linear extrapolation, and the run then matches the
+    linear run bit for bit; the next guesses wait for warm more samples."""
+    def setup(S):
+        th = np.zeros(lp.nparam(), np.float32)
+        th[lp.nparam() - 5:] = 1e30
+        S.lp_set_params(th)
+        S.lp_config(train_steps=1, warm=2, lr=0.0, ymax=3e38)
+    S, st, reps = _run(abi.PRED_LEARNED, 4, setup)
+    _, st_lin, reps_lin = _run(abi.PRED_LINEAR, 4)
+    r = S.lp_report()
+    # steps 1-2: too few samples; step 3: guess, blow-up, restart; step 4: held
+    assert r["predictions"] == 1 and r["fallbacks"] == 1, r
+    for k in ("q", "qn", "qnm1", "nut"):
+        assert np.array_equal(st[k], st_lin[k]), k
+    assert [x["iterations"] for x in reps] == [x["iterations"] for x in reps_lin]
 
 
 def test_training_lowers_the_loss_on_a_sample():

@@ -108,7 +108,7 @@ def test_features_target_guess_identities():
     qnm1 = qnm2 + 0.01 * rng.normal(size=(5, N))
     qn = qnm1 + 0.01 * rng.normal(size=(5, N))
     q = 2 * qn - qnm1 + 1e-4 * rng.normal(size=(5, N))
-    rs = lp.scales(qn, qnm1, qnm2)
+    rs, s5 = lp.scales(qn, qnm1, qnm2)
     x = lp.features(qn, qnm1, qnm2, rs)
     assert x.shape == (16, N) and not x[15].any()
     # every scaled channel has RMS ~1 (up to BF16 rounding)
@@ -116,9 +116,28 @@ def test_features_target_guess_identities():
     assert np.allclose(rms, 1.0, atol=1e-2)
     t = lp.target(q, qn, qnm1, rs)
     # the guess with the exact target as output reproduces q to FP32 rounding
-    assert np.allclose(lp.guess(qn, qnm1, t, rs), q, rtol=0, atol=1e-9)
+    assert np.allclose(lp.guess(qn, qnm1, t, s5, ymax=1e30), q, rtol=0, atol=1e-9)
     # a non-finite output keeps the linear extrapolation
     y = t.copy()
     y[:, 3] = np.nan
-    gq = lp.guess(qn, qnm1, y, rs)
+    gq = lp.guess(qn, qnm1, y, s5)
     assert np.array_equal(gq[:, 3], 2.0 * qn[:, 3] - qnm1[:, 3])
+    # the output is limited to [-ymax, ymax] scale units
+    y = np.full_like(t, 100.0)
+    assert np.allclose(lp.guess(qn, qnm1, y, s5, ymax=8.0) - (2.0 * qn - qnm1), 8.0 * s5[:, None].astype(np.float64))
+
+
+def test_still_channels_have_zero_scale():
+    rng = np.random.default_rng(7)
+    qn = rng.normal(size=(5, N))
+    qn[4] = 0.0                                   # a zero field
+    qnm1 = qn.copy()
+    qnm1[1] += 1e-3 * rng.normal(size=N)          # only u moves between n-1 and n
+    qnm2 = qnm1 + 1e-15 * qn                      # below 1e-12 of the field: still
+    rs, s5 = lp.scales(qn, qnm1, qnm2)
+    assert rs[3 * 4] == 0 and rs[15] == 0
+    for f in range(5):
+        assert (s5[f] > 0) == (f == 1) and (rs[3 * f + 1] > 0) == (f == 1)
+        assert rs[3 * f + 2] == 0
+    t = lp.target(qn + 1e-3, qn, qnm1, rs)
+    assert not t[[0, 2, 3, 4]].any() and t[1].any()
