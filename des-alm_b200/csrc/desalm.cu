@@ -116,11 +116,13 @@ struct Level {
 struct LpState {
   bool on = false;
   long N = 0;
+  LpPad P{};                               // the fine level's zero-padded grid
   LpLayer ly[4];
   long nparam = 0;
   float *theta = nullptr, *grad = nullptr, *m = nullptr, *v = nullptr;  // flat parameters, gradient, Adam moments
   bf16 *wf[4] = {}, *wd[4] = {};           // forward / data-gradient weight blocks
-  float *dW[4] = {}, *db[4] = {};          // per-layer gradient accumulators
+  float *dW[4] = {}, *db[4] = {};          // per-layer weight and bias gradients (db inside dW's block)
+  float* part = nullptr;                   // per-CTA partial gradients of k_lp_wgrad
   bf16 *x0 = nullptr, *a[3] = {}, *dy4 = nullptr, *dya[2] = {};  // features, activations, gradients
   float *y = nullptr, *t = nullptr;        // network output, training target [5][N]
   float *rs = nullptr, *rs5 = nullptr, *s5 = nullptr;  // feature scales (1/RMS), target scales, output scales
@@ -705,40 +707,49 @@ int sa_conservation(desalm_ctx* ctx);
 
 
 // ----------------------------------------------------------- learned guess
-template <int CIN, int COUT_PAD>
+constexpr int kLpWgradGrid = 148 * 2;  // partial slots of k_lp_wgrad (its largest grid)
+
+template <int CIN, int COUT>
 int lp_conv(desalm_ctx* ctx, const bf16* in, const bf16* w, const float* bias, int relu, const bf16* mask, bf16* out,
-            float* out32, int cout_store) {
+            float* out32, int cout32) {
   LpState& lp = ctx->lp;
-  const Level& F = ctx->L[0];
-  LpGrid G{F.im, F.jm, F.km, lp.N};
-  const long tiles = (lp.N + LP_TM - 1) / LP_TM;
+  const long tiles = (lp.P.p1 - lp.P.p0 + LP_TM - 1) / LP_TM;
   const unsigned grid = (unsigned)std::min<long>(tiles, 148L * 2);
-  LAUNCH(KC_LEARN, 0, (double)lp.N, launch_k(k_lp_conv<CIN, COUT_PAD>, grid, 256, LpConvSmem<CIN, COUT_PAD>::total, ctx->stream,
-                                             G, in, w, bias, relu, mask, out, out32, cout_store));
+  LAUNCH(KC_LEARN, 0, (double)lp.N, launch_k(k_lp_conv<CIN, COUT>, grid, 256, LpConvSmem<CIN, COUT>::total, ctx->stream,
+                                             lp.P, in, w, bias, relu, mask, out, out32, cout32));
   CKL();
   return 0;
 }
 
-template <int CIN, int COUT_PAD>
-int lp_wgrad(desalm_ctx* ctx, const bf16* X, const bf16* dY, float* dW) {
+// Weight and bias gradient of one layer into dW ([27][CIN][COUT] then [COUT]).
+template <int CIN, int COUT>
+int lp_wgrad(desalm_ctx* ctx, const bf16* X, const bf16* D, float* dW) {
   LpState& lp = ctx->lp;
-  const Level& F = ctx->L[0];
-  LpGrid G{F.im, F.jm, F.km, lp.N};
-  const long per = (long)LP_TM * 64;  // nodes per CTA
-  LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_wgrad<CIN, COUT_PAD>, cdiv(lp.N, per), 128, 0, ctx->stream, G, X, dY, dW, per));
+  constexpr int NT = 32 * 3 * (CIN / 16) * (COUT / 16);
+  constexpr long SLOT = 27L * CIN * COUT + COUT;
+  // one CTA of 12 warps per SM (168 registers a thread), or two of 6
+  constexpr int grid = NT > 192 ? 148 : 2 * 148;
+  static_assert(grid <= kLpWgradGrid, "partial slots");
+  LAUNCH(KC_LEARN, 0, (double)lp.N, launch_k(k_lp_wgrad<CIN, COUT>, grid, NT, LpWgradSmem<CIN, COUT>::total,
+                                             ctx->stream, lp.P, X, D, lp.part));
+  LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_reduce, cdiv(SLOT, 256), 256, 0, ctx->stream, grid, SLOT,
+                                    (const float*)lp.part, dW));
   CKL();
   return 0;
+}
+
+template <class K>
+cudaError_t lp_optin(K* k, size_t bytes) {
+  return cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
 cudaError_t lp_attrs() {
-  cudaError_t e = cudaFuncSetAttribute((const void*)k_lp_conv<16, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)LpConvSmem<16, 32>::total);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute((const void*)k_lp_conv<32, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)LpConvSmem<32, 32>::total);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute((const void*)k_lp_conv<32, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)LpConvSmem<32, 16>::total);
+  cudaError_t e = lp_optin(k_lp_conv<16, 32>, LpConvSmem<16, 32>::total);
+  if (e == cudaSuccess) e = lp_optin(k_lp_conv<32, 32>, LpConvSmem<32, 32>::total);
+  if (e == cudaSuccess) e = lp_optin(k_lp_conv<32, 16>, LpConvSmem<32, 16>::total);
+  if (e == cudaSuccess) e = lp_optin(k_lp_wgrad<16, 32>, LpWgradSmem<16, 32>::total);
+  if (e == cudaSuccess) e = lp_optin(k_lp_wgrad<32, 32>, LpWgradSmem<32, 32>::total);
+  if (e == cudaSuccess) e = lp_optin(k_lp_wgrad<32, 16>, LpWgradSmem<32, 16>::total);
   return e;
 }
 
@@ -748,6 +759,7 @@ int lp_alloc(desalm_ctx* ctx) {
   LpState& lp = ctx->lp;
   const Level& F = ctx->L[0];
   lp.N = F.N;
+  lp.P = lp_pad(F.im, F.jm, F.km);
   const int cin[4] = {15, 32, 32, 32}, cout[4] = {32, 32, 32, 5};
   const int cinp[4] = {16, 32, 32, 32}, coutp[4] = {32, 32, 32, 16};
   long off = 0;
@@ -765,12 +777,16 @@ int lp_alloc(desalm_ctx* ctx) {
   for (int l = 0; l < 4; ++l) {
     const size_t wb = 27L * cinp[l] * coutp[l];
     RET(A((void**)&lp.wf[l], wb * sizeof(bf16))); RET(A((void**)&lp.wd[l], wb * sizeof(bf16)));
-    RET(A((void**)&lp.dW[l], wb * sizeof(float))); RET(A((void**)&lp.db[l], coutp[l] * sizeof(float)));
+    RET(A((void**)&lp.dW[l], (wb + coutp[l]) * sizeof(float)));
+    lp.db[l] = lp.dW[l] + wb;
   }
-  RET(A((void**)&lp.x0, 16L * N * sizeof(bf16)));
-  for (int l = 0; l < 3; ++l) RET(A((void**)&lp.a[l], 32L * N * sizeof(bf16)));
-  RET(A((void**)&lp.dy4, 16L * N * sizeof(bf16)));
-  for (int l = 0; l < 2; ++l) RET(A((void**)&lp.dya[l], 32L * N * sizeof(bf16)));
+  RET(A((void**)&lp.part, (size_t)kLpWgradGrid * (27L * 32 * 32 + 32) * sizeof(float)));
+  // channel-last rows of the padded grid; the halo rows stay zero
+  const long NP = lp.P.np;
+  RET(A((void**)&lp.x0, 16L * NP * sizeof(bf16)));
+  for (int l = 0; l < 3; ++l) RET(A((void**)&lp.a[l], 32L * NP * sizeof(bf16)));
+  RET(A((void**)&lp.dy4, 16L * NP * sizeof(bf16)));
+  for (int l = 0; l < 2; ++l) RET(A((void**)&lp.dya[l], 32L * NP * sizeof(bf16)));
   RET(A((void**)&lp.y, 5L * N * sizeof(float))); RET(A((void**)&lp.t, 5L * N * sizeof(float)));
   RET(A((void**)&lp.rs, 16 * sizeof(float))); RET(A((void**)&lp.rs5, 8 * sizeof(float)));
   RET(A((void**)&lp.s5, 8 * sizeof(float))); RET(A((void**)&lp.acc, 16 * sizeof(double)));
@@ -788,7 +804,6 @@ int lp_alloc(desalm_ctx* ctx) {
   }
   for (int e = 0; e < 20; ++e) lp.tab_h[e] = tab[e];
   CK(cudaMemcpyAsync(lp.tab, tab, sizeof(tab), cudaMemcpyHostToDevice, s));
-  CK(cudaMemsetAsync(lp.dy4, 0, 16L * N * sizeof(bf16), s));
   CK(cudaMemsetAsync(lp.m, 0, off * sizeof(float), s));
   CK(cudaMemsetAsync(lp.v, 0, off * sizeof(float), s));
   std::vector<float> th(off, 0.0f);
@@ -820,9 +835,9 @@ int lp_forward(desalm_ctx* ctx) {
   const float* b[4];
   for (int l = 0; l < 4; ++l) b[l] = lp.theta + lp.ly[l].boff;
   // the bias pointers index the flat vector: each layer's bias is contiguous there
-  RET((lp_conv<16, 32>(ctx, lp.x0, lp.wf[0], b[0], 1, nullptr, lp.a[0], nullptr, 32)));
-  RET((lp_conv<32, 32>(ctx, lp.a[0], lp.wf[1], b[1], 1, nullptr, lp.a[1], nullptr, 32)));
-  RET((lp_conv<32, 32>(ctx, lp.a[1], lp.wf[2], b[2], 1, nullptr, lp.a[2], nullptr, 32)));
+  RET((lp_conv<16, 32>(ctx, lp.x0, lp.wf[0], b[0], 1, nullptr, lp.a[0], nullptr, 0)));
+  RET((lp_conv<32, 32>(ctx, lp.a[0], lp.wf[1], b[1], 1, nullptr, lp.a[1], nullptr, 0)));
+  RET((lp_conv<32, 32>(ctx, lp.a[1], lp.wf[2], b[2], 1, nullptr, lp.a[2], nullptr, 0)));
   RET((lp_conv<32, 16>(ctx, lp.a[2], lp.wf[3], b[3], 0, nullptr, nullptr, lp.y, 5)));
   return 0;
 }
@@ -833,28 +848,20 @@ int lp_backward(desalm_ctx* ctx, double* loss) {
   LpState& lp = ctx->lp;
   cudaStream_t s = ctx->stream;
   const long N = lp.N;
-  for (int l = 0; l < 4; ++l) {
-    CK(cudaMemsetAsync(lp.dW[l], 0, 27L * lp.ly[l].cin_pad * lp.ly[l].cout_pad * sizeof(float), s));
-    CK(cudaMemsetAsync(lp.db[l], 0, lp.ly[l].cout_pad * sizeof(float), s));
-  }
   CK(cudaMemsetAsync(lp.acc, 0, sizeof(double), s));
-  LAUNCH(KC_LEARN, 0, (double)N, launch_k(k_lp_loss, 296, 256, 0, s, N, (const float*)lp.y, (const float*)lp.t, lp.dy4, lp.acc));
+  LAUNCH(KC_LEARN, 0, (double)N, launch_k(k_lp_loss, 296, 256, 0, s, lp.P, (const float*)lp.y, (const float*)lp.t, lp.dy4, lp.acc));
   CKL();
   // layer 4 (a[2] -> y)
   RET((lp_wgrad<32, 16>(ctx, lp.a[2], lp.dy4, lp.dW[3])));
-  LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_bias_grad, dim3(64, 5), 256, 0, s, N, (const bf16*)lp.dy4, lp.db[3]));
-  RET((lp_conv<16, 32>(ctx, lp.dy4, lp.wd[3], nullptr, 0, lp.a[2], lp.dya[0], nullptr, 32)));
+  RET((lp_conv<16, 32>(ctx, lp.dy4, lp.wd[3], nullptr, 0, lp.a[2], lp.dya[0], nullptr, 0)));
   // layer 3 (a[1] -> a[2])
   RET((lp_wgrad<32, 32>(ctx, lp.a[1], lp.dya[0], lp.dW[2])));
-  LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_bias_grad, dim3(64, 32), 256, 0, s, N, (const bf16*)lp.dya[0], lp.db[2]));
-  RET((lp_conv<32, 32>(ctx, lp.dya[0], lp.wd[2], nullptr, 0, lp.a[1], lp.dya[1], nullptr, 32)));
+  RET((lp_conv<32, 32>(ctx, lp.dya[0], lp.wd[2], nullptr, 0, lp.a[1], lp.dya[1], nullptr, 0)));
   // layer 2 (a[0] -> a[1])
   RET((lp_wgrad<32, 32>(ctx, lp.a[0], lp.dya[1], lp.dW[1])));
-  LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_bias_grad, dim3(64, 32), 256, 0, s, N, (const bf16*)lp.dya[1], lp.db[1]));
-  RET((lp_conv<32, 32>(ctx, lp.dya[1], lp.wd[1], nullptr, 0, lp.a[0], lp.dya[0], nullptr, 32)));
+  RET((lp_conv<32, 32>(ctx, lp.dya[1], lp.wd[1], nullptr, 0, lp.a[0], lp.dya[0], nullptr, 0)));
   // layer 1 (x0 -> a[0])
   RET((lp_wgrad<16, 32>(ctx, lp.x0, lp.dya[0], lp.dW[0])));
-  LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_bias_grad, dim3(64, 32), 256, 0, s, N, (const bf16*)lp.dya[0], lp.db[0]));
   const float gscale = float(2.0 / (5.0 * double(N)));
   for (int l = 0; l < 4; ++l) {
     const long n = (long)lp.ly[l].cout * lp.ly[l].cin * 27 + lp.ly[l].cout;
@@ -881,7 +888,7 @@ int lp_features(desalm_ctx* ctx, int a, int b, int c) {
   CK(cudaMemsetAsync(lp.acc, 0, 16 * sizeof(double), s));
   LAUNCH(KC_LEARN, 0, (double)N, launch_k(k_lp_sumsq, 296, 128, 0, s, N, A, B, C, lp.acc));
   LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_scales, 1, 32, 0, s, N, (const double*)lp.acc, lp.rs, lp.rs5, lp.s5));
-  LAUNCH(KC_LEARN, 0, (double)N, launch_k(k_lp_features, cdiv(N, 256), 256, 0, s, N, A, B, C, (const float*)lp.rs, lp.x0));
+  LAUNCH(KC_LEARN, 0, (double)N, launch_k(k_lp_features, cdiv(N, 256), 256, 0, s, lp.P, A, B, C, (const float*)lp.rs, lp.x0));
   CKL();
   return 0;
 }
@@ -1816,7 +1823,7 @@ int desalm_lp_eval(desalm_ctx* ctx, const float* x, const float* t, float* y, do
   for (long c0 = 0; c0 < 16; c0 += 8) {
     const long nc = std::min<long>(8, 16 - c0);
     CK(cudaMemcpyAsync(xf, x + c0 * N, nc * N * sizeof(float), cudaMemcpyHostToDevice, s));
-    LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_f2bf, cdiv(nc * N, 256), 256, 0, s, nc * N, (const float*)xf, lp.x0 + c0 * N));
+    LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_rows_in, cdiv(N, 256), 256, 0, s, lp.P, 16, (int)c0, (int)nc, (const float*)xf, lp.x0));
     CKL();
   }
   RET(lp_pack(ctx));
@@ -1844,7 +1851,7 @@ int desalm_lp_get_buffer(desalm_ctx* ctx, int which, float* out) {
       float* xf = reinterpret_cast<float*>(ctx->stage);
       for (long c0 = 0; c0 < 16; c0 += 8) {
         const long nc = std::min<long>(8, 16 - c0);
-        LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_bf2f, cdiv(nc * N, 256), 256, 0, s, nc * N, (const bf16*)(lp.x0 + c0 * N), xf));
+        LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_rows_out, cdiv(N, 256), 256, 0, s, lp.P, 16, (int)c0, (int)nc, (const bf16*)lp.x0, xf));
         CKL();
         CK(cudaMemcpyAsync(out + c0 * N, xf, nc * N * sizeof(float), cudaMemcpyDeviceToHost, s));
       }

@@ -11,14 +11,20 @@
 // difference channel whose RMS is below 1e-12 of the field's own RMS counts
 // as still: its scale is zero, so its features, target and correction are zero.
 //
-// Activations are BF16, channel-major ([channel][node], nodes in the level's
-// i-fastest order); products accumulate in FP32 on the tensor cores (WMMA,
-// m16n16k16 BF16).  A convolution is an implicit GEMM: for each of the 27
-// stencil offsets the CTA gathers the shifted input tile into shared memory
-// and multiplies it by that offset's weight block.  The data gradient of a
-// layer is the same kernel with the weights transposed and the stencil
-// flipped; the weight gradient is a GEMM that reduces over the nodes.
-// Master weights, Adam moments and the loss are FP32 / FP64.
+// Layout: activations and their gradients are BF16, channel-last rows of a
+// zero-padded grid ((im+2) x (jm+2) x (km+2) rows, i fastest; 16 or 32
+// channels, 32 or 64 bytes a row).  The halo rows stay zero, so the 27
+// neighbours of an interior row are the rows at fixed offsets with no bounds
+// checks, and the shifted operand of a stencil offset is a contiguous run of
+// rows.  Products accumulate in FP32 on the tensor cores (WMMA m16n16k16
+// BF16).  A convolution is an implicit GEMM over tiles of LP_TM consecutive
+// padded rows: for each of the 9 (dj, dk) pairs the CTA copies a window of
+// LP_TM + 2 rows into shared memory (16-byte cp.async, double-buffered) and
+// multiplies the window shifted by di = -1, 0, 1 rows by those offsets'
+// weight blocks.  The data gradient of a layer is the same kernel with the
+// weights transposed and the stencil flipped; the weight gradient reduces over
+// the rows with per-CTA partial sums and one reduction kernel.  Master
+// weights, Adam moments and the loss are FP32 / FP64.
 #pragma once
 #include <mma.h>
 #include <cuda_bf16.h>
@@ -28,218 +34,341 @@ namespace desalm {
 
 using bf16 = __nv_bfloat16;
 
-constexpr int LP_TM = 128;           // nodes per tile
+constexpr int LP_TM = 128;           // rows per tile
 constexpr float LP_YMAX = 8.0f;      // default limit of |output| (in units of s) in the guess
-constexpr int LP_LDA = LP_TM + 8;    // shared-memory row stride of a [channel][node] tile
+constexpr int LP_WROWS = LP_TM + 2;  // rows of a window (di = -1..1)
 
-struct LpGrid {
-  int im, jm, km;
-  long N;
+// The zero-padded grid of the fine level.
+struct LpPad {
+  int im, jm, km;    // interior extents (the level's nodes)
+  int ip, jp, kp;    // padded extents
+  long np;           // padded rows
+  long p0, p1;       // first interior row and one past the last
+  long N;            // interior nodes
 };
 
-// stencil offset o = 0..26 -> (di, dj, dk) in -1..1, o = (dk+1)*9 + (dj+1)*3 + (di+1)
-DESALM_DEV void lp_offset(int o, int& di, int& dj, int& dk) {
-  dk = o / 9 - 1;
-  dj = (o / 3) % 3 - 1;
-  di = o % 3 - 1;
+inline LpPad lp_pad(int im, int jm, int km) {
+  LpPad P;
+  P.im = im; P.jm = jm; P.km = km;
+  P.ip = im + 2; P.jp = jm + 2; P.kp = km + 2;
+  P.np = (long)P.ip * P.jp * P.kp;
+  P.p0 = 1 + (long)P.ip * (1 + (long)P.jp);
+  P.p1 = (long)im + (long)P.ip * (jm + (long)P.jp * km) + 1;
+  P.N = (long)im * jm * km;
+  return P;
+}
+
+// padded row of interior node l (level order, i fastest)
+DESALM_DEV long lp_row(const LpPad& P, long l) {
+  const long i = l % P.im, r = l / P.im;
+  const long j = r % P.jm, k = r / P.jm;
+  return (i + 1) + (long)P.ip * ((j + 1) + (long)P.jp * (k + 1));
+}
+
+// interior node of padded row p, or -1 for a halo row
+DESALM_DEV long lp_node(const LpPad& P, long p) {
+  const long ii = p % P.ip, r = p / P.ip;
+  const long jj = r % P.jp, kk = r / P.jp;
+  if (ii < 1 || ii > P.im || jj < 1 || jj > P.jm || kk < 1 || kk > P.km) return -1;
+  return (ii - 1) + (long)P.im * ((jj - 1) + (long)P.jm * (kk - 1));
+}
+
+DESALM_DEV void lp_cp16(void* smem, const void* gmem, bool ok) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = ok ? 16 : 0;  // 0: fill the 16 bytes with zeros
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(gmem), "r"(n) : "memory");
+}
+DESALM_DEV void lp_cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+DESALM_DEV void lp_cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Row stride (elements) of a channel-last tile in shared memory: a multiple
+// of 32 bytes, so that a window shifted by one row is still a legal WMMA
+// operand address.
+template <int C>
+struct LpStride {
+  static constexpr int v = C == 16 ? 16 : 48;
+};
+
+// Copy the window of (dj, dk) pair g for the tile starting at padded row
+// t0: rows t0 + off(0, dj, dk) - 1 .. + LP_WROWS; rows outside the padded
+// grid (only past the end of the last tile) read as zero.
+template <int C>
+DESALM_DEV void lp_load_window(const LpPad& P, const bf16* __restrict__ src, long t0, int g, bf16* dst, int tid,
+                               int nthreads) {
+  constexpr int S = LpStride<C>::v, CH = C / 8;
+  const int dj = g % 3 - 1, dk = g / 3 - 1;
+  const long base = t0 + (long)P.ip * (dj + (long)P.jp * dk) - 1;
+  for (int e = tid; e < LP_WROWS * CH; e += nthreads) {
+    const int r = e / CH, c = e - r * CH;
+    const long row = base + r;
+    const bool ok = row >= 0 && row < P.np;
+    lp_cp16(dst + r * S + 8 * c, src + (ok ? row : 0) * C + 8 * c, ok);
+  }
 }
 
 // Shared-memory layout of k_lp_conv (bytes).
-template <int CIN, int COUT_PAD>
+template <int CIN, int COUT>
 struct LpConvSmem {
-  static constexpr size_t w = size_t(27) * CIN * COUT_PAD * sizeof(bf16);
-  static constexpr size_t a = size_t(CIN) * LP_LDA * sizeof(bf16);
-  static constexpr size_t c = size_t(LP_TM) * (COUT_PAD + 4) * sizeof(float);
-  static constexpr size_t crd = size_t(LP_TM) * 4 * sizeof(int);
-  static constexpr size_t total = w + a + c + crd;
+  static constexpr int SA = LpStride<CIN>::v;
+  static constexpr size_t w = size_t(27) * CIN * COUT * sizeof(bf16);
+  static constexpr size_t win = size_t(LP_WROWS) * SA * sizeof(bf16);
+  static constexpr size_t c = size_t(LP_TM) * (COUT + 4) * sizeof(float);
+  static constexpr size_t total = w + 2 * win + c;
 };
 
-// out[co][l] = act(bias[co] + sum_{ci, o} W[o][ci][co] in[ci][l + off(o)]),
-// neighbours outside the grid read as zero.  act: ReLU when relu != 0; when
-// mask is given the result is multiplied by (mask[co][l] > 0) (the gradient
-// through the ReLU that produced mask).  out, when given, gets cout_store
-// channels in BF16; out32, when given, the same values in FP32.  Grid-stride over tiles of
-// LP_TM nodes; the weights stay in shared memory for the CTA's lifetime.
-template <int CIN, int COUT_PAD>
-__global__ void __launch_bounds__(256) k_lp_conv(LpGrid G, const bf16* __restrict__ in, const bf16* __restrict__ wk,
+// out[p][co] = act(bias[co] + sum_{ci, o} W[o][ci][co] in[p + off(o)][ci]) for
+// every interior row p (halo rows of out are not written).  act: ReLU when
+// relu != 0; when mask is given the result is multiplied by (mask[p][co] > 0)
+// (the gradient through the ReLU that produced mask).  out, when given, gets
+// the COUT channels in BF16; out32, when given, the first cout32 channels in
+// FP32 as [channel][node] in the level's node order.  Grid-stride over tiles;
+// the weights stay in shared memory for the CTA's lifetime.
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(256) k_lp_conv(LpPad P, const bf16* __restrict__ in, const bf16* __restrict__ wk,
                                                  const float* __restrict__ bias, int relu,
                                                  const bf16* __restrict__ mask, bf16* __restrict__ out,
-                                                 float* __restrict__ out32, int cout_store) {
+                                                 float* __restrict__ out32, int cout32) {
   pdl_wait();
   using namespace nvcuda;
-  using SM = LpConvSmem<CIN, COUT_PAD>;
-  constexpr int NF = COUT_PAD / 16, KC = CIN / 16;
+  using SM = LpConvSmem<CIN, COUT>;
+  constexpr int SA = SM::SA, NF = COUT / 16, KC = CIN / 16, LDC = COUT + 4;
   extern __shared__ __align__(128) unsigned char lp_smem[];
   bf16* Ws = reinterpret_cast<bf16*>(lp_smem);
-  bf16* As = reinterpret_cast<bf16*>(lp_smem + SM::w);
-  float* Cs = reinterpret_cast<float*>(lp_smem + SM::w + SM::a);
-  int* crd = reinterpret_cast<int*>(lp_smem + SM::w + SM::a + SM::c);
+  bf16* Win = reinterpret_cast<bf16*>(lp_smem + SM::w);
+  float* Cs = reinterpret_cast<float*>(lp_smem + SM::w + 2 * SM::win);
+  constexpr int WIN = int(SM::win / sizeof(bf16));
   const int tid = threadIdx.x, warp = tid >> 5;
-  for (int e = tid; e < 27 * CIN * COUT_PAD; e += blockDim.x) Ws[e] = wk[e];
-  const long N = G.N;
-  const long ntiles = (N + LP_TM - 1) / LP_TM;
-  for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const long l0 = tile * LP_TM;
-    __syncthreads();  // weights loaded / previous tile's reads of As, Cs, crd done
-    if (tid < LP_TM) {
-      const long l = l0 + tid;
-      const int i = int(l % G.im);
-      const long r = l / G.im;
-      crd[4 * tid + 0] = i;
-      crd[4 * tid + 1] = int(r % G.jm);
-      crd[4 * tid + 2] = int(r / G.jm);
-      crd[4 * tid + 3] = l < N;
-    }
+  const long ntiles = (P.p1 - P.p0 + LP_TM - 1) / LP_TM;
+  for (int e = tid; e < 27 * CIN * COUT / 8; e += 256) lp_cp16(Ws + 8 * e, wk + 8 * e, true);
+  lp_cp_commit();
+  long tile = blockIdx.x;
+  if (tile < ntiles) lp_load_window<CIN>(P, in, P.p0 + tile * LP_TM, 0, Win, tid, 256);
+  lp_cp_commit();
+  int buf = 0;
+  for (; tile < ntiles; tile += gridDim.x) {
     wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc[NF];
 #pragma unroll
     for (int f = 0; f < NF; ++f) wmma::fill_fragment(acc[f], 0.0f);
-    for (int o = 0; o < 27; ++o) {
-      int di, dj, dk;
-      lp_offset(o, di, dj, dk);
-      const long off = di + (long)G.im * (dj + (long)G.jm * dk);
-      __syncthreads();  // crd written / previous offset's fragments loaded
-      for (int e = tid; e < CIN * LP_TM; e += blockDim.x) {
-        const int c = e / LP_TM, r = e - c * LP_TM;
-        const int* cr = crd + 4 * r;
-        const int ii = cr[0] + di, jj = cr[1] + dj, kk = cr[2] + dk;
-        const bool ok = cr[3] && ii >= 0 && ii < G.im && jj >= 0 && jj < G.jm && kk >= 0 && kk < G.km;
-        As[c * LP_LDA + r] = ok ? in[(long)c * N + l0 + r + off] : __float2bfloat16(0.0f);
-      }
+    for (int g = 0; g < 9; ++g) {
+      // prefetch the next window (this tile's next pair, or the next tile's first)
+      const long nt = g < 8 ? tile : tile + gridDim.x;
+      if (nt < ntiles) lp_load_window<CIN>(P, in, P.p0 + nt * LP_TM, g < 8 ? g + 1 : 0, Win + (buf ^ 1) * WIN, tid, 256);
+      lp_cp_commit();
+      lp_cp_wait<1>();
       __syncthreads();
+      const bf16* A0 = Win + buf * WIN + warp * 16 * SA;
 #pragma unroll
-      for (int kc = 0; kc < KC; ++kc) {
-        wmma::fragment<wmma::matrix_a, 16, 16, 16, bf16, wmma::col_major> a;
-        wmma::load_matrix_sync(a, As + kc * 16 * LP_LDA + warp * 16, LP_LDA);
+      for (int di = 0; di < 3; ++di) {
+        const int o = 3 * g + di;
 #pragma unroll
-        for (int f = 0; f < NF; ++f) {
-          wmma::fragment<wmma::matrix_b, 16, 16, 16, bf16, wmma::row_major> b;
-          wmma::load_matrix_sync(b, Ws + (o * CIN + kc * 16) * COUT_PAD + f * 16, COUT_PAD);
-          wmma::mma_sync(acc[f], a, b, acc[f]);
+        for (int kc = 0; kc < KC; ++kc) {
+          wmma::fragment<wmma::matrix_a, 16, 16, 16, bf16, wmma::row_major> a;
+          wmma::load_matrix_sync(a, A0 + di * SA + kc * 16, SA);
+#pragma unroll
+          for (int f = 0; f < NF; ++f) {
+            wmma::fragment<wmma::matrix_b, 16, 16, 16, bf16, wmma::row_major> b;
+            wmma::load_matrix_sync(b, Ws + (o * CIN + kc * 16) * COUT + f * 16, COUT);
+            wmma::mma_sync(acc[f], a, b, acc[f]);
+          }
         }
       }
+      __syncthreads();  // the window is read before it is refilled
+      buf ^= 1;
     }
 #pragma unroll
     for (int f = 0; f < NF; ++f)
-      wmma::store_matrix_sync(Cs + warp * 16 * (COUT_PAD + 4) + f * 16, acc[f], COUT_PAD + 4, wmma::mem_row_major);
+      wmma::store_matrix_sync(Cs + warp * 16 * LDC + f * 16, acc[f], LDC, wmma::mem_row_major);
     __syncthreads();
-    for (int e = tid; e < cout_store * LP_TM; e += blockDim.x) {
-      const int co = e / LP_TM, r = e - co * LP_TM;
-      const long l = l0 + r;
-      if (l >= N) continue;
-      float v = Cs[r * (COUT_PAD + 4) + co] + (bias ? bias[co] : 0.0f);
-      if (relu) v = fmaxf(v, 0.0f);
-      if (mask && !(__bfloat162float(mask[(long)co * N + l]) > 0.0f)) v = 0.0f;
-      if (out) out[(long)co * N + l] = __float2bfloat16(v);
-      if (out32) out32[(long)co * N + l] = v;
+    const long t0 = P.p0 + tile * LP_TM;
+    for (int e = tid; e < LP_TM * (COUT / 8); e += 256) {
+      const int r = e / (COUT / 8), c8 = e - r * (COUT / 8);
+      const long p = t0 + r;
+      if (p >= P.p1) continue;
+      const long l = lp_node(P, p);
+      if (l < 0) continue;
+      float v[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        v[q] = Cs[r * LDC + 8 * c8 + q] + (bias ? bias[8 * c8 + q] : 0.0f);
+        if (relu) v[q] = fmaxf(v[q], 0.0f);
+      }
+      if (mask) {
+        const uint4 mv = *reinterpret_cast<const uint4*>(mask + p * COUT + 8 * c8);
+        const bf16* mb = reinterpret_cast<const bf16*>(&mv);
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          if (!(__bfloat162float(mb[q]) > 0.0f)) v[q] = 0.0f;
+      }
+      if (out) {
+        uint4 ov;
+        bf16* ob = reinterpret_cast<bf16*>(&ov);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) ob[q] = __float2bfloat16(v[q]);
+        *reinterpret_cast<uint4*>(out + p * COUT + 8 * c8) = ov;
+      }
+      if (out32) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          if (8 * c8 + q < cout32) out32[(long)(8 * c8 + q) * P.N + l] = v[q];
+      }
     }
+    // Cs is written again only after the next tile's window barriers
   }
+  lp_cp_wait<0>();
 }
 
-// dW[o][ci][co] += sum_l X[ci][l + off(o)] dY[co][l] over this CTA's range of
-// nodes (nodes_per_cta, a multiple of LP_TM), FP32 atomics into dW.  Warp w
-// owns output fragment w (CIN/16 x COUT_PAD/16 fragments of 16 x 16).
-template <int CIN, int COUT_PAD>
-__global__ void __launch_bounds__(128) k_lp_wgrad(LpGrid G, const bf16* __restrict__ X, const bf16* __restrict__ dY,
-                                                  float* __restrict__ dW, long nodes_per_cta) {
+// Shared-memory layout of k_lp_wgrad (bytes): two windows of X, two tiles of D.
+template <int CIN, int COUT>
+struct LpWgradSmem {
+  static constexpr int SA = LpStride<CIN>::v, SD = LpStride<COUT>::v;
+  static constexpr size_t win = size_t(LP_WROWS) * SA * sizeof(bf16);
+  static constexpr size_t d = size_t(LP_TM) * SD * sizeof(bf16);
+  static constexpr size_t total = 2 * win + 2 * d;
+};
+
+// Partial weight and bias gradients of one layer over a contiguous range of
+// tiles per CTA:
+//   part[cta][o][ci][co] = sum_p X[p + off(o)][ci] D[p][co],
+//   part[cta][27 CIN COUT + co] = sum_p D[p][co],
+// p over the tiles' rows (D is zero on halo rows and past the last interior
+// row).  3 * (CIN/16) * (COUT/16) warps; warp w owns the output fragment
+// (di, ci block, co block) of every (dj, dk) pair, so each window feeds every
+// warp once.
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(32 * 3 * (CIN / 16) * (COUT / 16))
+    k_lp_wgrad(LpPad P, const bf16* __restrict__ X, const bf16* __restrict__ D, float* __restrict__ part) {
   pdl_wait();
   using namespace nvcuda;
-  constexpr int MF = CIN / 16, NF = COUT_PAD / 16, F = MF * NF;
-  static_assert(F <= 4, "one output fragment per warp");
-  __shared__ __align__(128) bf16 Xs[CIN * LP_LDA];
-  __shared__ __align__(128) bf16 Ds[COUT_PAD * LP_LDA];
-  __shared__ __align__(128) float Cw[4][16 * 20];
-  __shared__ int crd[LP_TM * 4];
+  using SM = LpWgradSmem<CIN, COUT>;
+  constexpr int MF = CIN / 16, NF = COUT / 16, NW = 3 * MF * NF, NT = 32 * NW;
+  constexpr int SA = SM::SA, SD = SM::SD;
+  constexpr int WIN = int(SM::win / sizeof(bf16)), DT = int(SM::d / sizeof(bf16));
+  constexpr long SLOT = 27L * CIN * COUT + COUT;
+  extern __shared__ __align__(128) unsigned char lp_smem[];
+  bf16* Win = reinterpret_cast<bf16*>(lp_smem);
+  bf16* Dt = reinterpret_cast<bf16*>(lp_smem + 2 * SM::win);
+  __shared__ float bsum[NT];
   const int tid = threadIdx.x, warp = tid >> 5;
-  const long N = G.N;
-  const long n0 = blockIdx.x * nodes_per_cta;
-  const long n1 = min(N, n0 + nodes_per_cta);
-  const int mi = warp / NF, ni = warp % NF;
-  for (int o = 0; o < 27; ++o) {
-    int di, dj, dk;
-    lp_offset(o, di, dj, dk);
-    const long off = di + (long)G.im * (dj + (long)G.jm * dk);
-    wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc;
-    wmma::fill_fragment(acc, 0.0f);
-    for (long l0 = n0; l0 < n1; l0 += LP_TM) {
-      __syncthreads();  // previous chunk's fragments loaded
-      if (tid < LP_TM) {
-        const long l = l0 + tid;
-        const int i = int(l % G.im);
-        const long r = l / G.im;
-        crd[4 * tid + 0] = i;
-        crd[4 * tid + 1] = int(r % G.jm);
-        crd[4 * tid + 2] = int(r / G.jm);
-        crd[4 * tid + 3] = l < n1;
-      }
-      __syncthreads();
-      for (int e = tid; e < CIN * LP_TM; e += blockDim.x) {
-        const int c = e / LP_TM, r = e - c * LP_TM;
-        const int* cr = crd + 4 * r;
-        const int ii = cr[0] + di, jj = cr[1] + dj, kk = cr[2] + dk;
-        const bool ok = cr[3] && ii >= 0 && ii < G.im && jj >= 0 && jj < G.jm && kk >= 0 && kk < G.km;
-        Xs[c * LP_LDA + r] = ok ? X[(long)c * N + l0 + r + off] : __float2bfloat16(0.0f);
-      }
-      for (int e = tid; e < COUT_PAD * LP_TM; e += blockDim.x) {
-        const int c = e / LP_TM, r = e - c * LP_TM;
-        Ds[c * LP_LDA + r] = crd[4 * r + 3] ? dY[(long)c * N + l0 + r] : __float2bfloat16(0.0f);
-      }
-      __syncthreads();
-      if (warp < F) {
+  const int di = warp % 3, mi = (warp / 3) % MF, ni = warp / (3 * MF);
+  const long ntiles = (P.p1 - P.p0 + LP_TM - 1) / LP_TM;
+  const long per = (ntiles + gridDim.x - 1) / gridDim.x;
+  const long ta = blockIdx.x * per, tb = min(ntiles, ta + per);
+  auto load_d = [&](long tile, int b) {
+    const long t0 = P.p0 + tile * LP_TM;
+    for (int e = tid; e < LP_TM * (COUT / 8); e += NT) {
+      const int r = e / (COUT / 8), c = e - r * (COUT / 8);
+      const long row = t0 + r;
+      const bool ok = row < P.p1;
+      lp_cp16(Dt + b * DT + r * SD + 8 * c, D + (ok ? row : 0) * COUT + 8 * c, ok);
+    }
+  };
+  wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc[9];
 #pragma unroll
-        for (int ks = 0; ks < LP_TM / 16; ++ks) {
-          wmma::fragment<wmma::matrix_a, 16, 16, 16, bf16, wmma::row_major> a;   // (ci, node)
-          wmma::fragment<wmma::matrix_b, 16, 16, 16, bf16, wmma::col_major> b;   // (node, co)
-          wmma::load_matrix_sync(a, Xs + mi * 16 * LP_LDA + ks * 16, LP_LDA);
-          wmma::load_matrix_sync(b, Ds + ni * 16 * LP_LDA + ks * 16, LP_LDA);
-          wmma::mma_sync(acc, a, b, acc);
-        }
+  for (int g = 0; g < 9; ++g) wmma::fill_fragment(acc[g], 0.0f);
+  float bs = 0.0f;  // bias partial of channel tid % COUT
+  int buf = 0;
+  if (ta < tb) {
+    lp_load_window<CIN>(P, X, P.p0 + ta * LP_TM, 0, Win, tid, NT);
+    load_d(ta, 0);
+  }
+  lp_cp_commit();
+  for (long tile = ta; tile < tb; ++tile) {
+    const int db = int((tile - ta) & 1);
+#pragma unroll
+    for (int g = 0; g < 9; ++g) {
+      if (g < 8) {
+        lp_load_window<CIN>(P, X, P.p0 + tile * LP_TM, g + 1, Win + (buf ^ 1) * WIN, tid, NT);
+      } else if (tile + 1 < tb) {
+        lp_load_window<CIN>(P, X, P.p0 + (tile + 1) * LP_TM, 0, Win + (buf ^ 1) * WIN, tid, NT);
+        load_d(tile + 1, db ^ 1);
       }
-    }
-    if (warp < F) {
-      wmma::store_matrix_sync(Cw[warp], acc, 20, wmma::mem_row_major);
-      __syncwarp();
-      const int lane = tid & 31;
-      for (int e = lane; e < 256; e += 32) {
-        const int r = e / 16, c = e % 16;
-        atomicAdd(dW + ((long)o * CIN + mi * 16 + r) * COUT_PAD + ni * 16 + c, Cw[warp][r * 20 + c]);
+      lp_cp_commit();
+      lp_cp_wait<1>();
+      __syncthreads();
+      const bf16* A0 = Win + buf * WIN + di * SA + mi * 16;
+      const bf16* B0 = Dt + db * DT + ni * 16;
+#pragma unroll
+      for (int ks = 0; ks < LP_TM / 16; ++ks) {
+        wmma::fragment<wmma::matrix_a, 16, 16, 16, bf16, wmma::col_major> a;  // (ci, row)
+        wmma::fragment<wmma::matrix_b, 16, 16, 16, bf16, wmma::row_major> b;  // (row, co)
+        wmma::load_matrix_sync(a, A0 + ks * 16 * SA, SA);
+        wmma::load_matrix_sync(b, B0 + ks * 16 * SD, SD);
+        wmma::mma_sync(acc[g], a, b, acc[g]);
       }
+      if (g == 0) {
+        // bias partial: thread tid sums rows tid / COUT, + NT / COUT, ... of channel tid % COUT
+        const bf16* Db = Dt + db * DT;
+        for (int r = tid / COUT; r < LP_TM; r += NT / COUT) bs += __bfloat162float(Db[r * SD + tid % COUT]);
+      }
+      __syncthreads();  // the window (and, after the last pair, the D tile) is read before it is refilled
+      buf ^= 1;
     }
   }
-}
-
-// db[co] += sum_l dY[co][l] (FP32 atomics; blockIdx.y = co)
-__global__ void k_lp_bias_grad(long N, const bf16* __restrict__ dY, float* __restrict__ db) {
-  pdl_wait();
-  __shared__ float sh[256];
-  const int co = blockIdx.y;
-  float s = 0.0f;
-  for (long l = (long)blockIdx.x * blockDim.x + threadIdx.x; l < N; l += (long)gridDim.x * blockDim.x)
-    s += __bfloat162float(dY[(long)co * N + l]);
-  sh[threadIdx.x] = s;
+  lp_cp_wait<0>();
+  float* slot = part + blockIdx.x * SLOT;
+#pragma unroll
+  for (int g = 0; g < 9; ++g) {
+    const int o = 3 * g + di;
+    wmma::store_matrix_sync(slot + ((long)o * CIN + mi * 16) * COUT + ni * 16, acc[g], COUT, wmma::mem_row_major);
+  }
+  bsum[tid] = bs;
   __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
-    __syncthreads();
+  if (tid < COUT) {
+    float t = 0.0f;
+    for (int r = tid; r < NT; r += COUT) t += bsum[r];
+    slot[27L * CIN * COUT + tid] = t;
   }
-  if (threadIdx.x == 0) atomicAdd(db + co, sh[0]);
 }
 
-// Input features from the time levels, in[16][N] BF16 (channel 15 zero):
-// channel 3f + {0, 1, 2} = q^n_f, (q^n - q^{n-1})_f, (q^{n-1} - q^{n-2})_f,
-// each times rs[channel] (the reciprocal of its RMS).
-__global__ void k_lp_features(long N, const double* const* qn, const double* const* qnm1, const double* const* qnm2,
+// out[e] = sum over nslot slots of part[slot * len + e]
+__global__ void k_lp_reduce(int nslot, long len, const float* __restrict__ part, float* __restrict__ out) {
+  pdl_wait();
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= len) return;
+  float s = 0.0f;
+  for (int k = 0; k < nslot; ++k) s += part[(long)k * len + e];
+  out[e] = s;
+}
+
+// Input features from the time levels into the channel-last padded rows
+// in[p][16] (BF16; channel 15 zero): channel 3f + {0, 1, 2} = q^n_f,
+// (q^n - q^{n-1})_f, (q^{n-1} - q^{n-2})_f, each times rs[channel].
+__global__ void k_lp_features(LpPad P, const double* const* qn, const double* const* qnm1, const double* const* qnm2,
                               const float* __restrict__ rs, bf16* __restrict__ in) {
   pdl_wait();
   const long l = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (l >= N) return;
+  if (l >= P.N) return;
+  uint4 v[2];
+  bf16* x = reinterpret_cast<bf16*>(v);
 #pragma unroll
   for (int f = 0; f < 5; ++f) {
     const double a = qn[f][l], b = qnm1[f][l], c = qnm2[f][l];
-    in[(long)(3 * f + 0) * N + l] = __float2bfloat16(float(a) * rs[3 * f + 0]);
-    in[(long)(3 * f + 1) * N + l] = __float2bfloat16(float(a - b) * rs[3 * f + 1]);
-    in[(long)(3 * f + 2) * N + l] = __float2bfloat16(float(b - c) * rs[3 * f + 2]);
+    x[3 * f + 0] = __float2bfloat16(float(a) * rs[3 * f + 0]);
+    x[3 * f + 1] = __float2bfloat16(float(a - b) * rs[3 * f + 1]);
+    x[3 * f + 2] = __float2bfloat16(float(b - c) * rs[3 * f + 2]);
   }
-  in[15 * N + l] = __float2bfloat16(0.0f);
+  x[15] = __float2bfloat16(0.0f);
+  uint4* dst = reinterpret_cast<uint4*>(in + lp_row(P, l) * 16);
+  dst[0] = v[0];
+  dst[1] = v[1];
+}
+
+// [C][N] FP32 (node order) <-> channel-last padded rows [p][C] BF16
+__global__ void k_lp_rows_in(LpPad P, int C, int c0, int nc, const float* __restrict__ a, bf16* __restrict__ rows) {
+  pdl_wait();
+  const long l = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= P.N) return;
+  const long p = lp_row(P, l);
+  for (int c = 0; c < nc; ++c) rows[p * C + c0 + c] = __float2bfloat16(a[(long)c * P.N + l]);
+}
+
+__global__ void k_lp_rows_out(LpPad P, int C, int c0, int nc, const bf16* __restrict__ rows, float* __restrict__ a) {
+  pdl_wait();
+  const long l = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= P.N) return;
+  const long p = lp_row(P, l);
+  for (int c = 0; c < nc; ++c) a[(long)c * P.N + l] = __bfloat162float(rows[p * C + c0 + c]);
 }
 
 // Sums of squares of the 15 feature channels (before scaling) and of the
@@ -308,20 +437,22 @@ __global__ void k_lp_target(long N, const double* const* q, const double* const*
 }
 
 // Squared error of the network output y against t over the 5 output
-// channels: loss partial sums (acc[0], double) and dY = y - t in BF16
-// (channels 5..15 of dY stay zero); the factor 2 / (5 N) of the mean goes
-// into the gradient scale.
-__global__ void k_lp_loss(long N, const float* __restrict__ y, const float* __restrict__ t, bf16* __restrict__ dY,
+// channels: loss partial sums (acc[0], double) and dY = y - t in BF16 into
+// the channel-last padded rows dY[p][16] (channels 5..15 stay zero); the
+// factor 2 / (5 N) of the mean goes into the gradient scale.
+__global__ void k_lp_loss(LpPad P, const float* __restrict__ y, const float* __restrict__ t, bf16* __restrict__ dY,
                           double* acc) {
   pdl_wait();
   __shared__ double sh[256];
   double s = 0.0;
+  const long N = P.N;
   for (long l = (long)blockIdx.x * blockDim.x + threadIdx.x; l < N; l += (long)gridDim.x * blockDim.x) {
+    bf16* row = dY + lp_row(P, l) * 16;
 #pragma unroll
     for (int f = 0; f < 5; ++f) {
       const float d = y[(long)f * N + l] - t[(long)f * N + l];
       s += double(d) * double(d);
-      dY[(long)f * N + l] = __float2bfloat16(d);
+      row[f] = __float2bfloat16(d);
     }
   }
   sh[threadIdx.x] = s;
@@ -346,19 +477,6 @@ __global__ void k_lp_apply(long N, double* const* q, const double* const* qn, co
     const double corr = isfinite(c) ? double(s5[f]) * double(fminf(fmaxf(c, -ymax), ymax)) : 0.0;
     q[f][l] = 2.0 * qn[f][l] - qnm1[f][l] + corr;
   }
-}
-
-// FP32 <-> BF16 copies (host-given features, buffer reads)
-__global__ void k_lp_f2bf(long n, const float* __restrict__ a, bf16* __restrict__ b) {
-  pdl_wait();
-  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e < n) b[e] = __float2bfloat16(a[e]);
-}
-
-__global__ void k_lp_bf2f(long n, const bf16* __restrict__ a, float* __restrict__ b) {
-  pdl_wait();
-  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e < n) b[e] = __bfloat162float(a[e]);
 }
 
 // One layer's shape in the flat parameter vector: W[co][ci][o] (real
