@@ -11,7 +11,10 @@ ours:       value = device-timed seconds per physical step of the product
             FP32 line-sweep work; linear-extrapolation initial guess), state
             resident in HBM.  e2e = the same step through the C ABI with the
             state copied from pinned host memory and back every step.  The
-            plain FP64 path (q^n guess, as the reference) is timed too.
+            plain FP64 path (q^n guess, as the reference) is timed too, and
+            predictor_ab compares the three initial guesses (q^n, linear
+            extrapolation, the learned network) by iterations and seconds per
+            physical step to an absolute tolerance on the laminar cavity.
 reference:  the CPU oracle (C++ restatement of the reference, FP32 like the
             reference's own build, its loops on every host thread) on the same
             case; a bounded sample of pseudo-iterations scaled to one physical
@@ -147,6 +150,49 @@ def run_ours(args, rank, world, dist):
     def sum_over_ranks(x):
         return over_ranks(x, "sum", dist)
 
+    def predictor_ab(n_steps=24, skip=10):
+        """The three initial guesses on the laminar cavity 65^3 (MIXED, graph
+        path), each physical step run to an absolute tolerance of the
+        pseudo-time update: log10 mean |dq| of u, v, w below -7 (the
+        reference's eo_min test; its relative er_min test is switched off,
+        because it measures the drop from the guess's own first update and so
+        asks more of a better guess).  Steps skip+1 .. n_steps (after the lid's
+        start-up); seconds per step by CUDA events around mg_driver, training
+        of the network included."""
+        res = {"workload": "laminar lid-driven cavity Re=1000, 65^3, MIXED, steps %d-%d of dt=0.05, "
+                           "tolerance log10 mean|dq(u,v,w)| < -7, itmax 200" % (skip + 1, n_steps)}
+        for P, name in ((abi.PRED_QN, "qn"), (abi.PRED_LINEAR, "linear"), (abi.PRED_LEARNED, "learned")):
+            case, grid, state = cases.cavity(n=65, itmax=200)
+            case.precision_mode = abi.MIXED
+            case.predictor = P
+            case.use_graph = 1
+            case.er_min = -100.0
+            case.eo_min = -7.0
+            S = Solver(case)
+            S.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
+            S.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
+            stream = torch.cuda.ExternalStream(S.stream())
+            its, secs = [], []
+            for k in range(n_steps):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                S.sync()
+                e0.record(stream)
+                r = S.mg_driver()
+                e1.record(stream)
+                S.sync()
+                torch.cuda.synchronize()
+                if k >= skip:
+                    its.append(r["iterations"])
+                    secs.append(e0.elapsed_time(e1) / 1e3)
+            entry = {"iterations_per_step": its, "mean_iterations": float(np.mean(its)),
+                     "s_per_step": float(np.mean(secs))}
+            if P == abi.PRED_LEARNED:
+                entry["network"] = S.lp_report()
+            res[name] = entry
+            del S
+        return res
+
     def timed_steps(S, K, body):
         """K calls of body(), bracketed by barrier + synchronize, CUDA events
         on the library's stream; returns seconds per call (max over ranks)."""
@@ -262,6 +308,8 @@ def run_ours(args, rank, world, dist):
     field_err = {nm: float(np.linalg.norm(a[:, m] - b[:, m]) / max(1e-300, np.linalg.norm(b[:, m])))
                  for m, nm in enumerate(names)}
 
+    ab = predictor_ab() if not args.no_ab else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(args.case, max(1, int(np.mean(iters64))))
@@ -275,7 +323,8 @@ def run_ours(args, rank, world, dist):
         "impl": "ours",
         "config": {"workload": desc, "case": args.case, "grid": [case.im, case.jm, case.km],
                    "interior_nodes": nint, "precision": "mixed (FP64 state, residual, restriction, update and norm on every level; FP32 line-sweep work, modal transforms and SA ADI)",
-                   "predictor": "linear extrapolation", "learned_predictor": "not built",
+                   "predictor": "linear extrapolation",
+                   "learned_predictor": "built (predictor DESALM_PRED_LEARNED); compared in predictor_ab",
                    "pseudo_iterations_per_step": iters, "converged": conv,
                    "l2": "working set of every level > 126 MB L2 for the channel; no flush between steps",
                    "parallelism": "replicas only (%d independent replicas)" % world},
@@ -285,6 +334,7 @@ def run_ours(args, rank, world, dist):
                                  "how": "relative L2 over all nodes of the state after %d physical steps from the same "
                                         "initial state, both with the q^n guess" % (args.warmup + args.steps)},
         "cell_updates_per_s": sum_over_ranks(cell_updates),
+        "predictor_ab": ab,
         "e2e": {"value": e2e_sec, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "kernel": kind, "level": "fine", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -376,6 +426,7 @@ def main():
     ap.add_argument("--case", default="channel", choices=["cavity", "channel"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ab", action="store_true", help="skip the initial-guess comparison")
     ap.add_argument("--ncu-workload", action="store_true",
                     help="run one eager pseudo-iteration of --case for an ncu capture and exit")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])

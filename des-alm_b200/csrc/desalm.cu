@@ -127,6 +127,9 @@ struct LpState {
   float *y = nullptr, *t = nullptr;        // network output, training target [5][N]
   float *rs = nullptr, *rs5 = nullptr, *s5 = nullptr;  // feature scales (1/RMS), target scales, output scales
   double* acc = nullptr;                   // reductions
+  double* vacc = nullptr;                  // held-out check of the newest sample (k_lp_dot)
+  float* alpha = nullptr;                  // blend of each field's correction
+  float fixed_alpha = -1.0f;               // < 0: automatic blend
   double* qnm2[5] = {};                    // q^{n-2} of the fine level
   double* nut0 = nullptr;                  // nu_t at the start of a step begun from the network's guess
   double** tab = nullptr;                  // device table: q[5] qn[5] qnm1[5] qnm2[5]
@@ -790,6 +793,7 @@ int lp_alloc(desalm_ctx* ctx) {
   RET(A((void**)&lp.y, 5L * N * sizeof(float))); RET(A((void**)&lp.t, 5L * N * sizeof(float)));
   RET(A((void**)&lp.rs, 16 * sizeof(float))); RET(A((void**)&lp.rs5, 8 * sizeof(float)));
   RET(A((void**)&lp.s5, 8 * sizeof(float))); RET(A((void**)&lp.acc, 16 * sizeof(double)));
+  RET(A((void**)&lp.vacc, 16 * sizeof(double))); RET(A((void**)&lp.alpha, 8 * sizeof(float)));
   for (int f = 0; f < 5; ++f) RET(A((void**)&lp.qnm2[f], N * sizeof(double)));
   RET(A((void**)&lp.nut0, N * sizeof(double)));
   RET(A((void**)&lp.tab, 20 * sizeof(double*)));
@@ -921,6 +925,14 @@ int lp_learn(desalm_ctx* ctx) {
                                              (const double* const*)(lp.tab + 0), (const double* const*)(lp.tab + 5),
                                              (const double* const*)(lp.tab + 10), (const float*)lp.rs5, lp.t));
   CKL();
+  // held-out check: the current network on the new sample, before training on it
+  RET(lp_pack(ctx));
+  RET(lp_forward(ctx));
+  CK(cudaMemsetAsync(lp.vacc, 0, 16 * sizeof(double), ctx->stream));
+  LAUNCH(KC_LEARN, 0, (double)lp.N, launch_k(k_lp_dot, 296, 128, 0, ctx->stream, lp.N, (const float*)lp.y,
+                                             (const float*)lp.t, lp.ymax, lp.vacc));
+  LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_blend, 1, 32, 0, ctx->stream, (const double*)lp.vacc, lp.fixed_alpha, lp.alpha));
+  CKL();
   lp.samples += 1;
   for (int it = 0; it < lp.train_steps; ++it) {
     double loss = 0;
@@ -941,9 +953,11 @@ int lp_predict(desalm_ctx* ctx) {
   RET(lp_features(ctx, 5, 10, 15));
   RET(lp_pack(ctx));
   RET(lp_forward(ctx));
+  if (lp.fixed_alpha >= 0.0f)
+    LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_blend, 1, 32, 0, ctx->stream, (const double*)lp.vacc, lp.fixed_alpha, lp.alpha));
   LAUNCH(KC_LEARN, 0, (double)lp.N, launch_k(k_lp_apply, cdiv(lp.N, 256), 256, 0, ctx->stream, lp.N, lp.tab + 0,
                                              (const double* const*)(lp.tab + 5), (const double* const*)(lp.tab + 10),
-                                             (const float*)lp.s5, (const float*)lp.y, lp.ymax));
+                                             (const float*)lp.s5, (const float*)lp.alpha, (const float*)lp.y, lp.ymax));
   CKL();
   void* nut;
   int esz;
@@ -1763,6 +1777,14 @@ int graph_step(desalm_ctx* ctx, desalm_step_report* rep) {
 // ------------------------------------------------------ learned guess ABI
 extern "C" {
 
+int desalm_lp_blend(desalm_ctx* ctx, float alpha) {
+  if (!ctx) return DESALM_EINVAL;
+  if (!ctx->lp.on) { ctx->err = "the learned guess is off"; return DESALM_EINVAL; }
+  if (std::isnan(alpha) || alpha > 1.0f) { ctx->err = "lp_blend: alpha must be <= 1"; return DESALM_EINVAL; }
+  ctx->lp.fixed_alpha = alpha < 0.0f ? -1.0f : alpha;
+  return 0;
+}
+
 int desalm_lp_config(desalm_ctx* ctx, int train_steps, int warm, float lr, float ymax) {
   if (!ctx) return DESALM_EINVAL;
   if (!ctx->lp.on) { ctx->err = "the learned guess is off (predictor is not DESALM_PRED_LEARNED)"; return DESALM_EINVAL; }
@@ -1787,6 +1809,22 @@ int desalm_lp_report_get(desalm_ctx* ctx, desalm_lp_report* r) {
   r->fallbacks = lp.fallbacks;
   r->first_loss = lp.first_loss;
   r->last_loss = lp.last_loss;
+  r->heldout_ratio = -1.0;
+  for (int f = 0; f < 5; ++f) r->alpha[f] = 0.0;
+  if (lp.on && lp.samples > 0) {
+    double v[16];
+    float a[8];
+    CK(cudaMemcpyAsync(v, lp.vacc, sizeof(v), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(a, lp.alpha, sizeof(a), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    double num = 0.0, den = 0.0;
+    for (int f = 0; f < 5; ++f) {
+      num += v[10 + f] - 2.0 * a[f] * v[f] + double(a[f]) * a[f] * v[5 + f];
+      den += v[10 + f];
+      r->alpha[f] = a[f];
+    }
+    r->heldout_ratio = den > 0.0 ? num / den : -1.0;
+  }
   return 0;
 }
 
@@ -1860,6 +1898,7 @@ int desalm_lp_get_buffer(desalm_ctx* ctx, int which, float* out) {
     case DESALM_LP_TARGET: CK(cudaMemcpyAsync(out, lp.t, 5 * N * sizeof(float), cudaMemcpyDeviceToHost, s)); break;
     case DESALM_LP_OUTPUT: CK(cudaMemcpyAsync(out, lp.y, 5 * N * sizeof(float), cudaMemcpyDeviceToHost, s)); break;
     case DESALM_LP_SCALES: CK(cudaMemcpyAsync(out, lp.rs, 16 * sizeof(float), cudaMemcpyDeviceToHost, s)); break;
+    case DESALM_LP_ALPHA: CK(cudaMemcpyAsync(out, lp.alpha, 5 * sizeof(float), cudaMemcpyDeviceToHost, s)); break;
     default: ctx->err = "lp_get_buffer: unknown buffer"; return DESALM_EINVAL;
   }
   CK(cudaStreamSynchronize(s));

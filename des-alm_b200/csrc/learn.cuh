@@ -464,17 +464,67 @@ __global__ void k_lp_loss(LpPad P, const float* __restrict__ y, const float* __r
   if (threadIdx.x == 0) atomicAdd(acc, sh[0]);
 }
 
-// The guess q = 2 q^n - q^{n-1} + s_f min(max(y_f, -ymax), ymax); a node
-// whose network output is not finite keeps the linear extrapolation.
+// Held-out check of the network on a new sample, before it trains on it:
+// per field f, acc[f] += sum y_f t_f, acc[5 + f] += sum y_f^2,
+// acc[10 + f] += sum t_f^2 (y clipped to [-ymax, ymax] as in the guess).
+__global__ void k_lp_dot(long N, const float* __restrict__ y, const float* __restrict__ t, float ymax, double* acc) {
+  pdl_wait();
+  __shared__ double sh[15][128];
+  double s[15];
+#pragma unroll
+  for (int c = 0; c < 15; ++c) s[c] = 0.0;
+  for (long l = (long)blockIdx.x * blockDim.x + threadIdx.x; l < N; l += (long)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int f = 0; f < 5; ++f) {
+      const float yv = y[(long)f * N + l];
+      const double a = isfinite(yv) ? double(fminf(fmaxf(yv, -ymax), ymax)) : 0.0;
+      const double b = t[(long)f * N + l];
+      s[f] += a * b;
+      s[5 + f] += a * a;
+      s[10 + f] += b * b;
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 15; ++c) sh[c][threadIdx.x] = s[c];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+#pragma unroll
+      for (int c = 0; c < 15; ++c) sh[c][threadIdx.x] += sh[c][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x < 15) atomicAdd(acc + threadIdx.x, sh[threadIdx.x][0]);
+}
+
+// Blend of each field's correction: automatic (fixed < 0): the least-squares
+// factor alpha_f = <y, t> / <y, y> of the held-out check, limited to [0, 1]
+// (0 when the network's output is zero or not finite), so that a network that
+// does not help leaves the linear extrapolation; otherwise alpha_f = fixed.
+__global__ void k_lp_blend(const double* __restrict__ acc, float fixed, float* __restrict__ alpha) {
+  pdl_wait();
+  const int f = threadIdx.x;
+  if (f >= 5) return;
+  float a = fixed;
+  if (fixed < 0.0f) {
+    const double yt = acc[f], yy = acc[5 + f];
+    const double r = yy > 0.0 ? yt / yy : 0.0;
+    a = isfinite(r) ? float(fmin(fmax(r, 0.0), 1.0)) : 0.0f;
+  }
+  alpha[f] = a;
+}
+
+// The guess q = 2 q^n - q^{n-1} + s_f alpha_f min(max(y_f, -ymax), ymax); a
+// node whose network output is not finite keeps the linear extrapolation.
 __global__ void k_lp_apply(long N, double* const* q, const double* const* qn, const double* const* qnm1,
-                           const float* __restrict__ s5, const float* __restrict__ y, float ymax) {
+                           const float* __restrict__ s5, const float* __restrict__ alpha, const float* __restrict__ y,
+                           float ymax) {
   pdl_wait();
   const long l = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= N) return;
 #pragma unroll
   for (int f = 0; f < 5; ++f) {
     const float c = y[(long)f * N + l];
-    const double corr = isfinite(c) ? double(s5[f]) * double(fminf(fmaxf(c, -ymax), ymax)) : 0.0;
+    const double corr = isfinite(c) ? double(s5[f] * alpha[f]) * double(fminf(fmaxf(c, -ymax), ymax)) : 0.0;
     q[f][l] = 2.0 * qn[f][l] - qnm1[f][l] + corr;
   }
 }

@@ -21,7 +21,7 @@ PRED_QN = 0
 PRED_LINEAR = 1
 PRED_LEARNED = 2
 
-LP_FEATURES, LP_TARGET, LP_OUTPUT, LP_SCALES = 0, 1, 2, 3
+LP_FEATURES, LP_TARGET, LP_OUTPUT, LP_SCALES, LP_ALPHA = 0, 1, 2, 3, 4
 
 BC_INTERFACE, BC_WALL, BC_SYMMETRY, BC_FREESTREAM, BC_INFLOW, BC_PERIODIC = 0, 1, 2, 3, 4, 6
 
@@ -99,10 +99,14 @@ class LpReport(C.Structure):
         ("fallbacks", C.c_long),
         ("first_loss", C.c_double),
         ("last_loss", C.c_double),
+        ("heldout_ratio", C.c_double),
+        ("alpha", C.c_double * 5),
     ]
 
     def as_dict(self):
-        return {name: getattr(self, name) for name, _ in self._fields_}
+        d = {name: getattr(self, name) for name, _ in self._fields_}
+        d["alpha"] = list(self.alpha)
+        return d
 
 
 def level_dims(case, n):

@@ -72,6 +72,7 @@ def lib():
         for name, args in [
             ("lp_config", [vp, ip, ip, C.c_float, C.c_float]),
             ("lp_report_get", [vp, C.POINTER(LpReport)]),
+            ("lp_blend", [vp, C.c_float]),
             ("lp_get_params", [vp, fp]),
             ("lp_set_params", [vp, fp]),
             ("lp_eval", [vp, fp, fp, fp, dp, fp]),
@@ -234,6 +235,10 @@ class Solver:
     def lp_config(self, train_steps=-1, warm=-1, lr=-1.0, ymax=-1.0):
         self._ck(self.L.desalm_lp_config(self.ctx, int(train_steps), int(warm), float(lr), float(ymax)), "lp_config")
 
+    def lp_blend(self, alpha=-1.0):
+        """alpha < 0: automatic blend of each field's correction; else fixed."""
+        self._ck(self.L.desalm_lp_blend(self.ctx, float(alpha)), "lp_blend")
+
     def lp_report(self):
         r = LpReport()
         self._ck(self.L.desalm_lp_report_get(self.ctx, C.byref(r)), "lp_report_get")
@@ -264,7 +269,7 @@ class Solver:
 
     def lp_buffer(self, which):
         N = self.case.im * self.case.jm * self.case.km
-        size = {0: 16 * N, 1: 5 * N, 2: 5 * N, 3: 16}[which]
+        size = {0: 16 * N, 1: 5 * N, 2: 5 * N, 3: 16, 4: 5}[which]
         out = np.zeros(size, dtype=np.float32)
         self._ck(self.L.desalm_lp_get_buffer(self.ctx, which, _f32p(out)), "lp_get_buffer")
-        return out if which == 3 else out.reshape(-1, N)
+        return out if which >= 3 else out.reshape(-1, N)

@@ -221,8 +221,12 @@ int  desalm_mg_residual_noalloc(const double* q, const double* qold, int im,
  * the start of every physical step desalm_begin_step trains it on the step
  * just converged (train_steps Adam steps on the mean squared error) and, once
  * it has seen warm samples, starts the pseudo-time loop from
- * 2 q^n - q^{n-1} + s_f * output; a node whose output is not finite keeps the
- * linear extrapolation.  The scales are those of the time levels at hand; a
+ * 2 q^n - q^{n-1} + s_f * alpha_f * output; a node whose output is not
+ * finite keeps the linear extrapolation.  alpha_f, the blend, is by default
+ * the least-squares factor <y_f, t_f> / <y_f, y_f> limited to [0, 1], where
+ * y is the network's output on the newest sample before it trains on it and
+ * t that sample's target: a network that does not help gets alpha near 0 and
+ * leaves the linear guess.  The scales are those of the time levels at hand; a
  * difference whose RMS is below 1e-12 of its field's RMS has scale zero, so
  * that field gets no correction.  desalm_mg_driver restarts a step begun from
  * the network's guess from the linear guess when the step ends with a
@@ -241,6 +245,11 @@ typedef struct desalm_lp_report {
                          non-finite norm or a zero pivot                  */
   double first_loss;  /* loss of the first training step (-1: none yet)   */
   double last_loss;   /* loss of the latest training step                 */
+  double heldout_ratio; /* on the newest sample, before training on it: the
+                         squared error of the blended correction over that
+                         of no correction (the linear guess); < 1 means
+                         the network helps (-1: no sample yet)            */
+  double alpha[5];    /* current blend of each field's correction         */
 } desalm_lp_report;
 
 /* buffers readable with desalm_lp_get_buffer */
@@ -248,6 +257,7 @@ typedef struct desalm_lp_report {
 #define DESALM_LP_TARGET   1   /* [5][N] latest training target                          */
 #define DESALM_LP_OUTPUT   2   /* [5][N] latest network output (FP32)                    */
 #define DESALM_LP_SCALES   3   /* [16] reciprocal RMS of the 15 input channels (0: still) */
+#define DESALM_LP_ALPHA    4   /* [5] blend of each field's correction                   */
 
 /* Settings; a negative value keeps the current one.  Defaults: 8 Adam steps
  * per sample, warm = 2 samples before the first guess, lr = 1e-3, and
@@ -255,6 +265,8 @@ typedef struct desalm_lp_report {
 int  desalm_lp_config(desalm_ctx* ctx, int train_steps, int warm, float lr,
                       float ymax);
 int  desalm_lp_report_get(desalm_ctx* ctx, desalm_lp_report* r);
+/* Blend: alpha < 0 (default) automatic; 0 <= alpha <= 1 fixed for every field. */
+int  desalm_lp_blend(desalm_ctx* ctx, float alpha);
 /* nparam floats in the flat layout above; set restarts the Adam moments */
 int  desalm_lp_get_params(desalm_ctx* ctx, float* theta);
 int  desalm_lp_set_params(desalm_ctx* ctx, const float* theta);

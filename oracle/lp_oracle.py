@@ -197,12 +197,29 @@ def target(q, qn, qnm1, rs):
     return ((q - 2.0 * qn + qnm1).astype(np.float32) * rs5[:, None]).astype(np.float32)
 
 
-def guess(qn, qnm1, y, s5, ymax=8.0):
-    """2 q^n - q^{n-1} + s_f min(max(y_f, -ymax), ymax); the linear
-    extrapolation where y is not finite."""
+def blend(y, t, ymax=8.0):
+    """Least-squares factor <y_f, t_f> / <y_f, y_f> of each field, limited to
+    [0, 1] (0 when y_f is zero or the ratio is not finite), with y clipped to
+    [-ymax, ymax] and non-finite outputs counted as zero."""
     y = np.asarray(y, np.float32)
+    yc = np.where(np.isfinite(y), np.clip(y, np.float32(-ymax), np.float32(ymax)), 0.0).astype(np.float64)
+    t = np.asarray(t, np.float64)
+    a = np.zeros(5, np.float32)
+    for f in range(5):
+        yy = np.sum(yc[f] * yc[f])
+        r = np.sum(yc[f] * t[f]) / yy if yy > 0 else 0.0
+        a[f] = np.float32(min(max(r, 0.0), 1.0)) if np.isfinite(r) else 0.0
+    return a
+
+
+def guess(qn, qnm1, y, s5, ymax=8.0, alpha=None):
+    """2 q^n - q^{n-1} + s_f alpha_f min(max(y_f, -ymax), ymax) (alpha = 1 by
+    default); the linear extrapolation where y is not finite."""
+    y = np.asarray(y, np.float32)
+    a = np.ones(5, np.float32) if alpha is None else np.asarray(alpha, np.float32)
+    sa = (np.asarray(s5, np.float32) * a).astype(np.float32)
     yc = np.clip(y, np.float32(-ymax), np.float32(ymax)).astype(np.float64)
-    corr = np.where(np.isfinite(y), np.asarray(s5, np.float32)[:, None].astype(np.float64) * yc, 0.0)
+    corr = np.where(np.isfinite(y), sa[:, None].astype(np.float64) * yc, 0.0)
     return 2.0 * qn - qnm1 + corr
 
 

@@ -100,6 +100,7 @@ def test_zero_network_is_linear_extrapolation_bitwise():
     for k in ("q", "qn", "qnm1", "nut"):
         assert np.array_equal(st[k], st_lin[k]), k
     assert [r["iterations"] for r in reps] == [r["iterations"] for r in reps_lin]
+    assert S.lp_report()["alpha"] == [0.0] * 5
     r = S.lp_report()
     # step 1 cannot train (q^{n-2} unknown); steps 2..4 train on one sample each
     assert r["samples"] == 3 and r["train_steps"] == 6 and r["predictions"] == 4
@@ -146,11 +147,13 @@ def test_features_targets_and_guess_match_oracle():
             x = S.lp_buffer(abi.LP_FEATURES)
             assert np.array_equal(x, lp.features(q, qn, qnm1, got_rs))
             y = S.lp_buffer(abi.LP_OUTPUT)
+            alpha = S.lp_buffer(abi.LP_ALPHA)
+            assert ((alpha >= 0) & (alpha <= 1)).all()
             s5_gpu = np.array([np.float32(1.0) / got_rs[3 * f + 1] if got_rs[3 * f + 1] > 0 else 0.0
                                for f in range(5)], np.float32)
             assert np.allclose(s5_gpu, s5, rtol=1e-6, atol=0)
             g = _soa(S.get_state()["q"])
-            assert np.allclose(g, lp.guess(q, qn, y, s5), rtol=0, atol=1e-6 * max(1.0, np.abs(g).max()))
+            assert np.allclose(g, lp.guess(q, qn, y, s5, alpha=alpha), rtol=0, atol=1e-6 * max(1.0, np.abs(g).max()))
             checked += 1
         S.pseudo_iteration()
         hist.append(_soa(S.get_state()["q"]))
@@ -167,6 +170,7 @@ def test_blown_up_learned_step_restarts_from_linear_guess():
         th[lp.nparam() - 5:] = 1e30
         S.lp_set_params(th)
         S.lp_config(train_steps=1, warm=2, lr=0.0, ymax=3e38)
+        S.lp_blend(1.0)                                      # no held-out damping
     S, st, reps = _run(abi.PRED_LEARNED, 4, setup)
     _, st_lin, reps_lin = _run(abi.PRED_LINEAR, 4)
     r = S.lp_report()
@@ -187,3 +191,25 @@ def test_training_lowers_the_loss_on_a_sample():
     assert r["samples"] == 1 and r["train_steps"] == 40 and r["predictions"] == 0
     assert np.isfinite(r["first_loss"]) and np.isfinite(r["last_loss"])
     assert r["last_loss"] < r["first_loss"], r
+
+
+def test_heldout_blend_matches_oracle():
+    """With no training steps and no guesses, the output buffer after a
+    sample is the held-out pass of the current network on it: the blend and
+    the held-out error ratio follow from it and the target."""
+    def setup(S):
+        S.lp_set_params(lp.init_params(seed=11, last_scale=1.0))
+        S.lp_config(train_steps=0, warm=100)
+    S, _, _ = _run(abi.PRED_LEARNED, 3, setup)
+    y = S.lp_buffer(abi.LP_OUTPUT)
+    t = S.lp_buffer(abi.LP_TARGET)
+    want = lp.blend(y, t)
+    got = S.lp_buffer(abi.LP_ALPHA)
+    assert np.allclose(got, want, rtol=1e-5, atol=1e-7)
+    r = S.lp_report()
+    a = want.astype(np.float64)
+    yc = np.clip(y, -8.0, 8.0).astype(np.float64)
+    num = sum(np.sum((t[f] - a[f] * yc[f]) ** 2) for f in range(5))
+    den = sum(np.sum(t[f].astype(np.float64) ** 2) for f in range(5))
+    assert abs(r["heldout_ratio"] - num / den) <= 1e-5 * max(1.0, num / den)
+    assert r["heldout_ratio"] <= 1.0 + 1e-9

@@ -141,3 +141,17 @@ def test_still_channels_have_zero_scale():
         assert rs[3 * f + 2] == 0
     t = lp.target(qn + 1e-3, qn, qnm1, rs)
     assert not t[[0, 2, 3, 4]].any() and t[1].any()
+
+
+def test_blend_least_squares_factor():
+    rng = np.random.default_rng(8)
+    t = rng.normal(size=(5, N)).astype(np.float32)
+    y = np.stack([2 * t[0], -t[1], np.zeros(N), 0.5 * t[3], t[4]]).astype(np.float32)
+    y[4, 0] = np.nan
+    a = lp.blend(y, t, ymax=1e30)
+    assert np.allclose(a[[0, 1, 2, 3]], [0.5, 0.0, 0.0, 1.0], atol=1e-6)
+    assert 0.0 < a[4] <= 1.0
+    # the blended correction never does worse than none on the sample it was fitted to
+    for f in range(5):
+        yc = np.where(np.isfinite(y[f]), y[f], 0.0).astype(np.float64)
+        assert np.sum((t[f] - a[f] * yc) ** 2) <= np.sum(t[f].astype(np.float64) ** 2) + 1e-9
