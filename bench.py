@@ -402,20 +402,28 @@ def run_reference(args):
 REF_ITERS = {"cavity": 200, "channel": 400}
 
 
-def ncu_workload(case_name, precision):
+def ncu_workload(case_name, precision, learned=False):
     """A short, eager run for Nsight Compute captures: the case's setup, the
     start of a physical step and one pseudo-iteration, without CUDA graphs
-    (so every kernel is a separate, capturable launch)."""
+    (so every kernel is a separate, capturable launch).  learned: instead,
+    four physical steps of two pseudo-iterations with the learned guess, so
+    that steps 2-4 train the network and steps 3-4 start from its guess."""
     from desalm.solver import Solver
-    case, grid, state, _ = build_case(case_name, precision, abi.PRED_LINEAR)
+    case, grid, state, _ = build_case(case_name, precision, abi.PRED_LEARNED if learned else abi.PRED_LINEAR)
     case.use_graph = 0
+    if learned:
+        case.itmax = 2
     S = Solver(case)
     S.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
     S.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
-    S.begin_step()
-    S.pseudo_iteration()
+    if learned:
+        for _ in range(4):
+            S.mg_driver()
+    else:
+        S.begin_step()
+        S.pseudo_iteration()
     S.sync()
-    print(json.dumps({"ncu_workload": case_name, "precision": precision}))
+    print(json.dumps({"ncu_workload": case_name, "precision": precision, "learned": learned}))
 
 
 def main():
@@ -430,9 +438,10 @@ def main():
     ap.add_argument("--ncu-workload", action="store_true",
                     help="run one eager pseudo-iteration of --case for an ncu capture and exit")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--learned", action="store_true", help="with --ncu-workload: learned-guess steps")
     args = ap.parse_args()
     if args.ncu_workload:
-        ncu_workload(args.case, abi.MIXED if args.precision == "mixed" else abi.FP64)
+        ncu_workload(args.case, abi.MIXED if args.precision == "mixed" else abi.FP64, args.learned)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
