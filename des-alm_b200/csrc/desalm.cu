@@ -23,6 +23,7 @@
 #include "mg.cuh"
 #include "sa.cuh"
 #include "learn.cuh"
+#include "learn_tc.cuh"
 
 using namespace desalm;
 
@@ -123,6 +124,8 @@ struct LpState {
   bf16 *wf[4] = {}, *wd[4] = {};           // forward / data-gradient weight blocks
   float *dW[4] = {}, *db[4] = {};          // per-layer weight and bias gradients (db inside dW's block)
   float* part = nullptr;                   // per-CTA partial gradients of k_lp_wgrad
+  CUtensorMap tm_x0, tm_a[3], tm_dy4, tm_dya[2];  // TMA maps of the convolutions' inputs
+  int* err = nullptr;                      // set by a tensor-core kernel whose wait timed out
   bf16 *x0 = nullptr, *a[3] = {}, *dy4 = nullptr, *dya[2] = {};  // features, activations, gradients
   float *y = nullptr, *t = nullptr;        // network output, training target [5][N]
   float *rs = nullptr, *rs5 = nullptr, *s5 = nullptr;  // feature scales (1/RMS), target scales, output scales
@@ -712,15 +715,62 @@ int sa_conservation(desalm_ctx* ctx);
 // ----------------------------------------------------------- learned guess
 constexpr int kLpWgradGrid = 148 * 2;  // partial slots of k_lp_wgrad (its largest grid)
 
+// cuTensorMapEncodeTiled, reached through the runtime's driver entry point
+typedef CUresult (*LpEncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// TMA map of channel-last rows [np][C] (BF16): boxes of 8 channels x 130 rows,
+// no swizzle, rows past the ends read as zero.
+int lp_tmap(desalm_ctx* ctx, CUtensorMap* m, const bf16* rows, int C, long np) {
+  static LpEncodeTiled enc = nullptr;
+  if (!enc) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+    if (!fn || q != cudaDriverEntryPointSuccess) {
+      ctx->err = "cuTensorMapEncodeTiled is not available";
+      return DESALM_ECUDA;
+    }
+    enc = (LpEncodeTiled)fn;
+  }
+  const cuuint64_t dims[2] = {(cuuint64_t)C, (cuuint64_t)np};
+  const cuuint64_t strides[1] = {(cuuint64_t)C * sizeof(bf16)};
+  const cuuint32_t box[2] = {8, (cuuint32_t)LP_WROWS};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)rows, dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    ctx->err = "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")";
+    return DESALM_ECUDA;
+  }
+  return 0;
+}
+
+// One convolution on the tensor cores (k_lp_conv_tc); map describes `in`.
 template <int CIN, int COUT>
-int lp_conv(desalm_ctx* ctx, const bf16* in, const bf16* w, const float* bias, int relu, const bf16* mask, bf16* out,
-            float* out32, int cout32) {
+int lp_conv(desalm_ctx* ctx, const CUtensorMap& map, const bf16* w, const float* bias, int relu, const bf16* mask,
+            bf16* out, float* out32, int cout32) {
   LpState& lp = ctx->lp;
   const long tiles = (lp.P.p1 - lp.P.p0 + LP_TM - 1) / LP_TM;
   const unsigned grid = (unsigned)std::min<long>(tiles, 148L * 2);
-  LAUNCH(KC_LEARN, 0, (double)lp.N, launch_k(k_lp_conv<CIN, COUT>, grid, 256, LpConvSmem<CIN, COUT>::total, ctx->stream,
-                                             lp.P, in, w, bias, relu, mask, out, out32, cout32));
+  LAUNCH(KC_LEARN, 0, (double)lp.N, launch_k(k_lp_conv_tc<CIN, COUT>, grid, LP_TC_THREADS, LpTcSmem<CIN, COUT>::total,
+                                             ctx->stream, map, lp.P, w, bias, relu, mask, out, out32, cout32, lp.err));
   CKL();
+  return 0;
+}
+
+// The tensor-core kernels' error flag (read after a synchronisation): a wait
+// that timed out leaves DESALM_ETIMEOUT and clears the flag.
+int lp_check(desalm_ctx* ctx) {
+  int e = 0;
+  CK(cudaMemcpy(&e, ctx->lp.err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) {
+    CK(cudaMemset(ctx->lp.err, 0, sizeof(int)));
+    ctx->err = "learned guess: a tensor-core kernel gave up waiting for its copies or MMAs";
+    return DESALM_ETIMEOUT;
+  }
   return 0;
 }
 
@@ -747,9 +797,9 @@ cudaError_t lp_optin(K* k, size_t bytes) {
 }
 
 cudaError_t lp_attrs() {
-  cudaError_t e = lp_optin(k_lp_conv<16, 32>, LpConvSmem<16, 32>::total);
-  if (e == cudaSuccess) e = lp_optin(k_lp_conv<32, 32>, LpConvSmem<32, 32>::total);
-  if (e == cudaSuccess) e = lp_optin(k_lp_conv<32, 16>, LpConvSmem<32, 16>::total);
+  cudaError_t e = lp_optin(k_lp_conv_tc<16, 32>, LpTcSmem<16, 32>::total);
+  if (e == cudaSuccess) e = lp_optin(k_lp_conv_tc<32, 32>, LpTcSmem<32, 32>::total);
+  if (e == cudaSuccess) e = lp_optin(k_lp_conv_tc<32, 16>, LpTcSmem<32, 16>::total);
   if (e == cudaSuccess) e = lp_optin(k_lp_wgrad<16, 32>, LpWgradSmem<16, 32>::total);
   if (e == cudaSuccess) e = lp_optin(k_lp_wgrad<32, 32>, LpWgradSmem<32, 32>::total);
   if (e == cudaSuccess) e = lp_optin(k_lp_wgrad<32, 16>, LpWgradSmem<32, 16>::total);
@@ -790,6 +840,11 @@ int lp_alloc(desalm_ctx* ctx) {
   for (int l = 0; l < 3; ++l) RET(A((void**)&lp.a[l], 32L * NP * sizeof(bf16)));
   RET(A((void**)&lp.dy4, 16L * NP * sizeof(bf16)));
   for (int l = 0; l < 2; ++l) RET(A((void**)&lp.dya[l], 32L * NP * sizeof(bf16)));
+  RET(A((void**)&lp.err, sizeof(int)));
+  RET(lp_tmap(ctx, &lp.tm_x0, lp.x0, 16, NP));
+  for (int l = 0; l < 3; ++l) RET(lp_tmap(ctx, &lp.tm_a[l], lp.a[l], 32, NP));
+  RET(lp_tmap(ctx, &lp.tm_dy4, lp.dy4, 16, NP));
+  for (int l = 0; l < 2; ++l) RET(lp_tmap(ctx, &lp.tm_dya[l], lp.dya[l], 32, NP));
   RET(A((void**)&lp.y, 5L * N * sizeof(float))); RET(A((void**)&lp.t, 5L * N * sizeof(float)));
   RET(A((void**)&lp.rs, 16 * sizeof(float))); RET(A((void**)&lp.rs5, 8 * sizeof(float)));
   RET(A((void**)&lp.s5, 8 * sizeof(float))); RET(A((void**)&lp.acc, 16 * sizeof(double)));
@@ -827,7 +882,7 @@ int lp_pack(desalm_ctx* ctx) {
   LpState& lp = ctx->lp;
   for (int l = 0; l < 4; ++l) {
     const long total = 27L * lp.ly[l].cin_pad * lp.ly[l].cout_pad;
-    LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_pack, cdiv(total, 256), 256, 0, ctx->stream, lp.ly[l], (const float*)lp.theta, lp.wf[l], lp.wd[l]));
+    LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_pack_tc, cdiv(total, 256), 256, 0, ctx->stream, lp.ly[l], (const float*)lp.theta, lp.wf[l], lp.wd[l]));
   }
   CKL();
   return 0;
@@ -839,10 +894,10 @@ int lp_forward(desalm_ctx* ctx) {
   const float* b[4];
   for (int l = 0; l < 4; ++l) b[l] = lp.theta + lp.ly[l].boff;
   // the bias pointers index the flat vector: each layer's bias is contiguous there
-  RET((lp_conv<16, 32>(ctx, lp.x0, lp.wf[0], b[0], 1, nullptr, lp.a[0], nullptr, 0)));
-  RET((lp_conv<32, 32>(ctx, lp.a[0], lp.wf[1], b[1], 1, nullptr, lp.a[1], nullptr, 0)));
-  RET((lp_conv<32, 32>(ctx, lp.a[1], lp.wf[2], b[2], 1, nullptr, lp.a[2], nullptr, 0)));
-  RET((lp_conv<32, 16>(ctx, lp.a[2], lp.wf[3], b[3], 0, nullptr, nullptr, lp.y, 5)));
+  RET((lp_conv<16, 32>(ctx, lp.tm_x0, lp.wf[0], b[0], 1, nullptr, lp.a[0], nullptr, 0)));
+  RET((lp_conv<32, 32>(ctx, lp.tm_a[0], lp.wf[1], b[1], 1, nullptr, lp.a[1], nullptr, 0)));
+  RET((lp_conv<32, 32>(ctx, lp.tm_a[1], lp.wf[2], b[2], 1, nullptr, lp.a[2], nullptr, 0)));
+  RET((lp_conv<32, 16>(ctx, lp.tm_a[2], lp.wf[3], b[3], 0, nullptr, nullptr, lp.y, 5)));
   return 0;
 }
 
@@ -857,13 +912,13 @@ int lp_backward(desalm_ctx* ctx, double* loss) {
   CKL();
   // layer 4 (a[2] -> y)
   RET((lp_wgrad<32, 16>(ctx, lp.a[2], lp.dy4, lp.dW[3])));
-  RET((lp_conv<16, 32>(ctx, lp.dy4, lp.wd[3], nullptr, 0, lp.a[2], lp.dya[0], nullptr, 0)));
+  RET((lp_conv<16, 32>(ctx, lp.tm_dy4, lp.wd[3], nullptr, 0, lp.a[2], lp.dya[0], nullptr, 0)));
   // layer 3 (a[1] -> a[2])
   RET((lp_wgrad<32, 32>(ctx, lp.a[1], lp.dya[0], lp.dW[2])));
-  RET((lp_conv<32, 32>(ctx, lp.dya[0], lp.wd[2], nullptr, 0, lp.a[1], lp.dya[1], nullptr, 0)));
+  RET((lp_conv<32, 32>(ctx, lp.tm_dya[0], lp.wd[2], nullptr, 0, lp.a[1], lp.dya[1], nullptr, 0)));
   // layer 2 (a[0] -> a[1])
   RET((lp_wgrad<32, 32>(ctx, lp.a[0], lp.dya[1], lp.dW[1])));
-  RET((lp_conv<32, 32>(ctx, lp.dya[1], lp.wd[1], nullptr, 0, lp.a[0], lp.dya[0], nullptr, 0)));
+  RET((lp_conv<32, 32>(ctx, lp.tm_dya[1], lp.wd[1], nullptr, 0, lp.a[0], lp.dya[0], nullptr, 0)));
   // layer 1 (x0 -> a[0])
   RET((lp_wgrad<16, 32>(ctx, lp.x0, lp.dya[0], lp.dW[0])));
   const float gscale = float(2.0 / (5.0 * double(N)));
@@ -876,6 +931,7 @@ int lp_backward(desalm_ctx* ctx, double* loss) {
   double sum = 0;
   CK(cudaMemcpyAsync(&sum, lp.acc, sizeof(double), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
+  RET(lp_check(ctx));
   if (loss) *loss = sum / (5.0 * double(N));
   return 0;
 }
@@ -1875,6 +1931,7 @@ int desalm_lp_eval(desalm_ctx* ctx, const float* x, const float* t, float* y, do
     if (grad) CK(cudaMemcpyAsync(grad, lp.grad, lp.nparam * sizeof(float), cudaMemcpyDeviceToHost, s));
   }
   CK(cudaStreamSynchronize(s));
+  RET(lp_check(ctx));
   return 0;
 }
 

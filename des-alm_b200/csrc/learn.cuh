@@ -16,15 +16,15 @@
 // channels, 32 or 64 bytes a row).  The halo rows stay zero, so the 27
 // neighbours of an interior row are the rows at fixed offsets with no bounds
 // checks, and the shifted operand of a stencil offset is a contiguous run of
-// rows.  Products accumulate in FP32 on the tensor cores (WMMA m16n16k16
-// BF16).  A convolution is an implicit GEMM over tiles of LP_TM consecutive
-// padded rows: for each of the 9 (dj, dk) pairs the CTA copies a window of
-// LP_TM + 2 rows into shared memory (16-byte cp.async, double-buffered) and
-// multiplies the window shifted by di = -1, 0, 1 rows by those offsets'
-// weight blocks.  The data gradient of a layer is the same kernel with the
-// weights transposed and the stencil flipped; the weight gradient reduces over
-// the rows with per-CTA partial sums and one reduction kernel.  Master
-// weights, Adam moments and the loss are FP32 / FP64.
+// rows.  Products accumulate in FP32 on the tensor cores.  The convolution
+// (forward, and the data gradient with the weights transposed and the stencil
+// flipped) is the tcgen05 kernel of learn_tc.cuh.  The weight gradient here
+// is an implicit GEMM on WMMA m16n16k16 BF16 that reduces over the rows: for
+// each of the 9 (dj, dk) pairs the CTA copies a window of LP_TM + 2 rows into
+// shared memory (16-byte cp.async, double-buffered) and multiplies the window
+// shifted by di = -1, 0, 1 rows with the output gradient, with per-CTA
+// partial sums and one reduction kernel.  Master weights, Adam moments and
+// the loss are FP32 / FP64.
 #pragma once
 #include <mma.h>
 #include <cuda_bf16.h>
@@ -105,117 +105,6 @@ DESALM_DEV void lp_load_window(const LpPad& P, const bf16* __restrict__ src, lon
     const bool ok = row >= 0 && row < P.np;
     lp_cp16(dst + r * S + 8 * c, src + (ok ? row : 0) * C + 8 * c, ok);
   }
-}
-
-// Shared-memory layout of k_lp_conv (bytes).
-template <int CIN, int COUT>
-struct LpConvSmem {
-  static constexpr int SA = LpStride<CIN>::v;
-  static constexpr size_t w = size_t(27) * CIN * COUT * sizeof(bf16);
-  static constexpr size_t win = size_t(LP_WROWS) * SA * sizeof(bf16);
-  static constexpr size_t c = size_t(LP_TM) * (COUT + 4) * sizeof(float);
-  static constexpr size_t total = w + 2 * win + c;
-};
-
-// out[p][co] = act(bias[co] + sum_{ci, o} W[o][ci][co] in[p + off(o)][ci]) for
-// every interior row p (halo rows of out are not written).  act: ReLU when
-// relu != 0; when mask is given the result is multiplied by (mask[p][co] > 0)
-// (the gradient through the ReLU that produced mask).  out, when given, gets
-// the COUT channels in BF16; out32, when given, the first cout32 channels in
-// FP32 as [channel][node] in the level's node order.  Grid-stride over tiles;
-// the weights stay in shared memory for the CTA's lifetime.
-template <int CIN, int COUT>
-__global__ void __launch_bounds__(256) k_lp_conv(LpPad P, const bf16* __restrict__ in, const bf16* __restrict__ wk,
-                                                 const float* __restrict__ bias, int relu,
-                                                 const bf16* __restrict__ mask, bf16* __restrict__ out,
-                                                 float* __restrict__ out32, int cout32) {
-  pdl_wait();
-  using namespace nvcuda;
-  using SM = LpConvSmem<CIN, COUT>;
-  constexpr int SA = SM::SA, NF = COUT / 16, KC = CIN / 16, LDC = COUT + 4;
-  extern __shared__ __align__(128) unsigned char lp_smem[];
-  bf16* Ws = reinterpret_cast<bf16*>(lp_smem);
-  bf16* Win = reinterpret_cast<bf16*>(lp_smem + SM::w);
-  float* Cs = reinterpret_cast<float*>(lp_smem + SM::w + 2 * SM::win);
-  constexpr int WIN = int(SM::win / sizeof(bf16));
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const long ntiles = (P.p1 - P.p0 + LP_TM - 1) / LP_TM;
-  for (int e = tid; e < 27 * CIN * COUT / 8; e += 256) lp_cp16(Ws + 8 * e, wk + 8 * e, true);
-  lp_cp_commit();
-  long tile = blockIdx.x;
-  if (tile < ntiles) lp_load_window<CIN>(P, in, P.p0 + tile * LP_TM, 0, Win, tid, 256);
-  lp_cp_commit();
-  int buf = 0;
-  for (; tile < ntiles; tile += gridDim.x) {
-    wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc[NF];
-#pragma unroll
-    for (int f = 0; f < NF; ++f) wmma::fill_fragment(acc[f], 0.0f);
-    for (int g = 0; g < 9; ++g) {
-      // prefetch the next window (this tile's next pair, or the next tile's first)
-      const long nt = g < 8 ? tile : tile + gridDim.x;
-      if (nt < ntiles) lp_load_window<CIN>(P, in, P.p0 + nt * LP_TM, g < 8 ? g + 1 : 0, Win + (buf ^ 1) * WIN, tid, 256);
-      lp_cp_commit();
-      lp_cp_wait<1>();
-      __syncthreads();
-      const bf16* A0 = Win + buf * WIN + warp * 16 * SA;
-#pragma unroll
-      for (int di = 0; di < 3; ++di) {
-        const int o = 3 * g + di;
-#pragma unroll
-        for (int kc = 0; kc < KC; ++kc) {
-          wmma::fragment<wmma::matrix_a, 16, 16, 16, bf16, wmma::row_major> a;
-          wmma::load_matrix_sync(a, A0 + di * SA + kc * 16, SA);
-#pragma unroll
-          for (int f = 0; f < NF; ++f) {
-            wmma::fragment<wmma::matrix_b, 16, 16, 16, bf16, wmma::row_major> b;
-            wmma::load_matrix_sync(b, Ws + (o * CIN + kc * 16) * COUT + f * 16, COUT);
-            wmma::mma_sync(acc[f], a, b, acc[f]);
-          }
-        }
-      }
-      __syncthreads();  // the window is read before it is refilled
-      buf ^= 1;
-    }
-#pragma unroll
-    for (int f = 0; f < NF; ++f)
-      wmma::store_matrix_sync(Cs + warp * 16 * LDC + f * 16, acc[f], LDC, wmma::mem_row_major);
-    __syncthreads();
-    const long t0 = P.p0 + tile * LP_TM;
-    for (int e = tid; e < LP_TM * (COUT / 8); e += 256) {
-      const int r = e / (COUT / 8), c8 = e - r * (COUT / 8);
-      const long p = t0 + r;
-      if (p >= P.p1) continue;
-      const long l = lp_node(P, p);
-      if (l < 0) continue;
-      float v[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        v[q] = Cs[r * LDC + 8 * c8 + q] + (bias ? bias[8 * c8 + q] : 0.0f);
-        if (relu) v[q] = fmaxf(v[q], 0.0f);
-      }
-      if (mask) {
-        const uint4 mv = *reinterpret_cast<const uint4*>(mask + p * COUT + 8 * c8);
-        const bf16* mb = reinterpret_cast<const bf16*>(&mv);
-#pragma unroll
-        for (int q = 0; q < 8; ++q)
-          if (!(__bfloat162float(mb[q]) > 0.0f)) v[q] = 0.0f;
-      }
-      if (out) {
-        uint4 ov;
-        bf16* ob = reinterpret_cast<bf16*>(&ov);
-#pragma unroll
-        for (int q = 0; q < 8; ++q) ob[q] = __float2bfloat16(v[q]);
-        *reinterpret_cast<uint4*>(out + p * COUT + 8 * c8) = ov;
-      }
-      if (out32) {
-#pragma unroll
-        for (int q = 0; q < 8; ++q)
-          if (8 * c8 + q < cout32) out32[(long)(8 * c8 + q) * P.N + l] = v[q];
-      }
-    }
-    // Cs is written again only after the next tile's window barriers
-  }
-  lp_cp_wait<0>();
 }
 
 // Shared-memory layout of k_lp_wgrad (bytes): two windows of X, two tiles of D.
@@ -536,25 +425,6 @@ struct LpLayer {
   int cin_pad, cout_pad;
   long woff, boff;      // offsets of W and b in the flat vector
 };
-
-// Forward and data-gradient weight blocks from the master weights:
-// wf[o][ci][co] = W[co][ci][o], wd[o][co][ci] = W[co][ci][26 - o] (zero in
-// the padded channels).
-__global__ void k_lp_pack(LpLayer ly, const float* __restrict__ theta, bf16* __restrict__ wf, bf16* __restrict__ wd) {
-  pdl_wait();
-  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long total = 27L * ly.cin_pad * ly.cout_pad;
-  if (e >= total) return;
-  // e indexes wf[o][ci][co]
-  const int co = int(e % ly.cout_pad);
-  const int ci = int((e / ly.cout_pad) % ly.cin_pad);
-  const int o = int(e / ((long)ly.cout_pad * ly.cin_pad));
-  float w = 0.0f;
-  if (ci < ly.cin && co < ly.cout) w = theta[ly.woff + ((long)co * ly.cin + ci) * 27 + o];
-  wf[e] = __float2bfloat16(w);
-  // wd[26 - o][co][ci] takes the same weight
-  wd[((long)(26 - o) * ly.cout_pad + co) * ly.cin_pad + ci] = __float2bfloat16(w);
-}
 
 // Gradient of the flat parameter vector from dW[o][ci][co] and db[co] of one
 // layer, times gscale.
