@@ -713,7 +713,7 @@ int sa_conservation(desalm_ctx* ctx);
 
 
 // ----------------------------------------------------------- learned guess
-constexpr int kLpWgradGrid = 148 * 2;  // partial slots of k_lp_wgrad (its largest grid)
+constexpr int kLpWgradGrid = 148;  // partial slots of k_lp_wgrad_tc (one CTA per SM)
 
 // cuTensorMapEncodeTiled, reached through the runtime's driver entry point
 typedef CUresult (*LpEncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -774,17 +774,17 @@ int lp_check(desalm_ctx* ctx) {
   return 0;
 }
 
-// Weight and bias gradient of one layer into dW ([27][CIN][COUT] then [COUT]).
+// Weight and bias gradient of one layer into dW ([27][CIN][COUT] then [COUT])
+// on the tensor cores: per-CTA partials (k_lp_wgrad_tc, one CTA per SM),
+// then their sum.  xmap describes X, dmap D.
 template <int CIN, int COUT>
-int lp_wgrad(desalm_ctx* ctx, const bf16* X, const bf16* D, float* dW) {
+int lp_wgrad(desalm_ctx* ctx, const CUtensorMap& xmap, const CUtensorMap& dmap, float* dW) {
   LpState& lp = ctx->lp;
-  constexpr int NT = 32 * 3 * (CIN / 16) * (COUT / 16);
   constexpr long SLOT = 27L * CIN * COUT + COUT;
-  // one CTA of 12 warps per SM (168 registers a thread), or two of 6
-  constexpr int grid = NT > 192 ? 148 : 2 * 148;
+  constexpr int grid = 148;
   static_assert(grid <= kLpWgradGrid, "partial slots");
-  LAUNCH(KC_LEARN, 0, (double)lp.N, launch_k(k_lp_wgrad<CIN, COUT>, grid, NT, LpWgradSmem<CIN, COUT>::total,
-                                             ctx->stream, lp.P, X, D, lp.part));
+  LAUNCH(KC_LEARN, 0, (double)lp.N, launch_k(k_lp_wgrad_tc<CIN, COUT>, grid, LP_TC_THREADS, LpWgTc<CIN, COUT>::total,
+                                             ctx->stream, xmap, dmap, lp.P, lp.part, lp.err));
   LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_reduce, cdiv(SLOT, 256), 256, 0, ctx->stream, grid, SLOT,
                                     (const float*)lp.part, dW));
   CKL();
@@ -800,9 +800,9 @@ cudaError_t lp_attrs() {
   cudaError_t e = lp_optin(k_lp_conv_tc<16, 32>, LpTcSmem<16, 32>::total);
   if (e == cudaSuccess) e = lp_optin(k_lp_conv_tc<32, 32>, LpTcSmem<32, 32>::total);
   if (e == cudaSuccess) e = lp_optin(k_lp_conv_tc<32, 16>, LpTcSmem<32, 16>::total);
-  if (e == cudaSuccess) e = lp_optin(k_lp_wgrad<16, 32>, LpWgradSmem<16, 32>::total);
-  if (e == cudaSuccess) e = lp_optin(k_lp_wgrad<32, 32>, LpWgradSmem<32, 32>::total);
-  if (e == cudaSuccess) e = lp_optin(k_lp_wgrad<32, 16>, LpWgradSmem<32, 16>::total);
+  if (e == cudaSuccess) e = lp_optin(k_lp_wgrad_tc<16, 32>, LpWgTc<16, 32>::total);
+  if (e == cudaSuccess) e = lp_optin(k_lp_wgrad_tc<32, 32>, LpWgTc<32, 32>::total);
+  if (e == cudaSuccess) e = lp_optin(k_lp_wgrad_tc<32, 16>, LpWgTc<32, 16>::total);
   return e;
 }
 
@@ -911,16 +911,16 @@ int lp_backward(desalm_ctx* ctx, double* loss) {
   LAUNCH(KC_LEARN, 0, (double)N, launch_k(k_lp_loss, 296, 256, 0, s, lp.P, (const float*)lp.y, (const float*)lp.t, lp.dy4, lp.acc));
   CKL();
   // layer 4 (a[2] -> y)
-  RET((lp_wgrad<32, 16>(ctx, lp.a[2], lp.dy4, lp.dW[3])));
+  RET((lp_wgrad<32, 16>(ctx, lp.tm_a[2], lp.tm_dy4, lp.dW[3])));
   RET((lp_conv<16, 32>(ctx, lp.tm_dy4, lp.wd[3], nullptr, 0, lp.a[2], lp.dya[0], nullptr, 0)));
   // layer 3 (a[1] -> a[2])
-  RET((lp_wgrad<32, 32>(ctx, lp.a[1], lp.dya[0], lp.dW[2])));
+  RET((lp_wgrad<32, 32>(ctx, lp.tm_a[1], lp.tm_dya[0], lp.dW[2])));
   RET((lp_conv<32, 32>(ctx, lp.tm_dya[0], lp.wd[2], nullptr, 0, lp.a[1], lp.dya[1], nullptr, 0)));
   // layer 2 (a[0] -> a[1])
-  RET((lp_wgrad<32, 32>(ctx, lp.a[0], lp.dya[1], lp.dW[1])));
+  RET((lp_wgrad<32, 32>(ctx, lp.tm_a[0], lp.tm_dya[1], lp.dW[1])));
   RET((lp_conv<32, 32>(ctx, lp.tm_dya[1], lp.wd[1], nullptr, 0, lp.a[0], lp.dya[0], nullptr, 0)));
   // layer 1 (x0 -> a[0])
-  RET((lp_wgrad<16, 32>(ctx, lp.x0, lp.dya[0], lp.dW[0])));
+  RET((lp_wgrad<16, 32>(ctx, lp.tm_x0, lp.tm_dya[0], lp.dW[0])));
   const float gscale = float(2.0 / (5.0 * double(N)));
   for (int l = 0; l < 4; ++l) {
     const long n = (long)lp.ly[l].cout * lp.ly[l].cin * 27 + lp.ly[l].cout;

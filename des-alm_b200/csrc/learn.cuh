@@ -16,17 +16,13 @@
 // channels, 32 or 64 bytes a row).  The halo rows stay zero, so the 27
 // neighbours of an interior row are the rows at fixed offsets with no bounds
 // checks, and the shifted operand of a stencil offset is a contiguous run of
-// rows.  Products accumulate in FP32 on the tensor cores.  The convolution
-// (forward, and the data gradient with the weights transposed and the stencil
-// flipped) is the tcgen05 kernel of learn_tc.cuh.  The weight gradient here
-// is an implicit GEMM on WMMA m16n16k16 BF16 that reduces over the rows: for
-// each of the 9 (dj, dk) pairs the CTA copies a window of LP_TM + 2 rows into
-// shared memory (16-byte cp.async, double-buffered) and multiplies the window
-// shifted by di = -1, 0, 1 rows with the output gradient, with per-CTA
-// partial sums and one reduction kernel.  Master weights, Adam moments and
-// the loss are FP32 / FP64.
+// rows.  The convolution (forward, and the data gradient with the weights
+// transposed and the stencil flipped) and the weight gradient are the tcgen05
+// kernels of learn_tc.cuh, BF16 products accumulated in FP32 in tensor
+// memory; this file holds the layout, the element-wise kernels (features,
+// scales, targets, loss, guess), the per-CTA partial reduction, the gradient
+// gather and Adam.  Master weights, Adam moments and the loss are FP32 / FP64.
 #pragma once
-#include <mma.h>
 #include <cuda_bf16.h>
 #include "common.cuh"
 
@@ -71,143 +67,6 @@ DESALM_DEV long lp_node(const LpPad& P, long p) {
   const long jj = r % P.jp, kk = r / P.jp;
   if (ii < 1 || ii > P.im || jj < 1 || jj > P.jm || kk < 1 || kk > P.km) return -1;
   return (ii - 1) + (long)P.im * ((jj - 1) + (long)P.jm * (kk - 1));
-}
-
-DESALM_DEV void lp_cp16(void* smem, const void* gmem, bool ok) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
-  const int n = ok ? 16 : 0;  // 0: fill the 16 bytes with zeros
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(gmem), "r"(n) : "memory");
-}
-DESALM_DEV void lp_cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-DESALM_DEV void lp_cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-
-// Row stride (elements) of a channel-last tile in shared memory: a multiple
-// of 32 bytes, so that a window shifted by one row is still a legal WMMA
-// operand address.
-template <int C>
-struct LpStride {
-  static constexpr int v = C == 16 ? 16 : 48;
-};
-
-// Copy the window of (dj, dk) pair g for the tile starting at padded row
-// t0: rows t0 + off(0, dj, dk) - 1 .. + LP_WROWS; rows outside the padded
-// grid (only past the end of the last tile) read as zero.
-template <int C>
-DESALM_DEV void lp_load_window(const LpPad& P, const bf16* __restrict__ src, long t0, int g, bf16* dst, int tid,
-                               int nthreads) {
-  constexpr int S = LpStride<C>::v, CH = C / 8;
-  const int dj = g % 3 - 1, dk = g / 3 - 1;
-  const long base = t0 + (long)P.ip * (dj + (long)P.jp * dk) - 1;
-  for (int e = tid; e < LP_WROWS * CH; e += nthreads) {
-    const int r = e / CH, c = e - r * CH;
-    const long row = base + r;
-    const bool ok = row >= 0 && row < P.np;
-    lp_cp16(dst + r * S + 8 * c, src + (ok ? row : 0) * C + 8 * c, ok);
-  }
-}
-
-// Shared-memory layout of k_lp_wgrad (bytes): two windows of X, two tiles of D.
-template <int CIN, int COUT>
-struct LpWgradSmem {
-  static constexpr int SA = LpStride<CIN>::v, SD = LpStride<COUT>::v;
-  static constexpr size_t win = size_t(LP_WROWS) * SA * sizeof(bf16);
-  static constexpr size_t d = size_t(LP_TM) * SD * sizeof(bf16);
-  static constexpr size_t total = 2 * win + 2 * d;
-};
-
-// Partial weight and bias gradients of one layer over a contiguous range of
-// tiles per CTA:
-//   part[cta][o][ci][co] = sum_p X[p + off(o)][ci] D[p][co],
-//   part[cta][27 CIN COUT + co] = sum_p D[p][co],
-// p over the tiles' rows (D is zero on halo rows and past the last interior
-// row).  3 * (CIN/16) * (COUT/16) warps; warp w owns the output fragment
-// (di, ci block, co block) of every (dj, dk) pair, so each window feeds every
-// warp once.
-template <int CIN, int COUT>
-__global__ void __launch_bounds__(32 * 3 * (CIN / 16) * (COUT / 16))
-    k_lp_wgrad(LpPad P, const bf16* __restrict__ X, const bf16* __restrict__ D, float* __restrict__ part) {
-  pdl_wait();
-  using namespace nvcuda;
-  using SM = LpWgradSmem<CIN, COUT>;
-  constexpr int MF = CIN / 16, NF = COUT / 16, NW = 3 * MF * NF, NT = 32 * NW;
-  constexpr int SA = SM::SA, SD = SM::SD;
-  constexpr int WIN = int(SM::win / sizeof(bf16)), DT = int(SM::d / sizeof(bf16));
-  constexpr long SLOT = 27L * CIN * COUT + COUT;
-  extern __shared__ __align__(128) unsigned char lp_smem[];
-  bf16* Win = reinterpret_cast<bf16*>(lp_smem);
-  bf16* Dt = reinterpret_cast<bf16*>(lp_smem + 2 * SM::win);
-  __shared__ float bsum[NT];
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const int di = warp % 3, mi = (warp / 3) % MF, ni = warp / (3 * MF);
-  const long ntiles = (P.p1 - P.p0 + LP_TM - 1) / LP_TM;
-  const long per = (ntiles + gridDim.x - 1) / gridDim.x;
-  const long ta = blockIdx.x * per, tb = min(ntiles, ta + per);
-  auto load_d = [&](long tile, int b) {
-    const long t0 = P.p0 + tile * LP_TM;
-    for (int e = tid; e < LP_TM * (COUT / 8); e += NT) {
-      const int r = e / (COUT / 8), c = e - r * (COUT / 8);
-      const long row = t0 + r;
-      const bool ok = row < P.p1;
-      lp_cp16(Dt + b * DT + r * SD + 8 * c, D + (ok ? row : 0) * COUT + 8 * c, ok);
-    }
-  };
-  wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc[9];
-#pragma unroll
-  for (int g = 0; g < 9; ++g) wmma::fill_fragment(acc[g], 0.0f);
-  float bs = 0.0f;  // bias partial of channel tid % COUT
-  int buf = 0;
-  if (ta < tb) {
-    lp_load_window<CIN>(P, X, P.p0 + ta * LP_TM, 0, Win, tid, NT);
-    load_d(ta, 0);
-  }
-  lp_cp_commit();
-  for (long tile = ta; tile < tb; ++tile) {
-    const int db = int((tile - ta) & 1);
-#pragma unroll
-    for (int g = 0; g < 9; ++g) {
-      if (g < 8) {
-        lp_load_window<CIN>(P, X, P.p0 + tile * LP_TM, g + 1, Win + (buf ^ 1) * WIN, tid, NT);
-      } else if (tile + 1 < tb) {
-        lp_load_window<CIN>(P, X, P.p0 + (tile + 1) * LP_TM, 0, Win + (buf ^ 1) * WIN, tid, NT);
-        load_d(tile + 1, db ^ 1);
-      }
-      lp_cp_commit();
-      lp_cp_wait<1>();
-      __syncthreads();
-      const bf16* A0 = Win + buf * WIN + di * SA + mi * 16;
-      const bf16* B0 = Dt + db * DT + ni * 16;
-#pragma unroll
-      for (int ks = 0; ks < LP_TM / 16; ++ks) {
-        wmma::fragment<wmma::matrix_a, 16, 16, 16, bf16, wmma::col_major> a;  // (ci, row)
-        wmma::fragment<wmma::matrix_b, 16, 16, 16, bf16, wmma::row_major> b;  // (row, co)
-        wmma::load_matrix_sync(a, A0 + ks * 16 * SA, SA);
-        wmma::load_matrix_sync(b, B0 + ks * 16 * SD, SD);
-        wmma::mma_sync(acc[g], a, b, acc[g]);
-      }
-      if (g == 0) {
-        // bias partial: thread tid sums rows tid / COUT, + NT / COUT, ... of channel tid % COUT
-        const bf16* Db = Dt + db * DT;
-        for (int r = tid / COUT; r < LP_TM; r += NT / COUT) bs += __bfloat162float(Db[r * SD + tid % COUT]);
-      }
-      __syncthreads();  // the window (and, after the last pair, the D tile) is read before it is refilled
-      buf ^= 1;
-    }
-  }
-  lp_cp_wait<0>();
-  float* slot = part + blockIdx.x * SLOT;
-#pragma unroll
-  for (int g = 0; g < 9; ++g) {
-    const int o = 3 * g + di;
-    wmma::store_matrix_sync(slot + ((long)o * CIN + mi * 16) * COUT + ni * 16, acc[g], COUT, wmma::mem_row_major);
-  }
-  bsum[tid] = bs;
-  __syncthreads();
-  if (tid < COUT) {
-    float t = 0.0f;
-    for (int r = tid; r < NT; r += COUT) t += bsum[r];
-    slot[27L * CIN * COUT + tid] = t;
-  }
 }
 
 // out[e] = sum over nslot slots of part[slot * len + e]

@@ -362,4 +362,228 @@ __global__ void __launch_bounds__(LP_TC_THREADS) k_lp_conv_tc(const __grid_const
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Weight and bias gradients of one layer on the tensor cores:
+//   part[cta][o][ci][co] = sum_p X[p + off(o)][ci] D[p][co],
+//   part[cta][27 CIN COUT + co] = sum_p D[p][co],
+// p over a contiguous range of tiles per CTA (D is zero on halo rows; rows
+// past the last interior row read as zero).  The contraction runs over rows,
+// so both operands are MN-major: A = X windows, M = (window, channel); B = D,
+// N = the output channels.  G = 128 / CIN windows of consecutive (dj, dk)
+// pairs sit in consecutive buffers one window apart, so (window, 8-channel
+// chunk) is a uniform core-matrix stride of one slab and one M = 128 MMA
+// covers G offsets of the same di.  Groups of G windows: 3 (CIN 32) or 2
+// (CIN 16) per tile, the last one partly used.  Each (group, di) owns an
+// accumulator of COUT columns in tensor memory for the CTA's whole tile
+// range; one CTA per SM.  Warp 0 (one lane) issues the copies and MMAs; warps
+// 1-4 sum the bias gradient from each staged D tile and, at the end, move the
+// accumulators to the partial slot.
+// ---------------------------------------------------------------------------
+template <int CIN, int COUT>
+struct LpWgTc {
+  static constexpr int G = 128 / CIN;                  // windows per group
+  static constexpr int NG = (9 + G - 1) / G;           // groups per tile
+  static constexpr int NACC = NG * 3;                  // accumulators
+  static constexpr int COLS = NACC * COUT <= 256 ? 256 : 512;
+  static constexpr int KCH = CIN / 8, DCH = COUT / 8;
+  static constexpr size_t win = size_t(KCH) * LP_TC_SLAB;
+  static constexpr size_t grp = G * win;               // one group buffer
+  static constexpr size_t dt = size_t(DCH) * LP_TC_SLAB;
+  static constexpr int NGS = 4;                        // group stages
+  static constexpr size_t bars = 8 * (2 * NGS + 6);    // gfull, gempty, dfull x2, dempty x2, done, drain
+  static constexpr size_t total = NGS * grp + 2 * dt + bars + 16 + 4 * 128 * COUT;
+  static_assert(NACC * COUT <= 512, "accumulators fit tensor memory");
+  static_assert(grp % 128 == 0 && dt % 128 == 0, "TMA destinations stay 128-byte aligned");
+};
+
+// MN-major instruction descriptor: FP32 accumulator, BF16 A and B, M = 128.
+DESALM_HD constexpr unsigned lp_idesc_mn(int n) { return lp_idesc(n) | (1u << 15) | (1u << 16); }
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(LP_TC_THREADS, 1)
+    k_lp_wgrad_tc(const __grid_constant__ CUtensorMap xmap, const __grid_constant__ CUtensorMap dmap, LpPad P,
+                  float* __restrict__ part, int* err) {
+  pdl_wait();
+  using C = LpWgTc<CIN, COUT>;
+  constexpr int G = C::G, NG = C::NG, KCH = C::KCH, DCH = C::DCH, NGS = C::NGS;
+  constexpr unsigned IDESC = lp_idesc_mn(COUT);
+  constexpr unsigned COLS = C::COLS;
+  constexpr long SLOT = 27L * CIN * COUT + COUT;
+  extern __shared__ __align__(128) unsigned char lp_wg_smem[];
+  unsigned char* Gb = lp_wg_smem;                      // NGS group buffers
+  unsigned char* Db = lp_wg_smem + NGS * C::grp;       // two D tiles
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(lp_wg_smem + NGS * C::grp + 2 * C::dt);
+  unsigned* tmem_slot = reinterpret_cast<unsigned*>(lp_wg_smem + NGS * C::grp + 2 * C::dt + C::bars);
+  float* bred = reinterpret_cast<float*>(lp_wg_smem + NGS * C::grp + 2 * C::dt + C::bars + 16);  // [128][COUT]
+  const unsigned gfull = lp_smem_u32(bars), gempty = gfull + 8 * NGS, dfull = gempty + 8 * NGS, dempty = dfull + 16;
+  const unsigned done = dempty + 16, dbar = done + 8;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long ntiles = (P.p1 - P.p0 + LP_TM - 1) / LP_TM;
+  const long per = (ntiles + gridDim.x - 1) / gridDim.x;
+  const long ta = blockIdx.x * per, tb = min(ntiles, ta + per);
+  const long my = tb > ta ? tb - ta : 0;
+  const long S = my * NG;  // (tile, group) steps
+
+  if (tid == 0) {
+    for (int b = 0; b < NGS; ++b) {
+      lp_bar_init(gfull + 8 * b, 1);
+      lp_bar_init(gempty + 8 * b, 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      lp_bar_init(dfull + 8 * b, 1);
+      lp_bar_init(dempty + 8 * b, 1 + 4);  // the last group's MMAs and the four bias warps
+    }
+    lp_bar_init(done, 1);
+    lp_bar_init(dbar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(lp_smem_u32(tmem_slot)),
+                 "r"(COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  lp_tc_fence_before();
+  __syncthreads();
+  lp_tc_fence_after();
+  const unsigned tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0 && S > 0) {
+      auto t0_of = [&](long tl) { return P.p0 + (ta + tl) * LP_TM; };
+      // copies of step (tile tl, group gr) into group buffer gr's stage; the
+      // D tile with the first group
+      auto issue = [&](long step) {
+        const long tl = step / NG;
+        const int gr = int(step % NG);
+        const int b = int(step % NGS);
+        const int nw = min(G, 9 - G * gr);
+        const long t0 = t0_of(tl);
+        const unsigned dst = lp_smem_u32(Gb + b * C::grp);
+        lp_bar_expect_tx(gfull + 8 * b, nw * KCH * LP_WROWS * 16);
+        for (int w = 0; w < nw; ++w) {
+          const int g = G * gr + w;
+          const int dj = g % 3 - 1, dk = g / 3 - 1;
+          const int y = int(t0 + (long)P.ip * (dj + (long)P.jp * dk) - 1);
+          for (int c = 0; c < KCH; ++c) lp_tma_2d(dst + w * C::win + c * LP_TC_SLAB, &xmap, 8 * c, y, gfull + 8 * b);
+        }
+      };
+      auto issue_d = [&](long tl) {
+        const int b = int(tl & 1);
+        const unsigned dst = lp_smem_u32(Db + b * C::dt);
+        lp_bar_expect_tx(dfull + 8 * b, DCH * LP_WROWS * 16);
+        for (int c = 0; c < DCH; ++c) lp_tma_2d(dst + c * LP_TC_SLAB, &dmap, 8 * c, int(t0_of(tl)), dfull + 8 * b);
+      };
+      long issued = 0, dissued = 0;
+      issue_d(0);
+      dissued = 1;
+      for (; issued < NGS && issued < S; ++issued) issue(issued);
+      bool ok = true;
+      long step = 0;
+      for (; step < S; ++step) {
+        const long tl = step / NG;
+        const int gr = int(step % NG);
+        const int b = int(step % NGS), db = int(tl & 1);
+        if (gr == 0) {
+          // the next D tile goes into the other buffer once the tile before has released it
+          if (tl + 1 < my) {
+            if (tl >= 1 && !lp_bar_wait(dempty + 8 * (db ^ 1), unsigned(((tl - 1) >> 1) & 1), err)) { ok = false; break; }
+            issue_d(tl + 1);
+            ++dissued;
+          }
+          if (!lp_bar_wait(dfull + 8 * db, unsigned((tl >> 1) & 1), err)) { ok = false; break; }
+        }
+        if (!lp_bar_wait(gfull + 8 * b, unsigned((step / NGS) & 1), err)) { ok = false; break; }
+        lp_tc_fence_after();
+        const unsigned abase = lp_smem_u32(Gb + b * C::grp), bbase = lp_smem_u32(Db + db * C::dt);
+#pragma unroll
+        for (int di = 0; di < 3; ++di) {
+#pragma unroll
+          for (int ks = 0; ks < LP_TM / 16; ++ks) {
+            const unsigned long long a = lp_desc(abase + 16 * di + 256 * ks, 128, LP_TC_SLAB);
+            const unsigned long long bd = lp_desc(bbase + 256 * ks, 128, LP_TC_SLAB);
+            lp_mma(tmem + (gr * 3 + di) * COUT, a, bd, IDESC, (tl | ks) != 0);
+          }
+        }
+        lp_commit(gempty + 8 * b);
+        if (gr == NG - 1) lp_commit(dempty + 8 * db);
+        // refill the previous step's group buffer once its MMAs are done
+        if (step >= 1 && step - 1 + NGS < S) {
+          const long ps = step - 1;
+          if (!lp_bar_wait(gempty + 8 * int(ps % NGS), unsigned((ps / NGS) & 1), err)) { ++step; ok = false; break; }
+          issue(ps + NGS);
+          ++issued;
+        }
+      }
+      lp_commit(done);
+      if (!ok) {
+        // drain: the MMAs issued so far, and the copies started but not consumed
+        lp_commit(dbar);
+        lp_bar_wait(dbar, 0, err, true);
+        for (long w = step; w < issued; ++w) lp_bar_wait(gfull + 8 * int(w % NGS), unsigned((w / NGS) & 1), err, true);
+        for (long t = (step + NG - 1) / NG; t < dissued; ++t)
+          lp_bar_wait(dfull + 8 * int(t & 1), unsigned((t >> 1) & 1), err, true);
+      }
+    }
+  } else {
+    // ---- bias warps: row 32 (w % 4) + lane of every D tile
+    const int q = warp & 3, row = 32 * q + lane;
+    float bs[COUT];
+#pragma unroll
+    for (int c = 0; c < COUT; ++c) bs[c] = 0.0f;
+    bool ok = true;
+    for (long tl = 0; tl < my; ++tl) {
+      const int db = int(tl & 1);
+      if (!lp_bar_wait(dfull + 8 * db, unsigned((tl >> 1) & 1), err)) { ok = false; break; }
+      const unsigned char* D0 = Db + db * C::dt + row * 16;
+#pragma unroll
+      for (int c = 0; c < DCH; ++c) {
+        const uint4 v = *reinterpret_cast<const uint4*>(D0 + c * LP_TC_SLAB);
+        const bf16* e = reinterpret_cast<const bf16*>(&v);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) bs[8 * c + j] += __bfloat162float(e[j]);
+      }
+      __syncwarp();
+      if (lane == 0) lp_bar_arrive(dempty + 8 * db);
+    }
+#pragma unroll
+    for (int c = 0; c < COUT; ++c) bred[row * COUT + c] = bs[c];
+    // ---- accumulators -> partial slot (after every MMA)
+    if (ok && my > 0 && lp_bar_wait(done, 0, err)) {
+      lp_tc_fence_after();
+      float* slot = part + blockIdx.x * SLOT;
+      for (int gr = 0; gr < NG; ++gr)
+        for (int di = 0; di < 3; ++di) {
+          float v[COUT];
+          lp_tmem_ld<COUT>(tmem + (unsigned(32 * q) << 16) + (gr * 3 + di) * COUT, v);
+          const int gi = row / CIN, ci = row % CIN, g = G * gr + gi;
+          if (g < 9) {
+            const int o = 3 * g + di;
+            float4* dst = reinterpret_cast<float4*>(slot + ((long)o * CIN + ci) * COUT);
+#pragma unroll
+            for (int c = 0; c < COUT / 4; ++c) dst[c] = make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+          }
+        }
+      lp_tc_fence_before();
+    } else if (my == 0) {
+      float* slot = part + blockIdx.x * SLOT;
+      for (long e = row; e < 27L * CIN * COUT; e += 128) slot[e] = 0.0f;
+    }
+  }
+  __syncthreads();
+  if (tid >= 32 && tid < 32 + COUT) {
+    const int c = tid - 32;
+    float t = 0.0f;
+    for (int r = 0; r < 128; ++r) t += bred[r * COUT + c];
+    part[blockIdx.x * SLOT + 27L * CIN * COUT + c] = t;
+  }
+  lp_tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    lp_tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(COLS) : "memory");
+  }
+}
+
 }  // namespace desalm
