@@ -360,6 +360,9 @@ void rs_factors(int n, double e, std::vector<double>& fac, std::vector<double>& 
 dim3 blk3() { return dim3(32, 4, 1); }
 template <class T, class W>
 dim3 grid_interior(const Lv<T, W>& L) { return dim3(cdiv(L.im - 2, 32), cdiv(L.jm - 2, 4), L.km - 2); }
+// the residual kernels' CTA shape (DESALM_KR_BY j rows x DESALM_KR_BZ k planes)
+dim3 blk_r() { return dim3(32, DESALM_KR_BY, DESALM_KR_BZ); }
+dim3 grid_r(int im, int jm, int km) { return dim3(cdiv(im - 2, 32), cdiv(jm - 2, DESALM_KR_BY), cdiv(km - 2, DESALM_KR_BZ)); }
 
 // One DAF line sweep as k_sweep4 with the widest slab (lines per CTA) whose
 // shared memory leaves room for two CTAs per SM, else the widest that fits
@@ -460,7 +463,7 @@ int launch_daf(desalm_ctx* ctx, Lv<T, W>& L, Level& G, int n, int recalc, int it
   const int upwind = fine ? 2 : 1;
   const int bback = fine && c.btype[0] != 5;
   const double nin = double(L.im - 2) * (L.jm - 2) * (L.km - 2);
-  LAUNCH(KC_RESID, n, nin, launch_k(k_resid<T, W, 0>, grid_interior(L), blk3(), 0, s, L, P, upwind, itr == 1 ? 1 : 0, n > 0 ? 1 : 0, bback));
+  LAUNCH(KC_RESID, n, nin, launch_k(k_resid<T, W, 0>, grid_r(L.im, L.jm, L.km), blk_r(), 0, s, L, P, upwind, itr == 1 ? 1 : 0, n > 0 ? 1 : 0, bback));
   CKL();
   RET((launch_sweep<T, W, 0>(ctx, L, P, n, bback, 0)));
   RET((launch_sweep<T, W, 1>(ctx, L, P, n, fine && c.btype[2] != 5, fine && c.btype[3] != 5)));
@@ -472,7 +475,7 @@ template <class T, class W>
 int launch_recalc(desalm_ctx* ctx, Lv<T, W>& L, int n) {
   Par P = ctx->par;
   P.fine = (n == 0);
-  LAUNCH(KC_RECALC, n, double(L.im - 2) * (L.jm - 2) * (L.km - 2), launch_k(k_resid<T, W, 1>, grid_interior(L), blk3(), 0, ctx->stream, L, P, n == 0 ? 2 : 1, 0, n > 0 ? 1 : 0, 0));
+  LAUNCH(KC_RECALC, n, double(L.im - 2) * (L.jm - 2) * (L.km - 2), launch_k(k_resid<T, W, 1>, grid_r(L.im, L.jm, L.km), blk_r(), 0, ctx->stream, L, P, n == 0 ? 2 : 1, 0, n > 0 ? 1 : 0, 0));
   CKL();
   return 0;
 }
@@ -1687,7 +1690,7 @@ int sa_run(desalm_ctx* ctx, Lv<double, W>& L) {
   LAUNCH(KC_SA_AUX, 0, nin, launch_k(k_sa_source<W>, gi, blk3(), 0, s, S));
   LAUNCH(KC_SA_AUX, 0, L.N, launch_k(k_sa_ucn<W>, cdiv(L.N, 256), 256, 0, s, S));
   for (int it = 0; it < ctx->c.itk; ++it) {
-    LAUNCH(KC_SA_RHS, 0, nin, launch_k(k_sa_rhs<W>, gi, blk3(), 0, s, S));
+    LAUNCH(KC_SA_RHS, 0, nin, launch_k(k_sa_rhs<W>, grid_r(L.im, L.jm, L.km), blk_r(), 0, s, S));
     RET((sa_sweep<W, 0>(ctx, S, L.jm - 2, L.im - 2, L.km - 2, nin)));
     RET((sa_sweep<W, 1>(ctx, S, L.im - 2, L.jm - 2, L.km - 2, nin)));
     RET((sa_sweep<W, 2>(ctx, S, L.im - 2, L.km - 2, L.jm - 2, nin)));
@@ -1959,6 +1962,89 @@ int desalm_lp_get_buffer(desalm_ctx* ctx, int which, float* out) {
     default: ctx->err = "lp_get_buffer: unknown buffer"; return DESALM_EINVAL;
   }
   CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------ checkpoint / restart
+extern "C" {
+
+// The reference's restart file from the device state (output_restart,
+// src/main.F90:315-393): q(1..me), nu_t when turbulent, qn(1..me), FP32.
+int desalm_checkpoint_write(desalm_ctx* ctx, const char* path) {
+  if (!ctx || !path) return DESALM_EINVAL;
+  if (!ctx->have_state) { ctx->err = "no state to write"; return DESALM_ENOTREADY; }
+  const desalm_case& c = ctx->c;
+  const size_t N = size_t(c.im) * c.jm * c.km;
+  std::vector<double> q(5 * N), qn(5 * N), nut(N);
+  RET(desalm_get_state(ctx, q.data(), qn.data(), nullptr, nut.data()));
+  const int r = desalm_solu_write(path, c.im, c.jm, c.km, c.turbulence, q.data(), qn.data(), nut.data());
+  if (r) ctx->err = desalm_io_error();
+  return r;
+}
+
+// The device state from a restart file (init_solu, src/init.F90:2324-2475).
+// q^{n-1} is not in the file: the reference starts it at zero
+// (src/init.F90:1089) and the first step's history shift refills it.
+int desalm_checkpoint_read(desalm_ctx* ctx, const char* path) {
+  if (!ctx || !path) return DESALM_EINVAL;
+  const desalm_case& c = ctx->c;
+  const size_t N = size_t(c.im) * c.jm * c.km;
+  std::vector<double> q(5 * N), qn(5 * N), nut(N, 0.0);
+  const int r = desalm_solu_read(path, c.im, c.jm, c.km, c.turbulence, q.data(), qn.data(), nut.data());
+  if (r) {
+    ctx->err = desalm_io_error();
+    return r;
+  }
+  return desalm_set_state(ctx, q.data(), qn.data(), nullptr, nut.data());
+}
+
+// The learned guess's training state: parameters, Adam moments and counters.
+// Layout (little-endian): "DESALMLP", int32 version 1, int64 nparam, int64
+// adam steps, int64 samples, then nparam FP32 each of theta, m, v.
+int desalm_lp_checkpoint_write(desalm_ctx* ctx, const char* path) {
+  if (!ctx || !path) return DESALM_EINVAL;
+  LpState& lp = ctx->lp;
+  if (!lp.on) { ctx->err = "the learned guess is off"; return DESALM_EINVAL; }
+  const size_t n = size_t(lp.nparam);
+  std::vector<float> buf(3 * n);
+  CK(cudaMemcpyAsync(buf.data(), lp.theta, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(buf.data() + n, lp.m, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(buf.data() + 2 * n, lp.v, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  FILE* f = fopen(path, "wb");
+  if (!f) { ctx->err = std::string("cannot open ") + path; return DESALM_EIO; }
+  const int32_t ver = 1;
+  const int64_t hdr[3] = {int64_t(n), int64_t(lp.adam_t), int64_t(lp.samples)};
+  bool ok = fwrite("DESALMLP", 1, 8, f) == 8 && fwrite(&ver, 4, 1, f) == 1 && fwrite(hdr, 8, 3, f) == 3 &&
+            fwrite(buf.data(), 4, 3 * n, f) == 3 * n;
+  ok = (fclose(f) == 0) && ok;
+  if (!ok) { ctx->err = std::string("write to ") + path + " failed"; return DESALM_EIO; }
+  return 0;
+}
+
+int desalm_lp_checkpoint_read(desalm_ctx* ctx, const char* path) {
+  if (!ctx || !path) return DESALM_EINVAL;
+  LpState& lp = ctx->lp;
+  if (!lp.on) { ctx->err = "the learned guess is off"; return DESALM_EINVAL; }
+  FILE* f = fopen(path, "rb");
+  if (!f) { ctx->err = std::string("cannot open ") + path; return DESALM_EIO; }
+  char magic[8];
+  int32_t ver = 0;
+  int64_t hdr[3] = {0, 0, 0};
+  const size_t n = size_t(lp.nparam);
+  std::vector<float> buf(3 * n);
+  bool ok = fread(magic, 1, 8, f) == 8 && memcmp(magic, "DESALMLP", 8) == 0 && fread(&ver, 4, 1, f) == 1 && ver == 1 &&
+            fread(hdr, 8, 3, f) == 3 && hdr[0] == int64_t(n) && fread(buf.data(), 4, 3 * n, f) == 3 * n;
+  fclose(f);
+  if (!ok) { ctx->err = std::string(path) + ": not a learned-guess checkpoint of this network"; return DESALM_EIO; }
+  CK(cudaMemcpyAsync(lp.theta, buf.data(), n * 4, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(lp.m, buf.data() + n, n * 4, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(lp.v, buf.data() + 2 * n, n * 4, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  lp.adam_t = long(hdr[1]);
+  lp.samples = long(hdr[2]);
   return 0;
 }
 

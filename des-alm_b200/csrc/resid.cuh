@@ -105,6 +105,12 @@ DESALM_DEV T diss_fv(const Lv<T, W>& L, int dir, int l, int st, T dsq) {
 #ifndef DESALM_KR_MINBLOCKS
 #define DESALM_KR_MINBLOCKS 3
 #endif
+// CTA shape of K_R and of the SA residual (i extent 32; j x k = 4), another
+// build-time knob: j rows and k planes per CTA.
+#ifndef DESALM_KR_BY
+#define DESALM_KR_BY 4
+#endif
+#define DESALM_KR_BZ (4 / DESALM_KR_BY)
 
 // MODE 0: first pass of a DAF step; MODE 1: recalculation for restriction.
 template <class T, class W, int MODE>
@@ -112,8 +118,8 @@ __global__ void __launch_bounds__(128, DESALM_KR_MINBLOCKS) k_resid(Lv<T, W> L, 
   pdl_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int k = blockIdx.z + 1;
-  if (i > L.im - 2 || j > L.jm - 2) return;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+  if (i > L.im - 2 || j > L.jm - 2 || k > L.km - 2) return;
   const int sj = L.sj, sk = L.sk;
   const int l = i + sj * j + sk * k;
   const T rei = T(1) / T(P.ren);

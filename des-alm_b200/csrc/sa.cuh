@@ -181,8 +181,8 @@ __global__ void __launch_bounds__(128) k_sa_rhs(SaT<SW> S) {
   pdl_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int k = blockIdx.z + 1;
-  if (i > S.im - 2 || j > S.jm - 2) return;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+  if (i > S.im - 2 || j > S.jm - 2 || k > S.km - 2) return;
   const int sj = S.sj, sk = S.sk;
   const int l = i + sj * j + sk * k;
   const double cb1 = 0.1355, cb2 = 0.622, rsig = 1.5, capa = 0.41;  // rsig = 1 / sigma_SA

@@ -14,6 +14,7 @@ DESALM_ENONFINITE = -4
 DESALM_ESINGULAR = -5
 DESALM_ETIMEOUT = -6
 DESALM_ENOTREADY = -7
+DESALM_EIO = -8
 
 FP64 = 0
 MIXED = 1

@@ -81,6 +81,24 @@ def lib():
             f = getattr(L, "desalm_" + name)
             f.argtypes = args
             f.restype = C.c_int
+        cp = C.c_char_p
+        for name, args in [
+            ("grid_read", [cp, ip, ip, ip, ip, dp, dp, dp, dp]),
+            ("grid_write", [cp, ip, ip, ip, ip, dp, dp, dp, dp]),
+            ("solu_read", [cp, ip, ip, ip, ip, dp, dp, dp]),
+            ("solu_write", [cp, ip, ip, ip, ip, dp, dp, dp]),
+            ("filestat_read", [cp, dp, C.POINTER(C.c_int), dp, ip]),
+            ("filestat_write", [cp, C.c_double, ip, dp, ip]),
+            ("checkpoint_read", [vp, cp]),
+            ("checkpoint_write", [vp, cp]),
+            ("lp_checkpoint_read", [vp, cp]),
+            ("lp_checkpoint_write", [vp, cp]),
+        ]:
+            f = getattr(L, "desalm_" + name)
+            f.argtypes = args
+            f.restype = C.c_int
+        L.desalm_io_error.argtypes = []
+        L.desalm_io_error.restype = C.c_char_p
         L.desalm_stream.argtypes = [vp]
         L.desalm_stream.restype = C.c_void_p
         L.desalm_kernel_class_count.argtypes = []
@@ -109,6 +127,55 @@ def _f32p(a):
 
 def _f32(a):
     return None if a is None else np.ascontiguousarray(a, dtype=np.float32)
+
+
+# ---------------------------------------------------------------- file formats
+def _io(rc, what):
+    if rc:
+        raise DesalmError("%s failed (%d): %s" % (what, rc, lib().desalm_io_error().decode()))
+
+
+def _b(path):
+    return os.fsencode(path)
+
+
+def grid_read(path, im, jm, km, turbulence):
+    """The reference's grid file -> dict(x, y, z, wd) of (im*jm*km,) doubles."""
+    N = im * jm * km
+    x, y, z, wd = (np.zeros(N) for _ in range(4))
+    _io(lib().desalm_grid_read(_b(path), im, jm, km, int(turbulence), _p(x), _p(y), _p(z), _p(wd)), "grid_read")
+    return dict(x=x, y=y, z=z, wd=wd if turbulence else None)
+
+
+def grid_write(path, im, jm, km, turbulence, x, y, z, wd=None):
+    x, y, z, wd = map(_f64, (x, y, z, wd))
+    _io(lib().desalm_grid_write(_b(path), im, jm, km, int(turbulence), _p(x), _p(y), _p(z), _p(wd)), "grid_write")
+
+
+def solu_read(path, im, jm, km, turbulence):
+    """The reference's restart file -> dict(q, qn, nut) in the ABI layouts."""
+    N = im * jm * km
+    q, qn, nut = np.zeros(5 * N), np.zeros(5 * N), np.zeros(N)
+    _io(lib().desalm_solu_read(_b(path), im, jm, km, int(turbulence), _p(q), _p(qn), _p(nut)), "solu_read")
+    return dict(q=q, qn=qn, nut=nut)
+
+
+def solu_write(path, im, jm, km, turbulence, q, qn, nut=None):
+    q, qn, nut = map(_f64, (q, qn, nut))
+    _io(lib().desalm_solu_write(_b(path), im, jm, km, int(turbulence), _p(q), _p(qn), _p(nut)), "solu_write")
+
+
+def filestat_read(path, n_tur):
+    t, n = C.c_double(0.0), C.c_int(0)
+    ang = np.zeros(max(1, n_tur))
+    _io(lib().desalm_filestat_read(_b(path), C.byref(t), C.byref(n), _p(ang), n_tur), "filestat_read")
+    return t.value, n.value, ang[:n_tur]
+
+
+def filestat_write(path, time, ntime, angles=()):
+    a = _f64(np.asarray(angles, dtype=np.float64).reshape(-1))
+    _io(lib().desalm_filestat_write(_b(path), float(time), int(ntime), _p(a) if a.size else None, a.size),
+        "filestat_write")
 
 
 class Solver:
@@ -230,6 +297,19 @@ class Solver:
                 if la[t]:
                     out.setdefault(name, {})[lvl + 1] = (float(ms[t]), int(la[t]), float(nodes[t]))
         return out, int(tot.value)
+
+    # ------------------------------------------------ checkpoint / restart
+    def checkpoint_write(self, path):
+        self._ck(self.L.desalm_checkpoint_write(self.ctx, _b(path)), "checkpoint_write")
+
+    def checkpoint_read(self, path):
+        self._ck(self.L.desalm_checkpoint_read(self.ctx, _b(path)), "checkpoint_read")
+
+    def lp_checkpoint_write(self, path):
+        self._ck(self.L.desalm_lp_checkpoint_write(self.ctx, _b(path)), "lp_checkpoint_write")
+
+    def lp_checkpoint_read(self, path):
+        self._ck(self.L.desalm_lp_checkpoint_read(self.ctx, _b(path)), "lp_checkpoint_read")
 
     # ------------------------------------------------ learned initial guess
     def lp_config(self, train_steps=-1, warm=-1, lr=-1.0, ymax=-1.0):

@@ -36,6 +36,8 @@ extern "C" {
 #define DESALM_ESINGULAR  -5   /* zero pivot in a line solve                    */
 #define DESALM_ETIMEOUT   -6   /* bounded device wait gave up                   */
 #define DESALM_ENOTREADY  -7   /* grid or state not bound yet                   */
+#define DESALM_EIO        -8   /* file missing, unreadable, or not in the
+                                  expected record layout                        */
 
 /* precision_mode */
 #define DESALM_FP64   0        /* everything in FP64                            */
@@ -277,6 +279,56 @@ int  desalm_lp_set_params(desalm_ctx* ctx, const float* theta);
 int  desalm_lp_eval(desalm_ctx* ctx, const float* x, const float* t, float* y,
                     double* loss, float* grad);
 int  desalm_lp_get_buffer(desalm_ctx* ctx, int which, float* out);
+
+/* ---------------------------------------------------------------------
+ * On-disk formats of the reference, for drivers that run real cases and
+ * checkpoint from the device.  Grid and solution files are Fortran
+ * unformatted sequential files (each record: 4-byte little-endian byte count,
+ * payload, the count again) of FP32 values, i fastest, one block.  Host arrays
+ * use this header's layouts: q and qn as (1:5, i, j, k) with the component
+ * fastest, x, y, z, wd and nu_t as (i, j, k).  me = 4 for a laminar case, 5
+ * with Spalart-Allmaras (q(5) = nu_tilde).  These functions make no CUDA call;
+ * on failure they return DESALM_EIO (or DESALM_EINVAL) and
+ * desalm_io_error() describes it.
+ * --------------------------------------------------------------------- */
+const char* desalm_io_error(void);
+
+/* 'grid' (src/init.F90:2226-2243): records x, y, z and, when turbulent, the
+ * wall distance wd. */
+int  desalm_grid_read(const char* path, int im, int jm, int km, int turbulence,
+                      double* x, double* y, double* z, double* wd);
+int  desalm_grid_write(const char* path, int im, int jm, int km, int turbulence,
+                       const double* x, const double* y, const double* z,
+                       const double* wd);
+
+/* Restart file.  Write (output_restart, src/main.F90:315-393): one record each
+ * of q(1..me), then nu_t when turbulent, then qn(1..me).  Read (init_solu,
+ * src/init.F90:2324-2475): the same records; for a laminar case the reference
+ * reads q(1..me) as one record of me*N values and then qn likewise, and both
+ * laminar layouts are accepted here.  Components past me read as zero; nut may
+ * be NULL. */
+int  desalm_solu_write(const char* path, int im, int jm, int km, int turbulence,
+                       const double* q, const double* qn, const double* nut);
+int  desalm_solu_read(const char* path, int im, int jm, int km, int turbulence,
+                      double* q, double* qn, double* nut);
+
+/* 'filestat' (src/main.F90:374-381 writes, src/init.F90:268-276 reads):
+ * list-directed text, time and step, then one turbine angle a line; reading
+ * brings an angle >= 2 pi back by 2 pi, as the reference does. */
+int  desalm_filestat_write(const char* path, double time, int ntime,
+                           const double* angle, int n_tur);
+int  desalm_filestat_read(const char* path, double* time, int* ntime,
+                          double* angle, int n_tur);
+
+/* The context's device state to / from a restart file (layouts above).
+ * After a read, q^{n-1} is zero, as after the reference's restart
+ * (src/init.F90:1089); the next physical step's history shift refills it. */
+int  desalm_checkpoint_write(desalm_ctx* ctx, const char* path);
+int  desalm_checkpoint_read(desalm_ctx* ctx, const char* path);
+/* The learned guess's parameters, Adam moments and counters (a format of
+ * this library; the reference has no network). */
+int  desalm_lp_checkpoint_write(desalm_ctx* ctx, const char* path);
+int  desalm_lp_checkpoint_read(desalm_ctx* ctx, const char* path);
 
 #ifdef __cplusplus
 }
