@@ -14,7 +14,8 @@ ours:       value = device-timed seconds per physical step of the product
             plain FP64 path (q^n guess, as the reference) is timed too, and
             predictor_ab compares the three initial guesses (q^n, linear
             extrapolation, the learned network) by iterations and seconds per
-            physical step to an absolute tolerance on the laminar cavity.
+            physical step to an absolute tolerance on the laminar cavity, and
+            alm gives the cost of the actuator-line forcing.
 reference:  the CPU oracle (C++ restatement of the reference, FP32 like the
             reference's own build, its loops on every host thread) on the same
             case; a bounded sample of pseudo-iterations scaled to one physical
@@ -193,6 +194,36 @@ def run_ours(args, rank, world, dist):
             del S
         return res
 
+    def alm_cost(steps=2):
+        """Actuator-line forcing (rhs_lines) on the SA channel 129x97x65 (MIXED,
+        graph path) with three seeded synthetic rotors: seconds per physical step
+        with and without the forcing, and the forcing kernels' time per
+        pseudo-iteration from one profiled (eager) step."""
+        case, grid, state, spec = cases.channel_alm(im=129, jm=97, km=65, n_tur=3, itmax=400)
+        case.precision_mode = abi.MIXED
+        case.predictor = abi.PRED_LINEAR
+        case.use_graph = 1
+        res = {"workload": "SA channel 129x97x65, MIXED, 3 synthetic rotors (3 blades x 12 elements, %d kernel nodes)"
+                           % sum(len(T["ker_index"]) for T in spec["turbines"])}
+        for name, on in (("without", False), ("with", True)):
+            S = Solver(case)
+            S.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
+            S.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
+            if on:
+                S.alm_set(spec)
+            S.mg_driver()
+            sec, reps = timed_steps(S, steps, S.mg_driver)
+            res["s_per_step_" + name] = sec
+            if on:
+                S.profile(True)
+                r = S.mg_driver()
+                stats, _ = S.kernel_stats()
+                S.profile(False)
+                ms = sum(v[0] for v in stats.get("alm", {}).values())
+                res["alm_kernel_ms_per_iteration"] = ms / max(1, r["iterations"])
+            del S
+        return res
+
     def timed_steps(S, K, body):
         """K calls of body(), bracketed by barrier + synchronize, CUDA events
         on the library's stream; returns seconds per call (max over ranks)."""
@@ -309,6 +340,7 @@ def run_ours(args, rank, world, dist):
                  for m, nm in enumerate(names)}
 
     ab = predictor_ab() if not args.no_ab else None
+    alm = alm_cost() if not args.no_ab else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -335,6 +367,7 @@ def run_ours(args, rank, world, dist):
                                         "initial state, both with the q^n guess" % (args.warmup + args.steps)},
         "cell_updates_per_s": sum_over_ranks(cell_updates),
         "predictor_ab": ab,
+        "alm": alm,
         "e2e": {"value": e2e_sec, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "kernel": kind, "level": "fine", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -434,7 +467,7 @@ def main():
     ap.add_argument("--case", default="channel", choices=["cavity", "channel"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--no-ab", action="store_true", help="skip the initial-guess comparison")
+    ap.add_argument("--no-ab", action="store_true", help="skip the initial-guess and forcing sections")
     ap.add_argument("--ncu-workload", action="store_true",
                     help="run one eager pseudo-iteration of --case for an ncu capture and exit")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])

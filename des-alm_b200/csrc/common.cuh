@@ -39,6 +39,7 @@ struct Lv {
   const T* zet[3];
   const T* aj;
   const T* rj;      // 1/aj, formed once whenever aj is set
+  const T* falm;    // actuator-line force added to rh(2:4), [3][N], or null
   // DAF work: transformed residual and row coefficients
   W* wk[4];
   W* sig;          // sigma = sqrt(beta alpha) of each interior node, from the first residual pass

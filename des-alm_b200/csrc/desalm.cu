@@ -24,6 +24,7 @@
 #include "sa.cuh"
 #include "learn.cuh"
 #include "learn_tc.cuh"
+#include "alm.cuh"
 
 using namespace desalm;
 
@@ -172,6 +173,13 @@ struct desalm_ctx {
   double* stage = nullptr;    // device staging of one host state array, 5 N (component-fastest)
   double** ftab = nullptr;    // device table of the fine level's q[5], qn[5], qnm1[5] field pointers
   LpState lp;                 // learned initial guess (predictor DESALM_PRED_LEARNED)
+  struct {
+    bool on = false;
+    AlmDev dev{};
+    std::vector<int> nker, elem0;     // per turbine
+    double* falm = nullptr;           // [3][N] force added to rh(2:4) on the fine level
+    std::vector<void*> allocs;        // this forcing's device tables
+  } alm;                      // actuator-line forcing (rhs_lines)
   int* flags = nullptr;       // device [2]
   SaWork sa{};
   // per-kernel CUDA-event timing (desalm_profile) and launch counter
@@ -223,7 +231,7 @@ inline unsigned cdiv(long a, long b) { return (unsigned)((a + b - 1) / b); }
 // kernel classes for desalm_kernel_stats
 enum KClass { KC_DTAU = 0, KC_RESID, KC_SWEEP_I, KC_SWEEP_J, KC_SWEEP_K, KC_RECALC, KC_BCOND, KC_PFIX,
               KC_NLEVEL, KC_PROLONG, KC_RSMOOTH, KC_NORM, KC_SA_RHS, KC_SA_SWEEP, KC_SA_BC,
-              KC_XFORM_I, KC_XFORM_J, KC_XFORM_K, KC_SA_AUX, KC_LEARN, KC_MISC, KC_COUNT };
+              KC_XFORM_I, KC_XFORM_J, KC_XFORM_K, KC_SA_AUX, KC_LEARN, KC_ALM, KC_MISC, KC_COUNT };
 
 struct ProfScope {
   desalm_ctx* ctx;
@@ -261,6 +269,7 @@ int alloc_level(desalm_ctx* ctx, Level& G, Lv<T, W>& L) {
   L.im = G.im; L.jm = G.jm; L.km = G.km;
   L.N = (int)N;
   L.sj = G.im; L.sk = G.im * G.jm;
+  L.falm = nullptr;
   L.dc = T(G.dc); L.de = T(G.de); L.dz = T(G.dz);
   auto A = [&](T** p) { return dalloc(ctx, G.allocs, (void**)p, N * sizeof(T)); };
   auto AW = [&](W** p) { return dalloc(ctx, G.allocs, (void**)p, N * sizeof(W)); };
@@ -448,6 +457,20 @@ int launch_sweep(desalm_ctx* ctx, Lv<T, W>& L, const Par& P, int lvl, int blo, i
   return DESALM_EINVAL;
 }
 
+// rhs_lines on the fine level (src/solver_daf.F90:378-381): element forces,
+// then each turbine's projection into alm.falm, which K_R's first pass adds.
+template <class T, class W>
+int alm_run(desalm_ctx* ctx, Lv<T, W>& L) {
+  auto& A = ctx->alm;
+  cudaStream_t s = ctx->stream;
+  CK(cudaMemsetAsync(A.falm, 0, 3L * L.N * sizeof(double), s));
+  LAUNCH(KC_ALM, 0, double(A.dev.E), launch_k(k_alm_forces<T, W>, 1, 256, 0, s, A.dev, L));
+  if (A.dev.nker_all > 0)
+    LAUNCH(KC_ALM, 0, double(A.dev.nker_all), launch_k(k_alm_project<T, W>, cdiv(A.dev.nker_all, 128), 128, 0, s, A.dev, L, A.falm));
+  CKL();
+  return 0;
+}
+
 template <class T, class W>
 int launch_daf(desalm_ctx* ctx, Lv<T, W>& L, Level& G, int n, int recalc, int itr) {
   Par P = ctx->par;
@@ -463,6 +486,7 @@ int launch_daf(desalm_ctx* ctx, Lv<T, W>& L, Level& G, int n, int recalc, int it
   const int upwind = fine ? 2 : 1;
   const int bback = fine && c.btype[0] != 5;
   const double nin = double(L.im - 2) * (L.jm - 2) * (L.km - 2);
+  if (n == 0 && ctx->alm.on) RET(alm_run(ctx, L));
   LAUNCH(KC_RESID, n, nin, launch_k(k_resid<T, W, 0>, grid_r(L.im, L.jm, L.km), blk_r(), 0, s, L, P, upwind, itr == 1 ? 1 : 0, n > 0 ? 1 : 0, bback));
   CKL();
   RET((launch_sweep<T, W, 0>(ctx, L, P, n, bback, 0)));
@@ -1063,6 +1087,7 @@ void desalm_destroy(desalm_ctx* ctx) {
   for (auto& G : ctx->L)
     for (void* p : G.allocs) cudaFree(p);
   for (void* p : ctx->allocs) cudaFree(p);
+  for (void* p : ctx->alm.allocs) cudaFree(p);
   for (auto& r : ctx->prof) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
   if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
   if (ctx->graph) cudaGraphDestroy(ctx->graph);
@@ -2045,6 +2070,186 @@ int desalm_lp_checkpoint_read(desalm_ctx* ctx, const char* path) {
   CK(cudaStreamSynchronize(ctx->stream));
   lp.adam_t = long(hdr[1]);
   lp.samples = long(hdr[2]);
+  return 0;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------ actuator-line forcing
+namespace {
+
+// Drop the captured physical step so that the next one is captured again
+// with the current kernels and parameters.
+void drop_graph(desalm_ctx* ctx) {
+  if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+  if (ctx->graph) cudaGraphDestroy(ctx->graph);
+  ctx->gexec = nullptr;
+  ctx->graph = nullptr;
+}
+
+template <class V>
+int alm_copy(desalm_ctx* ctx, const std::vector<V>& h, const V** out) {
+  void* p = nullptr;
+  const size_t bytes = std::max<size_t>(1, h.size()) * sizeof(V);
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) { ctx->err = std::string("cudaMalloc: ") + cudaGetErrorString(e); return DESALM_ENOMEM; }
+  ctx->alm.allocs.push_back(p);
+  if (!h.empty()) CK(cudaMemcpyAsync(p, h.data(), h.size() * sizeof(V), cudaMemcpyHostToDevice, ctx->stream));
+  *out = (const V*)p;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int desalm_alm_set(desalm_ctx* ctx, const desalm_alm* a) {
+  if (!ctx) return DESALM_EINVAL;
+  auto& A = ctx->alm;
+  auto bad = [&](const std::string& why) { ctx->err = "alm_set: " + why; return DESALM_EINVAL; };
+  const Level& F = ctx->L[0];
+  const int im = F.im, jm = F.jm, km = F.km;
+  if (a && a->n_tur > 0) {
+    if (!a->tur || a->npolar < 1 || !a->polar_offset || !a->polar_count || !a->polar_rows)
+      return bad("missing turbine or polar tables");
+    if (!(a->length_scale > 0.0) || !(a->vel_infty >= 0.0)) return bad("length_scale must be > 0");
+    for (int p = 0; p < a->npolar; ++p) {
+      const int o = a->polar_offset[p], n = a->polar_count[p];
+      if (o < 0 || n < 2) return bad("polar " + std::to_string(p) + " needs two rows or more");
+      if (a->polar_rows[3L * (o + n - 1)] != -999.0) return bad("polar " + std::to_string(p) + " must end with angle -999");
+    }
+    for (int t = 0; t < a->n_tur; ++t) {
+      const desalm_alm_turbine& T = a->tur[t];
+      if (T.nblades < 1 || T.nelems < 1 || T.nangles < 1 || T.nker < 0 || !(T.tur_rad > 0.0))
+        return bad("turbine " + std::to_string(t + 1) + ": bad sizes or radius");
+      if (!T.node_index || !T.node_pos || !T.disk_dat || !T.polar_b || !T.polar_a ||
+          (T.nker > 0 && (!T.ker_index || !T.ker_pos || !T.ker_dat)))
+        return bad("turbine " + std::to_string(t + 1) + ": missing table");
+      const long ne = long(T.nangles) * T.nelems;
+      for (long e = 0; e < ne; ++e) {
+        const int i = T.node_index[3 * e], j = T.node_index[3 * e + 1], k = T.node_index[3 * e + 2];
+        // cells whose lower corner is not interior are skipped on the device; any
+        // cell that is used must lie inside the grid
+        const bool inner = i >= 2 && i <= im - 1 && j >= 2 && j <= jm - 1 && k >= 2 && k <= km - 1;
+        if (!inner && (i < 1 || i > im || j < 1 || j > jm || k < 1 || k > km))
+          return bad("turbine " + std::to_string(t + 1) + ": element cell outside the grid");
+        if (inner) {
+          const long jk = long(j - 1) + long(jm) * (k - 1);
+          if (T.polar_b[jk] < 0 || T.polar_b[jk] >= a->npolar || T.polar_a[jk] < 0 || T.polar_a[jk] >= a->npolar)
+            return bad("turbine " + std::to_string(t + 1) + ": polar index out of range");
+        }
+      }
+      for (int n = 0; n < T.nker; ++n) {
+        const int* I = T.ker_index + 3 * n;
+        if (I[0] < 1 || I[0] > im || I[1] < 1 || I[1] > jm || I[2] < 1 || I[2] > km)
+          return bad("turbine " + std::to_string(t + 1) + ": kernel node outside the grid");
+      }
+    }
+  }
+  // the previous tables are released once the stream has finished with them
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (void* p : A.allocs) cudaFree(p);
+  A.allocs.clear();
+  A.on = false;
+  A.nker.clear();
+  A.elem0.clear();
+  drop_graph(ctx);
+  auto set_falm = [&](double* f) {
+    if (kind_of(ctx, 0) == K_DD) ctx->L[0].dd.falm = f;
+    else ctx->L[0].df.falm = f;
+  };
+  set_falm(nullptr);
+  if (!a || a->n_tur <= 0) return 0;
+
+  std::vector<int> tur_of, ker_tur, meta, node_index, polar_b, polar_a, ker_index, polar_off(a->polar_offset, a->polar_offset + a->npolar);
+  std::vector<double> par, angle, node_pos, disk_dat, ker_pos, ker_dat;
+  long nrows = 0;
+  for (int p = 0; p < a->npolar; ++p) nrows = std::max<long>(nrows, a->polar_offset[p] + a->polar_count[p]);
+  std::vector<double> polar_rows(a->polar_rows, a->polar_rows + 3 * nrows);
+  int E = 0;
+  long nodeoff = 0, keroff = 0;
+  const long JK = long(jm) * km;
+  for (int t = 0; t < a->n_tur; ++t) {
+    const desalm_alm_turbine& T = a->tur[t];
+    const int ne = T.nblades * T.nelems;
+    const int m[ALM_META] = {T.nblades, T.nelems, T.nangles, T.nker, E, int(nodeoff), int(t * JK), int(keroff)};
+    meta.insert(meta.end(), m, m + ALM_META);
+    par.push_back(T.tsr); par.push_back(T.tur_rad); par.push_back(T.hub_rad);
+    angle.push_back(T.angle);
+    for (int g = 0; g < ne; ++g) tur_of.push_back(t);
+    const long nn = long(T.nangles) * T.nelems;
+    node_index.insert(node_index.end(), T.node_index, T.node_index + 3 * nn);
+    node_pos.insert(node_pos.end(), T.node_pos, T.node_pos + 27 * nn);
+    disk_dat.insert(disk_dat.end(), T.disk_dat, T.disk_dat + 8 * JK);
+    polar_b.insert(polar_b.end(), T.polar_b, T.polar_b + JK);
+    polar_a.insert(polar_a.end(), T.polar_a, T.polar_a + JK);
+    for (int n = 0; n < T.nker; ++n) ker_tur.push_back(t);
+    if (T.nker > 0) {
+      ker_index.insert(ker_index.end(), T.ker_index, T.ker_index + 3L * T.nker);
+      ker_pos.insert(ker_pos.end(), T.ker_pos, T.ker_pos + 3L * T.nker);
+      ker_dat.insert(ker_dat.end(), T.ker_dat, T.ker_dat + 4L * T.nker);
+    }
+    A.nker.push_back(T.nker);
+    A.elem0.push_back(E);
+    E += ne;
+    nodeoff += nn;
+    keroff += T.nker;
+  }
+  AlmDev& D = A.dev;
+  D.n_tur = a->n_tur;
+  D.E = E;
+  D.im = im; D.jm = jm; D.km = km;
+  D.length_scale = a->length_scale;
+  D.vel_scale = ctx->c.ren * 10E-7 / a->length_scale;
+  D.vel_infty = a->vel_infty;
+  D.nker_all = int(keroff);
+  D.nrows = int(nrows);
+  RET(alm_copy(ctx, tur_of, &D.tur_of));
+  RET(alm_copy(ctx, ker_tur, &D.ker_tur));
+  RET(alm_copy(ctx, meta, &D.meta));
+  RET(alm_copy(ctx, par, &D.par));
+  RET(alm_copy(ctx, angle, &D.angle));
+  RET(alm_copy(ctx, node_index, &D.node_index));
+  RET(alm_copy(ctx, node_pos, &D.node_pos));
+  RET(alm_copy(ctx, disk_dat, &D.disk_dat));
+  RET(alm_copy(ctx, polar_b, &D.polar_b));
+  RET(alm_copy(ctx, polar_a, &D.polar_a));
+  RET(alm_copy(ctx, ker_index, &D.ker_index));
+  RET(alm_copy(ctx, ker_pos, &D.ker_pos));
+  RET(alm_copy(ctx, ker_dat, &D.ker_dat));
+  RET(alm_copy(ctx, polar_off, &D.polar_off));
+  RET(alm_copy(ctx, polar_rows, &D.polar_rows));
+  std::vector<double> zero_scr(size_t(E) * ALM_SCR, 0.0), zero_f(size_t(E) * 6, 0.0), zero_field(3 * size_t(F.N), 0.0);
+  const double* p = nullptr;
+  RET(alm_copy(ctx, zero_scr, &p)); D.scr = const_cast<double*>(p);
+  RET(alm_copy(ctx, zero_f, &p)); D.forces = const_cast<double*>(p);
+  RET(alm_copy(ctx, zero_field, &p)); A.falm = const_cast<double*>(p);
+  CK(cudaStreamSynchronize(ctx->stream));
+  set_falm(A.falm);
+  A.on = true;
+  return 0;
+}
+
+int desalm_alm_set_angle(desalm_ctx* ctx, int n_t, double angle) {
+  if (!ctx) return DESALM_EINVAL;
+  auto& A = ctx->alm;
+  if (!A.on || n_t < 1 || n_t > A.dev.n_tur) { ctx->err = "alm_set_angle: no such turbine"; return DESALM_EINVAL; }
+  CK(cudaMemcpyAsync(const_cast<double*>(A.dev.angle) + (n_t - 1), &angle, sizeof(double), cudaMemcpyHostToDevice,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+int desalm_alm_get(desalm_ctx* ctx, int what, double* out) {
+  if (!ctx || !out) return DESALM_EINVAL;
+  auto& A = ctx->alm;
+  if (!A.on) { ctx->err = "alm_get: the forcing is off"; return DESALM_EINVAL; }
+  if (what == DESALM_ALM_FORCES)
+    CK(cudaMemcpyAsync(out, A.dev.forces, 6 * size_t(A.dev.E) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  else if (what == DESALM_ALM_FIELD)
+    CK(cudaMemcpyAsync(out, A.falm, 3 * size_t(ctx->L[0].N) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  else { ctx->err = "alm_get: unknown item"; return DESALM_EINVAL; }
+  CK(cudaStreamSynchronize(ctx->stream));
   return 0;
 }
 

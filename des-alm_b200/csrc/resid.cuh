@@ -235,6 +235,13 @@ __global__ void __launch_bounds__(128, DESALM_KR_MINBLOCKS) k_resid(Lv<T, W> L, 
     }
   }
 
+  // actuator-line forcing, first pass only (src/solver_daf.F90:378-381)
+  if (MODE == 0 && L.falm) {
+    rh[1] = rh[1] + L.falm[l];
+    rh[2] = rh[2] + L.falm[L.N + l];
+    rh[3] = rh[3] + L.falm[2 * L.N + l];
+  }
+
   if (MODE == 1) {
 #pragma unroll
     for (int m = 0; m < 4; ++m) L.rh[m][l] = rh[m];

@@ -110,6 +110,69 @@ class LpReport(C.Structure):
         return d
 
 
+class AlmTurbine(C.Structure):
+    _fields_ = [
+        ("nblades", C.c_int), ("nelems", C.c_int), ("nangles", C.c_int),
+        ("tsr", C.c_double), ("tur_rad", C.c_double), ("hub_rad", C.c_double), ("angle", C.c_double),
+        ("node_index", C.POINTER(C.c_int)), ("node_pos", C.POINTER(C.c_double)),
+        ("disk_dat", C.POINTER(C.c_double)), ("polar_b", C.POINTER(C.c_int)), ("polar_a", C.POINTER(C.c_int)),
+        ("nker", C.c_int), ("ker_index", C.POINTER(C.c_int)), ("ker_pos", C.POINTER(C.c_double)),
+        ("ker_dat", C.POINTER(C.c_double)),
+    ]
+
+
+class Alm(C.Structure):
+    _fields_ = [
+        ("n_tur", C.c_int), ("tur", C.POINTER(AlmTurbine)),
+        ("vel_infty", C.c_double), ("length_scale", C.c_double),
+        ("npolar", C.c_int), ("polar_offset", C.POINTER(C.c_int)), ("polar_count", C.POINTER(C.c_int)),
+        ("polar_rows", C.POINTER(C.c_double)),
+    ]
+
+
+ALM_FORCES, ALM_FIELD = 0, 1
+
+
+def make_alm(spec):
+    """A desalm_alm structure from a dict (see cases.alm_rotor); returns the
+    structure and the arrays it points into, which must outlive the call."""
+    import numpy as np
+    keep = []
+
+    def arr(a, dt):
+        a = np.ascontiguousarray(np.asarray(a, dtype=dt).reshape(-1))
+        keep.append(a)
+        return a.ctypes.data_as(C.POINTER(C.c_int if dt == np.int32 else C.c_double))
+
+    tur = (AlmTurbine * len(spec["turbines"]))()
+    for t, T in enumerate(spec["turbines"]):
+        u = tur[t]
+        u.nblades, u.nelems, u.nangles = T["nblades"], T["nelems"], T["nangles"]
+        u.tsr, u.tur_rad, u.hub_rad, u.angle = T["tsr"], T["tur_rad"], T["hub_rad"], T["angle"]
+        u.node_index = arr(T["node_index"], np.int32)
+        u.node_pos = arr(T["node_pos"], np.float64)
+        u.disk_dat = arr(T["disk_dat"], np.float64)
+        u.polar_b = arr(T["polar_b"], np.int32)
+        u.polar_a = arr(T["polar_a"], np.int32)
+        u.nker = len(T["ker_index"])
+        u.ker_index = arr(T["ker_index"], np.int32)
+        u.ker_pos = arr(T["ker_pos"], np.float64)
+        u.ker_dat = arr(T["ker_dat"], np.float64)
+    keep.append(tur)
+    polars = spec["polars"]
+    counts = [len(p) for p in polars]
+    offs = list(np.cumsum([0] + counts[:-1]))
+    a = Alm()
+    a.n_tur = len(spec["turbines"])
+    a.tur = C.cast(tur, C.POINTER(AlmTurbine))
+    a.vel_infty, a.length_scale = spec["vel_infty"], spec["length_scale"]
+    a.npolar = len(polars)
+    a.polar_offset = arr(offs, np.int32)
+    a.polar_count = arr(counts, np.int32)
+    a.polar_rows = arr(np.concatenate([np.asarray(p, np.float64).reshape(-1) for p in polars]), np.float64)
+    return a, keep
+
+
 def level_dims(case, n):
     """Extents of level n (1-based): src/init.F90:257-263."""
     im, jm, km = case.im, case.jm, case.km

@@ -229,4 +229,96 @@ def ogrid(im=257, jm=129, km=65, seed=0, re=3900.0, rfar=20.0, itmax=400):
     return c, grid, state
 
 
+def alm_rotor(xs, ys, zs, center, radius, nblades=3, nelems=12, nangles=24, tsr=7.0, hub_frac=0.1,
+              length_scale=1.0, vel_infty=0.1, angle=0.3, seed=0, ker_cells=3):
+    """Seeded synthetic actuator-line tables for one rotor on a product grid
+    (coordinates xs[i], ys[j], zs[k]) with its plane normal to x, as the
+    reference's init_lines places it (src/init.F90:1446-1535): element elem
+    of azimuth bin nang sits at (xc, yc + r_e cos th, zc + r_e sin th) with
+    r_e = radius elem / nelems and th = nang 2 pi / nangles.  Lengths are grid
+    units except tur_rad and hub_rad (m = grid units x length_scale).  Three
+    polars: wide, medium and one so narrow ([-2, 2] degrees) that many
+    elements fall outside it.  Returns the turbine dict and the polars."""
+    rng = np.random.default_rng(seed)
+    im, jm, km = len(xs), len(ys), len(zs)
+    xc, yc, zc = center
+
+    def cell(v, a, n):  # 1-based lower-corner index of the cell holding v
+        return int(min(max(np.searchsorted(a, v, side="right"), 1), n - 1))
+
+    node_index, node_pos = [], []
+    dth = 2 * np.pi / nangles
+    for nang in range(1, nangles + 1):
+        th = nang * dth
+        for elem in range(1, nelems + 1):
+            x = xc
+            y = yc + (radius / nelems) * elem * np.cos(th)
+            z = zc + (radius / nelems) * elem * np.sin(th)
+            i, j, k = cell(x, xs, im), cell(y, ys, jm), cell(z, zs, km)
+            node_index.append((i, j, k))
+            c = []
+            for (a, b, d) in ((0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0), (0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1)):
+                c += [xs[i - 1 + a], ys[j - 1 + b], zs[k - 1 + d]]
+            node_pos.append([x, y, z] + c)
+    J, K = np.meshgrid(np.arange(jm), np.arange(km), indexing="xy")  # [k][j]
+    Y, Z = ys[J], zs[K]
+    r = np.sqrt((Y - yc) ** 2 + (Z - zc) ** 2)
+    dy = np.gradient(ys)[J]
+    dz = np.gradient(zs)[K]
+    dx = float(np.gradient(xs)[int(np.argmin(np.abs(xs - xc)))])
+    rr = np.clip(r / radius, 0.0, 1.5)
+    disk = np.zeros((km, jm, 8))
+    disk[..., 0] = r
+    disk[..., 1] = dy * dz
+    disk[..., 2] = np.arctan2(Z - zc, Y - yc)
+    disk[..., 3] = dx * dy * dz
+    disk[..., 4] = 0.02 * (1.0 - 0.5 * rr)
+    disk[..., 5] = 10.0 - 8.0 * rr + rng.normal(0.0, 0.5, size=r.shape)
+    disk[..., 6] = rng.uniform(0.0, 1.0, size=r.shape)
+    disk[..., 7] = 0.2
+    polars = []
+    for lo, hi, n in ((-30.0, 30.0, 25), (-12.0, 16.0, 15), (-2.0, 2.0, 5)):
+        a = np.linspace(lo, hi, n)
+        cl = 2 * np.pi * np.deg2rad(a) * (1.0 + 0.05 * rng.normal(size=n))
+        cd = 0.01 + 0.02 * (np.deg2rad(a)) ** 2 + 0.001 * rng.uniform(size=n)
+        polars.append(np.vstack([np.column_stack([a, cl, cd]), [[-999.0, 0.0, 0.0]]]))
+    pb = rng.integers(0, len(polars), size=(km, jm))
+    pa = rng.integers(0, len(polars), size=(km, jm))
+    h = max(dx, float(np.max(np.gradient(ys))), float(np.max(np.gradient(zs))))
+    gx, gy, gz = np.gradient(xs), np.gradient(ys), np.gradient(zs)
+    K3, J3, I3 = np.meshgrid(np.arange(2, km), np.arange(2, jm), np.arange(2, im), indexing="ij")
+    X3, Y3, Z3 = xs[I3 - 1], ys[J3 - 1], zs[K3 - 1]
+    R3 = np.hypot(Y3 - yc, Z3 - zc)
+    sel = (np.abs(X3 - xc) <= ker_cells * dx) & (R3 <= radius + ker_cells * h)  # k, j, i order
+    ker_index = np.column_stack([I3[sel], J3[sel], K3[sel]])
+    ker_pos = np.column_stack([X3[sel], Y3[sel], Z3[sel]])
+    ker_dat = np.column_stack([R3[sel], (gy[J3 - 1] * gz[K3 - 1])[sel], np.arctan2(Z3 - zc, Y3 - yc)[sel],
+                               (gx[I3 - 1] * gy[J3 - 1] * gz[K3 - 1])[sel]])
+    tur = dict(nblades=nblades, nelems=nelems, nangles=nangles, tsr=tsr,
+               tur_rad=radius * length_scale, hub_rad=hub_frac * radius * length_scale, angle=angle,
+               node_index=np.array(node_index, np.int32), node_pos=np.array(node_pos),
+               disk_dat=disk.reshape(-1, 8), polar_b=pb.reshape(-1).astype(np.int32),
+               polar_a=pa.reshape(-1).astype(np.int32),
+               ker_index=np.array(ker_index, np.int32).reshape(-1, 3), ker_pos=np.array(ker_pos).reshape(-1, 3),
+               ker_dat=np.array(ker_dat).reshape(-1, 4))
+    return tur, polars
+
+
+def channel_alm(im=33, jm=25, km=25, itmax=20, n_tur=1, seed=0):
+    """The SA channel with n_tur synthetic rotors (alm_rotor) along x; the
+    Reynolds number gives vel_scale = ren 1e-6 / length_scale."""
+    case, grid, state = channel(im=im, jm=jm, km=km, itmax=itmax, seed=seed)
+    xs = np.linspace(0.0, 2 * np.pi, im)
+    ys = _tanh_stretch(jm, 1.0 / 395.0)
+    zs = np.linspace(0.0, np.pi, km)
+    turs, polars = [], None
+    for t in range(n_tur):
+        xc = xs[int((t + 1) * im / (n_tur + 1))]
+        tur, pol = alm_rotor(xs, ys, zs, (xc, 1.0, np.pi / 2), 0.5, seed=seed + t, angle=0.3 + 1.1 * t)
+        turs.append(tur)
+        polars = pol if polars is None else polars
+    spec = dict(turbines=turs, polars=polars, vel_infty=0.1, length_scale=1.0)
+    return case, grid, state, spec
+
+
 PRESETS = {"cavity": cavity, "channel": channel, "ogrid": ogrid}

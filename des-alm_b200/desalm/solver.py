@@ -11,7 +11,7 @@ import subprocess
 
 import numpy as np
 
-from .abi import Case, LpReport, StepReport, level_dims
+from .abi import Alm, Case, LpReport, StepReport, level_dims, make_alm
 
 PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 # DESALM_LIBRARY selects another build of the same library (tuning variants)
@@ -93,6 +93,9 @@ def lib():
             ("checkpoint_write", [vp, cp]),
             ("lp_checkpoint_read", [vp, cp]),
             ("lp_checkpoint_write", [vp, cp]),
+            ("alm_set", [vp, C.POINTER(Alm)]),
+            ("alm_set_angle", [vp, ip, C.c_double]),
+            ("alm_get", [vp, ip, dp]),
         ]:
             f = getattr(L, "desalm_" + name)
             f.argtypes = args
@@ -110,7 +113,7 @@ def lib():
 # kernel classes reported by desalm_kernel_stats (order of the C enum)
 KERNEL_CLASSES = ["dtau", "resid", "sweep_i", "sweep_j", "sweep_k", "recalc", "bcond", "pfix",
                   "nlevel", "prolong", "rsmooth", "norm", "sa_rhs", "sa_sweep", "sa_bc",
-                  "xform_i", "xform_j", "xform_k", "sa_aux", "learn", "misc"]
+                  "xform_i", "xform_j", "xform_k", "sa_aux", "learn", "alm", "misc"]
 
 
 def _p(a):
@@ -297,6 +300,26 @@ class Solver:
                 if la[t]:
                     out.setdefault(name, {})[lvl + 1] = (float(ms[t]), int(la[t]), float(nodes[t]))
         return out, int(tot.value)
+
+    # ------------------------------------------------ actuator-line forcing
+    def alm_set(self, spec):
+        """Turn the actuator-line forcing on (spec: see cases.alm_rotor) or off (None)."""
+        if spec is None:
+            self._ck(self.L.desalm_alm_set(self.ctx, None), "alm_set")
+            self._alm_n = 0
+            return
+        a, keep = make_alm(spec)
+        self._ck(self.L.desalm_alm_set(self.ctx, C.byref(a)), "alm_set")
+        self._alm_n = sum(T["nblades"] * T["nelems"] for T in spec["turbines"])
+
+    def alm_set_angle(self, n_t, angle):
+        self._ck(self.L.desalm_alm_set_angle(self.ctx, int(n_t), float(angle)), "alm_set_angle")
+
+    def alm_get(self, what):
+        N = self.case.im * self.case.jm * self.case.km
+        out = np.zeros(6 * self._alm_n if what == 0 else 3 * N)
+        self._ck(self.L.desalm_alm_get(self.ctx, int(what), _p(out)), "alm_get")
+        return out.reshape(-1, 6) if what == 0 else out.reshape(3, N)
 
     # ------------------------------------------------ checkpoint / restart
     def checkpoint_write(self, path):

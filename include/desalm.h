@@ -281,6 +281,82 @@ int  desalm_lp_eval(desalm_ctx* ctx, const float* x, const float* t, float* y,
 int  desalm_lp_get_buffer(desalm_ctx* ctx, int which, float* out);
 
 /* ---------------------------------------------------------------------
+ * Actuator-line forcing (the reference's rhs_lines, src/rhs_lines.F90:47-483,
+ * called inside solver_daf on the fine level when turbines are on,
+ * src/solver_daf.F90:378-381).  The driver computes the geometry tables the
+ * reference's init_lines builds (src/init.F90:1156-1710) and passes them once;
+ * every fine-level DAF step then, on the GPU, interpolates the velocity at each
+ * blade element, looks up lift and drag in the airfoil polars, forms the
+ * element forces and projects them with a Gaussian kernel onto the kernel
+ * nodes, adding them to rh(2:4) before the modal transforms.  The
+ * recalculated residual (src/solver_daf.F90:432-463) does not call rhs_lines
+ * and gets no forcing.  Indices are 1-based global (i, j, k) as in the
+ * reference; arrays are copied at desalm_alm_set.  As in the reference, a
+ * polar lookup that finds no interval keeps the previous element's values,
+ * and elements or kernel nodes whose cell is not interior are skipped.
+ * Differences: the forcing acts on the fine level only (the reference also
+ * calls rhs_lines on coarse levels with fine-grid indices, which is
+ * meaningful only without coarsening); an azimuth that rounds to one bin past
+ * the last wraps to the first (the reference reads past its table); the
+ * polars come in arrays instead of the airfoil files the reference reopens
+ * for every element; its per-element prints are not reproduced.  Two
+ * turbines whose kernel lists share a node add to it in either order.
+ * --------------------------------------------------------------------- */
+typedef struct desalm_alm_turbine {
+  int nblades, nelems, nangles;  /* nangles azimuth bins: dtheta_interp = 2 pi / nangles */
+  double tsr;                     /* tip-speed ratio                                    */
+  double tur_rad, hub_rad;        /* rotor and hub radius (m)                           */
+  double angle;                   /* azimuth of blade 1 (rad); desalm_alm_set_angle     */
+  /* element cells per azimuth bin, entry e = (nang - 1) * nelems + (elem - 1):
+   * node_index[3 e + 0..2] = i, j, k of the cell's lower corner;
+   * node_pos[27 e + 0..26] = xf, yf, zf, then the corners 000, 100, 110, 010,
+   * 001, 101, 111, 011 as x, y, z each (node_indexes_pos(...,1:27)) */
+  const int* node_index;
+  const double* node_pos;
+  /* per fine-grid (j, k), index (j - 1) + jm (k - 1): disk_dat[8 index + c]
+   * = radius, area, theta, dV, chord, twist, inter, relthick (the reference's
+   * disk_dat(j, k, 1:8)); polar_b / polar_a = the airfoil polar before / after */
+  const double* disk_dat;
+  const int* polar_b;
+  const int* polar_a;
+  /* kernel nodes: nker entries; ker_index[3 n] = i, j, k; ker_pos[3 n] = x, y,
+   * z; ker_dat[4 n] = radius, area, theta, dV (disk_dat_ker(i, j, k, 1:4)) */
+  int nker;
+  const int* ker_index;
+  const double* ker_pos;
+  const double* ker_dat;
+} desalm_alm_turbine;
+
+typedef struct desalm_alm {
+  int n_tur;
+  const desalm_alm_turbine* tur;
+  double vel_infty;               /* free-stream velocity (m/s): omega = vel_infty tsr / tur_rad */
+  double length_scale;            /* m per grid unit; vel_scale = ren 1e-6 / length_scale        */
+  /* airfoil polars as the reference's airfoil files hold them: table p has
+   * polar_count[p] rows (angle in degrees, Cl, Cd) at polar_rows[3 (polar_offset[p] + r)];
+   * its last row has angle -999, the end marker */
+  int npolar;
+  const int* polar_offset;
+  const int* polar_count;
+  const double* polar_rows;
+} desalm_alm;
+
+/* Turns the forcing on for this context (n_tur = 0 turns it off).  Every
+ * element cell and kernel node must be an interior fine node (the cell's
+ * upper corner included), every polar index valid. */
+int  desalm_alm_set(desalm_ctx* ctx, const desalm_alm* alm);
+/* The azimuth of turbine n_t (1-based); the driver advances it once per
+ * physical step, as src/main.F90:42-50 does. */
+int  desalm_alm_set_angle(desalm_ctx* ctx, int n_t, double angle);
+/* After a fine-level DAF step: what = 0, the element forces of the last call
+ * as (xf, yf, zf, fx, fy, fz) per element, turbines, blades, elements in
+ * that order (forces_lines); what = 1, the force added to rh(2:4), [3][N]
+ * over the fine level. */
+#define DESALM_ALM_FORCES 0
+#define DESALM_ALM_FIELD  1
+int  desalm_alm_get(desalm_ctx* ctx, int what, double* out);
+
+/* ---------------------------------------------------------------------
  * On-disk formats of the reference, for drivers that run real cases and
  * checkpoint from the device.  Grid and solution files are Fortran
  * unformatted sequential files (each record: 4-byte little-endian byte count,

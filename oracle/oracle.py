@@ -12,7 +12,7 @@ import subprocess
 
 import numpy as np
 
-from desalm.abi import Case, StepReport, level_dims
+from desalm.abi import Alm, Case, StepReport, level_dims, make_alm
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
@@ -52,6 +52,9 @@ def lib():
             ("begin_step", [vp]),
             ("pseudo_iteration", [vp, C.POINTER(StepReport)]),
             ("mg_driver", [vp, C.POINTER(StepReport)]),
+            ("alm_set", [vp, C.POINTER(Alm)]),
+            ("alm_set_angle", [vp, ip, C.c_double]),
+            ("alm_get", [vp, ip, dp]),
         ]:
             f = getattr(L, "desalm_oracle_" + name)
             f.argtypes = args
@@ -172,6 +175,24 @@ class OracleSolver:
         rep = StepReport()
         self._ck(self.L.desalm_oracle_mg_driver(self.ctx, C.byref(rep)), "mg_driver")
         return rep.as_dict()
+
+    def alm_set(self, spec):
+        if spec is None:
+            self._ck(self.L.desalm_oracle_alm_set(self.ctx, None), "alm_set")
+            self._alm_n = 0
+            return
+        a, keep = make_alm(spec)
+        self._ck(self.L.desalm_oracle_alm_set(self.ctx, C.byref(a)), "alm_set")
+        self._alm_n = sum(T["nblades"] * T["nelems"] for T in spec["turbines"])
+
+    def alm_set_angle(self, n_t, angle):
+        self._ck(self.L.desalm_oracle_alm_set_angle(self.ctx, int(n_t), float(angle)), "alm_set_angle")
+
+    def alm_get(self, what):
+        N = self.case.im * self.case.jm * self.case.km
+        out = np.zeros(6 * self._alm_n if what == 0 else 3 * N)
+        self._ck(self.L.desalm_oracle_alm_get(self.ctx, int(what), _p(out)), "alm_get")
+        return out.reshape(-1, 6) if what == 0 else out.reshape(3, N)
 
     def phase_times(self):
         t = np.zeros(8)

@@ -28,6 +28,9 @@ struct Base {
   virtual int save_qold() = 0;
   virtual int begin_step() = 0;
   virtual int pseudo_iteration(desalm_step_report*) = 0;
+  virtual int alm_set(const desalm_alm*) = 0;
+  virtual int alm_angle(int, double) = 0;
+  virtual int alm_get(int, double*) = 0;
   virtual int mg_driver(desalm_step_report*) = 0;
   virtual void phase_times(double*) = 0;
 };
@@ -105,6 +108,59 @@ struct Impl : Base {
     if (!lvl_ok(n)) return DESALM_EINVAL;
     d[0] = s.L[n - 1].im; d[1] = s.L[n - 1].jm; d[2] = s.L[n - 1].km;
     return 0;
+  }
+  int alm_set(const desalm_alm* a) override {
+    s.alm.clear();
+    s.alm_on = a && a->n_tur > 0;
+    if (!s.alm_on) return 0;
+    const int jm = s.L[0].jm, km = s.L[0].km;
+    s.alm_vel_infty = R(a->vel_infty);
+    s.alm_length_scale = R(a->length_scale);
+    s.polar_off.assign(a->polar_offset, a->polar_offset + a->npolar);
+    s.polar_cnt.assign(a->polar_count, a->polar_count + a->npolar);
+    long nrows = 0;
+    for (int p = 0; p < a->npolar; ++p) nrows = std::max<long>(nrows, a->polar_offset[p] + a->polar_count[p]);
+    s.polar_rows.resize(3 * nrows);
+    for (long r = 0; r < 3 * nrows; ++r) s.polar_rows[r] = R(a->polar_rows[r]);
+    for (int t = 0; t < a->n_tur; ++t) {
+      const desalm_alm_turbine& T = a->tur[t];
+      typename orc::Solver<R>::AlmTur U;
+      U.nblades = T.nblades; U.nelems = T.nelems; U.nangles = T.nangles; U.nker = T.nker;
+      U.tsr = R(T.tsr); U.tur_rad = R(T.tur_rad); U.hub_rad = R(T.hub_rad); U.angle = R(T.angle);
+      const long ne = long(T.nangles) * T.nelems;
+      U.node_index.assign(T.node_index, T.node_index + 3 * ne);
+      U.node_pos.resize(27 * ne);
+      for (long e = 0; e < 27 * ne; ++e) U.node_pos[e] = R(T.node_pos[e]);
+      U.disk_dat.resize(8L * jm * km);
+      for (long e = 0; e < 8L * jm * km; ++e) U.disk_dat[e] = R(T.disk_dat[e]);
+      U.polar_b.assign(T.polar_b, T.polar_b + long(jm) * km);
+      U.polar_a.assign(T.polar_a, T.polar_a + long(jm) * km);
+      U.ker_index.assign(T.ker_index, T.ker_index + 3L * T.nker);
+      U.ker_pos.resize(3L * T.nker);
+      U.ker_dat.resize(4L * T.nker);
+      for (long e = 0; e < 3L * T.nker; ++e) U.ker_pos[e] = R(T.ker_pos[e]);
+      for (long e = 0; e < 4L * T.nker; ++e) U.ker_dat[e] = R(T.ker_dat[e]);
+      s.alm.push_back(std::move(U));
+    }
+    return 0;
+  }
+  int alm_angle(int t, double angle) override {
+    if (t < 1 || t > (int)s.alm.size()) return DESALM_EINVAL;
+    s.alm[t - 1].angle = R(angle);
+    return 0;
+  }
+  int alm_get(int what, double* out) override {
+    if (what == DESALM_ALM_FORCES) {
+      for (size_t e = 0; e < s.forces_lines.size(); ++e) out[e] = double(s.forces_lines[e]);
+      return 0;
+    }
+    if (what == DESALM_ALM_FIELD) {
+      const long N = s.L[0].N;
+      for (int d = 0; d < 3; ++d)
+        for (long l = 0; l < N; ++l) out[d * N + l] = s.falm[d].empty() ? 0.0 : double(s.falm[d][l]);
+      return 0;
+    }
+    return DESALM_EINVAL;
   }
   int solver_daf(int n, int recalc, int itr) override {
     if (!lvl_ok(n)) return DESALM_EINVAL;
@@ -225,6 +281,9 @@ int desalm_oracle_begin_step(void* ctx) { return ((Base*)ctx)->begin_step(); }
 int desalm_oracle_pseudo_iteration(void* ctx, desalm_step_report* r) { return ((Base*)ctx)->pseudo_iteration(r); }
 int desalm_oracle_mg_driver(void* ctx, desalm_step_report* r) { return ((Base*)ctx)->mg_driver(r); }
 void desalm_oracle_phase_times(void* ctx, double* t) { ((Base*)ctx)->phase_times(t); }
+int desalm_oracle_alm_set(void* ctx, const desalm_alm* a) { return ((Base*)ctx)->alm_set(a); }
+int desalm_oracle_alm_set_angle(void* ctx, int t, double angle) { return ((Base*)ctx)->alm_angle(t, angle); }
+int desalm_oracle_alm_get(void* ctx, int what, double* out) { return ((Base*)ctx)->alm_get(what, out); }
 
 // Standalone LAPACK-style tridiagonal solve (SGTSV restatement) for tests.
 int desalm_oracle_gtsv(int n, int nrhs, double* dl, double* d, double* du, double* b, int ldb, long* npiv) {

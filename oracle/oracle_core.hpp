@@ -236,6 +236,21 @@ struct Solver {
   double phase_s[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // residual, modal+sweeps, bc, transfers, sa, norm
   std::string err;
 
+  // actuator-line forcing: the tables init_lines builds (src/init.F90:1156-1710)
+  struct AlmTur {
+    int nblades = 0, nelems = 0, nangles = 0, nker = 0;
+    R tsr = 0, tur_rad = 0, hub_rad = 0, angle = 0;
+    std::vector<int> node_index, polar_b, polar_a, ker_index;
+    std::vector<R> node_pos, disk_dat, ker_pos, ker_dat;
+  };
+  bool alm_on = false;
+  std::vector<AlmTur> alm;
+  R alm_vel_infty = 0, alm_length_scale = 1;
+  std::vector<int> polar_off, polar_cnt;
+  std::vector<R> polar_rows;
+  std::vector<R> forces_lines;  // (xf, yf, zf, fx, fy, fz) per turbine, blade, element
+  std::vector<R> falm[3];       // what rhs_lines added to rh(2:4)
+
   explicit Solver(const desalm_case& cc) : c(cc) {
     ng = c.ng;
     L.resize(ng);
@@ -1002,12 +1017,141 @@ ORC_PARFOR
     phase_s[2] += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   }
 
+  // ------------------------------------------------- actuator-line forcing
+  // Airfoil polar lookup of src/rhs_lines.F90:241-281: a linear scan for the
+  // interval [angle1, angle2] holding AOA, stopping unassigned when AOA is at
+  // or below an interval's start or the end marker (-999) is reached; an
+  // unassigned lookup leaves the caller's previous values.
+  bool polar_lookup(int p, R aoa, R& cl, R& cd) const {
+    const R* rows = polar_rows.data() + 3 * polar_off[p];
+    int idx = 0, counter = 1;
+    R angle1 = 1000, angle2 = 1000, cl1 = 0, cd1 = 0, cl2 = 0, cd2 = 0;
+    while (angle2 != R(-999)) {
+      if (counter == 1) { angle1 = rows[3 * idx]; cl1 = rows[3 * idx + 1]; cd1 = rows[3 * idx + 2]; ++idx; }
+      else { angle1 = angle2; cl1 = cl2; cd1 = cd2; }
+      angle2 = rows[3 * idx]; cl2 = rows[3 * idx + 1]; cd2 = rows[3 * idx + 2]; ++idx;
+      if (aoa <= angle1) {
+        angle2 = R(-999);
+      } else if (angle2 == R(-999)) {
+      } else if (aoa <= angle2 && aoa >= angle1) {
+        R m = (cl2 - cl1) / (angle2 - angle1);
+        cl = m * (aoa - angle1) + cl1;
+        m = (cd2 - cd1) / (angle2 - angle1);
+        cd = m * (aoa - angle1) + cd1;
+        return true;
+      } else {
+        ++counter;
+      }
+    }
+    return false;
+  }
+
+  // rhs_lines (src/rhs_lines.F90:47-483) on the fine level: element forces
+  // from the interpolated velocity and the polars, then their Gaussian
+  // projection onto each turbine's kernel nodes, added to rh(2:4).
+  void rhs_lines(Level<R>& G) {
+    const R pi = R(3.141592653589793);  // src/precision.F90:43
+    const R rho = R(1178.62);
+    const R ls = alm_length_scale;
+    const R vel_scale = R(c.ren) * R(10E-7) / ls;
+    for (int d = 0; d < 3; ++d) falm[d].assign(G.N, R(0));
+    size_t nel = 0;
+    for (auto& T : alm) nel += size_t(T.nblades) * T.nelems;
+    forces_lines.assign(6 * nel, R(0));
+    // the lookups' outputs persist from element to element within a call
+    R cl_b = 0, cd_b = 0, cl_a = 0, cd_a = 0;
+    size_t base = 0;
+    for (auto& T : alm) {
+      const R omega = (alm_vel_infty * T.tsr) / T.tur_rad;
+      const R dth = R(2) * pi / R(T.nangles);
+      for (int bld = 1; bld <= T.nblades; ++bld) {
+        R angle_aux = T.angle + R(bld - 1) * R(2) * pi / R(T.nblades);
+        if (angle_aux > R(2) * pi) angle_aux = angle_aux - R(2) * pi;
+        int nang = int(std::lround(double(angle_aux / dth))) + 1;
+        if (nang > T.nangles) nang -= T.nangles;  // the reference reads one bin past its table here
+        for (int elem = 1; elem <= T.nelems; ++elem) {
+          const long e = long(nang - 1) * T.nelems + (elem - 1);
+          const int i = T.node_index[3 * e], j = T.node_index[3 * e + 1], k = T.node_index[3 * e + 2];
+          // only cells whose lower corner is in the rank's interior (src/rhs_lines.F90:166-167)
+          if (i < 2 || i > G.im - 1 || j < 2 || j > G.jm - 1 || k < 2 || k > G.km - 1) continue;
+          const R* P = T.node_pos.data() + 27 * e;
+          // node_indexes_pos(...,1:27): xf, yf, zf, then corners 000 100 110 010 001 101 111 011
+          const R xf = P[0], yf = P[1], zf = P[2];
+          const R x000 = P[3], z000 = P[5], x100 = P[6], y100 = P[7], y110 = P[10];
+          const R x001 = P[15], z001 = P[17], x101 = P[18], y101 = P[19], y111 = P[22];
+          const long jk = (long)(j - 1) + (long)G.jm * (k - 1);
+          const R* D = T.disk_dat.data() + 8 * jk;
+          const R radius = D[0] * ls, chord = D[4], twist = D[5], inter = D[6];
+          auto q = [&](int m, int ii, int jj, int kk) { return G.q[m][G.id(ii, jj, kk)]; };
+          R v[3];
+          for (int m = 1; m <= 3; ++m) {  // src/rhs_lines.F90:192-214
+            const R down = R(1) / ((x100 - x000) * (y110 - y100)) *
+                           ((x100 - xf) * ((y110 - yf) * (q(m, i, j, k) + q(m, i, j + 1, k))) +
+                            (xf - x000) * ((yf - y100) * (q(m, i + 1, j, k) + q(m, i + 1, j + 1, k))));
+            const R up = R(1) / ((x101 - x001) * (y111 - y101)) *
+                         ((x101 - xf) * ((y111 - yf) * (q(m, i, j, k + 1) + q(m, i, j + 1, k + 1))) +
+                          (xf - x001) * ((yf - y101) * (q(m, i + 1, j, k + 1) + q(m, i + 1, j + 1, k + 1))));
+            v[m - 1] = down + (up - down) / (z001 - z000) * (zf - z000);
+          }
+          const R u_x = v[0] * vel_scale, u_y = v[1] * vel_scale, u_z = v[2] * vel_scale;
+          const R u_theta = omega * radius + u_y * std::sin(angle_aux) - u_z * std::cos(angle_aux);
+          const R phi = std::atan2(u_x, u_theta);
+          const R aoa = phi * R(180.0) / pi - twist;
+          polar_lookup(T.polar_b[jk], aoa, cl_b, cd_b);
+          polar_lookup(T.polar_a[jk], aoa, cl_a, cd_a);
+          const R cl = (cl_a - cl_b) * inter + cl_b;
+          const R cd = (cd_a - cd_b) * inter + cd_b;
+          const R urel = std::sqrt(u_theta * u_theta + u_x * u_x);
+          const R fl = R(0.5) * cl * rho * (urel * urel) * chord;
+          const R fd = R(0.5) * cd * rho * (urel * urel) * chord;
+          R* F = forces_lines.data() + 6 * (base + size_t(bld - 1) * T.nelems + (elem - 1));
+          F[0] = xf; F[1] = yf; F[2] = zf;
+          F[3] = fl * std::cos(phi) + fd * std::sin(phi);
+          F[4] = fl * std::sin(angle_aux) * std::sin(phi) - fd * std::sin(angle_aux) * std::sin(phi);
+          F[5] = fl * std::cos(angle_aux) * std::sin(phi) - fd * std::cos(angle_aux) * std::cos(phi);
+        }
+      }
+      // projection (src/rhs_lines.F90:382-448)
+      const R deltar = std::abs(T.tur_rad - T.hub_rad) / R(T.nelems);
+      const size_t ne = size_t(T.nblades) * T.nelems;
+      for (int n = 0; n < T.nker; ++n) {
+        const int* I = T.ker_index.data() + 3 * n;
+        if (I[0] < 2 || I[0] > G.im - 1 || I[1] < 2 || I[1] > G.jm - 1 || I[2] < 2 || I[2] > G.km - 1) continue;
+        const R radius = T.ker_dat[4 * n] * ls;
+        const R dV = T.ker_dat[4 * n + 3] * (ls * ls * ls);
+        if (!(radius > T.hub_rad)) continue;
+        const R xk = T.ker_pos[3 * n], yk = T.ker_pos[3 * n + 1], zk = T.ker_pos[3 * n + 2];
+        R fx = 0, fy = 0, fz = 0;
+        for (size_t e = 0; e < ne; ++e) {
+          const R* F = forces_lines.data() + 6 * (base + e);
+          const R rdis =
+              std::sqrt((xk - F[0]) * (xk - F[0]) + (yk - F[1]) * (yk - F[1]) + (zk - F[2]) * (zk - F[2])) * ls;
+          const R eps = R(2) * std::pow(dV, R(1.0) / R(3.0));
+          const R ker =
+              R(1) / ((eps * eps * eps) * std::pow(pi, R(3.0) / R(2.0))) * std::exp(-(rdis * rdis) / (eps * eps));
+          fx = fx + ker * F[3] * deltar;
+          fy = fy + ker * F[4] * deltar;
+          fz = fz + ker * F[5] * deltar;
+        }
+        const long l = G.id(T.ker_index[3 * n], T.ker_index[3 * n + 1], T.ker_index[3 * n + 2]);
+        const R sc = (ls / (rho * vel_scale * vel_scale)) * (R(1) / G.aj[l]);
+        const R d[3] = {fx * sc, fy * sc, fz * sc};
+        for (int m = 0; m < 3; ++m) {
+          G.rh[m + 1][l] = G.rh[m + 1][l] + d[m];
+          falm[m][l] = falm[m][l] + d[m];
+        }
+      }
+      base += ne;
+    }
+  }
+
   // solver_daf (src/solver_daf.F90:138-488) on level index n (0 = fine).
   void solver_daf(int n, int recalc, int itr) {
     Level<R>& G = L[n];
     const int im = G.im, jm = G.jm, km = G.km;
     for (int m = 0; m < 4; ++m) std::fill(G.rh[m].begin(), G.rh[m].end(), R(0));
     residual(G, n, true, itr == 1 ? 1 : 0);
+    if (n == 0 && alm_on) rhs_lines(G);  // src/solver_daf.F90:378-381
     diag_solver(G, n);
     ORC_PARFOR
     for (int k = 2; k <= km - 1; ++k)
