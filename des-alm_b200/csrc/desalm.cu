@@ -1992,6 +1992,35 @@ int desalm_lp_get_buffer(desalm_ctx* ctx, int which, float* out) {
 
 }  // extern "C"
 
+// ------------------------------------------------------ watchdog self-test
+extern "C" {
+
+int desalm_watchdog_selftest(desalm_ctx* ctx, double seconds) {
+  if (!ctx || !(seconds > 0.0) || seconds > 10.0) return DESALM_EINVAL;
+  int* e = nullptr;
+  CK(cudaMalloc(&e, sizeof(int)));
+  cudaError_t r = cudaMemsetAsync(e, 0, sizeof(int), ctx->stream);
+  if (r == cudaSuccess) {
+    k_wait_probe<<<1, 32, 0, ctx->stream>>>((unsigned long long)(seconds * 1e9), e);
+    r = cudaGetLastError();
+  }
+  int h = 0;
+  if (r == cudaSuccess) r = cudaMemcpyAsync(&h, e, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+  if (r == cudaSuccess) r = cudaStreamSynchronize(ctx->stream);
+  cudaFree(e);
+  if (r != cudaSuccess) {
+    ctx->err = std::string("watchdog self-test: ") + cudaGetErrorString(r);
+    return DESALM_ECUDA;
+  }
+  if (h) {
+    ctx->err = "watchdog self-test: the bounded wait gave up as it should";
+    return DESALM_ETIMEOUT;
+  }
+  return 0;
+}
+
+}  // extern "C"
+
 // ------------------------------------------------------ checkpoint / restart
 extern "C" {
 

@@ -85,10 +85,10 @@ DESALM_DEV void lp_bar_arrive(unsigned bar) {
   asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
-// Wait for the phase of parity `parity` to complete; false after the time
-// limit (or, unless draining, when another thread already gave up), with
-// *err set.
-DESALM_DEV bool lp_bar_wait(unsigned bar, unsigned parity, int* err, bool drain = false) {
+// Wait for the phase of parity `parity` to complete; false after `limit_ns`
+// (or, unless draining, when another thread already gave up), with *err set.
+DESALM_DEV bool lp_bar_wait(unsigned bar, unsigned parity, int* err, bool drain = false,
+                            unsigned long long limit_ns = LP_TC_WAIT_NS) {
   const unsigned long long t0 = lp_ns();
   for (unsigned n = 0;; ++n) {
     unsigned ok;
@@ -102,7 +102,7 @@ DESALM_DEV bool lp_bar_wait(unsigned bar, unsigned parity, int* err, bool drain 
     if (ok) return true;
     if ((n & 255u) == 255u) {
       if (!drain && *(volatile int*)err) return false;
-      if (lp_ns() - t0 > LP_TC_WAIT_NS) {
+      if (lp_ns() - t0 > limit_ns) {
         atomicExch(err, 1);
         return false;
       }
@@ -584,6 +584,18 @@ __global__ void __launch_bounds__(LP_TC_THREADS, 1)
     lp_tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(COLS) : "memory");
   }
+}
+
+// Watchdog self-test: one thread waits on an mbarrier that nothing completes,
+// with a limit of limit_ns, through the same bounded wait as the kernels
+// above; it must give up and set *err.  Nothing else is in flight.
+__global__ void k_wait_probe(unsigned long long limit_ns, int* err) {
+  __shared__ unsigned long long bar;
+  if (threadIdx.x != 0) return;
+  const unsigned b = lp_smem_u32(&bar);
+  lp_bar_init(b, 1);
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  lp_bar_wait(b, 0, err, false, limit_ns);
 }
 
 }  // namespace desalm

@@ -94,6 +94,7 @@ def lib():
             ("lp_checkpoint_read", [vp, cp]),
             ("lp_checkpoint_write", [vp, cp]),
             ("alm_set", [vp, C.POINTER(Alm)]),
+            ("watchdog_selftest", [vp, C.c_double]),
             ("alm_set_angle", [vp, ip, C.c_double]),
             ("alm_get", [vp, ip, dp]),
         ]:
@@ -300,6 +301,14 @@ class Solver:
                 if la[t]:
                     out.setdefault(name, {})[lvl + 1] = (float(ms[t]), int(la[t]), float(nodes[t]))
         return out, int(tot.value)
+
+    def watchdog_selftest(self, seconds):
+        """The status of desalm_watchdog_selftest (DESALM_ETIMEOUT when the
+        device's bounded wait gave up as it must)."""
+        return int(self.L.desalm_watchdog_selftest(self.ctx, float(seconds)))
+
+    def last_error(self):
+        return self.L.desalm_last_error(self.ctx).decode()
 
     # ------------------------------------------------ actuator-line forcing
     def alm_set(self, spec):

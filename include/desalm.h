@@ -356,6 +356,12 @@ int  desalm_alm_set_angle(desalm_ctx* ctx, int n_t, double angle);
 #define DESALM_ALM_FIELD  1
 int  desalm_alm_get(desalm_ctx* ctx, int what, double* out);
 
+/* Self-test of the device watchdog: a kernel waits, through the same bounded
+ * wait as the tensor-core kernels, on a barrier that nothing completes, for
+ * `seconds` (<= 10); the call returns DESALM_ETIMEOUT when the wait gave up
+ * and reported it, as it must.  No counterpart in the reference. */
+int  desalm_watchdog_selftest(desalm_ctx* ctx, double seconds);
+
 /* ---------------------------------------------------------------------
  * On-disk formats of the reference, for drivers that run real cases and
  * checkpoint from the device.  Grid and solution files are Fortran
