@@ -51,6 +51,8 @@ struct Lv {
   W* bj;           // j-face: [4][4][im*km]  (rows 2, 3, jm-1, jm-2 after the i sweep)
   W* bk;           // k-face: [4][4][im*jm]
   int* flags;      // [0] pivot-would-swap count, [1] zero pivot count
+  int oute;        // 1: the characteristics outlet plane i = im is solved
+                   // with the interior (fine level, btype(2) = 5)
 };
 
 // Scalar parameters of the case used by kernels (constant per context).

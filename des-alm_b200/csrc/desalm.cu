@@ -25,6 +25,7 @@
 #include "learn.cuh"
 #include "learn_tc.cuh"
 #include "alm.cuh"
+#include "outlet.cuh"
 
 using namespace desalm;
 
@@ -231,7 +232,7 @@ inline unsigned cdiv(long a, long b) { return (unsigned)((a + b - 1) / b); }
 // kernel classes for desalm_kernel_stats
 enum KClass { KC_DTAU = 0, KC_RESID, KC_SWEEP_I, KC_SWEEP_J, KC_SWEEP_K, KC_RECALC, KC_BCOND, KC_PFIX,
               KC_NLEVEL, KC_PROLONG, KC_RSMOOTH, KC_NORM, KC_SA_RHS, KC_SA_SWEEP, KC_SA_BC,
-              KC_XFORM_I, KC_XFORM_J, KC_XFORM_K, KC_SA_AUX, KC_LEARN, KC_ALM, KC_MISC, KC_COUNT };
+              KC_XFORM_I, KC_XFORM_J, KC_XFORM_K, KC_SA_AUX, KC_LEARN, KC_ALM, KC_OUTLET, KC_MISC, KC_COUNT };
 
 struct ProfScope {
   desalm_ctx* ctx;
@@ -270,6 +271,7 @@ int alloc_level(desalm_ctx* ctx, Level& G, Lv<T, W>& L) {
   L.N = (int)N;
   L.sj = G.im; L.sk = G.im * G.jm;
   L.falm = nullptr;
+  L.oute = 0;
   L.dc = T(G.dc); L.de = T(G.de); L.dz = T(G.dz);
   auto A = [&](T** p) { return dalloc(ctx, G.allocs, (void**)p, N * sizeof(T)); };
   auto AW = [&](W** p) { return dalloc(ctx, G.allocs, (void**)p, N * sizeof(W)); };
@@ -304,8 +306,6 @@ int check_case(desalm_ctx* ctx, const desalm_case& c) {
   if (c.im < 5 || c.jm < 5 || c.km < 5) return bad("each extent must be >= 5");
   if ((c.icrs != 0 && c.icrs != 1) || (c.jcrs != 0 && c.jcrs != 1) || (c.kcrs != 0 && c.kcrs != 1))
     return bad("icrs/jcrs/kcrs must be 0 or 1");
-  for (int b = 0; b < 6; ++b)
-    if (c.btype[b] == 5) return bad("btype 5 (characteristics outlet) is not supported");
   if (c.precision_mode != DESALM_FP64 && c.precision_mode != DESALM_MIXED) return bad("unknown precision_mode");
   if (c.predictor != DESALM_PRED_QN && c.predictor != DESALM_PRED_LINEAR && c.predictor != DESALM_PRED_LEARNED)
     return bad("unknown predictor");
@@ -388,8 +388,8 @@ template <class T, class W, int DIR, int NL>
 int sweep4_nl(desalm_ctx* ctx, Lv<T, W>& L, const Par& P, int lvl, int blo, int bhi) {
   int amax, n, nb;
   if (DIR == 0) { amax = L.jm - 2; n = L.im - 2; nb = L.km - 2; }
-  else if (DIR == 1) { amax = L.im - 2; n = L.jm - 2; nb = L.km - 2; }
-  else { amax = L.im - 2; n = L.km - 2; nb = L.jm - 2; }
+  else if (DIR == 1) { amax = L.im - 2 + L.oute; n = L.jm - 2; nb = L.km - 2; }
+  else { amax = L.im - 2 + L.oute; n = L.km - 2; nb = L.jm - 2; }
   const size_t bytes = slab_bytes<W>(n, NL);
   const int cls = DIR == 0 ? KC_SWEEP_I : (DIR == 1 ? KC_SWEEP_J : KC_SWEEP_K);
   const double nin = double(amax) * n * nb;
@@ -400,7 +400,8 @@ int sweep4_nl(desalm_ctx* ctx, Lv<T, W>& L, const Par& P, int lvl, int blo, int 
     LAUNCH(cls, lvl, nin, launch_k(k_sweep4<T, W, DIR, NL, kSlabThreads>, dim3(cdiv(amax, NL), nb), kSlabThreads, bytes, s, L, P, blo, bhi));
   CKL();
   const int xcls = DIR == 0 ? KC_XFORM_I : (DIR == 1 ? KC_XFORM_J : KC_XFORM_K);
-  LAUNCH(xcls, lvl, nin, launch_k(k_xform<T, W, DIR>, grid_interior(L), blk3(), 0, s, L));
+  const dim3 gx(cdiv(L.im - 2 + L.oute, 32), cdiv(L.jm - 2, 4), L.km - 2);
+  LAUNCH(xcls, lvl, nin, launch_k(k_xform<T, W, DIR>, gx, blk3(), 0, s, L));
   CKL();
   return 0;
 }
@@ -489,6 +490,14 @@ int launch_daf(desalm_ctx* ctx, Lv<T, W>& L, Level& G, int n, int recalc, int it
   if (n == 0 && ctx->alm.on) RET(alm_run(ctx, L));
   LAUNCH(KC_RESID, n, nin, launch_k(k_resid<T, W, 0>, grid_r(L.im, L.jm, L.km), blk_r(), 0, s, L, P, upwind, itr == 1 ? 1 : 0, n > 0 ? 1 : 0, bback));
   CKL();
+  if (L.oute) {
+    // the outlet plane's residual and its preparation for the sweeps
+    // (src/solver_daf.F90:318-358); the back face's call writes a plane that
+    // nothing reads, so it is not made
+    LAUNCH(KC_OUTLET, n, double(L.jm - 2) * (L.km - 2),
+           launch_k(k_outlet<T, W>, dim3(cdiv(L.jm - 2, 32), cdiv(L.km - 2, 4)), dim3(32, 4), 0, s, L, P));
+    CKL();
+  }
   RET((launch_sweep<T, W, 0>(ctx, L, P, n, bback, 0)));
   RET((launch_sweep<T, W, 1>(ctx, L, P, n, fine && c.btype[2] != 5, fine && c.btype[3] != 5)));
   RET((launch_sweep<T, W, 2>(ctx, L, P, n, fine && c.btype[4] != 5, fine && c.btype[5] != 5 && c.btype[5] != 6)));
@@ -1142,6 +1151,9 @@ int desalm_init(const desalm_case* c, desalm_ctx** out) {
     if (k == K_DD) rc = alloc_level(ctx, G, G.dd);
     else rc = alloc_level(ctx, G, G.df);
     if (rc) { *out = ctx; return rc; }
+    // the characteristics outlet plane is solved on the fine level only
+    // (src/solver_daf.F90:371-373)
+    G.dd.oute = G.df.oute = (n == 0 && c->btype[1] == 5) ? 1 : 0;
     G.tbytes = 8;
     G.wbytes = k == K_DD ? 8 : 4;
     if (n + 1 < ctx->ng) {
@@ -1683,6 +1695,8 @@ SaT<SW> make_sa(desalm_ctx* ctx, Lv<double, W>& L) {
   S.flags = ctx->flags;
   S.ren = ctx->c.ren; S.delti = ctx->c.delti; S.es = ctx->c.unsteady ? 1.0 : 0.0;
   for (int b = 0; b < 6; ++b) { S.sa1[b] = ctx->par.sa[0][b]; S.sb1[b] = ctx->par.sb[0][b]; S.btype[b] = ctx->c.btype[b]; }
+  S.rat = (const double*)ctx->rat;
+  S.ratdim = ctx->ratdim;
   return S;
 }
 

@@ -40,6 +40,8 @@ struct SaT {
   double ren, delti, es;
   double sa1[6], sb1[6];  // pressure-row extrapolation coefficients, sa(1,b), sb(1,b)
   int btype[6];
+  const double* rat;      // extrapolation ratios rat(:,:,b), [6][ratdim][ratdim]
+  int ratdim;
 };
 
 using Sa = SaT<double>;
@@ -465,7 +467,10 @@ __global__ void k_sa_bc(SaT<SW> S) {
     const int s = side == 0 ? st : -st;
     if (bt == 1) q5[l] = 0.0;
     else if (bt == 2 || bt == 3) q5[l] = S.sa1[bi] * q5[l + s] + S.sb1[bi] * q5[l + 2 * s];
-    else if (bt == 6) q5[l] = side == 0 ? q5[lb + (n - 2) * st] : q5[lb + st];
+    else if (bt == 5) {
+      const double r = S.rat[(size_t)bi * S.ratdim * S.ratdim + a + (size_t)S.ratdim * b];
+      q5[l] = (1.0 + r) * q5[l + s] - r * q5[l + 2 * s];
+    } else if (bt == 6) q5[l] = side == 0 ? q5[lb + (n - 2) * st] : q5[lb + st];
     else if (bt == 8 && DIR == 0 && side == 1) q5[l] = q5[l - 1];
   }
 }

@@ -65,10 +65,14 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
   const int tid = threadIdx.x;
   const int a0 = blockIdx.x * NL + 1;
   const int b = blockIdx.y + 1;
+  // oute: the fine level's characteristics outlet plane i = im is solved
+  // too (idend = i_myend + 1, src/solver_daf.F90:371-373): one more row on
+  // each i line, one more line of j and k lines per plane
   int amax, n, st, sa;
   if (DIR == 0) { amax = L.jm - 2; n = L.im - 2; st = 1; sa = L.sj; }
-  else if (DIR == 1) { amax = L.im - 2; n = L.jm - 2; st = L.sj; sa = 1; }
-  else { amax = L.im - 2; n = L.km - 2; st = L.sk; sa = 1; }
+  else if (DIR == 1) { amax = L.im - 2 + L.oute; n = L.jm - 2; st = L.sj; sa = 1; }
+  else { amax = L.im - 2 + L.oute; n = L.km - 2; st = L.sk; sa = 1; }
+  const int ext = DIR == 0 ? L.oute : 0;
   const int base = (DIR == 2) ? L.sj * b : L.sk * b;
   const int nl = min(NL, amax - a0 + 1);
   const int np = n + 2;
@@ -90,8 +94,8 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
       const int l = base + (a0 + li) * sa + p * st;
       const int so = p * NLP + li;
       cp_async_elem(s_hc + so, hc + l);
-      if (p >= 1 && p <= n) {
-        cp_async_elem(s_tc + so, tc + l);
+      if (p >= 1 && p <= n) cp_async_elem(s_tc + so, tc + l);
+      if (p >= 1 && p <= n + ext) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) cp_async_elem(s_r + q * fs + so, L.wk[q] + l);
       }
@@ -183,6 +187,18 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
     const W bem = sbe[li][m];
     W he = chc[at(n + 1)], hcur = chc[at(n)];
     W dprev = 0, rdprev = 0, awprev = 0, bprev = 0;
+    if (ext) {
+      // the outlet row (src/rhs_diag_solver.F90:207-221): ap = 1, 1,
+      // 1 + dtau dc spr, 1 and aw = 0, 0, -dtau(im-1) dc spr(im-1), 0;
+      // dtau dc spr = 2 h exactly
+      const W d = m == 2 ? W(1) + W(2) * he : W(1);
+      nzero += d == W(0);
+      rdprev = sweep_rcp(d);
+      sd[at(n + 1)] = rdprev;
+      bprev = r[at(n + 1)];
+      dprev = d;
+      awprev = m == 2 ? -(W(2) * hcur) : W(0);
+    }
     for (int p0 = n; p0 > h; p0 -= R) {
       W bt[R], bh[R], br[R];
 #pragma unroll
@@ -197,7 +213,7 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
           const W ap = W(1) + W(2) * bt[u];
           W rr = br[u];
           W d;
-          if (p == n) { rr = rr - ae * bem; d = ap; bprev = rr; }
+          if (p == n && !ext) { rr = rr - ae * bem; d = ap; bprev = rr; }
           else {
             npiv += dabs(dprev) < dabs(ae);
             const W f = ae * rdprev;
@@ -260,16 +276,22 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
           }
         }
       }
+      if (ext) {
+        const W aw = m == 2 ? -(W(2) * chc[at(n)]) : W(0);
+        x = (r[at(n + 1)] - aw * x) * sd[at(n + 1)];
+        r[at(n + 1)] = x;
+      }
     }
   }
   __syncthreads();
 
   // ---- phase 2: the solved values back to wk (the modal transform follows
   // in k_xform, at full occupancy)
-  const int total = nl * n;
+  const int ne = n + ext;
+  const int total = nl * ne;
   for (int t = tid; t < total; t += NT) {
     int lq, p;
-    if (DIR == 0) { lq = t / n; p = t - lq * n; }
+    if (DIR == 0) { lq = t / ne; p = t - lq * ne; }
     else { p = t / nl; lq = t - p * nl; }
     const int l = base + (a0 + lq) * sa + (p + 1) * st;
     const int so = (p + 1) * NLP + lq;
@@ -290,7 +312,7 @@ __global__ void __launch_bounds__(128) k_xform(Lv<T, W> L) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int k = blockIdx.z + 1;
-  if (i > L.im - 2 || j > L.jm - 2) return;
+  if (i > L.im - 2 + L.oute || j > L.jm - 2) return;
   const int l = i + L.sj * j + L.sk * k;
   W xv[4];
 #pragma unroll

@@ -24,7 +24,7 @@ PRED_LEARNED = 2
 
 LP_FEATURES, LP_TARGET, LP_OUTPUT, LP_SCALES, LP_ALPHA = 0, 1, 2, 3, 4
 
-BC_INTERFACE, BC_WALL, BC_SYMMETRY, BC_FREESTREAM, BC_INFLOW, BC_PERIODIC = 0, 1, 2, 3, 4, 6
+BC_INTERFACE, BC_WALL, BC_SYMMETRY, BC_FREESTREAM, BC_INFLOW, BC_OUTLET, BC_PERIODIC = 0, 1, 2, 3, 4, 5, 6
 
 F_Q, F_QN, F_QNM1, F_QOLD, F_RH, F_PK = 0, 8, 16, 24, 32, 40
 F_CSI, F_ETA, F_ZET, F_AJ, F_NUT, F_DTAU, F_DTEV, F_WD = 48, 52, 56, 60, 61, 62, 63, 64

@@ -13,10 +13,12 @@ Presets
            cell y+ ~ 1), nu_tilde = 3 nu, periodic i/k faces.
   ogrid    O-grid around a circular cylinder (radial geometric stretching to
            20 D, span pi D), SA, Re = 3900, delti = 0.005.
+  wake     open box with uniform inflow and the characteristics outlet
+           (btype 5), stretched and perturbed grid, SA or laminar.
 """
 import numpy as np
 
-from .abi import Case, BC_WALL, BC_INFLOW, BC_PERIODIC, BC_FREESTREAM, FP64, PRED_QN
+from .abi import Case, BC_WALL, BC_SYMMETRY, BC_INFLOW, BC_OUTLET, BC_PERIODIC, BC_FREESTREAM, FP64, PRED_QN
 
 
 def _base_case(im, jm, km):
@@ -304,6 +306,60 @@ def alm_rotor(xs, ys, zs, center, radius, nblades=3, nelems=12, nangles=24, tsr=
     return tur, polars
 
 
+def wake(im=49, jm=25, km=25, seed=0, re=1000.0, turbulence=1, itmax=20, amp=0.05, side=BC_SYMMETRY, ng=3):
+    """Open box [0, 4] x [0, 2] x [0, 2] with a stream through it: uniform
+    inflow u = 1 at i = 1 (btype 4: velocity held, pressure extrapolated with
+    the grid ratio), the characteristics outlet at i = im (btype 5), 'side'
+    on the j faces (symmetry planes by default) and periodic k faces.  x is
+    stretched geometrically (ratio 1.02) so that the extrapolation ratios
+    differ from 1; interior nodes and the outlet plane's y move by a seeded
+    sinusoid, so that the outlet's csi metrics have cross components.  The
+    state is the stream plus O(1e-2) seeded noise; nu_tilde = 3 nu and the
+    wall distance is uniform (no walls) when turbulent."""
+    rng = np.random.default_rng(seed)
+    c = _base_case(im, jm, km)
+    c.ng = ng
+    c.ren = re
+    c.itmax = itmax
+    c.turbulence = turbulence
+    c.btype[0], c.btype[1] = BC_INFLOW, BC_OUTLET
+    c.btype[2] = c.btype[3] = side
+    c.btype[4] = c.btype[5] = BC_PERIODIC
+    g = 1.02 ** np.arange(im - 1)
+    xs = np.concatenate(([0.0], np.cumsum(g))) * (4.0 / g.sum())
+    ys = np.linspace(0.0, 2.0, jm)
+    zs = np.linspace(0.0, 2.0, km)
+    X, Y, Z = _mesh(xs, ys, zs)
+    h = 2.0 / (jm - 1)
+    ph = rng.uniform(0, 2 * np.pi, size=3)
+    sy = np.sin(np.pi * Y / 2.0)
+    sz = np.sin(np.pi * Z / 2.0)
+    sx = np.sin(np.pi * X / 4.0)
+    dx = amp * h * sx * sy * sz * np.cos(np.pi * Z + ph[0])
+    dy = amp * h * (X / 4.0) * sy * sz * np.sin(np.pi * X + ph[1])
+    dz = amp * h * sx * sy * sz * np.sin(np.pi * Y + ph[2])
+    grid = dict(x=_flat(X + dx), y=_flat(Y + dy), z=_flat(Z + dz),
+                wd=np.full(im * jm * km, 10.0) if turbulence else None)
+    N = im * jm * km
+    q = np.zeros((N, 5))
+    q[:, 0] = rng.normal(0.0, 1e-3, size=N)
+    q[:, 1] = 1.0 + rng.normal(0.0, 1e-2, size=N)
+    q[:, 2:4] = rng.normal(0.0, 1e-2, size=(N, 2))
+    q = q.reshape(km, jm, im, 5)
+    q[:, :, 0, 1] = 1.0               # inflow plane
+    q[:, :, 0, 2:4] = 0.0
+    if side == BC_SYMMETRY:
+        q[:, 0, :, 2] = 0.0
+        q[:, -1, :, 2] = 0.0
+    nut = np.zeros(N)
+    if turbulence:
+        q[..., 4] = 3.0 / re
+        nut[:] = _sa_fv1(q[..., 4].reshape(-1), re)
+    q = q.reshape(-1)
+    state = dict(q=q.copy(), qn=q.copy(), qnm1=q.copy(), nut=nut)
+    return c, grid, state
+
+
 def channel_alm(im=33, jm=25, km=25, itmax=20, n_tur=1, seed=0):
     """The SA channel with n_tur synthetic rotors (alm_rotor) along x; the
     Reynolds number gives vel_scale = ren 1e-6 / length_scale."""
@@ -321,4 +377,4 @@ def channel_alm(im=33, jm=25, km=25, itmax=20, n_tur=1, seed=0):
     return case, grid, state, spec
 
 
-PRESETS = {"cavity": cavity, "channel": channel, "ogrid": ogrid}
+PRESETS = {"cavity": cavity, "channel": channel, "ogrid": ogrid, "wake": wake}

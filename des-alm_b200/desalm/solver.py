@@ -114,7 +114,7 @@ def lib():
 # kernel classes reported by desalm_kernel_stats (order of the C enum)
 KERNEL_CLASSES = ["dtau", "resid", "sweep_i", "sweep_j", "sweep_k", "recalc", "bcond", "pfix",
                   "nlevel", "prolong", "rsmooth", "norm", "sa_rhs", "sa_sweep", "sa_bc",
-                  "xform_i", "xform_j", "xform_k", "sa_aux", "learn", "alm", "misc"]
+                  "xform_i", "xform_j", "xform_k", "sa_aux", "learn", "alm", "outlet", "misc"]
 
 
 def _p(a):

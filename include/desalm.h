@@ -56,6 +56,7 @@ extern "C" {
 #define DESALM_BC_SYMMETRY  2
 #define DESALM_BC_FREESTREAM 3
 #define DESALM_BC_INFLOW    4
+#define DESALM_BC_OUTLET    5   /* characteristics (LODI) exit; solved on the i = im face */
 #define DESALM_BC_PERIODIC  6
 
 /* Case description: the part of ind3dmg.dat (read in src/init.F90:176-236)

@@ -55,6 +55,7 @@ def lib():
             ("alm_set", [vp, C.POINTER(Alm)]),
             ("alm_set_angle", [vp, ip, C.c_double]),
             ("alm_get", [vp, ip, dp]),
+            ("outlet_rhs", [vp, dp]),
         ]:
             f = getattr(L, "desalm_oracle_" + name)
             f.argtypes = args
@@ -193,6 +194,14 @@ class OracleSolver:
         out = np.zeros(6 * self._alm_n if what == 0 else 3 * N)
         self._ck(self.L.desalm_oracle_alm_get(self.ctx, int(what), _p(out)), "alm_get")
         return out.reshape(-1, 6) if what == 0 else out.reshape(3, N)
+
+    def outlet_rhs(self):
+        """The fine level's residual with the characteristics outlet's on the
+        plane i = im: rh(1:4) there as a (4, km, jm) array."""
+        c = self.case
+        out = np.zeros(4 * c.jm * c.km)
+        self._ck(self.L.desalm_oracle_outlet_rhs(self.ctx, _p(out)), "outlet_rhs")
+        return out.reshape(4, c.km, c.jm)
 
     def phase_times(self):
         t = np.zeros(8)

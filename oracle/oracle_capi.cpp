@@ -33,6 +33,7 @@ struct Base {
   virtual int alm_get(int, double*) = 0;
   virtual int mg_driver(desalm_step_report*) = 0;
   virtual void phase_times(double*) = 0;
+  virtual int outlet_rhs(double*) = 0;
 };
 
 template <class R>
@@ -102,6 +103,20 @@ struct Impl : Base {
     std::vector<R>* v = field(n, f);
     if (!v) return DESALM_EINVAL;
     for (size_t l = 0; l < v->size(); ++l) (*v)[l] = R(in[l]);
+    return 0;
+  }
+  // The fine level's first-pass residual, then the outlet plane's
+  // (mg_brhs + nonreflect_ibc); out = rh(1:4) on the plane i = im, [4][jm*km].
+  int outlet_rhs(double* out) override {
+    orc::Level<R>& G = s.L[0];
+    for (int m = 0; m < 4; ++m) std::fill(G.rh[m].begin(), G.rh[m].end(), R(0));
+    s.residual(G, 0, true, 0);
+    s.outlet_rhs(G);
+    const long P = (long)G.jm * G.km;
+    for (int m = 0; m < 4; ++m)
+      for (int k = 1; k <= G.km; ++k)
+        for (int j = 1; j <= G.jm; ++j)
+          out[m * P + (j - 1) + (long)G.jm * (k - 1)] = double(G.rh[m][G.id(G.im, j, k)]);
     return 0;
   }
   int dims(int n, int* d) override {
@@ -223,8 +238,6 @@ int check_case(const desalm_case* c, std::string& why) {
   if (!c) { why = "null case"; return DESALM_EINVAL; }
   if (c->ng < 1 || c->ng > 4) { why = "ng must be 1..4"; return DESALM_EINVAL; }
   if (c->im < 5 || c->jm < 5 || c->km < 5) { why = "each extent must be >= 5"; return DESALM_EINVAL; }
-  for (int b = 0; b < 6; ++b)
-    if (c->btype[b] == 5) { why = "btype 5 (characteristics outlet) is not supported"; return DESALM_EINVAL; }
   return 0;
 }
 
@@ -284,6 +297,7 @@ void desalm_oracle_phase_times(void* ctx, double* t) { ((Base*)ctx)->phase_times
 int desalm_oracle_alm_set(void* ctx, const desalm_alm* a) { return ((Base*)ctx)->alm_set(a); }
 int desalm_oracle_alm_set_angle(void* ctx, int t, double angle) { return ((Base*)ctx)->alm_angle(t, angle); }
 int desalm_oracle_alm_get(void* ctx, int what, double* out) { return ((Base*)ctx)->alm_get(what, out); }
+int desalm_oracle_outlet_rhs(void* ctx, double* out) { return ((Base*)ctx)->outlet_rhs(out); }
 
 // Standalone LAPACK-style tridiagonal solve (SGTSV restatement) for tests.
 int desalm_oracle_gtsv(int n, int nrhs, double* dl, double* d, double* du, double* b, int ldb, long* npiv) {

@@ -742,6 +742,183 @@ struct Solver {
     phase_s[0] += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   }
 
+  // Characteristics outlet on the front face (btype(2) = 5), fine level,
+  // after the interior residual and the boundary zeroing
+  // (src/solver_daf.F90:318-358): mg_brhs (src/mg_brhs.F90:58-97) forms the
+  // residual of the plane i = im from its eta and zeta derivatives alone --
+  //   brhs_viscous          src/brhs_viscous.F90:40-160
+  //   brhs_diss_p           src/brhs_diss_p.F90:33-89
+  //   brhs_flux_sans_convec src/brhs_flux_sans_convec.F90:45-86
+  //   brhs_convec_quick(2)  src/brhs_convec_quick.F90:41-205
+  //   brhs_unst_visc_diss   src/brhs_unst_visc_diss.F90:30-44
+  // -- then nonreflect_ibc (src/nonreflect_ibc.F90:86-242) adds the LODI
+  // csi terms from the one-sided difference q(im) - q(im-1).  Interior j, k
+  // of the plane only; the plane's edges keep rh = 0.  The back face's call
+  // (inout = 1) writes the plane i = 1, which no later step reads (the solve
+  // starts at i_mysta and the recalculation zeroes it), so it is not made.
+  // nu_t enters the viscous coefficient as in the interior (rei + nu_t; zero
+  // for laminar cases).
+  void outlet_rhs(Level<R>& G) const {
+    const int im = G.im, jm = G.jm, km = G.km, I = im;
+    auto P = [&](int j, int k) { return G.id(I, j, k); };
+    auto pl = [&](int j, int k) { return (long)(j - 1) + (long)jm * (k - 1); };
+    const long NP = (long)jm * km;
+    const R rei = R(1) / R(c.ren), one_fourth = R(0.25);
+    const R de = G.de, dz = G.dz, de4 = R(0.25) * de, dz4 = R(0.25) * dz;
+    const R de2 = R(0.5) * de, dz2 = R(0.5) * dz;
+    const std::vector<R>* Q = G.q;
+    auto ret = [&](long l) { return rei + G.nut[l]; };
+    std::vector<R> ucn[3];
+    for (int d = 0; d < 3; ++d) ucn[d].assign(G.N, R(0));
+    contra_j(G, ucn);
+    // ---- brhs_viscous: visc(1:3) on the plane
+    std::vector<R> visc[3], fv[3];
+    for (int m = 0; m < 3; ++m) { visc[m].assign(NP, R(0)); fv[m].assign(NP, R(0)); }
+    auto face = [&](long l0, long l1, R ue, R ve, R we, R uz, R vz, R wz, bool eta_face, R* out) {
+      R b1 = G.eta[0][l1] + G.eta[0][l0], b2 = G.eta[1][l1] + G.eta[1][l0], b3 = G.eta[2][l1] + G.eta[2][l0];
+      R c1 = G.zet[0][l1] + G.zet[0][l0], c2 = G.zet[1][l1] + G.zet[1][l0], c3 = G.zet[2][l1] + G.zet[2][l0];
+      R uu1 = b1 * ue + c1 * uz, vv1 = b1 * ve + c1 * vz, ww1 = b1 * we + c1 * wz;
+      R uu2 = b2 * ue + c2 * uz, vv2 = b2 * ve + c2 * vz, ww2 = b2 * we + c2 * wz;
+      R uu3 = b3 * ue + c3 * uz, vv3 = b3 * ve + c3 * vz, ww3 = b3 * we + c3 * wz;
+      R vtj = one_fourth * (ret(l1) + ret(l0)) / (G.aj[l1] + G.aj[l0]);
+      if (eta_face) {
+        R c22 = b1 * b1 + b2 * b2 + b3 * b3, c23 = b1 * c1 + b2 * c2 + b3 * c3;
+        out[0] = vtj * (b1 * uu1 + b2 * vv1 + b3 * ww1 + c22 * ue + c23 * uz);
+        out[1] = vtj * (b1 * uu2 + b2 * vv2 + b3 * ww2 + c22 * ve + c23 * vz);
+        out[2] = vtj * (b1 * uu3 + b2 * vv3 + b3 * ww3 + c22 * we + c23 * wz);
+      } else {
+        R c32 = c1 * b1 + c2 * b2 + c3 * b3, c33 = c1 * c1 + c2 * c2 + c3 * c3;
+        out[0] = vtj * (c1 * uu1 + c2 * vv1 + c3 * ww1 + c32 * ue + c33 * uz);
+        out[1] = vtj * (c1 * uu2 + c2 * vv2 + c3 * ww2 + c32 * ve + c33 * vz);
+        out[2] = vtj * (c1 * uu3 + c2 * vv3 + c3 * ww3 + c32 * we + c33 * wz);
+      }
+    };
+    for (int k = 2; k <= km - 1; ++k)
+      for (int j = 1; j <= jm - 1; ++j) {
+        long l0 = P(j, k), l1 = P(j + 1, k);
+        R d[3], z[3], o[3];
+        for (int m = 0; m < 3; ++m) {
+          const std::vector<R>& v = Q[m + 1];
+          d[m] = de * (v[l1] - v[l0]);
+          z[m] = dz4 * (v[P(j + 1, k + 1)] - v[P(j + 1, k - 1)] + v[P(j, k + 1)] - v[P(j, k - 1)]);
+        }
+        face(l0, l1, d[0], d[1], d[2], z[0], z[1], z[2], true, o);
+        for (int m = 0; m < 3; ++m) fv[m][pl(j, k)] = o[m];
+      }
+    for (int k = 2; k <= km - 1; ++k)
+      for (int j = 2; j <= jm - 1; ++j)
+        for (int m = 0; m < 3; ++m) visc[m][pl(j, k)] = de * (fv[m][pl(j, k)] - fv[m][pl(j - 1, k)]);
+    for (int k = 1; k <= km - 1; ++k)
+      for (int j = 2; j <= jm - 1; ++j) {
+        long l0 = P(j, k), l1 = P(j, k + 1);
+        R e[3], z[3], o[3];
+        for (int m = 0; m < 3; ++m) {
+          const std::vector<R>& v = Q[m + 1];
+          e[m] = de4 * (v[P(j + 1, k + 1)] - v[P(j - 1, k + 1)] + v[P(j + 1, k)] - v[P(j - 1, k)]);
+          z[m] = dz * (v[l1] - v[l0]);
+        }
+        face(l0, l1, e[0], e[1], e[2], z[0], z[1], z[2], false, o);
+        for (int m = 0; m < 3; ++m) fv[m][pl(j, k)] = o[m];
+      }
+    for (int k = 2; k <= km - 1; ++k)
+      for (int j = 2; j <= jm - 1; ++j)
+        for (int m = 0; m < 3; ++m)
+          visc[m][pl(j, k)] = visc[m][pl(j, k)] + dz * (fv[m][pl(j, k)] - fv[m][pl(j, k - 1)]);
+    // ---- brhs_diss_p: diss(1) on the plane
+    std::vector<R> aux1(NP, R(0)), aux2(NP, R(0)), diss1(NP, R(0));
+    const std::vector<R>& p = Q[0];
+    const R desq = de * de, dzsq = dz * dz;
+    for (int k = 2; k <= km - 1; ++k)
+      for (int j = 2; j <= jm - 1; ++j) {
+        long l = P(j, k);
+        R g2 = G.eta[0][l] * G.eta[0][l] + G.eta[1][l] * G.eta[1][l] + G.eta[2][l] * G.eta[2][l];
+        aux1[pl(j, k)] = (g2 * G.dtau[l] / G.aj[l]) * (desq * (p[P(j + 1, k)] - R(2) * p[l] + p[P(j - 1, k)]));
+        R g3 = G.zet[0][l] * G.zet[0][l] + G.zet[1][l] * G.zet[1][l] + G.zet[2][l] * G.zet[2][l];
+        aux2[pl(j, k)] = (g3 * G.dtau[l] / G.aj[l]) * (dzsq * (p[P(j, k + 1)] - R(2) * p[l] + p[P(j, k - 1)]));
+      }
+    for (int k = 1; k <= km; ++k) { aux1[pl(1, k)] = aux1[pl(2, k)]; aux1[pl(jm, k)] = aux1[pl(jm - 1, k)]; }
+    for (int j = 1; j <= jm; ++j) { aux2[pl(j, 1)] = aux2[pl(j, 2)]; aux2[pl(j, km)] = aux2[pl(j, km - 1)]; }
+    const R pd = R(c.pdiss_coef);
+    for (int k = 2; k <= km - 1; ++k)
+      for (int j = 2; j <= jm - 1; ++j)
+        diss1[pl(j, k)] = pd * ((aux1[pl(j + 1, k)] - R(2) * aux1[pl(j, k)] + aux1[pl(j - 1, k)]) +
+                                (aux2[pl(j, k + 1)] - R(2) * aux2[pl(j, k)] + aux2[pl(j, k - 1)]));
+    // ---- brhs_flux_sans_convec, brhs_convec_quick(2), brhs_unst_visc_diss
+    const R coef = R(0.125);
+    for (int k = 2; k <= km - 1; ++k)
+      for (int j = 2; j <= jm - 1; ++j) {
+        long l = P(j, k), jp = P(j + 1, k), jn = P(j - 1, k), kp = P(j, k + 1), kn = P(j, k - 1);
+        R r[4];
+        for (int d = 0; d < 3; ++d) {
+          R v = de2 * (p[jp] / G.aj[jp] * G.eta[d][jp] - p[jn] / G.aj[jn] * G.eta[d][jn]);
+          r[d + 1] = v + dz2 * (p[kp] / G.aj[kp] * G.zet[d][kp] - p[kn] / G.aj[kn] * G.zet[d][kn]);
+        }
+        r[0] = R(0) + de2 * (ucn[1][jp] - ucn[1][jn]) + dz2 * (ucn[2][kp] - ucn[2][kn]);
+        const int pos[2] = {j, k}, ext[2] = {jm, km};
+        const long st[2] = {(long)im, (long)im * jm};
+        const R h[2] = {de, dz};
+        for (int d = 0; d < 2; ++d) {
+          R ucon = R(0.5) * ucn[d + 1][l];
+          R up = ucon + std::fabs(ucon), um = ucon - std::fabs(ucon);
+          bool first = pos[d] == 2 || pos[d] == ext[d] - 1;
+          const long s = st[d];
+          for (int m = 0; m < 3; ++m) {
+            const std::vector<R>& v = Q[m + 1];
+            R f;
+            if (first) f = h[d] * (up * (v[l] - v[l - s]) + um * (v[l + s] - v[l]));
+            else
+              f = coef * h[d] * (up * (R(3) * v[l + s] + R(3) * v[l] - R(7) * v[l - s] + v[l - 2 * s]) +
+                                 um * (-R(3) * v[l - s] - R(3) * v[l] + R(7) * v[l + s] - v[l + 2 * s]));
+            r[m + 1] = r[m + 1] + f;
+          }
+        }
+        R dtaj = R(2) * R(c.delti) * G.aj[l];
+        r[0] = r[0] + diss1[pl(j, k)];
+        for (int m = 1; m < 4; ++m) {
+          R dq = es * (R(3) * Q[m][l] - R(4) * G.qn[m][l] + G.qnm1[m][l]) / dtaj;
+          r[m] = r[m] + R(0) + dq - visc[m - 1][pl(j, k)];
+        }
+        // ---- nonreflect_ibc, inout = 2: L_max of the general LODI vector
+        R u = Q[1][l], v = Q[2][l], w = Q[3][l];
+        R ucon = ucn[0][l] * G.aj[l];
+        R c1 = G.csi[0][l], c2 = G.csi[1][l], c3 = G.csi[2][l];
+        R gjj = c1 * c1 + c2 * c2 + c3 * c3;
+        R sg = std::sqrt(gjj);
+        R cj = std::sqrt(ucon * ucon + gjj);
+        long lw = G.id(I - 1, j, k);
+        R dq[4];
+        for (int m = 0; m < 4; ++m) dq[m] = Q[m][l] - Q[m][lw];
+        R lam1 = ucon - cj, lam2 = ucon + cj, lam3 = ucon, lam4 = ucon;
+        R kj = c1 + c2 + c3;
+        R d1 = (c2 - c1 + lam1 * (v - u)) / kj, d2 = (c2 - c1 + lam2 * (v - u)) / kj;
+        R d3 = (c3 - c1 + lam1 * (w - u)) / kj, d4 = (c3 - c1 + lam2 * (w - u)) / kj;
+        R d5 = (c2 - c1 + lam3 * (v - u)) / kj * R(2), d6 = (c3 - c1 + lam4 * (w - u)) / kj * R(2);
+        R cc = R(2) * cj * cj / kj;
+        R si[4][4] = {{-lam2, c1, c2, c3},
+                      {-lam1, c1, c2, c3},
+                      {lam2 * d1 + lam1 * d2, -cc - c1 * d5, cc - c2 * d5, -c3 * d5},
+                      {lam2 * d3 + lam1 * d4, -cc - c1 * d6, -c2 * d6, cc - c3 * d6}};
+        R den = R(2) * cj * cj;
+        R lg[4];
+        for (int a = 0; a < 4; ++a) {
+          R s = R(0);
+          for (int b = 0; b < 4; ++b) s = s + si[a][b] * sg / den * dq[b];
+          lg[a] = s;
+        }
+        lg[0] = lam1 * lg[0]; lg[1] = lam2 * lg[1]; lg[2] = lam3 * lg[2]; lg[3] = lam4 * lg[3];
+        R L1 = 0, L2 = lg[1], L3 = 0, L4 = 0;
+        if (!(ucon < R(0))) { L3 = lg[2]; L4 = lg[3]; }
+        R rh1 = (-cj * L1 + cj * L2) / sg;
+        R rh2 = ((c1 + u * lam1) * L1 + (c1 + u * lam2) * L2 - c2 * L3 - c3 * L4) / sg;
+        R rh3 = ((c2 + v * lam1) * L1 + (c2 + v * lam2) * L2 + (c1 + c3) * L3 - c3 * L4) / sg;
+        R rh4 = ((c3 + w * lam1) * L1 + (c3 + w * lam2) * L2 - c2 * L3 + (c1 + c2) * L4) / sg;
+        G.rh[0][l] = r[0] + rh1 / G.aj[l];
+        G.rh[1][l] = r[1] + rh2 / G.aj[l];
+        G.rh[2][l] = r[2] + rh3 / G.aj[l];
+        G.rh[3][l] = r[3] + rh4 / G.aj[l];
+      }
+  }
+
   // ----------------------------------------------------------- DAF solve
   // Modal quantities of one node (src/rhs_modal_matrices.F90:50-268); each
   // stage of the diagonal solver builds the matrix it needs.
@@ -798,25 +975,32 @@ struct Solver {
     const R dh[3] = {R(0.5) * G.dc, R(0.5) * G.de, R(0.5) * G.dz};
     const R dsq[3] = {G.dc * G.dc, G.de * G.de, G.dz * G.dz};
     const R lam[4] = {0, 0, 1, -1};
+    const bool fine = (n == 0);
     std::vector<R> spr[3];
     spectral_radii(G, spr);
     // r <- S * (-dtau * rh * J) (src/rhs_diag_solver.F90:53-72)
     const R alpha_mult = es * R(1.5) / R(c.delti);
+    // idend (src/solver_daf.F90:371-373): the fine level's characteristics
+    // outlet plane i = im is solved with the interior
+    const int ie = (n == 0 && c.btype[1] == 5) ? im : im - 1;
     ORC_PARFOR
     for (int k = 2; k <= km - 1; ++k)
       for (int j = 2; j <= jm - 1; ++j)
-        for (int i = 2; i <= im - 1; ++i) {
+        for (int i = 2; i <= ie; ++i) {
           long l = G.id(i, j, k);
           R alpha = R(1) + alpha_mult * G.dtau[l];
           R s[4] = {beta, R(1) / alpha, R(1) / alpha, R(1) / alpha};
           for (int m = 0; m < 4; ++m) G.rh[m][l] = s[m] * (-G.dtau[l] * G.rh[m][l] * G.aj[l]);
         }
-    const bool fine = (n == 0);
     // one line of one direction: ids = interior node ids along the line,
     // lprev / lnext = the boundary nodes before and after it; bw / be = the
     // semi-explicit boundary vectors (brh) or null.  Scratch is per call, so
     // lines may be solved concurrently.
-    auto sweep_line = [&](int dir, const std::vector<long>& ids, long lprev, long lnext, const R* bw, const R* be) {
+    // With outrow the last node is the characteristics outlet node i = im
+    // and its row is (src/rhs_diag_solver.F90:207-221): ap = 1, 1,
+    // 1 + dtau dc spr, 1; aw = 0, 0, -dtau(im-1) dc spr(im-1), 0.
+    auto sweep_line = [&](int dir, const std::vector<long>& ids, long lprev, long lnext, const R* bw, const R* be,
+                          bool outrow = false) {
       int len = (int)ids.size();
       std::vector<R> aw(len, 0), ap(len, 0), ae(len, 0), aq(len, 0), dl, du;
       long piv = 0;
@@ -835,6 +1019,14 @@ struct Solver {
           aw[p] = (m < 2) ? -tmp : (-ddsw * lam[m] - tmp);
           ae[p] = (m < 2) ? -tmp : (ddse * lam[m] - tmp);
           aq[p] = G.rh[m][l];
+        }
+        if (outrow) {
+          const int p = len - 1;
+          const long l = ids[p], lw = ids[p - 1];
+          R dds = G.dtau[l] * G.dc * spr[0][l];
+          ap[p] = m == 2 ? R(1) + dds * lam[2] : R(1);
+          R ddw = G.dtau[lw] * G.dc * spr[0][lw];
+          aw[p] = m == 2 ? -ddw * lam[2] : R(0);
         }
         if (bw) aq[0] = aq[0] - aw[0] * bw[m];
         if (be) aq[len - 1] = aq[len - 1] - ae[len - 1] * be[m];
@@ -874,16 +1066,16 @@ struct Solver {
       ORC_PARFOR
       for (int k = 2; k <= km - 1; ++k)
         for (int j = 2; j <= jm - 1; ++j)
-          for (int i = 2; i <= im - 1; ++i) { long l = G.id(i, j, k); xform(l, mat_mai(G, l)); }
+          for (int i = 2; i <= ie; ++i) { long l = G.id(i, j, k); xform(l, mat_mai(G, l)); }
       if (bback)
         for (int k = 2; k <= km - 1; ++k)
           for (int j = 2; j <= jm - 1; ++j) xvec(&brh[bo(j, k)], mat_mai(G, G.id(1, j, k)));
 ORC_PARFOR
       for (int k = 2; k <= km - 1; ++k)
         for (int j = 2; j <= jm - 1; ++j) {
-          std::vector<long> ids(im - 2);
-          for (int i = 2; i <= im - 1; ++i) ids[i - 2] = G.id(i, j, k);
-          sweep_line(0, ids, G.id(1, j, k), G.id(im, j, k), bback ? &brh[bo(j, k)] : nullptr, nullptr);
+          std::vector<long> ids(ie - 1);
+          for (int i = 2; i <= ie; ++i) ids[i - 2] = G.id(i, j, k);
+          sweep_line(0, ids, G.id(1, j, k), G.id(im, j, k), bback ? &brh[bo(j, k)] : nullptr, nullptr, ie == im);
         }
     }
     // ---- eta sweep (src/rhs_diag_solver.F90:265-434)
@@ -892,7 +1084,7 @@ ORC_PARFOR
       bool bl = fine && c.btype[2] != 5, br = fine && c.btype[3] != 5;
       auto bo = [&](int i, int k) { return (long)4 * ((i - 1) + (long)im * (k - 1)); };
       for (int k = 2; k <= km - 1; ++k)
-        for (int i = 2; i <= im - 1; ++i) {
+        for (int i = 2; i <= ie; ++i) {
           R r1[4], r2[4];
           if (bl) { getr(G.id(i, 2, k), r1); getr(G.id(i, 3, k), r2); sabc(2, r1, r2, &b1[bo(i, k)]); }
           if (br) { getr(G.id(i, jm - 1, k), r1); getr(G.id(i, jm - 2, k), r2); sabc(3, r1, r2, &b2[bo(i, k)]); }
@@ -900,15 +1092,15 @@ ORC_PARFOR
       ORC_PARFOR
       for (int k = 2; k <= km - 1; ++k)
         for (int j = 2; j <= jm - 1; ++j)
-          for (int i = 2; i <= im - 1; ++i) { long l = G.id(i, j, k); xform(l, mat_n1i(G, l)); }
+          for (int i = 2; i <= ie; ++i) { long l = G.id(i, j, k); xform(l, mat_n1i(G, l)); }
       for (int k = 2; k <= km - 1; ++k)
-        for (int i = 2; i <= im - 1; ++i) {
+        for (int i = 2; i <= ie; ++i) {
           if (bl) xvec(&b1[bo(i, k)], mat_n1i(G, G.id(i, 1, k)));
           if (br) xvec(&b2[bo(i, k)], mat_n1i(G, G.id(i, jm, k)));
         }
 ORC_PARFOR
       for (int k = 2; k <= km - 1; ++k)
-        for (int i = 2; i <= im - 1; ++i) {
+        for (int i = 2; i <= ie; ++i) {
           std::vector<long> ids(jm - 2);
           for (int j = 2; j <= jm - 1; ++j) ids[j - 2] = G.id(i, j, k);
           sweep_line(1, ids, G.id(i, 1, k), G.id(i, jm, k), bl ? &b1[bo(i, k)] : nullptr, br ? &b2[bo(i, k)] : nullptr);
@@ -923,7 +1115,7 @@ ORC_PARFOR
       bool bu_set = fine && c.btype[5] != 6, bu_use = fine && c.btype[5] != 5;
       auto bo = [&](int i, int j) { return (long)4 * ((i - 1) + (long)im * (j - 1)); };
       for (int j = 2; j <= jm - 1; ++j)
-        for (int i = 2; i <= im - 1; ++i) {
+        for (int i = 2; i <= ie; ++i) {
           R r1[4], r2[4];
           if (bd) { getr(G.id(i, j, 2), r1); getr(G.id(i, j, 3), r2); sabc(4, r1, r2, &b1[bo(i, j)]); }
           if (bu_set) { getr(G.id(i, j, km - 1), r1); getr(G.id(i, j, km - 2), r2); sabc(5, r1, r2, &b2[bo(i, j)]); }
@@ -931,15 +1123,15 @@ ORC_PARFOR
       ORC_PARFOR
       for (int k = 2; k <= km - 1; ++k)
         for (int j = 2; j <= jm - 1; ++j)
-          for (int i = 2; i <= im - 1; ++i) { long l = G.id(i, j, k); xform(l, mat_n2i(G, l)); }
+          for (int i = 2; i <= ie; ++i) { long l = G.id(i, j, k); xform(l, mat_n2i(G, l)); }
       for (int j = 2; j <= jm - 1; ++j)
-        for (int i = 2; i <= im - 1; ++i) {
+        for (int i = 2; i <= ie; ++i) {
           if (bd) xvec(&b1[bo(i, j)], mat_n2i(G, G.id(i, j, 1)));
           if (bu_use) xvec(&b2[bo(i, j)], mat_n2i(G, G.id(i, j, km)));
         }
 ORC_PARFOR
       for (int j = 2; j <= jm - 1; ++j)
-        for (int i = 2; i <= im - 1; ++i) {
+        for (int i = 2; i <= ie; ++i) {
           std::vector<long> ids(km - 2);
           for (int k = 2; k <= km - 1; ++k) ids[k - 2] = G.id(i, j, k);
           sweep_line(2, ids, G.id(i, j, 1), G.id(i, j, km), bd ? &b1[bo(i, j)] : nullptr, bu_use ? &b2[bo(i, j)] : nullptr);
@@ -949,7 +1141,7 @@ ORC_PARFOR
     ORC_PARFOR
     for (int k = 2; k <= km - 1; ++k)
       for (int j = 2; j <= jm - 1; ++j)
-        for (int i = 2; i <= im - 1; ++i) { long l = G.id(i, j, k); xform(l, mat_mc(G, l)); }
+        for (int i = 2; i <= ie; ++i) { long l = G.id(i, j, k); xform(l, mat_mc(G, l)); }
     phase_s[1] += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   }
 
@@ -1151,12 +1343,16 @@ ORC_PARFOR
     const int im = G.im, jm = G.jm, km = G.km;
     for (int m = 0; m < 4; ++m) std::fill(G.rh[m].begin(), G.rh[m].end(), R(0));
     residual(G, n, true, itr == 1 ? 1 : 0);
+    const bool outlet = n == 0 && c.btype[1] == 5;
+    if (outlet) outlet_rhs(G);
     if (n == 0 && alm_on) rhs_lines(G);  // src/solver_daf.F90:378-381
     diag_solver(G, n);
+    // q <- qold_af + rh up to idend (src/solver_daf.F90:409-418)
+    const int ie = outlet ? im : im - 1;
     ORC_PARFOR
     for (int k = 2; k <= km - 1; ++k)
       for (int j = 2; j <= jm - 1; ++j)
-        for (int i = 2; i <= im - 1; ++i) {
+        for (int i = 2; i <= ie; ++i) {
           long l = G.id(i, j, k);
           for (int m = 0; m < 4; ++m) G.q[m][l] = G.q[m][l] + G.rh[m][l];
         }
@@ -1568,6 +1764,7 @@ ORC_PARFOR
         for (int j = 1; j <= jm; ++j) {
           if (bt == 1) Q(i, j, k) = zero;
           else if (bt == 2 || bt == 3) Q(i, j, k) = sa[0][b] * Q(i + s, j, k) + sb[0][b] * Q(i + 2 * s, j, k);
+          else if (bt == 5) Q(i, j, k) = (one + ratv(b, j, k)) * Q(i + s, j, k) - ratv(b, j, k) * Q(i + 2 * s, j, k);
           else if (bt == 6) Q(i, j, k) = Q(side ? 2 : im - 1, j, k);
           else if (bt == 8 && side == 1) Q(i, j, k) = Q(i - 1, j, k);
         }
@@ -1579,6 +1776,7 @@ ORC_PARFOR
         for (int i = 1; i <= im; ++i) {
           if (bt == 1) Q(i, j, k) = zero;
           else if (bt == 2 || bt == 3) Q(i, j, k) = sa[0][b] * Q(i, j + s, k) + sb[0][b] * Q(i, j + 2 * s, k);
+          else if (bt == 5) Q(i, j, k) = (one + ratv(b, i, k)) * Q(i, j + s, k) - ratv(b, i, k) * Q(i, j + 2 * s, k);
           else if (bt == 6) Q(i, j, k) = Q(i, side ? 2 : jm - 1, k);
         }
     }
@@ -1589,6 +1787,7 @@ ORC_PARFOR
         for (int i = 1; i <= im; ++i) {
           if (bt == 1) Q(i, j, k) = zero;
           else if (bt == 2 || bt == 3) Q(i, j, k) = sa[0][b] * Q(i, j, k + s) + sb[0][b] * Q(i, j, k + 2 * s);
+          else if (bt == 5) Q(i, j, k) = (one + ratv(b, i, j)) * Q(i, j, k + s) - ratv(b, i, j) * Q(i, j, k + 2 * s);
           else if (bt == 6) Q(i, j, k) = Q(i, j, side ? 2 : km - 1);
         }
     }

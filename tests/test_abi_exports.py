@@ -42,7 +42,7 @@ def test_invalid_case_is_rejected_without_gpu():
         Solver(case)
     assert "odd extents" in str(e.value)
     case.im = 17
-    case.btype[1] = 5
+    case.ifix = 18
     with pytest.raises(DesalmError) as e:
         Solver(case)
-    assert "btype 5" in str(e.value)
+    assert "pressure reference node" in str(e.value)
