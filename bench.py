@@ -15,7 +15,8 @@ ours:       value = device-timed seconds per physical step of the product
             predictor_ab compares the three initial guesses (q^n, linear
             extrapolation, the learned network) by iterations and seconds per
             physical step to an absolute tolerance on the laminar cavity, and
-            alm gives the cost of the actuator-line forcing.
+            alm gives the cost of the actuator-line forcing, outlet that
+            of the characteristics outlet on an open wake box.
 reference:  the CPU oracle (C++ restatement of the reference, FP32 like the
             reference's own build, its loops on every host thread) on the same
             case; a bounded sample of pseudo-iterations scaled to one physical
@@ -224,6 +225,37 @@ def run_ours(args, rank, world, dist):
             del S
         return res
 
+    def outlet_cost(steps=2):
+        """Characteristics outlet (btype 5) on the SA wake box 129x97x65 (MIXED,
+        graph path): seconds and pseudo-iterations per physical step with the
+        outlet and with a first-order extrapolation exit (btype 3) on the same
+        grid and state, and the outlet kernel's time per pseudo-iteration from
+        one profiled (eager) step."""
+        case, grid, state = cases.wake(im=129, jm=97, km=65, turbulence=1, itmax=200)
+        case.precision_mode = abi.MIXED
+        case.predictor = abi.PRED_LINEAR
+        case.use_graph = 1
+        res = {"workload": "SA wake box 129x97x65, MIXED, uniform inflow, outlet at i = im, itmax 200"}
+        for name, bt in (("extrapolation_exit", abi.BC_FREESTREAM), ("outlet", abi.BC_OUTLET)):
+            c = case.copy()
+            c.btype[1] = bt
+            S = Solver(c)
+            S.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
+            S.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
+            S.mg_driver()
+            sec, reps = timed_steps(S, steps, S.mg_driver)
+            its = float(np.mean([r["iterations"] for r in reps]))
+            res[name] = {"s_per_step": sec, "pseudo_iterations_per_step": its, "ms_per_iteration": 1e3 * sec / its}
+            if bt == abi.BC_OUTLET:
+                S.profile(True)
+                r = S.mg_driver()
+                stats, _ = S.kernel_stats()
+                S.profile(False)
+                ms = sum(v[0] for v in stats.get("outlet", {}).values())
+                res["outlet_kernel_ms_per_iteration"] = ms / max(1, r["iterations"])
+            del S
+        return res
+
     def timed_steps(S, K, body):
         """K calls of body(), bracketed by barrier + synchronize, CUDA events
         on the library's stream; returns seconds per call (max over ranks)."""
@@ -341,6 +373,7 @@ def run_ours(args, rank, world, dist):
 
     ab = predictor_ab() if not args.no_ab else None
     alm = alm_cost() if not args.no_ab else None
+    outlet = outlet_cost() if not args.no_ab else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -368,6 +401,7 @@ def run_ours(args, rank, world, dist):
         "cell_updates_per_s": sum_over_ranks(cell_updates),
         "predictor_ab": ab,
         "alm": alm,
+        "outlet": outlet,
         "e2e": {"value": e2e_sec, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "kernel": kind, "level": "fine", "achieved": achieved, "peak": peak, "unit": "GB/s",
