@@ -26,6 +26,7 @@
 #include "learn_tc.cuh"
 #include "alm.cuh"
 #include "outlet.cuh"
+#include "wallfn.cuh"
 
 using namespace desalm;
 
@@ -232,7 +233,7 @@ inline unsigned cdiv(long a, long b) { return (unsigned)((a + b - 1) / b); }
 // kernel classes for desalm_kernel_stats
 enum KClass { KC_DTAU = 0, KC_RESID, KC_SWEEP_I, KC_SWEEP_J, KC_SWEEP_K, KC_RECALC, KC_BCOND, KC_PFIX,
               KC_NLEVEL, KC_PROLONG, KC_RSMOOTH, KC_NORM, KC_SA_RHS, KC_SA_SWEEP, KC_SA_BC,
-              KC_XFORM_I, KC_XFORM_J, KC_XFORM_K, KC_SA_AUX, KC_LEARN, KC_ALM, KC_OUTLET, KC_MISC, KC_COUNT };
+              KC_XFORM_I, KC_XFORM_J, KC_XFORM_K, KC_SA_AUX, KC_LEARN, KC_ALM, KC_OUTLET, KC_WALLFN, KC_MISC, KC_COUNT };
 
 struct ProfScope {
   desalm_ctx* ctx;
@@ -307,6 +308,7 @@ int check_case(desalm_ctx* ctx, const desalm_case& c) {
   if ((c.icrs != 0 && c.icrs != 1) || (c.jcrs != 0 && c.jcrs != 1) || (c.kcrs != 0 && c.kcrs != 1))
     return bad("icrs/jcrs/kcrs must be 0 or 1");
   if (c.precision_mode != DESALM_FP64 && c.precision_mode != DESALM_MIXED) return bad("unknown precision_mode");
+  if (c.wall_functions != 0 && c.wall_functions != 1) return bad("wall_functions must be 0 or 1");
   if (c.predictor != DESALM_PRED_QN && c.predictor != DESALM_PRED_LINEAR && c.predictor != DESALM_PRED_LEARNED)
     return bad("unknown predictor");
   if (c.ifix < 1 || c.ifix > c.im || c.jfix < 1 || c.jfix > c.jm || c.kfix < 1 || c.kfix > c.km)
@@ -642,6 +644,22 @@ int do_daf(desalm_ctx* ctx, int n, int recalc, int itr) {
 int do_bcond(desalm_ctx* ctx) {
   Level& G = ctx->L[0];
   return kind_of(ctx, 0) == K_DD ? launch_bcond(ctx, G.dd) : launch_bcond(ctx, G.df);
+}
+
+// wf_eta(1) and wf_eta(2) on the fine level (src/mg_driver.F90:221-224)
+template <class T, class W>
+int launch_wallfn(desalm_ctx* ctx, Lv<T, W>& L) {
+  Par P = ctx->par;
+  P.fine = 1;
+  LAUNCH(KC_WALLFN, 0, 2.0 * (L.im - 2) * (L.km - 2),
+         launch_k(k_wallfn<T, W>, dim3(cdiv(L.im - 2, 32), cdiv(L.km - 2, 4), 2), dim3(32, 4), 0, ctx->stream, L, P,
+                  (const double*)ctx->x, (const double*)ctx->y, (const double*)ctx->z, (const double*)ctx->wd));
+  CKL();
+  return 0;
+}
+int do_wallfn(desalm_ctx* ctx) {
+  Level& G = ctx->L[0];
+  return kind_of(ctx, 0) == K_DD ? launch_wallfn(ctx, G.dd) : launch_wallfn(ctx, G.df);
 }
 
 int do_nlevel(desalm_ctx* ctx, int n) {  // n = coarse level index (>= 1)
@@ -1464,6 +1482,14 @@ int desalm_des_eddy(desalm_ctx* ctx) {
   return 0;
 }
 
+int desalm_wall_functions(desalm_ctx* ctx) {
+  if (!ctx) return DESALM_EINVAL;
+  if (ctx->L.empty()) return DESALM_ENOTREADY;
+  RET(do_wallfn(ctx));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
 int desalm_conservation(desalm_ctx* ctx) {
   if (!ctx) return DESALM_EINVAL;
   RET(sa_conservation(ctx));
@@ -1586,6 +1612,7 @@ int enqueue_iteration(desalm_ctx* ctx) {
       // the recalculated residual on the coarsest level feeds nothing
       int rc_eff = (n == ctx->ng - 1) ? 0 : recalc;
       RET(do_daf(ctx, n, rc_eff, itr));
+      if (c.wall_functions && n == 0) RET(do_wallfn(ctx));
     }
   }
   for (int n = ctx->ng - 2; n >= 0; --n) RET(do_prolong(ctx, n));

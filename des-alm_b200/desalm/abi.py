@@ -55,7 +55,8 @@ class Case(C.Structure):
         ("precision_mode", C.c_int),
         ("predictor", C.c_int),
         ("use_graph", C.c_int),
-        ("reserved", C.c_int * 6),
+        ("wall_functions", C.c_int),
+        ("reserved", C.c_int * 5),
     ]
 
     def copy(self):

@@ -141,10 +141,12 @@ def _sa_fv1(nut_tilde, ren):
     return nut_tilde * chic / (chic + 357.911)
 
 
-def channel(im=129, jm=97, km=65, seed=0, re_tau=395.0, itmax=400):
+def channel(im=129, jm=97, km=65, seed=0, re_tau=395.0, itmax=400, wall_first=None):
     """SA channel: i streamwise (2 pi), j wall-normal (walls at j = 1, jm),
     k spanwise (pi); half height 1, bulk velocity ~ 1.  Re based on the half
-    height and bulk velocity (6875 for Re_tau = 395, Dean's correlation)."""
+    height and bulk velocity (6875 for Re_tau = 395, Dean's correlation).
+    The first wall spacing is 1 / Re_tau (y+ ~ 1) unless wall_first gives it
+    (a coarse wall spacing, for the wall functions)."""
     rng = np.random.default_rng(seed)
     c = _base_case(im, jm, km)
     re_b = 2.0 * (re_tau / 0.09) ** (1.0 / 0.88)   # Re_bulk on 2 delta
@@ -158,7 +160,7 @@ def channel(im=129, jm=97, km=65, seed=0, re_tau=395.0, itmax=400):
     c.ifix, c.jfix, c.kfix = im // 2, jm // 2, km // 2
     xs = np.linspace(0.0, 2 * np.pi, im)
     zs = np.linspace(0.0, np.pi, km)
-    ys = _tanh_stretch(jm, 1.0 / re_tau)
+    ys = _tanh_stretch(jm, wall_first if wall_first else 1.0 / re_tau)
     X, Y, Z = _mesh(xs, ys, zs)
     wd = np.minimum(Y, 2.0 - Y)
     grid = dict(x=_flat(X), y=_flat(Y), z=_flat(Z), wd=_flat(wd))

@@ -57,6 +57,7 @@ def lib():
             ("bcond_fm", [vp]),
             ("des_eddy", [vp]),
             ("conservation", [vp]),
+            ("wall_functions", [vp]),
             ("save_qold", [vp]),
             ("begin_step", [vp]),
             ("pseudo_iteration", [vp, C.POINTER(StepReport)]),
@@ -114,7 +115,7 @@ def lib():
 # kernel classes reported by desalm_kernel_stats (order of the C enum)
 KERNEL_CLASSES = ["dtau", "resid", "sweep_i", "sweep_j", "sweep_k", "recalc", "bcond", "pfix",
                   "nlevel", "prolong", "rsmooth", "norm", "sa_rhs", "sa_sweep", "sa_bc",
-                  "xform_i", "xform_j", "xform_k", "sa_aux", "learn", "alm", "outlet", "misc"]
+                  "xform_i", "xform_j", "xform_k", "sa_aux", "learn", "alm", "outlet", "wallfn", "misc"]
 
 
 def _p(a):
@@ -258,6 +259,9 @@ class Solver:
 
     def conservation(self):
         self._ck(self.L.desalm_conservation(self.ctx), "conservation")
+
+    def wall_functions(self):
+        self._ck(self.L.desalm_wall_functions(self.ctx), "wall_functions")
 
     def save_qold(self):
         self._ck(self.L.desalm_save_qold(self.ctx), "save_qold")

@@ -86,7 +86,10 @@ typedef struct desalm_case {
     int    precision_mode;  /* DESALM_FP64 or DESALM_MIXED                      */
     int    predictor;       /* DESALM_PRED_*                                    */
     int    use_graph;       /* 1: replay each pseudo-iteration as a CUDA graph  */
-    int    reserved[6];
+    int    wall_functions;  /* 1: wf_eta(1) and wf_eta(2) after every fine DAF
+                               step (src/mg_driver.F90:221-224); 0 (the
+                               default): off, as for wall-resolved grids     */
+    int    reserved[5];
 } desalm_case;
 
 /* Outcome of one physical time step (desalm_mg_driver). */
@@ -167,6 +170,17 @@ int  desalm_bcond_fm(desalm_ctx* ctx);
 int  desalm_des_eddy(desalm_ctx* ctx);
 /* Outlet mass-flux correction: src/conservation.F90:2-162. */
 int  desalm_conservation(desalm_ctx* ctx);
+/* Log-law wall functions on the fine level's j walls, wf_eta(1) and
+ * wf_eta(2) (src/wf_mpi.F90:246-413), which the reference's mg_driver calls
+ * after every fine solver_daf (src/mg_driver.F90:221-224);
+ * desalm_mg_driver / desalm_pseudo_iteration do the same when
+ * desalm_case.wall_functions = 1.  Layer 2 (j = 2 and jm-1) gets the wall
+ * law's speed at its wall distance in the direction of layer 3's
+ * wall-parallel velocity, and nu_tilde = kappa y+ / Re; u_tau solves the
+ * reference's wall law (funcv, src/wf_mpi.F90:602-628) to full precision,
+ * where the reference stops its Newton search at |F| < 1e-4.  Needs the
+ * wall distance given to desalm_set_grid. */
+int  desalm_wall_functions(desalm_ctx* ctx);
 /* qold_mg <- q on the fine level (src/mg_driver.F90:98-100). */
 int  desalm_save_qold(desalm_ctx* ctx);
 /* Start of a physical time step (src/mg_driver.F90:42-75): qnm1 <- qn,

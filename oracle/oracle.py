@@ -48,6 +48,7 @@ def lib():
             ("bcond_fm", [vp]),
             ("des_eddy", [vp]),
             ("conservation", [vp]),
+            ("wall_functions", [vp]),
             ("save_qold", [vp]),
             ("begin_step", [vp]),
             ("pseudo_iteration", [vp, C.POINTER(StepReport)]),
@@ -160,6 +161,9 @@ class OracleSolver:
 
     def conservation(self):
         self._ck(self.L.desalm_oracle_conservation(self.ctx), "conservation")
+
+    def wall_functions(self):
+        self._ck(self.L.desalm_oracle_wall_functions(self.ctx), "wall_functions")
 
     def save_qold(self):
         self._ck(self.L.desalm_oracle_save_qold(self.ctx), "save_qold")

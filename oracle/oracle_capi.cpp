@@ -25,6 +25,7 @@ struct Base {
   virtual int bcond() = 0;
   virtual int des_eddy() = 0;
   virtual int conservation() = 0;
+  virtual int wall_functions() = 0;
   virtual int save_qold() = 0;
   virtual int begin_step() = 0;
   virtual int pseudo_iteration(desalm_step_report*) = 0;
@@ -200,6 +201,7 @@ struct Impl : Base {
   int bcond() override { s.bcond_fm(); return 0; }
   int des_eddy() override { s.des_eddy(); return 0; }
   int conservation() override { s.conservation(); return 0; }
+  int wall_functions() override { s.wall_functions(); return 0; }
   int save_qold() override { s.save_qold(); return 0; }
   int begin_step() override { s.begin_step(); return 0; }
   int pseudo_iteration(desalm_step_report* rep) override {
@@ -289,6 +291,7 @@ int desalm_oracle_mg_residual(void* ctx, int n, double* r) { return ((Base*)ctx)
 int desalm_oracle_bcond_fm(void* ctx) { return ((Base*)ctx)->bcond(); }
 int desalm_oracle_des_eddy(void* ctx) { return ((Base*)ctx)->des_eddy(); }
 int desalm_oracle_conservation(void* ctx) { return ((Base*)ctx)->conservation(); }
+int desalm_oracle_wall_functions(void* ctx) { return ((Base*)ctx)->wall_functions(); }
 int desalm_oracle_save_qold(void* ctx) { return ((Base*)ctx)->save_qold(); }
 int desalm_oracle_begin_step(void* ctx) { return ((Base*)ctx)->begin_step(); }
 int desalm_oracle_pseudo_iteration(void* ctx, desalm_step_report* r) { return ((Base*)ctx)->pseudo_iteration(r); }

@@ -39,6 +39,7 @@
 #define ORC_PARFOR
 #endif
 #include <algorithm>
+#include <limits>
 #include <stdexcept>
 #include <chrono>
 #include "desalm.h"
@@ -1801,6 +1802,102 @@ ORC_PARFOR
     }
   }
 
+  // Friction velocity u_tau of the wall law the reference solves
+  // (funcv, src/wf_mpi.F90:602-628, ks = 0): with c = Re y,
+  //   c u_tau^2 = u0                          when c u_tau <= 11.3,
+  //   u_tau (ln(c u_tau) / kappa + B) = u0    when c u_tau > 11.3,
+  // and funcv's zero band at c u_tau = 11.3 (:627) taken as the root where
+  // u0 falls in the jump between the two branches.  The reference finds it
+  // with a third-party Newton / line-search driver stopped at |F| < 1e-4
+  // (:640); this restatement solves the equation to full precision: the
+  // linear branch in closed form, the log branch (convex, increasing) by
+  // Newton's method from the branch point, whose first step lands right of
+  // the root and whose later steps decrease monotonically onto it.
+  static R wf_utau(R u0, R c) {
+    const R kapa = R(0.41), blog = R(5.45), yk = R(11.3);
+    if (!(c > R(0)) || !(u0 > R(0))) return R(0);
+    if (c * u0 <= yk * yk) return std::sqrt(u0 / c);
+    const R us = yk / c;
+    if (us * (std::log(yk) / kapa + blog) >= u0) return us;
+    R ut = us;
+    for (int it = 0; it < 100; ++it) {
+      const R lg = std::log(c * ut);
+      const R g = ut * (lg / kapa + blog) - u0;
+      const R dg = lg / kapa + blog + R(1) / kapa;
+      const R nx = ut - g / dg;
+      const bool done = std::fabs(nx - ut) <= R(4) * std::numeric_limits<R>::epsilon() * nx;
+      ut = nx;
+      if (done) break;
+    }
+    return ut;
+  }
+
+  // wf_eta(jb) (src/wf_mpi.F90:246-413) on the fine level, jb = 1 (j = 1
+  // wall, layers j = 2, 3) and jb = 2 (j = jm wall, layers jm-1, jm-2); the
+  // driver calls both after every fine solver_daf (src/mg_driver.F90:
+  // 221-224).  u_tau comes from the wall-parallel speed at layer 3 and its
+  // wall distance; the velocity at layer 2 is set to the wall law's speed at
+  // layer 2's wall distance, in the direction of layer 3's velocity resolved
+  // along the wall's csi and zeta lines; nu_tilde there to kappa y+ / Re.
+  // Interior (i, k) only.  A wall-parallel speed whose square root argument
+  // rounds below zero is taken as zero (the reference's sqrt would return
+  // NaN there).
+  void wall_functions() {
+    Level<R>& G = L[0];
+    const int im = G.im, jm = G.jm, km = G.km;
+    const R kapa = R(0.41), blog = R(5.45), yplm = R(11.3), qmin = R(1.0E-08);
+    const R ren = R(c.ren), half = R(0.5);
+    std::vector<R>* Q = G.q;
+    for (int jb = 1; jb <= 2; ++jb) {
+      const int j = jb == 1 ? 1 : jm, j1 = jb == 1 ? 2 : jm - 1, j2 = jb == 1 ? 3 : jm - 2;
+      std::vector<R> ut0((long)im * km, R(0));
+      auto uo = [&](int i, int k) -> R& { return ut0[(long)(i - 1) + (long)im * (k - 1)]; };
+      for (int k = 2; k <= km - 1; ++k)
+        for (int i = 2; i <= im - 1; ++i) {
+          long l = G.id(i, j, k), l2 = G.id(i, j2, k);
+          R vmod = std::sqrt(G.eta[0][l] * G.eta[0][l] + G.eta[1][l] * G.eta[1][l] + G.eta[2][l] * G.eta[2][l]);
+          R qnor = (Q[1][l2] * G.eta[0][l] + Q[2][l2] * G.eta[1][l] + Q[3][l2] * G.eta[2][l]) / vmod;
+          R qpar = Q[1][l2] * Q[1][l2] + Q[2][l2] * Q[2][l2] + Q[3][l2] * Q[3][l2];
+          qpar = std::sqrt(std::max(qpar - qnor * qnor, R(0)));
+          uo(i, k) = wf_utau(qpar, ren * G.wd[l2]);
+        }
+      for (int k = 2; k <= km - 1; ++k)
+        for (int i = 2; i <= im - 1; ++i) {
+          long l1 = G.id(i, j1, k), l2 = G.id(i, j2, k);
+          R qsq = Q[1][l2] * Q[1][l2] + Q[2][l2] * Q[2][l2] + Q[3][l2] * Q[3][l2];
+          if (qsq > qmin) {
+            const R ut = uo(i, k);
+            R yplus = G.wd[l1] * ren * ut;
+            R q2 = yplus > yplm ? (std::log(yplus) / kapa + blog) * ut : yplus * ut;
+            long lu = G.id(i + 1, j, k), ld = G.id(i - 1, j, k);
+            R xc = half * (G.x[lu] - G.x[ld]), yc = half * (G.y[lu] - G.y[ld]), zc = half * (G.z[lu] - G.z[ld]);
+            lu = G.id(i, j, k + 1); ld = G.id(i, j, k - 1);
+            R xz = half * (G.x[lu] - G.x[ld]), yz = half * (G.y[lu] - G.y[ld]), zz = half * (G.z[lu] - G.z[ld]);
+            R sg11 = std::sqrt(xc * xc + yc * yc + zc * zc);
+            R sg33 = std::sqrt(xz * xz + yz * yz + zz * zz);
+            R qc1 = (G.csi[0][l2] * Q[1][l2] + G.csi[1][l2] * Q[2][l2] + G.csi[2][l2] * Q[3][l2]) * sg11;
+            R qc2 = (G.zet[0][l2] * Q[1][l2] + G.zet[1][l2] * Q[2][l2] + G.zet[2][l2] * Q[3][l2]) * sg33;
+            R cgama = (xc * xz + yc * yz + zc * zz) / (sg11 * sg33);
+            R fb = std::sqrt(qc1 * qc1 + qc2 * qc2 + R(2) * qc1 * qc2 * cgama);
+            fb = (qc1 + qc2 * cgama) / fb;
+            fb = std::min(fb, R(1));
+            fb = std::max(fb, R(-1));
+            R fbeta = qc2 > R(0) ? std::acos(fb) : -std::acos(fb);
+            R qstar = q2;
+            R c2 = qstar * std::sin(fbeta) / std::sin(std::acos(cgama));
+            R c1 = qstar * std::cos(fbeta) - c2 * cgama;
+            Q[1][l1] = c1 * xc / sg11 + c2 * xz / sg33;
+            Q[2][l1] = c1 * yc / sg11 + c2 * yz / sg33;
+            Q[3][l1] = c1 * zc / sg11 + c2 * zz / sg33;
+            Q[4][l1] = kapa * yplus / ren;
+          } else {
+            Q[1][l1] = Q[2][l1] = Q[3][l1] = R(0);
+            Q[4][l1] = R(0.1) / ren;
+          }
+        }
+    }
+  }
+
   // conservation (src/conservation.F90:64-160): on one rank the first and
   // last i planes are the domain's inflow and outflow planes.
   void conservation() {
@@ -1854,6 +1951,7 @@ ORC_PARFOR
         if (n != ng - 1) recalc = (itr != c.iter[n]) ? 0 : 1;  // kept at n = ng (Q5)
         if (c.turbulence && n == 0) des_eddy();
         solver_daf(n, recalc, itr);
+        if (c.wall_functions && n == 0) wall_functions();  // src/mg_driver.F90:221-224
       }
     }
     for (int n = ng - 2; n >= 0; --n) mg_prolong(n);
