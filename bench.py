@@ -16,7 +16,8 @@ ours:       value = device-timed seconds per physical step of the product
             extrapolation, the learned network) by iterations and seconds per
             physical step to an absolute tolerance on the laminar cavity, and
             alm gives the cost of the actuator-line forcing, outlet that
-            of the characteristics outlet on an open wake box.
+            of the characteristics outlet on an open wake box, and
+            wall_functions that of the log-law wall functions.
 reference:  the CPU oracle (C++ restatement of the reference, FP32 like the
             reference's own build, its loops on every host thread) on the same
             case; a bounded sample of pseudo-iterations scaled to one physical
@@ -256,6 +257,36 @@ def run_ours(args, rank, world, dist):
             del S
         return res
 
+    def wallfn_cost(steps=2):
+        """Wall functions (wf_eta after every fine DAF step) on the SA channel
+        129x97x65 with a first wall spacing of 0.08 (layer 2 in the log law),
+        MIXED, graph path: seconds and pseudo-iterations per physical step
+        with and without them, and the kernel's time per pseudo-iteration."""
+        case, grid, state = cases.channel(im=129, jm=97, km=65, wall_first=0.08, itmax=200)
+        case.precision_mode = abi.MIXED
+        case.predictor = abi.PRED_LINEAR
+        case.use_graph = 1
+        res = {"workload": "SA channel 129x97x65, first wall spacing 0.08, MIXED, itmax 200"}
+        for name, on in (("without", 0), ("with", 1)):
+            c = case.copy()
+            c.wall_functions = on
+            S = Solver(c)
+            S.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
+            S.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
+            S.mg_driver()
+            sec, reps = timed_steps(S, steps, S.mg_driver)
+            its = float(np.mean([r["iterations"] for r in reps]))
+            res[name] = {"s_per_step": sec, "pseudo_iterations_per_step": its, "ms_per_iteration": 1e3 * sec / its}
+            if on:
+                S.profile(True)
+                r = S.mg_driver()
+                stats, _ = S.kernel_stats()
+                S.profile(False)
+                ms = sum(v[0] for v in stats.get("wallfn", {}).values())
+                res["wallfn_kernel_ms_per_iteration"] = ms / max(1, r["iterations"])
+            del S
+        return res
+
     def timed_steps(S, K, body):
         """K calls of body(), bracketed by barrier + synchronize, CUDA events
         on the library's stream; returns seconds per call (max over ranks)."""
@@ -374,6 +405,7 @@ def run_ours(args, rank, world, dist):
     ab = predictor_ab() if not args.no_ab else None
     alm = alm_cost() if not args.no_ab else None
     outlet = outlet_cost() if not args.no_ab else None
+    wallfn = wallfn_cost() if not args.no_ab else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -402,6 +434,7 @@ def run_ours(args, rank, world, dist):
         "predictor_ab": ab,
         "alm": alm,
         "outlet": outlet,
+        "wall_functions": wallfn,
         "e2e": {"value": e2e_sec, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "kernel": kind, "level": "fine", "achieved": achieved, "peak": peak, "unit": "GB/s",
