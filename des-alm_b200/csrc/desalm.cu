@@ -761,6 +761,8 @@ void outlet_ratios(const desalm_case& c, const double* x, const double* y, const
 int pseudo_iter(desalm_ctx* ctx, desalm_step_report* rep);
 int enqueue_iteration(desalm_ctx* ctx);
 int graph_step(desalm_ctx* ctx, desalm_step_report* rep);
+int graph_launch(desalm_ctx* ctx);
+int graph_finish(desalm_ctx* ctx, desalm_step_report* rep);
 int run_step(desalm_ctx* ctx, desalm_step_report* rep);
 int sa_des_eddy(desalm_ctx* ctx);
 int sa_conservation(desalm_ctx* ctx);
@@ -1583,6 +1585,36 @@ int desalm_mg_driver(desalm_ctx* ctx, desalm_step_report* rep) {
   return rc;
 }
 
+int desalm_mg_driver_batch(desalm_ctx* const* ctxs, int n, desalm_step_report* reps) {
+  if (!ctxs || n < 0) return DESALM_EINVAL;
+  for (int b = 0; b < n; ++b)
+    if (!ctxs[b]) return DESALM_EINVAL;
+  // contexts on the graph path (not the learned guess, which trains and
+  // falls back on the host) have their steps in flight together; the others
+  // step one after another in between
+  std::vector<char> inflight(n, 0);
+  int first = 0;
+  for (int b = 0; b < n && !first; ++b) {
+    desalm_ctx* ctx = ctxs[b];
+    desalm_step_report* rep = reps ? reps + b : nullptr;
+    const bool batched = ctx->c.use_graph && !ctx->prof_on && ctx->c.predictor != DESALM_PRED_LEARNED;
+    if (!batched) {
+      first = desalm_mg_driver(ctx, rep);
+      continue;
+    }
+    first = desalm_begin_step(ctx);
+    if (!first) first = graph_launch(ctx);
+    if (!first) inflight[b] = 1;
+  }
+  // every step in flight is finished, also after an error
+  for (int b = 0; b < n; ++b) {
+    if (!inflight[b]) continue;
+    const int rc = graph_finish(ctxs[b], reps ? reps + b : nullptr);
+    if (!first) first = rc;
+  }
+  return first;
+}
+
 int desalm_sync(desalm_ctx* ctx) {
   if (!ctx) return DESALM_EINVAL;
   CK(cudaStreamSynchronize(ctx->stream));
@@ -1875,13 +1907,21 @@ int run_step(desalm_ctx* ctx, desalm_step_report* rep) {
   return 0;
 }
 
-int graph_step(desalm_ctx* ctx, desalm_step_report* rep) {
+// The captured physical step in two halves, so that several contexts can
+// have theirs in flight at once (desalm_mg_driver_batch): graph_launch
+// enqueues the graph and the read-back of its convergence state on the
+// context's stream; graph_finish waits for that stream alone.
+int graph_launch(desalm_ctx* ctx) {
   if (!ctx->gexec) RET(build_graph(ctx));
   cudaStream_t s = ctx->stream;
   CK(cudaMemsetAsync(ctx->dconv, 0, sizeof(DevConv), s));
   CK(cudaGraphLaunch(ctx->gexec, s));
   CK(cudaMemcpyAsync(ctx->hconv, ctx->dconv, sizeof(DevConv), cudaMemcpyDeviceToHost, s));
-  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+int graph_finish(desalm_ctx* ctx, desalm_step_report* rep) {
+  CK(cudaStreamSynchronize(ctx->stream));
   const DevConv& st = *ctx->hconv;
   ctx->itc = st.itc;
   for (int m = 0; m < 5; ++m) ctx->init_resd[m] = st.init[m];
@@ -1895,6 +1935,11 @@ int graph_step(desalm_ctx* ctx, desalm_step_report* rep) {
   if (st.zero_pivots) { ctx->err = "zero pivot in a line solve"; return DESALM_ESINGULAR; }
   if (st.nonfinite) { ctx->err = "non-finite convergence norm"; return DESALM_ENONFINITE; }
   return 0;
+}
+
+int graph_step(desalm_ctx* ctx, desalm_step_report* rep) {
+  RET(graph_launch(ctx));
+  return graph_finish(ctx, rep);
 }
 
 }  // namespace

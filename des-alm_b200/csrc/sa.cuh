@@ -178,8 +178,14 @@ DESALM_DEV void sa_adi_row(const SaT<SW>& S, int l) {
 // zero.  Divisions by J and by sigma_SA are multiplications by 1/J and 1.5,
 // U/J comes from k_sa_ucn, and f_w's sixth root is cbrt(sqrt(x)); the results
 // equal the reference's expressions up to rounding.
+// Minimum resident CTAs per SM requested for k_sa_rhs (128 threads each); a
+// build-time tuning knob.  5 (96 registers, 96 B of spills) against 4 (127
+// registers): 0.477 against 0.492 s per MIXED channel step on one box.
+#ifndef DESALM_SA_MINBLOCKS
+#define DESALM_SA_MINBLOCKS 5
+#endif
 template <class SW>
-__global__ void __launch_bounds__(128) k_sa_rhs(SaT<SW> S) {
+__global__ void __launch_bounds__(128, DESALM_SA_MINBLOCKS) k_sa_rhs(SaT<SW> S) {
   pdl_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;

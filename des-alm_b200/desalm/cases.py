@@ -308,7 +308,8 @@ def alm_rotor(xs, ys, zs, center, radius, nblades=3, nelems=12, nangles=24, tsr=
     return tur, polars
 
 
-def wake(im=49, jm=25, km=25, seed=0, re=1000.0, turbulence=1, itmax=20, amp=0.05, side=BC_SYMMETRY, ng=3):
+def wake(im=49, jm=25, km=25, seed=0, re=1000.0, turbulence=1, itmax=20, amp=0.05, side=BC_SYMMETRY, ng=3,
+         noise=0.01):
     """Open box [0, 4] x [0, 2] x [0, 2] with a stream through it: uniform
     inflow u = 1 at i = 1 (btype 4: velocity held, pressure extrapolated with
     the grid ratio), the characteristics outlet at i = im (btype 5), 'side'
@@ -316,8 +317,9 @@ def wake(im=49, jm=25, km=25, seed=0, re=1000.0, turbulence=1, itmax=20, amp=0.0
     stretched geometrically (ratio 1.02) so that the extrapolation ratios
     differ from 1; interior nodes and the outlet plane's y move by a seeded
     sinusoid, so that the outlet's csi metrics have cross components.  The
-    state is the stream plus O(1e-2) seeded noise; nu_tilde = 3 nu and the
-    wall distance is uniform (no walls) when turbulent."""
+    state is the stream plus seeded noise of standard deviation 'noise'
+    (velocity) and noise / 10 (pressure); nu_tilde = 3 nu and the wall
+    distance is uniform (no walls) when turbulent."""
     rng = np.random.default_rng(seed)
     c = _base_case(im, jm, km)
     c.ng = ng
@@ -344,9 +346,9 @@ def wake(im=49, jm=25, km=25, seed=0, re=1000.0, turbulence=1, itmax=20, amp=0.0
                 wd=np.full(im * jm * km, 10.0) if turbulence else None)
     N = im * jm * km
     q = np.zeros((N, 5))
-    q[:, 0] = rng.normal(0.0, 1e-3, size=N)
-    q[:, 1] = 1.0 + rng.normal(0.0, 1e-2, size=N)
-    q[:, 2:4] = rng.normal(0.0, 1e-2, size=(N, 2))
+    q[:, 0] = rng.normal(0.0, 0.1 * noise, size=N)
+    q[:, 1] = 1.0 + rng.normal(0.0, noise, size=N)
+    q[:, 2:4] = rng.normal(0.0, noise, size=(N, 2))
     q = q.reshape(km, jm, im, 5)
     q[:, :, 0, 1] = 1.0               # inflow plane
     q[:, :, 0, 2:4] = 0.0

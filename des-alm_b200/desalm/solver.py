@@ -108,6 +108,8 @@ def lib():
         L.desalm_stream.restype = C.c_void_p
         L.desalm_kernel_class_count.argtypes = []
         L.desalm_kernel_class_count.restype = C.c_int
+        L.desalm_mg_driver_batch.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(StepReport)]
+        L.desalm_mg_driver_batch.restype = C.c_int
         _LIB = L
     return _LIB
 
@@ -181,6 +183,20 @@ def filestat_write(path, time, ntime, angles=()):
     a = _f64(np.asarray(angles, dtype=np.float64).reshape(-1))
     _io(lib().desalm_filestat_write(_b(path), float(time), int(ntime), _p(a) if a.size else None, a.size),
         "filestat_write")
+
+
+def mg_driver_batch(solvers):
+    """One physical step of each independent block (desalm_mg_driver_batch):
+    the graph-path steps run concurrently.  Returns the step reports."""
+    L = lib()
+    n = len(solvers)
+    ctxs = (C.c_void_p * n)(*[s.ctx for s in solvers])
+    reps = (StepReport * n)()
+    rc = L.desalm_mg_driver_batch(ctxs, n, reps)
+    if rc:
+        why = "; ".join(L.desalm_last_error(s.ctx).decode() for s in solvers if L.desalm_last_error(s.ctx))
+        raise DesalmError("mg_driver_batch failed (%d): %s" % (rc, why))
+    return [r.as_dict() for r in reps]
 
 
 class Solver:

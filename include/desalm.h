@@ -191,6 +191,17 @@ int  desalm_begin_step(desalm_ctx* ctx);
  * injection of qn/qnm1, predictor, optional conservation, pseudo-time loop
  * with down-leg V-cycle, prolongation, bcond_fm and mg_ck_conver). */
 int  desalm_mg_driver(desalm_ctx* ctx, desalm_step_report* rep);
+/* One physical step of each of n independent blocks (contexts), as
+ * desalm_mg_driver on each: the reference gives each zone its own MPI ranks
+ * (myzone, src/init.F90:579-590), and each runs mg_driver on its blocks.
+ * Contexts on the graph path
+ * (use_graph = 1, not the learned guess) have their captured steps in
+ * flight on their own streams at once, so small blocks share the GPU; the
+ * others step in turn.  Each block's result equals its desalm_mg_driver
+ * bit for bit (there is no exchange between blocks).  reps (n entries) may
+ * be NULL.  Returns the first error; the steps already in flight are
+ * finished first. */
+int  desalm_mg_driver_batch(desalm_ctx* const* ctxs, int n, desalm_step_report* reps);
 /* One pseudo-time iteration of the loop above (for callers that drive the
  * loop themselves); rep->residual receives the iteration's residual. */
 int  desalm_pseudo_iteration(desalm_ctx* ctx, desalm_step_report* rep);
