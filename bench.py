@@ -77,6 +77,9 @@ def build_case(name, precision, predictor):
     elif name == "channel":
         case, grid, state = cases.channel()
         desc = "SA RANS channel Re_tau=395, 129x97x65 tanh-stretched, periodic i/k, 3-level FAS"
+    elif name == "wake":
+        case, grid, state = cases.wake(im=129, jm=97, km=65, turbulence=1, itmax=200)
+        desc = "SA wake box 129x97x65, uniform inflow, characteristics outlet, 3-level FAS"
     else:
         raise SystemExit("unknown case " + name)
     case.precision_mode = precision
@@ -422,6 +425,16 @@ def run_ours(args, rank, world, dist):
     achieved = byts / (ms_sum / 1e3) / 1e9 if ms_sum > 0 else 0.0
     share = {k: round(sum(v[0] for v in p.values()) / max(1e-9, sum(sum(w[0] for w in q.values()) for q in stats.values())), 4)
              for k, p in stats.items()}
+    # every class with an algorithmic-byte count, on its fine-level launches
+    by_kernel = {}
+    for k, p in stats.items():
+        b1 = alg_bytes(k, T[1], W[1], False)
+        if not b1 or 1 not in p or p[1][0] <= 0:
+            continue
+        ms1, n1, nodes1 = p[1]
+        gbs = b1 * nodes1 / (ms1 / 1e3) / 1e9
+        by_kernel[k] = {"achieved_gbs": round(gbs, 1), "frac": round(gbs / peak, 4),
+                        "avg_launch_us": round(1e3 * ms1 / max(1, n1), 2), "alg_bytes_per_node": b1}
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tfile):
@@ -499,6 +512,7 @@ def run_ours(args, rank, world, dist):
                      "avg_launch_ms": ms_sum / max(1, nlaunch),
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s"},
         "kernel_time_share": share,
+        "roofline_by_kernel": by_kernel,
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
@@ -587,7 +601,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--case", default="channel", choices=["cavity", "channel"])
+    ap.add_argument("--case", default="channel", choices=["cavity", "channel", "wake"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ab", action="store_true", help="skip the initial-guess and forcing sections")
