@@ -369,6 +369,7 @@ def run_ours(args, rank, world, dist):
     S = Solver(case)
     S.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
     S.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
+    widths = S.sweep_widths()[:case.ng].tolist()
     for _ in range(args.warmup):
         S.mg_driver()
     clk = Clocks(dev)
@@ -492,7 +493,10 @@ def run_ours(args, rank, world, dist):
                    "learned_predictor": "built (predictor DESALM_PRED_LEARNED); compared in predictor_ab",
                    "pseudo_iterations_per_step": iters, "converged": conv,
                    "l2": "working set of every level > 126 MB L2 for the channel; no flush between steps",
-                   "parallelism": "replicas only (%d independent replicas)" % world},
+                   "parallelism": "replicas only (%d independent replicas)" % world,
+                   "sweep_lines_per_cta": {"levels_x_ijk": widths,
+                                           "how": "timed per level and direction when the grid is set "
+                                                  "(0 = shared-memory rule, DESALM_AUTOTUNE=0)"}},
         "fp64_plain": {"value": sec64, "unit": UNIT, "pseudo_iterations_per_step": iters64,
                        "speedup_mixed_vs_fp64": sec64 / sec},
         "mixed_vs_fp64_rel_l2": {"fields": field_err,

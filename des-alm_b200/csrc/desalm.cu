@@ -167,6 +167,9 @@ struct desalm_ctx {
   double** dcov = nullptr;    // device copy of cov[]
   double* rat = nullptr;
   int ratdim = 0;
+  // lines per CTA of each level's DAF sweeps [level][direction], picked by
+  // timing when the grid is set (autotune_sweeps); 0: the shared-memory rule
+  int sweep_nl[4][3] = {};
   double* pfix = nullptr;     // device scalar (type of the fine level: double)
   double* part = nullptr;     // norm partials
   int part_blocks = 0;
@@ -387,7 +390,7 @@ size_t slab_bytes(int n, int nl) { return (size_t)10 * slab_fs(n + 2, nl + 1) * 
 // static arrays come on top of the slab.
 constexpr size_t kSlabFourPerSm = 48 * 1024;
 template <class T, class W, int DIR, int NL>
-int sweep4_nl(desalm_ctx* ctx, Lv<T, W>& L, const Par& P, int lvl, int blo, int bhi) {
+int sweep4_nl(desalm_ctx* ctx, Lv<T, W>& L, const Par& P, int lvl, int blo, int bhi, bool xform = true) {
   int amax, n, nb;
   if (DIR == 0) { amax = L.jm - 2; n = L.im - 2; nb = L.km - 2; }
   else if (DIR == 1) { amax = L.im - 2 + L.oute; n = L.jm - 2; nb = L.km - 2; }
@@ -401,6 +404,7 @@ int sweep4_nl(desalm_ctx* ctx, Lv<T, W>& L, const Par& P, int lvl, int blo, int 
   else
     LAUNCH(cls, lvl, nin, launch_k(k_sweep4<T, W, DIR, NL, kSlabThreads>, dim3(cdiv(amax, NL), nb), kSlabThreads, bytes, s, L, P, blo, bhi));
   CKL();
+  if (!xform) return 0;
   const int xcls = DIR == 0 ? KC_XFORM_I : (DIR == 1 ? KC_XFORM_J : KC_XFORM_K);
   const dim3 gx(cdiv(L.im - 2 + L.oute, 32), cdiv(L.jm - 2, 4), L.km - 2);
   LAUNCH(xcls, lvl, nin, launch_k(k_xform<T, W, DIR>, gx, blk3(), 0, s, L));
@@ -450,12 +454,21 @@ cudaError_t slab_attrs() {
   return e;
 }
 
+// One DAF sweep (and its transform unless xform is false) with the lines per
+// CTA that autotune_sweeps picked for this level and direction, else the
+// widest slab that leaves room for two CTAs per SM, else the widest that fits
+// one.  Every line is solved by the same operations whatever the width, so
+// the choice changes the time only.
 template <class T, class W, int DIR>
-int launch_sweep(desalm_ctx* ctx, Lv<T, W>& L, const Par& P, int lvl, int blo, int bhi) {
+int launch_sweep(desalm_ctx* ctx, Lv<T, W>& L, const Par& P, int lvl, int blo, int bhi, bool xform = true) {
   const int n = DIR == 0 ? L.im - 2 : (DIR == 1 ? L.jm - 2 : L.km - 2);
-  if (slab_bytes<W>(n, 16) <= kSlabTwoPerSm) return sweep4_nl<T, W, DIR, 16>(ctx, L, P, lvl, blo, bhi);
-  if (slab_bytes<W>(n, 8) <= kSlabTwoPerSm) return sweep4_nl<T, W, DIR, 8>(ctx, L, P, lvl, blo, bhi);
-  if (slab_bytes<W>(n, 4) <= kSlabMax) return sweep4_nl<T, W, DIR, 4>(ctx, L, P, lvl, blo, bhi);
+  const int want = lvl < 4 ? ctx->sweep_nl[lvl][DIR] : 0;
+  if (want == 16 && slab_bytes<W>(n, 16) <= kSlabMax) return sweep4_nl<T, W, DIR, 16>(ctx, L, P, lvl, blo, bhi, xform);
+  if (want == 8 && slab_bytes<W>(n, 8) <= kSlabMax) return sweep4_nl<T, W, DIR, 8>(ctx, L, P, lvl, blo, bhi, xform);
+  if (want == 4 && slab_bytes<W>(n, 4) <= kSlabMax) return sweep4_nl<T, W, DIR, 4>(ctx, L, P, lvl, blo, bhi, xform);
+  if (slab_bytes<W>(n, 16) <= kSlabTwoPerSm) return sweep4_nl<T, W, DIR, 16>(ctx, L, P, lvl, blo, bhi, xform);
+  if (slab_bytes<W>(n, 8) <= kSlabTwoPerSm) return sweep4_nl<T, W, DIR, 8>(ctx, L, P, lvl, blo, bhi, xform);
+  if (slab_bytes<W>(n, 4) <= kSlabMax) return sweep4_nl<T, W, DIR, 4>(ctx, L, P, lvl, blo, bhi, xform);
   ctx->err = "grid line too long for the shared-memory line sweep";
   return DESALM_EINVAL;
 }
@@ -662,6 +675,71 @@ int do_wallfn(desalm_ctx* ctx) {
   return kind_of(ctx, 0) == K_DD ? launch_wallfn(ctx, G.dd) : launch_wallfn(ctx, G.df);
 }
 
+// ------------------------------------------------------------ autotuning
+// The DAF sweeps of one level and direction timed at 16, 8 and 4 lines per
+// CTA (each width whose slab fits): one warm-up launch, then five timed with
+// CUDA events on the context's stream; the fastest width is kept.  Wide
+// slabs copy longer contiguous runs; narrow ones give short coarse-level
+// planes enough CTAs to fill the SMs.  Only the sweep runs (its transform,
+// which for k updates q, does not): it solves the work arrays in place, and
+// those are rewritten by k_resid before every use, so timing them changes
+// no result.
+template <class T, class W, int DIR>
+int tune_sweep(desalm_ctx* ctx, Lv<T, W>& L, int lvl, cudaEvent_t e0, cudaEvent_t e1) {
+  Par P = ctx->par;
+  P.fine = (lvl == 0);
+  const int n = DIR == 0 ? L.im - 2 : (DIR == 1 ? L.jm - 2 : L.km - 2);
+  float best = 0.f;
+  int pick = 0;
+  for (int nl : {16, 8, 4}) {
+    const size_t bytes = slab_bytes<W>(n, nl);
+    if (bytes > kSlabMax) continue;
+    ctx->sweep_nl[lvl][DIR] = nl;
+    RET((launch_sweep<T, W, DIR>(ctx, L, P, lvl, 0, 0, false)));
+    CK(cudaEventRecord(e0, ctx->stream));
+    for (int r = 0; r < 5; ++r) RET((launch_sweep<T, W, DIR>(ctx, L, P, lvl, 0, 0, false)));
+    CK(cudaEventRecord(e1, ctx->stream));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    if (!pick || ms < best) { best = ms; pick = nl; }
+  }
+  ctx->sweep_nl[lvl][DIR] = pick;
+  return 0;
+}
+
+template <class T, class W>
+int tune_level(desalm_ctx* ctx, Lv<T, W>& L, int lvl, cudaEvent_t e0, cudaEvent_t e1) {
+  RET((tune_sweep<T, W, 0>(ctx, L, lvl, e0, e1)));
+  RET((tune_sweep<T, W, 1>(ctx, L, lvl, e0, e1)));
+  return tune_sweep<T, W, 2>(ctx, L, lvl, e0, e1);
+}
+
+// Picks the sweep widths of every level, unless DESALM_AUTOTUNE=0 in the
+// environment (then the shared-memory rule alone decides).
+int autotune_sweeps(desalm_ctx* ctx) {
+  for (int n = 0; n < 4; ++n)
+    for (int d = 0; d < 3; ++d) ctx->sweep_nl[n][d] = 0;
+  const char* env = std::getenv("DESALM_AUTOTUNE");
+  if (env && std::string(env) == "0") return 0;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CK(cudaEventCreate(&e0));
+  cudaError_t ce = cudaEventCreate(&e1);
+  if (ce != cudaSuccess) {
+    cudaEventDestroy(e0);
+    ctx->err = std::string("cudaEventCreate: ") + cudaGetErrorString(ce);
+    return DESALM_ECUDA;
+  }
+  int rc = 0;
+  for (int n = 0; n < ctx->ng && n < 4 && !rc; ++n) {
+    Level& G = ctx->L[n];
+    rc = kind_of(ctx, n) == K_DD ? tune_level(ctx, G.dd, n, e0, e1) : tune_level(ctx, G.df, n, e0, e1);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
+}
+
 int do_nlevel(desalm_ctx* ctx, int n) {  // n = coarse level index (>= 1)
   Level& F = ctx->L[n - 1];
   Level& C = ctx->L[n];
@@ -763,6 +841,8 @@ int enqueue_iteration(desalm_ctx* ctx);
 int graph_step(desalm_ctx* ctx, desalm_step_report* rep);
 int graph_launch(desalm_ctx* ctx);
 int graph_finish(desalm_ctx* ctx, desalm_step_report* rep);
+void drop_graph(desalm_ctx* ctx);
+int autotune_sweeps(desalm_ctx* ctx);
 int run_step(desalm_ctx* ctx, desalm_step_report* rep);
 int sa_des_eddy(desalm_ctx* ctx);
 int sa_conservation(desalm_ctx* ctx);
@@ -1337,6 +1417,9 @@ int desalm_set_grid(desalm_ctx* ctx, const double* x, const double* y, const dou
     ctx->err = std::string("set_grid: ") + cudaGetErrorString(e);
     return DESALM_ECUDA;
   }
+  // the sweep widths for this grid; a captured step uses the old ones
+  RET(autotune_sweeps(ctx));
+  drop_graph(ctx);
   ctx->have_grid = true;
   return 0;
 }
@@ -1613,6 +1696,13 @@ int desalm_mg_driver_batch(desalm_ctx* const* ctxs, int n, desalm_step_report* r
     if (!first) first = rc;
   }
   return first;
+}
+
+int desalm_sweep_widths(desalm_ctx* ctx, int nl[12]) {
+  if (!ctx || !nl) return DESALM_EINVAL;
+  for (int n = 0; n < 4; ++n)
+    for (int d = 0; d < 3; ++d) nl[3 * n + d] = n < ctx->ng ? ctx->sweep_nl[n][d] : 0;
+  return 0;
 }
 
 int desalm_sync(desalm_ctx* ctx) {

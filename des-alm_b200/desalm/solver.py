@@ -108,6 +108,8 @@ def lib():
         L.desalm_stream.restype = C.c_void_p
         L.desalm_kernel_class_count.argtypes = []
         L.desalm_kernel_class_count.restype = C.c_int
+        L.desalm_sweep_widths.argtypes = [vp, C.POINTER(C.c_int)]
+        L.desalm_sweep_widths.restype = C.c_int
         L.desalm_mg_driver_batch.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(StepReport)]
         L.desalm_mg_driver_batch.restype = C.c_int
         _LIB = L
@@ -275,6 +277,12 @@ class Solver:
 
     def conservation(self):
         self._ck(self.L.desalm_conservation(self.ctx), "conservation")
+
+    def sweep_widths(self):
+        """Lines per CTA of the DAF sweeps, [level][direction] (0: not tuned)."""
+        out = (C.c_int * 12)()
+        self._ck(self.L.desalm_sweep_widths(self.ctx, out), "sweep_widths")
+        return np.array(list(out)).reshape(4, 3)
 
     def wall_functions(self):
         self._ck(self.L.desalm_wall_functions(self.ctx), "wall_functions")

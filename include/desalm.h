@@ -202,6 +202,14 @@ int  desalm_mg_driver(desalm_ctx* ctx, desalm_step_report* rep);
  * be NULL.  Returns the first error; the steps already in flight are
  * finished first. */
 int  desalm_mg_driver_batch(desalm_ctx* const* ctxs, int n, desalm_step_report* reps);
+/* Lines per CTA of each level's DAF line sweeps, nl[3 * level + direction]
+ * (directions i, j, k; 0 for levels the case does not have): 16, 8 or 4, as
+ * timed on this GPU when the grid was set (desalm_set_grid tries each width
+ * whose shared-memory slab fits and keeps the fastest), or 0 where the
+ * timing is off (environment DESALM_AUTOTUNE=0) and the widest slab that
+ * leaves room for two CTAs per SM is used.  The width changes the time
+ * only: every line is solved by the same operations. */
+int  desalm_sweep_widths(desalm_ctx* ctx, int nl[12]);
 /* One pseudo-time iteration of the loop above (for callers that drive the
  * loop themselves); rep->residual receives the iteration's residual. */
 int  desalm_pseudo_iteration(desalm_ctx* ctx, desalm_step_report* rep);

@@ -1,0 +1,46 @@
+"""The sweep-width autotuner: desalm_set_grid times the DAF sweeps of every
+level and direction at 16, 8 and 4 lines per CTA and keeps the fastest.  The
+width may change the time only, so a tuned context must step exactly like
+one on the shared-memory rule (DESALM_AUTOTUNE=0), and the timing runs must
+leave the state alone."""
+import numpy as np
+import pytest
+
+from desalm import abi, cases
+
+pytestmark = pytest.mark.gpu
+
+
+def _solver(case, grid, state):
+    from desalm.solver import Solver
+    S = Solver(case)
+    S.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
+    S.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
+    return S
+
+
+@pytest.mark.parametrize("precision", [abi.FP64, abi.MIXED])
+def test_tuned_widths_change_nothing_but_time(precision, monkeypatch):
+    case, grid, state = cases.wake(im=65, jm=33, km=33, turbulence=1, seed=4, itmax=5)
+    case.precision_mode = precision
+    case.use_graph = 1
+    tuned = _solver(case, grid, state)
+    monkeypatch.setenv("DESALM_AUTOTUNE", "0")
+    rule = _solver(case, grid, state)
+    monkeypatch.delenv("DESALM_AUTOTUNE")
+    w = tuned.sweep_widths()
+    assert set(np.unique(w[:case.ng])) <= {4, 8, 16} and not w[case.ng:].any()
+    assert not rule.sweep_widths().any()
+    # the timing runs at set_grid touched no state
+    assert np.array_equal(tuned.get_state()["q"], rule.get_state()["q"])
+    for _ in range(2):
+        ra, rb = tuned.mg_driver(), rule.mg_driver()
+        assert ra["iterations"] == rb["iterations"]
+    for k in ("q", "nut"):
+        assert np.array_equal(tuned.get_state()[k], rule.get_state()[k]), k
+    # setting the grid again re-tunes and drops the captured step
+    tuned.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
+    rule.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
+    tuned.mg_driver()
+    rule.mg_driver()
+    assert np.array_equal(tuned.get_state()["q"], rule.get_state()["q"])
