@@ -158,6 +158,11 @@ struct desalm_ctx {
   int ng = 0;
   std::vector<Level> L;
   cudaStream_t stream = nullptr;
+  // a second stream for kernels that need not wait for the ones before them
+  // (fork_side / join_side); forks and joins are captured as graph edges
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  bool alm_pending = false;  // this iteration's forcing runs on the side stream
   Par par{};
   std::string err;
   bool have_grid = false, have_state = false;
@@ -473,12 +478,25 @@ int launch_sweep(desalm_ctx* ctx, Lv<T, W>& L, const Par& P, int lvl, int blo, i
   return DESALM_EINVAL;
 }
 
+// Fork: the side stream waits for everything enqueued so far on the main
+// stream.  Join: the main stream waits for everything enqueued so far on the
+// side stream.
+int fork_side(desalm_ctx* ctx) {
+  CK(cudaEventRecord(ctx->ev_fork, ctx->stream));
+  CK(cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0));
+  return 0;
+}
+int join_side(desalm_ctx* ctx) {
+  CK(cudaEventRecord(ctx->ev_join, ctx->side));
+  CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
+  return 0;
+}
+
 // rhs_lines on the fine level (src/solver_daf.F90:378-381): element forces,
 // then each turbine's projection into alm.falm, which K_R's first pass adds.
 template <class T, class W>
-int alm_run(desalm_ctx* ctx, Lv<T, W>& L) {
+int alm_run(desalm_ctx* ctx, Lv<T, W>& L, cudaStream_t s) {
   auto& A = ctx->alm;
-  cudaStream_t s = ctx->stream;
   CK(cudaMemsetAsync(A.falm, 0, 3L * L.N * sizeof(double), s));
   LAUNCH(KC_ALM, 0, double(A.dev.E), launch_k(k_alm_forces<T, W>, 1, 256, 0, s, A.dev, L));
   if (A.dev.nker_all > 0)
@@ -502,13 +520,31 @@ int launch_daf(desalm_ctx* ctx, Lv<T, W>& L, Level& G, int n, int recalc, int it
   const int upwind = fine ? 2 : 1;
   const int bback = fine && c.btype[0] != 5;
   const double nin = double(L.im - 2) * (L.jm - 2) * (L.km - 2);
-  if (n == 0 && ctx->alm.on) RET(alm_run(ctx, L));
+  if (n == 0 && ctx->alm.on) {
+    // the forcing was started beside the SA sub-iterations (enqueue_iteration)
+    // or runs here
+    if (ctx->alm_pending) {
+      RET(join_side(ctx));
+      ctx->alm_pending = false;
+    } else {
+      RET(alm_run(ctx, L, s));
+    }
+  }
+  // the outlet plane's residual and its preparation for the sweeps
+  // (src/solver_daf.F90:318-358) reads only q and dtau and writes only the
+  // plane, so it runs beside k_resid on the side stream; the back face's
+  // call writes a plane that nothing reads, so it is not made
+  const bool out_side = L.oute && !ctx->prof_on;
+  if (out_side) {
+    RET(fork_side(ctx));
+    LAUNCH(KC_OUTLET, n, double(L.jm - 2) * (L.km - 2),
+           launch_k(k_outlet<T, W>, dim3(cdiv(L.jm - 2, 32), cdiv(L.km - 2, 4)), dim3(32, 4), 0, ctx->side, L, P));
+    CKL();
+  }
   LAUNCH(KC_RESID, n, nin, launch_k(k_resid<T, W, 0>, grid_r(L.im, L.jm, L.km), blk_r(), 0, s, L, P, upwind, itr == 1 ? 1 : 0, n > 0 ? 1 : 0, bback));
   CKL();
-  if (L.oute) {
-    // the outlet plane's residual and its preparation for the sweeps
-    // (src/solver_daf.F90:318-358); the back face's call writes a plane that
-    // nothing reads, so it is not made
+  if (out_side) RET(join_side(ctx));
+  if (L.oute && !out_side) {
     LAUNCH(KC_OUTLET, n, double(L.jm - 2) * (L.km - 2),
            launch_k(k_outlet<T, W>, dim3(cdiv(L.jm - 2, 32), cdiv(L.km - 2, 4)), dim3(32, 4), 0, s, L, P));
     CKL();
@@ -1202,7 +1238,11 @@ void desalm_destroy(desalm_ctx* ctx) {
   if (ctx->graph) cudaGraphDestroy(ctx->graph);
   if (ctx->hconv) cudaFreeHost(ctx->hconv);
   if (ctx->h_norm) cudaFreeHost(ctx->h_norm);
+  if (ctx->side) cudaStreamSynchronize(ctx->side);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  if (ctx->side) cudaStreamDestroy(ctx->side);
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+  if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
   delete ctx;
 }
 
@@ -1226,6 +1266,9 @@ int desalm_init(const desalm_case* c, desalm_ctx** out) {
     return DESALM_ECUDA;
   }
   e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming);
   if (e != cudaSuccess) {
     ctx->err = std::string("cudaStreamCreate: ") + cudaGetErrorString(e);
     *out = ctx;
@@ -1723,6 +1766,7 @@ namespace {
 // and under stream capture.
 int enqueue_iteration(desalm_ctx* ctx) {
   const desalm_case& c = ctx->c;
+  ctx->alm_pending = false;
   CK(cudaMemsetAsync(ctx->flags, 0, 2 * sizeof(int), ctx->stream));
   int recalc = 0;
   for (int n = 0; n < ctx->ng; ++n) {
@@ -1730,6 +1774,14 @@ int enqueue_iteration(desalm_ctx* ctx) {
     for (int itr = 1; itr <= c.iter[n]; ++itr) {
       // decide_recalc_rh keeps its last value on the coarsest level (Q5)
       if (n != ctx->ng - 1) recalc = (itr != c.iter[n]) ? 0 : 1;
+      // the forcing reads the velocities, which the SA sub-iterations leave
+      // alone: it runs beside them and joins before k_resid
+      if (n == 0 && ctx->alm.on && c.turbulence && !ctx->prof_on) {
+        RET(fork_side(ctx));
+        Level& G0 = ctx->L[0];
+        RET(kind_of(ctx, 0) == K_DD ? alm_run(ctx, G0.dd, ctx->side) : alm_run(ctx, G0.df, ctx->side));
+        ctx->alm_pending = true;
+      }
       if (c.turbulence && n == 0) RET(sa_des_eddy(ctx));
       // the recalculated residual on the coarsest level feeds nothing
       int rc_eff = (n == ctx->ng - 1) ? 0 : recalc;
