@@ -470,11 +470,14 @@ def run_ours(args, rank, world, dist):
     field_err = {nm: float(np.linalg.norm(a[:, m] - b[:, m]) / max(1e-300, np.linalg.norm(b[:, m])))
                  for m, nm in enumerate(names)}
 
-    ab = predictor_ab() if not args.no_ab else None
-    alm = alm_cost() if not args.no_ab else None
-    outlet = outlet_cost() if not args.no_ab else None
-    wallfn = wallfn_cost() if not args.no_ab else None
-    batched = batched_blocks() if not args.no_ab else None
+    # one-GPU characterisations (initial guesses, option costs, batching):
+    # run once, not on every replica of a multi-GPU run
+    extra = not args.no_ab and world == 1
+    ab = predictor_ab() if extra else None
+    alm = alm_cost() if extra else None
+    outlet = outlet_cost() if extra else None
+    wallfn = wallfn_cost() if extra else None
+    batched = batched_blocks() if extra else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -166,6 +166,7 @@ struct desalm_ctx {
   Par par{};
   std::string err;
   bool have_grid = false, have_state = false;
+  bool have_wd = false;  // desalm_set_grid was given the wall distance
   // fine-level extras (always FP64)
   double *x = nullptr, *y = nullptr, *z = nullptr, *wd = nullptr, *dtev = nullptr;
   double* cov[9] = {};
@@ -1381,6 +1382,7 @@ int desalm_set_grid(desalm_ctx* ctx, const double* x, const double* y, const dou
   CK(cudaMemcpyAsync(ctx->z, z, NF * sizeof(double), cudaMemcpyHostToDevice, s));
   if (wd) CK(cudaMemcpyAsync(ctx->wd, wd, NF * sizeof(double), cudaMemcpyHostToDevice, s));
   else CK(cudaMemsetAsync(ctx->wd, 0, NF * sizeof(double), s));
+  ctx->have_wd = wd != nullptr;
   // coordinates of every level (injection), metrics per level in FP64
   double* xs[3] = {ctx->x, ctx->y, ctx->z};
   std::vector<double*> lvl_xyz(3 * ctx->ng, nullptr);
@@ -1612,7 +1614,8 @@ int desalm_des_eddy(desalm_ctx* ctx) {
 
 int desalm_wall_functions(desalm_ctx* ctx) {
   if (!ctx) return DESALM_EINVAL;
-  if (ctx->L.empty()) return DESALM_ENOTREADY;
+  if (!ctx->have_grid || !ctx->have_state) { ctx->err = "grid or state not set"; return DESALM_ENOTREADY; }
+  if (!ctx->have_wd) { ctx->err = "the wall functions need the wall distance (desalm_set_grid wd)"; return DESALM_EINVAL; }
   RET(do_wallfn(ctx));
   CK(cudaStreamSynchronize(ctx->stream));
   return 0;
@@ -1642,6 +1645,10 @@ int desalm_save_qold(desalm_ctx* ctx) {
 int desalm_begin_step(desalm_ctx* ctx) {
   if (!ctx) return DESALM_EINVAL;
   if (!ctx->have_grid || !ctx->have_state) { ctx->err = "grid or state not set"; return DESALM_ENOTREADY; }
+  if (ctx->c.wall_functions && !ctx->have_wd) {
+    ctx->err = "the wall functions need the wall distance (desalm_set_grid wd)";
+    return DESALM_EINVAL;
+  }
   const desalm_case& c = ctx->c;
   cudaStream_t s = ctx->stream;
   Level& F = ctx->L[0];

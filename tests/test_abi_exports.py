@@ -46,3 +46,8 @@ def test_invalid_case_is_rejected_without_gpu():
     with pytest.raises(DesalmError) as e:
         Solver(case)
     assert "pressure reference node" in str(e.value)
+    case.ifix = 1
+    case.wall_functions = 2
+    with pytest.raises(DesalmError) as e:
+        Solver(case)
+    assert "wall_functions" in str(e.value)

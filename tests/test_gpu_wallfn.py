@@ -84,3 +84,16 @@ def test_wall_functions_graph_matches_eager():
         out.append(s.get_state())
     assert np.array_equal(out[0]["q"], out[1]["q"])
     assert np.array_equal(out[0]["nut"], out[1]["nut"])
+
+
+def test_wall_functions_need_the_wall_distance():
+    from desalm.solver import Solver, DesalmError
+    case, grid, state = _case(4)
+    case.wall_functions = 1
+    S = Solver(case)
+    S.set_grid(grid["x"], grid["y"], grid["z"])          # no wall distance
+    S.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
+    with pytest.raises(DesalmError, match="wall distance"):
+        S.mg_driver()
+    with pytest.raises(DesalmError, match="wall distance"):
+        S.wall_functions()
