@@ -565,10 +565,12 @@ def run_reference(args):
     cb = vals[-1]
     cb["value"] = v
     _, _, _, desc = build_case(args.case, abi.FP64, abi.PRED_QN)
-    return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+    # n_gpus: the N this arm was launched with, as the arm it is compared
+    # with; the work runs on rank 0's host cores
+    return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic", "impl": "reference",
-            "config": {"workload": desc, "case": args.case},
+            "config": {"workload": desc, "case": args.case, "device": "host cores of rank 0 (no GPU)"},
             "cpu_baseline": cb,
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
