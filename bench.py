@@ -169,7 +169,8 @@ def run_ours(args, rank, world, dist):
         of the network included."""
         res = {"workload": "laminar lid-driven cavity Re=1000, 65^3, MIXED, steps %d-%d of dt=0.05, "
                            "tolerance log10 mean|dq(u,v,w)| < -7, itmax 200" % (skip + 1, n_steps)}
-        for P, name in ((abi.PRED_QN, "qn"), (abi.PRED_LINEAR, "linear"), (abi.PRED_LEARNED, "learned")):
+        for P, name, mask in ((abi.PRED_QN, "qn", None), (abi.PRED_LINEAR, "linear", None),
+                              (abi.PRED_LEARNED, "learned", None), (abi.PRED_LEARNED, "learned_all_fields", 0x1f)):
             case, grid, state = cases.cavity(n=65, itmax=200)
             case.precision_mode = abi.MIXED
             case.predictor = P
@@ -179,6 +180,8 @@ def run_ours(args, rank, world, dist):
             S = Solver(case)
             S.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
             S.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
+            if mask is not None:
+                S.lp_fields(mask)
             stream = torch.cuda.ExternalStream(S.stream())
             its, secs = [], []
             for k in range(n_steps):
@@ -197,6 +200,12 @@ def run_ours(args, rank, world, dist):
                      "s_per_step": float(np.mean(secs))}
             if P == abi.PRED_LEARNED:
                 entry["network"] = S.lp_report()
+                entry["fields_corrected"] = "p, u, v, w, nu_tilde" if mask == 0x1f else "p, nu_tilde (default)"
+                lin = res["linear"]["iterations_per_step"]
+                d = np.array(its, float) - np.array(lin, float)
+                entry["vs_linear_paired"] = {"mean_iteration_difference": float(d.mean()),
+                                             "standard_error": float(d.std(ddof=1) / np.sqrt(len(d))),
+                                             "steps_with_fewer_iterations": int((d < 0).sum()), "steps": len(d)}
             res[name] = entry
             del S
         return res

@@ -248,10 +248,14 @@ __global__ void k_lp_dot(long N, const float* __restrict__ y, const float* __res
 // factor alpha_f = <y, t> / <y, y> of the held-out check, limited to [0, 1]
 // (0 when the network's output is zero or not finite), so that a network that
 // does not help leaves the linear extrapolation; otherwise alpha_f = fixed.
-__global__ void k_lp_blend(const double* __restrict__ acc, float fixed, float* __restrict__ alpha) {
+__global__ void k_lp_blend(const double* __restrict__ acc, float fixed, int mask, float* __restrict__ alpha) {
   pdl_wait();
   const int f = threadIdx.x;
   if (f >= 5) return;
+  if (!((mask >> f) & 1)) {
+    alpha[f] = 0.0f;
+    return;
+  }
   float a = fixed;
   if (fixed < 0.0f) {
     const double yt = acc[f], yy = acc[5 + f];

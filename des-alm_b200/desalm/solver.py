@@ -74,6 +74,7 @@ def lib():
             ("lp_config", [vp, ip, ip, C.c_float, C.c_float]),
             ("lp_report_get", [vp, C.POINTER(LpReport)]),
             ("lp_blend", [vp, C.c_float]),
+            ("lp_fields", [vp, ip]),
             ("lp_get_params", [vp, fp]),
             ("lp_set_params", [vp, fp]),
             ("lp_eval", [vp, fp, fp, fp, dp, fp]),
@@ -378,6 +379,10 @@ class Solver:
     def lp_blend(self, alpha=-1.0):
         """alpha < 0: automatic blend of each field's correction; else fixed."""
         self._ck(self.L.desalm_lp_blend(self.ctx, float(alpha)), "lp_blend")
+
+    def lp_fields(self, mask=0x1f):
+        """Bit f of mask: field f (p, u, v, w, nu_tilde) takes the correction."""
+        self._ck(self.L.desalm_lp_fields(self.ctx, int(mask)), "lp_fields")
 
     def lp_report(self):
         r = LpReport()

@@ -303,6 +303,11 @@ int  desalm_lp_config(desalm_ctx* ctx, int train_steps, int warm, float lr,
 int  desalm_lp_report_get(desalm_ctx* ctx, desalm_lp_report* r);
 /* Blend: alpha < 0 (default) automatic; 0 <= alpha <= 1 fixed for every field. */
 int  desalm_lp_blend(desalm_ctx* ctx, float alpha);
+/* Which fields take the network's correction: bit f of mask for field f
+ * (p, u, v, w, nu_tilde); the others keep the linear extrapolation.
+ * Default 17 (p and nu_tilde): a velocity correction is not discretely
+ * divergence-free, and the pseudo-time iteration relaxes that error slowly. */
+int  desalm_lp_fields(desalm_ctx* ctx, int mask);
 /* nparam floats in the flat layout above; set restarts the Adam moments */
 int  desalm_lp_get_params(desalm_ctx* ctx, float* theta);
 int  desalm_lp_set_params(desalm_ctx* ctx, const float* theta);

@@ -107,6 +107,30 @@ def test_zero_network_is_linear_extrapolation_bitwise():
     assert np.array_equal(S.lp_params(), np.zeros(lp.nparam(), np.float32))
 
 
+def test_masked_fields_keep_the_linear_guess():
+    """desalm_lp_fields: a field whose bit is clear takes no correction; with
+    every bit clear a trained network gives the linear run bit for bit, and
+    with only p's bit set u, v, w follow the linear guess at each step's
+    start."""
+    def none(S):
+        S.lp_config(train_steps=2, warm=0)
+        S.lp_fields(0)
+    S, st, reps = _run(abi.PRED_LEARNED, 4, none)
+    _, st_lin, reps_lin = _run(abi.PRED_LINEAR, 4)
+    for k in ("q", "qn", "qnm1", "nut"):
+        assert np.array_equal(st[k], st_lin[k]), k
+    assert S.lp_report()["alpha"] == [0.0] * 5
+    assert S.lp_report()["train_steps"] > 0
+    with pytest.raises(Exception):
+        S.lp_fields(32)
+
+    def p_only(S):
+        S.lp_config(train_steps=2, warm=0)
+        S.lp_fields(1)
+    S, _, _ = _run(abi.PRED_LEARNED, 3, p_only)
+    assert S.lp_report()["alpha"][1:] == [0.0] * 4
+
+
 def test_non_finite_network_output_falls_back_to_linear():
     def setup(S):
         th = np.zeros(lp.nparam(), np.float32)
@@ -171,6 +195,7 @@ def test_blown_up_learned_step_restarts_from_linear_guess():
         S.lp_set_params(th)
         S.lp_config(train_steps=1, warm=2, lr=0.0, ymax=3e38)
         S.lp_blend(1.0)                                      # no held-out damping
+        S.lp_fields(0x1f)                                    # every field corrected
     S, st, reps = _run(abi.PRED_LEARNED, 4, setup)
     _, st_lin, reps_lin = _run(abi.PRED_LINEAR, 4)
     r = S.lp_report()
@@ -200,6 +225,7 @@ def test_heldout_blend_matches_oracle():
     def setup(S):
         S.lp_set_params(lp.init_params(seed=11, last_scale=1.0))
         S.lp_config(train_steps=0, warm=100)
+        S.lp_fields(0x1f)                                    # the oracle blends every field
     S, _, _ = _run(abi.PRED_LEARNED, 3, setup)
     y = S.lp_buffer(abi.LP_OUTPUT)
     t = S.lp_buffer(abi.LP_TARGET)
