@@ -58,9 +58,9 @@ def alg_bytes(kind, T, W, coarse):
         "sweep_i": 10 * W,                # line solve: wk4 in/out, tc, hc
         "sweep_j": 10 * W,
         "sweep_k": 10 * W,
-        "xform_i": 9 * W + 6 * T,         # wk4 in/out, sigma, csi3, eta3 (j-face rows: not counted)
-        "xform_j": 9 * W + 6 * T,         # wk4 in/out, sigma, eta3, zet3
-        "xform_k": 5 * W + 11 * T,        # wk4, sigma, zet3, q4 in/out
+        "xform_i": 15 * W,                # wk4 in/out, sigma, csi3, eta3 (metrics stored in W; j-face rows: not counted)
+        "xform_j": 15 * W,                # wk4 in/out, sigma, eta3, zet3
+        "xform_k": 8 * W + 8 * T,         # wk4, sigma, zet3 | q4 in/out
         "dtau": 11 * T,                   # metrics9 nut | dtau
         "norm": 15 * T,                   # q5 qold5 | qold5
         "rsmooth": (20 * W + 8 * T) / 3,  # dq4 in/out in W; the k direction reads dq4 and updates q4 (mean of 3)

@@ -40,6 +40,8 @@ struct Lv {
   const T* aj;
   const T* rj;      // 1/aj, formed once whenever aj is set
   const T* falm;    // actuator-line force added to rh(2:4), [3][N], or null
+  const W* mw[9];   // csi, eta, zet rounded to W once (the same arrays when
+                    // W = T): the modal transforms of the sweeps read these
   // DAF work: transformed residual and row coefficients
   W* wk[4];
   W* sig;          // sigma = sqrt(beta alpha) of each interior node, from the first residual pass

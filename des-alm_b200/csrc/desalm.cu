@@ -298,6 +298,11 @@ int alloc_level(desalm_ctx* ctx, Level& G, Lv<T, W>& L) {
   }
   RET(A((T**)&L.aj));
   RET(A((T**)&L.rj));
+  for (int t = 0; t < 9; ++t) {
+    const T* m = t < 3 ? L.csi[t] : (t < 6 ? L.eta[t - 3] : L.zet[t - 6]);
+    if (sizeof(W) == sizeof(T)) L.mw[t] = (const W*)m;
+    else RET(AW((W**)&L.mw[t]));
+  }
   for (int m = 0; m < 4; ++m) RET(AW(&L.wk[m]));
   RET(AW(&L.sig));
   for (int m = 0; m < 3; ++m) { RET(AW(&L.tc[m])); RET(AW(&L.hc[m])); }
@@ -811,6 +816,21 @@ int refresh_rj(desalm_ctx* ctx, int n) {
   cudaStream_t s = ctx->stream;
   if (kind_of(ctx, n) == K_DD) launch_k(k_recip<double>, cdiv(G.N, 256), 256, 0, s, (double*)G.dd.rj, G.dd.aj, G.N);
   else launch_k(k_recip<double>, cdiv(G.N, 256), 256, 0, s, (double*)G.df.rj, G.df.aj, G.N);
+  CKL();
+  return 0;
+}
+
+// The FP32 copies of a MIXED level's metrics that the sweeps' modal
+// transforms read (the same rounding the transforms applied to the FP64
+// metrics before, so their results do not change); nothing to do in FP64.
+int refresh_mw(desalm_ctx* ctx, int n) {
+  Level& G = ctx->L[n];
+  if (kind_of(ctx, n) == K_DD) return 0;
+  Lv<double, float>& L = G.df;
+  for (int t = 0; t < 9; ++t) {
+    const double* m = t < 3 ? L.csi[t] : (t < 6 ? L.eta[t - 3] : L.zet[t - 6]);
+    launch_k(k_copy<float, double>, cdiv(G.N, 256), 256, 0, ctx->stream, (float*)L.mw[t], m, G.N);
+  }
   CKL();
   return 0;
 }
@@ -1452,6 +1472,7 @@ int desalm_set_grid(desalm_ctx* ctx, const double* x, const double* y, const dou
     }
     CKL();
     RET(refresh_rj(ctx, n));
+    RET(refresh_mw(ctx, n));
     if (n == 0)
       launch_k(k_dtev, cdiv(G.N, 256), 256, 0, s, dcov, ctx->dtev, G.N, c.cfl2, c.vnn2, c.ren, c.delti, c.unsteady);
     CKL();
@@ -1570,6 +1591,7 @@ int desalm_set_field(desalm_ctx* ctx, int n, int f, const double* in) {
     cudaFree(d);
   }
   if (f == DESALM_F_AJ) RET(refresh_rj(ctx, n - 1));
+  if (f >= DESALM_F_CSI && f < DESALM_F_ZET + 3) RET(refresh_mw(ctx, n - 1));
   CK(cudaStreamSynchronize(s));
   if (f == DESALM_F_NUT || (f >= DESALM_F_CSI && f <= DESALM_F_AJ)) ctx->L[n - 1].dtau_valid = false;
   return 0;

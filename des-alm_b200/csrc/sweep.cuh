@@ -327,8 +327,8 @@ __global__ void __launch_bounds__(128) k_xform(Lv<T, W> L) {
       if (j == tgt[s])
 #pragma unroll
         for (int q = 0; q < 4; ++q) L.bj[(s * 4 + q) * S + o] = xv[q];
-    mfwd_apply<W>(W(L.csi[0][l]), W(L.csi[1][l]), W(L.csi[2][l]), sg, xv, y);
-    minv_apply<W>(W(L.eta[0][l]), W(L.eta[1][l]), W(L.eta[2][l]), sg, y, z);
+    mfwd_apply<W>(L.mw[0][l], L.mw[1][l], L.mw[2][l], sg, xv, y);
+    minv_apply<W>(L.mw[3][l], L.mw[4][l], L.mw[5][l], sg, y, z);
 #pragma unroll
     for (int q = 0; q < 4; ++q) L.wk[q][l] = z[q];
   } else if (DIR == 1) {
@@ -339,12 +339,12 @@ __global__ void __launch_bounds__(128) k_xform(Lv<T, W> L) {
       if (k == tgt[s])
 #pragma unroll
         for (int q = 0; q < 4; ++q) L.bk[(s * 4 + q) * S + o] = xv[q];
-    mfwd_apply<W>(W(L.eta[0][l]), W(L.eta[1][l]), W(L.eta[2][l]), sg, xv, y);
-    minv_apply<W>(W(L.zet[0][l]), W(L.zet[1][l]), W(L.zet[2][l]), sg, y, z);
+    mfwd_apply<W>(L.mw[3][l], L.mw[4][l], L.mw[5][l], sg, xv, y);
+    minv_apply<W>(L.mw[6][l], L.mw[7][l], L.mw[8][l], sg, y, z);
 #pragma unroll
     for (int q = 0; q < 4; ++q) L.wk[q][l] = z[q];
   } else {
-    mfwd_apply<W>(W(L.zet[0][l]), W(L.zet[1][l]), W(L.zet[2][l]), sg, xv, y);
+    mfwd_apply<W>(L.mw[6][l], L.mw[7][l], L.mw[8][l], sg, xv, y);
 #pragma unroll
     for (int q = 0; q < 4; ++q) L.q[q][l] = L.q[q][l] + T(y[q]);
   }
