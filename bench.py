@@ -61,7 +61,7 @@ def alg_bytes(kind, T, W, coarse):
         "xform_i": 15 * W,                # wk4 in/out, sigma, csi3, eta3 (metrics stored in W; j-face rows: not counted)
         "xform_j": 15 * W,                # wk4 in/out, sigma, eta3, zet3
         "xform_k": 8 * W + 8 * T,         # wk4, sigma, zet3 | q4 in/out
-        "dtau": 11 * T,                   # metrics9 nut | dtau
+        "dtau": 4 * T,                    # nut, the two metric parts | dtau
         "norm": 15 * T,                   # q5 qold5 | qold5
         "rsmooth": (20 * W + 8 * T) / 3,  # dq4 in/out in W; the k direction reads dq4 and updates q4 (mean of 3)
         "prolong": 4 * W,                 # dq4 out in W (coarse reads amortised)

@@ -32,6 +32,8 @@ struct Lv {
   T* pk[4];        // FAS forcing
   T* nut;
   T* dtau;
+  T* dtc;          // metric parts of dtau: the largest convective limit
+  T* dtv;          // reciprocal, and the viscous one without (1/Re + nu_t)
   T* diss1;        // diss(1) of the first residual pass (reused by the recalc)
   // geometry
   const T* csi[3];

@@ -293,6 +293,7 @@ int alloc_level(desalm_ctx* ctx, Level& G, Lv<T, W>& L) {
   for (int m = 0; m < 5; ++m) { RET(A(&L.q[m])); RET(A(&L.qn[m])); RET(A(&L.qnm1[m])); RET(A(&L.qold[m])); }
   for (int m = 0; m < 4; ++m) { RET(A(&L.rh[m])); RET(A(&L.pk[m])); }
   RET(A(&L.nut)); RET(A(&L.dtau)); RET(A(&L.diss1));
+  RET(A(&L.dtc)); RET(A(&L.dtv));
   for (int d = 0; d < 3; ++d) {
     RET(A((T**)&L.csi[d])); RET(A((T**)&L.eta[d])); RET(A((T**)&L.zet[d]));
   }
@@ -820,11 +821,16 @@ int refresh_rj(desalm_ctx* ctx, int n) {
   return 0;
 }
 
-// The FP32 copies of a MIXED level's metrics that the sweeps' modal
-// transforms read (the same rounding the transforms applied to the FP64
-// metrics before, so their results do not change); nothing to do in FP64.
+// What depends on a level's metrics alone: the metric parts of dtau
+// (k_dtau_pre), and the FP32 copies of a MIXED level's metrics that the
+// sweeps' modal transforms read (the same rounding the transforms applied to
+// the FP64 metrics before, so their results do not change).
 int refresh_mw(desalm_ctx* ctx, int n) {
   Level& G = ctx->L[n];
+  Par P = ctx->par;
+  if (kind_of(ctx, n) == K_DD) launch_k(k_dtau_pre<double, double>, cdiv(G.N, 256), 256, 0, ctx->stream, G.dd, P);
+  else launch_k(k_dtau_pre<double, float>, cdiv(G.N, 256), 256, 0, ctx->stream, G.df, P);
+  CKL();
   if (kind_of(ctx, n) == K_DD) return 0;
   Lv<double, float>& L = G.df;
   for (int t = 0; t < 9; ++t) {

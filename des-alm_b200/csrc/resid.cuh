@@ -319,25 +319,38 @@ __global__ void __launch_bounds__(128, DESALM_KR_MINBLOCKS) k_resid(Lv<T, W> L, 
 // convective limits cfl / (|grad xi_d| dxi_d) and the viscous limits
 // vnn / ((1/Re + nu_t) dxi_d^2 g_dd), formed as 1 / (the largest of their
 // reciprocals) so that a node costs one division; equal to the reference's
-// minimum up to rounding.
+// minimum up to rounding.  The metric parts change only with the grid:
+// k_dtau_pre stores, per node, the largest convective reciprocal and the
+// largest g_dd dxi_d^2 / vnn; k_dtau then needs nu_t and those two (1/Re +
+// nu_t > 0, so the largest viscous reciprocal is (1/Re + nu_t) times the
+// largest of the rest).
+template <class T, class W>
+__global__ void k_dtau_pre(Lv<T, W> L, Par P) {
+  pdl_wait();
+  int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= L.N) return;
+  const T rcfl = T(1) / T(P.cfl1), rvnn = T(1) / T(P.vnn1);
+  const T dcsq = L.dc * L.dc, desq = L.de * L.de, dzsq = L.dz * L.dz;
+  T g1 = L.csi[0][l] * L.csi[0][l] + L.csi[1][l] * L.csi[1][l] + L.csi[2][l] * L.csi[2][l];
+  T g2 = L.eta[0][l] * L.eta[0][l] + L.eta[1][l] * L.eta[1][l] + L.eta[2][l] * L.eta[2][l];
+  T g3 = L.zet[0][l] * L.zet[0][l] + L.zet[1][l] * L.zet[1][l] + L.zet[2][l] * L.zet[2][l];
+  T c = sqrt(g1) * L.dc * rcfl;
+  c = dmax(c, sqrt(g2) * L.de * rcfl);
+  c = dmax(c, sqrt(g3) * L.dz * rcfl);
+  T v = dcsq * g1 * rvnn;
+  v = dmax(v, desq * g2 * rvnn);
+  v = dmax(v, dzsq * g3 * rvnn);
+  L.dtc[l] = c;
+  L.dtv[l] = v;
+}
+
 template <class T, class W>
 __global__ void k_dtau(Lv<T, W> L, Par P) {
   pdl_wait();
   int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= L.N) return;
-  const T rcfl = T(1) / T(P.cfl1), rvnn = T(1) / T(P.vnn1), rei = T(1) / T(P.ren);
-  const T dcsq = L.dc * L.dc, desq = L.de * L.de, dzsq = L.dz * L.dz;
-  T g1 = L.csi[0][l] * L.csi[0][l] + L.csi[1][l] * L.csi[1][l] + L.csi[2][l] * L.csi[2][l];
-  T g2 = L.eta[0][l] * L.eta[0][l] + L.eta[1][l] * L.eta[1][l] + L.eta[2][l] * L.eta[2][l];
-  T g3 = L.zet[0][l] * L.zet[0][l] + L.zet[1][l] * L.zet[1][l] + L.zet[2][l] * L.zet[2][l];
-  T ret = rei + L.nut[l];
-  T m = sqrt(g1) * L.dc * rcfl;
-  m = dmax(m, sqrt(g2) * L.de * rcfl);
-  m = dmax(m, sqrt(g3) * L.dz * rcfl);
-  m = dmax(m, ret * dcsq * g1 * rvnn);
-  m = dmax(m, ret * desq * g2 * rvnn);
-  m = dmax(m, ret * dzsq * g3 * rvnn);
-  L.dtau[l] = T(1) / m;
+  const T ret = T(1) / T(P.ren) + L.nut[l];
+  L.dtau[l] = T(1) / dmax(L.dtc[l], ret * L.dtv[l]);
 }
 
 }  // namespace desalm
