@@ -133,6 +133,7 @@ struct LpState {
   float *y = nullptr, *t = nullptr;        // network output, training target [5][N]
   float *rs = nullptr, *rs5 = nullptr, *s5 = nullptr;  // feature scales (1/RMS), target scales, output scales
   double* acc = nullptr;                   // reductions
+  double* red = nullptr;                   // their per-CTA partial sums [kLpRedBlocks][16]
   double* vacc = nullptr;                  // held-out check of the newest sample (k_lp_dot)
   float* alpha = nullptr;                  // blend of each field's correction
   float fixed_alpha = -1.0f;               // < 0: automatic blend
@@ -918,6 +919,7 @@ int sa_conservation(desalm_ctx* ctx);
 
 // ----------------------------------------------------------- learned guess
 constexpr int kLpWgradGrid = 148;  // partial slots of k_lp_wgrad_tc (one CTA per SM)
+constexpr int kLpRedBlocks = 296;  // CTAs (and partial rows) of the learned guess's reductions
 
 // cuTensorMapEncodeTiled, reached through the runtime's driver entry point
 typedef CUresult (*LpEncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -1052,6 +1054,7 @@ int lp_alloc(desalm_ctx* ctx) {
   RET(A((void**)&lp.y, 5L * N * sizeof(float))); RET(A((void**)&lp.t, 5L * N * sizeof(float)));
   RET(A((void**)&lp.rs, 16 * sizeof(float))); RET(A((void**)&lp.rs5, 8 * sizeof(float)));
   RET(A((void**)&lp.s5, 8 * sizeof(float))); RET(A((void**)&lp.acc, 16 * sizeof(double)));
+  RET(A((void**)&lp.red, kLpRedBlocks * 16 * sizeof(double)));
   RET(A((void**)&lp.vacc, 16 * sizeof(double))); RET(A((void**)&lp.alpha, 8 * sizeof(float)));
   for (int f = 0; f < 5; ++f) RET(A((void**)&lp.qnm2[f], N * sizeof(double)));
   RET(A((void**)&lp.nut0, N * sizeof(double)));
@@ -1111,8 +1114,8 @@ int lp_backward(desalm_ctx* ctx, double* loss) {
   LpState& lp = ctx->lp;
   cudaStream_t s = ctx->stream;
   const long N = lp.N;
-  CK(cudaMemsetAsync(lp.acc, 0, sizeof(double), s));
-  LAUNCH(KC_LEARN, 0, (double)N, launch_k(k_lp_loss, 296, 256, 0, s, lp.P, (const float*)lp.y, (const float*)lp.t, lp.dy4, lp.acc));
+  LAUNCH(KC_LEARN, 0, (double)N, launch_k(k_lp_loss, kLpRedBlocks, 256, 0, s, lp.P, (const float*)lp.y, (const float*)lp.t, lp.dy4, lp.red));
+  LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_fold, 1, 32, 0, s, (const double*)lp.red, kLpRedBlocks, 1, lp.acc));
   CKL();
   // layer 4 (a[2] -> y)
   RET((lp_wgrad<32, 16>(ctx, lp.tm_a[2], lp.tm_dy4, lp.dW[3])));
@@ -1149,8 +1152,8 @@ int lp_features(desalm_ctx* ctx, int a, int b, int c) {
   const double* const* A = (const double* const*)(lp.tab + a);
   const double* const* B = (const double* const*)(lp.tab + b);
   const double* const* C = (const double* const*)(lp.tab + c);
-  CK(cudaMemsetAsync(lp.acc, 0, 16 * sizeof(double), s));
-  LAUNCH(KC_LEARN, 0, (double)N, launch_k(k_lp_sumsq, 296, 128, 0, s, N, A, B, C, lp.acc));
+  LAUNCH(KC_LEARN, 0, (double)N, launch_k(k_lp_sumsq, kLpRedBlocks, 128, 0, s, N, A, B, C, lp.red));
+  LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_fold, 1, 32, 0, s, (const double*)lp.red, kLpRedBlocks, 15, lp.acc));
   LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_scales, 1, 32, 0, s, N, (const double*)lp.acc, lp.rs, lp.rs5, lp.s5));
   LAUNCH(KC_LEARN, 0, (double)N, launch_k(k_lp_features, cdiv(N, 256), 256, 0, s, lp.P, A, B, C, (const float*)lp.rs, lp.x0));
   CKL();
@@ -1188,9 +1191,9 @@ int lp_learn(desalm_ctx* ctx) {
   // held-out check: the current network on the new sample, before training on it
   RET(lp_pack(ctx));
   RET(lp_forward(ctx));
-  CK(cudaMemsetAsync(lp.vacc, 0, 16 * sizeof(double), ctx->stream));
-  LAUNCH(KC_LEARN, 0, (double)lp.N, launch_k(k_lp_dot, 296, 128, 0, ctx->stream, lp.N, (const float*)lp.y,
-                                             (const float*)lp.t, lp.ymax, lp.vacc));
+  LAUNCH(KC_LEARN, 0, (double)lp.N, launch_k(k_lp_dot, kLpRedBlocks, 128, 0, ctx->stream, lp.N, (const float*)lp.y,
+                                             (const float*)lp.t, lp.ymax, lp.red));
+  LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_fold, 1, 32, 0, ctx->stream, (const double*)lp.red, kLpRedBlocks, 15, lp.vacc));
   LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_blend, 1, 32, 0, ctx->stream, (const double*)lp.vacc, lp.fixed_alpha, lp.field_mask, lp.alpha));
   CKL();
   lp.samples += 1;

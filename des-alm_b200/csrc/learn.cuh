@@ -119,10 +119,22 @@ __global__ void k_lp_rows_out(LpPad P, int C, int c0, int nc, const bf16* __rest
   for (int c = 0; c < nc; ++c) a[(long)c * P.N + l] = __bfloat162float(rows[p * C + c0 + c]);
 }
 
-// Sums of squares of the 15 feature channels (before scaling) and of the
-// target's second difference, for the RMS scales: acc[16] doubles.
+// The reductions below leave one row of 16 partial sums per CTA in part
+// (part[16 b + c]); k_lp_fold then adds the rows in CTA order, so that every
+// sum is the same from run to run.
+__global__ void k_lp_fold(const double* __restrict__ part, int nblk, int nc, double* __restrict__ acc) {
+  pdl_wait();
+  const int c = threadIdx.x;
+  if (c >= nc) return;
+  double s = 0.0;
+  for (int b = 0; b < nblk; ++b) s += part[16 * b + c];
+  acc[c] = s;
+}
+
+// Sums of squares of the 15 feature channels (before scaling): the partial
+// sums of the RMS scales (k_lp_fold gives acc[0..14]).
 __global__ void k_lp_sumsq(long N, const double* const* qn, const double* const* qnm1, const double* const* qnm2,
-                           double* acc) {
+                           double* part) {
   pdl_wait();
   __shared__ double sh[15][128];
   double s[15];
@@ -146,7 +158,7 @@ __global__ void k_lp_sumsq(long N, const double* const* qn, const double* const*
       for (int c = 0; c < 15; ++c) sh[c][threadIdx.x] += sh[c][threadIdx.x + w];
     __syncthreads();
   }
-  if (threadIdx.x < 15) atomicAdd(acc + threadIdx.x, sh[threadIdx.x][0]);
+  if (threadIdx.x < 15) part[16 * blockIdx.x + threadIdx.x] = sh[threadIdx.x][0];
 }
 
 // Scales from the sums of squares acc[0..14] (one thread block of 32):
@@ -185,11 +197,11 @@ __global__ void k_lp_target(long N, const double* const* q, const double* const*
 }
 
 // Squared error of the network output y against t over the 5 output
-// channels: loss partial sums (acc[0], double) and dY = y - t in BF16 into
+// channels: loss partial sums (part, column 0) and dY = y - t in BF16 into
 // the channel-last padded rows dY[p][16] (channels 5..15 stay zero); the
 // factor 2 / (5 N) of the mean goes into the gradient scale.
 __global__ void k_lp_loss(LpPad P, const float* __restrict__ y, const float* __restrict__ t, bf16* __restrict__ dY,
-                          double* acc) {
+                          double* part) {
   pdl_wait();
   __shared__ double sh[256];
   double s = 0.0;
@@ -209,13 +221,13 @@ __global__ void k_lp_loss(LpPad P, const float* __restrict__ y, const float* __r
     if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
     __syncthreads();
   }
-  if (threadIdx.x == 0) atomicAdd(acc, sh[0]);
+  if (threadIdx.x == 0) part[16 * blockIdx.x] = sh[0];
 }
 
 // Held-out check of the network on a new sample, before it trains on it:
-// per field f, acc[f] += sum y_f t_f, acc[5 + f] += sum y_f^2,
-// acc[10 + f] += sum t_f^2 (y clipped to [-ymax, ymax] as in the guess).
-__global__ void k_lp_dot(long N, const float* __restrict__ y, const float* __restrict__ t, float ymax, double* acc) {
+// partial sums of, per field f, y_f t_f (column f), y_f^2 (5 + f) and t_f^2
+// (10 + f), y clipped to [-ymax, ymax] as in the guess.
+__global__ void k_lp_dot(long N, const float* __restrict__ y, const float* __restrict__ t, float ymax, double* part) {
   pdl_wait();
   __shared__ double sh[15][128];
   double s[15];
@@ -241,7 +253,7 @@ __global__ void k_lp_dot(long N, const float* __restrict__ y, const float* __res
       for (int c = 0; c < 15; ++c) sh[c][threadIdx.x] += sh[c][threadIdx.x + w];
     __syncthreads();
   }
-  if (threadIdx.x < 15) atomicAdd(acc + threadIdx.x, sh[threadIdx.x][0]);
+  if (threadIdx.x < 15) part[16 * blockIdx.x + threadIdx.x] = sh[threadIdx.x][0];
 }
 
 // Blend of each field's correction: automatic (fixed < 0): the least-squares

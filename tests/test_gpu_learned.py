@@ -131,6 +131,21 @@ def test_masked_fields_keep_the_linear_guess():
     assert S.lp_report()["alpha"][1:] == [0.0] * 4
 
 
+def test_learned_runs_repeat_bit_for_bit():
+    """The learned guess's sums (scales, loss, held-out dots) add their
+    per-CTA partials in a fixed order, so two identical runs agree bit for
+    bit: parameters, report and state."""
+    def setup(S):
+        S.lp_config(train_steps=3, warm=1)
+    A, sa, ra = _run(abi.PRED_LEARNED, 4, setup)
+    B, sb, rb = _run(abi.PRED_LEARNED, 4, setup)
+    assert np.array_equal(A.lp_params(), B.lp_params())
+    assert A.lp_report() == B.lp_report()
+    for k in ("q", "qn", "qnm1", "nut"):
+        assert np.array_equal(sa[k], sb[k]), k
+    assert [r["iterations"] for r in ra] == [r["iterations"] for r in rb]
+
+
 def test_non_finite_network_output_falls_back_to_linear():
     def setup(S):
         th = np.zeros(lp.nparam(), np.float32)
