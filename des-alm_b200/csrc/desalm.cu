@@ -583,15 +583,15 @@ int launch_bcond(desalm_ctx* ctx, Lv<T, W>& L) {
   P.fine = 1;
   cudaStream_t s = ctx->stream;
   const T* rat = (const T*)ctx->rat;
-  LAUNCH(KC_BCOND, 0, 2.0 * L.jm * L.km, launch_k(k_bcond<T, W, 0>, dim3(cdiv(L.jm, 64), L.km), 64, 0, s, L, P, rat, ctx->ratdim));
-  CKL();
-  LAUNCH(KC_BCOND, 0, 2.0 * L.im * L.km, launch_k(k_bcond<T, W, 1>, dim3(cdiv(L.im, 64), L.km), 64, 0, s, L, P, rat, ctx->ratdim));
-  CKL();
-  LAUNCH(KC_BCOND, 0, 2.0 * L.im * L.jm, launch_k(k_bcond<T, W, 2>, dim3(cdiv(L.im, 64), L.jm), 64, 0, s, L, P, rat, ctx->ratdim));
-  CKL();
   const desalm_case& c = ctx->c;
-  int lfix = (c.ifix - 1) + L.sj * (c.jfix - 1) + L.sk * (c.kfix - 1);
-  LAUNCH(KC_PFIX, 0, 1, launch_k(k_pfix_read<T, W>, 1, 1, 0, s, L, lfix, (T*)ctx->pfix));
+  const int lfix = (c.ifix - 1) + L.sj * (c.jfix - 1) + L.sk * (c.kfix - 1);
+  T* pfix = (T*)ctx->pfix;
+  LAUNCH(KC_BCOND, 0, 2.0 * L.jm * L.km, launch_k(k_bcond<T, W, 0>, dim3(cdiv(L.jm, 64), L.km), 64, 0, s, L, P, rat, ctx->ratdim, -1, -1, lfix, pfix));
+  CKL();
+  LAUNCH(KC_BCOND, 0, 2.0 * L.im * L.km, launch_k(k_bcond<T, W, 1>, dim3(cdiv(L.im, 64), L.km), 64, 0, s, L, P, rat, ctx->ratdim, -1, -1, lfix, pfix));
+  CKL();
+  // the k faces, then p(ifix, jfix, kfix) into pfix
+  LAUNCH(KC_BCOND, 0, 2.0 * L.im * L.jm, launch_k(k_bcond<T, W, 2>, dim3(cdiv(L.im, 64), L.jm), 64, 0, s, L, P, rat, ctx->ratdim, c.ifix - 1, c.jfix - 1, lfix, pfix));
   CKL();
   LAUNCH(KC_PFIX, 0, L.N, launch_k(k_pfix_sub<T, W>, cdiv(L.N, 256), 256, 0, s, L, (const T*)ctx->pfix));
   CKL();

@@ -11,8 +11,12 @@ namespace desalm {
 // and applies the low face before the high face.  i_mysta/i_myend are the
 // boundary nodes themselves there (src/bcond_fm.F90:60-66), so every kernel
 // covers the full transverse range (edges and corners included).
+// The k-face kernel also reads the pressure reference value p(ifix, jfix,
+// kfix) after the face updates (src/bcond_fm.F90:310), in the thread of the
+// (i, j) column through that node: it is the only one that writes there, and
+// the i and j face kernels before it have finished.
 template <class T, class W, int DIR>
-__global__ void k_bcond(Lv<T, W> L, Par P, const T* rat, int ratdim) {
+__global__ void k_bcond(Lv<T, W> L, Par P, const T* rat, int ratdim, int fix_a, int fix_b, int lfix, T* pfix) {
   pdl_wait();
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   const int b = blockIdx.y;
@@ -42,13 +46,7 @@ __global__ void k_bcond(Lv<T, W> L, Par P, const T* rat, int ratdim) {
       for (int m = 0; m < 4; ++m) L.q[m][l] = L.q[m][l - 1];
     }
   }
-}
-
-// pressure reference value after the face updates (src/bcond_fm.F90:310)
-template <class T, class W>
-__global__ void k_pfix_read(Lv<T, W> L, int lfix, T* pfix) {
-  pdl_wait();
-  *pfix = L.q[0][lfix];
+  if (DIR == 2 && a == fix_a && b == fix_b) *pfix = L.q[0][lfix];
 }
 // p <- p - pfix over the whole level (src/bcond_fm.F90:316-322)
 template <class T, class W>
