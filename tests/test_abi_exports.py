@@ -51,3 +51,19 @@ def test_invalid_case_is_rejected_without_gpu():
     with pytest.raises(DesalmError) as e:
         Solver(case)
     assert "wall_functions" in str(e.value)
+
+
+def test_entry_points_reject_null_arguments_without_gpu():
+    """Host-side argument checks that return before any CUDA call."""
+    from desalm import abi
+    from desalm.solver import lib
+    L = lib()
+    assert L.desalm_mg_driver_batch(None, 1, None) == abi.DESALM_EINVAL
+    ctxs = (C.c_void_p * 2)(None, None)
+    assert L.desalm_mg_driver_batch(ctxs, 2, None) == abi.DESALM_EINVAL
+    assert L.desalm_mg_driver_batch(ctxs, -1, None) == abi.DESALM_EINVAL
+    assert L.desalm_mg_driver_batch(ctxs, 0, None) == 0          # nothing to step
+    out = (C.c_int * 12)()
+    assert L.desalm_sweep_widths(None, out) == abi.DESALM_EINVAL
+    assert L.desalm_wall_functions(None) == abi.DESALM_EINVAL
+    assert L.desalm_lp_fields(None, 1) == abi.DESALM_EINVAL
