@@ -8,6 +8,10 @@ identities of the mathematics it implements:
     difference q(im) - q(im-1) and divided by J: checked against numpy's
     eigen-decomposition of A on a sheared affine grid, for outflow (ucon > 0:
     three outgoing characteristics) and backflow (ucon < 0: one);
+  * mg_brhs's 2D residual equals the interior residual of any plane when the
+    state does not vary along i on an affine grid (every csi term and the
+    LODI terms vanish then), which pins the brhs_* restatement on the
+    interior residual's;
   * a uniform stream is a fixed point of a DAF step with the outlet solved;
   * rhs_sa_bcond's btype-5 rows extrapolate nu_tilde with the grid ratio
     (src/rhs_sa_bcond.F90:61-67, 98-104, 144-150, 181-187);
@@ -131,3 +135,29 @@ def test_btype5_side_faces_keep_their_values(oracle_mod):
         assert np.array_equal(b[1:-1, jb, 1:-1, 1:4], a[1:-1, jb, 1:-1, 1:4])
     # the outlet plane is solved
     assert np.abs(b[1:-1, 1:-1, -1, 1:4] - a[1:-1, 1:-1, -1, 1:4]).max() > 1e-6
+
+
+def test_plane_residual_equals_interior_residual_without_i_variation(oracle_mod):
+    """mg_brhs's terms are the interior residual's eta and zeta terms: on an
+    affine grid with a state that does not vary along i (so every csi term of
+    the interior residual vanishes, and so do the LODI terms, dq = 0), the
+    outlet plane's residual equals the interior residual of any plane."""
+    n = 13
+    case, grid = _affine_case(n)
+    o = oracle_mod.OracleSolver(case)
+    o.set_grid(grid["x"], grid["y"], grid["z"])
+    rng = np.random.default_rng(8)
+    q = np.zeros((n, n, n, 5))                       # [k][j][i][m]
+    q[..., :4] = rng.normal(0.0, 0.3, size=(n, n, 1, 4))
+    q[..., 1] += 1.0
+    qn = q.copy()
+    qn[..., :4] += rng.normal(0.0, 1e-2, size=(n, n, 1, 4))
+    qnm1 = qn.copy()
+    qnm1[..., :4] += rng.normal(0.0, 1e-2, size=(n, n, 1, 4))
+    o.set_state(q.reshape(-1), qn.reshape(-1), qnm1.reshape(-1))
+    plane = o.outlet_rhs()                           # (4, km, jm)
+    rh = np.stack([o.get_field(1, abi.F_RH + m).reshape(n, n, n) for m in range(4)])
+    assert np.abs(plane).max() > 1e-3
+    for i0 in (3, n // 2, n - 2):
+        interior = rh[:, 1:-1, 1:-1, i0]
+        assert np.allclose(plane[:, 1:-1, 1:-1], interior, rtol=1e-10, atol=1e-12 * np.abs(interior).max())
