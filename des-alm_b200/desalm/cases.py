@@ -15,6 +15,8 @@ Presets
            20 D, span pi D), SA, Re = 3900, delti = 0.005.
   wake     open box with uniform inflow and the characteristics outlet
            (btype 5), stretched and perturbed grid, SA or laminar.
+  turbine  actuator-line turbine box 10 D x 5 D x 5 D (385 x 193 x 193), a
+           3-blade rotor, TSR 7, eps = 0.05 D, inflow, outlet, SA.
 """
 import numpy as np
 
@@ -234,7 +236,7 @@ def ogrid(im=257, jm=129, km=65, seed=0, re=3900.0, rfar=20.0, itmax=400):
 
 
 def alm_rotor(xs, ys, zs, center, radius, nblades=3, nelems=12, nangles=24, tsr=7.0, hub_frac=0.1,
-              length_scale=1.0, vel_infty=0.1, angle=0.3, seed=0, ker_cells=3):
+              length_scale=1.0, vel_infty=0.1, angle=0.3, seed=0, ker_cells=3, eps=None, narrow_polar=True):
     """Seeded synthetic actuator-line tables for one rotor on a product grid
     (coordinates xs[i], ys[j], zs[k]) with its plane normal to x, as the
     reference's init_lines places it (src/init.F90:1446-1535): element elem
@@ -242,7 +244,12 @@ def alm_rotor(xs, ys, zs, center, radius, nblades=3, nelems=12, nangles=24, tsr=
     r_e = radius elem / nelems and th = nang 2 pi / nangles.  Lengths are grid
     units except tur_rad and hub_rad (m = grid units x length_scale).  Three
     polars: wide, medium and one so narrow ([-2, 2] degrees) that many
-    elements fall outside it.  Returns the turbine dict and the polars."""
+    elements fall outside it (narrow_polar=False: a second wide one instead).
+    The Gaussian width is the reference's eps = 2 dV^(1/3) of each kernel
+    node (src/rhs_lines.F90:434); eps (grid units) fixes it instead: the
+    kernel nodes are those within 3 eps of the rotor disc, and each carries
+    dV = (eps / 2)^3, so that 2 dV^(1/3) = eps.  Returns the turbine dict and
+    the polars."""
     rng = np.random.default_rng(seed)
     im, jm, km = len(xs), len(ys), len(zs)
     xc, yc, zc = center
@@ -281,7 +288,8 @@ def alm_rotor(xs, ys, zs, center, radius, nblades=3, nelems=12, nangles=24, tsr=
     disk[..., 6] = rng.uniform(0.0, 1.0, size=r.shape)
     disk[..., 7] = 0.2
     polars = []
-    for lo, hi, n in ((-30.0, 30.0, 25), (-12.0, 16.0, 15), (-2.0, 2.0, 5)):
+    spans = ((-30.0, 30.0, 25), (-12.0, 16.0, 15), (-2.0, 2.0, 5) if narrow_polar else (-90.0, 90.0, 37))
+    for lo, hi, n in spans:
         a = np.linspace(lo, hi, n)
         cl = 2 * np.pi * np.deg2rad(a) * (1.0 + 0.05 * rng.normal(size=n))
         cd = 0.01 + 0.02 * (np.deg2rad(a)) ** 2 + 0.001 * rng.uniform(size=n)
@@ -293,11 +301,15 @@ def alm_rotor(xs, ys, zs, center, radius, nblades=3, nelems=12, nangles=24, tsr=
     K3, J3, I3 = np.meshgrid(np.arange(2, km), np.arange(2, jm), np.arange(2, im), indexing="ij")
     X3, Y3, Z3 = xs[I3 - 1], ys[J3 - 1], zs[K3 - 1]
     R3 = np.hypot(Y3 - yc, Z3 - zc)
-    sel = (np.abs(X3 - xc) <= ker_cells * dx) & (R3 <= radius + ker_cells * h)  # k, j, i order
+    if eps is None:
+        sel = (np.abs(X3 - xc) <= ker_cells * dx) & (R3 <= radius + ker_cells * h)  # k, j, i order
+        dV = (gx[I3 - 1] * gy[J3 - 1] * gz[K3 - 1])[sel]
+    else:
+        sel = (np.abs(X3 - xc) <= 3.0 * eps) & (R3 <= radius + 3.0 * eps)
+        dV = np.full(int(sel.sum()), (0.5 * eps) ** 3)
     ker_index = np.column_stack([I3[sel], J3[sel], K3[sel]])
     ker_pos = np.column_stack([X3[sel], Y3[sel], Z3[sel]])
-    ker_dat = np.column_stack([R3[sel], (gy[J3 - 1] * gz[K3 - 1])[sel], np.arctan2(Z3 - zc, Y3 - yc)[sel],
-                               (gx[I3 - 1] * gy[J3 - 1] * gz[K3 - 1])[sel]])
+    ker_dat = np.column_stack([R3[sel], (gy[J3 - 1] * gz[K3 - 1])[sel], np.arctan2(Z3 - zc, Y3 - yc)[sel], dV])
     tur = dict(nblades=nblades, nelems=nelems, nangles=nangles, tsr=tsr,
                tur_rad=radius * length_scale, hub_rad=hub_frac * radius * length_scale, angle=angle,
                node_index=np.array(node_index, np.int32), node_pos=np.array(node_pos),
@@ -379,6 +391,78 @@ def channel_alm(im=33, jm=25, km=25, itmax=20, n_tur=1, seed=0):
         polars = pol if polars is None else polars
     spec = dict(turbines=turs, polars=polars, vel_infty=0.1, length_scale=1.0)
     return case, grid, state, spec
+
+
+def _sinh_cluster(n, length, centre, c):
+    """n nodes on [0, length] clustered at x = centre: x = centre + B sinh(c (s - s0)),
+    s uniform on [0, 1], s0 and B chosen so that the ends land on 0 and length."""
+    s = np.linspace(0.0, 1.0, n)
+    ratio = (length - centre) / centre
+    lo, hi = 1e-6, 1.0 - 1e-6
+    for _ in range(200):      # sinh(c (1 - s0)) / sinh(c s0) = ratio
+        s0 = 0.5 * (lo + hi)
+        if np.sinh(c * (1.0 - s0)) / np.sinh(c * s0) > ratio:
+            lo = s0
+        else:
+            hi = s0
+    s0 = 0.5 * (lo + hi)
+    B = centre / np.sinh(c * s0)
+    x = centre + B * np.sinh(c * (s - s0))
+    x[0], x[-1] = 0.0, length
+    return x
+
+
+def turbine(im=385, jm=193, km=193, seed=0, re=1.0e5, itmax=400, delti=0.005, nelems=40, nangles=72,
+            eps=0.05, stretch=2.0, ng=3, polar_seed=0):
+    """Actuator-line turbine box: a 3-blade rotor of diameter D = 1 (the
+    length unit) at (2.5, 2.5, 2.5) in a [0, 10] x [0, 5] x [0, 5] box
+    (10 D x 5 D x 5 D), its plane normal to x; tip-speed ratio 7; Gaussian
+    projection of width eps = 0.05 D; seeded synthetic polars (alm_rotor).
+    The grid is a product of sinh-clustered lines (finest at the rotor,
+    growing toward every face), uniform inflow u = 1 at i = 1 (btype 4), the
+    characteristics outlet at i = im (btype 5) and symmetry planes on the
+    j and k faces; SA with nu_tilde = 3 nu and no walls (wall distance 10).
+    Velocities are scaled by vel_infty = Re 1e-6 / length_scale (0.1 m/s
+    for Re_D = 1e5 and D = 1 m), so that the free stream is u = 1.
+    Returns (case, grid, state, alm spec, omega), omega the rotor's angular
+    speed in radians per unit of nondimensional time (D / U): the driver
+    advances each azimuth by omega * delti between physical steps."""
+    rng = np.random.default_rng(seed)
+    c = _base_case(im, jm, km)
+    c.ng = ng
+    c.ren = re
+    c.itmax = itmax
+    c.delti = delti
+    c.turbulence = 1
+    c.btype[0], c.btype[1] = BC_INFLOW, BC_OUTLET
+    c.btype[2] = c.btype[3] = BC_SYMMETRY
+    c.btype[4] = c.btype[5] = BC_SYMMETRY
+    c.ifix, c.jfix, c.kfix = im - 1, 2, 2
+    xs = _sinh_cluster(im, 10.0, 2.5, stretch)
+    ys = _sinh_cluster(jm, 5.0, 2.5, stretch)
+    zs = _sinh_cluster(km, 5.0, 2.5, stretch)
+    X, Y, Z = _mesh(xs, ys, zs)
+    N = im * jm * km
+    grid = dict(x=_flat(X), y=_flat(Y), z=_flat(Z), wd=np.full(N, 10.0))
+    q = np.zeros((km, jm, im, 5))
+    q[..., 1] = 1.0
+    q[..., 1:4] += rng.normal(0.0, 1e-3, size=(km, jm, im, 3))
+    q[:, :, 0, 1] = 1.0
+    q[:, :, 0, 2:4] = 0.0
+    q[:, 0, :, 2] = q[:, -1, :, 2] = 0.0
+    q[0, :, :, 3] = q[-1, :, :, 3] = 0.0
+    q[..., 4] = 3.0 / re
+    q = q.reshape(-1)
+    nut = _sa_fv1(q[4::5], re)
+    state = dict(q=q.copy(), qn=q.copy(), qnm1=q.copy(), nut=nut)
+    length_scale = 1.0
+    vel = re * 1e-6 / length_scale
+    tur, polars = alm_rotor(xs, ys, zs, (2.5, 2.5, 2.5), 0.5, nblades=3, nelems=nelems, nangles=nangles,
+                            tsr=7.0, length_scale=length_scale, vel_infty=vel, angle=0.3, seed=polar_seed,
+                            eps=eps, narrow_polar=False)
+    spec = dict(turbines=[tur], polars=polars, vel_infty=vel, length_scale=length_scale)
+    omega = 7.0 * 1.0 / 0.5          # TSR U / R in units of U / D
+    return c, grid, state, spec, omega
 
 
 PRESETS = {"cavity": cavity, "channel": channel, "ogrid": ogrid, "wake": wake}

@@ -231,18 +231,23 @@ int  desalm_kernel_stats(desalm_ctx* ctx, double* ms, long* launches,
 int  desalm_kernel_class_count(void);
 
 /* No counterpart in the reference.  desalm_mg_residual for callers that
- * cannot allocate device memory (code running under CUDA stream capture,
- * hosts whose device memory belongs to another allocator): the same five
+ * cannot allocate device memory: Fortran drivers whose device arrays belong
+ * to another runtime or pool allocator that must see every allocation, and
+ * processes held to a fixed device-memory budget.  It gives the same five
  * log10 mean |q - qold| values over the interior of an im x jm x km level,
  * from caller-owned device arrays q and qold (five fields of im*jm*km
- * doubles each, field-major, i fastest), written to the host array res.
- * Allocates nothing: its scratch is a fixed device array of about 2.5 MiB
- * held by every GPU that loads the library until exit.  Grids with more than
- * 134,217,728 interior nodes do not fit it and are rejected with
- * DESALM_ENOMEM before any work is queued.  Calls share the
- * scratch, so calls that overlap on the GPU race; the first call on each
- * device resolves the scratch's address and should come before any stream
- * capture.  stream may be NULL (the legacy default stream). */
+ * doubles each, field-major, i fastest), written to the host array res; the
+ * call waits for its own work on `stream` before it returns.  It calls no
+ * cudaMalloc, cudaFree or allocating library routine: its scratch is a fixed
+ * device array of about 2.5 MiB that every GPU loading the library holds
+ * until exit.  Grids with more than 134,217,728 interior nodes (512^3) do not
+ * fit it and are rejected with DESALM_ENOMEM before any work is queued;
+ * null arrays give DESALM_EINVAL.  Calls share the scratch, so calls that
+ * overlap on the GPU race.  The first call on each device, with that device
+ * current, looks up the scratch's device address and keeps it for the
+ * process: make that first call before any stream capture, and do not call
+ * cudaDeviceReset after it.  stream may be NULL (the legacy default
+ * stream). */
 int  desalm_mg_residual_noalloc(const double* q, const double* qold, int im,
                                 int jm, int km, double res[5], void* stream);
 

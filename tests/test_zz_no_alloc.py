@@ -1,18 +1,17 @@
 """desalm_mg_residual_noalloc: the convergence norm for callers that cannot
-allocate device memory (for example while a CUDA stream is being captured
-into a graph, or when a Fortran host's device memory belongs to another
-allocator).  It must give the same five log10 values as the context's
+allocate device memory (a Fortran host whose device arrays belong to another
+runtime or pool allocator, or a process held to a fixed device-memory
+budget).  It must give the same five log10 values as the context's
 desalm_mg_residual on the same q and qold, call after call, while the
 library allocates nothing for it (its scratch is a fixed device array).
 
 This file is collected last on purpose; it runs alone or after the others.
+The argument checks run on the host only and need no GPU.
 """
 import ctypes as C
 
 import numpy as np
 import pytest
-
-pytestmark = pytest.mark.gpu
 
 
 def _noalloc_fn():
@@ -24,6 +23,7 @@ def _noalloc_fn():
     return f
 
 
+@pytest.mark.gpu
 def test_noalloc_residual_matches_context_residual():
     import torch
     from desalm import abi, cases
@@ -48,14 +48,24 @@ def test_noalloc_residual_matches_context_residual():
         finite = np.isfinite(want)
         assert np.array_equal(finite, np.isfinite(got))
         assert np.allclose(got[finite], want[finite], rtol=0, atol=1e-12), (call, got, want)
+    S.close()
 
 
-def test_noalloc_rejects_oversized_grid():
-    """1026^3 nodes (1024^3 interior) is beyond the fixed scratch: rejected
-    with DESALM_ENOMEM on the host.  The arrays passed are null, so nothing
-    could be launched even if the size check were wrong (that would return
-    DESALM_EINVAL instead)."""
+def _nblk(im, jm, km):
+    return -(-((im - 2) * (jm - 2) * (km - 2)) // 2048)
+
+
+def test_noalloc_size_limit_and_null_arrays():
+    """The size check comes first, then the pointers, both on the host before
+    any CUDA call, so null arrays make every case here launch-free.
+    514^3 nodes (512^3 interior, exactly 65,536 partials) fit the scratch:
+    with null arrays that is DESALM_EINVAL.  514 x 514 x 515 and 1026^3 do
+    not fit: DESALM_ENOMEM.  A small valid grid with null arrays: EINVAL."""
+    assert _nblk(514, 514, 514) == 65536 and _nblk(514, 514, 515) > 65536
     f = _noalloc_fn()
     got = (C.c_double * 5)()
-    rc = f(None, None, 1026, 1026, 1026, got, None)
-    assert rc == -2
+    assert f(None, None, 514, 514, 514, got, None) == -1
+    assert f(None, None, 514, 514, 515, got, None) == -2
+    assert f(None, None, 1026, 1026, 1026, got, None) == -2
+    assert f(None, None, 17, 17, 17, got, None) == -1
+    assert f(None, None, 2, 17, 17, got, None) == -1
