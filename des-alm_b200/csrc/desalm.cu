@@ -25,6 +25,7 @@
 #include "learn.cuh"
 #include "learn_tc.cuh"
 #include "alm.cuh"
+#include "kw.cuh"
 #include "outlet.cuh"
 #include "wallfn.cuh"
 
@@ -199,6 +200,8 @@ struct desalm_ctx {
   } alm;                      // actuator-line forcing (rhs_lines)
   int* flags = nullptr;       // device [2]
   SaWork sa{};
+  KwWork kw{};                // k-omega work (turbulence = 2)
+  double ckin = 1.0e-10, cein = 1.0e-6;  // k and omega floors on extrapolated faces
   // per-kernel CUDA-event timing (desalm_profile) and launch counter
   struct ProfRec { int cls, lvl; double nodes; cudaEvent_t a, b; };
   bool prof_on = false;
@@ -330,6 +333,7 @@ int check_case(desalm_ctx* ctx, const desalm_case& c) {
     return bad("icrs/jcrs/kcrs must be 0 or 1");
   if (c.precision_mode != DESALM_FP64 && c.precision_mode != DESALM_MIXED) return bad("unknown precision_mode");
   if (c.wall_functions != 0 && c.wall_functions != 1) return bad("wall_functions must be 0 or 1");
+  if (c.turbulence < 0 || c.turbulence > 2) return bad("turbulence must be 0 (laminar), 1 (Spalart-Allmaras) or 2 (k-omega)");
   if (c.predictor != DESALM_PRED_QN && c.predictor != DESALM_PRED_LINEAR && c.predictor != DESALM_PRED_LEARNED)
     return bad("unknown predictor");
   if (c.ifix < 1 || c.ifix > c.im || c.jfix < 1 || c.jfix > c.jm || c.kfix < 1 || c.kfix > c.km)
@@ -914,6 +918,7 @@ void drop_graph(desalm_ctx* ctx);
 int autotune_sweeps(desalm_ctx* ctx);
 int run_step(desalm_ctx* ctx, desalm_step_report* rep);
 int sa_des_eddy(desalm_ctx* ctx);
+int kw_eddy_run(desalm_ctx* ctx);
 int sa_conservation(desalm_ctx* ctx);
 
 
@@ -1241,6 +1246,9 @@ int lp_fallback(desalm_ctx* ctx) {
   for (int m = 0; m < 5; ++m)
     LAUNCH(KC_MISC, 0, F.N, launch_k(k_extrapolate<double>, cdiv(F.N, 256), 256, 0, s, lp.tab_h[m],
                                      (const double*)lp.tab_h[5 + m], (const double*)lp.tab_h[10 + m], F.N));
+  if (ctx->c.turbulence == 2)
+    LAUNCH(KC_MISC, 0, F.N, launch_k(k_extrapolate<double>, cdiv(F.N, 256), 256, 0, s, ctx->kw.a[0],
+                                     (const double*)ctx->kw.a[1], (const double*)ctx->kw.a[2], F.N));
   CKL();
   void* nut;
   int esz;
@@ -1368,6 +1376,8 @@ int desalm_init(const desalm_case* c, desalm_ctx** out) {
   if (!rc) rc = A(&ctx->norm, 5);
   if (!rc && c->turbulence)
     for (int t = 0; t < SaWork::NARR && !rc; ++t) rc = A(&ctx->sa.a[t], NF);
+  if (!rc && c->turbulence == 2)
+    for (int t = 0; t < KwWork::NARR && !rc; ++t) rc = A(&ctx->kw.a[t], NF);
   if (rc) { *out = ctx; return rc; }
   if (cudaMallocHost((void**)&ctx->h_norm, 5 * sizeof(double)) != cudaSuccess) {
     ctx->err = "cudaMallocHost failed";
@@ -1642,9 +1652,52 @@ int desalm_bcond_fm(desalm_ctx* ctx) {
 
 int desalm_des_eddy(desalm_ctx* ctx) {
   if (!ctx) return DESALM_EINVAL;
-  if (!ctx->c.turbulence) { ctx->err = "des_eddy needs turbulence = 1"; return DESALM_EINVAL; }
+  if (ctx->c.turbulence != 1) { ctx->err = "des_eddy needs turbulence = 1"; return DESALM_EINVAL; }
   RET(sa_des_eddy(ctx));
   CK(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+int desalm_kw_eddy(desalm_ctx* ctx) {
+  if (!ctx) return DESALM_EINVAL;
+  if (ctx->c.turbulence != 2) { ctx->err = "kw_eddy needs turbulence = 2"; return DESALM_EINVAL; }
+  if (!ctx->have_grid || !ctx->have_state) { ctx->err = "grid or state not set"; return DESALM_ENOTREADY; }
+  RET(kw_eddy_run(ctx));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+int desalm_set_omega(desalm_ctx* ctx, const double* omega, const double* omega_n, const double* omega_nm1) {
+  if (!ctx) return DESALM_EINVAL;
+  if (ctx->c.turbulence != 2) { ctx->err = "omega needs turbulence = 2"; return DESALM_EINVAL; }
+  if (!omega) { ctx->err = "null omega"; return DESALM_EINVAL; }
+  const size_t b = ctx->L[0].N * sizeof(double);
+  const double* src[3] = {omega, omega_n, omega_nm1};
+  for (int t = 0; t < 3; ++t) {
+    if (src[t]) CK(cudaMemcpyAsync(ctx->kw.a[t], src[t], b, cudaMemcpyHostToDevice, ctx->stream));
+    else CK(cudaMemsetAsync(ctx->kw.a[t], 0, b, ctx->stream));
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+int desalm_get_omega(desalm_ctx* ctx, double* omega, double* omega_n, double* omega_nm1) {
+  if (!ctx) return DESALM_EINVAL;
+  if (ctx->c.turbulence != 2) { ctx->err = "omega needs turbulence = 2"; return DESALM_EINVAL; }
+  const size_t b = ctx->L[0].N * sizeof(double);
+  double* dst[3] = {omega, omega_n, omega_nm1};
+  for (int t = 0; t < 3; ++t)
+    if (dst[t]) CK(cudaMemcpyAsync(dst[t], ctx->kw.a[t], b, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+int desalm_kw_config(desalm_ctx* ctx, double ckin, double cein) {
+  if (!ctx) return DESALM_EINVAL;
+  if (!(ckin >= 0.0) || !(cein > 0.0)) { ctx->err = "kw_config: ckin >= 0 and cein > 0"; return DESALM_EINVAL; }
+  ctx->ckin = ckin;
+  ctx->cein = cein;
+  drop_graph(ctx);  // the captured step holds the old floors
   return 0;
 }
 
@@ -1705,6 +1758,14 @@ int desalm_begin_step(desalm_ctx* ctx) {
       LAUNCH(KC_MISC, 0, F.N, launch_k(k_extrapolate<double>, cdiv(F.N, 256), 256, 0, s, (double*)q, (const double*)qn, (const double*)qnm1, F.N));
   }
   CKL();
+  if (c.turbulence == 2) {  // omega: qnm1(2) <- qn(2) <- q(6), then the same guess without the network
+    double* const* w = ctx->kw.a;
+    CK(cudaMemcpyAsync(w[2], w[1], F.N * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(w[1], w[0], F.N * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    if (c.predictor == DESALM_PRED_LINEAR || learned)
+      LAUNCH(KC_MISC, 0, F.N, launch_k(k_extrapolate<double>, cdiv(F.N, 256), 256, 0, s, w[0], (const double*)w[1], (const double*)w[2], F.N));
+    CKL();
+  }
   if (learned) {
     ctx->lp.shifts += 1;
     RET(lp_predict(ctx));
@@ -1825,7 +1886,8 @@ int enqueue_iteration(desalm_ctx* ctx) {
         RET(kind_of(ctx, 0) == K_DD ? alm_run(ctx, G0.dd, ctx->side) : alm_run(ctx, G0.df, ctx->side));
         ctx->alm_pending = true;
       }
-      if (c.turbulence && n == 0) RET(sa_des_eddy(ctx));
+      if (c.turbulence == 1 && n == 0) RET(sa_des_eddy(ctx));
+      if (c.turbulence == 2 && n == 0) RET(kw_eddy_run(ctx));
       // the recalculated residual on the coarsest level feeds nothing
       int rc_eff = (n == ctx->ng - 1) ? 0 : recalc;
       RET(do_daf(ctx, n, rc_eff, itr));
@@ -1941,6 +2003,7 @@ SaT<SW> make_sa(desalm_ctx* ctx, Lv<double, W>& L) {
   for (int b = 0; b < 6; ++b) { S.sa1[b] = ctx->par.sa[0][b]; S.sb1[b] = ctx->par.sb[0][b]; S.btype[b] = ctx->c.btype[b]; }
   S.rat = (const double*)ctx->rat;
   S.ratdim = ctx->ratdim;
+  S.upd = L.q[4];
   return S;
 }
 
@@ -1999,8 +2062,67 @@ int cons_run(desalm_ctx* ctx, Lv<double, W>& L) {
 }
 
 int sa_des_eddy(desalm_ctx* ctx) {
-  if (!ctx->c.turbulence) return 0;
+  if (ctx->c.turbulence != 1) return 0;
   return kind_of(ctx, 0) == K_DD ? sa_run(ctx, ctx->L[0].dd) : sa_run(ctx, ctx->L[0].df);
+}
+
+// k-omega view of the fine level: k's rows and right-hand side in the SA
+// work arrays, omega and the model's FP64 arrays in KwWork.
+template <class W>
+KwT<W> make_kw(desalm_ctx* ctx, Lv<double, W>& L) {
+  KwT<W> K{};
+  K.S = make_sa<W>(ctx, L);
+  double* const* a = ctx->kw.a;
+  K.om = a[0]; K.omn = a[1]; K.omnm1 = a[2];
+  K.As = a[3]; K.Ac = a[4]; K.Bs = a[5]; K.ptke = a[6]; K.dk = a[7]; K.dw = a[8];
+  for (int t = 0; t < 9; ++t) K.cow[t] = (W*)a[9 + t];
+  K.rhw = (W*)a[18];
+  K.ckin = ctx->ckin; K.cein = ctx->cein;
+  const int* bt = ctx->c.btype;
+  K.ista = bt[0] != 1 ? 0 : 1; K.iend = bt[1] != 1 ? L.im - 1 : L.im - 2;
+  K.jsta = bt[2] != 1 ? 0 : 1; K.jend = bt[3] != 1 ? L.jm - 1 : L.jm - 2;
+  K.ksta = bt[4] != 1 ? 0 : 1; K.kend = bt[5] != 1 ? L.km - 1 : L.km - 2;
+  return K;
+}
+
+// kw_eddy (src/kw_eddy.F90:109-289): the model's coefficients and
+// production once, then itk sub-iterations of the fused residual, the line
+// solves of k and of omega (each updating its scalar after its k sweep), the
+// boundary values, nu_t and the wall edges.
+template <class W>
+int kw_run(desalm_ctx* ctx, Lv<double, W>& L) {
+  KwT<W> K = make_kw<W>(ctx, L);
+  SaT<W> Sw = K.S;           // the omega line solves: omega's rows, right-hand side and field
+  for (int t = 0; t < 9; ++t) Sw.co[t] = K.cow[t];
+  Sw.rh = K.rhw;
+  Sw.upd = K.om;
+  cudaStream_t s = ctx->stream;
+  const double nin = double(L.im - 2) * (L.jm - 2) * (L.km - 2);
+  LAUNCH(KC_SA_AUX, 0, L.N, launch_k(k_sa_ucn<W>, cdiv(L.N, 256), 256, 0, s, K.S));
+  LAUNCH(KC_SA_AUX, 0, L.N, launch_k(k_kw_pre<W>, cdiv(L.N, 256), 256, 0, s, K));
+  for (int it = 0; it < ctx->c.itk; ++it) {
+    LAUNCH(KC_SA_RHS, 0, nin, launch_k(k_kw_rhs<W>, grid_r(L.im, L.jm, L.km), blk_r(), 0, s, K));
+    RET((sa_sweep<W, 0>(ctx, K.S, L.jm - 2, L.im - 2, L.km - 2, nin)));
+    RET((sa_sweep<W, 1>(ctx, K.S, L.im - 2, L.jm - 2, L.km - 2, nin)));
+    RET((sa_sweep<W, 2>(ctx, K.S, L.im - 2, L.km - 2, L.jm - 2, nin)));
+    RET((sa_sweep<W, 0>(ctx, Sw, L.jm - 2, L.im - 2, L.km - 2, nin)));
+    RET((sa_sweep<W, 1>(ctx, Sw, L.im - 2, L.jm - 2, L.km - 2, nin)));
+    RET((sa_sweep<W, 2>(ctx, Sw, L.im - 2, L.km - 2, L.jm - 2, nin)));
+    const int nj = K.jend - K.jsta + 1, ni = K.iend - K.ista + 1, nk = K.kend - K.ksta + 1;
+    LAUNCH(KC_SA_BC, 0, 2.0 * nj * nk, launch_k(k_kw_bc<W, 0>, dim3(cdiv(nj, 64), nk), 64, 0, s, K));
+    LAUNCH(KC_SA_BC, 0, 2.0 * ni * nk, launch_k(k_kw_bc<W, 1>, dim3(cdiv(ni, 64), nk), 64, 0, s, K));
+    LAUNCH(KC_SA_BC, 0, 2.0 * ni * nj, launch_k(k_kw_bc<W, 2>, dim3(cdiv(ni, 64), nj), 64, 0, s, K));
+    LAUNCH(KC_SA_BC, 0, L.N, launch_k(k_kw_nut<W>, cdiv(L.N, 256), 256, 0, s, K));
+    LAUNCH(KC_SA_BC, 0, 0.0, launch_k(k_kw_edges<W>, 1, 256, 0, s, K));
+  }
+  CKL();
+  ctx->L[0].dtau_valid = false;  // nu_t changed
+  return 0;
+}
+
+int kw_eddy_run(desalm_ctx* ctx) {
+  if (ctx->c.turbulence != 2) return 0;
+  return kind_of(ctx, 0) == K_DD ? kw_run(ctx, ctx->L[0].dd) : kw_run(ctx, ctx->L[0].df);
 }
 
 int sa_conservation(desalm_ctx* ctx) {

@@ -34,8 +34,9 @@ struct SaT {
   double* nut;
   double* wo;
   SW* rh;
-  SW* co[9];
-  double* uc[3];  // contravariant U/J of each direction on every node, for the current velocities  // co[3 d + 0..2] = aw, ap, ae of the direction-d line through each interior node
+  SW* co[9];        // co[3 d + 0..2] = aw, ap, ae of the direction-d line through each interior node
+  double* uc[3];  // contravariant U/J of each direction on every node, for the current velocities
+  double* upd;    // the scalar the last (k) sweep updates: nu_tilde (q[4]) for SA; k or omega for k-omega
   int* flags;
   double ren, delti, es;
   double sa1[6], sb1[6];  // pressure-row extrapolation coefficients, sa(1,b), sb(1,b)
@@ -437,7 +438,7 @@ __global__ void __launch_bounds__(kSlabThreads) k_sa_sweep4(SaT<SW> S) {
           int lq, p;
           ln[u] = node(t, lq, p);
           so[u] = p * NLP + lq;
-          nt[u] = S.q[4][ln[u]];
+          nt[u] = S.upd[ln[u]];
           dt[u] = __ldg(S.dtev + ln[u]);
         }
       }
@@ -446,7 +447,7 @@ __global__ void __launch_bounds__(kSlabThreads) k_sa_sweep4(SaT<SW> S) {
         if (ln[u] < 0) continue;
         const double qe5 = nt[u] + double(s_rh[so[u]]);
         const double dum = 1.0 + dmul * dt[u] / S.delti;
-        S.q[4][ln[u]] = nt[u] + (-nt[u] + qe5) / dum;
+        S.upd[ln[u]] = nt[u] + (-nt[u] + qe5) / dum;
       }
     }
   }

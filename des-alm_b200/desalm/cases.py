@@ -465,4 +465,54 @@ def turbine(im=385, jm=193, km=193, seed=0, re=1.0e5, itmax=400, delti=0.005, ne
     return c, grid, state, spec, omega
 
 
+def kw_coef_as(k, w, ren):
+    """Wilcox's alpha* = (0.15 + Re_t) / (6 + Re_t), Re_t = Re k / omega
+    (src/rhs_kw_coef.F90:47-49)."""
+    rt = ren * k / w
+    return (0.15 + rt) / (6.0 + rt)
+
+
+def with_kw(case, grid, state, intensity=0.01, nut_ratio=3.0):
+    """The same case with the k-omega model (turbulence = 2): k = 1.5 (I |u|)^2
+    from the state's velocity magnitude (at least 1.5 I^2 x 1e-4 of the
+    free-stream value), omega such that nu_t = As k / omega is nut_ratio
+    times the molecular viscosity, and k = 0 with the wall value of omega
+    60 / (Re 0.075 yd^2) on wall faces, as rhs_kw_bcond sets them.  Returns
+    (case, grid, state, omega) where state's fifth component is k and omega
+    = dict(omega, omega_n, omega_nm1)."""
+    c = case.copy()
+    c.turbulence = 2
+    N = c.im * c.jm * c.km
+    q = state["q"].reshape(N, 5).copy()
+    speed = np.sqrt(q[:, 1] ** 2 + q[:, 2] ** 2 + q[:, 3] ** 2)
+    k = np.maximum(1.5 * (intensity * speed) ** 2, 1.5 * intensity ** 2 * 1e-4)
+    nu = 1.0 / c.ren
+    As = 0.5084   # the fixed point of As(Re_t) with nu_t = 3 nu
+    w = As * k / (nut_ratio * nu)
+    wd = grid.get("wd")
+    kk = k.reshape(c.km, c.jm, c.im)
+    ww = w.reshape(c.km, c.jm, c.im)
+    wdr = None if wd is None else wd.reshape(c.km, c.jm, c.im)
+    srenp = 60.0 / c.ren / 0.075
+    faces = [(slice(None), slice(None), 0, (slice(None), slice(None), 1)),
+             (slice(None), slice(None), -1, (slice(None), slice(None), -2)),
+             (slice(None), 0, slice(None), (slice(None), 1, slice(None))),
+             (slice(None), -1, slice(None), (slice(None), -2, slice(None))),
+             (0, slice(None), slice(None), (1, slice(None), slice(None))),
+             (-1, slice(None), slice(None), (-2, slice(None), slice(None)))]
+    for b, f in enumerate(faces):
+        if c.btype[b] == BC_WALL and wdr is not None:
+            sl = f[:3]
+            kk[sl] = 0.0
+            yd = np.maximum(wdr[f[3]], 1e-12)
+            ww[sl] = srenp / yd / yd
+    k = kk.reshape(-1)
+    w = ww.reshape(-1)
+    q[:, 4] = k
+    nut = kw_coef_as(k, w, c.ren) * k / w
+    st = dict(q=q.reshape(-1).copy(), qn=q.reshape(-1).copy(), qnm1=q.reshape(-1).copy(), nut=nut)
+    om = dict(omega=w.copy(), omega_n=w.copy(), omega_nm1=w.copy())
+    return c, grid, st, om
+
+
 PRESETS = {"cavity": cavity, "channel": channel, "ogrid": ogrid, "wake": wake}

@@ -56,6 +56,10 @@ def lib():
             ("mg_residual", [vp, ip, dp]),
             ("bcond_fm", [vp]),
             ("des_eddy", [vp]),
+            ("kw_eddy", [vp]),
+            ("set_omega", [vp, dp, dp, dp]),
+            ("get_omega", [vp, dp, dp, dp]),
+            ("kw_config", [vp, C.c_double, C.c_double]),
             ("conservation", [vp]),
             ("wall_functions", [vp]),
             ("save_qold", [vp]),
@@ -275,6 +279,22 @@ class Solver:
 
     def des_eddy(self):
         self._ck(self.L.desalm_des_eddy(self.ctx), "des_eddy")
+
+    def kw_eddy(self):
+        self._ck(self.L.desalm_kw_eddy(self.ctx), "kw_eddy")
+
+    def set_omega(self, w, wn=None, wnm1=None):
+        w, wn, wnm1 = map(_f64, (w, wn, wnm1))
+        self._ck(self.L.desalm_set_omega(self.ctx, _p(w), _p(wn), _p(wnm1)), "set_omega")
+
+    def get_omega(self):
+        N = self.case.im * self.case.jm * self.case.km
+        w, wn, wnm1 = np.zeros(N), np.zeros(N), np.zeros(N)
+        self._ck(self.L.desalm_get_omega(self.ctx, _p(w), _p(wn), _p(wnm1)), "get_omega")
+        return dict(omega=w, omega_n=wn, omega_nm1=wnm1)
+
+    def kw_config(self, ckin, cein):
+        self._ck(self.L.desalm_kw_config(self.ctx, float(ckin), float(cein)), "kw_config")
 
     def conservation(self):
         self._ck(self.L.desalm_conservation(self.ctx), "conservation")

@@ -80,7 +80,9 @@ typedef struct desalm_case {
     double pdiss_coef;      /* pressure dissipation coefficient                 */
     int    btype[6], bdir[6];
     int    ifix, jfix, kfix;/* 1-based pressure reference node                  */
-    int    turbulence;      /* 0: laminar (nu_t = 0); 1: Spalart-Allmaras       */
+    int    turbulence;      /* 0: laminar (nu_t = 0); 1: Spalart-Allmaras;
+                               2: Wilcox k-omega (k in q(5), omega through
+                               desalm_set_omega)                              */
     int    unsteady;        /* e_source = 1 (BDF2 physical time terms) or 0     */
     int    conservation;    /* 1: outlet mass-flux fix once per physical step   */
     int    precision_mode;  /* DESALM_FP64 or DESALM_MIXED                      */
@@ -168,6 +170,30 @@ int  desalm_mg_residual(desalm_ctx* ctx, int n, double res[5]);
 int  desalm_bcond_fm(desalm_ctx* ctx);
 /* Spalart-Allmaras sub-iterations on the fine level: src/des_eddy.F90:2-297. */
 int  desalm_des_eddy(desalm_ctx* ctx);
+/* k-omega sub-iterations on the fine level (turbulence = 2): kw_eddy,
+ * src/kw_eddy.F90:2-296, with rhs_kw_ptke, rhs_kw_coef, rhs_kw_prod,
+ * rhs_kw_viscous, rhs_kw_flux, rhs_kw_unst_visc, rhs_kw_implicit_source and
+ * rhs_kw_bcond.  k is q(5); omega is the reference's q(6), set and read
+ * with desalm_set_omega / desalm_get_omega as (i, j, k) arrays of its three
+ * time levels.  desalm_mg_driver and desalm_pseudo_iteration call it where
+ * the reference's driver calls des_eddy.  The reference does not build this
+ * model (kw_eddy.F90 is not in its makefile and its ADI file
+ * rhs_kw_adi_solver_ijk.F90 does not exist): the ADI here follows the SA
+ * model's (src/rhs_sa_adi_solver.F90:50-244) for each of k and omega.
+ * nu_t = As k / omega on every node after each sub-iteration, as
+ * rhs_kw_bcond sets it (src/rhs_kw_bcond.F90:477-491).  A case with wall
+ * faces needs the wall distance given to desalm_set_grid. */
+int  desalm_kw_eddy(desalm_ctx* ctx);
+/* omega (q(6)), its previous time level qn(2) and the one before qnm1(2)
+ * of the fine level, (i, j, k) with i fastest; omega_n / omega_nm1 may be
+ * NULL (zero on set, skipped on get). */
+int  desalm_set_omega(desalm_ctx* ctx, const double* omega, const double* omega_n,
+                      const double* omega_nm1);
+int  desalm_get_omega(desalm_ctx* ctx, double* omega, double* omega_n, double* omega_nm1);
+/* Floors of k and omega on extrapolated, outlet and periodic faces: ckin,
+ * cein of ind3dmg.dat (read at src/init.F90:188, applied in
+ * src/rhs_kw_bcond.F90).  Defaults 1e-10 and 1e-6. */
+int  desalm_kw_config(desalm_ctx* ctx, double ckin, double cein);
 /* Outlet mass-flux correction: src/conservation.F90:2-162. */
 int  desalm_conservation(desalm_ctx* ctx);
 /* Log-law wall functions on the fine level's j walls, wf_eta(1) and

@@ -57,6 +57,10 @@ def lib():
             ("alm_set_angle", [vp, ip, C.c_double]),
             ("alm_get", [vp, ip, dp]),
             ("outlet_rhs", [vp, dp]),
+            ("kw_eddy", [vp]),
+            ("set_omega", [vp, dp, dp, dp]),
+            ("get_omega", [vp, dp, dp, dp]),
+            ("kw_config", [vp, C.c_double, C.c_double]),
         ]:
             f = getattr(L, "desalm_oracle_" + name)
             f.argtypes = args
@@ -161,6 +165,22 @@ class OracleSolver:
 
     def conservation(self):
         self._ck(self.L.desalm_oracle_conservation(self.ctx), "conservation")
+
+    def kw_eddy(self):
+        self._ck(self.L.desalm_oracle_kw_eddy(self.ctx), "kw_eddy")
+
+    def set_omega(self, w, wn=None, wnm1=None):
+        w, wn, wnm1 = map(_f64, (w, wn, wnm1))
+        self._ck(self.L.desalm_oracle_set_omega(self.ctx, _p(w), _p(wn), _p(wnm1)), "set_omega")
+
+    def get_omega(self):
+        N = self.case.im * self.case.jm * self.case.km
+        w, wn, wnm1 = np.zeros(N), np.zeros(N), np.zeros(N)
+        self._ck(self.L.desalm_oracle_get_omega(self.ctx, _p(w), _p(wn), _p(wnm1)), "get_omega")
+        return dict(omega=w, omega_n=wn, omega_nm1=wnm1)
+
+    def kw_config(self, ckin, cein):
+        self._ck(self.L.desalm_oracle_kw_config(self.ctx, float(ckin), float(cein)), "kw_config")
 
     def wall_functions(self):
         self._ck(self.L.desalm_oracle_wall_functions(self.ctx), "wall_functions")

@@ -24,6 +24,10 @@ struct Base {
   virtual int residual(int, double*) = 0;
   virtual int bcond() = 0;
   virtual int des_eddy() = 0;
+  virtual int kw_eddy() = 0;
+  virtual int set_omega(const double*, const double*, const double*) = 0;
+  virtual int get_omega(double*, double*, double*) = 0;
+  virtual int kw_config(double, double) = 0;
   virtual int conservation() = 0;
   virtual int wall_functions() = 0;
   virtual int save_qold() = 0;
@@ -200,6 +204,35 @@ struct Impl : Base {
   }
   int bcond() override { s.bcond_fm(); return 0; }
   int des_eddy() override { s.des_eddy(); return 0; }
+  int kw_eddy() override {
+    if (s.c.turbulence != 2) return DESALM_EINVAL;
+    s.kw_eddy();
+    return 0;
+  }
+  int set_omega(const double* w, const double* wn, const double* wnm1) override {
+    if (s.c.turbulence != 2 || !w) return DESALM_EINVAL;
+    for (long l = 0; l < s.L[0].N; ++l) {
+      s.om[l] = R(w[l]);
+      s.omn[l] = wn ? R(wn[l]) : R(0);
+      s.omnm1[l] = wnm1 ? R(wnm1[l]) : R(0);
+    }
+    return 0;
+  }
+  int get_omega(double* w, double* wn, double* wnm1) override {
+    if (s.c.turbulence != 2) return DESALM_EINVAL;
+    for (long l = 0; l < s.L[0].N; ++l) {
+      if (w) w[l] = double(s.om[l]);
+      if (wn) wn[l] = double(s.omn[l]);
+      if (wnm1) wnm1[l] = double(s.omnm1[l]);
+    }
+    return 0;
+  }
+  int kw_config(double ckin, double cein) override {
+    if (!(ckin >= 0) || !(cein > 0)) return DESALM_EINVAL;
+    s.ckin = R(ckin);
+    s.cein = R(cein);
+    return 0;
+  }
   int conservation() override { s.conservation(); return 0; }
   int wall_functions() override { s.wall_functions(); return 0; }
   int save_qold() override { s.save_qold(); return 0; }
@@ -240,6 +273,7 @@ int check_case(const desalm_case* c, std::string& why) {
   if (!c) { why = "null case"; return DESALM_EINVAL; }
   if (c->ng < 1 || c->ng > 4) { why = "ng must be 1..4"; return DESALM_EINVAL; }
   if (c->im < 5 || c->jm < 5 || c->km < 5) { why = "each extent must be >= 5"; return DESALM_EINVAL; }
+  if (c->turbulence < 0 || c->turbulence > 2) { why = "turbulence must be 0, 1 or 2"; return DESALM_EINVAL; }
   return 0;
 }
 
@@ -290,6 +324,14 @@ int desalm_oracle_mg_prolong(void* ctx, int n) { return ((Base*)ctx)->prolong(n)
 int desalm_oracle_mg_residual(void* ctx, int n, double* r) { return ((Base*)ctx)->residual(n, r); }
 int desalm_oracle_bcond_fm(void* ctx) { return ((Base*)ctx)->bcond(); }
 int desalm_oracle_des_eddy(void* ctx) { return ((Base*)ctx)->des_eddy(); }
+int desalm_oracle_kw_eddy(void* ctx) { return ((Base*)ctx)->kw_eddy(); }
+int desalm_oracle_set_omega(void* ctx, const double* w, const double* wn, const double* wnm1) {
+  return ((Base*)ctx)->set_omega(w, wn, wnm1);
+}
+int desalm_oracle_get_omega(void* ctx, double* w, double* wn, double* wnm1) {
+  return ((Base*)ctx)->get_omega(w, wn, wnm1);
+}
+int desalm_oracle_kw_config(void* ctx, double ckin, double cein) { return ((Base*)ctx)->kw_config(ckin, cein); }
 int desalm_oracle_conservation(void* ctx) { return ((Base*)ctx)->conservation(); }
 int desalm_oracle_wall_functions(void* ctx) { return ((Base*)ctx)->wall_functions(); }
 int desalm_oracle_save_qold(void* ctx) { return ((Base*)ctx)->save_qold(); }

@@ -279,6 +279,7 @@ struct Solver {
         if (m >= 1 && m <= 3) { sa[m][b] = 0; sb[m][b] = 0; }
       }
     }
+    if (c.turbulence == 2) { om.assign(L[0].N, R(0)); omn = om; omnm1 = om; }
     ratdim = std::max(c.im, std::max(c.jm, c.km));
     for (int b = 0; b < 6; ++b) rat[b].assign((long)ratdim * ratdim, R(0));
     for (int m = 0; m < 5; ++m) init_resd[m] = 0;
@@ -1802,6 +1803,321 @@ ORC_PARFOR
     }
   }
 
+  // ---------------------------------------------------------- k-omega model
+  // Wilcox's (1994) low-Reynolds-number k-omega model of kw_eddy
+  // (src/kw_eddy.F90:2-296), on the fine level: k is q(5) (the field SA
+  // uses for nu_tilde) and omega q(6), held here in om / omn / omnm1 (the
+  // reference's q(6), qn(2), qnm1(2)).  The reference builds none of this
+  // (kw_eddy.F90 is not in src/makefile, no routine calls it, and its ADI
+  // file rhs_kw_adi_solver_ijk.F90 does not exist), so this restatement is
+  // parity unpinned.  Its parts:
+  //   rhs_kw_ptke (src/rhs_kw_ptke.F90:42-96, nlinc = .false.), once per call;
+  //   rhs_kw_coef (src/rhs_kw_coef.F90:41-54) on every node;
+  //   per sub-iteration rhs_kw_prod (src/rhs_kw_prod.F90:18-31),
+  //   rhs_kw_viscous (src/rhs_kw_viscous.F90:39-243), rhs_kw_flux
+  //   (src/rhs_kw_flux.F90:20-166), rhs_kw_unst_visc
+  //   (src/rhs_kw_unst_visc.F90:23-37), rhs_kw_implicit_source
+  //   (src/rhs_kw_implicit_source.F90:41-53), the ADI, the update
+  //   (src/kw_eddy.F90:247-266) and rhs_kw_bcond.
+  // The ADI is restated from the SA model's (src/rhs_sa_adi_solver.F90:
+  // 50-244) for each of k and omega: its rows divide by the implicit-source
+  // factor dk (dw for omega) and the i sweep's right-hand side does too, as
+  // there; the face diffusivity is the one rhs_kw_viscous uses,
+  // 1/Re + (nu_t(l1) + nu_t(l0)) / (2 sigma).
+  std::vector<R> om, omn, omnm1;
+  R ckin = R(1.0e-10), cein = R(1.0e-6);
+
+  // rhs_kw_coef (src/rhs_kw_coef.F90:41-54) on every node
+  void kw_coef(std::vector<R>& As, std::vector<R>& Ac, std::vector<R>& Bs) const {
+    const Level<R>& G = L[0];
+    const std::vector<R>& k5 = G.q[4];
+    ORC_PARFOR
+    for (long l = 0; l < G.N; ++l) {
+      R Rt = R(c.ren) * k5[l] / om[l];
+      R Rt4 = Rt * Rt * Rt * Rt;
+      As[l] = (R(0.15) + Rt) / (R(6) + Rt);
+      Ac[l] = ((R(0.27) + Rt) / (R(2.70) + Rt)) * R(0.5555) / As[l];
+      Bs[l] = ((R(1137.77) + Rt4) / (R(4096.00) + Rt4)) * R(0.09);
+    }
+  }
+
+  void kw_eddy() {
+    auto t0 = std::chrono::steady_clock::now();
+    Level<R>& G = L[0];
+    const int im = G.im, jm = G.jm, km = G.km;
+    const R cw2 = R(0.075), sk = R(2), sw = R(2);
+    const R rei = R(1) / R(c.ren);
+    const R one = 1, two = 2, pt5 = R(0.5), pt25 = R(0.25);
+    const R dc = G.dc, de = G.de, dz = G.dz;
+    const R dc2 = pt5 * dc, de2 = pt5 * de, dz2 = pt5 * dz;
+    const R dc4 = pt25 * dc, de4 = pt25 * de, dz4 = pt25 * dz;
+    std::vector<R>& k5 = G.q[4];
+    std::vector<R> qold1(k5), qold2(om), ucn[3], ptke(G.N, R(0)), As(G.N), Ac(G.N), Bs(G.N);
+    std::vector<R> pk1(G.N, R(0)), pk2(G.N, R(0)), v1(G.N, R(0)), v2(G.N, R(0)), r1(G.N, R(0)), r2(G.N, R(0));
+    std::vector<R> f1(G.N, R(0)), f2(G.N, R(0)), dk(G.N, R(1)), dw(G.N, R(1));
+    for (int d = 0; d < 3; ++d) ucn[d].assign(G.N, R(0));
+    auto id = [&](int i, int j, int k) { return G.id(i, j, k); };
+    contra_j(G, ucn);
+    // rhs_kw_ptke, interior
+    ORC_PARFOR
+    for (int k = 2; k <= km - 1; ++k)
+      for (int j = 2; j <= jm - 1; ++j)
+        for (int i = 2; i <= im - 1; ++i) {
+          long l = id(i, j, k);
+          R g[3][3];  // g[var][dir]
+          for (int m = 0; m < 3; ++m) {
+            const std::vector<R>& v = G.q[m + 1];
+            g[m][0] = dc2 * (v[id(i + 1, j, k)] - v[id(i - 1, j, k)]);
+            g[m][1] = de2 * (v[id(i, j + 1, k)] - v[id(i, j - 1, k)]);
+            g[m][2] = dz2 * (v[id(i, j, k + 1)] - v[id(i, j, k - 1)]);
+          }
+          R d[3][3];  // d[var][x]: du_var / dx_x
+          for (int m = 0; m < 3; ++m)
+            for (int x = 0; x < 3; ++x) d[m][x] = g[m][0] * G.csi[x][l] + g[m][1] * G.eta[x][l] + g[m][2] * G.zet[x][l];
+          ptke[l] = G.nut[l] * (two * (d[0][0] * d[0][0] + d[1][1] * d[1][1] + d[2][2] * d[2][2]) +
+                                (d[0][1] + d[1][0]) * (d[0][1] + d[1][0]) +
+                                (d[0][2] + d[2][0]) * (d[0][2] + d[2][0]) +
+                                (d[1][2] + d[2][1]) * (d[1][2] + d[2][1]));
+        }
+    kw_coef(As, Ac, Bs);
+    const long st[3] = {1, (long)im, (long)im * jm};
+    const std::vector<R>* met[3] = {G.csi, G.eta, G.zet};
+    for (int iterk = 1; iterk <= c.itk; ++iterk) {
+      // rhs_kw_prod
+      ORC_PARFOR
+      for (int k = 2; k <= km - 1; ++k)
+        for (int j = 2; j <= jm - 1; ++j)
+          for (int i = 2; i <= im - 1; ++i) {
+            long l = id(i, j, k);
+            R pkw1a = Bs[l] * om[l] * k5[l];
+            pk1[l] = (-ptke[l] + pkw1a) / G.aj[l];
+            R pkw2a = -Ac[l] * om[l] * ptke[l] / k5[l];
+            R pkw2b = cw2 * om[l] * om[l];
+            pk2[l] = (pkw2a + pkw2b) / G.aj[l];
+          }
+      // rhs_kw_viscous: ret(1:2) on every node, then the face loops
+      std::vector<R> ret1(G.N), ret2(G.N);
+      for (long l = 0; l < G.N; ++l) { ret1[l] = rei + G.nut[l] / sk; ret2[l] = rei + G.nut[l] / sw; }
+      for (int dir = 0; dir < 3; ++dir) {
+        ORC_PARFOR
+        for (int k = (dir == 2 ? 1 : 2); k <= km - 1; ++k)
+          for (int j = (dir == 1 ? 1 : 2); j <= jm - 1; ++j)
+            for (int i = (dir == 0 ? 1 : 2); i <= im - 1; ++i) {
+              long l0 = id(i, j, k), l1 = l0 + st[dir];
+              R g1[3], g2[3];  // derivatives of k and omega along csi, eta, zeta on the face
+              for (int s = 0; s < 2; ++s) {
+                const std::vector<R>& v = s == 0 ? k5 : om;
+                R* g = s == 0 ? g1 : g2;
+                if (dir == 0) {
+                  g[0] = dc * (v[l1] - v[l0]);
+                  g[1] = de4 * (v[l1 + st[1]] - v[l1 - st[1]] + v[l0 + st[1]] - v[l0 - st[1]]);
+                  g[2] = dz4 * (v[l1 + st[2]] - v[l1 - st[2]] + v[l0 + st[2]] - v[l0 - st[2]]);
+                } else if (dir == 1) {
+                  g[0] = dc4 * (v[l1 + 1] - v[l1 - 1] + v[l0 + 1] - v[l0 - 1]);
+                  g[1] = de * (v[l1] - v[l0]);
+                  g[2] = dz4 * (v[l1 + st[2]] - v[l1 - st[2]] + v[l0 + st[2]] - v[l0 - st[2]]);
+                } else {
+                  g[0] = dc4 * (v[l1 + 1] - v[l1 - 1] + v[l0 + 1] - v[l0 - 1]);
+                  g[1] = de4 * (v[l1 + st[1]] - v[l1 - st[1]] + v[l0 + st[1]] - v[l0 - st[1]]);
+                  g[2] = dz * (v[l1] - v[l0]);
+                }
+              }
+              R a1 = G.csi[0][l1] + G.csi[0][l0], a2 = G.csi[1][l1] + G.csi[1][l0], a3 = G.csi[2][l1] + G.csi[2][l0];
+              R b1 = G.eta[0][l1] + G.eta[0][l0], b2 = G.eta[1][l1] + G.eta[1][l0], b3 = G.eta[2][l1] + G.eta[2][l0];
+              R c1 = G.zet[0][l1] + G.zet[0][l0], c2 = G.zet[1][l1] + G.zet[1][l0], c3 = G.zet[2][l1] + G.zet[2][l0];
+              R cc1, cc2, cc3;
+              if (dir == 0) { cc1 = a1 * a1 + a2 * a2 + a3 * a3; cc2 = a1 * b1 + a2 * b2 + a3 * b3; cc3 = a1 * c1 + a2 * c2 + a3 * c3; }
+              else if (dir == 1) { cc1 = b1 * a1 + b2 * a2 + b3 * a3; cc2 = b1 * b1 + b2 * b2 + b3 * b3; cc3 = b1 * c1 + b2 * c2 + b3 * c3; }
+              else { cc1 = c1 * a1 + c2 * a2 + c3 * a3; cc2 = c1 * b1 + c2 * b2 + c3 * b3; cc3 = c1 * c1 + c2 * c2 + c3 * c3; }
+              R vtj1 = pt25 * (ret1[l1] + ret1[l0]) / (G.aj[l1] + G.aj[l0]);
+              R vtj2 = pt25 * (ret2[l1] + ret2[l0]) / (G.aj[l1] + G.aj[l0]);
+              f1[l0] = vtj1 * (cc1 * g1[0] + cc2 * g1[1] + cc3 * g1[2]);
+              f2[l0] = vtj2 * (cc1 * g2[0] + cc2 * g2[1] + cc3 * g2[2]);
+            }
+        ORC_PARFOR
+        for (int k = 2; k <= km - 1; ++k)
+          for (int j = 2; j <= jm - 1; ++j)
+            for (int i = 2; i <= im - 1; ++i) {
+              long l = id(i, j, k);
+              if (dir == 0) { v1[l] = f1[l] - f1[l - 1]; v2[l] = f2[l] - f2[l - 1]; }
+              else { v1[l] = v1[l] + f1[l] - f1[l - st[dir]]; v2[l] = v2[l] + f2[l] - f2[l - st[dir]]; }
+            }
+      }
+      // rhs_kw_flux: first-order flux-difference upwinding
+      for (int dir = 0; dir < 3; ++dir) {
+        ORC_PARFOR
+        for (int k = (dir == 2 ? 1 : 2); k <= km - 1; ++k)
+          for (int j = (dir == 1 ? 1 : 2); j <= jm - 1; ++j)
+            for (int i = (dir == 0 ? 1 : 2); i <= im - 1; ++i) {
+              long l0 = id(i, j, k), l1 = l0 + st[dir];
+              R gcu = (met[dir][0][l1] + met[dir][0][l0]) * (G.q[1][l1] + G.q[1][l0]);
+              R gev = (met[dir][1][l1] + met[dir][1][l0]) * (G.q[2][l1] + G.q[2][l0]);
+              R gzw = (met[dir][2][l1] + met[dir][2][l0]) * (G.q[3][l1] + G.q[3][l0]);
+              R eigh = pt5 * std::fabs((gcu + gev + gzw) / (G.aj[l1] + G.aj[l0]));
+              f1[l0] = pt5 * (k5[l1] * ucn[dir][l1] + k5[l0] * ucn[dir][l0] - eigh * (k5[l1] - k5[l0]));
+              f2[l0] = pt5 * (om[l1] * ucn[dir][l1] + om[l0] * ucn[dir][l0] - eigh * (om[l1] - om[l0]));
+            }
+        ORC_PARFOR
+        for (int k = 2; k <= km - 1; ++k)
+          for (int j = 2; j <= jm - 1; ++j)
+            for (int i = 2; i <= im - 1; ++i) {
+              long l = id(i, j, k);
+              if (dir == 0) { r1[l] = f1[l] - f1[l - 1]; r2[l] = f2[l] - f2[l - 1]; }
+              else { r1[l] = r1[l] + f1[l] - f1[l - st[dir]]; r2[l] = r2[l] + f2[l] - f2[l - st[dir]]; }
+            }
+      }
+      // rhs_kw_unst_visc and rhs_kw_implicit_source (interior; the boundary
+      // rows are not read by the line solves)
+      ORC_PARFOR
+      for (int k = 2; k <= km - 1; ++k)
+        for (int j = 2; j <= jm - 1; ++j)
+          for (int i = 2; i <= im - 1; ++i) {
+            long l = id(i, j, k);
+            R dtj = two * R(c.delti) * G.aj[l];
+            R dq5dt = es * (R(3) * k5[l] - R(4) * G.qn[4][l] + G.qnm1[4][l]) / dtj;
+            R dq6dt = es * (R(3) * om[l] - R(4) * omn[l] + omnm1[l]) / dtj;
+            r1[l] = r1[l] + dq5dt - v1[l] + pk1[l];
+            r2[l] = r2[l] + dq6dt - v2[l] + pk2[l];
+            dk[l] = one + Bs[l] * G.dtev[l] * om[l];
+            dw[l] = one + cw2 * G.dtev[l] * om[l];
+            r1[l] = -G.dtev[l] * G.aj[l] * r1[l];
+            r2[l] = -G.dtev[l] * G.aj[l] * r2[l];
+          }
+      // the ADI of each scalar (restated from src/rhs_sa_adi_solver.F90:50-244)
+      const int ext[3] = {im, jm, km};
+      for (int s = 0; s < 2; ++s) {
+        std::vector<R>& rh = s == 0 ? r1 : r2;
+        const std::vector<R>& df = s == 0 ? dk : dw;
+        const R sig = s == 0 ? sk : sw;
+        for (int dir = 0; dir < 3; ++dir) {
+          int len = ext[dir] - 2;
+          int a1 = dir == 0 ? jm : im, a2 = dir == 2 ? jm : km;
+          ORC_PARFOR
+          for (int p2 = 2; p2 <= a2 - 1; ++p2)
+            for (int p1 = 2; p1 <= a1 - 1; ++p1) {
+              std::vector<R> av(len + 1), aw(len), ap(len), ae(len), aq(len);
+              auto node = [&](int t) { return dir == 0 ? id(t, p1, p2) : (dir == 1 ? id(p1, t, p2) : id(p1, p2, t)); };
+              for (int t = 1; t <= ext[dir] - 1; ++t) {  // av(t) on the face t+1/2
+                long l0 = node(t), l1 = node(t + 1);
+                R gx = met[dir][0][l1] + met[dir][0][l0];
+                R gy = met[dir][1][l1] + met[dir][1][l0];
+                R gz = met[dir][2][l1] + met[dir][2][l0];
+                R ev = rei + pt5 * (G.nut[l1] + G.nut[l0]) / sig;
+                R ucna = pt5 * std::fabs(ucn[dir][l1] + ucn[dir][l0]);
+                av[t - 1] = ucna + ev * (gx * gx + gy * gy + gz * gz) / (G.aj[l1] + G.aj[l0]);
+              }
+              for (int t = 2; t <= ext[dir] - 1; ++t) {
+                long l = node(t);
+                R dtj = pt5 * G.dtev[l] * G.aj[l] / df[l];
+                int p = t - 2;
+                aw[p] = -dtj * (ucn[dir][node(t - 1)] + av[t - 2]);
+                ap[p] = one + dtj * (av[t - 2] + av[t - 1]);
+                ae[p] = dtj * (ucn[dir][node(t + 1)] - av[t - 1]);
+                aq[p] = dir == 0 ? rh[l] / df[l] : rh[l];
+              }
+              std::vector<R> dl(aw.begin() + 1, aw.end()), du(ae.begin(), ae.end() - 1);
+              long piv = 0;
+              gtsv(len, 1, dl.data(), ap.data(), du.data(), aq.data(), len, &piv);
+              if (piv) {
+#ifdef _OPENMP
+#pragma omp atomic
+#endif
+                pivots += piv;
+              }
+              for (int t = 2; t <= ext[dir] - 1; ++t) rh[node(t)] = aq[t - 2];
+            }
+        }
+      }
+      // update (src/kw_eddy.F90:247-266)
+      ORC_PARFOR
+      for (int k = 2; k <= km - 1; ++k)
+        for (int j = 2; j <= jm - 1; ++j)
+          for (int i = 2; i <= im - 1; ++i) {
+            long l = id(i, j, k);
+            R qe5 = qold1[l] + r1[l];
+            R qe6 = qold2[l] + r2[l];
+            R dum = one + R(1.5) * es * G.dtev[l] / R(c.delti);
+            k5[l] = k5[l] + (-k5[l] + qe5) / dum;
+            om[l] = om[l] + (-om[l] + qe6) / dum;
+          }
+      kw_bcond(As, Ac, Bs);
+      qold1 = k5;
+      qold2 = om;
+    }
+    phase_s[4] += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+
+  // rhs_kw_bcond (src/rhs_kw_bcond.F90:22-519).  Face loops cover the
+  // face's interior plus the edges toward non-wall faces (ista = i_mysta - 1
+  // where btype(1) /= 1, :44-49); a wall face gets k = 0 and omega =
+  // 60 / (Re 0.075 yd^2) from the adjacent node's wall distance; then As,
+  // Ac, Bs and nu_t = As k / omega on every node (:477-491, nlinc =
+  // .false.); then omega on each edge where two wall faces meet is the mean
+  // of its two face neighbours, edges in the reference's order (:493-519;
+  // its first condition's ".and btype(3)" read as ".and. btype(3)").
+  void kw_bcond(std::vector<R>& As, std::vector<R>& Ac, std::vector<R>& Bs) {
+    Level<R>& G = L[0];
+    const int im = G.im, jm = G.jm, km = G.km;
+    std::vector<R>& k5 = G.q[4];
+    auto K = [&](int i, int j, int k) -> R& { return k5[G.id(i, j, k)]; };
+    auto W = [&](int i, int j, int k) -> R& { return om[G.id(i, j, k)]; };
+    const R srenp = R(60) / R(c.ren) / R(0.075), one = 1, pt5 = R(0.5);
+    const int ista = c.btype[0] != 1 ? 1 : 2, iend = c.btype[1] != 1 ? im : im - 1;
+    const int jsta = c.btype[2] != 1 ? 1 : 2, jend = c.btype[3] != 1 ? jm : jm - 1;
+    const int ksta = c.btype[4] != 1 ? 1 : 2, kend = c.btype[5] != 1 ? km : km - 1;
+    // one boundary node (i, j, k) of face b, its inward neighbours (i1..), (i2..)
+    auto face = [&](int b, int i, int j, int k, int i1, int j1, int k1, int i2, int j2, int k2, int ip, int jp, int kp, R r) {
+      const int bt = c.btype[b];
+      if (bt == 1) {
+        R yd = G.wd[G.id(i1, j1, k1)];
+        W(i, j, k) = srenp / yd / yd;
+        K(i, j, k) = 0;
+      } else if (bt == 2 || bt == 3) {
+        K(i, j, k) = sa[0][b] * K(i1, j1, k1) + sb[0][b] * K(i2, j2, k2);
+        W(i, j, k) = sa[0][b] * W(i1, j1, k1) + sb[0][b] * W(i2, j2, k2);
+        K(i, j, k) = std::max(ckin, K(i, j, k));
+        W(i, j, k) = std::max(cein, W(i, j, k));
+      } else if (bt == 5) {
+        K(i, j, k) = (one + r) * K(i1, j1, k1) - r * K(i2, j2, k2);
+        W(i, j, k) = (one + r) * W(i1, j1, k1) - r * W(i2, j2, k2);
+        K(i, j, k) = std::max(ckin, K(i, j, k));
+        W(i, j, k) = std::max(cein, W(i, j, k));
+      } else if (bt == 6) {
+        K(i, j, k) = K(ip, jp, kp);
+        W(i, j, k) = W(ip, jp, kp);
+        K(i, j, k) = std::max(ckin, K(i, j, k));
+        W(i, j, k) = std::max(cein, W(i, j, k));
+      }
+    };
+    for (int k = ksta; k <= kend; ++k)
+      for (int j = jsta; j <= jend; ++j) face(0, 1, j, k, 2, j, k, 3, j, k, im - 1, j, k, ratv(0, j, k));
+    for (int k = ksta; k <= kend; ++k)
+      for (int j = jsta; j <= jend; ++j) face(1, im, j, k, im - 1, j, k, im - 2, j, k, 2, j, k, ratv(1, j, k));
+    for (int k = ksta; k <= kend; ++k)
+      for (int i = ista; i <= iend; ++i) face(2, i, 1, k, i, 2, k, i, 3, k, i, jm - 1, k, ratv(2, i, k));
+    for (int k = ksta; k <= kend; ++k)
+      for (int i = ista; i <= iend; ++i) face(3, i, jm, k, i, jm - 1, k, i, jm - 2, k, i, 2, k, ratv(3, i, k));
+    for (int j = jsta; j <= jend; ++j)
+      for (int i = ista; i <= iend; ++i) face(4, i, j, 1, i, j, 2, i, j, 3, i, j, km - 1, ratv(4, i, j));
+    for (int j = jsta; j <= jend; ++j)
+      for (int i = ista; i <= iend; ++i) face(5, i, j, km, i, j, km - 1, i, j, km - 2, i, j, 2, ratv(5, i, j));
+    kw_coef(As, Ac, Bs);
+    for (long l = 0; l < G.N; ++l) G.nut[l] = As[l] * k5[l] / om[l];
+    const int* bt = c.btype;
+    if (bt[0] == 1 && bt[2] == 1) for (int k = 1; k <= km; ++k) W(1, 1, k) = pt5 * (W(2, 1, k) + W(1, 2, k));
+    if (bt[0] == 1 && bt[3] == 1) for (int k = 1; k <= km; ++k) W(1, jm, k) = pt5 * (W(2, jm, k) + W(1, jm - 1, k));
+    if (bt[0] == 1 && bt[4] == 1) for (int j = 1; j <= jm; ++j) W(1, j, 1) = pt5 * (W(2, j, 1) + W(1, j, 2));
+    if (bt[0] == 1 && bt[5] == 1) for (int j = 1; j <= jm; ++j) W(1, j, km) = pt5 * (W(2, j, km) + W(1, j, km - 1));
+    if (bt[1] == 1 && bt[2] == 1) for (int k = 1; k <= km; ++k) W(im, 1, k) = pt5 * (W(im - 1, 1, k) + W(im, 2, k));
+    if (bt[1] == 1 && bt[3] == 1) for (int k = 1; k <= km; ++k) W(im, jm, k) = pt5 * (W(im - 1, jm, k) + W(im, jm - 1, k));
+    if (bt[1] == 1 && bt[4] == 1) for (int j = 1; j <= jm; ++j) W(im, j, 1) = pt5 * (W(im - 1, j, 1) + W(im, j, 2));
+    if (bt[1] == 1 && bt[5] == 1) for (int j = 1; j <= jm; ++j) W(im, j, km) = pt5 * (W(im - 1, j, km) + W(im, j, km - 1));
+    if (bt[2] == 1 && bt[4] == 1) for (int i = 1; i <= im; ++i) W(i, 1, 1) = pt5 * (W(i, 2, 1) + W(i, 1, 2));
+    if (bt[2] == 1 && bt[5] == 1) for (int i = 1; i <= im; ++i) W(i, 1, km) = pt5 * (W(i, 2, km) + W(i, 1, km - 1));
+    if (bt[3] == 1 && bt[4] == 1) for (int i = 1; i <= im; ++i) W(i, jm, 1) = pt5 * (W(i, jm - 1, 1) + W(i, jm, 2));
+    if (bt[3] == 1 && bt[5] == 1) for (int i = 1; i <= im; ++i) W(i, jm, km) = pt5 * (W(i, jm - 1, km) + W(i, jm, km - 1));
+  }
+
   // Friction velocity u_tau of the wall law the reference solves
   // (funcv, src/wf_mpi.F90:602-628, ks = 0): with c = Re y,
   //   c u_tau^2 = u0                          when c u_tau <= 11.3,
@@ -1932,9 +2248,13 @@ ORC_PARFOR
   void begin_step() {
     Level<R>& F = L[0];
     for (int m = 0; m < 5; ++m) { F.qnm1[m] = F.qn[m]; F.qn[m] = F.q[m]; }
-    if (c.predictor == DESALM_PRED_LINEAR)
+    if (c.turbulence == 2) { omnm1 = omn; omn = om; }
+    if (c.predictor == DESALM_PRED_LINEAR) {
       for (int m = 0; m < 5; ++m)
         for (long l = 0; l < F.N; ++l) F.q[m][l] = R(2) * F.qn[m][l] - F.qnm1[m][l];
+      if (c.turbulence == 2)
+        for (long l = 0; l < F.N; ++l) om[l] = R(2) * omn[l] - omnm1[l];
+    }
     for (int m = 0; m < 5; ++m) { inject_arr(&Level<R>::qn, m); inject_arr(&Level<R>::qnm1, m); }
     if (c.conservation) conservation();
     itc = 0;
@@ -1949,7 +2269,8 @@ ORC_PARFOR
       if (n > 0) mg_nlevel(n);
       for (int itr = 1; itr <= c.iter[n]; ++itr) {
         if (n != ng - 1) recalc = (itr != c.iter[n]) ? 0 : 1;  // kept at n = ng (Q5)
-        if (c.turbulence && n == 0) des_eddy();
+        if (c.turbulence == 1 && n == 0) des_eddy();
+        if (c.turbulence == 2 && n == 0) kw_eddy();
         solver_daf(n, recalc, itr);
         if (c.wall_functions && n == 0) wall_functions();  // src/mg_driver.F90:221-224
       }
