@@ -1,32 +1,43 @@
 #!/usr/bin/env python
 """Benchmark of the B200 pseudo-time iteration: wall-seconds per physical time
-step (dual time stepping to a 1e-6 drop of the pseudo-time update, capped at
-the case's itmax), one replica per GPU.
+step of dual time stepping, each step run to the convergence test of the
+reference's mg_ck_conver, one replica per GPU.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--case channel|cavity]
-                  [--impl ours|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--case turbine|channel|cavity]
+                  [--model kw|sa] [--impl ours|reference] [--extras]
 
-ours:       value = device-timed seconds per physical step of the product
-            configuration (MIXED precision: FP64 state, residual and update,
-            FP32 line-sweep work; linear-extrapolation initial guess), state
-            resident in HBM.  e2e = the same step through the C ABI with the
-            state copied from pinned host memory and back every step.  The
-            plain FP64 path (q^n guess, as the reference) is timed too, and
-            predictor_ab compares the three initial guesses (q^n, linear
-            extrapolation, the learned network) by iterations and seconds per
-            physical step to an absolute tolerance on the laminar cavity, and
-            alm gives the cost of the actuator-line forcing, outlet that
-            of the characteristics outlet on an open wake box,
-            wall_functions that of the log-law wall functions, and
-            batched_blocks steps eight uneven blocks one after another and
-            together.
-reference:  the CPU oracle (C++ restatement of the reference, FP32 like the
-            reference's own build, its loops on every host thread) on the same
-            case; a bounded sample of pseudo-iterations scaled to one physical
-            step.
+Workload (default): the actuator-line turbine box of 385 x 193 x 193 nodes
+(10 D x 5 D x 5 D, sinh-clustered at the rotor; a 3-blade rotor of D = 1, TSR
+7, Gaussian projection eps = 0.05 D, seeded synthetic polars; uniform inflow,
+characteristics outlet, symmetry side faces), Re_D = 1e5, dt = 0.005 D/U,
+3-level FAS, with the k-omega model (--model kw; --model sa for
+Spalart-Allmaras).  The rotor advances by omega dt between physical steps.
 
-Under torchrun each rank runs an independent replica on its own GPU
-(the path does not shard: no collective in the data path); times are the max
+Convergence test (mg_ck_conver, src/mg_driver.F90:372-398): after it_min = 7
+pseudo-iterations, stop when the largest of the u, v, w updates has dropped
+by 6 decades from the step's first update (er_min = -6, the 1e-6 drop) or is
+below 10^-7.5 in absolute terms (eo_min = -7.5, the reference's own input
+deck, ind3dmg.dat:4); at most 400 pseudo-iterations.  On this method the
+relative drop slows to about 0.15 decades per 100 iterations after the first
+ones (the CPU oracle shows the same rate), so the absolute test is the one
+that ends the steps; the line reports which test ended each step.
+
+ours:       value = device-timed seconds per physical step of the learned,
+            mixed-precision path (FP64 state, residual, restriction, update and
+            norm; FP32 line sweeps, modal transforms and turbulence ADI; the
+            network's initial guess), state resident in HBM, K steps after W
+            warm-up steps.  On the same physical steps: the plain FP64 path
+            (linear extrapolation, the plain guess) and FP64 with the
+            reference's q^n guess, and MIXED with linear extrapolation (what
+            the network adds).  e2e = the learned mixed step through the C ABI
+            with the state copied from pinned host memory and back every step.
+reference:  the CPU oracle (C++ restatement of the reference, FP64, its loops
+            on every host thread), the reference's own method (q^n guess), on
+            the same workload: one whole physical step, run to the same
+            convergence test.
+
+Under torchrun each rank runs an independent replica on its own GPU (the
+path does not shard: no collective in the data path); times are the max
 over ranks.
 """
 import argparse
@@ -45,13 +56,17 @@ from desalm import abi, cases  # noqa: E402
 
 METRIC = "wall-s per physical step to 1e-6 residual drop: learned+mixed vs plain FP64 GPU"
 UNIT = "s/step"
+CRITERION = {"it_min": 7, "er_min": -6.0, "eo_min": -7.5, "itmax": 400}
+SECONDARY_STEPS = 3     # timed steps of each comparison variant (after the same W warm-up steps)
+
 
 # Algorithmic bytes per interior node of each kernel class: every distinct
 # array element the kernel must read or write once, at its stored precision
 # (T = state bytes, W = line-sweep work bytes).  Halo re-reads and the
 # line-solve scratch are not algorithmic.
-def alg_bytes(kind, T, W, coarse):
+def alg_bytes(kind, T, W, coarse, model="sa"):
     pk = 4 * T if coarse else 0
+    turb_rhs = (22 * 8 + 10 * W) if model == "sa" else (27 * 8 + 2 * 8 + 20 * W)
     return {
         "resid": 24 * T + 11 * W + pk,    # q4 qn3 qnm1-3 metrics9 aj 1/aj nut dtau | wk4 sigma tc3 hc3, diss1
         "recalc": 26 * T + pk,            # q4 qn3 qnm1-3 metrics9 aj 1/aj nut diss1 | rh4
@@ -65,27 +80,39 @@ def alg_bytes(kind, T, W, coarse):
         "norm": 15 * T,                   # q5 qold5 | qold5
         "rsmooth": (20 * W + 8 * T) / 3,  # dq4 in/out in W; the k direction reads dq4 and updates q4 (mean of 3)
         "prolong": 4 * W,                 # dq4 out in W (coarse reads amortised)
-        "sa_rhs": 22 * 8 + 10 * W,        # q5 qn5 qnm1-5, U/J 3, metrics9, aj, 1/aj, wd, wo, dtev | rh, ADI rows 9
-        "sa_sweep": 5 * W + 8,            # ADI row 3, rh in/out; k sweep: q5 in/out, dtev (1/3 each)
+        # SA: q5 qn5 qnm1-5, U/J 3, metrics9, aj, 1/aj, wd, wo, dtev | rh, ADI rows 9
+        # k-omega: k w kn km1 wn wm1 u v w U/J3 metrics9 aj nut ptke As Ac Bs dtev | dk dw | rh2 rows18
+        "sa_rhs": turb_rhs,
+        "sa_sweep": 5 * W + 8,            # ADI row 3, rh in/out; k sweep: scalar in/out, dtev (1/3 each)
     }.get(kind)
 
 
-def build_case(name, precision, predictor):
-    if name == "cavity":
+def build_case(name, precision, predictor, model="kw"):
+    """(case, grid, state, omega, alm spec, rotor rate, description)."""
+    omega, spec, rate = None, None, 0.0
+    if name == "turbine":
+        case, grid, state, spec, rate = cases.turbine(itmax=CRITERION["itmax"])
+        desc = ("actuator-line turbine box 385x193x193 (10Dx5Dx5D, sinh-clustered), 3-blade rotor D=1, TSR 7, "
+                "eps=0.05D, seeded polars, inflow/characteristics outlet/symmetry, Re_D=1e5, dt=0.005 D/U, "
+                "3-level FAS, %s" % ("k-omega (Wilcox 1994)" if model == "kw" else "Spalart-Allmaras"))
+        if model == "kw":
+            case, grid, state, omega = cases.with_kw(case, grid, state)
+    elif name == "cavity":
         case, grid, state = cases.cavity(n=65, itmax=200)
-        desc = "laminar lid-driven cavity Re=1000, 65^3 perturbed cube, 3-level FAS, 200 pseudo-iterations/step"
+        desc = "laminar lid-driven cavity Re=1000, 65^3 perturbed cube, 3-level FAS"
     elif name == "channel":
         case, grid, state = cases.channel()
         desc = "SA RANS channel Re_tau=395, 129x97x65 tanh-stretched, periodic i/k, 3-level FAS"
-    elif name == "wake":
-        case, grid, state = cases.wake(im=129, jm=97, km=65, turbulence=1, itmax=200)
-        desc = "SA wake box 129x97x65, uniform inflow, characteristics outlet, 3-level FAS"
     else:
         raise SystemExit("unknown case " + name)
+    case.it_min = CRITERION["it_min"]
+    case.er_min = CRITERION["er_min"]
+    case.eo_min = CRITERION["eo_min"]
+    case.itmax = CRITERION["itmax"]
     case.precision_mode = precision
     case.predictor = predictor
     case.use_graph = 1      # each physical step replays one CUDA graph (device-side while loop)
-    return case, grid, state, desc
+    return case, grid, state, omega, spec, rate, desc
 
 
 class Clocks:
@@ -140,9 +167,80 @@ def over_ranks(x, op, dist, device="cuda"):
     return float(t.item())
 
 
+def which_test(rep):
+    """Which mg_ck_conver test ended a step: 'drop' (er_min), 'absolute'
+    (eo_min), or 'cap' (itmax reached unconverged)."""
+    r = np.array(rep["residual"])
+    r0 = np.array(rep["init_residual"])
+    if not rep["converged"]:
+        return "cap"
+    if (r - r0)[1:4].max() < CRITERION["er_min"]:
+        return "drop"
+    return "absolute"
+
+
+class Workload:
+    """One solver on the bench workload, with the rotor advanced between
+    physical steps (src/main.F90:42-50)."""
+
+    def __init__(self, name, precision, predictor, model):
+        from desalm.solver import Solver
+        (self.case, grid, state, omega, self.spec, self.rate, self.desc) = build_case(name, precision, predictor, model)
+        self.S = Solver(self.case)
+        self.S.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
+        self.S.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
+        if omega is not None:
+            self.S.set_omega(omega["omega"], omega["omega_n"], omega["omega_nm1"])
+        self.angle = None
+        if self.spec is not None:
+            self.S.alm_set(self.spec)
+            self.angle = self.spec["turbines"][0]["angle"]
+        self.nint = (self.case.im - 2) * (self.case.jm - 2) * (self.case.km - 2)
+
+    def step(self):
+        r = self.S.mg_driver()
+        if self.angle is not None:
+            self.angle += self.rate * self.case.delti
+            self.S.alm_set_angle(1, self.angle)
+        return r
+
+    def close(self):
+        self.S.close()
+
+
+def timed(S, K, body, barrier, max_over_ranks):
+    """K calls of body(), bracketed by barrier + synchronize, CUDA events on
+    the library's stream around each; returns (seconds per call over the K
+    calls, max over ranks; the calls' results; per-call seconds)."""
+    import torch
+    stream = torch.cuda.ExternalStream(S.stream())
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(K + 1)]
+    barrier()
+    S.sync()
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    reps = []
+    for k in range(K):
+        reps.append(body())
+        ev[k + 1].record(stream)
+    S.sync()
+    torch.cuda.synchronize()
+    barrier()
+    per = [ev[k].elapsed_time(ev[k + 1]) / 1e3 for k in range(K)]
+    return max_over_ranks(sum(per) / K), reps, per
+
+
+def steps_summary(reps, per):
+    return {"pseudo_iterations_per_step": [r["iterations"] for r in reps],
+            "ended_by": [which_test(r) for r in reps],
+            "drop_reached": [round(float((np.array(r["residual"]) - np.array(r["init_residual"]))[1:4].max()), 3)
+                             for r in reps],
+            "s_per_step_each": [round(p, 4) for p in per],
+            "would_swap_rows": int(sum(r["pivots"] for r in reps))}
+
+
 def run_ours(args, rank, world, dist):
     import torch
-    from desalm.solver import Solver
 
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
@@ -158,19 +256,182 @@ def run_ours(args, rank, world, dist):
     def sum_over_ranks(x):
         return over_ranks(x, "sum", dist)
 
+    K, W = args.steps, max(1, args.warmup)
+    KS = min(K, SECONDARY_STEPS)
+
+    # ---- the learned, mixed-precision path (the headline)
+    wl = Workload(args.case, abi.MIXED, abi.PRED_LEARNED, args.model)
+    S = wl.S
+    for _ in range(W):
+        wl.step()
+    clk = Clocks(dev)
+    clk.start()
+    S.profile(False)  # resets the launch counter
+    sec, reps, per = timed(S, K, wl.step, barrier, max_over_ranks)
+    clocks = clk.stop()
+    _, launches = S.kernel_stats()
+    lp = S.lp_report()
+    head = steps_summary(reps, per)
+
+    # ---- e2e through the C ABI with host buffers (pinned), H2D + D2H per step
+    import ctypes as C
+    case = wl.case
+    N = case.im * case.jm * case.km
+    pin = lambda n: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    hq, hqn, hqnm1, hnut = pin(5 * N), pin(5 * N), pin(5 * N), pin(N)
+    st = S.get_state()
+    hq[:], hqn[:], hqnm1[:], hnut[:] = st["q"], st["qn"], st["qnm1"], st["nut"]
+    kw = case.turbulence == 2
+    hw = [pin(N) for _ in range(3)] if kw else None
+    if kw:
+        om = S.get_omega()
+        hw[0][:], hw[1][:], hw[2][:] = om["omega"], om["omega_n"], om["omega_nm1"]
+    L = S.L
+    P = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+
+    def e2e_step():
+        S._ck(L.desalm_set_state(S.ctx, P(hq), P(hqn), P(hqnm1), P(hnut)), "set_state")
+        if kw:
+            S._ck(L.desalm_set_omega(S.ctx, P(hw[0]), P(hw[1]), P(hw[2])), "set_omega")
+        r = wl.step()
+        S._ck(L.desalm_get_state(S.ctx, P(hq), P(hqn), P(hqnm1), P(hnut)), "get_state")
+        if kw:
+            S._ck(L.desalm_get_omega(S.ctx, P(hw[0]), P(hw[1]), P(hw[2])), "get_omega")
+        return r
+
+    e2e_sec, e2e_reps, e2e_per = timed(S, KS, e2e_step, barrier, max_over_ranks)
+    nbytes = (3 * 5 * N + N + (3 * N if kw else 0)) * 8
+
+    # ---- per-kernel CUDA-event timing of one more step (eager, profiled)
+    S.profile(True)
+    rprof = wl.step()
+    stats, _ = S.kernel_stats()
+    S.profile(False)
+    wl.close()
+
+    T = {1: 8, 2: 8, 3: 8, 4: 8}      # MIXED: FP64 state on every level
+    Wb = {1: 4, 2: 4, 3: 4, 4: 4}     # FP32 line-sweep work
+    best = None
+    for kind_, per_ in stats.items():
+        ms = sum(v[0] for v in per_.values())
+        if best is None or ms > best[1]:
+            best = (kind_, ms, per_)
+    kind, ms_tot, perk = best
+    ms_sum, nlaunch, nodes = perk[1]
+    byts = (alg_bytes(kind, T[1], Wb[1], False, args.model) or 0) * nodes
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = byts / (ms_sum / 1e3) / 1e9 if ms_sum > 0 else 0.0
+    tot_ms = sum(sum(w[0] for w in q.values()) for q in stats.values())
+    share = {k: round(sum(v[0] for v in p.values()) / max(1e-9, tot_ms), 4) for k, p in stats.items()}
+    by_kernel = {}
+    for k, p in stats.items():
+        b1 = alg_bytes(k, T[1], Wb[1], False, args.model)
+        if not b1 or 1 not in p or p[1][0] <= 0:
+            continue
+        ms1, n1, nodes1 = p[1]
+        gbs = b1 * nodes1 / (ms1 / 1e3) / 1e9
+        by_kernel[k] = {"achieved_gbs": round(gbs, 1), "frac": round(gbs / peak, 4),
+                        "avg_launch_us": round(1e3 * ms1 / max(1, n1), 2), "alg_bytes_per_node": b1}
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tfile):
+        traffic = json.load(open(tfile)).get("%s_%s" % (args.case, args.model), {}).get(kind)
+
+    # ---- the comparison paths on the same physical steps (W warm-up, KS timed)
+    variants = {}
+    finals = {}
+    for name, prec, pred in (("fp64_plain", abi.FP64, abi.PRED_LINEAR), ("fp64_qn", abi.FP64, abi.PRED_QN),
+                             ("mixed_linear", abi.MIXED, abi.PRED_LINEAR)):
+        v = Workload(args.case, prec, pred, args.model)
+        _, wreps, wper = timed(v.S, W, v.step, barrier, max_over_ranks)
+        vsec, vreps, vper = timed(v.S, KS, v.step, barrier, max_over_ranks)
+        variants[name] = dict({"value": vsec, "unit": UNIT, "steps": "%d-%d" % (W + 1, W + KS)}, **steps_summary(vreps, vper))
+        variants[name]["step1"] = {"s": wper[0], "pseudo_iterations": wreps[0]["iterations"],
+                                   "ended_by": which_test(wreps[0])}
+        if name in ("fp64_plain", "mixed_linear"):
+            finals[name] = v.S.get_state()["q"]
+        v.close()
+        torch.cuda.empty_cache()
+    variants["fp64_plain"]["guess"] = "linear extrapolation (the plain guess)"
+    variants["fp64_qn"]["guess"] = "q^n (the reference's mg_driver)"
+    variants["mixed_linear"]["guess"] = "linear extrapolation"
+    a = np.asarray(finals["mixed_linear"]).reshape(-1, 5)
+    b = np.asarray(finals["fp64_plain"]).reshape(-1, 5)
+    names = ["p", "u", "v", "w", "k" if kw else "nu_tilde"]
+    field_err = {nm: float(np.linalg.norm(a[:, m] - b[:, m]) / max(1e-300, np.linalg.norm(b[:, m])))
+                 for m, nm in enumerate(names)}
+
+    extra = args.extras and world == 1
+    extras = run_extras(barrier, max_over_ranks) if extra else None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(args.case, args.model, max(1, variants["fp64_qn"]["step1"]["pseudo_iterations"]))
+
+    mean_its = float(np.mean(head["pseudo_iterations_per_step"]))
+    cell_updates = wl.nint * mean_its / sec
+    out = {
+        "metric": METRIC, "value": sec, "unit": UNIT, "n_gpus": world, "steps": K,
+        "warmup": W, "ms_per_step": sec * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
+        "data": "synthetic (seeded numpy generator; the reference ships no grids or solutions)",
+        "impl": "ours",
+        "config": {"workload": wl.desc, "case": args.case, "model": args.model, "grid": [case.im, case.jm, case.km],
+                   "interior_nodes": wl.nint,
+                   "precision": "mixed (FP64 state, residual, restriction, update and norm on every level; FP32 line "
+                                "sweeps, modal transforms and turbulence ADI)",
+                   "predictor": "learned (3D conv network trained online on the GPU; linear extrapolation plus its "
+                                "blended correction)",
+                   "convergence": "mg_ck_conver: after it_min=7, u,v,w update drop below 1e-6 of the step's first "
+                                  "(er_min=-6) or below 10^-7.5 absolute (eo_min=-7.5, the reference deck "
+                                  "ind3dmg.dat:4); itmax 400",
+                   "steps_timed": "%d-%d" % (W + 1, W + K),
+                   "l2": "working set of every level > 126 MB L2; no flush between steps",
+                   "parallelism": "replicas only (%d independent replicas)" % world,
+                   "batching": "one block (the overset blocks of the reference exchange donor data; not built)"},
+        "steps_detail": head,
+        "network": lp,
+        "fp64_plain": variants["fp64_plain"],
+        "fp64_qn": variants["fp64_qn"],
+        "mixed_linear": variants["mixed_linear"],
+        "speedup_vs_fp64_plain": variants["fp64_plain"]["value"] / sec,
+        "mixed_vs_fp64_rel_l2": {"fields": field_err,
+                                 "how": "relative L2 over all nodes after %d physical steps from the same state, "
+                                        "MIXED and FP64 both with linear extrapolation (the FP64 GPU path equals "
+                                        "the FP64 oracle to 1e-10 at this size: tests/test_gpu_fullsize.py)" % (W + KS)},
+        "cell_updates_per_s": sum_over_ranks(cell_updates),
+        "e2e": {"value": e2e_sec, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+                "steps": KS},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": kind, "level": "fine", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "alg_bytes_per_launch": byts / max(1, nlaunch), "launches": nlaunch,
+                     "avg_launch_ms": ms_sum / max(1, nlaunch),
+                     "measured_over": "one eager profiled step (%d pseudo-iterations)" % rprof["iterations"],
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s"},
+        "kernel_time_share": share,
+        "roofline_by_kernel": by_kernel,
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+        "extras": extras,
+    }
+    return out
+
+
+def run_extras(barrier, max_over_ranks):
+    """One-GPU characterisations of the options (--extras): the initial
+    guesses on the laminar cavity, and what the actuator-line forcing, the
+    characteristics outlet, the wall functions and block batching cost."""
+    import torch
+    from desalm.solver import Solver, mg_driver_batch
+
     def predictor_ab(n_steps=24, skip=10):
-        """The three initial guesses on the laminar cavity 65^3 (MIXED, graph
-        path), each physical step run to an absolute tolerance of the
-        pseudo-time update: log10 mean |dq| of u, v, w below -7 (the
-        reference's eo_min test; its relative er_min test is switched off,
-        because it measures the drop from the guess's own first update and so
-        asks more of a better guess).  Steps skip+1 .. n_steps (after the lid's
-        start-up); seconds per step by CUDA events around mg_driver, training
-        of the network included."""
         res = {"workload": "laminar lid-driven cavity Re=1000, 65^3, MIXED, steps %d-%d of dt=0.05, "
                            "tolerance log10 mean|dq(u,v,w)| < -7, itmax 200" % (skip + 1, n_steps)}
         for P, name, mask in ((abi.PRED_QN, "qn", None), (abi.PRED_LINEAR, "linear", None),
-                              (abi.PRED_LEARNED, "learned", None), (abi.PRED_LEARNED, "learned_all_fields", 0x1f)):
+                              (abi.PRED_LEARNED, "learned", None)):
             case, grid, state = cases.cavity(n=65, itmax=200)
             case.precision_mode = abi.MIXED
             case.predictor = P
@@ -180,43 +441,18 @@ def run_ours(args, rank, world, dist):
             S = Solver(case)
             S.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
             S.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
-            if mask is not None:
-                S.lp_fields(mask)
-            stream = torch.cuda.ExternalStream(S.stream())
             its, secs = [], []
             for k in range(n_steps):
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                S.sync()
-                e0.record(stream)
-                r = S.mg_driver()
-                e1.record(stream)
-                S.sync()
-                torch.cuda.synchronize()
+                s, reps, _ = timed(S, 1, S.mg_driver, barrier, max_over_ranks)
                 if k >= skip:
-                    its.append(r["iterations"])
-                    secs.append(e0.elapsed_time(e1) / 1e3)
-            entry = {"iterations_per_step": its, "mean_iterations": float(np.mean(its)),
-                     "s_per_step": float(np.mean(secs))}
-            if P == abi.PRED_LEARNED:
-                entry["network"] = S.lp_report()
-                entry["fields_corrected"] = "p, u, v, w, nu_tilde" if mask == 0x1f else "p, nu_tilde (default)"
-                lin = res["linear"]["iterations_per_step"]
-                d = np.array(its, float) - np.array(lin, float)
-                entry["vs_linear_paired"] = {"mean_iteration_difference": float(d.mean()),
-                                             "standard_error": float(d.std(ddof=1) / np.sqrt(len(d))),
-                                             "steps_with_fewer_iterations": int((d < 0).sum()), "steps": len(d)}
-            res[name] = entry
-            del S
+                    its.append(reps[0]["iterations"])
+                    secs.append(s)
+            res[name] = {"iterations_per_step": its, "mean_iterations": float(np.mean(its)),
+                         "s_per_step": float(np.mean(secs))}
+            S.close()
         return res
 
-    def option_cost(case, grid, state, variants, kernel_class, rounds=3, steps=1):
-        """Seconds per physical step of one case under several options, each
-        variant a (setup(solver), case edit) pair on its own solver.  The
-        variants are timed in turn, rounds times, and each keeps its fastest
-        round, so that a drift of the box between runs does not pose as the
-        option's cost.  One profiled (eager) step of the last variant gives
-        kernel_class's time per pseudo-iteration."""
+    def option_cost(case, grid, state, variants, rounds=3):
         solvers = {}
         for name, (setup, edit) in variants.items():
             c = case.copy()
@@ -230,321 +466,93 @@ def run_ours(args, rank, world, dist):
         best = {}
         for _ in range(rounds):
             for name, S in solvers.items():
-                sec, reps = timed_steps(S, steps, S.mg_driver)
-                its = float(np.mean([r["iterations"] for r in reps]))
+                sec, reps, _ = timed(S, 1, S.mg_driver, barrier, max_over_ranks)
+                its = float(reps[0]["iterations"])
                 if name not in best or sec < best[name]["s_per_step"]:
-                    best[name] = {"s_per_step": sec, "pseudo_iterations_per_step": its,
-                                  "ms_per_iteration": 1e3 * sec / its}
-        S = solvers[list(variants)[-1]]
-        S.profile(True)
-        r = S.mg_driver()
-        stats, _ = S.kernel_stats()
-        S.profile(False)
-        ms = sum(v[0] for v in stats.get(kernel_class, {}).values())
-        best["kernel_ms_per_iteration"] = ms / max(1, r["iterations"])
-        best["method"] = "fastest of %d alternating rounds of %d step(s) per variant" % (rounds, steps)
-        solvers.clear()
+                    best[name] = {"s_per_step": sec, "ms_per_iteration": 1e3 * sec / its}
+        for S in solvers.values():
+            S.close()
+        best["method"] = "fastest of %d alternating rounds of one step per variant" % rounds
         return best
 
-    def alm_cost():
-        """Actuator-line forcing (rhs_lines) on the SA channel 129x97x65 (MIXED,
-        graph path) with three seeded synthetic rotors, with and without the
-        forcing; the forcing kernels' time per pseudo-iteration."""
-        case, grid, state, spec = cases.channel_alm(im=129, jm=97, km=65, n_tur=3, itmax=400)
-        case.precision_mode = abi.MIXED
-        case.predictor = abi.PRED_LINEAR
-        case.use_graph = 1
-        res = option_cost(case, grid, state, {"without": (lambda S: None, lambda c: None),
-                                               "with": (lambda S: S.alm_set(spec), lambda c: None)}, "alm")
-        res["workload"] = ("SA channel 129x97x65, MIXED, 3 synthetic rotors (3 blades x 12 elements, %d kernel nodes)"
-                           % sum(len(T["ker_index"]) for T in spec["turbines"]))
-        return res
+    out = {"predictor_ab": predictor_ab()}
+    case, grid, state, spec = cases.channel_alm(im=129, jm=97, km=65, n_tur=3, itmax=400)
+    case.precision_mode, case.predictor, case.use_graph = abi.MIXED, abi.PRED_LINEAR, 1
+    out["alm"] = option_cost(case, grid, state, {"without": (lambda S: None, lambda c: None),
+                                                 "with": (lambda S: S.alm_set(spec), lambda c: None)})
+    case, grid, state = cases.wake(im=129, jm=97, km=65, turbulence=1, itmax=200)
+    case.precision_mode, case.predictor, case.use_graph = abi.MIXED, abi.PRED_LINEAR, 1
 
-    def outlet_cost():
-        """Characteristics outlet (btype 5) on the SA wake box 129x97x65 (MIXED,
-        graph path), against a first-order extrapolation exit (btype 3) on the
-        same grid and state; the outlet kernel's time per pseudo-iteration."""
-        case, grid, state = cases.wake(im=129, jm=97, km=65, turbulence=1, itmax=200)
-        case.precision_mode = abi.MIXED
-        case.predictor = abi.PRED_LINEAR
-        case.use_graph = 1
+    def exit_as(bt):
+        def edit(c):
+            c.btype[1] = bt
+        return edit
+    out["outlet"] = option_cost(case, grid, state, {"extrapolation_exit": (lambda S: None, exit_as(abi.BC_FREESTREAM)),
+                                                    "outlet": (lambda S: None, exit_as(abi.BC_OUTLET))})
+    shapes = [(33, 33, 33), (49, 49, 33), (49, 49, 33), (65, 49, 49), (97, 65, 65), (97, 65, 65),
+              (129, 65, 65), (161, 97, 65)]
+    built = []
+    for b, (im, jm, km) in enumerate(shapes):
+        c, g, s = cases.wake(im=im, jm=jm, km=km, turbulence=1, seed=b, itmax=100, noise=0.05)
+        c.precision_mode, c.predictor, c.use_graph = abi.MIXED, abi.PRED_LINEAR, 1
+        built.append((c, g, s))
 
-        def exit_as(bt):
-            def edit(c):
-                c.btype[1] = bt
-            return edit
-        res = option_cost(case, grid, state, {"extrapolation_exit": (lambda S: None, exit_as(abi.BC_FREESTREAM)),
-                                              "outlet": (lambda S: None, exit_as(abi.BC_OUTLET))}, "outlet")
-        res["workload"] = "SA wake box 129x97x65, MIXED, uniform inflow, outlet at i = im, itmax 200"
-        return res
-
-    def wallfn_cost():
-        """Wall functions (wf_eta after every fine DAF step) on the SA channel
-        129x97x65 with a first wall spacing of 0.08 (layer 2 in the log law),
-        MIXED, graph path, with and without them; the kernel's time per
-        pseudo-iteration."""
-        case, grid, state = cases.channel(im=129, jm=97, km=65, wall_first=0.08, itmax=200)
-        case.precision_mode = abi.MIXED
-        case.predictor = abi.PRED_LINEAR
-        case.use_graph = 1
-
-        def wf(on):
-            def edit(c):
-                c.wall_functions = on
-            return edit
-        res = option_cost(case, grid, state, {"without": (lambda S: None, wf(0)), "with": (lambda S: None, wf(1))},
-                          "wallfn")
-        res["workload"] = "SA channel 129x97x65, first wall spacing 0.08, MIXED, itmax 200"
-        return res
-
-    def batched_blocks(rounds=3):
-        """Eight independent blocks of uneven sizes (33^3, 2 x 49x49x33,
-        65x49x49, 2 x 97x65x65, 129x65x65, 161x97x65: 2,730,248 nodes), each
-        an open wake box with 5% seeded inflow noise, SA, MIXED, graph path,
-        itmax 100: wall-seconds for one physical step of all blocks, stepped
-        one after another (desalm_mg_driver each) and together
-        (desalm_mg_driver_batch).  Fastest of alternating rounds; each
-        round's blocks start from the same state."""
-        from desalm.solver import mg_driver_batch
-        shapes = [(33, 33, 33), (49, 49, 33), (49, 49, 33), (65, 49, 49), (97, 65, 65), (97, 65, 65),
-                  (129, 65, 65), (161, 97, 65)]
-        built = []
-        for b, (im, jm, km) in enumerate(shapes):
-            case, grid, state = cases.wake(im=im, jm=jm, km=km, turbulence=1, seed=b, itmax=100, noise=0.05)
-            case.precision_mode = abi.MIXED
-            case.predictor = abi.PRED_LINEAR
-            case.use_graph = 1
-            built.append((case, grid, state))
-
-        def fresh():
-            out = []
-            for case, grid, state in built:
-                S = Solver(case)
-                S.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
-                S.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
-                out.append(S)
-            return out
-        seq, bat = fresh(), fresh()
-        for S in seq:          # graph capture and warm-up, outside the timing
+    def fresh():
+        out_ = []
+        for c, g, s in built:
+            S = Solver(c)
+            S.set_grid(g["x"], g["y"], g["z"], g.get("wd"))
+            S.set_state(s["q"], s["qn"], s["qnm1"], s["nut"])
+            out_.append(S)
+        return out_
+    seq, bat = fresh(), fresh()
+    for S in seq:
+        S.mg_driver()
+    mg_driver_batch(bat)
+    bestb = {"one_after_another": None, "batched": None}
+    for _ in range(3):
+        for group in (seq, bat):
+            for S, (_, _, s) in zip(group, built):
+                S.set_state(s["q"], s["qn"], s["qnm1"], s["nut"])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for S in seq:
             S.mg_driver()
+        t1 = time.perf_counter()
         mg_driver_batch(bat)
-        best = {"one_after_another": None, "batched": None}
-        its = None
-        for _ in range(rounds):
-            for group in (seq, bat):
-                for S, (_, _, st) in zip(group, built):
-                    S.set_state(st["q"], st["qn"], st["qnm1"], st["nut"])
-            t0 = time.perf_counter()
-            reps = [S.mg_driver() for S in seq]
-            t1 = time.perf_counter()
-            repb = mg_driver_batch(bat)
-            t2 = time.perf_counter()
-            its = [r["iterations"] for r in repb]
-            assert [r["iterations"] for r in reps] == its
-            for name, t in (("one_after_another", t1 - t0), ("batched", t2 - t1)):
-                if best[name] is None or t < best[name]:
-                    best[name] = t
-        nodes = sum(a * b * c for a, b, c in shapes)
-        return {"workload": "8 wake blocks %s, %d nodes, SA, MIXED, itmax 100" % (shapes, nodes),
-                "s_per_step_one_after_another": best["one_after_another"],
-                "s_per_step_batched": best["batched"],
-                "speedup": best["one_after_another"] / best["batched"],
-                "pseudo_iterations_per_block": its,
-                "timing": "host wall clock around the whole step of all blocks (each call ends synchronised); "
-                          "fastest of %d alternating rounds" % rounds}
-
-    def timed_steps(S, K, body):
-        """K calls of body(), bracketed by barrier + synchronize, CUDA events
-        on the library's stream; returns seconds per call (max over ranks)."""
-        stream = torch.cuda.ExternalStream(S.stream())
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        barrier()
-        S.sync()
-        torch.cuda.synchronize()
-        e0.record(stream)
-        reps = []
-        for _ in range(K):
-            reps.append(body())
-        e1.record(stream)
-        S.sync()
-        torch.cuda.synchronize()
-        barrier()
-        return max_over_ranks(e0.elapsed_time(e1) / 1e3 / K), reps
-
-    # ---- product configuration: MIXED + linear extrapolation
-    case, grid, state, desc = build_case(args.case, abi.MIXED, abi.PRED_LINEAR)
-    nint = (case.im - 2) * (case.jm - 2) * (case.km - 2)
-    S = Solver(case)
-    S.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
-    S.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
-    widths = S.sweep_widths()[:case.ng].tolist()
-    for _ in range(args.warmup):
-        S.mg_driver()
-    clk = Clocks(dev)
-    clk.start()
-    S.profile(False)
-    S.profile(False)  # resets the launch counter
-    sec, reps = timed_steps(S, args.steps, S.mg_driver)
-    clocks = clk.stop()
-    _, launches = S.kernel_stats()
-    iters = [r["iterations"] for r in reps]
-    conv = [r["converged"] for r in reps]
-
-    # ---- e2e through the C ABI with host buffers (pinned), H2D + D2H per step
-    N = case.im * case.jm * case.km
-    pin = lambda n: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
-    hq, hqn, hqnm1, hnut = pin(5 * N), pin(5 * N), pin(5 * N), pin(N)
-    st = S.get_state()
-    hq[:], hqn[:], hqnm1[:], hnut[:] = st["q"], st["qn"], st["qnm1"], st["nut"]
-    import ctypes as C
-    L = S.L
-    P = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
-
-    def e2e_step():
-        S._ck(L.desalm_set_state(S.ctx, P(hq), P(hqn), P(hqnm1), P(hnut)), "set_state")
-        r = S.mg_driver()
-        S._ck(L.desalm_get_state(S.ctx, P(hq), P(hqn), P(hqnm1), P(hnut)), "get_state")
-        return r
-
-    e2e_sec, _ = timed_steps(S, args.steps, e2e_step)
-    h2d = (3 * 5 * N + N) * 8
-    d2h = (3 * 5 * N + N) * 8
-
-    # ---- per-kernel CUDA-event timing over the same workload (roofline)
-    S.profile(True)
-    for _ in range(args.steps):
-        S.mg_driver()
-    stats, _ = S.kernel_stats()
-    S.profile(False)
-    T = {1: 8, 2: 8, 3: 8, 4: 8}      # MIXED: FP64 state on every level
-    W = {1: 4, 2: 4, 3: 4, 4: 4}      # FP32 line-sweep work
-    best = None
-    for kind, per in stats.items():
-        ms = sum(v[0] for v in per.values())
-        if best is None or ms > best[1]:
-            best = (kind, ms, per)
-    kind, ms_tot, per = best
-    # roofline of the dominant class on its fine-level launches (the ones the
-    # ncu traffic figures in profiles/ describe)
-    ms_sum, nlaunch, nodes = per[1]
-    byts = (alg_bytes(kind, T[1], W[1], False) or 0) * nodes
-    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
-    peak = peaks.get("hbm_gbs", 6650.0)
-    achieved = byts / (ms_sum / 1e3) / 1e9 if ms_sum > 0 else 0.0
-    share = {k: round(sum(v[0] for v in p.values()) / max(1e-9, sum(sum(w[0] for w in q.values()) for q in stats.values())), 4)
-             for k, p in stats.items()}
-    # every class with an algorithmic-byte count, on its fine-level launches
-    by_kernel = {}
-    for k, p in stats.items():
-        b1 = alg_bytes(k, T[1], W[1], False)
-        if not b1 or 1 not in p or p[1][0] <= 0:
-            continue
-        ms1, n1, nodes1 = p[1]
-        gbs = b1 * nodes1 / (ms1 / 1e3) / 1e9
-        by_kernel[k] = {"achieved_gbs": round(gbs, 1), "frac": round(gbs / peak, 4),
-                        "avg_launch_us": round(1e3 * ms1 / max(1, n1), 2), "alg_bytes_per_node": b1}
-    traffic = None
-    tfile = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tfile):
-        traffic = json.load(open(tfile)).get(args.case, {}).get(kind)
-    del S
-
-    # ---- plain FP64 GPU path (q^n guess, as the reference's mg_driver)
-    case64, grid, state, _ = build_case(args.case, abi.FP64, abi.PRED_QN)
-    S64 = Solver(case64)
-    S64.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
-    S64.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
-    for _ in range(args.warmup):
-        S64.mg_driver()
-    sec64, reps64 = timed_steps(S64, args.steps, S64.mg_driver)
-    iters64 = [r["iterations"] for r in reps64]
-    st64 = S64.get_state()
-    del S64
-
-    # ---- per-field error of the mixed path against the FP64 path: MIXED with
-    # the same q^n guess, the same number of physical steps from the same state
-    caseq, _, _, _ = build_case(args.case, abi.MIXED, abi.PRED_QN)
-    SQ = Solver(caseq)
-    SQ.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
-    SQ.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
-    for _ in range(args.warmup + args.steps):
-        SQ.mg_driver()
-    stq = SQ.get_state()
-    del SQ
-    a = np.asarray(stq["q"]).reshape(-1, 5)
-    b = np.asarray(st64["q"]).reshape(-1, 5)
-    names = ["p", "u", "v", "w", "nu_tilde"] if case.turbulence else ["p", "u", "v", "w"]
-    field_err = {nm: float(np.linalg.norm(a[:, m] - b[:, m]) / max(1e-300, np.linalg.norm(b[:, m])))
-                 for m, nm in enumerate(names)}
-
-    # one-GPU characterisations (initial guesses, option costs, batching):
-    # run once, not on every replica of a multi-GPU run
-    extra = not args.no_ab and world == 1
-    ab = predictor_ab() if extra else None
-    alm = alm_cost() if extra else None
-    outlet = outlet_cost() if extra else None
-    wallfn = wallfn_cost() if extra else None
-    batched = batched_blocks() if extra else None
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(args.case, max(1, int(np.mean(iters64))))
-
-    cell_updates = nint * float(np.mean(iters)) / sec
-    out = {
-        "metric": METRIC, "value": sec, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
-        "data": "synthetic (seeded numpy generator; the reference ships no grids or solutions)",
-        "impl": "ours",
-        "config": {"workload": desc, "case": args.case, "grid": [case.im, case.jm, case.km],
-                   "interior_nodes": nint, "precision": "mixed (FP64 state, residual, restriction, update and norm on every level; FP32 line-sweep work, modal transforms and SA ADI)",
-                   "predictor": "linear extrapolation",
-                   "learned_predictor": "built (predictor DESALM_PRED_LEARNED); compared in predictor_ab",
-                   "pseudo_iterations_per_step": iters, "converged": conv,
-                   "l2": "working set of every level > 126 MB L2 for the channel; no flush between steps",
-                   "parallelism": "replicas only (%d independent replicas)" % world,
-                   "sweep_lines_per_cta": {"levels_x_ijk": widths,
-                                           "how": "timed per level and direction when the grid is set "
-                                                  "(0 = shared-memory rule, DESALM_AUTOTUNE=0)"}},
-        "fp64_plain": {"value": sec64, "unit": UNIT, "pseudo_iterations_per_step": iters64,
-                       "speedup_mixed_vs_fp64": sec64 / sec},
-        "mixed_vs_fp64_rel_l2": {"fields": field_err,
-                                 "how": "relative L2 over all nodes of the state after %d physical steps from the same "
-                                        "initial state, both with the q^n guess" % (args.warmup + args.steps)},
-        "cell_updates_per_s": sum_over_ranks(cell_updates),
-        "predictor_ab": ab,
-        "alm": alm,
-        "outlet": outlet,
-        "wall_functions": wallfn,
-        "batched_blocks": batched,
-        "e2e": {"value": e2e_sec, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "kernel": kind, "level": "fine", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic,
-                     "alg_bytes_per_launch": byts / max(1, nlaunch), "launches": nlaunch,
-                     "avg_launch_ms": ms_sum / max(1, nlaunch),
-                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s"},
-        "kernel_time_share": share,
-        "roofline_by_kernel": by_kernel,
-        "clocks": clocks,
-        "cpu_baseline": cpu,
-    }
+        t2 = time.perf_counter()
+        for nm, t in (("one_after_another", t1 - t0), ("batched", t2 - t1)):
+            if bestb[nm] is None or t < bestb[nm]:
+                bestb[nm] = t
+    for S in seq + bat:
+        S.close()
+    out["batched_blocks"] = {"workload": "8 wake blocks %s, SA, MIXED, itmax 100" % (shapes,),
+                             "s_per_step_one_after_another": bestb["one_after_another"],
+                             "s_per_step_batched": bestb["batched"],
+                             "speedup": bestb["one_after_another"] / bestb["batched"]}
     return out
 
 
-def cpu_baseline(case_name, iters_per_step, budget_s=20.0):
-    """The CPU oracle in FP32 (the reference's precision) on every host
-    thread its OpenMP loops can use: a bounded sample of pseudo-iterations,
-    scaled to one physical step."""
+def _oracle_solver(case_name, model, real_bytes, predictor):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    case, grid, state, _ = build_case(case_name, abi.FP64, abi.PRED_QN)
-    o = oracle.OracleSolver(case, 4)
+    case, grid, state, omega, spec, rate, desc = build_case(case_name, abi.FP64, predictor, model)
+    o = oracle.OracleSolver(case, real_bytes)
     o.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
     o.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
+    if omega is not None:
+        o.set_omega(omega["omega"], omega["omega_n"], omega["omega_nm1"])
+    if spec is not None:
+        o.alm_set(spec)
+    return o, oracle, desc
+
+
+def cpu_baseline(case_name, model, iters_per_step, budget_s=20.0):
+    """The CPU oracle in FP64 on every host thread its OpenMP loops can use:
+    a bounded sample of pseudo-iterations of physical step 1, scaled by the
+    pseudo-iterations the FP64 GPU path (whose iterates follow the oracle's)
+    needed for that step with the same q^n guess."""
+    o, oracle, _ = _oracle_solver(case_name, model, 8, abi.PRED_QN)
     o.begin_step()
     t0 = time.perf_counter()
     k = 0
@@ -556,54 +564,55 @@ def cpu_baseline(case_name, iters_per_step, budget_s=20.0):
     per_it = (time.perf_counter() - t0) / k
     nth = oracle.threads()
     return {"value": per_it * iters_per_step, "unit": UNIT, "cores": nth, "kind": "port",
-            "sample": "%d pseudo-iterations of the first physical step (%.2f s each, FP32 oracle, %d threads), "
-                      "scaled by the %d pseudo-iterations the FP64 GPU path needed per step"
-                      % (k, per_it, nth, iters_per_step)}
+            "sample": "%d pseudo-iterations of physical step 1 (%.2f s each, FP64 oracle, %d threads), "
+                      "scaled by the %d pseudo-iterations that step needs (FP64 GPU path, q^n guess, measured "
+                      "in this run)" % (k, per_it, nth, iters_per_step)}
 
 
 def run_reference(args):
-    """--impl reference: the oracle (CPU port of the reference) on this case."""
-    iters = {"cavity": 200}.get(args.case)
-    if iters is None:
-        iters = REF_ITERS.get(args.case, 200)
-    vals = []
-    for _ in range(args.warmup + args.steps):
-        cb = cpu_baseline(args.case, iters, budget_s=max(5.0, 60.0 / max(1, args.steps + args.warmup)))
-        vals.append(cb)
-    v = float(np.mean([c["value"] for c in vals[args.warmup:]]))
-    cb = vals[-1]
-    cb["value"] = v
-    _, _, _, desc = build_case(args.case, abi.FP64, abi.PRED_QN)
+    """--impl reference: the oracle (CPU restatement of the reference, FP64,
+    every host thread), the reference's own method (q^n guess), one whole
+    physical step of the workload from the seeded state, run to the same
+    convergence test.  It times what it reports: steps = 1, warmup = 0."""
+    o, oracle, desc = _oracle_solver(args.case, args.model, 8, abi.PRED_QN)
+    t0 = time.perf_counter()
+    rep = o.mg_driver()
+    sec = time.perf_counter() - t0
+    nth = oracle.threads()
+    cb = {"value": sec, "unit": UNIT, "cores": nth, "kind": "port",
+          "sample": "physical step 1 of the workload, whole, %d pseudo-iterations to the convergence test (%s), "
+                    "FP64 oracle, q^n guess, %d threads" % (rep["iterations"], which_test(rep), nth)}
     # n_gpus: the N this arm was launched with, as the arm it is compared
     # with; the work runs on rank 0's host cores
-    return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic", "impl": "reference",
-            "config": {"workload": desc, "case": args.case, "device": "host cores of rank 0 (no GPU)"},
+    return {"metric": METRIC, "value": sec, "unit": UNIT, "n_gpus": args.gpus, "steps": 1, "warmup": 0,
+            "ms_per_step": sec * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": desc, "case": args.case, "model": args.model, "device": "host cores of rank 0 (no GPU)",
+                       "pseudo_iterations": rep["iterations"], "ended_by": which_test(rep),
+                       "requested_steps_warmup": [args.steps, args.warmup]},
             "cpu_baseline": cb,
-            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": sec, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
-# pseudo-iterations per physical step of the FP64 path (q^n guess) on each
-# case, as measured on the GPU path whose iterates follow the oracle's
-# (used only to scale the reference arm's bounded CPU sample)
-REF_ITERS = {"cavity": 200, "channel": 400}
-
-
-def ncu_workload(case_name, precision, learned=False):
+def ncu_workload(case_name, precision, model, learned=False):
     """A short, eager run for Nsight Compute captures: the case's setup, the
     start of a physical step and one pseudo-iteration, without CUDA graphs
     (so every kernel is a separate, capturable launch).  learned: instead,
     four physical steps of two pseudo-iterations with the learned guess, so
     that steps 2-4 train the network and steps 3-4 start from its guess."""
     from desalm.solver import Solver
-    case, grid, state, _ = build_case(case_name, precision, abi.PRED_LEARNED if learned else abi.PRED_LINEAR)
+    case, grid, state, omega, spec, rate, _ = build_case(
+        case_name, precision, abi.PRED_LEARNED if learned else abi.PRED_LINEAR, model)
     case.use_graph = 0
     if learned:
         case.itmax = 2
     S = Solver(case)
     S.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
     S.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
+    if omega is not None:
+        S.set_omega(omega["omega"], omega["omega_n"], omega["omega_nm1"])
+    if spec is not None:
+        S.alm_set(spec)
     if learned:
         for _ in range(4):
             S.mg_driver()
@@ -619,17 +628,18 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--case", default="channel", choices=["cavity", "channel", "wake"])
+    ap.add_argument("--case", default="turbine", choices=["turbine", "cavity", "channel"])
+    ap.add_argument("--model", default="kw", choices=["kw", "sa"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--no-ab", action="store_true", help="skip the initial-guess and forcing sections")
+    ap.add_argument("--extras", action="store_true", help="add the option-cost and initial-guess sections")
     ap.add_argument("--ncu-workload", action="store_true",
                     help="run one eager pseudo-iteration of --case for an ncu capture and exit")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--learned", action="store_true", help="with --ncu-workload: learned-guess steps")
     args = ap.parse_args()
     if args.ncu_workload:
-        ncu_workload(args.case, abi.MIXED if args.precision == "mixed" else abi.FP64, args.learned)
+        ncu_workload(args.case, abi.MIXED if args.precision == "mixed" else abi.FP64, args.model, args.learned)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -138,11 +138,14 @@ struct LpState {
   double* vacc = nullptr;                  // held-out check of the newest sample (k_lp_dot)
   float* alpha = nullptr;                  // blend of each field's correction
   float fixed_alpha = -1.0f;               // < 0: automatic blend
-  // bit f: field f takes the correction.  Default p and nu_tilde: a
-  // correction of the velocities is not discretely divergence-free, and the
-  // artificial compressibility relaxes that error slowly (on the cavity the
-  // velocity corrections cost 8.6 more pseudo-iterations per step)
-  int field_mask = 0x11;
+  // bit f: field f takes the correction.  Default p only: a correction of
+  // the velocities is not discretely divergence-free, and the artificial
+  // compressibility relaxes that error slowly (on the cavity the velocity
+  // corrections cost 8.6 more pseudo-iterations per step); a correction of
+  // the turbulence field (nu_tilde or k) moves nu_t and so the momentum
+  // residual (on the turbine box it raised steps from about 92 to 103-190
+  // pseudo-iterations)
+  int field_mask = 0x01;
   double* qnm2[5] = {};                    // q^{n-2} of the fine level
   double* nut0 = nullptr;                  // nu_t at the start of a step begun from the network's guess
   double** tab = nullptr;                  // device table: q[5] qn[5] qnm1[5] qnm2[5]

@@ -336,8 +336,10 @@ int  desalm_lp_report_get(desalm_ctx* ctx, desalm_lp_report* r);
 int  desalm_lp_blend(desalm_ctx* ctx, float alpha);
 /* Which fields take the network's correction: bit f of mask for field f
  * (p, u, v, w, nu_tilde); the others keep the linear extrapolation.
- * Default 17 (p and nu_tilde): a velocity correction is not discretely
- * divergence-free, and the pseudo-time iteration relaxes that error slowly. */
+ * Default 1 (p only): a velocity correction is not discretely
+ * divergence-free, and the pseudo-time iteration relaxes that error slowly;
+ * a correction of the turbulence field moves nu_t and the momentum residual
+ * with it. */
 int  desalm_lp_fields(desalm_ctx* ctx, int mask);
 /* nparam floats in the flat layout above; set restarts the Adam moments */
 int  desalm_lp_get_params(desalm_ctx* ctx, float* theta);

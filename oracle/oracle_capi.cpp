@@ -5,6 +5,7 @@
 // the real type (8 = FP64 oracle, 4 = FP32 mirror of the reference's own
 // arithmetic).
 #include "oracle_core.hpp"
+#include <malloc.h>
 #include <memory>
 
 namespace {
@@ -286,6 +287,13 @@ int check_case(const desalm_case* c, std::string& why) {
 extern "C" {
 
 int desalm_oracle_init(const desalm_case* c, int real_bytes, void** out) {
+  // The restatement allocates its full-size temporaries per call, as the
+  // reference's routines do.  Keep freed blocks in the heap instead of
+  // returning them to the system, so that the next call reuses pages that
+  // are already mapped (large-grid runs otherwise spend much of their time
+  // in page faults).
+  mallopt(M_MMAP_MAX, 0);
+  mallopt(M_TRIM_THRESHOLD, 0x7fffffff);
   std::string why;
   int rc = check_case(c, why);
   if (rc) return rc;
