@@ -87,11 +87,13 @@ def alg_bytes(kind, T, W, coarse, model="sa"):
     }.get(kind)
 
 
-def build_case(name, precision, predictor, model="kw"):
-    """(case, grid, state, omega, alm spec, rotor rate, description)."""
+def build_case(name, precision, predictor, model="kw", small=False):
+    """(case, grid, state, omega, alm spec, rotor rate, description); small:
+    the turbine box at 193 x 97 x 97 (profiler captures)."""
     omega, spec, rate = None, None, 0.0
     if name == "turbine":
-        case, grid, state, spec, rate = cases.turbine(itmax=CRITERION["itmax"])
+        dims = dict(im=193, jm=97, km=97) if small else {}
+        case, grid, state, spec, rate = cases.turbine(itmax=CRITERION["itmax"], **dims)
         desc = ("actuator-line turbine box 385x193x193 (10Dx5Dx5D, sinh-clustered), 3-blade rotor D=1, TSR 7, "
                 "eps=0.05D, seeded polars, inflow/characteristics outlet/symmetry, Re_D=1e5, dt=0.005 D/U, "
                 "3-level FAS, %s" % ("k-omega (Wilcox 1994)" if model == "kw" else "Spalart-Allmaras"))
@@ -594,7 +596,7 @@ def run_reference(args):
             "e2e": {"value": sec, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
-def ncu_workload(case_name, precision, model, learned=False):
+def ncu_workload(case_name, precision, model, learned=False, small=False):
     """A short, eager run for Nsight Compute captures: the case's setup, the
     start of a physical step and one pseudo-iteration, without CUDA graphs
     (so every kernel is a separate, capturable launch).  learned: instead,
@@ -602,7 +604,7 @@ def ncu_workload(case_name, precision, model, learned=False):
     that steps 2-4 train the network and steps 3-4 start from its guess."""
     from desalm.solver import Solver
     case, grid, state, omega, spec, rate, _ = build_case(
-        case_name, precision, abi.PRED_LEARNED if learned else abi.PRED_LINEAR, model)
+        case_name, precision, abi.PRED_LEARNED if learned else abi.PRED_LINEAR, model, small)
     case.use_graph = 0
     if learned:
         case.itmax = 2
@@ -637,9 +639,11 @@ def main():
                     help="run one eager pseudo-iteration of --case for an ncu capture and exit")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--learned", action="store_true", help="with --ncu-workload: learned-guess steps")
+    ap.add_argument("--small", action="store_true", help="with --ncu-workload: the turbine box at 193x97x97")
     args = ap.parse_args()
     if args.ncu_workload:
-        ncu_workload(args.case, abi.MIXED if args.precision == "mixed" else abi.FP64, args.model, args.learned)
+        ncu_workload(args.case, abi.MIXED if args.precision == "mixed" else abi.FP64, args.model, args.learned,
+                     args.small)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
