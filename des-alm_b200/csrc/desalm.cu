@@ -1574,6 +1574,81 @@ int desalm_get_state(desalm_ctx* ctx, double* q, double* qn, double* qnm1, doubl
   return 0;
 }
 
+// The reference's own arrays are real(rdf) = FP32 (src/precision.F90:11):
+// these variants take them as they are.  The state goes through the device
+// staging array as FP32 (5 N floats fit in its 5 N doubles) and is widened
+// on the device; the grid, read once, is widened on the host.
+int desalm_set_state_f32(desalm_ctx* ctx, const float* q, const float* qn, const float* qnm1, const float* nut) {
+  if (!ctx || !q) return DESALM_EINVAL;
+  cudaStream_t s = ctx->stream;
+  const long N = ctx->L[0].N;
+  float* st = (float*)ctx->stage;
+  const float* srcs[3] = {q, qn, qnm1};
+  for (int a = 0; a < 3; ++a) {
+    double** dst = ctx->ftab + 5 * a;
+    if (!srcs[a]) {
+      for (int m = 0; m < 5; ++m) {
+        void* p;
+        int esz;
+        RET(field_ptr(ctx, 0, DESALM_F_Q + 8 * a + m, &p, &esz));
+        CK(cudaMemsetAsync(p, 0, N * sizeof(double), s));
+      }
+      continue;
+    }
+    CK(cudaMemcpyAsync(st, srcs[a], 5 * N * sizeof(float), cudaMemcpyHostToDevice, s));
+    LAUNCH(KC_MISC, 0, N, launch_k(k_aos_to_soa<double, float>, cdiv(N, 256), 256, 0, s, dst, (const float*)st, 5, N));
+    CKL();
+  }
+  void* dn;
+  int esz;
+  RET(field_ptr(ctx, 0, DESALM_F_NUT, &dn, &esz));
+  if (nut) {
+    CK(cudaMemcpyAsync(st, nut, N * sizeof(float), cudaMemcpyHostToDevice, s));
+    LAUNCH(KC_MISC, 0, N, launch_k(k_copy<double, float>, cdiv(N, 256), 256, 0, s, (double*)dn, (const float*)st, N));
+    CKL();
+  } else {
+    CK(cudaMemsetAsync(dn, 0, N * sizeof(double), s));
+  }
+  CK(cudaStreamSynchronize(s));
+  for (auto& L : ctx->L) L.dtau_valid = false;
+  ctx->have_state = true;
+  ctx->lp.shifts = qnm1 ? 0 : (qn ? -1 : -2);
+  return 0;
+}
+
+int desalm_get_state_f32(desalm_ctx* ctx, float* q, float* qn, float* qnm1, float* nut) {
+  if (!ctx) return DESALM_EINVAL;
+  cudaStream_t s = ctx->stream;
+  const long N = ctx->L[0].N;
+  float* st = (float*)ctx->stage;
+  float* dsts[3] = {q, qn, qnm1};
+  for (int a = 0; a < 3; ++a) {
+    if (!dsts[a]) continue;
+    LAUNCH(KC_MISC, 0, N, launch_k(k_soa_to_aos<double, float>, cdiv(N, 256), 256, 0, s, st, ctx->ftab + 5 * a, 5, N));
+    CKL();
+    CK(cudaMemcpyAsync(dsts[a], st, 5 * N * sizeof(float), cudaMemcpyDeviceToHost, s));
+  }
+  if (nut) {
+    void* dn;
+    int esz;
+    RET(field_ptr(ctx, 0, DESALM_F_NUT, &dn, &esz));
+    LAUNCH(KC_MISC, 0, N, launch_k(k_copy<float, double>, cdiv(N, 256), 256, 0, s, st, (const double*)dn, N));
+    CKL();
+    CK(cudaMemcpyAsync(nut, st, N * sizeof(float), cudaMemcpyDeviceToHost, s));
+  }
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+int desalm_set_grid_f32(desalm_ctx* ctx, const float* x, const float* y, const float* z, const float* wd) {
+  if (!ctx || !x || !y || !z) return DESALM_EINVAL;
+  if (ctx->L.empty()) return DESALM_ENOTREADY;
+  const long N = ctx->L[0].N;
+  std::vector<double> X(x, x + N), Y(y, y + N), Z(z, z + N), D;
+  if (wd) D.assign(wd, wd + N);
+  return desalm_set_grid(ctx, X.data(), Y.data(), Z.data(), wd ? D.data() : nullptr);
+}
+
 int desalm_get_field(desalm_ctx* ctx, int n, int f, double* out) {
   if (!ctx || !out || n < 1 || n > ctx->ng) return DESALM_EINVAL;
   void* p;

@@ -240,19 +240,19 @@ __global__ void k_extrapolate(T* q, const T* qn, const T* qnm1, long n) {
   if (t < n) q[t] = T(2) * qn[t] - qnm1[t];
 }
 // Reference-layout AoS (me, i, j, k) <-> SoA
-template <class T>
-__global__ void k_aos_to_soa(T* const* dst, const double* src, int me, long n) {
+template <class T, class S = double>
+__global__ void k_aos_to_soa(T* const* dst, const S* src, int me, long n) {
   pdl_wait();
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   for (int m = 0; m < me; ++m) dst[m][t] = T(src[t * me + m]);
 }
-template <class T>
-__global__ void k_soa_to_aos(double* dst, T* const* src, int me, long n) {
+template <class T, class D = double>
+__global__ void k_soa_to_aos(D* dst, T* const* src, int me, long n) {
   pdl_wait();
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
-  for (int m = 0; m < me; ++m) dst[t * me + m] = double(src[m][t]);
+  for (int m = 0; m < me; ++m) dst[t * me + m] = D(src[m][t]);
 }
 
 // Injection of one scalar field to the next coarser level (src/mg_inject.F90:26-62)

@@ -37,6 +37,7 @@ def lib():
             raise DesalmError("libdesalm.so is not built (run make -C des-alm_b200/csrc)")
         L = C.CDLL(LIB_PATH)
         vp, ip, dp = C.c_void_p, C.c_int, C.POINTER(C.c_double)
+        fp = C.POINTER(C.c_float)
         L.desalm_init.argtypes = [C.POINTER(Case), C.POINTER(vp)]
         L.desalm_init.restype = C.c_int
         L.desalm_destroy.argtypes = [vp]
@@ -57,6 +58,9 @@ def lib():
             ("bcond_fm", [vp]),
             ("des_eddy", [vp]),
             ("kw_eddy", [vp]),
+            ("set_state_f32", [vp, fp, fp, fp, fp]),
+            ("get_state_f32", [vp, fp, fp, fp, fp]),
+            ("set_grid_f32", [vp, fp, fp, fp, fp]),
             ("set_omega", [vp, dp, dp, dp]),
             ("get_omega", [vp, dp, dp, dp]),
             ("kw_config", [vp, C.c_double, C.c_double]),
@@ -249,6 +253,21 @@ class Solver:
         q, qn, qnm1, nut = (np.zeros(5 * N), np.zeros(5 * N), np.zeros(5 * N), np.zeros(N))
         self._ck(self.L.desalm_get_state(self.ctx, _p(q), _p(qn), _p(qnm1), _p(nut)), "get_state")
         return dict(q=q, qn=qn, qnm1=qnm1, nut=nut)
+
+    def set_state_f32(self, q, qn=None, qnm1=None, nut=None):
+        q, qn, qnm1, nut = map(_f32, (q, qn, qnm1, nut))
+        self._ck(self.L.desalm_set_state_f32(self.ctx, _f32p(q), _f32p(qn), _f32p(qnm1), _f32p(nut)), "set_state_f32")
+
+    def get_state_f32(self):
+        N = self.case.im * self.case.jm * self.case.km
+        q, qn, qnm1, nut = (np.zeros(5 * N, np.float32), np.zeros(5 * N, np.float32), np.zeros(5 * N, np.float32),
+                            np.zeros(N, np.float32))
+        self._ck(self.L.desalm_get_state_f32(self.ctx, _f32p(q), _f32p(qn), _f32p(qnm1), _f32p(nut)), "get_state_f32")
+        return dict(q=q, qn=qn, qnm1=qnm1, nut=nut)
+
+    def set_grid_f32(self, x, y, z, wd=None):
+        x, y, z, wd = map(_f32, (x, y, z, wd))
+        self._ck(self.L.desalm_set_grid_f32(self.ctx, _f32p(x), _f32p(y), _f32p(z), _f32p(wd)), "set_grid_f32")
 
     def get_field(self, n, f):
         im, jm, km = self.dims(n)

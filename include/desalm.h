@@ -150,6 +150,18 @@ int  desalm_set_state(desalm_ctx* ctx, const double* q, const double* qn,
 int  desalm_get_state(desalm_ctx* ctx, double* q, double* qn, double* qnm1,
                       double* nut);
 
+/* The same three calls for FP32 host arrays in the same layouts: the
+ * reference's q, qn, qnm1, xnut, x, y, z and wd are real(rdf) = FP32
+ * (src/precision.F90:11), so a Fortran caller passes them without keeping a
+ * double copy.  Values are widened to FP64 on the way in and rounded to
+ * nearest on the way out. */
+int  desalm_set_state_f32(desalm_ctx* ctx, const float* q, const float* qn,
+                          const float* qnm1, const float* nut);
+int  desalm_get_state_f32(desalm_ctx* ctx, float* q, float* qn, float* qnm1,
+                          float* nut);
+int  desalm_set_grid_f32(desalm_ctx* ctx, const float* x, const float* y,
+                         const float* z, const float* wd);
+
 /* One SoA field of one level (values converted to/from double). */
 int  desalm_get_field(desalm_ctx* ctx, int n, int field, double* out);
 int  desalm_set_field(desalm_ctx* ctx, int n, int field, const double* in);
