@@ -289,6 +289,7 @@ __global__ void __launch_bounds__(kSlabThreads) k_sa_sweep4(SaT<SW> S) {
   constexpr int NT = kSlabThreads, NLP = NL + 1;
   extern __shared__ __align__(16) unsigned char sa_slab[];
   __shared__ SW m_d[NL], m_c[NL], m_b[NL], n_d[NL], n_c[NL], n_b[NL];
+  __shared__ int s_ndom[NL];  // columns of the line's matrix that are not diagonally dominant
   const int tid = threadIdx.x;
   const int a0 = blockIdx.x * NL + 1;
   const int b = blockIdx.y + 1;
@@ -310,6 +311,7 @@ __global__ void __launch_bounds__(kSlabThreads) k_sa_sweep4(SaT<SW> S) {
   };
 
   // ---- phase 0
+  if (tid < NL) s_ndom[tid] = 0;
   for (int t = tid; t < total; t += NT) {
     int li, p;
     const int l = node(t, li, p);
@@ -328,7 +330,12 @@ __global__ void __launch_bounds__(kSlabThreads) k_sa_sweep4(SaT<SW> S) {
   const int h = n / 2;
   auto at = [&](int p) { return p * NLP + li; };
   constexpr int R = 4;  // rows read ahead of the elimination chain
-  int npiv = 0;
+  // column checks, |ap_p| >= |ae_{p-1}| + |aw_{p+1}| (no interchange under
+  // partial pivoting when every column passes): the previous row's ap and the
+  // ae before it (top half), or the next row's ap and the aw after it
+  // (bottom half)
+  int ndom = 0;
+  SW apc = 0, aec2 = 0;
   if (act && half == 0) {
     SW dprev = 0, rdprev = 0, duprev = 0, bprev = 0;
     for (int p0 = 0; p0 < h; p0 += R) {
@@ -343,11 +350,12 @@ __global__ void __launch_bounds__(kSlabThreads) k_sa_sweep4(SaT<SW> S) {
           SW d;
           if (p == 0) { d = bap[u]; bprev = brr[u]; }
           else {
-            npiv += dabs(dprev) < dabs(baw[u]);
+            ndom += dabs(apc) < dabs(aec2) + dabs(baw[u]);
             const SW f = baw[u] * rdprev;
             d = bap[u] - f * duprev;
             bprev = brr[u] - f * bprev;
           }
+          aec2 = duprev; apc = bap[u];
           rdprev = sweep_rcp(d);
           s_ap[at(p)] = rdprev; s_rh[at(p)] = bprev;
           dprev = d; duprev = bae[u];
@@ -369,11 +377,12 @@ __global__ void __launch_bounds__(kSlabThreads) k_sa_sweep4(SaT<SW> S) {
           SW d;
           if (p == n - 1) { d = bap[u]; bprev = brr[u]; }
           else {
-            npiv += dabs(dprev) < dabs(bae[u]);
+            ndom += dabs(apc) < dabs(bae[u]) + dabs(aec2);
             const SW f = bae[u] * rdprev;
             d = bap[u] - f * awprev;
             bprev = brr[u] - f * bprev;
           }
+          aec2 = awprev; apc = bap[u];
           rdprev = sweep_rcp(d);
           s_ap[at(p)] = rdprev; s_rh[at(p)] = bprev;
           dprev = d; awprev = baw[u];
@@ -382,12 +391,16 @@ __global__ void __launch_bounds__(kSlabThreads) k_sa_sweep4(SaT<SW> S) {
     }
     n_d[li] = dprev; n_c[li] = awprev; n_b[li] = bprev;
   }
-  if (npiv) atomicAdd(&S.flags[0], npiv);
   __syncthreads();
   if (act) {
     const SW d1 = m_d[li], u1 = m_c[li], b1 = m_b[li];
     const SW d2 = n_d[li], l2 = n_c[li], b2 = n_b[li];
     const SW det = d1 * d2 - u1 * l2;
+    // the middle columns h - 1 (needs the bottom half's aw_h, l2) and h
+    // (needs the top half's ae_{h-1}, u1)
+    if (half == 0) ndom += dabs(apc) < dabs(aec2) + dabs(l2);
+    else ndom += dabs(apc) < dabs(u1) + dabs(aec2);
+    if (ndom) atomicAdd(&s_ndom[li], ndom);
     if (half == 0) {
       SW x = (b1 * d2 - u1 * b2) / det;
       s_rh[at(h - 1)] = x;
@@ -413,6 +426,61 @@ __global__ void __launch_bounds__(kSlabThreads) k_sa_sweep4(SaT<SW> S) {
           if (p0 + u < n) { x = (brr[u] - baw[u] * x) * brd[u]; s_rh[at(p0 + u)] = x; }
       }
     }
+  }
+  __syncthreads();
+
+  // ---- a line whose matrix has a column that is not dominant: solved again
+  // from its original rows by SGTSV's elimination with partial pivoting
+  // (src/sgtsv.f:107-162, 232-257), one thread per line, in the line's own
+  // columns: ap and the right-hand side are reloaded, aw (dl, with the
+  // fill-in of a swap) and ae (du) are modified in place.  Interchanges are
+  // counted in flags[0], zero pivots in flags[1].
+  if (tid < nl && s_ndom[tid]) {
+    const int lf = tid;
+    auto fat = [&](int p) { return p * NLP + lf; };
+    const int l0 = base + (a0 + lf) * sa + st;   // node of row 0
+    for (int p = 0; p < n; ++p) {
+      s_ap[fat(p)] = S.co[3 * DIR + 1][l0 + p * st];
+      s_rh[fat(p)] = S.rh[l0 + p * st];
+    }
+    int nsw = 0;
+    bool sing = false;
+    for (int i = 0; i <= n - 2 && !sing; ++i) {
+      const SW dli = s_aw[fat(i + 1)];
+      if (dabs(s_ap[fat(i)]) >= dabs(dli)) {
+        if (s_ap[fat(i)] != SW(0)) {
+          const SW fact = dli / s_ap[fat(i)];
+          s_ap[fat(i + 1)] = s_ap[fat(i + 1)] - fact * s_ae[fat(i)];
+          s_rh[fat(i + 1)] = s_rh[fat(i + 1)] - fact * s_rh[fat(i)];
+        } else {
+          sing = true;
+        }
+        s_aw[fat(i + 1)] = SW(0);
+      } else {
+        ++nsw;
+        const SW fact = s_ap[fat(i)] / dli;
+        s_ap[fat(i)] = dli;
+        const SW temp = s_ap[fat(i + 1)];
+        s_ap[fat(i + 1)] = s_ae[fat(i)] - fact * temp;
+        if (i <= n - 3) {
+          s_aw[fat(i + 1)] = s_ae[fat(i + 1)];        // du2(i), the fill-in
+          s_ae[fat(i + 1)] = -fact * s_aw[fat(i + 1)];
+        }
+        s_ae[fat(i)] = temp;
+        const SW tb = s_rh[fat(i)];
+        s_rh[fat(i)] = s_rh[fat(i + 1)];
+        s_rh[fat(i + 1)] = tb - fact * s_rh[fat(i + 1)];
+      }
+    }
+    if (sing || s_ap[fat(n - 1)] == SW(0)) {
+      atomicAdd(&S.flags[1], 1);
+    } else {
+      s_rh[fat(n - 1)] = s_rh[fat(n - 1)] / s_ap[fat(n - 1)];
+      if (n > 1) s_rh[fat(n - 2)] = (s_rh[fat(n - 2)] - s_ae[fat(n - 2)] * s_rh[fat(n - 1)]) / s_ap[fat(n - 2)];
+      for (int i = n - 3; i >= 0; --i)
+        s_rh[fat(i)] = (s_rh[fat(i)] - s_ae[fat(i)] * s_rh[fat(i + 1)] - s_aw[fat(i + 1)] * s_rh[fat(i + 2)]) / s_ap[fat(i)];
+    }
+    if (nsw) atomicAdd(&S.flags[0], nsw);
   }
   __syncthreads();
 

@@ -5,9 +5,11 @@
 // +1, -1).  Row coefficients come from the per-node tc/hc arrays written by
 // K_R; the semi-explicit boundary rows (brh) are applied to the first/last
 // interior rows; the elimination follows LAPACK SGTSV's no-interchange
-// branch (src/sgtsv.f:107-121, 232-243), and a row where SGTSV would swap
-// rows (|d_i| < |dl_i|) is counted in flags[0], a zero pivot (where SGTSV
-// returns INFO > 0, src/sgtsv.f:112-119) or a singular middle 2x2 block in
+// branch (src/sgtsv.f:107-121, 232-243) wherever every column of the line's
+// matrix is diagonally dominant (partial pivoting then interchanges no rows);
+// other line systems are solved again by SGTSV's pivoting elimination, whose
+// interchanges are counted in flags[0].  A zero pivot (where SGTSV returns
+// INFO > 0, src/sgtsv.f:112-119) or a singular middle 2x2 block is counted in
 // flags[1].
 // After the solve each node gets the next modal transform (N1^-1 after the i
 // sweep, N2^-1 after the j sweep) or, after the k sweep, Mc and the update
@@ -62,6 +64,8 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
   __shared__ W sbw[NL][4], sbe[NL][4];
   __shared__ W mt_d[NL][4], mt_u[NL][4], mt_b[NL][4];   // top half's last eliminated row
   __shared__ W mb_d[NL][4], mb_l[NL][4], mb_b[NL][4];   // bottom half's last eliminated row
+  __shared__ int s_ndom[NL][4];   // columns of (line, system) that are not diagonally dominant
+  __shared__ int s_nz[NL][4];     // zero pivots of the two-ended elimination
   const int tid = threadIdx.x;
   const int a0 = blockIdx.x * NL + 1;
   const int b = blockIdx.y + 1;
@@ -125,10 +129,17 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
 #pragma unroll
     for (int q = 0; q < 4; ++q) { sbw[tid][q] = W(bw[q]); sbe[tid][q] = W(be[q]); }
   }
+  if (tid < 4 * NL) { (&s_ndom[0][0])[tid] = 0; (&s_nz[0][0])[tid] = 0; }
   cp_async_wait_all();
   __syncthreads();
 
-  // ---- phase 1: two-ended elimination in shared memory
+  // ---- phase 1: two-ended elimination in shared memory.  Each half also
+  // checks that the columns of its rows are diagonally dominant, |ap_p| >=
+  // |ae_{p-1}| + |aw_{p+1}|: then Gaussian elimination with partial pivoting
+  // interchanges no rows, so SGTSV (src/sgtsv.f:107-135) takes its
+  // no-interchange branch throughout, which is the elimination done here.
+  // A line system with a column that is not dominant is solved again below
+  // with SGTSV's pivoting elimination.
   const int li = tid % NL, combo = tid / NL;
   const int m = combo & 3, half = combo >> 2;
   const bool act = tid < 8 * NL && li < nl;  // solver threads
@@ -145,7 +156,9 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
     else { aw = dw - t; ae = -de - t; }
   };
   const int h = n / 2;  // rows 0..h-1 top (nodes 1..h), h..n-1 bottom (nodes h+1..n)
-  int npiv = 0, nzero = 0;
+  int nzero = 0, ndom = 0;
+  W apc = 0, aec2 = 0;   // ap of the previous row and ae of the row before it (top half), or ap and aw of
+                         // the next rows (bottom half): the column checks
   constexpr int R = 4;  // rows whose shared-memory operands are read ahead of the elimination chain
   // sd holds 1/d of every eliminated row, so that back-substitution multiplies
   if (act && half == 0) {
@@ -168,11 +181,12 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
           W d;
           if (p == 1) { rr = rr - aw * bwm; d = ap; bprev = rr; }
           else {
-            npiv += dabs(dprev) < dabs(aw);
+            ndom += dabs(apc) < dabs(aec2) + dabs(aw);   // column p - 1
             const W f = aw * rdprev;
             d = ap - f * duprev;
             bprev = rr - f * bprev;
           }
+          aec2 = duprev; apc = ap;
           nzero += d == W(0);
           rdprev = sweep_rcp(d);
           sd[at(p)] = rdprev;
@@ -198,6 +212,7 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
       bprev = r[at(n + 1)];
       dprev = d;
       awprev = m == 2 ? -(W(2) * hcur) : W(0);
+      apc = d;
     }
     for (int p0 = n; p0 > h; p0 -= R) {
       W bt[R], bh[R], br[R];
@@ -215,11 +230,12 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
           W d;
           if (p == n && !ext) { rr = rr - ae * bem; d = ap; bprev = rr; }
           else {
-            npiv += dabs(dprev) < dabs(ae);
+            ndom += dabs(apc) < dabs(ae) + dabs(aec2);   // column p + 1
             const W f = ae * rdprev;
             d = ap - f * awprev;
             bprev = rr - f * bprev;
           }
+          aec2 = awprev; apc = ap;
           nzero += d == W(0);
           rdprev = sweep_rcp(d);
           sd[at(p)] = rdprev;
@@ -231,7 +247,6 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
     }
     mb_d[li][m] = dprev; mb_l[li][m] = awprev; mb_b[li][m] = bprev;
   }
-  if (npiv) atomicAdd(&L.flags[0], npiv);
   __syncthreads();
   if (act) {
     // the two middle rows: d1 x1 + u1 x2 = b1 (row h-1), l2 x1 + d2 x2 = b2 (row h)
@@ -239,7 +254,12 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
     const W d2 = mb_d[li][m], l2 = mb_l[li][m], b2 = mb_b[li][m];
     const W det = d1 * d2 - u1 * l2;
     nzero += half == 0 && det == W(0);
-    if (nzero) atomicAdd(&L.flags[1], nzero);
+    // the two middle columns: column h needs the bottom half's aw_{h+1}
+    // (l2), column h+1 the top half's ae_h (u1)
+    if (half == 0) ndom += dabs(apc) < dabs(aec2) + dabs(l2);
+    else ndom += dabs(apc) < dabs(u1) + dabs(aec2);
+    if (ndom) atomicAdd(&s_ndom[li][m], ndom);
+    if (nzero) atomicAdd(&s_nz[li][m], nzero);
     if (half == 0) {
       W x = (b1 * d2 - u1 * b2) / det;
       r[at(h)] = x;
@@ -282,6 +302,92 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
         r[at(n + 1)] = x;
       }
     }
+  }
+  __syncthreads();
+
+  // ---- a line system with a column that is not dominant: solved again from
+  // its original rows by SGTSV's elimination with partial pivoting
+  // (src/sgtsv.f:107-162, back-substitution :232-257), one thread per line,
+  // its systems in turn.  The 1/d columns of the line are free now; three
+  // of them hold d, du and dl (dl keeps the fill-in of a swap, as SGTSV
+  // does).  Rows that interchange are counted in flags[0], zero pivots
+  // (SGTSV's INFO > 0) in flags[1].
+  if (tid < nl) {
+    const int lf = tid;
+    int nsw = 0, nz = 0;
+    for (int q = 0; q < 4; ++q) {
+      if (!s_ndom[lf][q]) { nz += s_nz[lf][q]; continue; }
+      const int N = n + ext;                       // rows 1..N
+      W* bq = s_r + q * fs;
+      W* dd = s_d;                                 // d
+      W* du = s_d + fs;                            // du (and du2 after a swap goes to dl)
+      W* dl = s_d + 2 * fs;                        // dl
+      auto fat = [&](int p) { return p * NLP + lf; };
+      const int l0 = base + (a0 + lf) * sa;
+      for (int p = 1; p <= N; ++p) {
+        W aw, ae, ap;
+        if (p <= n) {
+          const W t = s_tc[fat(p)];
+          const W hw_ = s_hc[fat(p - 1)], he_ = s_hc[fat(p + 1)];
+          const W dw = t != W(0) ? hw_ : W(0), de = t != W(0) ? he_ : W(0);
+          if (q < 2) { aw = -t; ae = -t; }
+          else if (q == 2) { aw = -dw - t; ae = de - t; }
+          else { aw = dw - t; ae = -de - t; }
+          ap = W(1) + W(2) * t;
+        } else {  // the outlet row
+          ap = q == 2 ? W(1) + W(2) * s_hc[fat(n + 1)] : W(1);
+          aw = q == 2 ? -(W(2) * s_hc[fat(n)]) : W(0);
+          ae = W(0);
+        }
+        W b = L.wk[q][l0 + p * st];
+        if (p == 1) b = b - aw * sbw[lf][q];
+        if (p == n && !ext) b = b - ae * sbe[lf][q];
+        bq[fat(p)] = b;
+        dd[fat(p)] = ap;
+        du[fat(p)] = ae;                           // row p's super-diagonal
+        dl[fat(p)] = p > 1 ? aw : W(0);            // dl[p] couples row p to row p - 1
+      }
+      // forward elimination (0-based i of SGTSV = row i + 1 here)
+      bool sing = false;
+      for (int p = 1; p <= N - 1 && !sing; ++p) {
+        const W dlp = dl[fat(p + 1)];
+        if (dabs(dd[fat(p)]) >= dabs(dlp)) {
+          if (dd[fat(p)] != W(0)) {
+            const W fact = dlp / dd[fat(p)];
+            dd[fat(p + 1)] = dd[fat(p + 1)] - fact * du[fat(p)];
+            bq[fat(p + 1)] = bq[fat(p + 1)] - fact * bq[fat(p)];
+          } else {
+            sing = true;
+          }
+          dl[fat(p + 1)] = W(0);
+        } else {
+          ++nsw;
+          const W fact = dd[fat(p)] / dlp;
+          dd[fat(p)] = dlp;
+          const W temp = dd[fat(p + 1)];
+          dd[fat(p + 1)] = du[fat(p)] - fact * temp;
+          if (p <= N - 2) {
+            dl[fat(p + 1)] = du[fat(p + 1)];                 // fill-in of row p: du2
+            du[fat(p + 1)] = -fact * dl[fat(p + 1)];
+          } else {
+            dl[fat(p + 1)] = W(0);
+          }
+          du[fat(p)] = temp;
+          const W tb = bq[fat(p)];
+          bq[fat(p)] = bq[fat(p + 1)];
+          bq[fat(p + 1)] = tb - fact * bq[fat(p + 1)];
+        }
+      }
+      if (sing || dd[fat(N)] == W(0)) { ++nz; continue; }
+      // back-substitution: x_p = (b_p - du_p x_{p+1} - du2_p x_{p+2}) / d_p,
+      // du2_p held in dl[p + 1]
+      bq[fat(N)] = bq[fat(N)] / dd[fat(N)];
+      if (N > 1) bq[fat(N - 1)] = (bq[fat(N - 1)] - du[fat(N - 1)] * bq[fat(N)]) / dd[fat(N - 1)];
+      for (int p = N - 2; p >= 1; --p)
+        bq[fat(p)] = (bq[fat(p)] - du[fat(p)] * bq[fat(p + 1)] - dl[fat(p + 1)] * bq[fat(p + 2)]) / dd[fat(p)];
+    }
+    if (nsw) atomicAdd(&L.flags[0], nsw);
+    if (nz) atomicAdd(&L.flags[1], nz);
   }
   __syncthreads();
 

@@ -100,7 +100,11 @@ typedef struct desalm_step_report {
     int    converged;       /* 1 if the mg_ck_conver test passed                */
     double residual[5];     /* last log10 mean |q - q_old| per field            */
     double init_residual[5];/* first-iteration values (init_resd)               */
-    int    pivots;          /* line-solve rows where partial pivoting would swap */
+    int    pivots;          /* rows interchanged by partial pivoting in the line
+                               solves (SGTSV, src/sgtsv.f:107-135): a line
+                               system with a column that is not diagonally
+                               dominant is solved by the pivoting elimination;
+                               the others need no interchange               */
     int    reserved[7];
 } desalm_step_report;
 
