@@ -2152,7 +2152,7 @@ KwT<W> make_kw(desalm_ctx* ctx, Lv<double, W>& L) {
   K.S = make_sa<W>(ctx, L);
   double* const* a = ctx->kw.a;
   K.om = a[0]; K.omn = a[1]; K.omnm1 = a[2];
-  K.As = a[3]; K.Ac = a[4]; K.Bs = a[5]; K.ptke = a[6]; K.dk = a[7]; K.dw = a[8];
+  K.As = a[3]; K.Ac = a[4]; K.Bs = a[5]; K.ptke = a[6];
   for (int t = 0; t < 9; ++t) K.cow[t] = (W*)a[9 + t];
   K.rhw = (W*)a[18];
   K.ckin = ctx->ckin; K.cein = ctx->cein;

@@ -31,7 +31,7 @@ namespace desalm {
 // slots, used as SW)
 struct KwWork {
   static const int NARR = 19;
-  // om, omn, omnm1, As, Ac, Bs, ptke, dk, dw | co_w[9], rh_w
+  // om, omn, omnm1, As, Ac, Bs, ptke, (two spare) | co_w[9], rh_w
   double* a[NARR];
 };
 
@@ -45,8 +45,6 @@ struct KwT {
   double* Ac;
   double* Bs;
   double* ptke;
-  double* dk;
-  double* dw;
   SW* cow[9];
   SW* rhw;
   double ckin, cein;
@@ -154,10 +152,12 @@ DESALM_DEV void kw_conv_face(const KwT<SW>& K, int dir, int l0, int st, double o
   out[1] = 0.5 * (K.om[l1] * u1 + K.om[l0] * u0 - eigh * (K.om[l1] - K.om[l0]));
 }
 
-// ADI rows of k (s = 0) or omega (s = 1) along DIR at interior node l,
-// divided by the node's implicit-source factor f (dk or dw).
+// ADI rows of k and of omega along DIR at interior node l.  With sigma_k =
+// sigma_w = 2 both scalars have the same face coefficients av (convection
+// plus diffusivity), so they are formed once; the rows differ only in the
+// implicit-source factor that divides them (dk for k, dw for omega).
 template <class SW, int DIR>
-DESALM_DEV void kw_adi_row(const KwT<SW>& K, int l, double f, SW* const* co) {
+DESALM_DEV void kw_adi_rows(const KwT<SW>& K, int l, double fk, double fw) {
   const SaT<SW>& S = K.S;
   const int st = DIR == 0 ? 1 : (DIR == 1 ? S.sj : S.sk);
   const double* const* mt = DIR == 0 ? S.csi : (DIR == 1 ? S.eta : S.zet);
@@ -178,10 +178,15 @@ DESALM_DEV void kw_adi_row(const KwT<SW>& K, int l, double f, SW* const* co) {
     const SW ucna = half_ * dabs(u[g + 1] + u[g]);
     av[g] = ucna + ev * (gx * gx + gy * gy + gz * gz) / (aj[g + 1] + aj[g]);
   }
-  const SW dtj = half_ * SW(S.dtev[l]) * aj[1] / SW(f);
-  co[3 * DIR + 0][l] = -dtj * (u[0] + av[0]);
-  co[3 * DIR + 1][l] = SW(1) + dtj * (av[0] + av[1]);
-  co[3 * DIR + 2][l] = dtj * (u[2] - av[1]);
+  const SW base = half_ * SW(S.dtev[l]) * aj[1];
+  const SW cw = u[0] + av[0], cp = av[0] + av[1], ce = u[2] - av[1];
+  const SW dk = base / SW(fk), dw = base / SW(fw);
+  S.co[3 * DIR + 0][l] = -dk * cw;
+  S.co[3 * DIR + 1][l] = SW(1) + dk * cp;
+  S.co[3 * DIR + 2][l] = dk * ce;
+  K.cow[3 * DIR + 0][l] = -dw * cw;
+  K.cow[3 * DIR + 1][l] = SW(1) + dw * cp;
+  K.cow[3 * DIR + 2][l] = dw * ce;
 }
 
 // One fused pass over the interior of rhs_kw_prod, rhs_kw_viscous,
@@ -230,16 +235,11 @@ __global__ void __launch_bounds__(128) k_kw_rhs(KwT<SW> K) {
   const double dtev = S.dtev[l];
   const double dkv = 1.0 + K.Bs[l] * dtev * wv;
   const double dwv = 1.0 + cw2 * dtev * wv;
-  K.dk[l] = dkv;
-  K.dw[l] = dwv;
   S.rh[l] = SW((-dtev * aj * r1) / dkv);
   K.rhw[l] = SW((-dtev * aj * r2) / dwv);
-  kw_adi_row<SW, 0>(K, l, dkv, S.co);
-  kw_adi_row<SW, 1>(K, l, dkv, S.co);
-  kw_adi_row<SW, 2>(K, l, dkv, S.co);
-  kw_adi_row<SW, 0>(K, l, dwv, K.cow);
-  kw_adi_row<SW, 1>(K, l, dwv, K.cow);
-  kw_adi_row<SW, 2>(K, l, dwv, K.cow);
+  kw_adi_rows<SW, 0>(K, l, dkv, dwv);
+  kw_adi_rows<SW, 1>(K, l, dkv, dwv);
+  kw_adi_rows<SW, 2>(K, l, dkv, dwv);
 }
 
 // rhs_kw_bcond's faces of one direction (src/rhs_kw_bcond.F90:51-475): side
