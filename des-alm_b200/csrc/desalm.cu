@@ -128,9 +128,20 @@ struct LpState {
   bf16 *wf[4] = {}, *wd[4] = {};           // forward / data-gradient weight blocks
   float *dW[4] = {}, *db[4] = {};          // per-layer weight and bias gradients (db inside dW's block)
   float* part = nullptr;                   // per-CTA partial gradients of k_lp_wgrad
-  CUtensorMap tm_x0, tm_a[3], tm_dy4, tm_dya[2];  // TMA maps of the convolutions' inputs
+  CUtensorMap tm_x0, tm_x1, tm_a[3], tm_dy4, tm_dya[2];  // TMA maps of the convolutions' inputs
   int* err = nullptr;                      // set by a tensor-core kernel whose wait timed out
   bf16 *x0 = nullptr, *a[3] = {}, *dy4 = nullptr, *dya[2] = {};  // features, activations, gradients
+  bf16* x1 = nullptr;                      // features of the newest training sample
+  float* yt = nullptr;                     // the training passes' output [5][N] (y keeps the guess's)
+  // Training overlaps the physical step it precedes: its Adam steps run on
+  // their own stream (ls while they are launched, the context's stream
+  // otherwise) beside the pseudo-iterations, which touch none of the
+  // network's buffers; the next use of the network waits for them (lp_join).
+  cudaStream_t ls = nullptr, tstream = nullptr;
+  cudaEvent_t ev_pred = nullptr, ev_train = nullptr;
+  bool pending = false, inflight = false;
+  double* h_loss = nullptr;                // pinned: the losses of the training in flight
+  int h_loss_n = 0;
   float *y = nullptr, *t = nullptr;        // network output, training target [5][N]
   float *rs = nullptr, *rs5 = nullptr, *s5 = nullptr;  // feature scales (1/RMS), target scales, output scales
   double* acc = nullptr;                   // reductions
@@ -970,7 +981,7 @@ int lp_conv(desalm_ctx* ctx, const CUtensorMap& map, const bf16* w, const float*
   const long tiles = (lp.P.p1 - lp.P.p0 + LP_TM - 1) / LP_TM;
   const unsigned grid = (unsigned)std::min<long>(tiles, 148L * 2);
   LAUNCH(KC_LEARN, 0, (double)lp.N, launch_k(k_lp_conv_tc<CIN, COUT>, grid, LP_TC_THREADS, LpTcSmem<CIN, COUT>::total,
-                                             ctx->stream, map, lp.P, w, bias, relu, mask, out, out32, cout32, lp.err));
+                                             lp.ls, map, lp.P, w, bias, relu, mask, out, out32, cout32, lp.err));
   CKL();
   return 0;
 }
@@ -998,8 +1009,8 @@ int lp_wgrad(desalm_ctx* ctx, const CUtensorMap& xmap, const CUtensorMap& dmap, 
   constexpr int grid = 148;
   static_assert(grid <= kLpWgradGrid, "partial slots");
   LAUNCH(KC_LEARN, 0, (double)lp.N, launch_k(k_lp_wgrad_tc<CIN, COUT>, grid, LP_TC_THREADS, LpWgTc<CIN, COUT>::total,
-                                             ctx->stream, xmap, dmap, lp.P, lp.part, lp.err));
-  LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_reduce, cdiv(SLOT, 256), 256, 0, ctx->stream, grid, SLOT,
+                                             lp.ls, xmap, dmap, lp.P, lp.part, lp.err));
+  LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_reduce, cdiv(SLOT, 256), 256, 0, lp.ls, grid, SLOT,
                                     (const float*)lp.part, dW));
   CKL();
   return 0;
@@ -1051,15 +1062,26 @@ int lp_alloc(desalm_ctx* ctx) {
   // channel-last rows of the padded grid; the halo rows stay zero
   const long NP = lp.P.np;
   RET(A((void**)&lp.x0, 16L * NP * sizeof(bf16)));
+  RET(A((void**)&lp.x1, 16L * NP * sizeof(bf16)));
   for (int l = 0; l < 3; ++l) RET(A((void**)&lp.a[l], 32L * NP * sizeof(bf16)));
   RET(A((void**)&lp.dy4, 16L * NP * sizeof(bf16)));
   for (int l = 0; l < 2; ++l) RET(A((void**)&lp.dya[l], 32L * NP * sizeof(bf16)));
   RET(A((void**)&lp.err, sizeof(int)));
   RET(lp_tmap(ctx, &lp.tm_x0, lp.x0, 16, NP));
+  RET(lp_tmap(ctx, &lp.tm_x1, lp.x1, 16, NP));
+  CK(cudaStreamCreateWithFlags(&lp.tstream, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&lp.ev_pred, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&lp.ev_train, cudaEventDisableTiming));
+  if (cudaMallocHost((void**)&lp.h_loss, 256 * sizeof(double)) != cudaSuccess) {
+    ctx->err = "cudaMallocHost failed";
+    return DESALM_ENOMEM;
+  }
+  lp.ls = ctx->stream;
   for (int l = 0; l < 3; ++l) RET(lp_tmap(ctx, &lp.tm_a[l], lp.a[l], 32, NP));
   RET(lp_tmap(ctx, &lp.tm_dy4, lp.dy4, 16, NP));
   for (int l = 0; l < 2; ++l) RET(lp_tmap(ctx, &lp.tm_dya[l], lp.dya[l], 32, NP));
   RET(A((void**)&lp.y, 5L * N * sizeof(float))); RET(A((void**)&lp.t, 5L * N * sizeof(float)));
+  RET(A((void**)&lp.yt, 5L * N * sizeof(float)));
   RET(A((void**)&lp.rs, 16 * sizeof(float))); RET(A((void**)&lp.rs5, 8 * sizeof(float)));
   RET(A((void**)&lp.s5, 8 * sizeof(float))); RET(A((void**)&lp.acc, 16 * sizeof(double)));
   RET(A((void**)&lp.red, kLpRedBlocks * 16 * sizeof(double)));
@@ -1097,32 +1119,35 @@ int lp_pack(desalm_ctx* ctx) {
   LpState& lp = ctx->lp;
   for (int l = 0; l < 4; ++l) {
     const long total = 27L * lp.ly[l].cin_pad * lp.ly[l].cout_pad;
-    LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_pack_tc, cdiv(total, 256), 256, 0, ctx->stream, lp.ly[l], (const float*)lp.theta, lp.wf[l], lp.wd[l]));
+    LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_pack_tc, cdiv(total, 256), 256, 0, lp.ls, lp.ly[l], (const float*)lp.theta, lp.wf[l], lp.wd[l]));
   }
   CKL();
   return 0;
 }
 
-// Forward pass on lp.x0: activations a[0..2], output y (FP32).
-int lp_forward(desalm_ctx* ctx) {
+// Forward pass on the features xin describes (lp.x0 or lp.x1): activations
+// a[0..2], output yout (FP32: lp.y, or lp.yt for training).
+int lp_forward(desalm_ctx* ctx, const CUtensorMap& xin, float* yout) {
   LpState& lp = ctx->lp;
   const float* b[4];
   for (int l = 0; l < 4; ++l) b[l] = lp.theta + lp.ly[l].boff;
   // the bias pointers index the flat vector: each layer's bias is contiguous there
-  RET((lp_conv<16, 32>(ctx, lp.tm_x0, lp.wf[0], b[0], 1, nullptr, lp.a[0], nullptr, 0)));
+  RET((lp_conv<16, 32>(ctx, xin, lp.wf[0], b[0], 1, nullptr, lp.a[0], nullptr, 0)));
   RET((lp_conv<32, 32>(ctx, lp.tm_a[0], lp.wf[1], b[1], 1, nullptr, lp.a[1], nullptr, 0)));
   RET((lp_conv<32, 32>(ctx, lp.tm_a[1], lp.wf[2], b[2], 1, nullptr, lp.a[2], nullptr, 0)));
-  RET((lp_conv<32, 16>(ctx, lp.tm_a[2], lp.wf[3], b[3], 0, nullptr, nullptr, lp.y, 5)));
+  RET((lp_conv<32, 16>(ctx, lp.tm_a[2], lp.wf[3], b[3], 0, nullptr, nullptr, yout, 5)));
   return 0;
 }
 
-// Loss against lp.t and the gradient of the mean squared error in lp.grad;
-// the loss goes to *loss (host, after a synchronize).
-int lp_backward(desalm_ctx* ctx, double* loss) {
+// Loss against lp.t and the gradient of the mean squared error in lp.grad
+// for the features xin describes.  On the context's stream the loss goes to
+// *loss (host, after a synchronize); on the training stream its sum goes to
+// the pinned slot *hsum without waiting (read by lp_join).
+int lp_backward(desalm_ctx* ctx, const CUtensorMap& xin, const float* yin, double* loss, double* hsum = nullptr) {
   LpState& lp = ctx->lp;
-  cudaStream_t s = ctx->stream;
+  cudaStream_t s = lp.ls;
   const long N = lp.N;
-  LAUNCH(KC_LEARN, 0, (double)N, launch_k(k_lp_loss, kLpRedBlocks, 256, 0, s, lp.P, (const float*)lp.y, (const float*)lp.t, lp.dy4, lp.red));
+  LAUNCH(KC_LEARN, 0, (double)N, launch_k(k_lp_loss, kLpRedBlocks, 256, 0, s, lp.P, yin, (const float*)lp.t, lp.dy4, lp.red));
   LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_fold, 1, 32, 0, s, (const double*)lp.red, kLpRedBlocks, 1, lp.acc));
   CKL();
   // layer 4 (a[2] -> y)
@@ -1135,7 +1160,7 @@ int lp_backward(desalm_ctx* ctx, double* loss) {
   RET((lp_wgrad<32, 32>(ctx, lp.tm_a[0], lp.tm_dya[1], lp.dW[1])));
   RET((lp_conv<32, 32>(ctx, lp.tm_dya[1], lp.wd[1], nullptr, 0, lp.a[0], lp.dya[0], nullptr, 0)));
   // layer 1 (x0 -> a[0])
-  RET((lp_wgrad<16, 32>(ctx, lp.tm_x0, lp.tm_dya[0], lp.dW[0])));
+  RET((lp_wgrad<16, 32>(ctx, xin, lp.tm_dya[0], lp.dW[0])));
   const float gscale = float(2.0 / (5.0 * double(N)));
   for (int l = 0; l < 4; ++l) {
     const long n = (long)lp.ly[l].cout * lp.ly[l].cin * 27 + lp.ly[l].cout;
@@ -1143,6 +1168,10 @@ int lp_backward(desalm_ctx* ctx, double* loss) {
                                       (const float*)lp.db[l], gscale, lp.grad));
   }
   CKL();
+  if (hsum) {
+    CK(cudaMemcpyAsync(hsum, lp.acc, sizeof(double), cudaMemcpyDeviceToHost, s));
+    return 0;
+  }
   double sum = 0;
   CK(cudaMemcpyAsync(&sum, lp.acc, sizeof(double), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
@@ -1151,9 +1180,9 @@ int lp_backward(desalm_ctx* ctx, double* loss) {
   return 0;
 }
 
-// Features of (qn, qnm1, qnm2) at table offsets (a, b, c) into lp.x0, with
-// the scales of these three levels (computed on the device).
-int lp_features(desalm_ctx* ctx, int a, int b, int c) {
+// Features of (qn, qnm1, qnm2) at table offsets (a, b, c) into x (lp.x0 or
+// lp.x1), with the scales of these three levels (computed on the device).
+int lp_features(desalm_ctx* ctx, int a, int b, int c, bf16* x) {
   LpState& lp = ctx->lp;
   cudaStream_t s = ctx->stream;
   const long N = lp.N;
@@ -1163,22 +1192,23 @@ int lp_features(desalm_ctx* ctx, int a, int b, int c) {
   LAUNCH(KC_LEARN, 0, (double)N, launch_k(k_lp_sumsq, kLpRedBlocks, 128, 0, s, N, A, B, C, lp.red));
   LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_fold, 1, 32, 0, s, (const double*)lp.red, kLpRedBlocks, 15, lp.acc));
   LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_scales, 1, 32, 0, s, N, (const double*)lp.acc, lp.rs, lp.rs5, lp.s5));
-  LAUNCH(KC_LEARN, 0, (double)N, launch_k(k_lp_features, cdiv(N, 256), 256, 0, s, lp.P, A, B, C, (const float*)lp.rs, lp.x0));
+  LAUNCH(KC_LEARN, 0, (double)N, launch_k(k_lp_features, cdiv(N, 256), 256, 0, s, lp.P, A, B, C, (const float*)lp.rs, x));
   CKL();
   return 0;
 }
 
-// One Adam step on the sample in lp.x0 / lp.t.
-int lp_train_step(desalm_ctx* ctx, double* loss) {
+// One Adam step on the sample whose features xin describes and target lp.t
+// (on lp.ls); hsum: see lp_backward.
+int lp_train_step(desalm_ctx* ctx, const CUtensorMap& xin, double* loss, double* hsum = nullptr) {
   LpState& lp = ctx->lp;
   RET(lp_pack(ctx));
-  RET(lp_forward(ctx));
-  RET(lp_backward(ctx, loss));
+  RET(lp_forward(ctx, xin, lp.yt));
+  RET(lp_backward(ctx, xin, lp.yt, loss, hsum));
   lp.adam_t += 1;
   const float b1 = 0.9f, b2 = 0.999f;
   const float c1 = float(1.0 / (1.0 - std::pow(double(b1), double(lp.adam_t))));
   const float c2 = float(1.0 / (1.0 - std::pow(double(b2), double(lp.adam_t))));
-  LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_adam, cdiv(lp.nparam, 256), 256, 0, ctx->stream, lp.nparam, lp.theta,
+  LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_adam, cdiv(lp.nparam, 256), 256, 0, lp.ls, lp.nparam, lp.theta,
                                     (const float*)lp.grad, lp.m, lp.v, lp.lr, b1, b2, 1e-8f, c1, c2));
   CKL();
   lp.steps += 1;
@@ -1191,27 +1221,68 @@ int lp_train_step(desalm_ctx* ctx, double* loss) {
 int lp_learn(desalm_ctx* ctx) {
   LpState& lp = ctx->lp;
   if (lp.shifts < 1) return 0;  // q^{n-2} not known yet
-  RET(lp_features(ctx, 5, 10, 15));
+  RET(lp_features(ctx, 5, 10, 15, lp.x1));
   LAUNCH(KC_LEARN, 0, (double)lp.N, launch_k(k_lp_target, cdiv(lp.N, 256), 256, 0, ctx->stream, lp.N,
                                              (const double* const*)(lp.tab + 0), (const double* const*)(lp.tab + 5),
                                              (const double* const*)(lp.tab + 10), (const float*)lp.rs5, lp.t));
   CKL();
   // held-out check: the current network on the new sample, before training on it
   RET(lp_pack(ctx));
-  RET(lp_forward(ctx));
+  RET(lp_forward(ctx, lp.tm_x1, lp.y));
   LAUNCH(KC_LEARN, 0, (double)lp.N, launch_k(k_lp_dot, kLpRedBlocks, 128, 0, ctx->stream, lp.N, (const float*)lp.y,
                                              (const float*)lp.t, lp.ymax, lp.red));
   LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_fold, 1, 32, 0, ctx->stream, (const double*)lp.red, kLpRedBlocks, 15, lp.vacc));
   LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_blend, 1, 32, 0, ctx->stream, (const double*)lp.vacc, lp.fixed_alpha, lp.field_mask, lp.alpha));
   CKL();
   lp.samples += 1;
-  for (int it = 0; it < lp.train_steps; ++it) {
+  if (!ctx->prof_on) {  // trained after the prediction, beside the step (lp_train_launch)
+    lp.pending = true;
+    return 0;
+  }
+  for (int it = 0; it < lp.train_steps; ++it) {  // profiling: in line, on the context's stream
     double loss = 0;
-    RET(lp_train_step(ctx, &loss));
+    RET(lp_train_step(ctx, lp.tm_x1, &loss));
     if (lp.first_loss < 0) lp.first_loss = loss;
     lp.last_loss = loss;
   }
   return 0;
+}
+
+// The pending Adam steps on the training stream, after everything the
+// context's stream has queued (the prediction's forward pass included).
+int lp_train_launch(desalm_ctx* ctx) {
+  LpState& lp = ctx->lp;
+  if (!lp.pending) return 0;
+  lp.pending = false;
+  CK(cudaEventRecord(lp.ev_pred, ctx->stream));
+  CK(cudaStreamWaitEvent(lp.tstream, lp.ev_pred, 0));
+  lp.ls = lp.tstream;
+  const int n = std::min(lp.train_steps, 256);
+  int rc = 0;
+  for (int it = 0; it < n && !rc; ++it) rc = lp_train_step(ctx, lp.tm_x1, nullptr, lp.h_loss + it);
+  lp.ls = ctx->stream;
+  RET(rc);
+  CK(cudaEventRecord(lp.ev_train, lp.tstream));
+  lp.h_loss_n = n;
+  lp.inflight = true;
+  return 0;
+}
+
+// Wait for the training in flight: the context's stream waits for it, and
+// its losses and error flag are read.
+int lp_join(desalm_ctx* ctx) {
+  LpState& lp = ctx->lp;
+  if (!lp.inflight) return 0;
+  lp.inflight = false;
+  CK(cudaStreamWaitEvent(ctx->stream, lp.ev_train, 0));
+  CK(cudaEventSynchronize(lp.ev_train));
+  const double scale = 1.0 / (5.0 * double(lp.N));
+  for (int it = 0; it < lp.h_loss_n; ++it) {
+    const double loss = lp.h_loss[it] * scale;
+    if (lp.first_loss < 0) lp.first_loss = loss;
+    lp.last_loss = loss;
+  }
+  return lp_check(ctx);
 }
 
 // After the shift and the linear extrapolation: q <- 2 q^n - q^{n-1} + the
@@ -1221,9 +1292,9 @@ int lp_predict(desalm_ctx* ctx) {
   LpState& lp = ctx->lp;
   lp.predicted = false;
   if (lp.samples < lp.warm || lp.samples < lp.hold_until || lp.shifts < 1) return 0;
-  RET(lp_features(ctx, 5, 10, 15));
+  RET(lp_features(ctx, 5, 10, 15, lp.x0));
   RET(lp_pack(ctx));
-  RET(lp_forward(ctx));
+  RET(lp_forward(ctx, lp.tm_x0, lp.y));
   if (lp.fixed_alpha >= 0.0f || lp.field_mask != 0x1f)
     LAUNCH(KC_LEARN, 0, 0.0, launch_k(k_lp_blend, 1, 32, 0, ctx->stream, (const double*)lp.vacc, lp.fixed_alpha, lp.field_mask, lp.alpha));
   LAUNCH(KC_LEARN, 0, (double)lp.N, launch_k(k_lp_apply, cdiv(lp.N, 256), 256, 0, ctx->stream, lp.N, lp.tab + 0,
@@ -1274,6 +1345,7 @@ const char* desalm_last_error(const desalm_ctx* ctx) { return ctx ? ctx->err.c_s
 
 void desalm_destroy(desalm_ctx* ctx) {
   if (!ctx) return;
+  if (ctx->lp.tstream) cudaStreamSynchronize(ctx->lp.tstream);  // training in flight
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (auto& G : ctx->L)
     for (void* p : G.allocs) cudaFree(p);
@@ -1289,6 +1361,10 @@ void desalm_destroy(desalm_ctx* ctx) {
   if (ctx->side) cudaStreamDestroy(ctx->side);
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+  if (ctx->lp.tstream) cudaStreamDestroy(ctx->lp.tstream);
+  if (ctx->lp.ev_pred) cudaEventDestroy(ctx->lp.ev_pred);
+  if (ctx->lp.ev_train) cudaEventDestroy(ctx->lp.ev_train);
+  if (ctx->lp.h_loss) cudaFreeHost(ctx->lp.h_loss);
   delete ctx;
 }
 
@@ -1821,7 +1897,10 @@ int desalm_begin_step(desalm_ctx* ctx) {
   Level& F = ctx->L[0];
   const bool learned = c.predictor == DESALM_PRED_LEARNED;
   // the learned guess trains on the step just converged before the shift
-  if (learned) RET(lp_learn(ctx));
+  if (learned) {
+    RET(lp_join(ctx));
+    RET(lp_learn(ctx));
+  }
   // qnm1 <- qn; qn <- q (src/mg_driver.F90:48-51)
   for (int m = 0; m < 5; ++m) {
     void *q, *qn, *qnm1;
@@ -1847,6 +1926,7 @@ int desalm_begin_step(desalm_ctx* ctx) {
   if (learned) {
     ctx->lp.shifts += 1;
     RET(lp_predict(ctx));
+    RET(lp_train_launch(ctx));
   }
   // inject qn, qnm1 to the coarse levels (src/mg_driver.F90:55-58)
   for (int n = 1; n < ctx->ng; ++n) {
@@ -2333,6 +2413,7 @@ int graph_step(desalm_ctx* ctx, desalm_step_report* rep) {
 extern "C" {
 
 int desalm_lp_blend(desalm_ctx* ctx, float alpha) {
+  if (ctx && ctx->lp.inflight) RET(lp_join(ctx));  // the training in flight first
   if (!ctx) return DESALM_EINVAL;
   if (!ctx->lp.on) { ctx->err = "the learned guess is off"; return DESALM_EINVAL; }
   if (std::isnan(alpha) || alpha > 1.0f) { ctx->err = "lp_blend: alpha must be <= 1"; return DESALM_EINVAL; }
@@ -2341,6 +2422,7 @@ int desalm_lp_blend(desalm_ctx* ctx, float alpha) {
 }
 
 int desalm_lp_fields(desalm_ctx* ctx, int mask) {
+  if (ctx && ctx->lp.inflight) RET(lp_join(ctx));  // the training in flight first
   if (!ctx) return DESALM_EINVAL;
   if (!ctx->lp.on) { ctx->err = "the learned guess is off"; return DESALM_EINVAL; }
   if (mask < 0 || mask > 0x1f) { ctx->err = "lp_fields: mask must be within 0..31"; return DESALM_EINVAL; }
@@ -2349,6 +2431,7 @@ int desalm_lp_fields(desalm_ctx* ctx, int mask) {
 }
 
 int desalm_lp_config(desalm_ctx* ctx, int train_steps, int warm, float lr, float ymax) {
+  if (ctx && ctx->lp.inflight) RET(lp_join(ctx));  // the training in flight first
   if (!ctx) return DESALM_EINVAL;
   if (!ctx->lp.on) { ctx->err = "the learned guess is off (predictor is not DESALM_PRED_LEARNED)"; return DESALM_EINVAL; }
   if (train_steps > 1000 || warm > 1000000 || !(lr < 1.0f) || std::isnan(ymax)) {
@@ -2363,6 +2446,7 @@ int desalm_lp_config(desalm_ctx* ctx, int train_steps, int warm, float lr, float
 }
 
 int desalm_lp_report_get(desalm_ctx* ctx, desalm_lp_report* r) {
+  if (ctx && ctx->lp.inflight) RET(lp_join(ctx));  // the training in flight first
   if (!ctx || !r) return DESALM_EINVAL;
   const LpState& lp = ctx->lp;
   r->nparam = lp.nparam;
@@ -2392,6 +2476,7 @@ int desalm_lp_report_get(desalm_ctx* ctx, desalm_lp_report* r) {
 }
 
 int desalm_lp_get_params(desalm_ctx* ctx, float* theta) {
+  if (ctx && ctx->lp.inflight) RET(lp_join(ctx));  // the training in flight first
   if (!ctx || !theta) return DESALM_EINVAL;
   if (!ctx->lp.on) { ctx->err = "the learned guess is off"; return DESALM_EINVAL; }
   CK(cudaMemcpyAsync(theta, ctx->lp.theta, ctx->lp.nparam * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
@@ -2400,6 +2485,7 @@ int desalm_lp_get_params(desalm_ctx* ctx, float* theta) {
 }
 
 int desalm_lp_set_params(desalm_ctx* ctx, const float* theta) {
+  if (ctx && ctx->lp.inflight) RET(lp_join(ctx));  // the training in flight first
   if (!ctx || !theta) return DESALM_EINVAL;
   LpState& lp = ctx->lp;
   if (!lp.on) { ctx->err = "the learned guess is off"; return DESALM_EINVAL; }
@@ -2413,6 +2499,7 @@ int desalm_lp_set_params(desalm_ctx* ctx, const float* theta) {
 }
 
 int desalm_lp_eval(desalm_ctx* ctx, const float* x, const float* t, float* y, double* loss, float* grad) {
+  if (ctx && ctx->lp.inflight) RET(lp_join(ctx));  // the training in flight first
   if (!ctx || !x) return DESALM_EINVAL;
   LpState& lp = ctx->lp;
   if (!lp.on) { ctx->err = "the learned guess is off"; return DESALM_EINVAL; }
@@ -2428,12 +2515,12 @@ int desalm_lp_eval(desalm_ctx* ctx, const float* x, const float* t, float* y, do
     CKL();
   }
   RET(lp_pack(ctx));
-  RET(lp_forward(ctx));
+  RET(lp_forward(ctx, lp.tm_x0, lp.y));
   if (y) CK(cudaMemcpyAsync(y, lp.y, 5 * N * sizeof(float), cudaMemcpyDeviceToHost, s));
   if (t) {
     CK(cudaMemcpyAsync(lp.t, t, 5 * N * sizeof(float), cudaMemcpyHostToDevice, s));
     double l = 0;
-    RET(lp_backward(ctx, &l));
+    RET(lp_backward(ctx, lp.tm_x0, lp.y, &l));
     if (loss) *loss = l;
     if (grad) CK(cudaMemcpyAsync(grad, lp.grad, lp.nparam * sizeof(float), cudaMemcpyDeviceToHost, s));
   }
@@ -2443,6 +2530,7 @@ int desalm_lp_eval(desalm_ctx* ctx, const float* x, const float* t, float* y, do
 }
 
 int desalm_lp_get_buffer(desalm_ctx* ctx, int which, float* out) {
+  if (ctx && ctx->lp.inflight) RET(lp_join(ctx));  // the training in flight first
   if (!ctx || !out) return DESALM_EINVAL;
   LpState& lp = ctx->lp;
   if (!lp.on) { ctx->err = "the learned guess is off"; return DESALM_EINVAL; }
@@ -2537,6 +2625,7 @@ int desalm_checkpoint_read(desalm_ctx* ctx, const char* path) {
 // Layout (little-endian): "DESALMLP", int32 version 1, int64 nparam, int64
 // adam steps, int64 samples, then nparam FP32 each of theta, m, v.
 int desalm_lp_checkpoint_write(desalm_ctx* ctx, const char* path) {
+  if (ctx && ctx->lp.inflight) RET(lp_join(ctx));  // the training in flight first
   if (!ctx || !path) return DESALM_EINVAL;
   LpState& lp = ctx->lp;
   if (!lp.on) { ctx->err = "the learned guess is off"; return DESALM_EINVAL; }
@@ -2558,6 +2647,7 @@ int desalm_lp_checkpoint_write(desalm_ctx* ctx, const char* path) {
 }
 
 int desalm_lp_checkpoint_read(desalm_ctx* ctx, const char* path) {
+  if (ctx && ctx->lp.inflight) RET(lp_join(ctx));  // the training in flight first
   if (!ctx || !path) return DESALM_EINVAL;
   LpState& lp = ctx->lp;
   if (!lp.on) { ctx->err = "the learned guess is off"; return DESALM_EINVAL; }
