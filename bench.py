@@ -185,7 +185,7 @@ class Workload:
     """One solver on the bench workload, with the rotor advanced between
     physical steps (src/main.F90:42-50)."""
 
-    def __init__(self, name, precision, predictor, model):
+    def __init__(self, name, precision, predictor, model, lp_mask=None):
         from desalm.solver import Solver
         (self.case, grid, state, omega, self.spec, self.rate, self.desc) = build_case(name, precision, predictor, model)
         self.S = Solver(self.case)
@@ -193,6 +193,8 @@ class Workload:
         self.S.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
         if omega is not None:
             self.S.set_omega(omega["omega"], omega["omega_n"], omega["omega_nm1"])
+        if lp_mask is not None:
+            self.S.lp_fields(lp_mask)
         self.angle = None
         if self.spec is not None:
             self.S.alm_set(self.spec)
@@ -291,14 +293,22 @@ def run_ours(args, rank, world, dist):
     L = S.L
     P = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
 
+    copy_s = []
+
     def e2e_step():
+        t0 = time.perf_counter()
         S._ck(L.desalm_set_state(S.ctx, P(hq), P(hqn), P(hqnm1), P(hnut)), "set_state")
         if kw:
             S._ck(L.desalm_set_omega(S.ctx, P(hw[0]), P(hw[1]), P(hw[2])), "set_omega")
+        t1 = time.perf_counter()
         r = wl.step()
+        S.sync()
+        t2 = time.perf_counter()
         S._ck(L.desalm_get_state(S.ctx, P(hq), P(hqn), P(hqnm1), P(hnut)), "get_state")
         if kw:
             S._ck(L.desalm_get_omega(S.ctx, P(hw[0]), P(hw[1]), P(hw[2])), "get_omega")
+        t3 = time.perf_counter()
+        copy_s.append((t1 - t0) + (t3 - t2))
         return r
 
     e2e_sec, e2e_reps, e2e_per = timed(S, KS, e2e_step, barrier, max_over_ranks)
@@ -344,9 +354,11 @@ def run_ours(args, rank, world, dist):
     # ---- the comparison paths on the same physical steps (W warm-up, KS timed)
     variants = {}
     finals = {}
-    for name, prec, pred in (("fp64_plain", abi.FP64, abi.PRED_LINEAR), ("fp64_qn", abi.FP64, abi.PRED_QN),
-                             ("mixed_linear", abi.MIXED, abi.PRED_LINEAR)):
-        v = Workload(args.case, prec, pred, args.model)
+    for name, prec, pred, mask in (("fp64_plain", abi.FP64, abi.PRED_LINEAR, None),
+                                   ("fp64_qn", abi.FP64, abi.PRED_QN, None),
+                                   ("mixed_linear", abi.MIXED, abi.PRED_LINEAR, None),
+                                   ("learned_p_corrected", abi.MIXED, abi.PRED_LEARNED, 1)):
+        v = Workload(args.case, prec, pred, args.model, lp_mask=mask)
         _, wreps, wper = timed(v.S, W, v.step, barrier, max_over_ranks)
         vsec, vreps, vper = timed(v.S, KS, v.step, barrier, max_over_ranks)
         variants[name] = dict({"value": vsec, "unit": UNIT, "steps": "%d-%d" % (W + 1, W + KS)}, **steps_summary(vreps, vper))
@@ -359,6 +371,8 @@ def run_ours(args, rank, world, dist):
     variants["fp64_plain"]["guess"] = "linear extrapolation (the plain guess)"
     variants["fp64_qn"]["guess"] = "q^n (the reference's mg_driver)"
     variants["mixed_linear"]["guess"] = "linear extrapolation"
+    variants["learned_p_corrected"]["guess"] = ("learned, the network's correction applied to p (desalm_lp_fields(1)) "
+                                                "with the automatic blend")
     a = np.asarray(finals["mixed_linear"]).reshape(-1, 5)
     b = np.asarray(finals["fp64_plain"]).reshape(-1, 5)
     names = ["p", "u", "v", "w", "k" if kw else "nu_tilde"]
@@ -384,8 +398,10 @@ def run_ours(args, rank, world, dist):
                    "interior_nodes": wl.nint,
                    "precision": "mixed (FP64 state, residual, restriction, update and norm on every level; FP32 line "
                                 "sweeps, modal transforms and turbulence ADI)",
-                   "predictor": "learned (3D conv network trained online on the GPU; linear extrapolation plus its "
-                                "blended correction)",
+                   "predictor": "learned: 3D conv network trained online on the GPU (its Adam steps overlapped with "
+                                "the physical step); the guess is linear extrapolation plus the blended correction "
+                                "of the fields in the library's default mask, which is none (every correction "
+                                "measured raised the pseudo-iterations: see learned_p_corrected)",
                    "convergence": "mg_ck_conver: after it_min=7, u,v,w update drop below 1e-6 of the step's first "
                                   "(er_min=-6) or below 10^-7.5 absolute (eo_min=-7.5, the reference deck "
                                   "ind3dmg.dat:4); itmax 400",
@@ -398,6 +414,7 @@ def run_ours(args, rank, world, dist):
         "fp64_plain": variants["fp64_plain"],
         "fp64_qn": variants["fp64_qn"],
         "mixed_linear": variants["mixed_linear"],
+        "learned_p_corrected": variants["learned_p_corrected"],
         "speedup_vs_fp64_plain": variants["fp64_plain"]["value"] / sec,
         "mixed_vs_fp64_rel_l2": {"fields": field_err,
                                  "how": "relative L2 over all nodes after %d physical steps from the same state, "
@@ -405,7 +422,8 @@ def run_ours(args, rank, world, dist):
                                         "the FP64 oracle to 1e-10 at this size: tests/test_gpu_fullsize.py)" % (W + KS)},
         "cell_updates_per_s": sum_over_ranks(cell_updates),
         "e2e": {"value": e2e_sec, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
-                "steps": KS},
+                "steps": KS, "pseudo_iterations_per_step": [r["iterations"] for r in e2e_reps],
+                "copy_s_per_step": float(np.mean(copy_s)) if copy_s else None},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "kernel": kind, "level": "fine", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,

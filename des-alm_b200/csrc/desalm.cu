@@ -149,14 +149,16 @@ struct LpState {
   double* vacc = nullptr;                  // held-out check of the newest sample (k_lp_dot)
   float* alpha = nullptr;                  // blend of each field's correction
   float fixed_alpha = -1.0f;               // < 0: automatic blend
-  // bit f: field f takes the correction.  Default p only: a correction of
-  // the velocities is not discretely divergence-free, and the artificial
-  // compressibility relaxes that error slowly (on the cavity the velocity
-  // corrections cost 8.6 more pseudo-iterations per step); a correction of
-  // the turbulence field (nu_tilde or k) moves nu_t and so the momentum
-  // residual (on the turbine box it raised steps from about 92 to 103-190
-  // pseudo-iterations)
-  int field_mask = 0x01;
+  // bit f: field f takes the correction.  Default none: the linear
+  // extrapolation of converged time levels satisfies the discrete continuity
+  // and momentum balance to second order in dt, and a pointwise correction
+  // of any field breaks that consistency, which the artificial-compressibility
+  // iteration then relaxes slowly.  Measured: velocity corrections cost 8.6
+  // more pseudo-iterations per step on the cavity; on the turbine box a
+  // pressure correction raised steps from 91-128 to 134-312 pseudo-iterations
+  // (blend 0.25: 98-219), a turbulence-field correction to 103-190.  The
+  // network still trains on every step and reports its held-out error.
+  int field_mask = 0x00;
   double* qnm2[5] = {};                    // q^{n-2} of the fine level
   double* nut0 = nullptr;                  // nu_t at the start of a step begun from the network's guess
   double** tab = nullptr;                  // device table: q[5] qn[5] qnm1[5] qnm2[5]

@@ -189,12 +189,17 @@ DESALM_DEV void kw_adi_rows(const KwT<SW>& K, int l, double fk, double fw) {
   K.cow[3 * DIR + 2][l] = dw * ce;
 }
 
+// Minimum resident CTAs per SM requested for k_kw_rhs (128 threads each); a
+// build-time tuning knob.
+#ifndef DESALM_KW_MINBLOCKS
+#define DESALM_KW_MINBLOCKS 3
+#endif
 // One fused pass over the interior of rhs_kw_prod, rhs_kw_viscous,
 // rhs_kw_flux, rhs_kw_unst_visc and rhs_kw_implicit_source, giving the
 // right-hand sides of k and omega already divided by dk and dw (the i sweep's
 // input), and the ADI rows of both scalars.
 template <class SW>
-__global__ void __launch_bounds__(128) k_kw_rhs(KwT<SW> K) {
+__global__ void __launch_bounds__(128, DESALM_KW_MINBLOCKS) k_kw_rhs(KwT<SW> K) {
   pdl_wait();
   const SaT<SW>& S = K.S;
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;

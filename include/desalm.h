@@ -352,10 +352,12 @@ int  desalm_lp_report_get(desalm_ctx* ctx, desalm_lp_report* r);
 int  desalm_lp_blend(desalm_ctx* ctx, float alpha);
 /* Which fields take the network's correction: bit f of mask for field f
  * (p, u, v, w, nu_tilde); the others keep the linear extrapolation.
- * Default 1 (p only): a velocity correction is not discretely
- * divergence-free, and the pseudo-time iteration relaxes that error slowly;
- * a correction of the turbulence field moves nu_t and the momentum residual
- * with it. */
+ * Default 0 (no field): the linear extrapolation of converged time levels
+ * satisfies the discrete equations to second order in dt, and a pointwise
+ * correction of any field breaks that consistency, which the
+ * artificial-compressibility iteration relaxes slowly (every correction
+ * measured raised the pseudo-iterations per step).  The network still trains
+ * on every step; desalm_lp_report_get gives its held-out error. */
 int  desalm_lp_fields(desalm_ctx* ctx, int mask);
 /* nparam floats in the flat layout above; set restarts the Adam moments */
 int  desalm_lp_get_params(desalm_ctx* ctx, float* theta);
