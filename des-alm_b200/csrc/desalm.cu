@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <utility>
 #include <random>
+#include <type_traits>
 
 #include "desalm.h"
 #include "common.cuh"
@@ -199,6 +200,15 @@ struct desalm_ctx {
   // lines per CTA of each level's DAF sweeps [level][direction], picked by
   // timing when the grid is set (autotune_sweeps); 0: the shared-memory rule
   int sweep_nl[4][3] = {};
+  // CTA tile (i, j, k threads) of each level's residual kernels [level][0 =
+  // K_R first pass, 1 = recalculation, 2 = turbulence residual], picked by
+  // timing when the grid is set (autotune_tiles); the build's default shape
+  // where the timing is off.  The tile changes the time only: every node is
+  // computed by the same operations.
+  unsigned tile[4][3][3] = {{{32, DESALM_KR_BY, DESALM_KR_BZ}, {32, DESALM_KR_BY, DESALM_KR_BZ}, {32, DESALM_KR_BY, DESALM_KR_BZ}},
+                            {{32, DESALM_KR_BY, DESALM_KR_BZ}, {32, DESALM_KR_BY, DESALM_KR_BZ}, {32, DESALM_KR_BY, DESALM_KR_BZ}},
+                            {{32, DESALM_KR_BY, DESALM_KR_BZ}, {32, DESALM_KR_BY, DESALM_KR_BZ}, {32, DESALM_KR_BY, DESALM_KR_BZ}},
+                            {{32, DESALM_KR_BY, DESALM_KR_BZ}, {32, DESALM_KR_BY, DESALM_KR_BZ}, {32, DESALM_KR_BY, DESALM_KR_BZ}}};
   double* pfix = nullptr;     // device scalar (type of the fine level: double)
   double* part = nullptr;     // norm partials
   int part_blocks = 0;
@@ -413,8 +423,15 @@ dim3 blk3() { return dim3(32, 4, 1); }
 template <class T, class W>
 dim3 grid_interior(const Lv<T, W>& L) { return dim3(cdiv(L.im - 2, 32), cdiv(L.jm - 2, 4), L.km - 2); }
 // the residual kernels' CTA shape (DESALM_KR_BY j rows x DESALM_KR_BZ k planes)
-dim3 blk_r() { return dim3(32, DESALM_KR_BY, DESALM_KR_BZ); }
-dim3 grid_r(int im, int jm, int km) { return dim3(cdiv(im - 2, 32), cdiv(jm - 2, DESALM_KR_BY), cdiv(km - 2, DESALM_KR_BZ)); }
+// the tuned tile of residual kernel `which` on level lvl, and its grid over the interior
+dim3 blk_t(const desalm_ctx* ctx, int lvl, int which) {
+  const unsigned* t = ctx->tile[lvl][which];
+  return dim3(t[0], t[1], t[2]);
+}
+dim3 grid_t(const desalm_ctx* ctx, int lvl, int which, int im, int jm, int km) {
+  const unsigned* t = ctx->tile[lvl][which];
+  return dim3(cdiv(im - 2, t[0]), cdiv(jm - 2, t[1]), cdiv(km - 2, t[2]));
+}
 
 // One DAF line sweep as k_sweep4 with the widest slab (lines per CTA) whose
 // shared memory leaves room for two CTAs per SM, else the widest that fits
@@ -574,7 +591,7 @@ int launch_daf(desalm_ctx* ctx, Lv<T, W>& L, Level& G, int n, int recalc, int it
            launch_k(k_outlet<T, W>, dim3(cdiv(L.jm - 2, 32), cdiv(L.km - 2, 4)), dim3(32, 4), 0, ctx->side, L, P));
     CKL();
   }
-  LAUNCH(KC_RESID, n, nin, launch_k(k_resid<T, W, 0>, grid_r(L.im, L.jm, L.km), blk_r(), 0, s, L, P, upwind, itr == 1 ? 1 : 0, n > 0 ? 1 : 0, bback));
+  LAUNCH(KC_RESID, n, nin, launch_k(k_resid<T, W, 0>, grid_t(ctx, n, 0, L.im, L.jm, L.km), blk_t(ctx, n, 0), 0, s, L, P, upwind, itr == 1 ? 1 : 0, n > 0 ? 1 : 0, bback));
   CKL();
   if (out_side) RET(join_side(ctx));
   if (L.oute && !out_side) {
@@ -592,7 +609,7 @@ template <class T, class W>
 int launch_recalc(desalm_ctx* ctx, Lv<T, W>& L, int n) {
   Par P = ctx->par;
   P.fine = (n == 0);
-  LAUNCH(KC_RECALC, n, double(L.im - 2) * (L.jm - 2) * (L.km - 2), launch_k(k_resid<T, W, 1>, grid_r(L.im, L.jm, L.km), blk_r(), 0, ctx->stream, L, P, n == 0 ? 2 : 1, 0, n > 0 ? 1 : 0, 0));
+  LAUNCH(KC_RECALC, n, double(L.im - 2) * (L.jm - 2) * (L.km - 2), launch_k(k_resid<T, W, 1>, grid_t(ctx, n, 1, L.im, L.jm, L.km), blk_t(ctx, n, 1), 0, ctx->stream, L, P, n == 0 ? 2 : 1, 0, n > 0 ? 1 : 0, 0));
   CKL();
   return 0;
 }
@@ -784,11 +801,68 @@ int tune_level(desalm_ctx* ctx, Lv<T, W>& L, int lvl, cudaEvent_t e0, cudaEvent_
   return tune_sweep<T, W, 2>(ctx, L, lvl, e0, e1);
 }
 
-// Picks the sweep widths of every level, unless DESALM_AUTOTUNE=0 in the
-// environment (then the shared-memory rule alone decides).
+template <class SW, class W> SaT<SW> make_sa(desalm_ctx* ctx, Lv<double, W>& L);
+template <class W> KwT<W> make_kw(desalm_ctx* ctx, Lv<double, W>& L);
+
+// CTA tiles of 128 threads the residual kernels are timed with
+constexpr unsigned kTiles[8][3] = {{32, 4, 1}, {32, 2, 2}, {32, 1, 4}, {64, 2, 1}, {64, 1, 2}, {128, 1, 1}, {16, 8, 1}, {16, 4, 2}};
+
+// Times one residual kernel (which: 0 = K_R, 1 = recalculation, 2 =
+// turbulence residual) on level lvl at every tile and keeps the fastest.
+// The kernels run on the level's current arrays; what they write (the line
+// sweeps' inputs, rh, the turbulence ADI rows) is rewritten before any use,
+// and the FAS forcing pk is left alone (no pk update is asked for).
+template <class T, class W>
+int tune_tile(desalm_ctx* ctx, Lv<T, W>& L, int lvl, int which, cudaEvent_t e0, cudaEvent_t e1) {
+  Par P = ctx->par;
+  P.fine = (lvl == 0);
+  cudaStream_t s = ctx->stream;
+  auto run = [&]() -> cudaError_t {
+    const dim3 g = grid_t(ctx, lvl, which, L.im, L.jm, L.km), b = blk_t(ctx, lvl, which);
+    if (which == 0) return launch_k(k_resid<T, W, 0>, g, b, 0, s, L, P, lvl > 0 ? 1 : 0, 0, lvl > 0 ? 1 : 0, 0);
+    if (which == 1) return launch_k(k_resid<T, W, 1>, g, b, 0, s, L, P, lvl == 0 ? 2 : 1, 0, lvl > 0 ? 1 : 0, 0);
+    if constexpr (std::is_same<T, double>::value) {
+      if (ctx->c.turbulence == 2) return launch_k(k_kw_rhs<W>, g, b, 0, s, make_kw<W>(ctx, L));
+      return launch_k(k_sa_rhs<W>, g, b, 0, s, make_sa<W>(ctx, L));
+    }
+    return cudaSuccess;
+  };
+  float best = 0.f;
+  int pick = -1;
+  for (int t = 0; t < 8; ++t) {
+    for (int d = 0; d < 3; ++d) ctx->tile[lvl][which][d] = kTiles[t][d];
+    CK(run());
+    CK(cudaEventRecord(e0, s));
+    for (int r = 0; r < 3; ++r) CK(run());
+    CK(cudaEventRecord(e1, s));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    if (pick < 0 || ms < best) { best = ms; pick = t; }
+  }
+  for (int d = 0; d < 3; ++d) ctx->tile[lvl][which][d] = kTiles[pick][d];
+  return 0;
+}
+
+template <class T, class W>
+int tune_tiles_level(desalm_ctx* ctx, Lv<T, W>& L, int lvl, cudaEvent_t e0, cudaEvent_t e1) {
+  RET((tune_tile<T, W>(ctx, L, lvl, 0, e0, e1)));
+  RET((tune_tile<T, W>(ctx, L, lvl, 1, e0, e1)));
+  if (lvl == 0 && ctx->c.turbulence) RET((tune_tile<T, W>(ctx, L, lvl, 2, e0, e1)));
+  return 0;
+}
+
+// Picks the sweep widths and the residual kernels' tiles of every level,
+// unless DESALM_AUTOTUNE=0 in the environment (then the shared-memory rule
+// and the build's default tile decide).
 int autotune_sweeps(desalm_ctx* ctx) {
   for (int n = 0; n < 4; ++n)
-    for (int d = 0; d < 3; ++d) ctx->sweep_nl[n][d] = 0;
+    for (int d = 0; d < 3; ++d) {
+      ctx->sweep_nl[n][d] = 0;
+      for (int w = 0; w < 3; ++w) {
+        ctx->tile[n][w][0] = 32; ctx->tile[n][w][1] = DESALM_KR_BY; ctx->tile[n][w][2] = DESALM_KR_BZ;
+      }
+    }
   const char* env = std::getenv("DESALM_AUTOTUNE");
   if (env && std::string(env) == "0") return 0;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -803,6 +877,7 @@ int autotune_sweeps(desalm_ctx* ctx) {
   for (int n = 0; n < ctx->ng && n < 4 && !rc; ++n) {
     Level& G = ctx->L[n];
     rc = kind_of(ctx, n) == K_DD ? tune_level(ctx, G.dd, n, e0, e1) : tune_level(ctx, G.df, n, e0, e1);
+    if (!rc) rc = kind_of(ctx, n) == K_DD ? tune_tiles_level(ctx, G.dd, n, e0, e1) : tune_tiles_level(ctx, G.df, n, e0, e1);
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -2012,6 +2087,14 @@ int desalm_sweep_widths(desalm_ctx* ctx, int nl[12]) {
   return 0;
 }
 
+int desalm_kernel_tiles(desalm_ctx* ctx, int tiles[36]) {
+  if (!ctx || !tiles) return DESALM_EINVAL;
+  for (int n = 0; n < 4; ++n)
+    for (int w = 0; w < 3; ++w)
+      for (int d = 0; d < 3; ++d) tiles[9 * n + 3 * w + d] = n < ctx->ng ? (int)ctx->tile[n][w][d] : 0;
+  return 0;
+}
+
 int desalm_sync(desalm_ctx* ctx) {
   if (!ctx) return DESALM_EINVAL;
   CK(cudaStreamSynchronize(ctx->stream));
@@ -2196,7 +2279,7 @@ int sa_run(desalm_ctx* ctx, Lv<double, W>& L) {
   LAUNCH(KC_SA_AUX, 0, nin, launch_k(k_sa_source<W>, gi, blk3(), 0, s, S));
   LAUNCH(KC_SA_AUX, 0, L.N, launch_k(k_sa_ucn<W>, cdiv(L.N, 256), 256, 0, s, S));
   for (int it = 0; it < ctx->c.itk; ++it) {
-    LAUNCH(KC_SA_RHS, 0, nin, launch_k(k_sa_rhs<W>, grid_r(L.im, L.jm, L.km), blk_r(), 0, s, S));
+    LAUNCH(KC_SA_RHS, 0, nin, launch_k(k_sa_rhs<W>, grid_t(ctx, 0, 2, L.im, L.jm, L.km), blk_t(ctx, 0, 2), 0, s, S));
     RET((sa_sweep<W, 0>(ctx, S, L.jm - 2, L.im - 2, L.km - 2, nin)));
     RET((sa_sweep<W, 1>(ctx, S, L.im - 2, L.jm - 2, L.km - 2, nin)));
     RET((sa_sweep<W, 2>(ctx, S, L.im - 2, L.km - 2, L.jm - 2, nin)));
@@ -2261,7 +2344,7 @@ int kw_run(desalm_ctx* ctx, Lv<double, W>& L) {
   LAUNCH(KC_SA_AUX, 0, L.N, launch_k(k_sa_ucn<W>, cdiv(L.N, 256), 256, 0, s, K.S));
   LAUNCH(KC_SA_AUX, 0, L.N, launch_k(k_kw_pre<W>, cdiv(L.N, 256), 256, 0, s, K));
   for (int it = 0; it < ctx->c.itk; ++it) {
-    LAUNCH(KC_SA_RHS, 0, nin, launch_k(k_kw_rhs<W>, grid_r(L.im, L.jm, L.km), blk_r(), 0, s, K));
+    LAUNCH(KC_SA_RHS, 0, nin, launch_k(k_kw_rhs<W>, grid_t(ctx, 0, 2, L.im, L.jm, L.km), blk_t(ctx, 0, 2), 0, s, K));
     RET((sa_sweep<W, 0>(ctx, K.S, L.jm - 2, L.im - 2, L.km - 2, nin)));
     RET((sa_sweep<W, 1>(ctx, K.S, L.im - 2, L.jm - 2, L.km - 2, nin)));
     RET((sa_sweep<W, 2>(ctx, K.S, L.im - 2, L.km - 2, L.jm - 2, nin)));

@@ -318,6 +318,13 @@ class Solver:
     def conservation(self):
         self._ck(self.L.desalm_conservation(self.ctx), "conservation")
 
+    def kernel_tiles(self):
+        """CTA tiles of the residual kernels, [level][kernel][axis] (kernel 0
+        K_R, 1 the recalculated residual, 2 the turbulence residual)."""
+        out = (C.c_int * 36)()
+        self._ck(self.L.desalm_kernel_tiles(self.ctx, out), "kernel_tiles")
+        return np.array(list(out)).reshape(4, 3, 3)
+
     def sweep_widths(self):
         """Lines per CTA of the DAF sweeps, [level][direction] (0: not tuned)."""
         out = (C.c_int * 12)()

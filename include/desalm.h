@@ -252,6 +252,14 @@ int  desalm_mg_driver_batch(desalm_ctx* const* ctxs, int n, desalm_step_report* 
  * leaves room for two CTAs per SM is used.  The width changes the time
  * only: every line is solved by the same operations. */
 int  desalm_sweep_widths(desalm_ctx* ctx, int nl[12]);
+/* CTA tile (threads along i, j, k; 128 in all) of each level's residual
+ * kernels, tiles[9 * level + 3 * kernel + axis], kernel 0 = the first
+ * residual pass (K_R), 1 = the recalculated residual, 2 = the turbulence
+ * residual (fine level only): timed at eight tiles when the grid is set and
+ * the fastest kept, or 32 x 4 x 1 where the timing is off (DESALM_AUTOTUNE=0).
+ * The tile changes the time only: every node is computed by the same
+ * operations. */
+int  desalm_kernel_tiles(desalm_ctx* ctx, int tiles[36]);
 /* One pseudo-time iteration of the loop above (for callers that drive the
  * loop themselves); rep->residual receives the iteration's residual. */
 int  desalm_pseudo_iteration(desalm_ctx* ctx, desalm_step_report* rep);

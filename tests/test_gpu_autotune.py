@@ -1,8 +1,10 @@
-"""The sweep-width autotuner: desalm_set_grid times the DAF sweeps of every
-level and direction at 16, 8 and 4 lines per CTA and keeps the fastest.  The
-width may change the time only, so a tuned context must step exactly like
-one on the shared-memory rule (DESALM_AUTOTUNE=0), and the timing runs must
-leave the state alone."""
+"""The autotuner: desalm_set_grid times the DAF sweeps of every level and
+direction at 16, 8 and 4 lines per CTA, and the residual kernels (first pass,
+recalculation, turbulence residual) at eight CTA tiles of 128 threads, and
+keeps the fastest of each.  Widths and tiles may change the time only, so a
+tuned context must step exactly like one on the shared-memory rule and the
+default tile (DESALM_AUTOTUNE=0), and the timing runs must leave the state
+alone."""
 import numpy as np
 import pytest
 
@@ -31,6 +33,12 @@ def test_tuned_widths_change_nothing_but_time(precision, monkeypatch):
     w = tuned.sweep_widths()
     assert set(np.unique(w[:case.ng])) <= {4, 8, 16} and not w[case.ng:].any()
     assert not rule.sweep_widths().any()
+    tiles = tuned.kernel_tiles()
+    shapes = {(32, 4, 1), (32, 2, 2), (32, 1, 4), (64, 2, 1), (64, 1, 2), (128, 1, 1), (16, 8, 1), (16, 4, 2)}
+    for n in range(case.ng):
+        for w in range(3 if n == 0 else 2):
+            assert tuple(tiles[n, w]) in shapes
+    assert all(tuple(t) == (32, 4, 1) for t in rule.kernel_tiles()[:case.ng, :2].reshape(-1, 3))
     # the timing runs at set_grid touched no state
     assert np.array_equal(tuned.get_state()["q"], rule.get_state()["q"])
     for _ in range(2):
