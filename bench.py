@@ -66,7 +66,7 @@ SECONDARY_STEPS = 3     # timed steps of each comparison variant (after the same
 # line-solve scratch are not algorithmic.
 def alg_bytes(kind, T, W, coarse, model="sa"):
     pk = 4 * T if coarse else 0
-    turb_rhs = (22 * 8 + 10 * W) if model == "sa" else (27 * 8 + 2 * 8 + 20 * W)
+    turb_rhs = (22 * 8 + 10 * W) if model == "sa" else (27 * 8 + 20 * W)
     return {
         "resid": 24 * T + 11 * W + pk,    # q4 qn3 qnm1-3 metrics9 aj 1/aj nut dtau | wk4 sigma tc3 hc3, diss1
         "recalc": 26 * T + pk,            # q4 qn3 qnm1-3 metrics9 aj 1/aj nut diss1 | rh4
@@ -81,7 +81,7 @@ def alg_bytes(kind, T, W, coarse, model="sa"):
         "rsmooth": (20 * W + 8 * T) / 3,  # dq4 in/out in W; the k direction reads dq4 and updates q4 (mean of 3)
         "prolong": 4 * W,                 # dq4 out in W (coarse reads amortised)
         # SA: q5 qn5 qnm1-5, U/J 3, metrics9, aj, 1/aj, wd, wo, dtev | rh, ADI rows 9
-        # k-omega: k w kn km1 wn wm1 u v w U/J3 metrics9 aj nut ptke As Ac Bs dtev | dk dw | rh2 rows18
+        # k-omega: k w kn km1 wn wm1 u v w U/J3 metrics9 aj nut ptke As Ac Bs dtev | rh2 rows18
         "sa_rhs": turb_rhs,
         "sa_sweep": 5 * W + 8,            # ADI row 3, rh in/out; k sweep: scalar in/out, dtev (1/3 each)
     }.get(kind)
