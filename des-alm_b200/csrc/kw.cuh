@@ -95,7 +95,7 @@ __global__ void k_kw_pre(KwT<SW> K) {
 // (src/rhs_kw_viscous.F90:49-238): rei + nu_t / sigma at both nodes,
 // sigma_k = sigma_w = 2.
 template <class SW>
-DESALM_DEV void kw_visc_face(const KwT<SW>& K, int dir, int l0, double rei, double out[2]) {
+DESALM_DEV void kw_visc_face(const KwT<SW>& K, int dir, int l0, double rei, double out[2], double* gvt = nullptr) {
   const SaT<SW>& S = K.S;
   const int sj = S.sj, sk = S.sk;
   int l1;
@@ -132,13 +132,16 @@ DESALM_DEV void kw_visc_face(const KwT<SW>& K, int dir, int l0, double rei, doub
   const double vtj = 0.25 * (r1 + r0) * rsa;
   out[0] = vtj * (k1 * g[0][0] + k2 * g[0][1] + k3 * g[0][2]);
   out[1] = vtj * (k1 * g[1][0] + k2 * g[1][1] + k3 * g[1][2]);
+  // the face's diffusive ADI coefficient: (1/Re + (nu_t1 + nu_t0) / 4)
+  // |g_dir|^2 / (J1 + J0) with the summed metrics, which is 2 vtj k1
+  if (gvt) *gvt = 2.0 * vtj * k1;
 }
 
 // First-order flux-difference upwind fluxes of k and omega through the
 // face l0 -> l0 + st (src/rhs_kw_flux.F90:20-166): the face speed is formed
 // from the summed metrics and velocities over the summed Jacobians.
 template <class SW>
-DESALM_DEV void kw_conv_face(const KwT<SW>& K, int dir, int l0, int st, double out[2]) {
+DESALM_DEV void kw_conv_face(const KwT<SW>& K, int dir, int l0, int st, double out[2], double* ucf = nullptr) {
   const SaT<SW>& S = K.S;
   const int l1 = l0 + st;
   const double* const* mt = dir == 0 ? S.csi : (dir == 1 ? S.eta : S.zet);
@@ -150,43 +153,32 @@ DESALM_DEV void kw_conv_face(const KwT<SW>& K, int dir, int l0, int st, double o
   const double* k5 = S.q[4];
   out[0] = 0.5 * (k5[l1] * u1 + k5[l0] * u0 - eigh * (k5[l1] - k5[l0]));
   out[1] = 0.5 * (K.om[l1] * u1 + K.om[l0] * u0 - eigh * (K.om[l1] - K.om[l0]));
+  if (ucf) { ucf[0] = u0; ucf[1] = u1; }
 }
 
-// ADI rows of k and of omega along DIR at interior node l.  With sigma_k =
-// sigma_w = 2 both scalars have the same face coefficients av (convection
-// plus diffusivity), so they are formed once; the rows differ only in the
-// implicit-source factor that divides them (dk for k, dw for omega).
-template <class SW, int DIR>
-DESALM_DEV void kw_adi_rows(const KwT<SW>& K, int l, double fk, double fw) {
+// ADI rows of k and of omega along direction d at interior node l
+// (restated from src/rhs_sa_adi_solver.F90:53-71), from the two faces the
+// residual has just formed: av = |U/J| on the face + the face's diffusive
+// coefficient (1/Re + (nu_t1 + nu_t0) / (2 sigma)) |g_d|^2 / (J1 + J0), with
+// sigma_k = sigma_w = 2 for both scalars; their rows differ only in the
+// implicit-source factor that divides them (dk for k, dw for omega).  gm, gp:
+// the diffusive coefficients of the faces (l - s, l) and (l, l + s); um, up:
+// their U/J pairs.
+template <class SW>
+DESALM_DEV void kw_adi_rows(const KwT<SW>& K, int l, int d, double gm, double gp, const double um[2],
+                            const double up[2], double aj, double dtev, double fk, double fw) {
   const SaT<SW>& S = K.S;
-  const int st = DIR == 0 ? 1 : (DIR == 1 ? S.sj : S.sk);
-  const double* const* mt = DIR == 0 ? S.csi : (DIR == 1 ? S.eta : S.zet);
-  const SW rei = SW(1.0 / S.ren), half_ = SW(0.5);
-  SW m0[3], m1[3], m2[3], nu[3], aj[3], u[3];
-#pragma unroll
-  for (int t = 0; t < 3; ++t) {
-    const int n = l + (t - 1) * st;
-    m0[t] = SW(mt[0][n]); m1[t] = SW(mt[1][n]); m2[t] = SW(mt[2][n]);
-    nu[t] = SW(S.nut[n]); aj[t] = SW(S.aj[n]);
-    u[t] = SW(S.uc[DIR][n]);
-  }
-  SW av[2];
-#pragma unroll
-  for (int g = 0; g < 2; ++g) {
-    const SW gx = m0[g + 1] + m0[g], gy = m1[g + 1] + m1[g], gz = m2[g + 1] + m2[g];
-    const SW ev = rei + half_ * (nu[g + 1] + nu[g]) * half_;  // sigma_k = sigma_w = 2
-    const SW ucna = half_ * dabs(u[g + 1] + u[g]);
-    av[g] = ucna + ev * (gx * gx + gy * gy + gz * gz) / (aj[g + 1] + aj[g]);
-  }
-  const SW base = half_ * SW(S.dtev[l]) * aj[1];
-  const SW cw = u[0] + av[0], cp = av[0] + av[1], ce = u[2] - av[1];
-  const SW dk = base / SW(fk), dw = base / SW(fw);
-  S.co[3 * DIR + 0][l] = -dk * cw;
-  S.co[3 * DIR + 1][l] = SW(1) + dk * cp;
-  S.co[3 * DIR + 2][l] = dk * ce;
-  K.cow[3 * DIR + 0][l] = -dw * cw;
-  K.cow[3 * DIR + 1][l] = SW(1) + dw * cp;
-  K.cow[3 * DIR + 2][l] = dw * ce;
+  const double av0 = 0.5 * fabs(um[1] + um[0]) + gm;
+  const double av1 = 0.5 * fabs(up[1] + up[0]) + gp;
+  const double base = 0.5 * dtev * aj;
+  const double cw = um[0] + av0, cp = av0 + av1, ce = up[1] - av1;
+  const double dk = base / fk, dw = base / fw;
+  S.co[3 * d + 0][l] = SW(-dk * cw);
+  S.co[3 * d + 1][l] = SW(1.0 + dk * cp);
+  S.co[3 * d + 2][l] = SW(dk * ce);
+  K.cow[3 * d + 0][l] = SW(-dw * cw);
+  K.cow[3 * d + 1][l] = SW(1.0 + dw * cp);
+  K.cow[3 * d + 2][l] = SW(dw * ce);
 }
 
 // Minimum resident CTAs per SM requested for k_kw_rhs (128 threads each); a
@@ -216,17 +208,19 @@ __global__ void __launch_bounds__(128, DESALM_KW_MINBLOCKS) k_kw_rhs(KwT<SW> K) 
   const double pkw2a = -K.Ac[l] * wv * K.ptke[l] / kv;
   const double pkw2b = cw2 * wv * wv;
   const double pk2 = (pkw2a + pkw2b) / aj;
-  // viscous and convective face fluxes
+  // viscous and convective face fluxes; each face also gives what the ADI
+  // rows of its direction need (diffusive coefficient, U/J pair)
   double v[2] = {0, 0}, r[2] = {0, 0}, fp[2], fm[2];
+  double gdm[3], gdp[3], ucm[3][2], ucp[3][2];
   const int st[3] = {1, sj, sk};
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    kw_visc_face(K, d, l, rei, fp);
-    kw_visc_face(K, d, l - st[d], rei, fm);
+    kw_visc_face(K, d, l, rei, fp, &gdp[d]);
+    kw_visc_face(K, d, l - st[d], rei, fm, &gdm[d]);
     v[0] = v[0] + fp[0] - fm[0];
     v[1] = v[1] + fp[1] - fm[1];
-    kw_conv_face(K, d, l, st[d], fp);
-    kw_conv_face(K, d, l - st[d], st[d], fm);
+    kw_conv_face(K, d, l, st[d], fp, ucp[d]);
+    kw_conv_face(K, d, l - st[d], st[d], fm, ucm[d]);
     r[0] = r[0] + fp[0] - fm[0];
     r[1] = r[1] + fp[1] - fm[1];
   }
@@ -242,9 +236,8 @@ __global__ void __launch_bounds__(128, DESALM_KW_MINBLOCKS) k_kw_rhs(KwT<SW> K) 
   const double dwv = 1.0 + cw2 * dtev * wv;
   S.rh[l] = SW((-dtev * aj * r1) / dkv);
   K.rhw[l] = SW((-dtev * aj * r2) / dwv);
-  kw_adi_rows<SW, 0>(K, l, dkv, dwv);
-  kw_adi_rows<SW, 1>(K, l, dkv, dwv);
-  kw_adi_rows<SW, 2>(K, l, dkv, dwv);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) kw_adi_rows(K, l, d, gdm[d], gdp[d], ucm[d], ucp[d], aj, dtev, dkv, dwv);
 }
 
 // rhs_kw_bcond's faces of one direction (src/rhs_kw_bcond.F90:51-475): side
