@@ -97,7 +97,7 @@ __global__ void k_sa_source(SaT<SW> S) {
 // viscous flux of nu_tilde through the face l0 -> l0 + st[dir]
 // (src/rhs_sa_viscous.F90:58-175)
 template <class SW>
-DESALM_DEV double sa_visc_face(const SaT<SW>& S, int dir, int l0, double rei, double rsig) {
+DESALM_DEV double sa_visc_face(const SaT<SW>& S, int dir, int l0, double rei, double rsig, double* gvt = nullptr) {
   const int sj = S.sj, sk = S.sk;
   const double* v = S.q[4];
   int l1;
@@ -126,51 +126,40 @@ DESALM_DEV double sa_visc_face(const SaT<SW>& S, int dir, int l0, double rei, do
   else if (dir == 1) { k1 = b1 * a1 + b2 * a2 + b3 * a3; k2 = b1 * b1 + b2 * b2 + b3 * b3; k3 = b1 * c1 + b2 * c2 + b3 * c3; }
   else { k1 = c1 * a1 + c2 * a2 + c3 * a3; k2 = c1 * b1 + c2 * b2 + c3 * b3; k3 = c1 * c1 + c2 * c2 + c3 * c3; }
   double vtj = 0.25 * ((rei + v[l1]) * rsig + (rei + v[l0]) * rsig) / (S.aj[l1] + S.aj[l0]);
+  // the face's diffusive ADI coefficient ((1/Re + (nu1 + nu0) / 2) / sigma)
+  // |g_dir|^2 / (J1 + J0) with the summed metrics, which is 2 vtj k1
+  if (gvt) *gvt = 2.0 * vtj * k1;
   return vtj * (k1 * vcs + k2 * vet + k3 * vze);
 }
 
 // first-order flux-difference upwind flux of nu_tilde through the face
 // l0 -> l0 + st (src/rhs_sa_flux.F90:32-109)
 template <class SW>
-DESALM_DEV double sa_conv_face(const SaT<SW>& S, int dir, int l0, int st) {
+DESALM_DEV double sa_conv_face(const SaT<SW>& S, int dir, int l0, int st, double* ucf = nullptr) {
   const int l1 = l0 + st;
   const double u1 = S.uc[dir][l1], u0 = S.uc[dir][l0];
+  if (ucf) { ucf[0] = u0; ucf[1] = u1; }
   const double* v = S.q[4];
   double eigh = 0.5 * fabs(u1 + u0);
   return 0.5 * (v[l1] * u1 + v[l0] * u0 - eigh * (v[l1] - v[l0]));
 }
 
 // Tridiagonal row (aw, ap, ae) of the scalar ADI for nu_tilde at interior
-// node l along direction DIR (src/rhs_sa_adi_solver.F90:50-244): first-order
-// upwind convection plus the face diffusivity, scaled by dtev J / 2.  It is
-// evaluated in SW from the nodal values rounded to SW, and stored per node so
-// that the three sweeps read three coefficients instead of rebuilding them
-// from eight state and metric arrays.
-template <class SW, int DIR>
-DESALM_DEV void sa_adi_row(const SaT<SW>& S, int l) {
-  const int st = DIR == 0 ? 1 : (DIR == 1 ? S.sj : S.sk);
-  const double* const* mt = DIR == 0 ? S.csi : (DIR == 1 ? S.eta : S.zet);
-  const SW rsig = SW(1.5), rei = SW(1.0 / S.ren), half_ = SW(0.5);  // rsig = 1 / sigma_SA
-  SW m0[3], m1[3], m2[3], nu[3], aj[3], u[3];
-#pragma unroll
-  for (int t = 0; t < 3; ++t) {
-    const int n = l + (t - 1) * st;
-    m0[t] = SW(mt[0][n]); m1[t] = SW(mt[1][n]); m2[t] = SW(mt[2][n]);
-    nu[t] = SW(S.q[4][n]); aj[t] = SW(S.aj[n]);
-    u[t] = SW(S.uc[DIR][n]);
-  }
-  SW av[2];
-#pragma unroll
-  for (int f = 0; f < 2; ++f) {  // faces (l - st, l) and (l, l + st)
-    const SW gx = m0[f + 1] + m0[f], gy = m1[f + 1] + m1[f], gz = m2[f + 1] + m2[f];
-    const SW ev = (rei + half_ * (nu[f + 1] + nu[f])) * rsig;
-    const SW ucna = half_ * dabs(u[f + 1] + u[f]);
-    av[f] = ucna + ev * (gx * gx + gy * gy + gz * gz) / (aj[f + 1] + aj[f]);
-  }
-  const SW dtj = half_ * SW(S.dtev[l]) * aj[1];
-  S.co[3 * DIR + 0][l] = -dtj * (u[0] + av[0]);
-  S.co[3 * DIR + 1][l] = SW(1) + dtj * (av[0] + av[1]);
-  S.co[3 * DIR + 2][l] = dtj * (u[2] - av[1]);
+// node l along direction d (src/rhs_sa_adi_solver.F90:50-244): first-order
+// upwind convection plus the face diffusivity, scaled by dtev J / 2, stored per
+// node so that the three sweeps read three coefficients.  It is formed from
+// the two faces the residual has just computed: av = |U/J| on the face + the
+// face's diffusive coefficient gm (face (l - s, l)) or gp (face (l, l + s));
+// um, up are the faces' U/J pairs.
+template <class SW>
+DESALM_DEV void sa_adi_row(const SaT<SW>& S, int l, int d, double gm, double gp, const double um[2],
+                           const double up[2]) {
+  const double av0 = 0.5 * fabs(um[1] + um[0]) + gm;
+  const double av1 = 0.5 * fabs(up[1] + up[0]) + gp;
+  const double dtj = 0.5 * S.dtev[l] * S.aj[l];
+  S.co[3 * d + 0][l] = SW(-dtj * (um[0] + av0));
+  S.co[3 * d + 1][l] = SW(1.0 + dtj * (av0 + av1));
+  S.co[3 * d + 2][l] = SW(dtj * (up[1] - av1));
 }
 
 // One fused pass of rhs_sa_grdnu, rhs_sa_prod, rhs_sa_viscous, rhs_sa_flux,
@@ -248,14 +237,15 @@ __global__ void __launch_bounds__(128, DESALM_SA_MINBLOCKS) k_sa_rhs(SaT<SW> S) 
     p = p + cb2 * dnu * rsig;
     psa = p;
   }
-  // viscous terms
-  double visc = sa_visc_face(S, 0, l, rei, rsig) - sa_visc_face(S, 0, l - 1, rei, rsig);
-  visc = visc + sa_visc_face(S, 1, l, rei, rsig) - sa_visc_face(S, 1, l - sj, rei, rsig);
-  visc = visc + sa_visc_face(S, 2, l, rei, rsig) - sa_visc_face(S, 2, l - sk, rei, rsig);
-  // convective flux
-  double rh = sa_conv_face(S, 0, l, 1) - sa_conv_face(S, 0, l - 1, 1);
-  rh = rh + sa_conv_face(S, 1, l, sj) - sa_conv_face(S, 1, l - sj, sj);
-  rh = rh + sa_conv_face(S, 2, l, sk) - sa_conv_face(S, 2, l - sk, sk);
+  // viscous terms and convective flux; each face also gives what the ADI
+  // rows of its direction need (diffusive coefficient, U/J pair)
+  double gdm[3], gdp[3], ucm[3][2], ucp[3][2];
+  double visc = sa_visc_face(S, 0, l, rei, rsig, &gdp[0]) - sa_visc_face(S, 0, l - 1, rei, rsig, &gdm[0]);
+  visc = visc + sa_visc_face(S, 1, l, rei, rsig, &gdp[1]) - sa_visc_face(S, 1, l - sj, rei, rsig, &gdm[1]);
+  visc = visc + sa_visc_face(S, 2, l, rei, rsig, &gdp[2]) - sa_visc_face(S, 2, l - sk, rei, rsig, &gdm[2]);
+  double rh = sa_conv_face(S, 0, l, 1, ucp[0]) - sa_conv_face(S, 0, l - 1, 1, ucm[0]);
+  rh = rh + sa_conv_face(S, 1, l, sj, ucp[1]) - sa_conv_face(S, 1, l - sj, sj, ucm[1]);
+  rh = rh + sa_conv_face(S, 2, l, sk, ucp[2]) - sa_conv_face(S, 2, l - sk, sk, ucm[2]);
   // unsteady term and implicit source scaling
   double rdtj = 1.0 / (2.0 * S.delti * S.aj[l]);
   double dq5dt = S.es * (3.0 * q5[l] - 4.0 * S.qn5[l] + S.qnm1_5[l]) * rdtj;
@@ -263,9 +253,8 @@ __global__ void __launch_bounds__(128, DESALM_SA_MINBLOCKS) k_sa_rhs(SaT<SW> S) 
   S.rh[l] = SW(-S.dtev[l] * S.aj[l] * r);
   // ADI rows of the three directions for this nu_tilde (its values change
   // only at the end of the k sweep)
-  sa_adi_row<SW, 0>(S, l);
-  sa_adi_row<SW, 1>(S, l);
-  sa_adi_row<SW, 2>(S, l);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) sa_adi_row<SW>(S, l, d, gdm[d], gdp[d], ucm[d], ucp[d]);
 }
 
 // Scalar ADI sweep of nu_tilde along one direction
