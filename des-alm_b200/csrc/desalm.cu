@@ -227,6 +227,7 @@ struct desalm_ctx {
   int* flags = nullptr;       // device [2]
   SaWork sa{};
   KwWork kw{};                // k-omega work (turbulence = 2)
+  int recalc = 0;             // decide_recalc_rh of the pseudo-iteration being enqueued
   double ckin = 1.0e-10, cein = 1.0e-6;  // k and omega floors on extrapolated faces
   // per-kernel CUDA-event timing (desalm_profile) and launch counter
   struct ProfRec { int cls, lvl; double nodes; cudaEvent_t a, b; };
@@ -2110,36 +2111,63 @@ namespace {
 // the first one and by the norm kernel of the previous one).
 // The kernels of one pseudo-time iteration up to bcond_fm
 // (src/mg_driver.F90:98-304), enqueued on the context stream; used eagerly
-// and under stream capture.
-int enqueue_iteration(desalm_ctx* ctx) {
+// and under stream capture.  It is split where the reference exchanges
+// overset donor data between blocks (desalm_overset_mg_driver): each
+// fine-level smoothing iteration itr is the turbulence sub-iterations
+// (part 0; mg_bintp_tur follows, src/mg_driver.F90:164-183) and the DAF step
+// with the wall functions (part 1; mg_bintp_mom follows, :237-244); then the
+// coarse levels, the prolongation and bcond_fm.
+int enqueue_fine(desalm_ctx* ctx, int itr, int part) {
   const desalm_case& c = ctx->c;
-  ctx->alm_pending = false;
-  CK(cudaMemsetAsync(ctx->flags, 0, 2 * sizeof(int), ctx->stream));
-  int recalc = 0;
-  for (int n = 0; n < ctx->ng; ++n) {
-    if (n > 0) RET(do_nlevel(ctx, n));
+  const int n = 0;
+  if (part == 0) {
+    if (itr == 1) {
+      ctx->alm_pending = false;
+      CK(cudaMemsetAsync(ctx->flags, 0, 2 * sizeof(int), ctx->stream));
+      ctx->recalc = 0;
+    }
+    // decide_recalc_rh keeps its last value on the coarsest level (Q5)
+    if (n != ctx->ng - 1) ctx->recalc = (itr != c.iter[n]) ? 0 : 1;
+    // the forcing reads the velocities, which the turbulence sub-iterations
+    // leave alone: it runs beside them and joins before k_resid
+    if (ctx->alm.on && c.turbulence && !ctx->prof_on) {
+      RET(fork_side(ctx));
+      Level& G0 = ctx->L[0];
+      RET(kind_of(ctx, 0) == K_DD ? alm_run(ctx, G0.dd, ctx->side) : alm_run(ctx, G0.df, ctx->side));
+      ctx->alm_pending = true;
+    }
+    if (c.turbulence == 1) RET(sa_des_eddy(ctx));
+    if (c.turbulence == 2) RET(kw_eddy_run(ctx));
+    return 0;
+  }
+  // the recalculated residual on the coarsest level feeds nothing
+  const int rc_eff = (n == ctx->ng - 1) ? 0 : ctx->recalc;
+  RET(do_daf(ctx, n, rc_eff, itr));
+  if (c.wall_functions) RET(do_wallfn(ctx));
+  return 0;
+}
+
+int enqueue_coarse(desalm_ctx* ctx) {
+  const desalm_case& c = ctx->c;
+  for (int n = 1; n < ctx->ng; ++n) {
+    RET(do_nlevel(ctx, n));
     for (int itr = 1; itr <= c.iter[n]; ++itr) {
-      // decide_recalc_rh keeps its last value on the coarsest level (Q5)
-      if (n != ctx->ng - 1) recalc = (itr != c.iter[n]) ? 0 : 1;
-      // the forcing reads the velocities, which the SA sub-iterations leave
-      // alone: it runs beside them and joins before k_resid
-      if (n == 0 && ctx->alm.on && c.turbulence && !ctx->prof_on) {
-        RET(fork_side(ctx));
-        Level& G0 = ctx->L[0];
-        RET(kind_of(ctx, 0) == K_DD ? alm_run(ctx, G0.dd, ctx->side) : alm_run(ctx, G0.df, ctx->side));
-        ctx->alm_pending = true;
-      }
-      if (c.turbulence == 1 && n == 0) RET(sa_des_eddy(ctx));
-      if (c.turbulence == 2 && n == 0) RET(kw_eddy_run(ctx));
-      // the recalculated residual on the coarsest level feeds nothing
-      int rc_eff = (n == ctx->ng - 1) ? 0 : recalc;
+      if (n != ctx->ng - 1) ctx->recalc = (itr != c.iter[n]) ? 0 : 1;
+      const int rc_eff = (n == ctx->ng - 1) ? 0 : ctx->recalc;
       RET(do_daf(ctx, n, rc_eff, itr));
-      if (c.wall_functions && n == 0) RET(do_wallfn(ctx));
     }
   }
   for (int n = ctx->ng - 2; n >= 0; --n) RET(do_prolong(ctx, n));
   RET(do_bcond(ctx));
   return 0;
+}
+
+int enqueue_iteration(desalm_ctx* ctx) {
+  for (int itr = 1; itr <= ctx->c.iter[0]; ++itr) {
+    RET(enqueue_fine(ctx, itr, 0));
+    RET(enqueue_fine(ctx, itr, 1));
+  }
+  return enqueue_coarse(ctx);
 }
 
 int pseudo_iter(desalm_ctx* ctx, desalm_step_report* rep) {
@@ -2933,6 +2961,278 @@ int desalm_alm_get(desalm_ctx* ctx, int what, double* out) {
     CK(cudaMemcpyAsync(out, A.falm, 3 * size_t(ctx->L[0].N) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   else { ctx->err = "alm_get: unknown item"; return DESALM_EINVAL; }
   CK(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------ overset blocks
+// Blocks of an overset grid exchange donor data inside the V-cycle: after
+// each fine-level turbulence update the donee nodes of every block receive the
+// turbulence fields trilinearly interpolated from their host cells in other
+// blocks (mg_bintp_tur), and after each fine-level DAF step the momentum
+// fields q(1:4) (mg_bintp_mom, src/mg_bintp_mom.F90:100-122; called at
+// src/mg_driver.F90:237-244).  The reference sends the values with
+// mpi_alltoallv between the ranks of different zones; here every block is a
+// context on the same GPU, and the exchange is a gather of all interpolated
+// values (reads of the host blocks' current fields) followed by a scatter
+// into the donee blocks, on a stream that waits for every block and that
+// every block then waits for.
+namespace {
+
+struct OvEntry {
+  int db, dl;        // donee block, node index (0-based, i fastest)
+  int hb, hl;        // host block, node index of the host cell's lower corner
+  int hsj, hsk;      // the host block's j and k strides
+  double c[3];       // xco, yco, zco
+};
+
+// Trilinear weights and corners in the reference's order (v000, v100, v010,
+// v001, v101, v011, v110, v111; src/mg_bintp_mom.F90:100-122).  Fields
+// f0..f1-1 of the per-block table tab[block * 6 + field] (q(1..5), omega).
+__global__ void k_ov_gather(const OvEntry* E, int n, double* const* tab, int f0, int f1, double* buf) {
+  pdl_wait();
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  const OvEntry& x = E[e];
+  const double xco = x.c[0], yco = x.c[1], zco = x.c[2], one = 1.0;
+  const double c000 = (one - xco) * (one - yco) * (one - zco);
+  const double c100 = xco * (one - yco) * (one - zco);
+  const double c010 = (one - xco) * yco * (one - zco);
+  const double c001 = (one - xco) * (one - yco) * zco;
+  const double c101 = xco * (one - yco) * zco;
+  const double c011 = (one - xco) * yco * zco;
+  const double c110 = xco * yco * (one - zco);
+  const double c111 = xco * yco * zco;
+  const int l = x.hl, sj = x.hsj, sk = x.hsk;
+  for (int f = f0; f < f1; ++f) {
+    const double* v = tab[x.hb * 6 + f];
+    buf[(size_t)e * 6 + f] = v[l] * c000 + v[l + 1] * c100 + v[l + sj] * c010 + v[l + sk] * c001 +
+                             v[l + 1 + sk] * c101 + v[l + sj + sk] * c011 + v[l + 1 + sj] * c110 +
+                             v[l + 1 + sj + sk] * c111;
+  }
+}
+
+__global__ void k_ov_scatter(const OvEntry* E, int n, double* const* tab, int f0, int f1, const double* buf) {
+  pdl_wait();
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  const OvEntry& x = E[e];
+  for (int f = f0; f < f1; ++f) tab[x.db * 6 + f][x.dl] = buf[(size_t)e * 6 + f];
+}
+
+}  // namespace
+
+struct desalm_overset {
+  std::vector<desalm_ctx*> blocks;
+  int n = 0;                       // donee nodes
+  OvEntry* entries = nullptr;      // device
+  double** tab = nullptr;          // device [blocks][6] field pointers of each block's fine level
+  double* buf = nullptr;           // device [n][6]
+  cudaStream_t s = nullptr;
+  cudaEvent_t ev = nullptr;
+  std::vector<cudaEvent_t> bev;    // one per block
+  std::string err;
+};
+
+namespace {
+
+int ov_fail(desalm_overset* ov, const std::string& why, int code) {
+  ov->err = why;
+  return code;
+}
+
+// The exchange of fields f0..f1-1 after every block's queued work.
+int ov_exchange(desalm_overset* ov, int f0, int f1) {
+  if (ov->n == 0) return 0;
+  const int nb = (int)ov->blocks.size();
+  for (int b = 0; b < nb; ++b) {
+    if (cudaEventRecord(ov->bev[b], ov->blocks[b]->stream) != cudaSuccess ||
+        cudaStreamWaitEvent(ov->s, ov->bev[b], 0) != cudaSuccess)
+      return ov_fail(ov, "overset: event", DESALM_ECUDA);
+  }
+  const unsigned g = (unsigned)((ov->n + 127) / 128);
+  if (launch_k(k_ov_gather, g, 128, 0, ov->s, (const OvEntry*)ov->entries, ov->n, (double* const*)ov->tab, f0, f1,
+               ov->buf) != cudaSuccess ||
+      launch_k(k_ov_scatter, g, 128, 0, ov->s, (const OvEntry*)ov->entries, ov->n, (double* const*)ov->tab, f0, f1,
+               (const double*)ov->buf) != cudaSuccess)
+    return ov_fail(ov, "overset: exchange launch", DESALM_ECUDA);
+  if (cudaEventRecord(ov->ev, ov->s) != cudaSuccess) return ov_fail(ov, "overset: event", DESALM_ECUDA);
+  for (int b = 0; b < nb; ++b)
+    if (cudaStreamWaitEvent(ov->blocks[b]->stream, ov->ev, 0) != cudaSuccess)
+      return ov_fail(ov, "overset: event", DESALM_ECUDA);
+  return 0;
+}
+
+int ov_turb_fields(const desalm_ctx* ctx, int& f0, int& f1) {
+  f0 = 4;
+  f1 = ctx->c.turbulence == 2 ? 6 : (ctx->c.turbulence == 1 ? 5 : 4);
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int desalm_overset_create(desalm_ctx* const* ctxs, int nblocks, const desalm_overset_map* map, desalm_overset** out) {
+  if (!ctxs || nblocks < 1 || !map || !out || map->n < 0 || (map->n > 0 && (!map->donee || !map->host || !map->coef)))
+    return DESALM_EINVAL;
+  *out = nullptr;
+  for (int b = 0; b < nblocks; ++b) {
+    if (!ctxs[b]) return DESALM_EINVAL;
+    const desalm_case& a = ctxs[0]->c;
+    const desalm_case& c = ctxs[b]->c;
+    bool same = c.ng == a.ng && c.itmax == a.itmax && c.it_min == a.it_min && c.er_min == a.er_min &&
+                c.eo_min == a.eo_min && c.turbulence == a.turbulence && c.wall_functions == a.wall_functions;
+    for (int n = 0; n < 4; ++n) same = same && c.iter[n] == a.iter[n];
+    if (!same) {
+      ctxs[b]->err = "overset blocks must share ng, iter, itmax, it_min, er_min, eo_min, the turbulence model and "
+                     "the wall-function switch";
+      return DESALM_EINVAL;
+    }
+  }
+  std::vector<OvEntry> E(map->n);
+  for (int e = 0; e < map->n; ++e) {
+    const int* d = map->donee + 4 * e;
+    const int* h = map->host + 4 * e;
+    if (d[0] < 0 || d[0] >= nblocks || h[0] < 0 || h[0] >= nblocks) return DESALM_EINVAL;
+    const Level& D = ctxs[d[0]]->L[0];
+    const Level& H = ctxs[h[0]]->L[0];
+    if (d[1] < 1 || d[1] > D.im || d[2] < 1 || d[2] > D.jm || d[3] < 1 || d[3] > D.km) return DESALM_EINVAL;
+    // the host cell's eight corners lie inside the host block
+    if (h[1] < 1 || h[1] > H.im - 1 || h[2] < 1 || h[2] > H.jm - 1 || h[3] < 1 || h[3] > H.km - 1) return DESALM_EINVAL;
+    OvEntry& x = E[e];
+    x.db = d[0];
+    x.dl = (d[1] - 1) + D.im * ((d[2] - 1) + D.jm * (d[3] - 1));
+    x.hb = h[0];
+    x.hl = (h[1] - 1) + H.im * ((h[2] - 1) + H.jm * (h[3] - 1));
+    x.hsj = H.im;
+    x.hsk = H.im * H.jm;
+    for (int t = 0; t < 3; ++t) x.c[t] = map->coef[3 * e + t];
+  }
+  desalm_overset* ov = new desalm_overset();
+  ov->blocks.assign(ctxs, ctxs + nblocks);
+  ov->n = map->n;
+  std::vector<double*> tab(6L * nblocks, nullptr);
+  for (int b = 0; b < nblocks; ++b) {
+    for (int f = 0; f < 5; ++f) {
+      void* p = nullptr;
+      int esz = 0;
+      if (field_ptr(ctxs[b], 0, DESALM_F_Q + f, &p, &esz) || esz != 8) { delete ov; return DESALM_EINVAL; }
+      tab[6 * b + f] = (double*)p;
+    }
+    tab[6 * b + 5] = ctxs[b]->c.turbulence == 2 ? ctxs[b]->kw.a[0] : nullptr;
+  }
+  bool ok = cudaMalloc((void**)&ov->entries, std::max<size_t>(1, E.size()) * sizeof(OvEntry)) == cudaSuccess &&
+            cudaMalloc((void**)&ov->tab, tab.size() * sizeof(double*)) == cudaSuccess &&
+            cudaMalloc((void**)&ov->buf, std::max<size_t>(1, 6 * E.size()) * sizeof(double)) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&ov->s, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&ov->ev, cudaEventDisableTiming) == cudaSuccess;
+  ov->bev.assign(nblocks, nullptr);
+  for (int b = 0; b < nblocks && ok; ++b) ok = cudaEventCreateWithFlags(&ov->bev[b], cudaEventDisableTiming) == cudaSuccess;
+  if (ok && !E.empty()) ok = cudaMemcpy(ov->entries, E.data(), E.size() * sizeof(OvEntry), cudaMemcpyHostToDevice) == cudaSuccess;
+  if (ok) ok = cudaMemcpy(ov->tab, tab.data(), tab.size() * sizeof(double*), cudaMemcpyHostToDevice) == cudaSuccess;
+  if (!ok) {
+    desalm_overset_destroy(ov);
+    return DESALM_ENOMEM;
+  }
+  *out = ov;
+  return 0;
+}
+
+void desalm_overset_destroy(desalm_overset* ov) {
+  if (!ov) return;
+  if (ov->s) cudaStreamSynchronize(ov->s);
+  cudaFree(ov->entries);
+  cudaFree(ov->tab);
+  cudaFree(ov->buf);
+  for (cudaEvent_t e : ov->bev)
+    if (e) cudaEventDestroy(e);
+  if (ov->ev) cudaEventDestroy(ov->ev);
+  if (ov->s) cudaStreamDestroy(ov->s);
+  delete ov;
+}
+
+const char* desalm_overset_last_error(const desalm_overset* ov) { return ov ? ov->err.c_str() : "null overset"; }
+
+int desalm_overset_exchange(desalm_overset* ov, int what) {
+  if (!ov || (what != 0 && what != 1)) return DESALM_EINVAL;
+  int f0 = 0, f1 = 4;
+  if (what == 1) ov_turb_fields(ov->blocks[0], f0, f1);
+  RET(ov_exchange(ov, f0, f1));
+  for (desalm_ctx* b : ov->blocks)
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess) return ov_fail(ov, "overset: synchronize", DESALM_ECUDA);
+  return 0;
+}
+
+int desalm_overset_mg_driver(desalm_overset* ov, desalm_step_report* reps) {
+  if (!ov) return DESALM_EINVAL;
+  const int nb = (int)ov->blocks.size();
+  desalm_ctx* c0 = ov->blocks[0];
+  const desalm_case& c = c0->c;
+  for (desalm_ctx* b : ov->blocks) {
+    const int rc = desalm_begin_step(b);
+    if (rc) return ov_fail(ov, std::string("overset: begin_step: ") + b->err, rc);
+  }
+  int tf0 = 4, tf1 = 4;
+  ov_turb_fields(c0, tf0, tf1);
+  double init_resd[5] = {0, 0, 0, 0, 0}, res[5] = {0, 0, 0, 0, 0};
+  bool conv = false;
+  int itc = 0, piv = 0;
+  // interior nodes of block 0: the reference divides the sum over every zone
+  // by its root's zone's count (src/mg_residual.F90:31,80)
+  const Level& G0 = c0->L[0];
+  const double tnu0 = double(G0.im - 2) * (G0.jm - 2) * (G0.km - 2);
+  while (!conv && itc < c.itmax) {
+    ++itc;
+    for (desalm_ctx* b : ov->blocks) b->itc = itc;
+    for (int itr = 1; itr <= c.iter[0]; ++itr) {
+      for (desalm_ctx* b : ov->blocks) {
+        const int rc = enqueue_fine(b, itr, 0);
+        if (rc) return ov_fail(ov, std::string("overset: ") + b->err, rc);
+      }
+      if (tf1 > tf0) RET(ov_exchange(ov, tf0, tf1));
+      for (desalm_ctx* b : ov->blocks) {
+        const int rc = enqueue_fine(b, itr, 1);
+        if (rc) return ov_fail(ov, std::string("overset: ") + b->err, rc);
+      }
+      RET(ov_exchange(ov, 0, 4));
+    }
+    double sum[5] = {0, 0, 0, 0, 0};
+    for (desalm_ctx* b : ov->blocks) {  // every block's coarse levels in flight at once
+      const int rc = enqueue_coarse(b);
+      if (rc) return ov_fail(ov, std::string("overset: ") + b->err, rc);
+    }
+    for (int bi = 0; bi < nb; ++bi) {
+      desalm_ctx* b = ov->blocks[bi];
+      double r[5];
+      const int rc = do_norm(b, 0, 1, r);   // also qold_mg <- q for the next iteration
+      if (rc) return ov_fail(ov, std::string("overset: ") + b->err, rc);
+      for (int m = 0; m < 5; ++m) sum[m] += b->h_norm[m];   // the block's sum of |q - qold_mg|
+      int hflags[2] = {0, 0};
+      if (cudaMemcpy(hflags, b->flags, 2 * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return ov_fail(ov, "overset: flags", DESALM_ECUDA);
+      if (hflags[1]) return ov_fail(ov, "overset: zero pivot in a line solve", DESALM_ESINGULAR);
+      piv += hflags[0];
+    }
+    for (int m = 0; m < 5; ++m) res[m] = std::log10(sum[m] / tnu0);
+    if (itc == 1)
+      for (int m = 0; m < 5; ++m) init_resd[m] = res[m];
+    for (int m = 1; m < 4; ++m)
+      if (!std::isfinite(res[m])) return ov_fail(ov, "overset: non-finite convergence norm", DESALM_ENONFINITE);
+    // mg_ck_conver (src/mg_driver.F90:372-398) on the combined norm
+    const double eomax = std::max(res[1], std::max(res[2], res[3]));
+    const double ermax = std::max(res[1] - init_resd[1], std::max(res[2] - init_resd[2], res[3] - init_resd[3]));
+    conv = (itc > c.it_min && ermax < c.er_min) || (itc > c.it_min && eomax < c.eo_min);
+  }
+  if (reps)
+    for (int bi = 0; bi < nb; ++bi) {
+      desalm_step_report& r = reps[bi];
+      r.iterations = itc;
+      r.converged = conv ? 1 : 0;
+      for (int m = 0; m < 5; ++m) { r.residual[m] = res[m]; r.init_residual[m] = init_resd[m]; }
+      r.pivots = piv;
+    }
   return 0;
 }
 

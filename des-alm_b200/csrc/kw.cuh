@@ -133,8 +133,9 @@ DESALM_DEV void kw_visc_face(const KwT<SW>& K, int dir, int l0, double rei, doub
   out[0] = vtj * (k1 * g[0][0] + k2 * g[0][1] + k3 * g[0][2]);
   out[1] = vtj * (k1 * g[1][0] + k2 * g[1][1] + k3 * g[1][2]);
   // the face's diffusive ADI coefficient: (1/Re + (nu_t1 + nu_t0) / 4)
-  // |g_dir|^2 / (J1 + J0) with the summed metrics, which is 2 vtj k1
-  if (gvt) *gvt = 2.0 * vtj * k1;
+  // |g_dir|^2 / (J1 + J0) with the summed metrics, which is 2 vtj times
+  // the direction's own product (k1, k2 or k3)
+  if (gvt) *gvt = 2.0 * vtj * (dir == 0 ? k1 : (dir == 1 ? k2 : k3));
 }
 
 // First-order flux-difference upwind fluxes of k and omega through the

@@ -127,8 +127,9 @@ DESALM_DEV double sa_visc_face(const SaT<SW>& S, int dir, int l0, double rei, do
   else { k1 = c1 * a1 + c2 * a2 + c3 * a3; k2 = c1 * b1 + c2 * b2 + c3 * b3; k3 = c1 * c1 + c2 * c2 + c3 * c3; }
   double vtj = 0.25 * ((rei + v[l1]) * rsig + (rei + v[l0]) * rsig) / (S.aj[l1] + S.aj[l0]);
   // the face's diffusive ADI coefficient ((1/Re + (nu1 + nu0) / 2) / sigma)
-  // |g_dir|^2 / (J1 + J0) with the summed metrics, which is 2 vtj k1
-  if (gvt) *gvt = 2.0 * vtj * k1;
+  // |g_dir|^2 / (J1 + J0) with the summed metrics, which is 2 vtj times the
+  // direction's own product (k1, k2 or k3)
+  if (gvt) *gvt = 2.0 * vtj * (dir == 0 ? k1 : (dir == 1 ? k2 : k3));
   return vtj * (k1 * vcs + k2 * vet + k3 * vze);
 }
 

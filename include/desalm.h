@@ -244,6 +244,48 @@ int  desalm_mg_driver(desalm_ctx* ctx, desalm_step_report* rep);
  * be NULL.  Returns the first error; the steps already in flight are
  * finished first. */
 int  desalm_mg_driver_batch(desalm_ctx* const* ctxs, int n, desalm_step_report* reps);
+/* Overset blocks (the reference's zones of one grid, src/init.F90:1950-2060):
+ * donee nodes of each block take the fields of a host cell in another block
+ * by trilinear interpolation, mg_bintp_mom (q(1:4), src/mg_bintp_mom.F90:
+ * 100-122) after every fine-level DAF step and mg_bintp_tur (the turbulence
+ * fields: nu_tilde, or k and omega) after every fine-level turbulence update
+ * (src/mg_driver.F90:164-183,237-244).  Entry e of the map: donee[4 e] =
+ * block (index into ctxs), i, j, k (1-based) of the node that receives;
+ * host[4 e] = block, i, j, k of the lower corner of the host cell, whose
+ * eight corners are interpolated with the weights (1 - x or x)(1 - y or
+ * y)(1 - z or z), coef[3 e] = x, y, z (xco, yco, zco).  All values are read
+ * before any is written, as the reference gathers them before its
+ * mpi_alltoallv.  A face whose nodes receive donor data is btype 0
+ * (interface): bcond_fm leaves it alone. */
+typedef struct desalm_overset_map {
+  int n;
+  const int* donee;
+  const int* host;
+  const double* coef;
+} desalm_overset_map;
+typedef struct desalm_overset desalm_overset;
+/* The blocks (contexts on the current GPU, with the same ng, iter, itmax,
+ * convergence settings, turbulence model and wall-function switch; their
+ * grids and states set) and their donor map; the map is copied. */
+int  desalm_overset_create(desalm_ctx* const* ctxs, int nblocks, const desalm_overset_map* map,
+                           desalm_overset** out);
+void desalm_overset_destroy(desalm_overset* ov);
+const char* desalm_overset_last_error(const desalm_overset* ov);
+/* One exchange now: what = 0 the momentum fields q(1:4), 1 the turbulence
+ * fields. */
+int  desalm_overset_exchange(desalm_overset* ov, int what);
+/* One physical step of every block in lockstep, as the reference's
+ * mg_driver runs its zones (src/mg_driver.F90:2-323): each block's begin_step,
+ * then pseudo-iterations whose fine-level smoothing steps exchange donor
+ * data as above; each block's kernels run on its own stream, concurrently
+ * with the other blocks' between exchanges.  The convergence test
+ * (mg_ck_conver) uses the sum of |q - qold_mg| over every block's interior
+ * divided by the interior node count of block 0 (the reference sums over
+ * all ranks and divides by its root's zone's count, src/mg_residual.F90:
+ * 31,64-80).  reps (nblocks entries, may be NULL) all get the combined
+ * report.  Blocks step eagerly (no CUDA graph). */
+int  desalm_overset_mg_driver(desalm_overset* ov, desalm_step_report* reps);
+
 /* Lines per CTA of each level's DAF line sweeps, nl[3 * level + direction]
  * (directions i, j, k; 0 for levels the case does not have): 16, 8 or 4, as
  * timed on this GPU when the grid was set (desalm_set_grid tries each width
