@@ -182,3 +182,27 @@ def level_dims(case, n):
         jm = (jm + case.jcrs) // (2 ** case.jcrs)
         km = (km + case.kcrs) // (2 ** case.kcrs)
     return im, jm, km
+
+
+class OversetMap(C.Structure):
+    _fields_ = [
+        ("n", C.c_int),
+        ("donee", C.POINTER(C.c_int)),
+        ("host", C.POINTER(C.c_int)),
+        ("coef", C.POINTER(C.c_double)),
+    ]
+
+
+def make_overset_map(ov):
+    """desalm_overset_map of the dict cases.overset_pair returns; the arrays
+    stay referenced by the returned keep list."""
+    import numpy as _np
+    d = _np.ascontiguousarray(ov["donee"], _np.int32)
+    h = _np.ascontiguousarray(ov["host"], _np.int32)
+    c = _np.ascontiguousarray(ov["coef"], _np.float64)
+    m = OversetMap()
+    m.n = int(ov["n"])
+    m.donee = d.ctypes.data_as(C.POINTER(C.c_int))
+    m.host = h.ctypes.data_as(C.POINTER(C.c_int))
+    m.coef = c.ctypes.data_as(C.POINTER(C.c_double))
+    return m, [d, h, c]

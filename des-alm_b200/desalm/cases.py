@@ -465,6 +465,63 @@ def turbine(im=385, jm=193, km=193, seed=0, re=1.0e5, itmax=400, delti=0.005, ne
     return c, grid, state, spec, omega
 
 
+def _host_cell(a, v):
+    """Lower-corner index (0-based) and fraction of v in the sorted nodes a."""
+    i = int(np.clip(np.searchsorted(a, v, side="right") - 1, 0, len(a) - 2))
+    return i, (v - a[i]) / (a[i + 1] - a[i])
+
+
+def overset_pair(seed=0, turbulence=1, itmax=20, re=1000.0):
+    """Two overlapping wake boxes along x with trilinear donor maps: block 0
+    spans x in [0, 2] (inflow at i = 1, an interface face at i = im), block 1
+    x in [1.5, 3.5] (an interface face at i = 1, the characteristics outlet at
+    i = im); both span y, z in [0, 2] but with different node counts, so the
+    host cells of the interface nodes are interpolated in all three
+    directions.  Each interface node (every j, k of the interface face) takes
+    its values from the host cell of the other block that contains it.
+    Returns ([(case, grid, state)] for the two blocks, map) with the map as
+    desalm_overset_map arrays (0-based blocks, 1-based nodes)."""
+    rng = np.random.default_rng(seed)
+    dims = [(33, 21, 17), (29, 17, 21)]
+    xr = [(0.0, 2.0), (1.5, 3.5)]
+    blocks, axes = [], []
+    for b, (im, jm, km) in enumerate(dims):
+        c, g, st = wake(im=im, jm=jm, km=km, seed=seed + b, turbulence=turbulence, itmax=itmax, amp=0.0, re=re)
+        c.btype[0] = BC_INFLOW if b == 0 else 0
+        c.btype[1] = 0 if b == 0 else BC_OUTLET
+        gx = 1.03 ** np.arange(im - 1)
+        xs = xr[b][0] + np.concatenate(([0.0], np.cumsum(gx))) * ((xr[b][1] - xr[b][0]) / gx.sum())
+        ys = np.linspace(0.0, 2.0, jm) ** 1.0
+        ys = 2.0 * (0.5 - 0.5 * np.cos(np.pi * np.linspace(0.0, 1.0, jm))) if b == 1 else ys
+        zs = np.linspace(0.0, 2.0, km)
+        X, Y, Z = _mesh(xs, ys, zs)
+        g = dict(x=_flat(X), y=_flat(Y), z=_flat(Z), wd=g.get("wd"))
+        q = st["q"].reshape(-1, 5)
+        q[:, 1] = 1.0 + 0.05 * np.sin(np.pi * X.reshape(-1)) * np.cos(np.pi * Y.reshape(-1) / 2.0)
+        q[:, 2] = 0.02 * rng.normal(size=q.shape[0])
+        st = dict(q=q.reshape(-1).copy(), qn=q.reshape(-1).copy(), qnm1=q.reshape(-1).copy(), nut=st["nut"])
+        blocks.append((c, g, st))
+        axes.append((xs, ys, zs))
+    donee, host, coef = [], [], []
+    for b in range(2):
+        other = 1 - b
+        im, jm, km = dims[b]
+        xs, ys, zs = axes[b]
+        ox, oy, oz = axes[other]
+        i = im if b == 0 else 1
+        for k in range(1, km + 1):
+            for j in range(1, jm + 1):
+                ih, fx = _host_cell(ox, xs[i - 1])
+                jh, fy = _host_cell(oy, ys[j - 1])
+                kh, fz = _host_cell(oz, zs[k - 1])
+                donee.append((b, i, j, k))
+                host.append((other, ih + 1, jh + 1, kh + 1))
+                coef.append((fx, fy, fz))
+    ov = dict(donee=np.array(donee, np.int32).reshape(-1), host=np.array(host, np.int32).reshape(-1),
+              coef=np.array(coef, np.float64).reshape(-1), n=len(donee))
+    return blocks, ov
+
+
 def kw_coef_as(k, w, ren):
     """Wilcox's alpha* = (0.15 + Re_t) / (6 + Re_t), Re_t = Re k / omega
     (src/rhs_kw_coef.F90:47-49)."""

@@ -210,6 +210,53 @@ def mg_driver_batch(solvers):
     return [r.as_dict() for r in reps]
 
 
+class Overset:
+    """Overset blocks (desalm_overset_*): Solvers on one GPU coupled by a
+    donor map (see cases.overset_pair)."""
+
+    def __init__(self, solvers, ov):
+        from .abi import make_overset_map
+        self.L = lib()
+        self.solvers = list(solvers)
+        L = self.L
+        L.desalm_overset_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_void_p, C.POINTER(C.c_void_p)]
+        L.desalm_overset_create.restype = C.c_int
+        L.desalm_overset_destroy.argtypes = [C.c_void_p]
+        L.desalm_overset_destroy.restype = None
+        L.desalm_overset_last_error.argtypes = [C.c_void_p]
+        L.desalm_overset_last_error.restype = C.c_char_p
+        L.desalm_overset_exchange.argtypes = [C.c_void_p, C.c_int]
+        L.desalm_overset_exchange.restype = C.c_int
+        L.desalm_overset_mg_driver.argtypes = [C.c_void_p, C.POINTER(StepReport)]
+        L.desalm_overset_mg_driver.restype = C.c_int
+        arr = (C.c_void_p * len(self.solvers))(*[s.ctx.value for s in self.solvers])
+        m, self._keep = make_overset_map(ov)
+        self.ov = C.c_void_p()
+        rc = L.desalm_overset_create(arr, len(self.solvers), C.cast(C.pointer(m), C.c_void_p), C.byref(self.ov))
+        if rc:
+            raise DesalmError("desalm_overset_create failed (%d)" % rc)
+
+    def _ck(self, rc, what):
+        if rc:
+            raise DesalmError("%s failed (%d): %s" % (what, rc, self.L.desalm_overset_last_error(self.ov).decode()))
+
+    def exchange(self, what):
+        self._ck(self.L.desalm_overset_exchange(self.ov, int(what)), "overset_exchange")
+
+    def mg_driver(self):
+        reps = (StepReport * len(self.solvers))()
+        self._ck(self.L.desalm_overset_mg_driver(self.ov, reps), "overset_mg_driver")
+        return [r.as_dict() for r in reps]
+
+    def close(self):
+        if getattr(self, "ov", None) is not None and self.ov.value:
+            self.L.desalm_overset_destroy(self.ov)
+            self.ov = C.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+
 class Solver:
     """One device context (one block, one GPU) of the pseudo-time iteration."""
 
