@@ -240,7 +240,8 @@ def steps_summary(reps, per):
             "drop_reached": [round(float((np.array(r["residual"]) - np.array(r["init_residual"]))[1:4].max()), 3)
                              for r in reps],
             "s_per_step_each": [round(p, 4) for p in per],
-            "would_swap_rows": int(sum(r["pivots"] for r in reps))}
+            "pivot_rows": int(sum(r["pivots"] for r in reps)),
+            "pivot_line_systems": int(sum(r.get("pivot_lines", 0) for r in reps))}
 
 
 def run_ours(args, rank, world, dist):

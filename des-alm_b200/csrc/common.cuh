@@ -54,7 +54,9 @@ struct Lv {
   W* bi;           // i-face boundary vectors: [2][4][jm*km]
   W* bj;           // j-face: [4][4][im*km]  (rows 2, 3, jm-1, jm-2 after the i sweep)
   W* bk;           // k-face: [4][4][im*jm]
-  int* flags;      // [0] pivot-would-swap count, [1] zero pivot count
+  W* gs;           // line-solve scratch of k_gsweep: 16 arrays gss elements apart
+  int gss;
+  int* flags;      // [0] rows interchanged, [1] zero pivots, [2] line systems solved by the pivoting path
   int oute;        // 1: the characteristics outlet plane i = im is solved
                    // with the interior (fine level, btype(2) = 5)
 };
@@ -89,6 +91,23 @@ constexpr int kSlabThreads = 256;
 DESALM_DEV void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
 
 template <class T> DESALM_DEV T dabs(T x) { return x < T(0) ? -x : x; }
+
+// The line eliminations write every multiply-add as an explicit fused
+// (fmaw: a b + c rounded once) or separate (mulw) operation, so that the
+// kernels that solve the same line systems (the shared-memory slab and the
+// lines-in-lanes variants) round alike: left to the compiler, a b + c is
+// contracted or not depending on the code around it.
+DESALM_DEV float fmaw(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+DESALM_DEV double fmaw(double a, double b, double c) { return __fma_rn(a, b, c); }
+DESALM_DEV float mulw(float a, float b) { return __fmul_rn(a, b); }
+DESALM_DEV double mulw(double a, double b) { return __dmul_rn(a, b); }
+// a b - c d as fma(a, b, -(c d)) with c d rounded first (the middle 2x2
+// block of a two-ended elimination)
+DESALM_DEV float fms2(float a, float b, float c, float d) { return __fmaf_rn(a, b, -__fmul_rn(c, d)); }
+DESALM_DEV double fms2(double a, double b, double c, double d) { return __fma_rn(a, b, -__dmul_rn(c, d)); }
+// a b + c d likewise
+DESALM_DEV float fma2(float a, float b, float c, float d) { return __fmaf_rn(a, b, __fmul_rn(c, d)); }
+DESALM_DEV double fma2(double a, double b, double c, double d) { return __fma_rn(a, b, __dmul_rn(c, d)); }
 
 // Reciprocal used by the line eliminations: in FP32 (the sweeps of MIXED mode,
 // a preconditioner) the hardware approximation __fdividef (2 ulp), in FP64 the

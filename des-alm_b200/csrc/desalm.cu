@@ -58,7 +58,7 @@ namespace {
 
 // Convergence state of the device-side pseudo-time loop.
 struct DevConv {
-  int itc, converged, pivots, nonfinite, zero_pivots, pad_;
+  int itc, converged, pivots, nonfinite, zero_pivots, pivot_lines;
   double res[5], init[5];
 };
 
@@ -84,6 +84,7 @@ __global__ void k_conv(const double* part, int nblk, DevConv* st, const int* fla
   st->itc += 1;
   st->pivots += flags[0];
   st->zero_pivots += flags[1];
+  st->pivot_lines += flags[2];
   if (st->itc == 1)
     for (int m = 0; m < 5; ++m) st->init[m] = res[m];
   double eomax = fmax(res[1], fmax(res[2], res[3]));
@@ -198,8 +199,13 @@ struct desalm_ctx {
   double* rat = nullptr;
   int ratdim = 0;
   // lines per CTA of each level's DAF sweeps [level][direction], picked by
-  // timing when the grid is set (autotune_sweeps); 0: the shared-memory rule
+  // timing when the grid is set (autotune_sweeps): 16, 8 or 4 for the
+  // shared-memory slab kernel, 1 for the lines-in-lanes kernel; 0: the
+  // default (lines in lanes)
   int sweep_nl[4][3] = {};
+  // the turbulence sweeps' kernel per direction: 1 lines in lanes, 16/8 the
+  // slab's lines per CTA; 0: the default (lines in lanes)
+  int sa_nl[3] = {};
   // CTA tile (i, j, k threads) of each level's residual kernels [level][0 =
   // K_R first pass, 1 = recalculation, 2 = turbulence residual], picked by
   // timing when the grid is set (autotune_tiles); the build's default shape
@@ -224,7 +230,12 @@ struct desalm_ctx {
     double* falm = nullptr;           // [3][N] force added to rh(2:4) on the fine level
     std::vector<void*> allocs;        // this forcing's device tables
   } alm;                      // actuator-line forcing (rhs_lines)
-  int* flags = nullptr;       // device [2]
+  int* flags = nullptr;       // device [3]
+  // scratch of the lines-in-lanes sweeps (k_gsweep, k_sa_gsweep): 16 arrays
+  // of the fine level's node count in the sweep precision, shared by every
+  // level and sweep (they run one after another on the stream)
+  void* gsweep = nullptr;
+  int gss = 0;
   SaWork sa{};
   KwWork kw{};                // k-omega work (turbulence = 2)
   int recalc = 0;             // decide_recalc_rh of the pseudo-iteration being enqueued
@@ -342,6 +353,8 @@ int alloc_level(desalm_ctx* ctx, Level& G, Lv<T, W>& L) {
   RET(dalloc(ctx, G.allocs, (void**)&L.bj, sizeof(W) * 16L * G.im * G.km));
   RET(dalloc(ctx, G.allocs, (void**)&L.bk, sizeof(W) * 16L * G.im * G.jm));
   L.flags = ctx->flags;
+  L.gs = (W*)ctx->gsweep;
+  L.gss = ctx->gss;
   return 0;
 }
 
@@ -516,9 +529,30 @@ cudaError_t slab_attrs() {
 // one.  Every line is solved by the same operations whatever the width, so
 // the choice changes the time only.
 template <class T, class W, int DIR>
+int gsweep(desalm_ctx* ctx, Lv<T, W>& L, const Par& P, int lvl, int blo, int bhi, bool xform) {
+  int amax, nb;
+  if (DIR == 0) { amax = L.jm - 2; nb = L.km - 2; }
+  else if (DIR == 1) { amax = L.im - 2 + L.oute; nb = L.km - 2; }
+  else { amax = L.im - 2 + L.oute; nb = L.jm - 2; }
+  const int n = DIR == 0 ? L.im - 2 : (DIR == 1 ? L.jm - 2 : L.km - 2);
+  const int cls = DIR == 0 ? KC_SWEEP_I : (DIR == 1 ? KC_SWEEP_J : KC_SWEEP_K);
+  const double nin = double(amax) * n * nb;
+  cudaStream_t s = ctx->stream;
+  LAUNCH(cls, lvl, nin, launch_k(k_gsweep<T, W, DIR>, dim3(cdiv(amax, 32), nb), 256, 0, s, L, P, blo, bhi));
+  CKL();
+  if (!xform) return 0;
+  const int xcls = DIR == 0 ? KC_XFORM_I : (DIR == 1 ? KC_XFORM_J : KC_XFORM_K);
+  const dim3 gx(cdiv(L.im - 2 + L.oute, 32), cdiv(L.jm - 2, 4), L.km - 2);
+  LAUNCH(xcls, lvl, nin, launch_k(k_xform<T, W, DIR>, gx, blk3(), 0, s, L));
+  CKL();
+  return 0;
+}
+
+template <class T, class W, int DIR>
 int launch_sweep(desalm_ctx* ctx, Lv<T, W>& L, const Par& P, int lvl, int blo, int bhi, bool xform = true) {
   const int n = DIR == 0 ? L.im - 2 : (DIR == 1 ? L.jm - 2 : L.km - 2);
   const int want = lvl < 4 ? ctx->sweep_nl[lvl][DIR] : 0;
+  if (want == 0 || want == 1) return gsweep<T, W, DIR>(ctx, L, P, lvl, blo, bhi, xform);
   if (want == 16 && slab_bytes<W>(n, 16) <= kSlabMax) return sweep4_nl<T, W, DIR, 16>(ctx, L, P, lvl, blo, bhi, xform);
   if (want == 8 && slab_bytes<W>(n, 8) <= kSlabMax) return sweep4_nl<T, W, DIR, 8>(ctx, L, P, lvl, blo, bhi, xform);
   if (want == 4 && slab_bytes<W>(n, 4) <= kSlabMax) return sweep4_nl<T, W, DIR, 4>(ctx, L, P, lvl, blo, bhi, xform);
@@ -778,9 +812,9 @@ int tune_sweep(desalm_ctx* ctx, Lv<T, W>& L, int lvl, cudaEvent_t e0, cudaEvent_
   const int n = DIR == 0 ? L.im - 2 : (DIR == 1 ? L.jm - 2 : L.km - 2);
   float best = 0.f;
   int pick = 0;
-  for (int nl : {16, 8, 4}) {
+  for (int nl : {1, 16, 8, 4}) {
     const size_t bytes = slab_bytes<W>(n, nl);
-    if (bytes > kSlabMax) continue;
+    if (nl != 1 && bytes > kSlabMax) continue;
     ctx->sweep_nl[lvl][DIR] = nl;
     RET((launch_sweep<T, W, DIR>(ctx, L, P, lvl, 0, 0, false)));
     CK(cudaEventRecord(e0, ctx->stream));
@@ -856,7 +890,10 @@ int tune_tiles_level(desalm_ctx* ctx, Lv<T, W>& L, int lvl, cudaEvent_t e0, cuda
 // Picks the sweep widths and the residual kernels' tiles of every level,
 // unless DESALM_AUTOTUNE=0 in the environment (then the shared-memory rule
 // and the build's default tile decide).
+int tune_sa_fine(desalm_ctx* ctx, cudaEvent_t e0, cudaEvent_t e1);
+
 int autotune_sweeps(desalm_ctx* ctx) {
+  for (int d = 0; d < 3; ++d) ctx->sa_nl[d] = 0;
   for (int n = 0; n < 4; ++n)
     for (int d = 0; d < 3; ++d) {
       ctx->sweep_nl[n][d] = 0;
@@ -880,6 +917,7 @@ int autotune_sweeps(desalm_ctx* ctx) {
     rc = kind_of(ctx, n) == K_DD ? tune_level(ctx, G.dd, n, e0, e1) : tune_level(ctx, G.df, n, e0, e1);
     if (!rc) rc = kind_of(ctx, n) == K_DD ? tune_tiles_level(ctx, G.dd, n, e0, e1) : tune_tiles_level(ctx, G.df, n, e0, e1);
   }
+  if (!rc) rc = tune_sa_fine(ctx, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return rc;
@@ -1482,8 +1520,15 @@ int desalm_init(const desalm_case* c, desalm_ctx** out) {
     ctx->L[n].jm = (ctx->L[n - 1].jm + c->jcrs) >> c->jcrs;
     ctx->L[n].km = (ctx->L[n - 1].km + c->kcrs) >> c->kcrs;
   }
-  rc = dalloc(ctx, ctx->allocs, (void**)&ctx->flags, 2 * sizeof(int));
+  rc = dalloc(ctx, ctx->allocs, (void**)&ctx->flags, 3 * sizeof(int));
   if (rc) { *out = ctx; return rc; }
+  {
+    const long NF = (long)c->im * c->jm * c->km;
+    const size_t wb = c->precision_mode == DESALM_FP64 ? 8 : 4;
+    ctx->gss = (int)NF;
+    rc = dalloc(ctx, ctx->allocs, &ctx->gsweep, 16 * (size_t)NF * wb);
+    if (rc) { *out = ctx; return rc; }
+  }
   for (int n = 0; n < ctx->ng; ++n) {
     Level& G = ctx->L[n];
     G.N = (long)G.im * G.jm * G.km;
@@ -2088,6 +2133,46 @@ int desalm_sweep_widths(desalm_ctx* ctx, int nl[12]) {
   return 0;
 }
 
+int desalm_turb_sweep_widths(desalm_ctx* ctx, int nl[3]) {
+  if (!ctx || !nl) return DESALM_EINVAL;
+  for (int d = 0; d < 3; ++d) nl[d] = ctx->sa_nl[d];
+  return 0;
+}
+
+int desalm_set_sweep_widths(desalm_ctx* ctx, const int nl[12], const int turb[3]) {
+  if (!ctx) return DESALM_EINVAL;
+  const size_t wb = ctx->c.precision_mode == DESALM_FP64 ? 8 : 4;
+  if (nl) {
+    for (int n = 0; n < 4; ++n)
+      for (int d = 0; d < 3; ++d) {
+        const int v = nl[3 * n + d];
+        if (n >= ctx->ng) {
+          if (v) { ctx->err = "sweep width given for a level the case does not have"; return DESALM_EINVAL; }
+          continue;
+        }
+        const Level& G = ctx->L[n];
+        const int len = d == 0 ? G.im - 2 : (d == 1 ? G.jm - 2 : G.km - 2);
+        const bool ok = v == 0 || v == 1 || ((v == 4 || v == 8 || v == 16) && (size_t)10 * slab_fs(len + 2, v + 1) * wb <= kSlabMax);
+        if (!ok) { ctx->err = "DAF sweep width must be 0, 1, or 4, 8, 16 with a slab that fits"; return DESALM_EINVAL; }
+      }
+  }
+  if (turb) {
+    for (int d = 0; d < 3; ++d) {
+      const int v = turb[d];
+      const int len = d == 0 ? ctx->c.im - 2 : (d == 1 ? ctx->c.jm - 2 : ctx->c.km - 2);
+      const bool ok = v == 0 || v == 1 || ((v == 8 || v == 16 || v == 32) && (size_t)4 * slab_fs(len, v + 1) * wb <= kSlabMax);
+      if (!ok) { ctx->err = "turbulence sweep width must be 0, 1, or 8, 16, 32 with a slab that fits"; return DESALM_EINVAL; }
+    }
+  }
+  if (nl)
+    for (int n = 0; n < ctx->ng; ++n)
+      for (int d = 0; d < 3; ++d) ctx->sweep_nl[n][d] = nl[3 * n + d];
+  if (turb)
+    for (int d = 0; d < 3; ++d) ctx->sa_nl[d] = turb[d];
+  drop_graph(ctx);
+  return 0;
+}
+
 int desalm_kernel_tiles(desalm_ctx* ctx, int tiles[36]) {
   if (!ctx || !tiles) return DESALM_EINVAL;
   for (int n = 0; n < 4; ++n)
@@ -2123,7 +2208,7 @@ int enqueue_fine(desalm_ctx* ctx, int itr, int part) {
   if (part == 0) {
     if (itr == 1) {
       ctx->alm_pending = false;
-      CK(cudaMemsetAsync(ctx->flags, 0, 2 * sizeof(int), ctx->stream));
+      CK(cudaMemsetAsync(ctx->flags, 0, 3 * sizeof(int), ctx->stream));
       ctx->recalc = 0;
     }
     // decide_recalc_rh keeps its last value on the coarsest level (Q5)
@@ -2176,8 +2261,8 @@ int pseudo_iter(desalm_ctx* ctx, desalm_step_report* rep) {
   RET(enqueue_iteration(ctx));
   double res[5];
   RET(do_norm(ctx, 0, 1, res));
-  int hflags[2] = {0, 0};
-  CK(cudaMemcpy(hflags, ctx->flags, 2 * sizeof(int), cudaMemcpyDeviceToHost));
+  int hflags[3] = {0, 0, 0};
+  CK(cudaMemcpy(hflags, ctx->flags, 3 * sizeof(int), cudaMemcpyDeviceToHost));
   if (ctx->itc == 1)
     for (int m = 0; m < 5; ++m) ctx->init_resd[m] = res[m];
   // mg_ck_conver (src/mg_driver.F90:372-398)
@@ -2191,6 +2276,7 @@ int pseudo_iter(desalm_ctx* ctx, desalm_step_report* rep) {
     rep->converged = conv ? 1 : 0;
     for (int m = 0; m < 5; ++m) { rep->residual[m] = res[m]; rep->init_residual[m] = ctx->init_resd[m]; }
     rep->pivots = hflags[0];
+    rep->pivot_lines = hflags[2];
   }
   if (hflags[1]) { ctx->err = "zero pivot in a line solve"; return DESALM_ESINGULAR; }
   for (int m = 1; m < 4; ++m)
@@ -2270,6 +2356,8 @@ SaT<SW> make_sa(desalm_ctx* ctx, Lv<double, W>& L) {
   for (int t = 0; t < 9; ++t) S.co[t] = (SW*)ctx->sa.a[2 + t];
   for (int d = 0; d < 3; ++d) S.uc[d] = ctx->sa.a[11 + d];
   S.flags = ctx->flags;
+  S.gs = (SW*)ctx->gsweep;
+  S.gss = ctx->gss;
   S.ren = ctx->c.ren; S.delti = ctx->c.delti; S.es = ctx->c.unsteady ? 1.0 : 0.0;
   for (int b = 0; b < 6; ++b) { S.sa1[b] = ctx->par.sa[0][b]; S.sb1[b] = ctx->par.sb[0][b]; S.btype[b] = ctx->c.btype[b]; }
   S.rat = (const double*)ctx->rat;
@@ -2291,11 +2379,65 @@ int sa_sweep_nl(desalm_ctx* ctx, SaT<SW>& S, int amax, int n, int nb, double nin
 }
 template <class SW, int DIR>
 int sa_sweep(desalm_ctx* ctx, SaT<SW>& S, int amax, int n, int nb, double nin) {
+  const int want = ctx->sa_nl[DIR];
+  if (want == 0 || want == 1) {
+    LAUNCH(KC_SA_SWEEP, 0, nin, launch_k(k_sa_gsweep<SW, DIR>, dim3(cdiv(amax, 64), nb), 128, 0, ctx->stream, S));
+    CKL();
+    return 0;
+  }
+  if (want == 32 && sa_slab_bytes<SW>(n, 32) <= kSlabMax) return sa_sweep_nl<SW, DIR, 32>(ctx, S, amax, n, nb, nin);
+  if (want == 16 && sa_slab_bytes<SW>(n, 16) <= kSlabMax) return sa_sweep_nl<SW, DIR, 16>(ctx, S, amax, n, nb, nin);
+  if (want == 8 && sa_slab_bytes<SW>(n, 8) <= kSlabMax) return sa_sweep_nl<SW, DIR, 8>(ctx, S, amax, n, nb, nin);
   if (sa_slab_bytes<SW>(n, 32) <= kSlabTwoPerSm) return sa_sweep_nl<SW, DIR, 32>(ctx, S, amax, n, nb, nin);
   if (sa_slab_bytes<SW>(n, 16) <= kSlabTwoPerSm) return sa_sweep_nl<SW, DIR, 16>(ctx, S, amax, n, nb, nin);
   if (sa_slab_bytes<SW>(n, 8) <= kSlabMax) return sa_sweep_nl<SW, DIR, 8>(ctx, S, amax, n, nb, nin);
   ctx->err = "grid line too long for the shared-memory SA sweep";
   return DESALM_EINVAL;
+}
+
+// The turbulence line sweep of one direction timed with the lines-in-lanes
+// kernel and with each slab width that fits (one warm-up launch, five timed
+// with CUDA events); the fastest is kept.  The sweeps of i and j write only
+// the model's right-hand-side work array, which the residual rewrites before
+// any use, so timing them changes no result.
+template <class W, int DIR>
+int tune_sa_dir(desalm_ctx* ctx, SaT<W>& S, cudaEvent_t e0, cudaEvent_t e1) {
+  const int amax = DIR == 0 ? S.jm - 2 : S.im - 2;
+  const int n = DIR == 0 ? S.im - 2 : (DIR == 1 ? S.jm - 2 : S.km - 2);
+  const int nb = DIR == 2 ? S.jm - 2 : S.km - 2;
+  const double nin = double(amax) * n * nb;
+  float best = 0.f;
+  int pick = 0;
+  for (int nl : {1, 32, 16, 8}) {
+    if (nl != 1 && sa_slab_bytes<W>(n, nl) > kSlabMax) continue;
+    ctx->sa_nl[DIR] = nl;
+    RET((sa_sweep<W, DIR>(ctx, S, amax, n, nb, nin)));
+    CK(cudaEventRecord(e0, ctx->stream));
+    for (int r = 0; r < 5; ++r) RET((sa_sweep<W, DIR>(ctx, S, amax, n, nb, nin)));
+    CK(cudaEventRecord(e1, ctx->stream));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    if (!pick || ms < best) { best = ms; pick = nl; }
+  }
+  ctx->sa_nl[DIR] = pick;
+  return 0;
+}
+
+// The i and j turbulence sweeps are timed; the k sweep, which also updates
+// the model's scalar, takes the j sweep's choice (both read their rows
+// coalesced across the lanes, with a stride along the line).
+template <class W>
+int tune_sa(desalm_ctx* ctx, Lv<double, W>& L, cudaEvent_t e0, cudaEvent_t e1) {
+  SaT<W> S = make_sa<W>(ctx, L);
+  RET((tune_sa_dir<W, 0>(ctx, S, e0, e1)));
+  RET((tune_sa_dir<W, 1>(ctx, S, e0, e1)));
+  ctx->sa_nl[2] = ctx->sa_nl[1];
+  return 0;
+}
+int tune_sa_fine(desalm_ctx* ctx, cudaEvent_t e0, cudaEvent_t e1) {
+  if (!ctx->c.turbulence) return 0;
+  return kind_of(ctx, 0) == K_DD ? tune_sa(ctx, ctx->L[0].dd, e0, e1) : tune_sa(ctx, ctx->L[0].df, e0, e1);
 }
 
 template <class W>
@@ -2474,13 +2616,15 @@ int build_graph(desalm_ctx* ctx) {
 int run_step(desalm_ctx* ctx, desalm_step_report* rep) {
   if (ctx->c.use_graph && !ctx->prof_on) return graph_step(ctx, rep);
   desalm_step_report r{};
-  int piv = 0;
+  int piv = 0, plines = 0;
   for (int it = 1; it <= ctx->c.itmax; ++it) {
     RET(pseudo_iter(ctx, &r));
     piv += r.pivots;
+    plines += r.pivot_lines;
     if (r.converged) break;
   }
   r.pivots = piv;
+  r.pivot_lines = plines;
   if (rep) *rep = r;
   return 0;
 }
@@ -2509,6 +2653,7 @@ int graph_finish(desalm_ctx* ctx, desalm_step_report* rep) {
     rep->converged = st.converged;
     for (int m = 0; m < 5; ++m) { rep->residual[m] = st.res[m]; rep->init_residual[m] = st.init[m]; }
     rep->pivots = st.pivots;
+    rep->pivot_lines = st.pivot_lines;
   }
   if (st.zero_pivots) { ctx->err = "zero pivot in a line solve"; return DESALM_ESINGULAR; }
   if (st.nonfinite) { ctx->err = "non-finite convergence norm"; return DESALM_ENONFINITE; }
@@ -3178,7 +3323,7 @@ int desalm_overset_mg_driver(desalm_overset* ov, desalm_step_report* reps) {
   ov_turb_fields(c0, tf0, tf1);
   double init_resd[5] = {0, 0, 0, 0, 0}, res[5] = {0, 0, 0, 0, 0};
   bool conv = false;
-  int itc = 0, piv = 0;
+  int itc = 0, piv = 0, plines = 0;
   // interior nodes of block 0: the reference divides the sum over every zone
   // by its root's zone's count (src/mg_residual.F90:31,80)
   const Level& G0 = c0->L[0];
@@ -3209,11 +3354,12 @@ int desalm_overset_mg_driver(desalm_overset* ov, desalm_step_report* reps) {
       const int rc = do_norm(b, 0, 1, r);   // also qold_mg <- q for the next iteration
       if (rc) return ov_fail(ov, std::string("overset: ") + b->err, rc);
       for (int m = 0; m < 5; ++m) sum[m] += b->h_norm[m];   // the block's sum of |q - qold_mg|
-      int hflags[2] = {0, 0};
-      if (cudaMemcpy(hflags, b->flags, 2 * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+      int hflags[3] = {0, 0, 0};
+      if (cudaMemcpy(hflags, b->flags, 3 * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
         return ov_fail(ov, "overset: flags", DESALM_ECUDA);
       if (hflags[1]) return ov_fail(ov, "overset: zero pivot in a line solve", DESALM_ESINGULAR);
       piv += hflags[0];
+      plines += hflags[2];
     }
     for (int m = 0; m < 5; ++m) res[m] = std::log10(sum[m] / tnu0);
     if (itc == 1)
@@ -3232,6 +3378,7 @@ int desalm_overset_mg_driver(desalm_overset* ov, desalm_step_report* reps) {
       r.converged = conv ? 1 : 0;
       for (int m = 0; m < 5; ++m) { r.residual[m] = res[m]; r.init_residual[m] = init_resd[m]; }
       r.pivots = piv;
+      r.pivot_lines = plines;
     }
   return 0;
 }

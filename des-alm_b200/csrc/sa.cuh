@@ -37,6 +37,8 @@ struct SaT {
   SW* co[9];        // co[3 d + 0..2] = aw, ap, ae of the direction-d line through each interior node
   double* uc[3];  // contravariant U/J of each direction on every node, for the current velocities
   double* upd;    // the scalar the last (k) sweep updates: nu_tilde (q[4]) for SA; k or omega for k-omega
+  SW* gs;         // line-solve scratch of k_sa_gsweep: 4 arrays gss elements apart
+  int gss;
   int* flags;
   double ren, delti, es;
   double sa1[6], sb1[6];  // pressure-row extrapolation coefficients, sa(1,b), sb(1,b)
@@ -341,9 +343,9 @@ __global__ void __launch_bounds__(kSlabThreads) k_sa_sweep4(SaT<SW> S) {
           if (p == 0) { d = bap[u]; bprev = brr[u]; }
           else {
             ndom += dabs(apc) < dabs(aec2) + dabs(baw[u]);
-            const SW f = baw[u] * rdprev;
-            d = bap[u] - f * duprev;
-            bprev = brr[u] - f * bprev;
+            const SW f = mulw(baw[u], rdprev);
+            d = fmaw(-f, duprev, bap[u]);
+            bprev = fmaw(-f, bprev, brr[u]);
           }
           aec2 = duprev; apc = bap[u];
           rdprev = sweep_rcp(d);
@@ -368,9 +370,9 @@ __global__ void __launch_bounds__(kSlabThreads) k_sa_sweep4(SaT<SW> S) {
           if (p == n - 1) { d = bap[u]; bprev = brr[u]; }
           else {
             ndom += dabs(apc) < dabs(bae[u]) + dabs(aec2);
-            const SW f = bae[u] * rdprev;
-            d = bap[u] - f * awprev;
-            bprev = brr[u] - f * bprev;
+            const SW f = mulw(bae[u], rdprev);
+            d = fmaw(-f, awprev, bap[u]);
+            bprev = fmaw(-f, bprev, brr[u]);
           }
           aec2 = awprev; apc = bap[u];
           rdprev = sweep_rcp(d);
@@ -385,14 +387,14 @@ __global__ void __launch_bounds__(kSlabThreads) k_sa_sweep4(SaT<SW> S) {
   if (act) {
     const SW d1 = m_d[li], u1 = m_c[li], b1 = m_b[li];
     const SW d2 = n_d[li], l2 = n_c[li], b2 = n_b[li];
-    const SW det = d1 * d2 - u1 * l2;
+    const SW det = fms2(d1, d2, u1, l2);
     // the middle columns h - 1 (needs the bottom half's aw_h, l2) and h
     // (needs the top half's ae_{h-1}, u1)
     if (half == 0) ndom += dabs(apc) < dabs(aec2) + dabs(l2);
     else ndom += dabs(apc) < dabs(u1) + dabs(aec2);
     if (ndom) atomicAdd(&s_ndom[li], ndom);
     if (half == 0) {
-      SW x = (b1 * d2 - u1 * b2) / det;
+      SW x = fms2(b1, d2, u1, b2) / det;
       s_rh[at(h - 1)] = x;
       for (int p0 = h - 2; p0 >= 0; p0 -= R) {
         SW bae[R], brr[R], brd[R];
@@ -401,10 +403,10 @@ __global__ void __launch_bounds__(kSlabThreads) k_sa_sweep4(SaT<SW> S) {
           if (p0 - u >= 0) { bae[u] = s_ae[at(p0 - u)]; brr[u] = s_rh[at(p0 - u)]; brd[u] = s_ap[at(p0 - u)]; }
 #pragma unroll
         for (int u = 0; u < R; ++u)
-          if (p0 - u >= 0) { x = (brr[u] - bae[u] * x) * brd[u]; s_rh[at(p0 - u)] = x; }
+          if (p0 - u >= 0) { x = mulw(fmaw(-bae[u], x, brr[u]), brd[u]); s_rh[at(p0 - u)] = x; }
       }
     } else {
-      SW x = (d1 * b2 - l2 * b1) / det;
+      SW x = fms2(d1, b2, l2, b1) / det;
       s_rh[at(h)] = x;
       for (int p0 = h + 1; p0 < n; p0 += R) {
         SW baw[R], brr[R], brd[R];
@@ -413,7 +415,7 @@ __global__ void __launch_bounds__(kSlabThreads) k_sa_sweep4(SaT<SW> S) {
           if (p0 + u < n) { baw[u] = s_aw[at(p0 + u)]; brr[u] = s_rh[at(p0 + u)]; brd[u] = s_ap[at(p0 + u)]; }
 #pragma unroll
         for (int u = 0; u < R; ++u)
-          if (p0 + u < n) { x = (brr[u] - baw[u] * x) * brd[u]; s_rh[at(p0 + u)] = x; }
+          if (p0 + u < n) { x = mulw(fmaw(-baw[u], x, brr[u]), brd[u]); s_rh[at(p0 + u)] = x; }
       }
     }
   }
@@ -424,7 +426,8 @@ __global__ void __launch_bounds__(kSlabThreads) k_sa_sweep4(SaT<SW> S) {
   // (src/sgtsv.f:107-162, 232-257), one thread per line, in the line's own
   // columns: ap and the right-hand side are reloaded, aw (dl, with the
   // fill-in of a swap) and ae (du) are modified in place.  Interchanges are
-  // counted in flags[0], zero pivots in flags[1].
+  // counted in flags[0], zero pivots in flags[1], the lines solved this way
+  // in flags[2].
   if (tid < nl && s_ndom[tid]) {
     const int lf = tid;
     auto fat = [&](int p) { return p * NLP + lf; };
@@ -440,8 +443,8 @@ __global__ void __launch_bounds__(kSlabThreads) k_sa_sweep4(SaT<SW> S) {
       if (dabs(s_ap[fat(i)]) >= dabs(dli)) {
         if (s_ap[fat(i)] != SW(0)) {
           const SW fact = dli / s_ap[fat(i)];
-          s_ap[fat(i + 1)] = s_ap[fat(i + 1)] - fact * s_ae[fat(i)];
-          s_rh[fat(i + 1)] = s_rh[fat(i + 1)] - fact * s_rh[fat(i)];
+          s_ap[fat(i + 1)] = fmaw(-fact, s_ae[fat(i)], s_ap[fat(i + 1)]);
+          s_rh[fat(i + 1)] = fmaw(-fact, s_rh[fat(i)], s_rh[fat(i + 1)]);
         } else {
           sing = true;
         }
@@ -451,7 +454,7 @@ __global__ void __launch_bounds__(kSlabThreads) k_sa_sweep4(SaT<SW> S) {
         const SW fact = s_ap[fat(i)] / dli;
         s_ap[fat(i)] = dli;
         const SW temp = s_ap[fat(i + 1)];
-        s_ap[fat(i + 1)] = s_ae[fat(i)] - fact * temp;
+        s_ap[fat(i + 1)] = fmaw(-fact, temp, s_ae[fat(i)]);
         if (i <= n - 3) {
           s_aw[fat(i + 1)] = s_ae[fat(i + 1)];        // du2(i), the fill-in
           s_ae[fat(i + 1)] = -fact * s_aw[fat(i + 1)];
@@ -459,18 +462,19 @@ __global__ void __launch_bounds__(kSlabThreads) k_sa_sweep4(SaT<SW> S) {
         s_ae[fat(i)] = temp;
         const SW tb = s_rh[fat(i)];
         s_rh[fat(i)] = s_rh[fat(i + 1)];
-        s_rh[fat(i + 1)] = tb - fact * s_rh[fat(i + 1)];
+        s_rh[fat(i + 1)] = fmaw(-fact, s_rh[fat(i + 1)], tb);
       }
     }
     if (sing || s_ap[fat(n - 1)] == SW(0)) {
       atomicAdd(&S.flags[1], 1);
     } else {
       s_rh[fat(n - 1)] = s_rh[fat(n - 1)] / s_ap[fat(n - 1)];
-      if (n > 1) s_rh[fat(n - 2)] = (s_rh[fat(n - 2)] - s_ae[fat(n - 2)] * s_rh[fat(n - 1)]) / s_ap[fat(n - 2)];
+      if (n > 1) s_rh[fat(n - 2)] = fmaw(-s_ae[fat(n - 2)], s_rh[fat(n - 1)], s_rh[fat(n - 2)]) / s_ap[fat(n - 2)];
       for (int i = n - 3; i >= 0; --i)
-        s_rh[fat(i)] = (s_rh[fat(i)] - s_ae[fat(i)] * s_rh[fat(i + 1)] - s_aw[fat(i + 1)] * s_rh[fat(i + 2)]) / s_ap[fat(i)];
+        s_rh[fat(i)] = fmaw(-s_aw[fat(i + 1)], s_rh[fat(i + 2)], fmaw(-s_ae[fat(i)], s_rh[fat(i + 1)], s_rh[fat(i)])) / s_ap[fat(i)];
     }
     if (nsw) atomicAdd(&S.flags[0], nsw);
+    atomicAdd(&S.flags[2], 1);
   }
   __syncthreads();
 
@@ -509,6 +513,231 @@ __global__ void __launch_bounds__(kSlabThreads) k_sa_sweep4(SaT<SW> S) {
       }
     }
   }
+}
+
+// The same scalar ADI sweep with the lines in the lanes: a warp owns 32
+// neighbouring lines of one plane and one half of each, a CTA 2 x 32 lines
+// (four warps).  The rows are read from global memory as the elimination
+// proceeds (rows of the j and k sweeps are coalesced across the lanes; the
+// i sweep's through L1 sectors), and the eliminated row of each node
+// (1/d, b') goes to a scratch laid out [row][line], coalesced across the
+// lanes, from which the back-substitution reads it.  No slab is staged, so
+// occupancy is set by registers alone and every line runs at once instead of
+// a few per SM.  The elimination is k_sa_sweep4's: the same operations in
+// the same order (two-ended, no interchange where every column is
+// diagonally dominant, SGTSV's pivoting elimination otherwise), so the two
+// kernels give the same values.
+// Scratch (S.gs, arrays S.gss apart): 1/d, b', and for the pivoting
+// elimination du and dl.
+template <class SW, int DIR>
+__global__ void __launch_bounds__(128) k_sa_gsweep(SaT<SW> S) {
+  pdl_wait();
+  constexpr int LG = 2;                       // line groups of 32 per CTA
+  constexpr int R = sizeof(SW) == 4 ? 8 : 4;  // rows loaded one block ahead of the elimination
+  __shared__ SW m_d[LG][32], m_c[LG][32], m_b[LG][32], n_d[LG][32], n_c[LG][32], n_b[LG][32];
+  __shared__ int s_ndom[LG][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int g = w >> 1, half = w & 1;
+  const int b = blockIdx.y + 1;
+  int amax, n, st, sa, base;
+  if (DIR == 0) { amax = S.jm - 2; n = S.im - 2; st = 1; sa = S.sj; base = S.sk * b; }
+  else if (DIR == 1) { amax = S.im - 2; n = S.jm - 2; st = S.sj; sa = 1; base = S.sk * b; }
+  else { amax = S.im - 2; n = S.km - 2; st = S.sk; sa = 1; base = S.sj * b; }
+  const int a = blockIdx.x * (32 * LG) + g * 32 + lane + 1;
+  const bool act = a <= amax;
+  const int nln = amax * (int)gridDim.y;            // lines of the sweep
+  const int line = (a - 1) + amax * (b - 1);
+  const int l0 = base + a * sa + st;                 // node of row 0
+  const SW* __restrict__ caw = S.co[3 * DIR + 0];
+  const SW* __restrict__ cap = S.co[3 * DIR + 1];
+  const SW* __restrict__ cae = S.co[3 * DIR + 2];
+  SW* __restrict__ gd = S.gs;
+  SW* __restrict__ gb = S.gs + S.gss;
+  auto sc = [&](int p) { return p * nln + line; };
+  if (half == 0) s_ndom[g][lane] = 0;
+  const int h = n / 2;
+  int ndom = 0;
+  SW apc = 0, aec2 = 0;
+  if (act && half == 0) {
+    SW dprev = 0, rdprev = 0, duprev = 0, bprev = 0;
+    SW caw_[R], cap_[R], cae_[R], crr_[R];
+#pragma unroll
+    for (int u = 0; u < R; ++u)
+      if (u < h) { const int l = l0 + u * st; caw_[u] = __ldg(caw + l); cap_[u] = __ldg(cap + l); cae_[u] = __ldg(cae + l); crr_[u] = S.rh[l]; }
+    for (int p0 = 0; p0 < h; p0 += R) {
+      SW naw[R], nap[R], nae[R], nrr[R];
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        naw[u] = nap[u] = nae[u] = nrr[u] = SW(0);
+        if (p0 + R + u < h) { const int l = l0 + (p0 + R + u) * st; naw[u] = __ldg(caw + l); nap[u] = __ldg(cap + l); nae[u] = __ldg(cae + l); nrr[u] = S.rh[l]; }
+      }
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int p = p0 + u;
+        if (p < h) {
+          SW d;
+          if (p == 0) { d = cap_[u]; bprev = crr_[u]; }
+          else {
+            ndom += dabs(apc) < dabs(aec2) + dabs(caw_[u]);
+            const SW f = mulw(caw_[u], rdprev);
+            d = fmaw(-f, duprev, cap_[u]);
+            bprev = fmaw(-f, bprev, crr_[u]);
+          }
+          aec2 = duprev; apc = cap_[u];
+          rdprev = sweep_rcp(d);
+          gd[sc(p)] = rdprev; gb[sc(p)] = bprev;
+          dprev = d; duprev = cae_[u];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < R; ++u) { caw_[u] = naw[u]; cap_[u] = nap[u]; cae_[u] = nae[u]; crr_[u] = nrr[u]; }
+    }
+    m_d[g][lane] = dprev; m_c[g][lane] = duprev; m_b[g][lane] = bprev;
+  } else if (act && half == 1) {
+    SW dprev = 0, rdprev = 0, awprev = 0, bprev = 0;
+    SW caw_[R], cap_[R], cae_[R], crr_[R];
+#pragma unroll
+    for (int u = 0; u < R; ++u)
+      if (n - 1 - u >= h) { const int l = l0 + (n - 1 - u) * st; caw_[u] = __ldg(caw + l); cap_[u] = __ldg(cap + l); cae_[u] = __ldg(cae + l); crr_[u] = S.rh[l]; }
+    for (int p0 = n - 1; p0 >= h; p0 -= R) {
+      SW naw[R], nap[R], nae[R], nrr[R];
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        naw[u] = nap[u] = nae[u] = nrr[u] = SW(0);
+        if (p0 - R - u >= h) { const int l = l0 + (p0 - R - u) * st; naw[u] = __ldg(caw + l); nap[u] = __ldg(cap + l); nae[u] = __ldg(cae + l); nrr[u] = S.rh[l]; }
+      }
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int p = p0 - u;
+        if (p >= h) {
+          SW d;
+          if (p == n - 1) { d = cap_[u]; bprev = crr_[u]; }
+          else {
+            ndom += dabs(apc) < dabs(cae_[u]) + dabs(aec2);
+            const SW f = mulw(cae_[u], rdprev);
+            d = fmaw(-f, awprev, cap_[u]);
+            bprev = fmaw(-f, bprev, crr_[u]);
+          }
+          aec2 = awprev; apc = cap_[u];
+          rdprev = sweep_rcp(d);
+          gd[sc(p)] = rdprev; gb[sc(p)] = bprev;
+          dprev = d; awprev = caw_[u];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < R; ++u) { caw_[u] = naw[u]; cap_[u] = nap[u]; cae_[u] = nae[u]; crr_[u] = nrr[u]; }
+    }
+    n_d[g][lane] = dprev; n_c[g][lane] = awprev; n_b[g][lane] = bprev;
+  }
+  __syncthreads();
+  SW d1 = 0, u1 = 0, b1 = 0, d2 = 0, l2 = 0, b2 = 0, det = 0;
+  if (act) {
+    d1 = m_d[g][lane]; u1 = m_c[g][lane]; b1 = m_b[g][lane];
+    d2 = n_d[g][lane]; l2 = n_c[g][lane]; b2 = n_b[g][lane];
+    det = fms2(d1, d2, u1, l2);
+    if (half == 0) ndom += dabs(apc) < dabs(aec2) + dabs(l2);
+    else ndom += dabs(apc) < dabs(u1) + dabs(aec2);
+    if (ndom) atomicAdd(&s_ndom[g][lane], ndom);
+  }
+  __syncthreads();
+  if (!act) return;
+  const double dmul = 1.5 * S.es;
+  // the solution of row p: into rh, or after the k sweep into the update
+  // nu <- nu + (-nu + (nu_old + dnu)) / (1 + 1.5 dtev / dt)
+  auto put = [&](int p, SW x) {
+    const int l = l0 + p * st;
+    if (DIR < 2) {
+      S.rh[l] = x;
+    } else {
+      const double nt = S.upd[l];
+      const double qe5 = nt + double(x);
+      const double dum = 1.0 + dmul * __ldg(S.dtev + l) / S.delti;
+      S.upd[l] = nt + (-nt + qe5) / dum;
+    }
+  };
+  if (!s_ndom[g][lane]) {
+    if (half == 0) {
+      SW x = fms2(b1, d2, u1, b2) / det;
+      put(h - 1, x);
+      for (int p0 = h - 2; p0 >= 0; p0 -= R) {
+        SW bae[R], brr[R], brd[R];
+#pragma unroll
+        for (int u = 0; u < R; ++u)
+          if (p0 - u >= 0) { bae[u] = __ldg(cae + l0 + (p0 - u) * st); brr[u] = gb[sc(p0 - u)]; brd[u] = gd[sc(p0 - u)]; }
+#pragma unroll
+        for (int u = 0; u < R; ++u)
+          if (p0 - u >= 0) { x = mulw(fmaw(-bae[u], x, brr[u]), brd[u]); put(p0 - u, x); }
+      }
+    } else {
+      SW x = fms2(d1, b2, l2, b1) / det;
+      put(h, x);
+      for (int p0 = h + 1; p0 < n; p0 += R) {
+        SW baw[R], brr[R], brd[R];
+#pragma unroll
+        for (int u = 0; u < R; ++u)
+          if (p0 + u < n) { baw[u] = __ldg(caw + l0 + (p0 + u) * st); brr[u] = gb[sc(p0 + u)]; brd[u] = gd[sc(p0 + u)]; }
+#pragma unroll
+        for (int u = 0; u < R; ++u)
+          if (p0 + u < n) { x = mulw(fmaw(-baw[u], x, brr[u]), brd[u]); put(p0 + u, x); }
+      }
+    }
+    return;
+  }
+  if (half != 0) return;
+  // ---- a line with a column that is not dominant: SGTSV's elimination with
+  // partial pivoting (src/sgtsv.f:107-162, 232-257) from the original rows,
+  // in the line's scratch: d (gd), b (gb), du (gu) and dl (gl, with the
+  // fill-in of a swap)
+  SW* __restrict__ gu = S.gs + 2 * (size_t)S.gss;
+  SW* __restrict__ gl = S.gs + 3 * (size_t)S.gss;
+  for (int p = 0; p < n; ++p) {
+    const int l = l0 + p * st;
+    gd[sc(p)] = cap[l];
+    gb[sc(p)] = S.rh[l];
+    gu[sc(p)] = cae[l];
+    gl[sc(p)] = caw[l];
+  }
+  int nsw = 0;
+  bool sing = false;
+  for (int i = 0; i <= n - 2 && !sing; ++i) {
+    const SW dli = gl[sc(i + 1)];
+    const SW di = gd[sc(i)];
+    if (dabs(di) >= dabs(dli)) {
+      if (di != SW(0)) {
+        const SW fact = dli / di;
+        gd[sc(i + 1)] = fmaw(-fact, gu[sc(i)], gd[sc(i + 1)]);
+        gb[sc(i + 1)] = fmaw(-fact, gb[sc(i)], gb[sc(i + 1)]);
+      } else {
+        sing = true;
+      }
+      gl[sc(i + 1)] = SW(0);
+    } else {
+      ++nsw;
+      const SW fact = di / dli;
+      gd[sc(i)] = dli;
+      const SW temp = gd[sc(i + 1)];
+      gd[sc(i + 1)] = fmaw(-fact, temp, gu[sc(i)]);
+      if (i <= n - 3) {
+        gl[sc(i + 1)] = gu[sc(i + 1)];               // du2(i), the fill-in
+        gu[sc(i + 1)] = -fact * gl[sc(i + 1)];
+      }
+      gu[sc(i)] = temp;
+      const SW tb = gb[sc(i)];
+      gb[sc(i)] = gb[sc(i + 1)];
+      gb[sc(i + 1)] = fmaw(-fact, gb[sc(i + 1)], tb);
+    }
+  }
+  if (sing || gd[sc(n - 1)] == SW(0)) {
+    atomicAdd(&S.flags[1], 1);
+  } else {
+    gb[sc(n - 1)] = gb[sc(n - 1)] / gd[sc(n - 1)];
+    if (n > 1) gb[sc(n - 2)] = fmaw(-gu[sc(n - 2)], gb[sc(n - 1)], gb[sc(n - 2)]) / gd[sc(n - 2)];
+    for (int i = n - 3; i >= 0; --i)
+      gb[sc(i)] = fmaw(-gl[sc(i + 1)], gb[sc(i + 2)], fmaw(-gu[sc(i)], gb[sc(i + 1)], gb[sc(i)])) / gd[sc(i)];
+    for (int p = 0; p < n; ++p) put(p, gb[sc(p)]);
+  }
+  if (nsw) atomicAdd(&S.flags[0], nsw);
+  atomicAdd(&S.flags[2], 1);
 }
 
 // boundary values of nu_tilde (src/rhs_sa_bcond.F90:40-269): one kernel per

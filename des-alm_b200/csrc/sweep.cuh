@@ -24,7 +24,7 @@ template <class T, class W, int KIND>
 DESALM_DEV void face_vec(const Lv<T, W>& L, const Par& P, int lb, int b, const W* r1, const W* r2, int stride, T out[4]) {
   T v[4];
 #pragma unroll
-  for (int m = 0; m < 4; ++m) v[m] = T(P.sa[m][b]) * T(r1[m * stride]) + T(P.sb[m][b]) * T(r2[m * stride]);
+  for (int m = 0; m < 4; ++m) v[m] = fma2(T(P.sa[m][b]), T(r1[m * stride]), T(P.sb[m][b]), T(r2[m * stride]));
   M4<T> A;
   if (KIND == 0) mat_mai(L, P, lb, A);
   else if (KIND == 1) mat_n1i(L, P, lb, A);
@@ -176,15 +176,15 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
         if (p <= h) {
           W aw, ae;
           coef(bt[u], hw, bh[u], aw, ae);
-          const W ap = W(1) + W(2) * bt[u];
+          const W ap = fmaw(W(2), bt[u], W(1));
           W rr = br[u];
           W d;
-          if (p == 1) { rr = rr - aw * bwm; d = ap; bprev = rr; }
+          if (p == 1) { rr = fmaw(-aw, bwm, rr); d = ap; bprev = rr; }
           else {
             ndom += dabs(apc) < dabs(aec2) + dabs(aw);   // column p - 1
-            const W f = aw * rdprev;
-            d = ap - f * duprev;
-            bprev = rr - f * bprev;
+            const W f = mulw(aw, rdprev);
+            d = fmaw(-f, duprev, ap);
+            bprev = fmaw(-f, bprev, rr);
           }
           aec2 = duprev; apc = ap;
           nzero += d == W(0);
@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
       // the outlet row (src/rhs_diag_solver.F90:207-221): ap = 1, 1,
       // 1 + dtau dc spr, 1 and aw = 0, 0, -dtau(im-1) dc spr(im-1), 0;
       // dtau dc spr = 2 h exactly
-      const W d = m == 2 ? W(1) + W(2) * he : W(1);
+      const W d = m == 2 ? fmaw(W(2), he, W(1)) : W(1);
       nzero += d == W(0);
       rdprev = sweep_rcp(d);
       sd[at(n + 1)] = rdprev;
@@ -225,15 +225,15 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
         if (p > h) {
           W aw, ae;
           coef(bt[u], bh[u], he, aw, ae);
-          const W ap = W(1) + W(2) * bt[u];
+          const W ap = fmaw(W(2), bt[u], W(1));
           W rr = br[u];
           W d;
-          if (p == n && !ext) { rr = rr - ae * bem; d = ap; bprev = rr; }
+          if (p == n && !ext) { rr = fmaw(-ae, bem, rr); d = ap; bprev = rr; }
           else {
             ndom += dabs(apc) < dabs(ae) + dabs(aec2);   // column p + 1
-            const W f = ae * rdprev;
-            d = ap - f * awprev;
-            bprev = rr - f * bprev;
+            const W f = mulw(ae, rdprev);
+            d = fmaw(-f, awprev, ap);
+            bprev = fmaw(-f, bprev, rr);
           }
           aec2 = awprev; apc = ap;
           nzero += d == W(0);
@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
     // the two middle rows: d1 x1 + u1 x2 = b1 (row h-1), l2 x1 + d2 x2 = b2 (row h)
     const W d1 = mt_d[li][m], u1 = mt_u[li][m], b1 = mt_b[li][m];
     const W d2 = mb_d[li][m], l2 = mb_l[li][m], b2 = mb_b[li][m];
-    const W det = d1 * d2 - u1 * l2;
+    const W det = fms2(d1, d2, u1, l2);
     nzero += half == 0 && det == W(0);
     // the two middle columns: column h needs the bottom half's aw_{h+1}
     // (l2), column h+1 the top half's ae_h (u1)
@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
     if (ndom) atomicAdd(&s_ndom[li][m], ndom);
     if (nzero) atomicAdd(&s_nz[li][m], nzero);
     if (half == 0) {
-      W x = (b1 * d2 - u1 * b2) / det;
+      W x = fms2(b1, d2, u1, b2) / det;
       r[at(h)] = x;
       for (int p0 = h - 1; p0 >= 1; p0 -= R) {
         W bt[R], bh[R], br[R], bd[R];
@@ -273,13 +273,13 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
           if (p0 - u >= 1) {
             W aw, ae;
             coef(bt[u], W(0), bh[u], aw, ae);
-            x = (br[u] - ae * x) * bd[u];
+            x = mulw(fmaw(-ae, x, br[u]), bd[u]);
             r[at(p0 - u)] = x;
           }
         }
       }
     } else {
-      W x = (d1 * b2 - l2 * b1) / det;
+      W x = fms2(d1, b2, l2, b1) / det;
       r[at(h + 1)] = x;
       for (int p0 = h + 2; p0 <= n; p0 += R) {
         W bt[R], bh[R], br[R], bd[R];
@@ -291,14 +291,14 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
           if (p0 + u <= n) {
             W aw, ae;
             coef(bt[u], bh[u], W(0), aw, ae);
-            x = (br[u] - aw * x) * bd[u];
+            x = mulw(fmaw(-aw, x, br[u]), bd[u]);
             r[at(p0 + u)] = x;
           }
         }
       }
       if (ext) {
         const W aw = m == 2 ? -(W(2) * chc[at(n)]) : W(0);
-        x = (r[at(n + 1)] - aw * x) * sd[at(n + 1)];
+        x = mulw(fmaw(-aw, x, r[at(n + 1)]), sd[at(n + 1)]);
         r[at(n + 1)] = x;
       }
     }
@@ -311,12 +311,13 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
   // its systems in turn.  The 1/d columns of the line are free now; three
   // of them hold d, du and dl (dl keeps the fill-in of a swap, as SGTSV
   // does).  Rows that interchange are counted in flags[0], zero pivots
-  // (SGTSV's INFO > 0) in flags[1].
+  // (SGTSV's INFO > 0) in flags[1], the systems solved this way in flags[2].
   if (tid < nl) {
     const int lf = tid;
-    int nsw = 0, nz = 0;
+    int nsw = 0, nz = 0, npl = 0;
     for (int q = 0; q < 4; ++q) {
       if (!s_ndom[lf][q]) { nz += s_nz[lf][q]; continue; }
+      ++npl;
       const int N = n + ext;                       // rows 1..N
       W* bq = s_r + q * fs;
       W* dd = s_d;                                 // d
@@ -333,15 +334,15 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
           if (q < 2) { aw = -t; ae = -t; }
           else if (q == 2) { aw = -dw - t; ae = de - t; }
           else { aw = dw - t; ae = -de - t; }
-          ap = W(1) + W(2) * t;
+          ap = fmaw(W(2), t, W(1));
         } else {  // the outlet row
-          ap = q == 2 ? W(1) + W(2) * s_hc[fat(n + 1)] : W(1);
+          ap = q == 2 ? fmaw(W(2), s_hc[fat(n + 1)], W(1)) : W(1);
           aw = q == 2 ? -(W(2) * s_hc[fat(n)]) : W(0);
           ae = W(0);
         }
         W b = L.wk[q][l0 + p * st];
-        if (p == 1) b = b - aw * sbw[lf][q];
-        if (p == n && !ext) b = b - ae * sbe[lf][q];
+        if (p == 1) b = fmaw(-aw, sbw[lf][q], b);
+        if (p == n && !ext) b = fmaw(-ae, sbe[lf][q], b);
         bq[fat(p)] = b;
         dd[fat(p)] = ap;
         du[fat(p)] = ae;                           // row p's super-diagonal
@@ -354,8 +355,8 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
         if (dabs(dd[fat(p)]) >= dabs(dlp)) {
           if (dd[fat(p)] != W(0)) {
             const W fact = dlp / dd[fat(p)];
-            dd[fat(p + 1)] = dd[fat(p + 1)] - fact * du[fat(p)];
-            bq[fat(p + 1)] = bq[fat(p + 1)] - fact * bq[fat(p)];
+            dd[fat(p + 1)] = fmaw(-fact, du[fat(p)], dd[fat(p + 1)]);
+            bq[fat(p + 1)] = fmaw(-fact, bq[fat(p)], bq[fat(p + 1)]);
           } else {
             sing = true;
           }
@@ -365,7 +366,7 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
           const W fact = dd[fat(p)] / dlp;
           dd[fat(p)] = dlp;
           const W temp = dd[fat(p + 1)];
-          dd[fat(p + 1)] = du[fat(p)] - fact * temp;
+          dd[fat(p + 1)] = fmaw(-fact, temp, du[fat(p)]);
           if (p <= N - 2) {
             dl[fat(p + 1)] = du[fat(p + 1)];                 // fill-in of row p: du2
             du[fat(p + 1)] = -fact * dl[fat(p + 1)];
@@ -375,19 +376,20 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
           du[fat(p)] = temp;
           const W tb = bq[fat(p)];
           bq[fat(p)] = bq[fat(p + 1)];
-          bq[fat(p + 1)] = tb - fact * bq[fat(p + 1)];
+          bq[fat(p + 1)] = fmaw(-fact, bq[fat(p + 1)], tb);
         }
       }
       if (sing || dd[fat(N)] == W(0)) { ++nz; continue; }
       // back-substitution: x_p = (b_p - du_p x_{p+1} - du2_p x_{p+2}) / d_p,
       // du2_p held in dl[p + 1]
       bq[fat(N)] = bq[fat(N)] / dd[fat(N)];
-      if (N > 1) bq[fat(N - 1)] = (bq[fat(N - 1)] - du[fat(N - 1)] * bq[fat(N)]) / dd[fat(N - 1)];
+      if (N > 1) bq[fat(N - 1)] = fmaw(-du[fat(N - 1)], bq[fat(N)], bq[fat(N - 1)]) / dd[fat(N - 1)];
       for (int p = N - 2; p >= 1; --p)
-        bq[fat(p)] = (bq[fat(p)] - du[fat(p)] * bq[fat(p + 1)] - dl[fat(p + 1)] * bq[fat(p + 2)]) / dd[fat(p)];
+        bq[fat(p)] = fmaw(-dl[fat(p + 1)], bq[fat(p + 2)], fmaw(-du[fat(p)], bq[fat(p + 1)], bq[fat(p)])) / dd[fat(p)];
     }
     if (nsw) atomicAdd(&L.flags[0], nsw);
     if (nz) atomicAdd(&L.flags[1], nz);
+    if (npl) atomicAdd(&L.flags[2], npl);
   }
   __syncthreads();
 
@@ -404,6 +406,320 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
 #pragma unroll
     for (int q = 0; q < 4; ++q) L.wk[q][l] = s_r[q * fs + so];
   }
+}
+
+// ---------------------------------------------------------------------------
+// The DAF line sweep with the lines in the lanes.  A CTA owns 32 neighbouring
+// lines of one plane (the lanes) and eight warps: warp w solves system
+// m = w & 3 of the top (w < 4) or bottom half of every line.  The rows are
+// read from global memory one block ahead of the elimination (coalesced
+// across the lanes for the j and k sweeps; the i sweep's rows come through L1
+// sectors, which the four systems of a half share), and each eliminated row
+// (1/d and b') goes to a scratch laid out [row][line], coalesced across the
+// lanes, for the back-substitution, which writes the solution straight into
+// wk.  Without a staged slab the occupancy is set by registers, and every
+// line of a level is in flight at once.  The operations and their order are
+// k_sweep4's (two-ended elimination, SGTSV's no-interchange branch where
+// every column is diagonally dominant, its pivoting elimination otherwise),
+// so both kernels give the same values.  Systems 0 and 1 share the matrix
+// (aw = ae = -tc), so system 1 reads system 0's 1/d instead of storing its
+// own.
+// Scratch (L.gs, arrays L.gss elements apart): per system m the arrays
+// 4m + 0..3 = 1/d (d in the pivoting elimination), b', du and dl.
+// ---------------------------------------------------------------------------
+template <class T, class W, int DIR>
+__global__ void __launch_bounds__(256, 3) k_gsweep(Lv<T, W> L, Par P, int blo, int bhi) {
+  pdl_wait();
+  constexpr int R = sizeof(W) == 4 ? 8 : 4;  // rows loaded one block ahead
+  __shared__ W mt_d[4][32], mt_u[4][32], mt_b[4][32];
+  __shared__ W mb_d[4][32], mb_l[4][32], mb_b[4][32];
+  __shared__ int s_ndom[4][32], s_nz[4][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int m = w & 3, half = w >> 2;
+  const int b = blockIdx.y + 1;
+  int amax, n, st, sa;
+  if (DIR == 0) { amax = L.jm - 2; n = L.im - 2; st = 1; sa = L.sj; }
+  else if (DIR == 1) { amax = L.im - 2 + L.oute; n = L.jm - 2; st = L.sj; sa = 1; }
+  else { amax = L.im - 2 + L.oute; n = L.km - 2; st = L.sk; sa = 1; }
+  const int ext = DIR == 0 ? L.oute : 0;
+  const int base = (DIR == 2) ? L.sj * b : L.sk * b;
+  const int a = blockIdx.x * 32 + lane + 1;
+  const bool act = a <= amax;
+  const int nln = amax * (int)gridDim.y;
+  const int line = (a - 1) + amax * (b - 1);
+  const int lb = base + a * sa;                // node 0 of the line
+  const W* __restrict__ tc = L.tc[DIR];
+  const W* __restrict__ hc = L.hc[DIR];
+  W* __restrict__ r = L.wk[m];
+  W* __restrict__ gd = L.gs + (size_t)(4 * m) * L.gss;
+  W* __restrict__ gb = L.gs + (size_t)(4 * m + 1) * L.gss;
+  const W* __restrict__ gdr = L.gs + (size_t)(4 * (m == 1 ? 0 : m)) * L.gss;  // the 1/d column read back
+  auto sc = [&](int p) { return (p - 1) * nln + line; };   // row p = node p of the line, 1..n + ext
+  auto coef = [&](W t, W hw_, W he_, W& aw, W& ae) {
+    const W dw = t != W(0) ? hw_ : W(0);
+    const W de = t != W(0) ? he_ : W(0);
+    if (m < 2) { aw = -t; ae = -t; }
+    else if (m == 2) { aw = -dw - t; ae = de - t; }
+    else { aw = dw - t; ae = -de - t; }
+  };
+  // semi-explicit boundary rows of the line (component m)
+  auto bvec = [&](int hi) -> W {
+    T v[4] = {0, 0, 0, 0};
+    if (DIR == 0) {
+      if (!hi && blo) {
+        const int S = L.jm * L.km, o = a + L.jm * b;
+        face_vec<T, W, 0>(L, P, lb, 0, L.bi + o, L.bi + 4 * S + o, S, v);
+      }
+    } else if (DIR == 1) {
+      const int S = L.im * L.km, o = a + L.im * b;
+      if (!hi && blo) face_vec<T, W, 1>(L, P, lb, 2, L.bj + o, L.bj + 4 * S + o, S, v);
+      if (hi && bhi) face_vec<T, W, 1>(L, P, lb + (n + 1) * st, 3, L.bj + 8 * S + o, L.bj + 12 * S + o, S, v);
+    } else {
+      const int S = L.im * L.jm, o = a + L.im * b;
+      if (!hi && blo) face_vec<T, W, 2>(L, P, lb, 4, L.bk + o, L.bk + 4 * S + o, S, v);
+      if (hi && bhi) face_vec<T, W, 2>(L, P, lb + (n + 1) * st, 5, L.bk + 8 * S + o, L.bk + 12 * S + o, S, v);
+    }
+    return W(v[m]);
+  };
+  if (half == 0) { s_ndom[m][lane] = 0; s_nz[m][lane] = 0; }
+  const int h = n / 2;  // nodes 1..h top, h+1..n bottom
+  int nzero = 0, ndom = 0;
+  W apc = 0, aec2 = 0;
+  if (act && half == 0) {
+    const W bwm = bvec(0);
+    W hw = hc[lb], hcur = hc[lb + st];
+    W dprev = 0, rdprev = 0, duprev = 0, bprev = 0;
+    W ct[R], ch[R], cr[R];
+#pragma unroll
+    for (int u = 0; u < R; ++u)
+      if (1 + u <= h) { const int l = lb + (1 + u) * st; ct[u] = tc[l]; ch[u] = hc[l + st]; cr[u] = r[l]; }
+    for (int p0 = 1; p0 <= h; p0 += R) {
+      W nt[R], nh[R], nr[R];
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        nt[u] = nh[u] = nr[u] = W(0);
+        if (p0 + R + u <= h) { const int l = lb + (p0 + R + u) * st; nt[u] = tc[l]; nh[u] = hc[l + st]; nr[u] = r[l]; }
+      }
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int p = p0 + u;
+        if (p <= h) {
+          W aw, ae;
+          coef(ct[u], hw, ch[u], aw, ae);
+          const W ap = fmaw(W(2), ct[u], W(1));
+          W rr = cr[u];
+          W d;
+          if (p == 1) { rr = fmaw(-aw, bwm, rr); d = ap; bprev = rr; }
+          else {
+            ndom += dabs(apc) < dabs(aec2) + dabs(aw);
+            const W f = mulw(aw, rdprev);
+            d = fmaw(-f, duprev, ap);
+            bprev = fmaw(-f, bprev, rr);
+          }
+          aec2 = duprev; apc = ap;
+          nzero += d == W(0);
+          rdprev = sweep_rcp(d);
+          if (m != 1) gd[sc(p)] = rdprev;
+          gb[sc(p)] = bprev;
+          dprev = d; duprev = ae;
+          hw = hcur; hcur = ch[u];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < R; ++u) { ct[u] = nt[u]; ch[u] = nh[u]; cr[u] = nr[u]; }
+    }
+    mt_d[m][lane] = dprev; mt_u[m][lane] = duprev; mt_b[m][lane] = bprev;
+  } else if (act && half == 1) {
+    const W bem = bvec(1);
+    W he = hc[lb + (n + 1) * st], hcur = hc[lb + n * st];
+    W dprev = 0, rdprev = 0, awprev = 0, bprev = 0;
+    if (ext) {
+      // the outlet row (src/rhs_diag_solver.F90:207-221)
+      const W d = m == 2 ? fmaw(W(2), he, W(1)) : W(1);
+      nzero += d == W(0);
+      rdprev = sweep_rcp(d);
+      if (m != 1) gd[sc(n + 1)] = rdprev;
+      bprev = r[lb + (n + 1) * st];
+      gb[sc(n + 1)] = bprev;
+      dprev = d;
+      awprev = m == 2 ? -(W(2) * hcur) : W(0);
+      apc = d;
+    }
+    W ct[R], ch[R], cr[R];
+#pragma unroll
+    for (int u = 0; u < R; ++u)
+      if (n - u > h) { const int l = lb + (n - u) * st; ct[u] = tc[l]; ch[u] = hc[l - st]; cr[u] = r[l]; }
+    for (int p0 = n; p0 > h; p0 -= R) {
+      W nt[R], nh[R], nr[R];
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        nt[u] = nh[u] = nr[u] = W(0);
+        if (p0 - R - u > h) { const int l = lb + (p0 - R - u) * st; nt[u] = tc[l]; nh[u] = hc[l - st]; nr[u] = r[l]; }
+      }
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int p = p0 - u;
+        if (p > h) {
+          W aw, ae;
+          coef(ct[u], ch[u], he, aw, ae);
+          const W ap = fmaw(W(2), ct[u], W(1));
+          W rr = cr[u];
+          W d;
+          if (p == n && !ext) { rr = fmaw(-ae, bem, rr); d = ap; bprev = rr; }
+          else {
+            ndom += dabs(apc) < dabs(ae) + dabs(aec2);
+            const W f = mulw(ae, rdprev);
+            d = fmaw(-f, awprev, ap);
+            bprev = fmaw(-f, bprev, rr);
+          }
+          aec2 = awprev; apc = ap;
+          nzero += d == W(0);
+          rdprev = sweep_rcp(d);
+          if (m != 1) gd[sc(p)] = rdprev;
+          gb[sc(p)] = bprev;
+          dprev = d; awprev = aw;
+          he = hcur; hcur = ch[u];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < R; ++u) { ct[u] = nt[u]; ch[u] = nh[u]; cr[u] = nr[u]; }
+    }
+    mb_d[m][lane] = dprev; mb_l[m][lane] = awprev; mb_b[m][lane] = bprev;
+  }
+  __syncthreads();
+  W d1 = 0, u1 = 0, b1 = 0, d2 = 0, l2 = 0, b2 = 0, det = 0;
+  if (act) {
+    d1 = mt_d[m][lane]; u1 = mt_u[m][lane]; b1 = mt_b[m][lane];
+    d2 = mb_d[m][lane]; l2 = mb_l[m][lane]; b2 = mb_b[m][lane];
+    det = fms2(d1, d2, u1, l2);
+    nzero += half == 0 && det == W(0);
+    if (half == 0) ndom += dabs(apc) < dabs(aec2) + dabs(l2);
+    else ndom += dabs(apc) < dabs(u1) + dabs(aec2);
+    if (ndom) atomicAdd(&s_ndom[m][lane], ndom);
+    if (nzero) atomicAdd(&s_nz[m][lane], nzero);
+  }
+  __syncthreads();
+  if (!act) return;
+  if (!s_ndom[m][lane]) {
+    if (half == 0) {
+      const int nz = s_nz[m][lane];
+      if (nz) atomicAdd(&L.flags[1], nz);
+      W x = fms2(b1, d2, u1, b2) / det;
+      r[lb + h * st] = x;
+      for (int p0 = h - 1; p0 >= 1; p0 -= R) {
+        W bt[R], bh[R], br[R], bd[R];
+#pragma unroll
+        for (int u = 0; u < R; ++u)
+          if (p0 - u >= 1) { const int l = lb + (p0 - u) * st; bt[u] = tc[l]; bh[u] = hc[l + st]; br[u] = gb[sc(p0 - u)]; bd[u] = gdr[sc(p0 - u)]; }
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+          if (p0 - u >= 1) {
+            W aw, ae;
+            coef(bt[u], W(0), bh[u], aw, ae);
+            x = mulw(fmaw(-ae, x, br[u]), bd[u]);
+            r[lb + (p0 - u) * st] = x;
+          }
+        }
+      }
+    } else {
+      W x = fms2(d1, b2, l2, b1) / det;
+      r[lb + (h + 1) * st] = x;
+      for (int p0 = h + 2; p0 <= n; p0 += R) {
+        W bt[R], bh[R], br[R], bd[R];
+#pragma unroll
+        for (int u = 0; u < R; ++u)
+          if (p0 + u <= n) { const int l = lb + (p0 + u) * st; bt[u] = tc[l]; bh[u] = hc[l - st]; br[u] = gb[sc(p0 + u)]; bd[u] = gdr[sc(p0 + u)]; }
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+          if (p0 + u <= n) {
+            W aw, ae;
+            coef(bt[u], bh[u], W(0), aw, ae);
+            x = mulw(fmaw(-aw, x, br[u]), bd[u]);
+            r[lb + (p0 + u) * st] = x;
+          }
+        }
+      }
+      if (ext) {
+        const W aw = m == 2 ? -(W(2) * hc[lb + n * st]) : W(0);
+        x = mulw(fmaw(-aw, x, gb[sc(n + 1)]), gdr[sc(n + 1)]);
+        r[lb + (n + 1) * st] = x;
+      }
+    }
+    return;
+  }
+  if (half != 0) return;
+  // ---- a system with a column that is not dominant: SGTSV's elimination
+  // with partial pivoting (src/sgtsv.f:107-162, back-substitution :232-257)
+  // from the original rows, in the system's scratch: d, b, du and dl (dl
+  // keeps the fill-in of a swap, as SGTSV does)
+  W* __restrict__ dd = gd;
+  W* __restrict__ bq = gb;
+  W* __restrict__ du = L.gs + (size_t)(4 * m + 2) * L.gss;
+  W* __restrict__ dl = L.gs + (size_t)(4 * m + 3) * L.gss;
+  const int N = n + ext;
+  const W bwm = bvec(0), bem = bvec(1);
+  for (int p = 1; p <= N; ++p) {
+    W aw, ae, ap;
+    if (p <= n) {
+      const W t = tc[lb + p * st];
+      coef(t, hc[lb + (p - 1) * st], hc[lb + (p + 1) * st], aw, ae);
+      ap = fmaw(W(2), t, W(1));
+    } else {  // the outlet row
+      ap = m == 2 ? fmaw(W(2), hc[lb + (n + 1) * st], W(1)) : W(1);
+      aw = m == 2 ? -(W(2) * hc[lb + n * st]) : W(0);
+      ae = W(0);
+    }
+    W bv = r[lb + p * st];
+    if (p == 1) bv = fmaw(-aw, bwm, bv);
+    if (p == n && !ext) bv = fmaw(-ae, bem, bv);
+    bq[sc(p)] = bv;
+    dd[sc(p)] = ap;
+    du[sc(p)] = ae;
+    dl[sc(p)] = p > 1 ? aw : W(0);
+  }
+  int nsw = 0;
+  bool sing = false;
+  for (int p = 1; p <= N - 1 && !sing; ++p) {
+    const W dlp = dl[sc(p + 1)];
+    const W dp = dd[sc(p)];
+    if (dabs(dp) >= dabs(dlp)) {
+      if (dp != W(0)) {
+        const W fact = dlp / dp;
+        dd[sc(p + 1)] = fmaw(-fact, du[sc(p)], dd[sc(p + 1)]);
+        bq[sc(p + 1)] = fmaw(-fact, bq[sc(p)], bq[sc(p + 1)]);
+      } else {
+        sing = true;
+      }
+      dl[sc(p + 1)] = W(0);
+    } else {
+      ++nsw;
+      const W fact = dp / dlp;
+      dd[sc(p)] = dlp;
+      const W temp = dd[sc(p + 1)];
+      dd[sc(p + 1)] = fmaw(-fact, temp, du[sc(p)]);
+      if (p <= N - 2) {
+        dl[sc(p + 1)] = du[sc(p + 1)];               // fill-in of row p: du2
+        du[sc(p + 1)] = -fact * dl[sc(p + 1)];
+      } else {
+        dl[sc(p + 1)] = W(0);
+      }
+      du[sc(p)] = temp;
+      const W tb = bq[sc(p)];
+      bq[sc(p)] = bq[sc(p + 1)];
+      bq[sc(p + 1)] = fmaw(-fact, bq[sc(p + 1)], tb);
+    }
+  }
+  if (sing || dd[sc(N)] == W(0)) {
+    atomicAdd(&L.flags[1], 1);
+  } else {
+    bq[sc(N)] = bq[sc(N)] / dd[sc(N)];
+    if (N > 1) bq[sc(N - 1)] = fmaw(-du[sc(N - 1)], bq[sc(N)], bq[sc(N - 1)]) / dd[sc(N - 1)];
+    for (int p = N - 2; p >= 1; --p)
+      bq[sc(p)] = fmaw(-dl[sc(p + 1)], bq[sc(p + 2)], fmaw(-du[sc(p)], bq[sc(p + 1)], bq[sc(p)])) / dd[sc(p)];
+    for (int p = 1; p <= N; ++p) r[lb + p * st] = bq[sc(p)];
+  }
+  if (nsw) atomicAdd(&L.flags[0], nsw);
+  atomicAdd(&L.flags[2], 1);
 }
 
 // Per-node step after a line sweep, in the sweep precision W, one thread per

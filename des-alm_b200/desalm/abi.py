@@ -83,13 +83,14 @@ class StepReport(C.Structure):
         ("residual", C.c_double * 5),
         ("init_residual", C.c_double * 5),
         ("pivots", C.c_int),
-        ("reserved", C.c_int * 7),
+        ("pivot_lines", C.c_int),
+        ("reserved", C.c_int * 6),
     ]
 
     def as_dict(self):
         return {"iterations": self.iterations, "converged": bool(self.converged),
                 "residual": list(self.residual), "init_residual": list(self.init_residual),
-                "pivots": self.pivots}
+                "pivots": self.pivots, "pivot_lines": self.pivot_lines}
 
 
 class LpReport(C.Structure):

@@ -119,6 +119,10 @@ def lib():
         L.desalm_kernel_class_count.restype = C.c_int
         L.desalm_sweep_widths.argtypes = [vp, C.POINTER(C.c_int)]
         L.desalm_sweep_widths.restype = C.c_int
+        L.desalm_turb_sweep_widths.argtypes = [vp, C.POINTER(C.c_int)]
+        L.desalm_turb_sweep_widths.restype = C.c_int
+        L.desalm_set_sweep_widths.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.desalm_set_sweep_widths.restype = C.c_int
         L.desalm_mg_driver_batch.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(StepReport)]
         L.desalm_mg_driver_batch.restype = C.c_int
         _LIB = L
@@ -373,10 +377,24 @@ class Solver:
         return np.array(list(out)).reshape(4, 3, 3)
 
     def sweep_widths(self):
-        """Lines per CTA of the DAF sweeps, [level][direction] (0: not tuned)."""
+        """Kernel of the DAF sweeps, [level][direction]: 1 lines in lanes,
+        16/8/4 slab lines per CTA (0: not tuned, lines in lanes)."""
         out = (C.c_int * 12)()
         self._ck(self.L.desalm_sweep_widths(self.ctx, out), "sweep_widths")
         return np.array(list(out)).reshape(4, 3)
+
+    def turb_sweep_widths(self):
+        """Kernel of the turbulence sweeps per direction: 1 lines in lanes,
+        32/16/8 slab lines per CTA (0: not tuned, lines in lanes)."""
+        out = (C.c_int * 3)()
+        self._ck(self.L.desalm_turb_sweep_widths(self.ctx, out), "turb_sweep_widths")
+        return np.array(list(out))
+
+    def set_sweep_widths(self, nl=None, turb=None):
+        """Sets the sweep kernels (nl: [4][3] or 12 values; turb: 3 values)."""
+        a = None if nl is None else (C.c_int * 12)(*[int(v) for v in np.asarray(nl).reshape(-1)])
+        b = None if turb is None else (C.c_int * 3)(*[int(v) for v in np.asarray(turb).reshape(-1)])
+        self._ck(self.L.desalm_set_sweep_widths(self.ctx, a, b), "set_sweep_widths")
 
     def wall_functions(self):
         self._ck(self.L.desalm_wall_functions(self.ctx), "wall_functions")

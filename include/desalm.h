@@ -105,7 +105,11 @@ typedef struct desalm_step_report {
                                system with a column that is not diagonally
                                dominant is solved by the pivoting elimination;
                                the others need no interchange               */
-    int    reserved[7];
+    int    pivot_lines;     /* line systems that took the pivoting elimination
+                               (a column not diagonally dominant), summed over
+                               the step's sweeps; the others were solved by
+                               the no-interchange elimination               */
+    int    reserved[6];
 } desalm_step_report;
 
 /* fields for desalm_get_field / desalm_set_field (SoA, one level) */
@@ -286,14 +290,26 @@ int  desalm_overset_exchange(desalm_overset* ov, int what);
  * report.  Blocks step eagerly (no CUDA graph). */
 int  desalm_overset_mg_driver(desalm_overset* ov, desalm_step_report* reps);
 
-/* Lines per CTA of each level's DAF line sweeps, nl[3 * level + direction]
- * (directions i, j, k; 0 for levels the case does not have): 16, 8 or 4, as
- * timed on this GPU when the grid was set (desalm_set_grid tries each width
- * whose shared-memory slab fits and keeps the fastest), or 0 where the
- * timing is off (environment DESALM_AUTOTUNE=0) and the widest slab that
- * leaves room for two CTAs per SM is used.  The width changes the time
- * only: every line is solved by the same operations. */
+/* Kernel of each level's DAF line sweeps, nl[3 * level + direction]
+ * (directions i, j, k; 0 for levels the case does not have): 1 for the
+ * lines-in-lanes kernel (each warp solves 32 lines, the eliminated rows kept
+ * in a global scratch), 16, 8 or 4 for the shared-memory slab kernel with
+ * that many lines per CTA, as timed on this GPU when the grid was set
+ * (desalm_set_grid tries each and keeps the fastest), or 0 where the timing
+ * is off (environment DESALM_AUTOTUNE=0) and the lines-in-lanes kernel is
+ * used.  The choice changes the time only: every line is solved by the same
+ * operations in the same order. */
 int  desalm_sweep_widths(desalm_ctx* ctx, int nl[12]);
+/* The same for the turbulence model's line sweeps of the fine level,
+ * nl[direction]: 1 lines in lanes, 32, 16 or 8 slab lines per CTA, 0 the
+ * default (lines in lanes).  The i and j sweeps are timed; the k sweep takes
+ * the j sweep's choice. */
+int  desalm_turb_sweep_widths(desalm_ctx* ctx, int nl[3]);
+/* Sets the kernels of the line sweeps (values as above; nl or turb may be
+ * NULL to leave that set alone).  A slab width whose shared memory does not
+ * fit, or a width for a level the case does not have, is DESALM_EINVAL and
+ * changes nothing.  Setting the grid again re-times them. */
+int  desalm_set_sweep_widths(desalm_ctx* ctx, const int nl[12], const int turb[3]);
 /* CTA tile (threads along i, j, k; 128 in all) of each level's residual
  * kernels, tiles[9 * level + 3 * kernel + axis], kernel 0 = the first
  * residual pass (K_R), 1 = the recalculated residual, 2 = the turbulence

@@ -1,9 +1,10 @@
 """The autotuner: desalm_set_grid times the DAF sweeps of every level and
-direction at 16, 8 and 4 lines per CTA, and the residual kernels (first pass,
+direction with the lines-in-lanes kernel and at 16, 8 and 4 slab lines per
+CTA, the turbulence sweeps likewise, and the residual kernels (first pass,
 recalculation, turbulence residual) at eight CTA tiles of 128 threads, and
 keeps the fastest of each.  Widths and tiles may change the time only, so a
 tuned context must step exactly like one on the shared-memory rule and the
-default tile (DESALM_AUTOTUNE=0), and the timing runs must leave the state
+default kernels and tile (DESALM_AUTOTUNE=0), and the timing runs must leave the state
 alone."""
 import numpy as np
 import pytest
@@ -31,7 +32,9 @@ def test_tuned_widths_change_nothing_but_time(precision, monkeypatch):
     rule = _solver(case, grid, state)
     monkeypatch.delenv("DESALM_AUTOTUNE")
     w = tuned.sweep_widths()
-    assert set(np.unique(w[:case.ng])) <= {4, 8, 16} and not w[case.ng:].any()
+    assert set(np.unique(w[:case.ng])) <= {1, 4, 8, 16} and not w[case.ng:].any()
+    assert set(tuned.turb_sweep_widths()) <= {1, 8, 16, 32}
+    assert not rule.turb_sweep_widths().any()
     assert not rule.sweep_widths().any()
     tiles = tuned.kernel_tiles()
     shapes = {(32, 4, 1), (32, 2, 2), (32, 1, 4), (64, 2, 1), (64, 1, 2), (128, 1, 1), (16, 8, 1), (16, 4, 2)}
