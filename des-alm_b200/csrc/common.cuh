@@ -101,6 +101,10 @@ DESALM_DEV float fmaw(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 DESALM_DEV double fmaw(double a, double b, double c) { return __fma_rn(a, b, c); }
 DESALM_DEV float mulw(float a, float b) { return __fmul_rn(a, b); }
 DESALM_DEV double mulw(double a, double b) { return __dmul_rn(a, b); }
+// Drops the 128-byte L2 line at p (128-byte aligned) without writing it
+// back: for line-solve scratch that has been read for the last time.
+DESALM_DEV void l2_discard(const void* p) { asm volatile("discard.global.L2 [%0], 128;\n" ::"l"(p) : "memory"); }
+
 // a b - c d as fma(a, b, -(c d)) with c d rounded first (the middle 2x2
 // block of a two-ended elimination)
 DESALM_DEV float fms2(float a, float b, float c, float d) { return __fmaf_rn(a, b, -__fmul_rn(c, d)); }

@@ -232,8 +232,9 @@ struct desalm_ctx {
   } alm;                      // actuator-line forcing (rhs_lines)
   int* flags = nullptr;       // device [3]
   // scratch of the lines-in-lanes sweeps (k_gsweep, k_sa_gsweep): 16 arrays
-  // of the fine level's node count in the sweep precision, shared by every
-  // level and sweep (they run one after another on the stream)
+  // of gss elements (rows x padded lines of the fine level's longest sweep)
+  // in the sweep precision, shared by every level and sweep (they run one
+  // after another on the stream)
   void* gsweep = nullptr;
   int gss = 0;
   SaWork sa{};
@@ -1523,10 +1524,16 @@ int desalm_init(const desalm_case* c, desalm_ctx** out) {
   rc = dalloc(ctx, ctx->allocs, (void**)&ctx->flags, 3 * sizeof(int));
   if (rc) { *out = ctx; return rc; }
   {
-    const long NF = (long)c->im * c->jm * c->km;
+    // rows x lines of the longest sweep, the lines of a plane padded to a
+    // multiple of 32 (each warp's row is whole 128-byte lines); the coarse
+    // levels and the turbulence sweeps need less
+    auto rup = [](long v) { return (v + 31) / 32 * 32; };
+    const long e = c->btype[1] == 5 ? 1 : 0;   // the outlet row and line of the fine level
+    const long im2 = c->im - 2, jm2 = c->jm - 2, km2 = c->km - 2;
+    const long g = std::max((im2 + e) * rup(jm2) * km2, std::max(jm2 * rup(im2 + e) * km2, km2 * rup(im2 + e) * jm2));
     const size_t wb = c->precision_mode == DESALM_FP64 ? 8 : 4;
-    ctx->gss = (int)NF;
-    rc = dalloc(ctx, ctx->allocs, &ctx->gsweep, 16 * (size_t)NF * wb);
+    ctx->gss = (int)rup(g);
+    rc = dalloc(ctx, ctx->allocs, &ctx->gsweep, 16 * (size_t)ctx->gss * wb);
     if (rc) { *out = ctx; return rc; }
   }
   for (int n = 0; n < ctx->ng; ++n) {
@@ -2381,7 +2388,7 @@ template <class SW, int DIR>
 int sa_sweep(desalm_ctx* ctx, SaT<SW>& S, int amax, int n, int nb, double nin) {
   const int want = ctx->sa_nl[DIR];
   if (want == 0 || want == 1) {
-    LAUNCH(KC_SA_SWEEP, 0, nin, launch_k(k_sa_gsweep<SW, DIR>, dim3(cdiv(amax, 64), nb), 128, 0, ctx->stream, S));
+    LAUNCH(KC_SA_SWEEP, 0, nin, launch_k(k_sa_gsweep<SW, DIR>, dim3(cdiv(amax, 64), nb, 1), 128, 0, ctx->stream, S, SaPair<SW>{}));
     CKL();
     return 0;
   }
@@ -2502,6 +2509,22 @@ KwT<W> make_kw(desalm_ctx* ctx, Lv<double, W>& L) {
 // production once, then itk sub-iterations of the fused residual, the line
 // solves of k and of omega (each updating its scalar after its k sweep), the
 // boundary values, nu_t and the wall edges.
+// The line solves of two independent scalars along one direction: one
+// launch of the lines-in-lanes kernel for both where that kernel is chosen,
+// else the two in turn.
+template <class SW, int DIR>
+int sa_sweep_pair(desalm_ctx* ctx, SaT<SW>& S, SaT<SW>& S2, int amax, int n, int nb, double nin) {
+  const int want = ctx->sa_nl[DIR];
+  if (want == 0 || want == 1) {
+    SaPair<SW> B{{S2.co[3 * DIR + 0], S2.co[3 * DIR + 1], S2.co[3 * DIR + 2]}, S2.rh, S2.upd};
+    LAUNCH(KC_SA_SWEEP, 0, 2 * nin, launch_k(k_sa_gsweep<SW, DIR>, dim3(cdiv(amax, 64), nb, 2), 128, 0, ctx->stream, S, B));
+    CKL();
+    return 0;
+  }
+  RET((sa_sweep<SW, DIR>(ctx, S, amax, n, nb, nin)));
+  return sa_sweep<SW, DIR>(ctx, S2, amax, n, nb, nin);
+}
+
 template <class W>
 int kw_run(desalm_ctx* ctx, Lv<double, W>& L) {
   KwT<W> K = make_kw<W>(ctx, L);
@@ -2515,12 +2538,12 @@ int kw_run(desalm_ctx* ctx, Lv<double, W>& L) {
   LAUNCH(KC_SA_AUX, 0, L.N, launch_k(k_kw_pre<W>, cdiv(L.N, 256), 256, 0, s, K));
   for (int it = 0; it < ctx->c.itk; ++it) {
     LAUNCH(KC_SA_RHS, 0, nin, launch_k(k_kw_rhs<W>, grid_t(ctx, 0, 2, L.im, L.jm, L.km), blk_t(ctx, 0, 2), 0, s, K));
-    RET((sa_sweep<W, 0>(ctx, K.S, L.jm - 2, L.im - 2, L.km - 2, nin)));
-    RET((sa_sweep<W, 1>(ctx, K.S, L.im - 2, L.jm - 2, L.km - 2, nin)));
-    RET((sa_sweep<W, 2>(ctx, K.S, L.im - 2, L.km - 2, L.jm - 2, nin)));
-    RET((sa_sweep<W, 0>(ctx, Sw, L.jm - 2, L.im - 2, L.km - 2, nin)));
-    RET((sa_sweep<W, 1>(ctx, Sw, L.im - 2, L.jm - 2, L.km - 2, nin)));
-    RET((sa_sweep<W, 2>(ctx, Sw, L.im - 2, L.km - 2, L.jm - 2, nin)));
+    // k's and omega's line solves are independent (each has its own rows and
+    // right-hand side from k_kw_rhs and updates its own field in its k
+    // sweep), so they run together direction by direction
+    RET((sa_sweep_pair<W, 0>(ctx, K.S, Sw, L.jm - 2, L.im - 2, L.km - 2, nin)));
+    RET((sa_sweep_pair<W, 1>(ctx, K.S, Sw, L.im - 2, L.jm - 2, L.km - 2, nin)));
+    RET((sa_sweep_pair<W, 2>(ctx, K.S, Sw, L.im - 2, L.km - 2, L.jm - 2, nin)));
     const int nj = K.jend - K.jsta + 1, ni = K.iend - K.ista + 1, nk = K.kend - K.ksta + 1;
     LAUNCH(KC_SA_BC, 0, 2.0 * nj * nk, launch_k(k_kw_bc<W, 0>, dim3(cdiv(nj, 64), nk), 64, 0, s, K));
     LAUNCH(KC_SA_BC, 0, 2.0 * ni * nk, launch_k(k_kw_bc<W, 1>, dim3(cdiv(ni, 64), nk), 64, 0, s, K));

@@ -515,6 +515,17 @@ __global__ void __launch_bounds__(kSlabThreads) k_sa_sweep4(SaT<SW> S) {
   }
 }
 
+// A second scalar solved in the same launch as S (blockIdx.z = 1): the
+// rows of the sweep's direction, the right-hand side and the field the k
+// sweep updates (k-omega's omega beside k: the two line solves share
+// nothing, and one launch puts twice the lines in flight).
+template <class SW>
+struct SaPair {
+  const SW* co[3];
+  SW* rh;
+  double* upd;
+};
+
 // The same scalar ADI sweep with the lines in the lanes: a warp owns 32
 // neighbouring lines of one plane and one half of each, a CTA 2 x 32 lines
 // (four warps).  The rows are read from global memory as the elimination
@@ -526,14 +537,25 @@ __global__ void __launch_bounds__(kSlabThreads) k_sa_sweep4(SaT<SW> S) {
 // a few per SM.  The elimination is k_sa_sweep4's: the same operations in
 // the same order (two-ended, no interchange where every column is
 // diagonally dominant, SGTSV's pivoting elimination otherwise), so the two
-// kernels give the same values.
+// kernels give the same values.  The back-substitution drops the scratch rows
+// it has read from L2 without write-back (lines of a plane padded to a
+// multiple of 32: a warp's row is one 128-byte line, two in FP64), unless a
+// lane of the warp takes the pivoting path, which reuses them.
 // Scratch (S.gs, arrays S.gss apart): 1/d, b', and for the pivoting
-// elimination du and dl.
+// elimination du and dl (arrays 4..7 for the second scalar); row p of line
+// (a, b) at p nln + (a - 1) + amaxp (b - 1), amaxp = amax rounded up to 32.
+// Build-time tuning knobs of k_sa_gsweep (as for k_gsweep).
+#ifndef DESALM_SAGS_MINBLOCKS
+#define DESALM_SAGS_MINBLOCKS 1
+#endif
+#ifndef DESALM_SAGS_ROWS
+#define DESALM_SAGS_ROWS 8
+#endif
 template <class SW, int DIR>
-__global__ void __launch_bounds__(128) k_sa_gsweep(SaT<SW> S) {
+__global__ void __launch_bounds__(128, DESALM_SAGS_MINBLOCKS) k_sa_gsweep(SaT<SW> S, SaPair<SW> B) {
   pdl_wait();
   constexpr int LG = 2;                       // line groups of 32 per CTA
-  constexpr int R = sizeof(SW) == 4 ? 8 : 4;  // rows loaded one block ahead of the elimination
+  constexpr int R = sizeof(SW) == 4 ? DESALM_SAGS_ROWS : DESALM_SAGS_ROWS / 2;  // rows loaded one block ahead
   __shared__ SW m_d[LG][32], m_c[LG][32], m_b[LG][32], n_d[LG][32], n_c[LG][32], n_b[LG][32];
   __shared__ int s_ndom[LG][32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -545,14 +567,23 @@ __global__ void __launch_bounds__(128) k_sa_gsweep(SaT<SW> S) {
   else { amax = S.im - 2; n = S.km - 2; st = S.sk; sa = 1; base = S.sj * b; }
   const int a = blockIdx.x * (32 * LG) + g * 32 + lane + 1;
   const bool act = a <= amax;
-  const int nln = amax * (int)gridDim.y;            // lines of the sweep
-  const int line = (a - 1) + amax * (b - 1);
+  const int amaxp = (amax + 31) & ~31;
+  const int nln = amaxp * (int)gridDim.y;           // padded lines of the sweep
+  const int line = (a - 1) + amaxp * (b - 1);
+  const int line0 = line - lane;                    // the warp's first line
+  const unsigned wact = __ballot_sync(0xffffffffu, act);
   const int l0 = base + a * sa + st;                 // node of row 0
-  const SW* __restrict__ caw = S.co[3 * DIR + 0];
-  const SW* __restrict__ cap = S.co[3 * DIR + 1];
-  const SW* __restrict__ cae = S.co[3 * DIR + 2];
-  SW* __restrict__ gd = S.gs;
-  SW* __restrict__ gb = S.gs + S.gss;
+  // blockIdx.z = 1: the second scalar of B (its rows, right-hand side,
+  // field and scratch arrays 4..7)
+  const bool second = blockIdx.z == 1;
+  const SW* __restrict__ caw = second ? B.co[0] : S.co[3 * DIR + 0];
+  const SW* __restrict__ cap = second ? B.co[1] : S.co[3 * DIR + 1];
+  const SW* __restrict__ cae = second ? B.co[2] : S.co[3 * DIR + 2];
+  SW* __restrict__ rhs = second ? B.rh : S.rh;
+  double* __restrict__ upd = second ? B.upd : S.upd;
+  SW* __restrict__ gs = S.gs + (second ? 4 * (size_t)S.gss : 0);
+  SW* __restrict__ gd = gs;
+  SW* __restrict__ gb = gs + S.gss;
   auto sc = [&](int p) { return p * nln + line; };
   if (half == 0) s_ndom[g][lane] = 0;
   const int h = n / 2;
@@ -563,13 +594,13 @@ __global__ void __launch_bounds__(128) k_sa_gsweep(SaT<SW> S) {
     SW caw_[R], cap_[R], cae_[R], crr_[R];
 #pragma unroll
     for (int u = 0; u < R; ++u)
-      if (u < h) { const int l = l0 + u * st; caw_[u] = __ldg(caw + l); cap_[u] = __ldg(cap + l); cae_[u] = __ldg(cae + l); crr_[u] = S.rh[l]; }
+      if (u < h) { const int l = l0 + u * st; caw_[u] = __ldg(caw + l); cap_[u] = __ldg(cap + l); cae_[u] = __ldg(cae + l); crr_[u] = rhs[l]; }
     for (int p0 = 0; p0 < h; p0 += R) {
       SW naw[R], nap[R], nae[R], nrr[R];
 #pragma unroll
       for (int u = 0; u < R; ++u) {
         naw[u] = nap[u] = nae[u] = nrr[u] = SW(0);
-        if (p0 + R + u < h) { const int l = l0 + (p0 + R + u) * st; naw[u] = __ldg(caw + l); nap[u] = __ldg(cap + l); nae[u] = __ldg(cae + l); nrr[u] = S.rh[l]; }
+        if (p0 + R + u < h) { const int l = l0 + (p0 + R + u) * st; naw[u] = __ldg(caw + l); nap[u] = __ldg(cap + l); nae[u] = __ldg(cae + l); nrr[u] = rhs[l]; }
       }
 #pragma unroll
       for (int u = 0; u < R; ++u) {
@@ -598,13 +629,13 @@ __global__ void __launch_bounds__(128) k_sa_gsweep(SaT<SW> S) {
     SW caw_[R], cap_[R], cae_[R], crr_[R];
 #pragma unroll
     for (int u = 0; u < R; ++u)
-      if (n - 1 - u >= h) { const int l = l0 + (n - 1 - u) * st; caw_[u] = __ldg(caw + l); cap_[u] = __ldg(cap + l); cae_[u] = __ldg(cae + l); crr_[u] = S.rh[l]; }
+      if (n - 1 - u >= h) { const int l = l0 + (n - 1 - u) * st; caw_[u] = __ldg(caw + l); cap_[u] = __ldg(cap + l); cae_[u] = __ldg(cae + l); crr_[u] = rhs[l]; }
     for (int p0 = n - 1; p0 >= h; p0 -= R) {
       SW naw[R], nap[R], nae[R], nrr[R];
 #pragma unroll
       for (int u = 0; u < R; ++u) {
         naw[u] = nap[u] = nae[u] = nrr[u] = SW(0);
-        if (p0 - R - u >= h) { const int l = l0 + (p0 - R - u) * st; naw[u] = __ldg(caw + l); nap[u] = __ldg(cap + l); nae[u] = __ldg(cae + l); nrr[u] = S.rh[l]; }
+        if (p0 - R - u >= h) { const int l = l0 + (p0 - R - u) * st; naw[u] = __ldg(caw + l); nap[u] = __ldg(cap + l); nae[u] = __ldg(cae + l); nrr[u] = rhs[l]; }
       }
 #pragma unroll
       for (int u = 0; u < R; ++u) {
@@ -640,25 +671,40 @@ __global__ void __launch_bounds__(128) k_sa_gsweep(SaT<SW> S) {
     if (ndom) atomicAdd(&s_ndom[g][lane], ndom);
   }
   __syncthreads();
+  const bool wdisc = __all_sync(0xffffffffu, !act || !s_ndom[g][lane]);
   if (!act) return;
+  // rows pb, pb + dir, ... (R of them, those in [lo, hi]) of the warp's 32
+  // lines read for the last time: lane t < 2 R SEG drops one 128-byte line
+  auto drop = [&](int pb, int dir, int lo, int hi) {
+    if (!wdisc) return;
+    __syncwarp(wact);
+    constexpr int SEG = 32 * (int)sizeof(SW) / 128;
+    static_assert(R * 2 * SEG <= 32, "one 128-byte line per lane");
+    if (lane < R * 2 * SEG) {
+      const int u = lane / (2 * SEG), col = (lane / SEG) & 1, piece = lane % SEG;
+      const int p = pb + dir * u;
+      if (p >= lo && p <= hi) l2_discard((col ? gd : gb) + p * nln + line0 + piece * (128 / (int)sizeof(SW)));
+    }
+  };
   const double dmul = 1.5 * S.es;
   // the solution of row p: into rh, or after the k sweep into the update
   // nu <- nu + (-nu + (nu_old + dnu)) / (1 + 1.5 dtev / dt)
   auto put = [&](int p, SW x) {
     const int l = l0 + p * st;
     if (DIR < 2) {
-      S.rh[l] = x;
+      rhs[l] = x;
     } else {
-      const double nt = S.upd[l];
+      const double nt = upd[l];
       const double qe5 = nt + double(x);
       const double dum = 1.0 + dmul * __ldg(S.dtev + l) / S.delti;
-      S.upd[l] = nt + (-nt + qe5) / dum;
+      upd[l] = nt + (-nt + qe5) / dum;
     }
   };
   if (!s_ndom[g][lane]) {
     if (half == 0) {
       SW x = fms2(b1, d2, u1, b2) / det;
       put(h - 1, x);
+      drop(h - 1, 1, h - 1, h - 1);     // the middle row is not read back
       for (int p0 = h - 2; p0 >= 0; p0 -= R) {
         SW bae[R], brr[R], brd[R];
 #pragma unroll
@@ -667,10 +713,12 @@ __global__ void __launch_bounds__(128) k_sa_gsweep(SaT<SW> S) {
 #pragma unroll
         for (int u = 0; u < R; ++u)
           if (p0 - u >= 0) { x = mulw(fmaw(-bae[u], x, brr[u]), brd[u]); put(p0 - u, x); }
+        drop(p0, -1, 0, h - 2);
       }
     } else {
       SW x = fms2(d1, b2, l2, b1) / det;
       put(h, x);
+      drop(h, 1, h, h);
       for (int p0 = h + 1; p0 < n; p0 += R) {
         SW baw[R], brr[R], brd[R];
 #pragma unroll
@@ -679,6 +727,7 @@ __global__ void __launch_bounds__(128) k_sa_gsweep(SaT<SW> S) {
 #pragma unroll
         for (int u = 0; u < R; ++u)
           if (p0 + u < n) { x = mulw(fmaw(-baw[u], x, brr[u]), brd[u]); put(p0 + u, x); }
+        drop(p0, 1, h + 1, n - 1);
       }
     }
     return;
@@ -688,12 +737,12 @@ __global__ void __launch_bounds__(128) k_sa_gsweep(SaT<SW> S) {
   // partial pivoting (src/sgtsv.f:107-162, 232-257) from the original rows,
   // in the line's scratch: d (gd), b (gb), du (gu) and dl (gl, with the
   // fill-in of a swap)
-  SW* __restrict__ gu = S.gs + 2 * (size_t)S.gss;
-  SW* __restrict__ gl = S.gs + 3 * (size_t)S.gss;
+  SW* __restrict__ gu = gs + 2 * (size_t)S.gss;
+  SW* __restrict__ gl = gs + 3 * (size_t)S.gss;
   for (int p = 0; p < n; ++p) {
     const int l = l0 + p * st;
     gd[sc(p)] = cap[l];
-    gb[sc(p)] = S.rh[l];
+    gb[sc(p)] = rhs[l];
     gu[sc(p)] = cae[l];
     gl[sc(p)] = caw[l];
   }

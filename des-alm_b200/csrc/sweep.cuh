@@ -421,16 +421,30 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
 // line of a level is in flight at once.  The operations and their order are
 // k_sweep4's (two-ended elimination, SGTSV's no-interchange branch where
 // every column is diagonally dominant, its pivoting elimination otherwise),
-// so both kernels give the same values.  Systems 0 and 1 share the matrix
-// (aw = ae = -tc), so system 1 reads system 0's 1/d instead of storing its
-// own.
+// so both kernels give the same values.
+// The scratch of a row lives a few microseconds: the back-substitution reads
+// it in the reverse order of the elimination, then drops its L2 lines
+// without write-back (the lines of a plane are padded to a multiple of 32, so
+// that a warp's row is whole 128-byte lines), so that it need not reach HBM.
+// Rows are not dropped where a lane of the warp takes the pivoting path,
+// which reuses them.
 // Scratch (L.gs, arrays L.gss elements apart): per system m the arrays
-// 4m + 0..3 = 1/d (d in the pivoting elimination), b', du and dl.
+// 4m + 0..3 = 1/d (d in the pivoting elimination), b', du and dl; row p of
+// line (a, b) at (p - 1) nln + (a - 1) + amaxp (b - 1), amaxp = amax rounded
+// up to 32.
 // ---------------------------------------------------------------------------
+// Build-time tuning knobs of k_gsweep: resident CTAs per SM requested, and
+// rows loaded one block ahead of the elimination in FP32 (half that in FP64).
+#ifndef DESALM_GS_MINBLOCKS
+#define DESALM_GS_MINBLOCKS 3
+#endif
+#ifndef DESALM_GS_ROWS
+#define DESALM_GS_ROWS 8
+#endif
 template <class T, class W, int DIR>
-__global__ void __launch_bounds__(256, 3) k_gsweep(Lv<T, W> L, Par P, int blo, int bhi) {
+__global__ void __launch_bounds__(256, DESALM_GS_MINBLOCKS) k_gsweep(Lv<T, W> L, Par P, int blo, int bhi) {
   pdl_wait();
-  constexpr int R = sizeof(W) == 4 ? 8 : 4;  // rows loaded one block ahead
+  constexpr int R = sizeof(W) == 4 ? DESALM_GS_ROWS : DESALM_GS_ROWS / 2;  // rows loaded one block ahead
   __shared__ W mt_d[4][32], mt_u[4][32], mt_b[4][32];
   __shared__ W mb_d[4][32], mb_l[4][32], mb_b[4][32];
   __shared__ int s_ndom[4][32], s_nz[4][32];
@@ -445,15 +459,17 @@ __global__ void __launch_bounds__(256, 3) k_gsweep(Lv<T, W> L, Par P, int blo, i
   const int base = (DIR == 2) ? L.sj * b : L.sk * b;
   const int a = blockIdx.x * 32 + lane + 1;
   const bool act = a <= amax;
-  const int nln = amax * (int)gridDim.y;
-  const int line = (a - 1) + amax * (b - 1);
+  const int amaxp = (amax + 31) & ~31;
+  const int nln = amaxp * (int)gridDim.y;
+  const int line = (a - 1) + amaxp * (b - 1);
+  const int line0 = line - lane;               // the warp's first line: 128-byte aligned rows
+  const unsigned wact = __ballot_sync(0xffffffffu, act);
   const int lb = base + a * sa;                // node 0 of the line
   const W* __restrict__ tc = L.tc[DIR];
   const W* __restrict__ hc = L.hc[DIR];
   W* __restrict__ r = L.wk[m];
   W* __restrict__ gd = L.gs + (size_t)(4 * m) * L.gss;
   W* __restrict__ gb = L.gs + (size_t)(4 * m + 1) * L.gss;
-  const W* __restrict__ gdr = L.gs + (size_t)(4 * (m == 1 ? 0 : m)) * L.gss;  // the 1/d column read back
   auto sc = [&](int p) { return (p - 1) * nln + line; };   // row p = node p of the line, 1..n + ext
   auto coef = [&](W t, W hw_, W he_, W& aw, W& ae) {
     const W dw = t != W(0) ? hw_ : W(0);
@@ -519,7 +535,7 @@ __global__ void __launch_bounds__(256, 3) k_gsweep(Lv<T, W> L, Par P, int blo, i
           aec2 = duprev; apc = ap;
           nzero += d == W(0);
           rdprev = sweep_rcp(d);
-          if (m != 1) gd[sc(p)] = rdprev;
+          gd[sc(p)] = rdprev;
           gb[sc(p)] = bprev;
           dprev = d; duprev = ae;
           hw = hcur; hcur = ch[u];
@@ -538,7 +554,7 @@ __global__ void __launch_bounds__(256, 3) k_gsweep(Lv<T, W> L, Par P, int blo, i
       const W d = m == 2 ? fmaw(W(2), he, W(1)) : W(1);
       nzero += d == W(0);
       rdprev = sweep_rcp(d);
-      if (m != 1) gd[sc(n + 1)] = rdprev;
+      gd[sc(n + 1)] = rdprev;
       bprev = r[lb + (n + 1) * st];
       gb[sc(n + 1)] = bprev;
       dprev = d;
@@ -575,7 +591,7 @@ __global__ void __launch_bounds__(256, 3) k_gsweep(Lv<T, W> L, Par P, int blo, i
           aec2 = awprev; apc = ap;
           nzero += d == W(0);
           rdprev = sweep_rcp(d);
-          if (m != 1) gd[sc(p)] = rdprev;
+          gd[sc(p)] = rdprev;
           gb[sc(p)] = bprev;
           dprev = d; awprev = aw;
           he = hcur; hcur = ch[u];
@@ -599,18 +615,36 @@ __global__ void __launch_bounds__(256, 3) k_gsweep(Lv<T, W> L, Par P, int blo, i
     if (nzero) atomicAdd(&s_nz[m][lane], nzero);
   }
   __syncthreads();
+  // the warp drops its scratch rows as it reads them back when none of its
+  // lines takes the pivoting path (which reuses them)
+  const bool wdisc = __all_sync(0xffffffffu, !act || !s_ndom[m][lane]);
   if (!act) return;
+  // rows pb, pb + dir, ... (R of them, those in [lo, hi]) of the warp's 32
+  // lines read for the last time: lane t < 2 R SEG drops one 128-byte line
+  // of the b' (t / SEG even) or 1/d column
+  auto drop = [&](int pb, int dir, int lo, int hi) {
+    if (!wdisc) return;
+    __syncwarp(wact);
+    constexpr int SEG = 32 * (int)sizeof(W) / 128;   // 128-byte lines per warp row
+    static_assert(R * 2 * SEG <= 32, "one 128-byte line per lane");
+    if (lane < R * 2 * SEG) {
+      const int u = lane / (2 * SEG), col = (lane / SEG) & 1, piece = lane % SEG;
+      const int p = pb + dir * u;
+      if (p >= lo && p <= hi) l2_discard((col ? gd : gb) + (p - 1) * nln + line0 + piece * (128 / (int)sizeof(W)));
+    }
+  };
   if (!s_ndom[m][lane]) {
     if (half == 0) {
       const int nz = s_nz[m][lane];
       if (nz) atomicAdd(&L.flags[1], nz);
       W x = fms2(b1, d2, u1, b2) / det;
       r[lb + h * st] = x;
+      drop(h, 1, h, h);                  // the middle row is not read back
       for (int p0 = h - 1; p0 >= 1; p0 -= R) {
         W bt[R], bh[R], br[R], bd[R];
 #pragma unroll
         for (int u = 0; u < R; ++u)
-          if (p0 - u >= 1) { const int l = lb + (p0 - u) * st; bt[u] = tc[l]; bh[u] = hc[l + st]; br[u] = gb[sc(p0 - u)]; bd[u] = gdr[sc(p0 - u)]; }
+          if (p0 - u >= 1) { const int l = lb + (p0 - u) * st; bt[u] = tc[l]; bh[u] = hc[l + st]; br[u] = gb[sc(p0 - u)]; bd[u] = gd[sc(p0 - u)]; }
 #pragma unroll
         for (int u = 0; u < R; ++u) {
           if (p0 - u >= 1) {
@@ -620,15 +654,17 @@ __global__ void __launch_bounds__(256, 3) k_gsweep(Lv<T, W> L, Par P, int blo, i
             r[lb + (p0 - u) * st] = x;
           }
         }
+        drop(p0, -1, 1, h - 1);
       }
     } else {
       W x = fms2(d1, b2, l2, b1) / det;
       r[lb + (h + 1) * st] = x;
+      drop(h + 1, 1, h + 1, h + 1);
       for (int p0 = h + 2; p0 <= n; p0 += R) {
         W bt[R], bh[R], br[R], bd[R];
 #pragma unroll
         for (int u = 0; u < R; ++u)
-          if (p0 + u <= n) { const int l = lb + (p0 + u) * st; bt[u] = tc[l]; bh[u] = hc[l - st]; br[u] = gb[sc(p0 + u)]; bd[u] = gdr[sc(p0 + u)]; }
+          if (p0 + u <= n) { const int l = lb + (p0 + u) * st; bt[u] = tc[l]; bh[u] = hc[l - st]; br[u] = gb[sc(p0 + u)]; bd[u] = gd[sc(p0 + u)]; }
 #pragma unroll
         for (int u = 0; u < R; ++u) {
           if (p0 + u <= n) {
@@ -638,11 +674,13 @@ __global__ void __launch_bounds__(256, 3) k_gsweep(Lv<T, W> L, Par P, int blo, i
             r[lb + (p0 + u) * st] = x;
           }
         }
+        drop(p0, 1, h + 2, n);
       }
       if (ext) {
         const W aw = m == 2 ? -(W(2) * hc[lb + n * st]) : W(0);
-        x = mulw(fmaw(-aw, x, gb[sc(n + 1)]), gdr[sc(n + 1)]);
+        x = mulw(fmaw(-aw, x, gb[sc(n + 1)]), gd[sc(n + 1)]);
         r[lb + (n + 1) * st] = x;
+        drop(n + 1, 1, n + 1, n + 1);
       }
     }
     return;
