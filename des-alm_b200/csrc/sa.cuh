@@ -546,7 +546,7 @@ struct SaPair {
 // (a, b) at p nln + (a - 1) + amaxp (b - 1), amaxp = amax rounded up to 32.
 // Build-time tuning knobs of k_sa_gsweep (as for k_gsweep).
 #ifndef DESALM_SAGS_MINBLOCKS
-#define DESALM_SAGS_MINBLOCKS 1
+#define DESALM_SAGS_MINBLOCKS 4
 #endif
 #ifndef DESALM_SAGS_ROWS
 #define DESALM_SAGS_ROWS 8

@@ -436,7 +436,7 @@ __global__ void __launch_bounds__(NT) k_sweep4(Lv<T, W> L, Par P, int blo, int b
 // Build-time tuning knobs of k_gsweep: resident CTAs per SM requested, and
 // rows loaded one block ahead of the elimination in FP32 (half that in FP64).
 #ifndef DESALM_GS_MINBLOCKS
-#define DESALM_GS_MINBLOCKS 3
+#define DESALM_GS_MINBLOCKS 2
 #endif
 #ifndef DESALM_GS_ROWS
 #define DESALM_GS_ROWS 8
@@ -478,31 +478,39 @@ __global__ void __launch_bounds__(256, DESALM_GS_MINBLOCKS) k_gsweep(Lv<T, W> L,
     else if (m == 2) { aw = -dw - t; ae = de - t; }
     else { aw = dw - t; ae = -de - t; }
   };
-  // semi-explicit boundary rows of the line (component m)
-  auto bvec = [&](int hi) -> W {
+  // semi-explicit boundary rows of the 32 lines, all four components: warp 0
+  // forms the west rows, warp 4 the east rows (before the elimination, so
+  // that the modal matrices' registers are not held through it)
+  __shared__ W s_bw[4][32], s_be[4][32];
+  if (w == 0 || w == 4) {
+    const int hi = w == 4;
     T v[4] = {0, 0, 0, 0};
-    if (DIR == 0) {
-      if (!hi && blo) {
-        const int S = L.jm * L.km, o = a + L.jm * b;
-        face_vec<T, W, 0>(L, P, lb, 0, L.bi + o, L.bi + 4 * S + o, S, v);
+    if (act) {
+      if (DIR == 0) {
+        if (!hi && blo) {
+          const int S = L.jm * L.km, o = a + L.jm * b;
+          face_vec<T, W, 0>(L, P, lb, 0, L.bi + o, L.bi + 4 * S + o, S, v);
+        }
+      } else if (DIR == 1) {
+        const int S = L.im * L.km, o = a + L.im * b;
+        if (!hi && blo) face_vec<T, W, 1>(L, P, lb, 2, L.bj + o, L.bj + 4 * S + o, S, v);
+        if (hi && bhi) face_vec<T, W, 1>(L, P, lb + (n + 1) * st, 3, L.bj + 8 * S + o, L.bj + 12 * S + o, S, v);
+      } else {
+        const int S = L.im * L.jm, o = a + L.im * b;
+        if (!hi && blo) face_vec<T, W, 2>(L, P, lb, 4, L.bk + o, L.bk + 4 * S + o, S, v);
+        if (hi && bhi) face_vec<T, W, 2>(L, P, lb + (n + 1) * st, 5, L.bk + 8 * S + o, L.bk + 12 * S + o, S, v);
       }
-    } else if (DIR == 1) {
-      const int S = L.im * L.km, o = a + L.im * b;
-      if (!hi && blo) face_vec<T, W, 1>(L, P, lb, 2, L.bj + o, L.bj + 4 * S + o, S, v);
-      if (hi && bhi) face_vec<T, W, 1>(L, P, lb + (n + 1) * st, 3, L.bj + 8 * S + o, L.bj + 12 * S + o, S, v);
-    } else {
-      const int S = L.im * L.jm, o = a + L.im * b;
-      if (!hi && blo) face_vec<T, W, 2>(L, P, lb, 4, L.bk + o, L.bk + 4 * S + o, S, v);
-      if (hi && bhi) face_vec<T, W, 2>(L, P, lb + (n + 1) * st, 5, L.bk + 8 * S + o, L.bk + 12 * S + o, S, v);
     }
-    return W(v[m]);
-  };
+#pragma unroll
+    for (int q = 0; q < 4; ++q) (hi ? s_be : s_bw)[q][lane] = W(v[q]);
+  }
   if (half == 0) { s_ndom[m][lane] = 0; s_nz[m][lane] = 0; }
+  __syncthreads();
   const int h = n / 2;  // nodes 1..h top, h+1..n bottom
   int nzero = 0, ndom = 0;
   W apc = 0, aec2 = 0;
   if (act && half == 0) {
-    const W bwm = bvec(0);
+    const W bwm = s_bw[m][lane];
     W hw = hc[lb], hcur = hc[lb + st];
     W dprev = 0, rdprev = 0, duprev = 0, bprev = 0;
     W ct[R], ch[R], cr[R];
@@ -546,7 +554,7 @@ __global__ void __launch_bounds__(256, DESALM_GS_MINBLOCKS) k_gsweep(Lv<T, W> L,
     }
     mt_d[m][lane] = dprev; mt_u[m][lane] = duprev; mt_b[m][lane] = bprev;
   } else if (act && half == 1) {
-    const W bem = bvec(1);
+    const W bem = s_be[m][lane];
     W he = hc[lb + (n + 1) * st], hcur = hc[lb + n * st];
     W dprev = 0, rdprev = 0, awprev = 0, bprev = 0;
     if (ext) {
@@ -695,7 +703,7 @@ __global__ void __launch_bounds__(256, DESALM_GS_MINBLOCKS) k_gsweep(Lv<T, W> L,
   W* __restrict__ du = L.gs + (size_t)(4 * m + 2) * L.gss;
   W* __restrict__ dl = L.gs + (size_t)(4 * m + 3) * L.gss;
   const int N = n + ext;
-  const W bwm = bvec(0), bem = bvec(1);
+  const W bwm = s_bw[m][lane], bem = s_be[m][lane];
   for (int p = 1; p <= N; ++p) {
     W aw, ae, ap;
     if (p <= n) {
