@@ -549,11 +549,43 @@ int gsweep(desalm_ctx* ctx, Lv<T, W>& L, const Par& P, int lvl, int blo, int bhi
   return 0;
 }
 
+// The warp-shuffle cyclic reduction of lines of at most 32 rows (k_psweep):
+// one CTA per line, a warp per system.
+template <class T, class W, int DIR>
+int psweep(desalm_ctx* ctx, Lv<T, W>& L, const Par& P, int lvl, int blo, int bhi, bool xform) {
+  int amax, nb;
+  if (DIR == 0) { amax = L.jm - 2; nb = L.km - 2; }
+  else if (DIR == 1) { amax = L.im - 2 + L.oute; nb = L.km - 2; }
+  else { amax = L.im - 2 + L.oute; nb = L.jm - 2; }
+  const int n = DIR == 0 ? L.im - 2 : (DIR == 1 ? L.jm - 2 : L.km - 2);
+  const int cls = DIR == 0 ? KC_SWEEP_I : (DIR == 1 ? KC_SWEEP_J : KC_SWEEP_K);
+  const double nin = double(amax) * n * nb;
+  cudaStream_t s = ctx->stream;
+  LAUNCH(cls, lvl, nin, launch_k(k_psweep<T, W, DIR>, dim3(amax, nb), 128, 0, s, L, P, blo, bhi));
+  CKL();
+  if (!xform) return 0;
+  const int xcls = DIR == 0 ? KC_XFORM_I : (DIR == 1 ? KC_XFORM_J : KC_XFORM_K);
+  const dim3 gx(cdiv(L.im - 2 + L.oute, 32), cdiv(L.jm - 2, 4), L.km - 2);
+  LAUNCH(xcls, lvl, nin, launch_k(k_xform<T, W, DIR>, gx, blk3(), 0, s, L));
+  CKL();
+  return 0;
+}
+
+// Rows of the DAF line systems of a direction: the interior nodes, and on the
+// i lines of the fine level the outlet row.
+template <class T, class W, int DIR>
+int sweep_rows(const Lv<T, W>& L) {
+  return DIR == 0 ? L.im - 2 + L.oute : (DIR == 1 ? L.jm - 2 : L.km - 2);
+}
+constexpr int kPcrRows = 32;   // lines this short are solved by k_psweep
+
 template <class T, class W, int DIR>
 int launch_sweep(desalm_ctx* ctx, Lv<T, W>& L, const Par& P, int lvl, int blo, int bhi, bool xform = true) {
   const int n = DIR == 0 ? L.im - 2 : (DIR == 1 ? L.jm - 2 : L.km - 2);
   const int want = lvl < 4 ? ctx->sweep_nl[lvl][DIR] : 0;
-  if (want == 0 || want == 1) return gsweep<T, W, DIR>(ctx, L, P, lvl, blo, bhi, xform);
+  const bool short_lines = sweep_rows<T, W, DIR>(L) <= kPcrRows;
+  if ((want == 0 || want == 2) && short_lines) return psweep<T, W, DIR>(ctx, L, P, lvl, blo, bhi, xform);
+  if (want == 0 || want == 1 || want == 2) return gsweep<T, W, DIR>(ctx, L, P, lvl, blo, bhi, xform);
   if (want == 16 && slab_bytes<W>(n, 16) <= kSlabMax) return sweep4_nl<T, W, DIR, 16>(ctx, L, P, lvl, blo, bhi, xform);
   if (want == 8 && slab_bytes<W>(n, 8) <= kSlabMax) return sweep4_nl<T, W, DIR, 8>(ctx, L, P, lvl, blo, bhi, xform);
   if (want == 4 && slab_bytes<W>(n, 4) <= kSlabMax) return sweep4_nl<T, W, DIR, 4>(ctx, L, P, lvl, blo, bhi, xform);
@@ -811,6 +843,12 @@ int tune_sweep(desalm_ctx* ctx, Lv<T, W>& L, int lvl, cudaEvent_t e0, cudaEvent_
   Par P = ctx->par;
   P.fine = (lvl == 0);
   const int n = DIR == 0 ? L.im - 2 : (DIR == 1 ? L.jm - 2 : L.km - 2);
+  // short lines always take the cyclic reduction (a different elimination
+  // order, so it is not one of the timed choices, which all give the same bits)
+  if (sweep_rows<T, W, DIR>(L) <= kPcrRows) {
+    ctx->sweep_nl[lvl][DIR] = 2;
+    return 0;
+  }
   float best = 0.f;
   int pick = 0;
   for (int nl : {1, 16, 8, 4}) {
@@ -2159,8 +2197,13 @@ int desalm_set_sweep_widths(desalm_ctx* ctx, const int nl[12], const int turb[3]
         }
         const Level& G = ctx->L[n];
         const int len = d == 0 ? G.im - 2 : (d == 1 ? G.jm - 2 : G.km - 2);
-        const bool ok = v == 0 || v == 1 || ((v == 4 || v == 8 || v == 16) && (size_t)10 * slab_fs(len + 2, v + 1) * wb <= kSlabMax);
-        if (!ok) { ctx->err = "DAF sweep width must be 0, 1, or 4, 8, 16 with a slab that fits"; return DESALM_EINVAL; }
+        const int rows = len + ((d == 0 && n == 0 && ctx->c.btype[1] == 5) ? 1 : 0);
+        const bool ok = v == 0 || v == 1 || (v == 2 && rows <= kPcrRows) ||
+                        ((v == 4 || v == 8 || v == 16) && (size_t)10 * slab_fs(len + 2, v + 1) * wb <= kSlabMax);
+        if (!ok) {
+          ctx->err = "DAF sweep width must be 0, 1, 2 (lines of at most 32 rows), or 4, 8, 16 with a slab that fits";
+          return DESALM_EINVAL;
+        }
       }
   }
   if (turb) {

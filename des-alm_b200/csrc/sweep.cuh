@@ -768,6 +768,162 @@ __global__ void __launch_bounds__(256, DESALM_GS_MINBLOCKS) k_gsweep(Lv<T, W> L,
   atomicAdd(&L.flags[2], 1);
 }
 
+// ---------------------------------------------------------------------------
+// Short lines (at most 32 rows: the coarse levels): one warp per line system,
+// one row per lane, solved by parallel cyclic reduction with warp shuffles.
+// In five steps every row eliminates its couplings to the rows s = 1, 2, 4,
+// 8, 16 away (rows past the ends act as identity rows), after which each row
+// stands alone: x = d / b.  The rows are k_gsweep's (coefficients, boundary
+// rows, outlet row) and so is the column test; cyclic reduction is Gaussian
+// elimination in another order, stable without interchanges when every
+// column is diagonally dominant.  A system with a column that is not is
+// solved by lane 0 with SGTSV's pivoting elimination in shared memory, as in
+// k_gsweep.  The elimination order differs from the Thomas kernels', so the
+// values agree with theirs to rounding.  A CTA is one line: warp m solves
+// system m.
+// ---------------------------------------------------------------------------
+template <class T, class W, int DIR>
+__global__ void __launch_bounds__(128) k_psweep(Lv<T, W> L, Par P, int blo, int bhi) {
+  pdl_wait();
+  const int lane = threadIdx.x & 31, m = threadIdx.x >> 5;
+  const int a = blockIdx.x + 1, b = blockIdx.y + 1;
+  int n, st, sa;
+  if (DIR == 0) { n = L.im - 2; st = 1; sa = L.sj; }
+  else if (DIR == 1) { n = L.jm - 2; st = L.sj; sa = 1; }
+  else { n = L.km - 2; st = L.sk; sa = 1; }
+  const int ext = DIR == 0 ? L.oute : 0;
+  const int N = n + ext;  // rows 1..N (N <= 32)
+  const int base = (DIR == 2) ? L.sj * b : L.sk * b;
+  const int lb = base + a * sa;
+  const W* __restrict__ tc = L.tc[DIR];
+  const W* __restrict__ hc = L.hc[DIR];
+  W* __restrict__ r = L.wk[m];
+  __shared__ W s_bv[2][4];
+  __shared__ W s_d[4][33], s_u[4][33], s_l[4][33], s_b[4][33];
+  if (threadIdx.x == 0 || threadIdx.x == 32) {
+    const int hi = threadIdx.x == 32;
+    T v[4] = {0, 0, 0, 0};
+    if (DIR == 0) {
+      if (!hi && blo) {
+        const int S = L.jm * L.km, o = a + L.jm * b;
+        face_vec<T, W, 0>(L, P, lb, 0, L.bi + o, L.bi + 4 * S + o, S, v);
+      }
+    } else if (DIR == 1) {
+      const int S = L.im * L.km, o = a + L.im * b;
+      if (!hi && blo) face_vec<T, W, 1>(L, P, lb, 2, L.bj + o, L.bj + 4 * S + o, S, v);
+      if (hi && bhi) face_vec<T, W, 1>(L, P, lb + (n + 1) * st, 3, L.bj + 8 * S + o, L.bj + 12 * S + o, S, v);
+    } else {
+      const int S = L.im * L.jm, o = a + L.im * b;
+      if (!hi && blo) face_vec<T, W, 2>(L, P, lb, 4, L.bk + o, L.bk + 4 * S + o, S, v);
+      if (hi && bhi) face_vec<T, W, 2>(L, P, lb + (n + 1) * st, 5, L.bk + 8 * S + o, L.bk + 12 * S + o, S, v);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) s_bv[hi][q] = W(v[q]);
+  }
+  __syncthreads();
+  // row p = lane + 1: aw x_{p-1} + ap x_p + ae x_{p+1} = d
+  const int p = lane + 1;
+  W aw = 0, ap = 1, ae = 0, d = 0;
+  if (p <= N) {
+    if (p <= n) {
+      const W t = tc[lb + p * st];
+      const W hw = hc[lb + (p - 1) * st], he = hc[lb + (p + 1) * st];
+      const W dw = t != W(0) ? hw : W(0), de = t != W(0) ? he : W(0);
+      if (m < 2) { aw = -t; ae = -t; }
+      else if (m == 2) { aw = -dw - t; ae = de - t; }
+      else { aw = dw - t; ae = -de - t; }
+      ap = fmaw(W(2), t, W(1));
+    } else {  // the outlet row (src/rhs_diag_solver.F90:207-221)
+      ap = m == 2 ? fmaw(W(2), hc[lb + (n + 1) * st], W(1)) : W(1);
+      aw = m == 2 ? -(W(2) * hc[lb + n * st]) : W(0);
+      ae = W(0);
+    }
+    d = r[lb + p * st];
+    if (p == 1) d = fmaw(-aw, s_bv[0][m], d);
+    if (p == n && !ext) d = fmaw(-ae, s_bv[1][m], d);
+  }
+  if (p == 1) aw = W(0);        // the couplings outside the system
+  if (p >= N) ae = W(0);
+  // column test: |ap_p| >= |ae_{p-1}| + |aw_{p+1}|
+  // (every lane takes part in each shuffle; the ends are masked afterwards)
+  W aeprev = __shfl_up_sync(0xffffffffu, ae, 1);
+  W awnext = __shfl_down_sync(0xffffffffu, aw, 1);
+  if (lane == 0) aeprev = W(0);
+  if (lane == 31) awnext = W(0);
+  const bool bad = p <= N && dabs(ap) < dabs(aeprev) + dabs(awnext);
+  if (!__any_sync(0xffffffffu, bad)) {
+    W ca = aw, cb = ap, cc = ae, cd = d;
+#pragma unroll
+    for (int s = 1; s < 32; s <<= 1) {
+      W am = __shfl_up_sync(0xffffffffu, ca, s), bm = __shfl_up_sync(0xffffffffu, cb, s);
+      W cm = __shfl_up_sync(0xffffffffu, cc, s), dm = __shfl_up_sync(0xffffffffu, cd, s);
+      W aq = __shfl_down_sync(0xffffffffu, ca, s), bq = __shfl_down_sync(0xffffffffu, cb, s);
+      W cq = __shfl_down_sync(0xffffffffu, cc, s), dq = __shfl_down_sync(0xffffffffu, cd, s);
+      if (lane < s) { am = W(0); bm = W(1); cm = W(0); dm = W(0); }
+      if (lane + s > 31) { aq = W(0); bq = W(1); cq = W(0); dq = W(0); }
+      const W k1 = ca / bm, k2 = cc / bq;
+      ca = -(k1 * am);
+      cc = -(k2 * cq);
+      cb = fmaw(-k2, aq, fmaw(-k1, cm, cb));
+      cd = fmaw(-k2, dq, fmaw(-k1, dm, cd));
+    }
+    if (p <= N) {
+      if (cb == W(0)) atomicAdd(&L.flags[1], 1);
+      r[lb + p * st] = cd / cb;
+    }
+    return;
+  }
+  // ---- SGTSV's elimination with partial pivoting (src/sgtsv.f:107-162,
+  // 232-257) by lane 0 on the rows in shared memory (index = row)
+  if (p <= N) { s_d[m][p] = ap; s_u[m][p] = ae; s_l[m][p] = aw; s_b[m][p] = d; }
+  __syncwarp();
+  if (lane == 0) {
+    W* dd = s_d[m]; W* du = s_u[m]; W* dl = s_l[m]; W* bq = s_b[m];
+    int nsw = 0;
+    bool sing = false;
+    for (int q = 1; q <= N - 1 && !sing; ++q) {
+      const W dlp = dl[q + 1], dp = dd[q];
+      if (dabs(dp) >= dabs(dlp)) {
+        if (dp != W(0)) {
+          const W fact = dlp / dp;
+          dd[q + 1] = fmaw(-fact, du[q], dd[q + 1]);
+          bq[q + 1] = fmaw(-fact, bq[q], bq[q + 1]);
+        } else {
+          sing = true;
+        }
+        dl[q + 1] = W(0);
+      } else {
+        ++nsw;
+        const W fact = dp / dlp;
+        dd[q] = dlp;
+        const W temp = dd[q + 1];
+        dd[q + 1] = fmaw(-fact, temp, du[q]);
+        if (q <= N - 2) {
+          dl[q + 1] = du[q + 1];                 // fill-in of row q: du2
+          du[q + 1] = -fact * dl[q + 1];
+        } else {
+          dl[q + 1] = W(0);
+        }
+        du[q] = temp;
+        const W tb = bq[q];
+        bq[q] = bq[q + 1];
+        bq[q + 1] = fmaw(-fact, bq[q + 1], tb);
+      }
+    }
+    if (sing || dd[N] == W(0)) {
+      atomicAdd(&L.flags[1], 1);
+    } else {
+      bq[N] = bq[N] / dd[N];
+      if (N > 1) bq[N - 1] = fmaw(-du[N - 1], bq[N], bq[N - 1]) / dd[N - 1];
+      for (int q = N - 2; q >= 1; --q) bq[q] = fmaw(-dl[q + 1], bq[q + 2], fmaw(-du[q], bq[q + 1], bq[q])) / dd[q];
+    }
+    if (nsw) atomicAdd(&L.flags[0], nsw);
+    atomicAdd(&L.flags[2], 1);
+  }
+  __syncwarp();
+  if (p <= N) r[lb + p * st] = s_b[m][p];
+}
+
 // Per-node step after a line sweep, in the sweep precision W, one thread per
 // interior node: after the i sweep the semi-explicit rows of the j faces are
 // copied out (rows 2, 3, jm-1, jm-2) and wk <- N1^-1 wk = Mb^-1 (Ma wk);

@@ -32,7 +32,7 @@ def test_tuned_widths_change_nothing_but_time(precision, monkeypatch):
     rule = _solver(case, grid, state)
     monkeypatch.delenv("DESALM_AUTOTUNE")
     w = tuned.sweep_widths()
-    assert set(np.unique(w[:case.ng])) <= {1, 4, 8, 16} and not w[case.ng:].any()
+    assert set(np.unique(w[:case.ng])) <= {1, 2, 4, 8, 16} and not w[case.ng:].any()
     assert set(tuned.turb_sweep_widths()) <= {1, 8, 16, 32}
     assert not rule.turb_sweep_widths().any()
     assert not rule.sweep_widths().any()
