@@ -291,14 +291,19 @@ int  desalm_overset_exchange(desalm_overset* ov, int what);
 int  desalm_overset_mg_driver(desalm_overset* ov, desalm_step_report* reps);
 
 /* Kernel of each level's DAF line sweeps, nl[3 * level + direction]
- * (directions i, j, k; 0 for levels the case does not have): 1 for the
- * lines-in-lanes kernel (each warp solves 32 lines, the eliminated rows kept
- * in a global scratch), 16, 8 or 4 for the shared-memory slab kernel with
- * that many lines per CTA, as timed on this GPU when the grid was set
- * (desalm_set_grid tries each and keeps the fastest), or 0 where the timing
- * is off (environment DESALM_AUTOTUNE=0) and the lines-in-lanes kernel is
- * used.  The choice changes the time only: every line is solved by the same
- * operations in the same order. */
+ * (directions i, j, k; 0 for levels the case does not have):
+ *   2  lines of at most 32 rows: warp-shuffle cyclic reduction, one warp per
+ *      line system (always chosen for such lines; it eliminates in another
+ *      order, so its values agree with the others' to rounding);
+ *   1  the lines-in-lanes Thomas kernel (each warp solves 32 lines, the
+ *      eliminated rows kept in a global scratch);
+ *   16, 8, 4  the shared-memory slab Thomas kernel with that many lines per
+ *      CTA;
+ * for longer lines the Thomas kernel timed fastest on this GPU when the grid
+ * was set (desalm_set_grid tries each), or 0 where the timing is off
+ * (environment DESALM_AUTOTUNE=0): cyclic reduction for short lines, the
+ * lines-in-lanes kernel for the others.  The Thomas kernels do the same
+ * operations in the same order: choosing among them changes the time only. */
 int  desalm_sweep_widths(desalm_ctx* ctx, int nl[12]);
 /* The same for the turbulence model's line sweeps of the fine level,
  * nl[direction]: 1 lines in lanes, 32, 16 or 8 slab lines per CTA, 0 the
@@ -307,8 +312,9 @@ int  desalm_sweep_widths(desalm_ctx* ctx, int nl[12]);
 int  desalm_turb_sweep_widths(desalm_ctx* ctx, int nl[3]);
 /* Sets the kernels of the line sweeps (values as above; nl or turb may be
  * NULL to leave that set alone).  A slab width whose shared memory does not
- * fit, or a width for a level the case does not have, is DESALM_EINVAL and
- * changes nothing.  Setting the grid again re-times them. */
+ * fit, 2 for lines longer than 32 rows, or a width for a level the case does
+ * not have, is DESALM_EINVAL and changes nothing.  Setting the grid again
+ * re-times them. */
 int  desalm_set_sweep_widths(desalm_ctx* ctx, const int nl[12], const int turb[3]);
 /* CTA tile (threads along i, j, k; 128 in all) of each level's residual
  * kernels, tiles[9 * level + 3 * kernel + axis], kernel 0 = the first
