@@ -3232,6 +3232,73 @@ __global__ void k_ov_scatter(const OvEntry* E, int n, double* const* tab, int f0
   for (int f = f0; f < f1; ++f) tab[x.db * 6 + f][x.dl] = buf[(size_t)e * 6 + f];
 }
 
+// Point lists of a rank's share of a sharded overset exchange: the
+// interpolated values of fields f0..f1-1 packed point-major, nf = f1 - f0 per
+// point (the send buffer of src/mg_bintp_mom.F90:100-135 for one
+// destination after another), and their write into donee nodes.
+__global__ void k_ovl_gather(const OvEntry* E, int n, double* const* tab, int f0, int f1, double* buf) {
+  pdl_wait();
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  const OvEntry& x = E[e];
+  const double xco = x.c[0], yco = x.c[1], zco = x.c[2], one = 1.0;
+  const double c000 = (one - xco) * (one - yco) * (one - zco);
+  const double c100 = xco * (one - yco) * (one - zco);
+  const double c010 = (one - xco) * yco * (one - zco);
+  const double c001 = (one - xco) * (one - yco) * zco;
+  const double c101 = xco * (one - yco) * zco;
+  const double c011 = (one - xco) * yco * zco;
+  const double c110 = xco * yco * (one - zco);
+  const double c111 = xco * yco * zco;
+  const int l = x.hl, sj = x.hsj, sk = x.hsk, nf = f1 - f0;
+  for (int f = f0; f < f1; ++f) {
+    const double* v = tab[x.hb * 6 + f];
+    buf[(size_t)e * nf + (f - f0)] = v[l] * c000 + v[l + 1] * c100 + v[l + sj] * c010 + v[l + sk] * c001 +
+                                     v[l + 1 + sk] * c101 + v[l + sj + sk] * c011 + v[l + 1 + sj] * c110 +
+                                     v[l + 1 + sj + sk] * c111;
+  }
+}
+
+__global__ void k_ovl_scatter(const OvEntry* E, int n, double* const* tab, int f0, int f1, const double* buf) {
+  pdl_wait();
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  const OvEntry& x = E[e];
+  const int nf = f1 - f0;
+  for (int f = f0; f < f1; ++f) tab[x.db * 6 + f][x.dl] = buf[(size_t)e * nf + (f - f0)];
+}
+
+}  // namespace
+
+struct desalm_ov_list {
+  std::vector<desalm_ctx*> blocks;
+  int n = 0;
+  bool gather = false;             // host cells and weights (else donee nodes)
+  OvEntry* entries = nullptr;      // device
+  double** tab = nullptr;          // device [blocks][6] field pointers of each block's fine level
+  cudaStream_t s = nullptr;
+  cudaEvent_t ev = nullptr;
+  std::vector<cudaEvent_t> bev;
+  std::string err;
+};
+
+namespace {
+
+// Device field table [block][6] of the blocks' fine levels: q(1..5), omega.
+int ov_field_table(desalm_ctx* const* ctxs, int nblocks, std::vector<double*>& tab) {
+  tab.assign(6L * nblocks, nullptr);
+  for (int b = 0; b < nblocks; ++b) {
+    for (int f = 0; f < 5; ++f) {
+      void* p = nullptr;
+      int esz = 0;
+      if (field_ptr(ctxs[b], 0, DESALM_F_Q + f, &p, &esz) || esz != 8) return DESALM_EINVAL;
+      tab[6 * b + f] = (double*)p;
+    }
+    tab[6 * b + 5] = ctxs[b]->c.turbulence == 2 ? ctxs[b]->kw.a[0] : nullptr;
+  }
+  return 0;
+}
+
 }  // namespace
 
 struct desalm_overset {
@@ -3321,19 +3388,11 @@ int desalm_overset_create(desalm_ctx* const* ctxs, int nblocks, const desalm_ove
     x.hsk = H.im * H.jm;
     for (int t = 0; t < 3; ++t) x.c[t] = map->coef[3 * e + t];
   }
+  std::vector<double*> tab;
+  RET(ov_field_table(ctxs, nblocks, tab));
   desalm_overset* ov = new desalm_overset();
   ov->blocks.assign(ctxs, ctxs + nblocks);
   ov->n = map->n;
-  std::vector<double*> tab(6L * nblocks, nullptr);
-  for (int b = 0; b < nblocks; ++b) {
-    for (int f = 0; f < 5; ++f) {
-      void* p = nullptr;
-      int esz = 0;
-      if (field_ptr(ctxs[b], 0, DESALM_F_Q + f, &p, &esz) || esz != 8) { delete ov; return DESALM_EINVAL; }
-      tab[6 * b + f] = (double*)p;
-    }
-    tab[6 * b + 5] = ctxs[b]->c.turbulence == 2 ? ctxs[b]->kw.a[0] : nullptr;
-  }
   bool ok = cudaMalloc((void**)&ov->entries, std::max<size_t>(1, E.size()) * sizeof(OvEntry)) == cudaSuccess &&
             cudaMalloc((void**)&ov->tab, tab.size() * sizeof(double*)) == cudaSuccess &&
             cudaMalloc((void**)&ov->buf, std::max<size_t>(1, 6 * E.size()) * sizeof(double)) == cudaSuccess &&
@@ -3374,6 +3433,125 @@ int desalm_overset_exchange(desalm_overset* ov, int what) {
   for (desalm_ctx* b : ov->blocks)
     if (cudaStreamSynchronize(b->stream) != cudaSuccess) return ov_fail(ov, "overset: synchronize", DESALM_ECUDA);
   return 0;
+}
+
+int desalm_ov_list_create(desalm_ctx* const* ctxs, int nctx, int n, const int* pts, const double* coef,
+                          desalm_ov_list** out) {
+  if (!ctxs || nctx < 1 || n < 0 || !out || (n > 0 && !pts)) return DESALM_EINVAL;
+  *out = nullptr;
+  for (int b = 0; b < nctx; ++b)
+    if (!ctxs[b] || ctxs[b]->c.turbulence != ctxs[0]->c.turbulence) return DESALM_EINVAL;
+  std::vector<OvEntry> E(n);
+  for (int e = 0; e < n; ++e) {
+    const int* q = pts + 4 * e;
+    if (q[0] < 0 || q[0] >= nctx) return DESALM_EINVAL;
+    const Level& G = ctxs[q[0]]->L[0];
+    OvEntry& x = E[e];
+    const int l = (q[1] - 1) + G.im * ((q[2] - 1) + G.jm * (q[3] - 1));
+    if (coef) {
+      // the host cell's eight corners lie inside the block
+      if (q[1] < 1 || q[1] > G.im - 1 || q[2] < 1 || q[2] > G.jm - 1 || q[3] < 1 || q[3] > G.km - 1) return DESALM_EINVAL;
+      x.hb = q[0];
+      x.hl = l;
+      x.hsj = G.im;
+      x.hsk = G.im * G.jm;
+      for (int t = 0; t < 3; ++t) x.c[t] = coef[3 * e + t];
+      x.db = 0;
+      x.dl = 0;
+    } else {
+      if (q[1] < 1 || q[1] > G.im || q[2] < 1 || q[2] > G.jm || q[3] < 1 || q[3] > G.km) return DESALM_EINVAL;
+      x.db = q[0];
+      x.dl = l;
+      x.hb = 0;
+      x.hl = 0;
+      x.hsj = x.hsk = 0;
+      x.c[0] = x.c[1] = x.c[2] = 0.0;
+    }
+  }
+  std::vector<double*> tab;
+  RET(ov_field_table(ctxs, nctx, tab));
+  desalm_ov_list* L = new desalm_ov_list();
+  L->blocks.assign(ctxs, ctxs + nctx);
+  L->n = n;
+  L->gather = coef != nullptr;
+  bool ok = cudaMalloc((void**)&L->entries, std::max<size_t>(1, E.size()) * sizeof(OvEntry)) == cudaSuccess &&
+            cudaMalloc((void**)&L->tab, tab.size() * sizeof(double*)) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&L->s, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&L->ev, cudaEventDisableTiming) == cudaSuccess;
+  L->bev.assign(nctx, nullptr);
+  for (int b = 0; b < nctx && ok; ++b) ok = cudaEventCreateWithFlags(&L->bev[b], cudaEventDisableTiming) == cudaSuccess;
+  if (ok && !E.empty()) ok = cudaMemcpy(L->entries, E.data(), E.size() * sizeof(OvEntry), cudaMemcpyHostToDevice) == cudaSuccess;
+  if (ok) ok = cudaMemcpy(L->tab, tab.data(), tab.size() * sizeof(double*), cudaMemcpyHostToDevice) == cudaSuccess;
+  if (!ok) {
+    desalm_ov_list_destroy(L);
+    return DESALM_ENOMEM;
+  }
+  *out = L;
+  return 0;
+}
+
+void desalm_ov_list_destroy(desalm_ov_list* L) {
+  if (!L) return;
+  if (L->s) cudaStreamSynchronize(L->s);
+  cudaFree(L->entries);
+  cudaFree(L->tab);
+  for (cudaEvent_t e : L->bev)
+    if (e) cudaEventDestroy(e);
+  if (L->ev) cudaEventDestroy(L->ev);
+  if (L->s) cudaStreamDestroy(L->s);
+  delete L;
+}
+
+const char* desalm_ov_list_last_error(const desalm_ov_list* L) { return L ? L->err.c_str() : "null list"; }
+
+int desalm_ov_list_fields(const desalm_ov_list* L, int what) {
+  if (!L || (what != 0 && what != 1)) return DESALM_EINVAL;
+  if (what == 0) return 4;
+  int f0 = 0, f1 = 0;
+  ov_turb_fields(L->blocks[0], f0, f1);
+  return f1 - f0;
+}
+
+namespace {
+// The list's kernel on its stream after every block's queued work, the
+// blocks' streams after it, then the list's stream drained (the buffer is
+// the caller's once this returns).
+int ovl_run(desalm_ov_list* L, int what, double* buf) {
+  if (!L || (what != 0 && what != 1) || (L->n > 0 && !buf)) return DESALM_EINVAL;
+  if (L->n == 0) return 0;
+  int f0 = 0, f1 = 4;
+  if (what == 1) ov_turb_fields(L->blocks[0], f0, f1);
+  if (f1 == f0) return 0;
+  const int nb = (int)L->blocks.size();
+  for (int b = 0; b < nb; ++b)
+    if (cudaEventRecord(L->bev[b], L->blocks[b]->stream) != cudaSuccess || cudaStreamWaitEvent(L->s, L->bev[b], 0) != cudaSuccess) {
+      L->err = "overset list: event";
+      return DESALM_ECUDA;
+    }
+  const unsigned g = (unsigned)((L->n + 127) / 128);
+  cudaError_t e = L->gather
+                      ? launch_k(k_ovl_gather, g, 128, 0, L->s, (const OvEntry*)L->entries, L->n, (double* const*)L->tab, f0, f1, buf)
+                      : launch_k(k_ovl_scatter, g, 128, 0, L->s, (const OvEntry*)L->entries, L->n, (double* const*)L->tab, f0, f1,
+                                 (const double*)buf);
+  if (e == cudaSuccess) e = cudaEventRecord(L->ev, L->s);
+  for (int b = 0; b < nb && e == cudaSuccess; ++b) e = cudaStreamWaitEvent(L->blocks[b]->stream, L->ev, 0);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(L->s);
+  if (e != cudaSuccess) {
+    L->err = std::string("overset list: ") + cudaGetErrorString(e);
+    return DESALM_ECUDA;
+  }
+  return 0;
+}
+}  // namespace
+
+int desalm_ov_list_gather(desalm_ov_list* L, int what, double* out) {
+  if (L && !L->gather) { L->err = "not a gather list (created without weights)"; return DESALM_EINVAL; }
+  return ovl_run(L, what, out);
+}
+
+int desalm_ov_list_scatter(desalm_ov_list* L, int what, const double* in) {
+  if (L && L->gather) { L->err = "not a scatter list (created with weights)"; return DESALM_EINVAL; }
+  return ovl_run(L, what, const_cast<double*>(in));
 }
 
 int desalm_overset_mg_driver(desalm_overset* ov, desalm_step_report* reps) {

@@ -481,18 +481,33 @@ def overset_pair(seed=0, turbulence=1, itmax=20, re=1000.0):
     its values from the host cell of the other block that contains it.
     Returns ([(case, grid, state)] for the two blocks, map) with the map as
     desalm_overset_map arrays (0-based blocks, 1-based nodes)."""
+    return overset_chain(2, seed=seed, turbulence=turbulence, itmax=itmax, re=re)
+
+
+_CHAIN_DIMS = [(33, 21, 17), (29, 17, 21), (25, 21, 17), (37, 17, 21)]   # odd at every coarsening of 3 levels
+
+
+def overset_chain(nblocks=2, seed=0, turbulence=1, itmax=20, re=1000.0):
+    """nblocks (2..4) overlapping wake boxes along x, block b spanning x in
+    [1.5 b, 1.5 b + 2] and y, z in [0, 2] with its own node counts (odd
+    blocks cosine-clustered in y): inflow at block 0's i = 1, the
+    characteristics outlet at the last block's i = im, interface faces
+    between neighbours.  Block b's i = im face takes its values from block
+    b + 1, its i = 1 face from block b - 1 (the donees in that order, block
+    by block).  Returns ([(case, grid, state)], map) as overset_pair."""
+    assert 2 <= nblocks <= len(_CHAIN_DIMS)
     rng = np.random.default_rng(seed)
-    dims = [(33, 21, 17), (29, 17, 21)]
-    xr = [(0.0, 2.0), (1.5, 3.5)]
+    dims = _CHAIN_DIMS[:nblocks]
+    xr = [(1.5 * b, 1.5 * b + 2.0) for b in range(nblocks)]
     blocks, axes = [], []
     for b, (im, jm, km) in enumerate(dims):
         c, g, st = wake(im=im, jm=jm, km=km, seed=seed + b, turbulence=turbulence, itmax=itmax, amp=0.0, re=re)
         c.btype[0] = BC_INFLOW if b == 0 else 0
-        c.btype[1] = 0 if b == 0 else BC_OUTLET
+        c.btype[1] = BC_OUTLET if b == nblocks - 1 else 0
         gx = 1.03 ** np.arange(im - 1)
         xs = xr[b][0] + np.concatenate(([0.0], np.cumsum(gx))) * ((xr[b][1] - xr[b][0]) / gx.sum())
         ys = np.linspace(0.0, 2.0, jm) ** 1.0
-        ys = 2.0 * (0.5 - 0.5 * np.cos(np.pi * np.linspace(0.0, 1.0, jm))) if b == 1 else ys
+        ys = 2.0 * (0.5 - 0.5 * np.cos(np.pi * np.linspace(0.0, 1.0, jm))) if b % 2 == 1 else ys
         zs = np.linspace(0.0, 2.0, km)
         X, Y, Z = _mesh(xs, ys, zs)
         g = dict(x=_flat(X), y=_flat(Y), z=_flat(Z), wd=g.get("wd"))
@@ -503,20 +518,24 @@ def overset_pair(seed=0, turbulence=1, itmax=20, re=1000.0):
         blocks.append((c, g, st))
         axes.append((xs, ys, zs))
     donee, host, coef = [], [], []
-    for b in range(2):
-        other = 1 - b
+    for b in range(nblocks):
         im, jm, km = dims[b]
         xs, ys, zs = axes[b]
-        ox, oy, oz = axes[other]
-        i = im if b == 0 else 1
-        for k in range(1, km + 1):
-            for j in range(1, jm + 1):
-                ih, fx = _host_cell(ox, xs[i - 1])
-                jh, fy = _host_cell(oy, ys[j - 1])
-                kh, fz = _host_cell(oz, zs[k - 1])
-                donee.append((b, i, j, k))
-                host.append((other, ih + 1, jh + 1, kh + 1))
-                coef.append((fx, fy, fz))
+        faces = []
+        if b < nblocks - 1:
+            faces.append((im, b + 1))
+        if b > 0:
+            faces.append((1, b - 1))
+        for i, other in faces:
+            ox, oy, oz = axes[other]
+            for k in range(1, km + 1):
+                for j in range(1, jm + 1):
+                    ih, fx = _host_cell(ox, xs[i - 1])
+                    jh, fy = _host_cell(oy, ys[j - 1])
+                    kh, fz = _host_cell(oz, zs[k - 1])
+                    donee.append((b, i, j, k))
+                    host.append((other, ih + 1, jh + 1, kh + 1))
+                    coef.append((fx, fy, fz))
     ov = dict(donee=np.array(donee, np.int32).reshape(-1), host=np.array(host, np.int32).reshape(-1),
               coef=np.array(coef, np.float64).reshape(-1), n=len(donee))
     return blocks, ov

@@ -214,6 +214,63 @@ def mg_driver_batch(solvers):
     return [r.as_dict() for r in reps]
 
 
+class OvList:
+    """A point list of a rank's share of a sharded overset exchange
+    (desalm_ov_list_*): host cells with trilinear weights (gather) or donee
+    nodes (scatter) on the given Solvers, values moved through device
+    buffers (integer addresses, e.g. torch's data_ptr())."""
+
+    def __init__(self, solvers, pts, coef=None):
+        self.L = lib()
+        L = self.L
+        L.desalm_ov_list_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.POINTER(C.c_int),
+                                            C.POINTER(C.c_double), C.POINTER(C.c_void_p)]
+        L.desalm_ov_list_create.restype = C.c_int
+        L.desalm_ov_list_destroy.argtypes = [C.c_void_p]
+        L.desalm_ov_list_destroy.restype = None
+        L.desalm_ov_list_last_error.argtypes = [C.c_void_p]
+        L.desalm_ov_list_last_error.restype = C.c_char_p
+        L.desalm_ov_list_fields.argtypes = [C.c_void_p, C.c_int]
+        L.desalm_ov_list_fields.restype = C.c_int
+        L.desalm_ov_list_gather.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        L.desalm_ov_list_gather.restype = C.c_int
+        L.desalm_ov_list_scatter.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        L.desalm_ov_list_scatter.restype = C.c_int
+        self.solvers = list(solvers)
+        self._pts = np.ascontiguousarray(np.asarray(pts, np.int32).reshape(-1, 4))
+        self.n = len(self._pts)
+        self._coef = None if coef is None else np.ascontiguousarray(np.asarray(coef, np.float64).reshape(-1, 3))
+        arr = (C.c_void_p * len(self.solvers))(*[s.ctx.value for s in self.solvers])
+        self.h = C.c_void_p()
+        pc = self._coef.ctypes.data_as(C.POINTER(C.c_double)) if self._coef is not None else None
+        rc = L.desalm_ov_list_create(arr, len(self.solvers), self.n, self._pts.ctypes.data_as(C.POINTER(C.c_int)), pc,
+                                     C.byref(self.h))
+        if rc:
+            raise DesalmError("desalm_ov_list_create failed (%d)" % rc)
+
+    def _ck(self, rc, what):
+        if rc < 0:
+            raise DesalmError("%s failed (%d): %s" % (what, rc, self.L.desalm_ov_list_last_error(self.h).decode()))
+        return rc
+
+    def fields(self, what):
+        return self._ck(self.L.desalm_ov_list_fields(self.h, int(what)), "ov_list_fields")
+
+    def gather(self, what, out_ptr):
+        self._ck(self.L.desalm_ov_list_gather(self.h, int(what), C.c_void_p(int(out_ptr))), "ov_list_gather")
+
+    def scatter(self, what, in_ptr):
+        self._ck(self.L.desalm_ov_list_scatter(self.h, int(what), C.c_void_p(int(in_ptr))), "ov_list_scatter")
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.L.desalm_ov_list_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+
 class Overset:
     """Overset blocks (desalm_overset_*): Solvers on one GPU coupled by a
     donor map (see cases.overset_pair)."""

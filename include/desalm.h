@@ -290,6 +290,32 @@ int  desalm_overset_exchange(desalm_overset* ov, int what);
  * report.  Blocks step eagerly (no CUDA graph). */
 int  desalm_overset_mg_driver(desalm_overset* ov, desalm_step_report* reps);
 
+/* Overset blocks sharded across processes (one GPU each): a rank steps the
+ * blocks it owns and exchanges donor values with the other ranks, as the
+ * reference fills a send buffer per destination, calls mpi_alltoallv and
+ * writes what it receives (src/mg_bintp_mom.F90:60-160,
+ * src/mg_bintp_tur.F90).  A list is n points on blocks of this process:
+ * pts[4 p + 0] the block (index into ctxs), pts[4 p + 1..3] its 1-based
+ * i, j, k.  With weights (coef[3 p + 0..2] = xco, yco, zco) the points are
+ * host cells (lower corners) and desalm_ov_list_gather writes the
+ * trilinear interpolation of the fields `what` selects (0: q(1..4); 1: the
+ * turbulence scalars, nu_tilde or k and omega) to out, point-major,
+ * desalm_ov_list_fields(l, what) values per point; without weights they are
+ * donee nodes and desalm_ov_list_scatter writes in's values into them.  out
+ * and in are device memory of the blocks' GPU; each call returns when its
+ * kernel is done, ordered after the blocks' queued work and before their
+ * next.  A host cell must have all eight corners in its block.  Which points
+ * go to which rank, and the transfer itself (NCCL), are the caller's: see
+ * desalm/overset_dist.py. */
+typedef struct desalm_ov_list desalm_ov_list;
+int  desalm_ov_list_create(desalm_ctx* const* ctxs, int nctx, int n, const int* pts, const double* coef,
+                           desalm_ov_list** out);
+void desalm_ov_list_destroy(desalm_ov_list* l);
+const char* desalm_ov_list_last_error(const desalm_ov_list* l);
+int  desalm_ov_list_fields(const desalm_ov_list* l, int what);
+int  desalm_ov_list_gather(desalm_ov_list* l, int what, double* out);
+int  desalm_ov_list_scatter(desalm_ov_list* l, int what, const double* in);
+
 /* Kernel of each level's DAF line sweeps, nl[3 * level + direction]
  * (directions i, j, k; 0 for levels the case does not have):
  *   2  lines of at most 32 rows: warp-shuffle cyclic reduction, one warp per

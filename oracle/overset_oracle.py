@@ -1,5 +1,5 @@
 """Overset blocks on the CPU oracle: the donor exchange and the multi-zone
-physical step.
+physical step, and one rank's exchange of a sharded run (DistExchange).
 
 TEST INFRASTRUCTURE ONLY: used by tests/ as the checker of the library's
 desalm_overset_* entry points; the product never loads it.
@@ -133,3 +133,52 @@ def mg_driver(blocks, ov):
         ermax = (res[1:4] - init[1:4]).max()
         conv = (itc > c.it_min and ermax < c.er_min) or (itc > c.it_min and eomax < c.eo_min)
     return {"iterations": itc, "converged": conv, "residual": list(res), "init_residual": list(init)}
+
+
+class DistExchange:
+    """exchange() for one rank of a sharded run (desalm.overset_dist): the
+    values this rank's host cells owe to each rank, interpolated with the
+    weights and in the summation order of exchange(), packed point-major in
+    the Partition's send order, crossed by overset_dist.transfer (gloo), and
+    written into this rank's donee nodes.  blocks: this rank's oracle
+    blocks in part.local_blocks order."""
+
+    def __init__(self, part, blocks, dist):
+        self.part, self.blocks, self.dist = part, blocks, dist
+        self.turbulence = blocks[0].case.turbulence
+
+    def __call__(self, what):
+        import torch
+        from desalm.overset_dist import transfer
+        fields = [0, 1, 2, 3] if what == 0 else TURB_FIELDS[self.turbulence]
+        nf = len(fields)
+        if nf == 0:
+            return
+        part, blocks = self.part, self.blocks
+        gp, gc = part.gather_pts, part.gather_coef
+        w = _weights(gc) if len(gc) else []
+        offs = [(0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1), (1, 0, 1), (0, 1, 1), (1, 1, 0), (1, 1, 1)]
+        send = np.zeros(max(1, len(gp) * nf))
+        for fi, f in enumerate(fields):
+            data = [_get(b, f) for b in blocks]
+            for e in range(len(gp)):
+                lb, ih, jh, kh = gp[e]
+                c = blocks[lb].case
+                v = data[lb]
+                acc = 0.0
+                for t, (a, bb, cc) in enumerate(offs):
+                    acc = acc + v[(ih - 1 + a) + c.im * ((jh - 1 + bb) + c.jm * (kh - 1 + cc))] * w[t][e]
+                send[e * nf + fi] = acc
+        sp = part.scatter_pts
+        st = torch.from_numpy(send)
+        rt = torch.zeros(max(1, len(sp) * nf), dtype=torch.float64)
+        transfer(self.dist, part, st, rt, nf)
+        recv = rt.numpy()
+        for fi, f in enumerate(fields):
+            data = [_get(b, f) for b in blocks]
+            for e in range(len(sp)):
+                lb, i, j, k = sp[e]
+                c = blocks[lb].case
+                data[lb][(i - 1) + c.im * ((j - 1) + c.jm * (k - 1))] = recv[e * nf + fi]
+            for lb, blk in enumerate(blocks):
+                _set(blk, f, data[lb])
