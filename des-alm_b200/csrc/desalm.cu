@@ -445,7 +445,8 @@ dim3 blk_t(const desalm_ctx* ctx, int lvl, int which) {
 }
 dim3 grid_t(const desalm_ctx* ctx, int lvl, int which, int im, int jm, int km) {
   const unsigned* t = ctx->tile[lvl][which];
-  return dim3(cdiv(im - 2, t[0]), cdiv(jm - 2, t[1]), cdiv(km - 2, t[2]));
+  const int kl = which < 2 ? DESALM_KR_KLOOP : 1;   // a K_R thread takes DESALM_KR_KLOOP k planes
+  return dim3(cdiv(im - 2, t[0]), cdiv(jm - 2, t[1]), cdiv(km - 2, t[2] * kl));
 }
 
 // One DAF line sweep as k_sweep4 with the widest slab (lines per CTA) whose
@@ -895,10 +896,7 @@ int tune_tile(desalm_ctx* ctx, Lv<T, W>& L, int lvl, int which, cudaEvent_t e0, 
     const dim3 g = grid_t(ctx, lvl, which, L.im, L.jm, L.km), b = blk_t(ctx, lvl, which);
     if (which == 0) return launch_k(k_resid<T, W, 0>, g, b, 0, s, L, P, lvl > 0 ? 1 : 0, 0, lvl > 0 ? 1 : 0, 0);
     if (which == 1) return launch_k(k_resid<T, W, 1>, g, b, 0, s, L, P, lvl == 0 ? 2 : 1, 0, lvl > 0 ? 1 : 0, 0);
-    if constexpr (std::is_same<T, double>::value) {
-      if (ctx->c.turbulence == 2) return launch_k(k_kw_rhs<W>, g, b, 0, s, make_kw<W>(ctx, L));
-      return launch_k(k_sa_rhs<W>, g, b, 0, s, make_sa<W>(ctx, L));
-    }
+    if constexpr (std::is_same<T, double>::value) return launch_k(k_sa_rhs<W>, g, b, 0, s, make_sa<W>(ctx, L));
     return cudaSuccess;
   };
   float best = 0.f;
@@ -922,7 +920,8 @@ template <class T, class W>
 int tune_tiles_level(desalm_ctx* ctx, Lv<T, W>& L, int lvl, cudaEvent_t e0, cudaEvent_t e1) {
   RET((tune_tile<T, W>(ctx, L, lvl, 0, e0, e1)));
   RET((tune_tile<T, W>(ctx, L, lvl, 1, e0, e1)));
-  if (lvl == 0 && ctx->c.turbulence) RET((tune_tile<T, W>(ctx, L, lvl, 2, e0, e1)));
+  // the SA residual's tile (k-omega's residual has its own fixed tile, KWF_*)
+  if (lvl == 0 && ctx->c.turbulence == 1) RET((tune_tile<T, W>(ctx, L, lvl, 2, e0, e1)));
   return 0;
 }
 
@@ -2580,7 +2579,7 @@ int kw_run(desalm_ctx* ctx, Lv<double, W>& L) {
   LAUNCH(KC_SA_AUX, 0, L.N, launch_k(k_sa_ucn<W>, cdiv(L.N, 256), 256, 0, s, K.S));
   LAUNCH(KC_SA_AUX, 0, L.N, launch_k(k_kw_pre<W>, cdiv(L.N, 256), 256, 0, s, K));
   for (int it = 0; it < ctx->c.itk; ++it) {
-    LAUNCH(KC_SA_RHS, 0, nin, launch_k(k_kw_rhs<W>, grid_t(ctx, 0, 2, L.im, L.jm, L.km), blk_t(ctx, 0, 2), 0, s, K));
+    LAUNCH(KC_SA_RHS, 0, nin, launch_k(k_kw_rhs<W>, dim3(cdiv(L.im - 2, KWF_TX), cdiv(L.jm - 2, KWF_TY), cdiv(L.km - 2, KWF_TZ)), 256, 0, s, K));
     // k's and omega's line solves are independent (each has its own rows and
     // right-hand side from k_kw_rhs and updates its own field in its k
     // sweep), so they run together direction by direction

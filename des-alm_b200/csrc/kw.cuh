@@ -182,26 +182,73 @@ DESALM_DEV void kw_adi_rows(const KwT<SW>& K, int l, int d, double gm, double gp
   K.cow[3 * d + 2][l] = SW(dw * ce);
 }
 
-// Minimum resident CTAs per SM requested for k_kw_rhs (128 threads each); a
-// build-time tuning knob.
-#ifndef DESALM_KW_MINBLOCKS
-#define DESALM_KW_MINBLOCKS 3
-#endif
 // One fused pass over the interior of rhs_kw_prod, rhs_kw_viscous,
 // rhs_kw_flux, rhs_kw_unst_visc and rhs_kw_implicit_source, giving the
 // right-hand sides of k and omega already divided by dk and dw (the i sweep's
-// input), and the ADI rows of both scalars.
+// input), and the ADI rows of both scalars, with every face flux formed once
+// (a kernel of one thread per node forms each face twice, once for each of
+// its nodes: 5% slower on the turbine box).  A CTA covers a tile of
+// 31 x 4 x 2 nodes with 32 x 4 x 2 threads.
+//   phase 1  lane L of row y, plane z forms the i face between nodes
+//            i0 + L - 1 and i0 + L; the tile's j faces (5 rows of 31, both
+//            planes) and k faces (3 planes of 4 x 31) are shared out over
+//            all threads; each face's viscous and convective fluxes of k and
+//            omega and its diffusive ADI coefficient go to shared memory
+//            (component-major, so that neighbouring lanes read neighbouring
+//            words);
+//   phase 2  thread (L < 31, y, z) adds its node's six faces (i, j, k; plus
+//            face minus minus face, viscous then convective) and finishes the
+//            node.
+constexpr int KWF_TX = 31, KWF_TY = 4, KWF_TZ = 2;
 template <class SW>
-__global__ void __launch_bounds__(128, DESALM_KW_MINBLOCKS) k_kw_rhs(KwT<SW> K) {
+__global__ void __launch_bounds__(256, 2) k_kw_rhs(KwT<SW> K) {
   pdl_wait();
   const SaT<SW>& S = K.S;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
-  if (i > S.im - 2 || j > S.jm - 2 || k > S.km - 2) return;
+  __shared__ double s_fi[5][KWF_TZ][KWF_TY][32];
+  __shared__ double s_fj[5][KWF_TZ][KWF_TY + 1][KWF_TX];
+  __shared__ double s_fk[5][KWF_TZ + 1][KWF_TY][KWF_TX];
+  const int L = threadIdx.x & 31, y = (threadIdx.x >> 5) & 3, z = threadIdx.x >> 7;
+  const int i0 = blockIdx.x * KWF_TX + 1, j0 = blockIdx.y * KWF_TY + 1, k0 = blockIdx.z * KWF_TZ + 1;
   const int sj = S.sj, sk = S.sk;
+  const int ni = S.im - 2, nj = S.jm - 2, nk = S.km - 2;
+  const double rei = 1.0 / S.ren;
+  // the face of direction dir whose lower node is l0 into component slots
+  // c * cs of out (c = 0, 1: viscous k, omega; 2: diffusive coefficient;
+  // 3, 4: convective k, omega)
+  auto face = [&](int dir, int l0, double* out, int cs) {
+    const int stp = dir == 0 ? 1 : (dir == 1 ? sj : sk);
+    double fv[2], fc[2], g;
+    kw_visc_face(K, dir, l0, rei, fv, &g);
+    kw_conv_face(K, dir, l0, stp, fc);
+    out[0] = fv[0];
+    out[cs] = fv[1];
+    out[2 * cs] = g;
+    out[3 * cs] = fc[0];
+    out[4 * cs] = fc[1];
+  };
+  constexpr int CI = KWF_TZ * KWF_TY * 32, CJ = KWF_TZ * (KWF_TY + 1) * KWF_TX, CK = (KWF_TZ + 1) * KWF_TY * KWF_TX;
+  {
+    const int i = i0 + L - 1, j = j0 + y, k = k0 + z;
+    if (i <= ni && j <= nj && k <= nk) face(0, i + sj * j + sk * k, &s_fi[0][z][y][L], CI);
+  }
+  for (int f = threadIdx.x; f < CJ + CK; f += 256) {
+    if (f < CJ) {
+      const int x = f % KWF_TX, r = f / KWF_TX, yy = r % (KWF_TY + 1), zz = r / (KWF_TY + 1);
+      const int i = i0 + x, j = j0 + yy - 1, k = k0 + zz;
+      if (i <= ni && j <= nj && k <= nk) face(1, i + sj * j + sk * k, &s_fj[0][zz][yy][x], CJ);
+    } else {
+      const int g = f - CJ;
+      const int x = g % KWF_TX, r = g / KWF_TX, yy = r % KWF_TY, zz = r / KWF_TY;
+      const int i = i0 + x, j = j0 + yy, k = k0 + zz - 1;
+      if (i <= ni && j <= nj && k <= nk) face(2, i + sj * j + sk * k, &s_fk[0][zz][yy][x], CK);
+    }
+  }
+  __syncthreads();
+  if (L >= KWF_TX) return;
+  const int i = i0 + L, j = j0 + y, k = k0 + z;
+  if (i > ni || j > nj || k > nk) return;
   const int l = i + sj * j + sk * k;
-  const double cw2 = 0.075, rei = 1.0 / S.ren;
+  const double cw2 = 0.075;
   const double kv = S.q[4][l], wv = K.om[l], aj = S.aj[l];
   // rhs_kw_prod (src/rhs_kw_prod.F90:18-31)
   const double pkw1a = K.Bs[l] * wv * kv;
@@ -209,21 +256,26 @@ __global__ void __launch_bounds__(128, DESALM_KW_MINBLOCKS) k_kw_rhs(KwT<SW> K) 
   const double pkw2a = -K.Ac[l] * wv * K.ptke[l] / kv;
   const double pkw2b = cw2 * wv * wv;
   const double pk2 = (pkw2a + pkw2b) / aj;
-  // viscous and convective face fluxes; each face also gives what the ADI
-  // rows of its direction need (diffusive coefficient, U/J pair)
-  double v[2] = {0, 0}, r[2] = {0, 0}, fp[2], fm[2];
+  double v[2] = {0, 0}, r[2] = {0, 0};
   double gdm[3], gdp[3], ucm[3][2], ucp[3][2];
   const int st[3] = {1, sj, sk};
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    kw_visc_face(K, d, l, rei, fp, &gdp[d]);
-    kw_visc_face(K, d, l - st[d], rei, fm, &gdm[d]);
+    // the plus face (l | l + s) and the minus face (l - s | l) of direction d
+    const double* fp = d == 0 ? &s_fi[0][z][y][L + 1] : (d == 1 ? &s_fj[0][z][y + 1][L] : &s_fk[0][z + 1][y][L]);
+    const double* fm = d == 0 ? &s_fi[0][z][y][L] : (d == 1 ? &s_fj[0][z][y][L] : &s_fk[0][z][y][L]);
+    const int cs = d == 0 ? CI : (d == 1 ? CJ : CK);
     v[0] = v[0] + fp[0] - fm[0];
-    v[1] = v[1] + fp[1] - fm[1];
-    kw_conv_face(K, d, l, st[d], fp, ucp[d]);
-    kw_conv_face(K, d, l - st[d], st[d], fm, ucm[d]);
-    r[0] = r[0] + fp[0] - fm[0];
-    r[1] = r[1] + fp[1] - fm[1];
+    v[1] = v[1] + fp[cs] - fm[cs];
+    r[0] = r[0] + fp[3 * cs] - fm[3 * cs];
+    r[1] = r[1] + fp[4 * cs] - fm[4 * cs];
+    gdp[d] = fp[2 * cs];
+    gdm[d] = fm[2 * cs];
+    const double u0 = S.uc[d][l];
+    ucm[d][0] = S.uc[d][l - st[d]];
+    ucm[d][1] = u0;
+    ucp[d][0] = u0;
+    ucp[d][1] = S.uc[d][l + st[d]];
   }
   // rhs_kw_unst_visc (src/rhs_kw_unst_visc.F90:23-37)
   const double dtj = 2.0 * S.delti * aj;

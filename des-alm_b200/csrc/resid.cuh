@@ -112,14 +112,17 @@ DESALM_DEV T diss_fv(const Lv<T, W>& L, int dir, int l, int st, T dsq) {
 #endif
 #define DESALM_KR_BZ (4 / DESALM_KR_BY)
 
-// MODE 0: first pass of a DAF step; MODE 1: recalculation for restriction.
+// k planes a thread of K_R takes in turn (the CTA tile's k extent apart), so
+// that the neighbour planes it has just read are still in L1 for the next;
+// a build-time tuning knob.
+#ifndef DESALM_KR_KLOOP
+#define DESALM_KR_KLOOP 2
+#endif
+
+// The residual of interior node (i, j, k); MODE 0: first pass of a DAF step;
+// MODE 1: recalculation for restriction.
 template <class T, class W, int MODE>
-__global__ void __launch_bounds__(128, DESALM_KR_MINBLOCKS) k_resid(Lv<T, W> L, Par P, int upwind, int calc_pk, int coarse, int bback) {
-  pdl_wait();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
-  if (i > L.im - 2 || j > L.jm - 2 || k > L.km - 2) return;
+DESALM_DEV void resid_node(const Lv<T, W>& L, const Par& P, int upwind, int calc_pk, int coarse, int bback, int i, int j, int k) {
   const int sj = L.sj, sk = L.sk;
   const int l = i + sj * j + sk * k;
   const T rei = T(1) / T(P.ren);
@@ -312,6 +315,20 @@ __global__ void __launch_bounds__(128, DESALM_KR_MINBLOCKS) k_resid(Lv<T, W> L, 
     L.tc[d][l] = tcv[d];
     L.hc[d][l] = hcv[d];
     if (pos[d] == 1 || pos[d] == ext[d] - 2) L.hc[d][pos[d] == 1 ? l - st[d] : l + st[d]] = hcb[d];
+  }
+}
+
+template <class T, class W, int MODE>
+__global__ void __launch_bounds__(128, DESALM_KR_MINBLOCKS) k_resid(Lv<T, W> L, Par P, int upwind, int calc_pk, int coarse, int bback) {
+  pdl_wait();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  if (i > L.im - 2 || j > L.jm - 2) return;
+#pragma unroll 1
+  for (int kk = 0; kk < DESALM_KR_KLOOP; ++kk) {
+    const int k = (blockIdx.z * DESALM_KR_KLOOP + kk) * blockDim.z + threadIdx.z + 1;
+    if (k > L.km - 2) return;
+    resid_node<T, W, MODE>(L, P, upwind, calc_pk, coarse, bback, i, j, k);
   }
 }
 

@@ -344,11 +344,12 @@ int  desalm_turb_sweep_widths(desalm_ctx* ctx, int nl[3]);
 int  desalm_set_sweep_widths(desalm_ctx* ctx, const int nl[12], const int turb[3]);
 /* CTA tile (threads along i, j, k; 128 in all) of each level's residual
  * kernels, tiles[9 * level + 3 * kernel + axis], kernel 0 = the first
- * residual pass (K_R), 1 = the recalculated residual, 2 = the turbulence
- * residual (fine level only): timed at eight tiles when the grid is set and
- * the fastest kept, or 32 x 4 x 1 where the timing is off (DESALM_AUTOTUNE=0).
- * The tile changes the time only: every node is computed by the same
- * operations. */
+ * residual pass (K_R), 1 = the recalculated residual, 2 = the SA residual
+ * (fine level only; the k-omega residual has a fixed tile of 31 x 4 x 2
+ * nodes): timed at eight tiles when the grid is set and the fastest kept, or
+ * 32 x 4 x 1 where the timing is off (DESALM_AUTOTUNE=0).  Each K_R thread
+ * computes two nodes, k planes apart by the tile's k extent.  The tile
+ * changes the time only: every node is computed by the same operations. */
 int  desalm_kernel_tiles(desalm_ctx* ctx, int tiles[36]);
 /* One pseudo-time iteration of the loop above (for callers that drive the
  * loop themselves); rep->residual receives the iteration's residual. */
