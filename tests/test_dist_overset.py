@@ -6,7 +6,8 @@ pseudo-iterations, report the same combined residual and leave every block
 with the same values, bit for bit, as the single-process oracle driver
 (oracle/overset_oracle.py mg_driver) on the same blocks: the exchange writes
 the same interpolated values and the combined norm is summed in global block
-order whatever the partition."""
+order whatever the partition.  The k-omega case moves omega across ranks with
+k (mg_bintp_tur's turbulence fields)."""
 import os
 import socket
 
@@ -54,19 +55,28 @@ def test_partition_pairs_senders_with_receivers():
 
 def _oracle_blocks(oracle_mod, specs):
     out = []
-    for case, grid, state in specs:
+    for case, grid, state, om in specs:
         o = oracle_mod.OracleSolver(case)
         o.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
         o.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
+        if om is not None:
+            o.set_omega(om["omega"], om["omega_n"], om["omega_nm1"])
         out.append(o)
     return out
 
 
 def _spec(nblocks, turbulence, itmax):
-    specs, ov = cases.overset_chain(nblocks, seed=5, turbulence=turbulence, itmax=itmax)
-    for c, _, _ in specs:
+    """([(case, grid, state, omega or None)], map); turbulence 2 is the
+    SA chain with the k-omega model (cases.with_kw)."""
+    specs, ov = cases.overset_chain(nblocks, seed=5, turbulence=min(turbulence, 1), itmax=itmax)
+    out = []
+    for c, g, st in specs:
+        om = None
+        if turbulence == 2:
+            c, g, st, om = cases.with_kw(c, g, st)
         c.iter[0], c.iter[1], c.iter[2] = 1, 1, 1
-    return specs, ov
+        out.append((c, g, st, om))
+    return out, ov
 
 
 def _worker(rank, world, port, owner, nblocks, turbulence, itmax, q):
@@ -89,14 +99,15 @@ def _worker(rank, world, port, owner, nblocks, turbulence, itmax, q):
         c0 = specs[0][0]
         tnu0 = (c0.im - 2) * (c0.jm - 2) * (c0.km - 2)
         rep = mg_driver(mine, part, oo.DistExchange(part, mine, dist), dist, nblocks, tnu0)
-        states = {b: mine[i].get_state()["q"] for i, b in enumerate(part.local_blocks)}
+        states = {b: (mine[i].get_state()["q"], mine[i].get_omega()["omega"] if turbulence == 2 else None)
+                  for i, b in enumerate(part.local_blocks)}
         q.put((rank, rep, states))
         dist.barrier()
     finally:
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("owner,turbulence", [([0, 1], 1), ([0, 1, 0], 1), ([0, 0, 1], 0)])
+@pytest.mark.parametrize("owner,turbulence", [([0, 1], 1), ([0, 1, 0], 1), ([0, 0, 1], 0), ([1, 0, 0], 2)])
 def test_sharded_step_equals_single_process(owner, turbulence, oracle_mod):
     import overset_oracle as oo
     nblocks, itmax = len(owner), 3
@@ -119,5 +130,7 @@ def test_sharded_step_equals_single_process(owner, turbulence, oracle_mod):
     for rank, rep, states in out:
         assert rep["iterations"] == ref["iterations"]
         assert rep["residual"] == ref["residual"] and rep["init_residual"] == ref["init_residual"]
-        for b, qv in states.items():
+        for b, (qv, wv) in states.items():
             assert np.array_equal(qv, blocks[b].get_state()["q"]), b
+            if wv is not None:
+                assert np.array_equal(wv, blocks[b].get_omega()["omega"]), b
