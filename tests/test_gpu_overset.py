@@ -60,3 +60,35 @@ def test_coupled_step_matches_oracle(precision, oracle_mod):
     if precision == abi.FP64:
         assert np.allclose(rg[0]["residual"][:4], ro["residual"][:4], rtol=0, atol=1e-9)
     X.close()
+
+
+def test_coupled_kw_step_matches_oracle(oracle_mod):
+    """Two k-omega blocks: the turbulence exchange carries k and omega
+    (mg_bintp_tur's fields), FP64, three coupled pseudo-iterations."""
+    import overset_oracle as oo
+    from desalm.solver import Overset, Solver
+    blocks, ov = cases.overset_pair(turbulence=1, itmax=3)
+    gs, os_ = [], []
+    for case, grid, state in blocks:
+        case, grid, state, om = cases.with_kw(case, grid, state)
+        case.er_min = -100.0
+        case.eo_min = -100.0
+        g = Solver(case)
+        o = oracle_mod.OracleSolver(case)
+        for s in (g, o):
+            s.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
+            s.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
+            s.set_omega(om["omega"], om["omega_n"], om["omega_nm1"])
+        gs.append(g)
+        os_.append(o)
+    X = Overset(gs, ov)
+    rg = X.mg_driver()
+    ro = oo.mg_driver(os_, ov)
+    assert rg[0]["iterations"] == ro["iterations"] == 3
+    for g, o in zip(gs, os_):
+        for f in [abi.F_Q + m for m in range(5)] + [abi.F_NUT]:
+            e = rel_l2(g.get_field(1, f), o.get_field(1, f))
+            assert e <= 1e-10, (f, e)
+        e = rel_l2(g.get_omega()["omega"], o.get_omega()["omega"])
+        assert e <= 1e-10, e
+    X.close()
