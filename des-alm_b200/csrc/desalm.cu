@@ -448,6 +448,20 @@ dim3 grid_t(const desalm_ctx* ctx, int lvl, int which, int im, int jm, int km) {
   const int kl = which < 2 ? DESALM_KR_KLOOP : 1;   // a K_R thread takes DESALM_KR_KLOOP k planes
   return dim3(cdiv(im - 2, t[0]), cdiv(jm - 2, t[1]), cdiv(km - 2, t[2] * kl));
 }
+// K_R (MODE 0) or the recalculation (MODE 1) on level lvl: the tile
+// KRF_TX x KRF_TY x KRF_TZ (31 x 4 x 2) is the face-shared k_resid_f, any
+// other the one-node-per-thread k_resid with that CTA shape.  Both compute
+// every node by the same operations.
+template <class T, class W, int MODE>
+cudaError_t launch_resid(const desalm_ctx* ctx, int lvl, cudaStream_t s, const Lv<T, W>& L, const Par& P, int upwind, int calc_pk,
+                         int coarse, int bback) {
+  const unsigned* t = ctx->tile[lvl][MODE];
+  if (t[0] == KRF_TX && t[1] == KRF_TY && t[2] == KRF_TZ)
+    return launch_k(k_resid_f<T, W, MODE>, dim3(cdiv(L.im - 2, KRF_TX), cdiv(L.jm - 2, KRF_TY), cdiv(L.km - 2, KRF_TZ)), 256, 0, s, L, P,
+                    upwind, calc_pk, coarse, bback);
+  return launch_k(k_resid<T, W, MODE>, grid_t(ctx, lvl, MODE, L.im, L.jm, L.km), blk_t(ctx, lvl, MODE), 0, s, L, P, upwind, calc_pk,
+                  coarse, bback);
+}
 
 // One DAF line sweep as k_sweep4 with the widest slab (lines per CTA) whose
 // shared memory leaves room for two CTAs per SM, else the widest that fits
@@ -660,7 +674,7 @@ int launch_daf(desalm_ctx* ctx, Lv<T, W>& L, Level& G, int n, int recalc, int it
            launch_k(k_outlet<T, W>, dim3(cdiv(L.jm - 2, 32), cdiv(L.km - 2, 4)), dim3(32, 4), 0, ctx->side, L, P));
     CKL();
   }
-  LAUNCH(KC_RESID, n, nin, launch_k(k_resid<T, W, 0>, grid_t(ctx, n, 0, L.im, L.jm, L.km), blk_t(ctx, n, 0), 0, s, L, P, upwind, itr == 1 ? 1 : 0, n > 0 ? 1 : 0, bback));
+  LAUNCH(KC_RESID, n, nin, (launch_resid<T, W, 0>(ctx, n, s, L, P, upwind, itr == 1 ? 1 : 0, n > 0 ? 1 : 0, bback)));
   CKL();
   if (out_side) RET(join_side(ctx));
   if (L.oute && !out_side) {
@@ -678,7 +692,7 @@ template <class T, class W>
 int launch_recalc(desalm_ctx* ctx, Lv<T, W>& L, int n) {
   Par P = ctx->par;
   P.fine = (n == 0);
-  LAUNCH(KC_RECALC, n, double(L.im - 2) * (L.jm - 2) * (L.km - 2), launch_k(k_resid<T, W, 1>, grid_t(ctx, n, 1, L.im, L.jm, L.km), blk_t(ctx, n, 1), 0, ctx->stream, L, P, n == 0 ? 2 : 1, 0, n > 0 ? 1 : 0, 0));
+  LAUNCH(KC_RECALC, n, double(L.im - 2) * (L.jm - 2) * (L.km - 2), (launch_resid<T, W, 1>(ctx, n, ctx->stream, L, P, n == 0 ? 2 : 1, 0, n > 0 ? 1 : 0, 0)));
   CKL();
   return 0;
 }
@@ -880,7 +894,9 @@ template <class SW, class W> SaT<SW> make_sa(desalm_ctx* ctx, Lv<double, W>& L);
 template <class W> KwT<W> make_kw(desalm_ctx* ctx, Lv<double, W>& L);
 
 // CTA tiles of 128 threads the residual kernels are timed with
-constexpr unsigned kTiles[8][3] = {{32, 4, 1}, {32, 2, 2}, {32, 1, 4}, {64, 2, 1}, {64, 1, 2}, {128, 1, 1}, {16, 8, 1}, {16, 4, 2}};
+// the last is the face-shared K_R tile (k_resid_f), tried for kernels 0 and 1 only
+constexpr unsigned kTiles[9][3] = {{32, 4, 1}, {32, 2, 2}, {32, 1, 4}, {64, 2, 1}, {64, 1, 2}, {128, 1, 1}, {16, 8, 1}, {16, 4, 2},
+                                   {KRF_TX, KRF_TY, KRF_TZ}};
 
 // Times one residual kernel (which: 0 = K_R, 1 = recalculation, 2 =
 // turbulence residual) on level lvl at every tile and keeps the fastest.
@@ -894,14 +910,14 @@ int tune_tile(desalm_ctx* ctx, Lv<T, W>& L, int lvl, int which, cudaEvent_t e0, 
   cudaStream_t s = ctx->stream;
   auto run = [&]() -> cudaError_t {
     const dim3 g = grid_t(ctx, lvl, which, L.im, L.jm, L.km), b = blk_t(ctx, lvl, which);
-    if (which == 0) return launch_k(k_resid<T, W, 0>, g, b, 0, s, L, P, lvl > 0 ? 1 : 0, 0, lvl > 0 ? 1 : 0, 0);
-    if (which == 1) return launch_k(k_resid<T, W, 1>, g, b, 0, s, L, P, lvl == 0 ? 2 : 1, 0, lvl > 0 ? 1 : 0, 0);
+    if (which == 0) return launch_resid<T, W, 0>(ctx, lvl, s, L, P, lvl > 0 ? 1 : 0, 0, lvl > 0 ? 1 : 0, 0);
+    if (which == 1) return launch_resid<T, W, 1>(ctx, lvl, s, L, P, lvl == 0 ? 2 : 1, 0, lvl > 0 ? 1 : 0, 0);
     if constexpr (std::is_same<T, double>::value) return launch_k(k_sa_rhs<W>, g, b, 0, s, make_sa<W>(ctx, L));
     return cudaSuccess;
   };
   float best = 0.f;
   int pick = -1;
-  for (int t = 0; t < 8; ++t) {
+  for (int t = 0; t < (which < 2 ? 9 : 8); ++t) {
     for (int d = 0; d < 3; ++d) ctx->tile[lvl][which][d] = kTiles[t][d];
     CK(run());
     CK(cudaEventRecord(e0, s));

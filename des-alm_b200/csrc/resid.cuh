@@ -83,9 +83,12 @@ DESALM_DEV void visc_face(const Lv<T, W>& L, int dir, int l0, T rei, T out[3]) {
     k1 = c1 * a1 + c2 * a2 + c3 * a3; k2 = c1 * b1 + c2 * b2 + c3 * b3; k3 = c1 * c1 + c2 * c2 + c3 * c3;
   }
   T vtj = T(0.25) * ((rei + L.nut[l1]) + (rei + L.nut[l0])) / (L.aj[l1] + L.aj[l0]);
-  out[0] = vtj * (n1 * uu1 + n2 * vv1 + n3 * ww1 + k1 * U[0] + k2 * E[0] + k3 * Z[0]);
-  out[1] = vtj * (n1 * uu2 + n2 * vv2 + n3 * ww2 + k1 * U[1] + k2 * E[1] + k3 * Z[1]);
-  out[2] = vtj * (n1 * uu3 + n2 * vv3 + n3 * ww3 + k1 * U[2] + k2 * E[2] + k3 * Z[2]);
+  // the flux is rounded here (mulw), so a node's difference of its two face
+  // fluxes is the same whether the faces were formed in registers (k_resid)
+  // or came from shared memory (k_resid_f)
+  out[0] = mulw(vtj, n1 * uu1 + n2 * vv1 + n3 * ww1 + k1 * U[0] + k2 * E[0] + k3 * Z[0]);
+  out[1] = mulw(vtj, n1 * uu2 + n2 * vv2 + n3 * ww2 + k1 * U[1] + k2 * E[1] + k3 * Z[1]);
+  out[2] = mulw(vtj, n1 * uu3 + n2 * vv3 + n3 * ww3 + k1 * U[2] + k2 * E[2] + k3 * Z[2]);
 }
 
 // Second difference of the pressure scaled by g_dd dtau / J at node l
@@ -121,8 +124,11 @@ DESALM_DEV T diss_fv(const Lv<T, W>& L, int dir, int l, int st, T dsq) {
 
 // The residual of interior node (i, j, k); MODE 0: first pass of a DAF step;
 // MODE 1: recalculation for restriction.
-template <class T, class W, int MODE>
-DESALM_DEV void resid_node(const Lv<T, W>& L, const Par& P, int upwind, int calc_pk, int coarse, int bback, int i, int j, int k) {
+// VGIVEN: the viscous terms come in vg (k_resid_f forms them from face
+// fluxes computed once per face).
+template <class T, class W, int MODE, bool VGIVEN = false>
+DESALM_DEV void resid_node(const Lv<T, W>& L, const Par& P, int upwind, int calc_pk, int coarse, int bback, int i, int j, int k,
+                           const T* vg = nullptr) {
   const int sj = L.sj, sk = L.sk;
   const int l = i + sj * j + sk * k;
   const T rei = T(1) / T(P.ren);
@@ -133,20 +139,23 @@ DESALM_DEV void resid_node(const Lv<T, W>& L, const Par& P, int upwind, int calc
 
   // ---- viscous terms
   T visc[3];
-  {
+  if constexpr (VGIVEN) {
+#pragma unroll
+    for (int m = 0; m < 3; ++m) visc[m] = vg[m];
+  } else {
     T fp[3], fm[3];
     visc_face(L, 0, l, rei, fp);
     visc_face(L, 0, l - 1, rei, fm);
 #pragma unroll
-    for (int m = 0; m < 3; ++m) visc[m] = L.dc * (fp[m] - fm[m]);
+    for (int m = 0; m < 3; ++m) visc[m] = mulw(L.dc, fp[m] - fm[m]);
     visc_face(L, 1, l, rei, fp);
     visc_face(L, 1, l - sj, rei, fm);
 #pragma unroll
-    for (int m = 0; m < 3; ++m) visc[m] = visc[m] + L.de * (fp[m] - fm[m]);
+    for (int m = 0; m < 3; ++m) visc[m] = fmaw(L.de, fp[m] - fm[m], visc[m]);
     visc_face(L, 2, l, rei, fp);
     visc_face(L, 2, l - sk, rei, fm);
 #pragma unroll
-    for (int m = 0; m < 3; ++m) visc[m] = visc[m] + L.dz * (fp[m] - fm[m]);
+    for (int m = 0; m < 3; ++m) visc[m] = fmaw(L.dz, fp[m] - fm[m], visc[m]);
   }
 
   // ---- pressure dissipation (first pass only; the recalculation reuses it)
@@ -330,6 +339,64 @@ __global__ void __launch_bounds__(128, DESALM_KR_MINBLOCKS) k_resid(Lv<T, W> L, 
     if (k > L.km - 2) return;
     resid_node<T, W, MODE>(L, P, upwind, calc_pk, coarse, bback, i, j, k);
   }
+}
+
+// K_R with every viscous face flux formed once (k_resid forms each twice,
+// once for each of its nodes): a CTA of 32 x 4 x 2 threads covers 31 x 4 x 2
+// nodes.  Phase 1: lane L of row y, plane z forms the i face between nodes
+// i0 + L - 1 and i0 + L, and the tile's j faces (5 rows of 31, both planes)
+// and k faces (3 planes of 4 x 31) are shared out over all threads, their
+// three momentum fluxes into shared memory (component-major).  Phase 2:
+// thread (L < 31, y, z) forms its node's viscous terms from its six faces in
+// k_resid's order and finishes the node with resid_node.
+constexpr int KRF_TX = 31, KRF_TY = 4, KRF_TZ = 2;
+template <class T, class W, int MODE>
+__global__ void __launch_bounds__(256, 2) k_resid_f(Lv<T, W> L, Par P, int upwind, int calc_pk, int coarse, int bback) {
+  pdl_wait();
+  __shared__ T s_fi[3][KRF_TZ][KRF_TY][32];
+  __shared__ T s_fj[3][KRF_TZ][KRF_TY + 1][KRF_TX];
+  __shared__ T s_fk[3][KRF_TZ + 1][KRF_TY][KRF_TX];
+  const int Ln = threadIdx.x & 31, y = (threadIdx.x >> 5) & 3, z = threadIdx.x >> 7;
+  const int i0 = blockIdx.x * KRF_TX + 1, j0 = blockIdx.y * KRF_TY + 1, k0 = blockIdx.z * KRF_TZ + 1;
+  const int sj = L.sj, sk = L.sk;
+  const int ni = L.im - 2, nj = L.jm - 2, nk = L.km - 2;
+  const T rei = T(1) / T(P.ren);
+  constexpr int CI = KRF_TZ * KRF_TY * 32, CJ = KRF_TZ * (KRF_TY + 1) * KRF_TX, CK = (KRF_TZ + 1) * KRF_TY * KRF_TX;
+  auto face = [&](int dir, int l0, T* out, int cs) {
+    T f[3];
+    visc_face(L, dir, l0, rei, f);
+    out[0] = f[0];
+    out[cs] = f[1];
+    out[2 * cs] = f[2];
+  };
+  {
+    const int i = i0 + Ln - 1, j = j0 + y, k = k0 + z;
+    if (i <= ni && j <= nj && k <= nk) face(0, i + sj * j + sk * k, &s_fi[0][z][y][Ln], CI);
+  }
+  for (int f = threadIdx.x; f < CJ + CK; f += 256) {
+    if (f < CJ) {
+      const int x = f % KRF_TX, r = f / KRF_TX, yy = r % (KRF_TY + 1), zz = r / (KRF_TY + 1);
+      const int i = i0 + x, j = j0 + yy - 1, k = k0 + zz;
+      if (i <= ni && j <= nj && k <= nk) face(1, i + sj * j + sk * k, &s_fj[0][zz][yy][x], CJ);
+    } else {
+      const int g = f - CJ;
+      const int x = g % KRF_TX, r = g / KRF_TX, yy = r % KRF_TY, zz = r / KRF_TY;
+      const int i = i0 + x, j = j0 + yy, k = k0 + zz - 1;
+      if (i <= ni && j <= nj && k <= nk) face(2, i + sj * j + sk * k, &s_fk[0][zz][yy][x], CK);
+    }
+  }
+  __syncthreads();
+  if (Ln >= KRF_TX) return;
+  const int i = i0 + Ln, j = j0 + y, k = k0 + z;
+  if (i > ni || j > nj || k > nk) return;
+  T visc[3];
+#pragma unroll
+  for (int m = 0; m < 3; ++m) visc[m] = mulw(L.dc, s_fi[m][z][y][Ln + 1] - s_fi[m][z][y][Ln]);
+#pragma unroll
+  for (int m = 0; m < 3; ++m) visc[m] = fmaw(L.de, s_fj[m][z][y + 1][Ln] - s_fj[m][z][y][Ln], visc[m]);
+#pragma unroll
+  for (int m = 0; m < 3; ++m) visc[m] = fmaw(L.dz, s_fk[m][z + 1][y][Ln] - s_fk[m][z][y][Ln], visc[m]);
+  resid_node<T, W, MODE, true>(L, P, upwind, calc_pk, coarse, bback, i, j, k, visc);
 }
 
 // dtau on every node (src/rhs_daf_dtau.F90:85-117): the smallest of the

@@ -348,8 +348,11 @@ int  desalm_set_sweep_widths(desalm_ctx* ctx, const int nl[12], const int turb[3
  * (fine level only; the k-omega residual has a fixed tile of 31 x 4 x 2
  * nodes): timed at eight tiles when the grid is set and the fastest kept, or
  * 32 x 4 x 1 where the timing is off (DESALM_AUTOTUNE=0).  Each K_R thread
- * computes two nodes, k planes apart by the tile's k extent.  The tile
- * changes the time only: every node is computed by the same operations. */
+ * computes two nodes, k planes apart by the tile's k extent.  Kernels 0 and
+ * 1 are also timed as the face-shared kernel, reported as the tile
+ * 31 x 4 x 2 (256 threads, each viscous face flux formed once for the two
+ * nodes beside it).  The tile changes the time only: every node is computed
+ * by the same operations. */
 int  desalm_kernel_tiles(desalm_ctx* ctx, int tiles[36]);
 /* One pseudo-time iteration of the loop above (for callers that drive the
  * loop themselves); rep->residual receives the iteration's residual. */
