@@ -29,6 +29,7 @@
 #include "kw.cuh"
 #include "outlet.cuh"
 #include "wallfn.cuh"
+#include "rfg.cuh"
 
 using namespace desalm;
 
@@ -239,6 +240,13 @@ struct desalm_ctx {
   int gss = 0;
   SaWork sa{};
   KwWork kw{};                // k-omega work (turbulence = 2)
+  struct {
+    bool on = false;
+    bool armed = false;               // desalm_rfg_inlet forced the plane since the last begin_step
+    double time = 0.0;                // the time it was forced for
+    RfgDev dev{};
+    std::vector<void*> allocs;        // the generator's device tables
+  } rfg;                      // synthetic inflow turbulence (rfg_inlet)
   int recalc = 0;             // decide_recalc_rh of the pseudo-iteration being enqueued
   double ckin = 1.0e-10, cein = 1.0e-6;  // k and omega floors on extrapolated faces
   // per-kernel CUDA-event timing (desalm_profile) and launch counter
@@ -1095,6 +1103,7 @@ void outlet_ratios(const desalm_case& c, const double* x, const double* y, const
 
 int pseudo_iter(desalm_ctx* ctx, desalm_step_report* rep);
 int enqueue_iteration(desalm_ctx* ctx);
+int rfg_launch(desalm_ctx* ctx, double time);
 int graph_step(desalm_ctx* ctx, desalm_step_report* rep);
 int graph_launch(desalm_ctx* ctx);
 int graph_finish(desalm_ctx* ctx, desalm_step_report* rep);
@@ -1521,6 +1530,7 @@ void desalm_destroy(desalm_ctx* ctx) {
     for (void* p : G.allocs) cudaFree(p);
   for (void* p : ctx->allocs) cudaFree(p);
   for (void* p : ctx->alm.allocs) cudaFree(p);
+  for (void* p : ctx->rfg.allocs) cudaFree(p);
   for (auto& r : ctx->prof) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
   if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
   if (ctx->graph) cudaGraphDestroy(ctx->graph);
@@ -2111,6 +2121,12 @@ int desalm_begin_step(desalm_ctx* ctx) {
     RET(lp_predict(ctx));
     RET(lp_train_launch(ctx));
   }
+  // The inflow plane that desalm_rfg_inlet forced for this step is an
+  // inflow boundary (velocity held through the step): an extrapolated or
+  // learned guess has overwritten it, so it is forced again for the same time
+  // (the same values, bit for bit).  Under the q^n guess it is untouched.
+  if (ctx->rfg.armed && (c.predictor == DESALM_PRED_LINEAR || learned)) RET(rfg_launch(ctx, ctx->rfg.time));
+  ctx->rfg.armed = false;
   // inject qn, qnm1 to the coarse levels (src/mg_driver.F90:55-58)
   for (int n = 1; n < ctx->ng; ++n) {
     Level& C = ctx->L[n];
@@ -3187,6 +3203,182 @@ int desalm_alm_get(desalm_ctx* ctx, int what, double* out) {
     CK(cudaMemcpyAsync(out, A.falm, 3 * size_t(ctx->L[0].N) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   else { ctx->err = "alm_get: unknown item"; return DESALM_EINVAL; }
   CK(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+}  // extern "C"
+
+// --------------------------------------------- synthetic inflow turbulence
+// The random flow generator (rfg.cuh): desalm_rfg_modes draws the spectrum's
+// modes on the host (initialize_rfg), desalm_rfg_set moves them and the inflow
+// tables to the device and decomposes every node's correlation tensor once
+// (rfg_init), desalm_rfg_inlet sets the inflow plane's velocities for a time
+// (rfg_mpi_inlet_forcing).
+namespace {
+
+// Normal deviates for the mode tables: a splitmix64 stream (Steele, Lea &
+// Flood 2014) of uniform doubles in (0, 1), turned into pairs of normal
+// deviates by the polar method (Marsaglia & Bray 1964), the second of each
+// pair kept for the next call.  The reference draws from its own generator
+// (src/rfg.F90:126-236) with the same polar method and call order.
+struct RfgGauss {
+  uint64_t s;
+  bool have = false;
+  double kept = 0.0;
+  double uniform() {
+    s += 0x9E3779B97F4A7C15ull;
+    uint64_t z = s;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return ((double)(z >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+  }
+  double next(double mean, double stdev) {
+    double g;
+    if (have) {
+      g = kept;
+      have = false;
+    } else {
+      double v1, v2, rsq;
+      do {
+        v1 = 2.0 * uniform() - 1.0;
+        v2 = 2.0 * uniform() - 1.0;
+        rsq = v1 * v1 + v2 * v2;
+      } while (rsq >= 1.0 || rsq == 0.0);
+      const double fac = std::sqrt(-2.0 * std::log(rsq) / rsq);
+      kept = v1 * fac;
+      have = true;
+      g = v2 * fac;
+    }
+    return mean + stdev * g;
+  }
+};
+
+constexpr int kRfgMaxModes = 1 << 20;
+
+void rfg_free(desalm_ctx* ctx) {
+  for (void* p : ctx->rfg.allocs) cudaFree(p);
+  ctx->rfg.allocs.clear();
+  ctx->rfg.on = false;
+  ctx->rfg.armed = false;
+  ctx->rfg.dev = RfgDev{};
+}
+
+int rfg_launch(desalm_ctx* ctx, double time) {
+  const Level& F = ctx->L[0];
+  void* qp[3];
+  int esz;
+  for (int d = 0; d < 3; ++d) RET(field_ptr(ctx, 0, DESALM_F_Q + 1 + d, &qp[d], &esz));
+  const long nn = (long)(F.jm - 2) * (F.km - 2);
+  LAUNCH(KC_MISC, 0, double(nn), launch_k(k_rfg_inlet, cdiv(nn, RFG_THREADS), RFG_THREADS, 0, ctx->stream, ctx->rfg.dev, time,
+                                          (double*)qp[0], (double*)qp[1], (double*)qp[2]));
+  CKL();
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int desalm_rfg_modes(int nmodes, long long seed, double* p, double* q, double* k, double* omega) {
+  if (nmodes < 1 || nmodes > kRfgMaxModes || !p || !q || !k || !omega) return DESALM_EINVAL;
+  RfgGauss g{(uint64_t)seed};
+  const size_t N = (size_t)nmodes;
+  std::vector<double> zet(3 * N), csi(3 * N);
+  // the draws in the order of initialize_rfg (src/rfg.F90:75-84): zet(1..3,:),
+  // csi(1..3,:) ~ N(0, 1), k(1..3,:) ~ N(0, 0.5^2), omega ~ N(0, 1)
+  for (int d = 0; d < 3; ++d)
+    for (size_t i = 0; i < N; ++i) zet[3 * i + d] = g.next(0.0, 1.0);
+  for (int d = 0; d < 3; ++d)
+    for (size_t i = 0; i < N; ++i) csi[3 * i + d] = g.next(0.0, 1.0);
+  for (int d = 0; d < 3; ++d)
+    for (size_t i = 0; i < N; ++i) k[3 * i + d] = g.next(0.0, 0.5);
+  for (size_t i = 0; i < N; ++i) omega[i] = g.next(0.0, 1.0);
+  // p = zet x k, q = csi x k (src/rfg.F90:87-90)
+  for (size_t i = 0; i < N; ++i) {
+    const double* a = &zet[3 * i];
+    const double* b = &csi[3 * i];
+    const double* kk = &k[3 * i];
+    p[3 * i + 0] = a[1] * kk[2] - a[2] * kk[1];
+    p[3 * i + 1] = a[2] * kk[0] - a[0] * kk[2];
+    p[3 * i + 2] = a[0] * kk[1] - a[1] * kk[0];
+    q[3 * i + 0] = b[1] * kk[2] - b[2] * kk[1];
+    q[3 * i + 1] = b[2] * kk[0] - b[0] * kk[2];
+    q[3 * i + 2] = b[0] * kk[1] - b[1] * kk[0];
+  }
+  return 0;
+}
+
+int desalm_rfg_set(desalm_ctx* ctx, const desalm_rfg* r) {
+  if (!ctx) return DESALM_EINVAL;
+  if (ctx->L.empty()) return DESALM_ENOTREADY;
+  auto bad = [&](const std::string& why) { ctx->err = "rfg_set: " + why; return DESALM_EINVAL; };
+  if (r && r->nmodes != 0) {
+    if (r->nmodes < 0 || r->nmodes > kRfgMaxModes) return bad("nmodes must be 1.." + std::to_string(kRfgMaxModes));
+    if (!r->p || !r->q || !r->k || !r->omega || !r->um || !r->uij || !r->t_ts || !r->t_ls) return bad("missing table");
+    if (!ctx->have_grid) { ctx->err = "rfg_set: set the grid first (the inflow nodes' coordinates)"; return DESALM_ENOTREADY; }
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  rfg_free(ctx);
+  if (!r || r->nmodes == 0) return 0;
+  const Level& F = ctx->L[0];
+  const size_t nm = (size_t)r->nmodes, njk = (size_t)F.jm * F.km;
+  std::vector<double> modes(nm * RFG_MODE);
+  for (size_t i = 0; i < nm; ++i) {
+    double* o = &modes[i * RFG_MODE];
+    for (int d = 0; d < 3; ++d) {
+      o[d] = r->p[3 * i + d];
+      o[3 + d] = r->q[3 * i + d];
+      o[6 + d] = r->k[3 * i + d];
+    }
+    o[9] = r->omega[i];
+  }
+  RfgDev& D = ctx->rfg.dev;
+  auto up = [&](const double* h, size_t n, const double** out) -> int {
+    void* d = nullptr;
+    if (dalloc(ctx, ctx->rfg.allocs, &d, n * sizeof(double))) return DESALM_ENOMEM;
+    if (h) CK(cudaMemcpyAsync(d, h, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    *out = (const double*)d;
+    return 0;
+  };
+  int rc = 0;
+  const double* tmp = nullptr;
+  if (!rc) rc = up(modes.data(), nm * RFG_MODE, &D.modes);
+  if (!rc) rc = up(r->um, 3 * njk, &D.um);
+  if (!rc) rc = up(r->uij, 6 * njk, &D.uij);
+  if (!rc) rc = up(r->t_ts, njk, &D.ts);
+  if (!rc) rc = up(r->t_ls, njk, &D.ls);
+  if (!rc) { rc = up(nullptr, RFG_NODE * njk, &tmp); D.node = const_cast<double*>(tmp); }
+  if (!rc) { rc = up(nullptr, 3 * njk, &tmp); D.x1 = const_cast<double*>(tmp); }
+  int* dbad = nullptr;
+  if (!rc && dalloc(ctx, ctx->rfg.allocs, (void**)&dbad, sizeof(int))) rc = DESALM_ENOMEM;
+  if (rc) { rfg_free(ctx); return rc; }
+  D.nm = r->nmodes;
+  D.im = F.im; D.jm = F.jm; D.km = F.km;
+  CK(cudaMemsetAsync(dbad, 0, sizeof(int), ctx->stream));
+  const long nn = (long)(F.jm - 2) * (F.km - 2);
+  LAUNCH(KC_MISC, 0, double(nn), launch_k(k_rfg_prep, cdiv(nn, RFG_THREADS), RFG_THREADS, 0, ctx->stream, D,
+                                          (const double*)ctx->x, (const double*)ctx->y, (const double*)ctx->z, dbad));
+  CKL();
+  int hbad = 0;
+  CK(cudaMemcpyAsync(&hbad, dbad, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (hbad) {
+    rfg_free(ctx);
+    return bad(std::to_string(hbad) + " inflow nodes have a correlation tensor that is not positive definite, "
+               "or a time or length scale that is not positive");
+  }
+  ctx->rfg.on = true;
+  return 0;
+}
+
+int desalm_rfg_inlet(desalm_ctx* ctx, double time) {
+  if (!ctx) return DESALM_EINVAL;
+  if (!ctx->rfg.on) { ctx->err = "rfg_inlet: no generator tables (desalm_rfg_set)"; return DESALM_EINVAL; }
+  if (!ctx->have_state) { ctx->err = "rfg_inlet: state not set"; return DESALM_ENOTREADY; }
+  RET(rfg_launch(ctx, time));
+  ctx->rfg.time = time;
+  ctx->rfg.armed = true;
   return 0;
 }
 

@@ -135,6 +135,17 @@ class Alm(C.Structure):
 ALM_FORCES, ALM_FIELD = 0, 1
 
 
+class Rfg(C.Structure):
+    """desalm_rfg: the random flow generator's tables (synthetic inflow)."""
+    _fields_ = [
+        ("nmodes", C.c_int),
+        ("p", C.POINTER(C.c_double)), ("q", C.POINTER(C.c_double)), ("k", C.POINTER(C.c_double)),
+        ("omega", C.POINTER(C.c_double)),
+        ("um", C.POINTER(C.c_double)), ("uij", C.POINTER(C.c_double)),
+        ("t_ts", C.POINTER(C.c_double)), ("t_ls", C.POINTER(C.c_double)),
+    ]
+
+
 def make_alm(spec):
     """A desalm_alm structure from a dict (see cases.alm_rotor); returns the
     structure and the arrays it points into, which must outlive the call."""

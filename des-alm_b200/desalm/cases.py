@@ -376,6 +376,28 @@ def wake(im=49, jm=25, km=25, seed=0, re=1000.0, turbulence=1, itmax=20, amp=0.0
     return c, grid, state
 
 
+def rfg_inflow(case, u=1.0, intensity=0.05, length_scale=0.2, time_scale=None, nmodes=1000, seed=0,
+               tables=None):
+    """Tables of the synthetic inflow turbulence (desalm_rfg) for the i = 1
+    plane of 'case': mean velocity (u, 0, 0), an isotropic correlation tensor
+    (intensity u)^2 I (the generator reproduces the tensor it is given: with
+    k ~ N(0, 0.5^2) each unit mode pair has unit variance), length scale
+    'length_scale', time scale 'time_scale' (default length_scale / u), and
+    'nmodes' modes drawn by desalm_rfg_modes from 'seed' (or the given
+    'tables': p, q, k, omega)."""
+    jm, km = case.jm, case.km
+    if tables is None:
+        from .solver import rfg_modes
+        tables = rfg_modes(nmodes, seed)
+    um = np.zeros((km, jm, 3))
+    um[..., 0] = u
+    uij = np.zeros((km, jm, 6))
+    uij[..., 0] = uij[..., 3] = uij[..., 5] = (intensity * u) ** 2
+    ts = np.full((km, jm), length_scale / u if time_scale is None else time_scale)
+    ls = np.full((km, jm), length_scale)
+    return dict(tables, um=um, uij=uij, t_ts=ts, t_ls=ls)
+
+
 def channel_alm(im=33, jm=25, km=25, itmax=20, n_tur=1, seed=0):
     """The SA channel with n_tur synthetic rotors (alm_rotor) along x; the
     Reynolds number gives vel_scale = ren 1e-6 / length_scale."""

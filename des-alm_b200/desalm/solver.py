@@ -11,7 +11,7 @@ import subprocess
 
 import numpy as np
 
-from .abi import Alm, Case, LpReport, StepReport, level_dims, make_alm
+from .abi import Alm, Case, LpReport, Rfg, StepReport, level_dims, make_alm
 
 PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 # DESALM_LIBRARY selects another build of the same library (tuning variants)
@@ -107,6 +107,9 @@ def lib():
             ("watchdog_selftest", [vp, C.c_double]),
             ("alm_set_angle", [vp, ip, C.c_double]),
             ("alm_get", [vp, ip, dp]),
+            ("rfg_set", [vp, C.POINTER(Rfg)]),
+            ("rfg_inlet", [vp, C.c_double]),
+            ("rfg_modes", [ip, C.c_longlong, dp, dp, dp, dp]),
         ]:
             f = getattr(L, "desalm_" + name)
             f.argtypes = args
@@ -198,6 +201,17 @@ def filestat_write(path, time, ntime, angles=()):
     a = _f64(np.asarray(angles, dtype=np.float64).reshape(-1))
     _io(lib().desalm_filestat_write(_b(path), float(time), int(ntime), _p(a) if a.size else None, a.size),
         "filestat_write")
+
+
+def rfg_modes(nmodes, seed):
+    """desalm_rfg_modes (host only): the generator's mode tables p, q, k
+    (nmodes, 3) and omega (nmodes,) for a seed."""
+    p, q, k = (np.zeros(3 * nmodes) for _ in range(3))
+    w = np.zeros(nmodes)
+    rc = lib().desalm_rfg_modes(int(nmodes), int(seed), _p(p), _p(q), _p(k), _p(w))
+    if rc:
+        raise DesalmError("rfg_modes failed (%d)" % rc)
+    return dict(p=p.reshape(nmodes, 3), q=q.reshape(nmodes, 3), k=k.reshape(nmodes, 3), omega=w)
 
 
 def mg_driver_batch(solvers):
@@ -526,6 +540,21 @@ class Solver:
         out = np.zeros(6 * self._alm_n if what == 0 else 3 * N)
         self._ck(self.L.desalm_alm_get(self.ctx, int(what), _p(out)), "alm_get")
         return out.reshape(-1, 6) if what == 0 else out.reshape(3, N)
+
+    def rfg_set(self, spec):
+        """Turn the synthetic inflow turbulence on (spec: dict with p, q, k
+        of shape (N, 3), omega (N,), um (km, jm, 3), uij (km, jm, 6), t_ts and
+        t_ls (km, jm); see cases.rfg_inflow) or off (None)."""
+        if spec is None:
+            self._ck(self.L.desalm_rfg_set(self.ctx, None), "rfg_set")
+            return
+        keep = {n: _f64(np.asarray(spec[n], dtype=np.float64).reshape(-1))
+                for n in ("p", "q", "k", "omega", "um", "uij", "t_ts", "t_ls")}
+        r = Rfg(len(keep["omega"]), *(_p(keep[n]) for n in ("p", "q", "k", "omega", "um", "uij", "t_ts", "t_ls")))
+        self._ck(self.L.desalm_rfg_set(self.ctx, C.byref(r)), "rfg_set")
+
+    def rfg_inlet(self, time):
+        self._ck(self.L.desalm_rfg_inlet(self.ctx, float(time)), "rfg_inlet")
 
     # ------------------------------------------------ checkpoint / restart
     def checkpoint_write(self, path):

@@ -548,6 +548,57 @@ int  desalm_alm_set_angle(desalm_ctx* ctx, int n_t, double angle);
 #define DESALM_ALM_FIELD  1
 int  desalm_alm_get(desalm_ctx* ctx, int what, double* out);
 
+/* ---------------------------------------------------------------------
+ * Synthetic inflow turbulence: the random flow generator of Smirnov, Shi &
+ * Celik (2001) that the reference runs when rfgt is set
+ * (src/global_param.F90:135; src/rfg_inlet.F90, src/rfg.F90).  Before each
+ * physical step the driver sets the velocities of the inflow plane i = 1,
+ * j = 2..jm-1, k = 2..km-1 to
+ *   q(2:4) = um + M diag(c) sqrt(2/N) sum_n [p_n cos(a_n) + q_n sin(a_n)],
+ *   a_n = (k_n upsilon / c) . (x / eta) + omega_n t / tau,  upsilon = eta / tau,
+ * with M diag(c^2) M^T the node's velocity correlation tensor, tau and eta its
+ * time and length scales.  The tables are those of the reference's
+ * inlet.bin.dat (rfg_um, rfg_uij, rfg_t_ts, rfg_t_ls over the fine (j, k)
+ * plane, Fortran layout) and of initialize_rfg (p_rfg, q_rfg, k_rfg,
+ * omega_rfg).  Hold the plane with an inflow face (btype(1) = 4).
+ * Differences: every node's tensor is decomposed once at desalm_rfg_set (the
+ * reference repeats it at every step), by Jacobi rotations with each
+ * eigenvector's largest component positive (the reference keeps the signs
+ * LAPACK ssyev returns); FP64 (the reference: real(rdf) = FP32).
+ * --------------------------------------------------------------------- */
+typedef struct desalm_rfg {
+  int nmodes;              /* N: spectrum samples (rfg_inlet_seed.dat), 0 turns it off */
+  const double* p;         /* p_rfg(3, N): p[3 n + d]                                   */
+  const double* q;         /* q_rfg(3, N)                                               */
+  const double* k;         /* k_rfg(3, N)                                               */
+  const double* omega;     /* omega_rfg(N)                                              */
+  const double* um;        /* rfg_um(3, jm, km): um[3 (j + jm k) + d], 0-based j, k      */
+  const double* uij;       /* rfg_uij(6, jm, km): r11, r12, r13, r22, r23, r33           */
+  const double* t_ts;      /* rfg_t_ts(jm, km): time scale tau                          */
+  const double* t_ls;      /* rfg_t_ls(jm, km): length scale eta                        */
+} desalm_rfg;
+
+/* initialize_rfg (src/rfg.F90:42-96) on the host: draws zeta, xi ~ N(0, 1)
+ * (3 N each), k ~ N(0, 0.5^2) (3 N), omega ~ N(0, 1) (N) in the reference's
+ * order and forms p = zeta x k, q = xi x k.  The normal deviates come from the
+ * polar method over a splitmix64 stream seeded by `seed`, not from the
+ * reference's generator, so a seed gives other samples of the same
+ * distribution.  1 <= nmodes <= 2^20.  Needs no GPU. */
+int  desalm_rfg_modes(int nmodes, long long seed, double* p, double* q, double* k, double* omega);
+/* rfg_init (src/rfg_inlet.F90:47-105): copies the tables to the device and
+ * decomposes every inflow node's correlation tensor.  Needs the grid
+ * (DESALM_ENOTREADY before desalm_set_grid); DESALM_EINVAL when a tensor is
+ * not positive definite or a scale is not positive.  NULL or nmodes = 0
+ * turns the generator off. */
+int  desalm_rfg_set(desalm_ctx* ctx, const desalm_rfg* rfg);
+/* rfg_mpi_inlet_forcing (src/rfg_inlet.F90:107-173) for physical time `time`:
+ * sets q(2:4) of the inflow plane on the device, ordered on the context's
+ * stream.  Call it before desalm_mg_driver / desalm_begin_step, as
+ * src/main.F90:60 does; the step then shifts the plane into q^n like the rest
+ * of q, and when the guess is extrapolated or learned, forces the plane again
+ * for the same time after the guess, so the step holds the forced values. */
+int  desalm_rfg_inlet(desalm_ctx* ctx, double time);
+
 /* Self-test of the device watchdog: a kernel waits, through the same bounded
  * wait as the tensor-core kernels, on a barrier that nothing completes, for
  * `seconds` (<= 10); the call returns DESALM_ETIMEOUT when the wait gave up
