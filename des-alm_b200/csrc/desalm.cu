@@ -1782,6 +1782,10 @@ int desalm_set_grid(desalm_ctx* ctx, const double* x, const double* y, const dou
   // the sweep widths for this grid; a captured step uses the old ones
   RET(autotune_sweeps(ctx));
   drop_graph(ctx);
+  // the inflow generator's node tables hold the old grid's coordinates:
+  // it is off until desalm_rfg_set is called again
+  ctx->rfg.on = false;
+  ctx->rfg.armed = false;
   ctx->have_grid = true;
   return 0;
 }

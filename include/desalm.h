@@ -41,8 +41,10 @@ extern "C" {
 
 /* precision_mode */
 #define DESALM_FP64   0        /* everything in FP64                            */
-#define DESALM_MIXED  1        /* FP64 residual/update, FP32 DAF sweeps and
-                                  FP32 coarse-grid levels                       */
+#define DESALM_MIXED  1        /* FP64 state, residual, restriction, update
+                                  and norm on every level; FP32 DAF line
+                                  sweeps, modal transforms, prolongation
+                                  correction and turbulence ADI              */
 /* predictor: initial guess of q^{n+1} for the pseudo-time loop */
 #define DESALM_PRED_QN      0  /* q^n, as src/mg_driver.F90:50-51              */
 #define DESALM_PRED_LINEAR  1  /* 2 q^n - q^{n-1}                               */
@@ -587,7 +589,8 @@ typedef struct desalm_rfg {
 int  desalm_rfg_modes(int nmodes, long long seed, double* p, double* q, double* k, double* omega);
 /* rfg_init (src/rfg_inlet.F90:47-105): copies the tables to the device and
  * decomposes every inflow node's correlation tensor.  Needs the grid
- * (DESALM_ENOTREADY before desalm_set_grid); DESALM_EINVAL when a tensor is
+ * (DESALM_ENOTREADY before desalm_set_grid); a later desalm_set_grid turns
+ * the generator off until it is set again.  DESALM_EINVAL when a tensor is
  * not positive definite or a scale is not positive.  NULL or nmodes = 0
  * turns the generator off. */
 int  desalm_rfg_set(desalm_ctx* ctx, const desalm_rfg* rfg);

@@ -94,7 +94,7 @@ def test_physical_step_holds_the_forced_plane(predictor):
     g.close()
 
 
-def test_rfg_rejects_tensors_that_are_not_positive_definite():
+def test_rfg_rejects_bad_tables_and_stale_grids():
     from desalm.solver import DesalmError, Solver
     case, grid, state = cases.wake(im=17, jm=21, km=19, turbulence=0, ng=2, seed=4)
     spec = _spec(case, "isotropic", 16, 1)
@@ -110,5 +110,12 @@ def test_rfg_rejects_tensors_that_are_not_positive_definite():
     assert "positive definite" in str(e.value)
     with pytest.raises(DesalmError) as e:
         g.rfg_inlet(0.0)                      # the failed set left the generator off
+    assert "no generator tables" in str(e.value)
+    spec["uij"][5, 7] = spec["uij"][5, 8]
+    g.rfg_set(spec)
+    g.rfg_inlet(0.0)
+    g.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))   # a new grid: the node tables are stale
+    with pytest.raises(DesalmError) as e:
+        g.rfg_inlet(0.0)
     assert "no generator tables" in str(e.value)
     g.close()

@@ -7,6 +7,9 @@ mathematical identities of the routines it restates:
   * the 27-point restriction weights sum to one (16/16)
   * metrics of an affine map are exact
   * a uniform flow on a Cartesian grid has zero residual (free stream)
+  * a linear velocity field on an affine grid has the exact convective and
+    divergence residual (QUICK and the central differences are exact on it)
+  * so does a quadratic one, with the full-stress viscous term
   * prolongation of a linear coarse correction is exact on interior nodes
   * the FP32 mirror stays within FP32 round-off of the FP64 oracle
 """
@@ -122,6 +125,100 @@ def test_uniform_flow_has_zero_residual(oracle_mod):
         assert np.max(np.abs(o.get_field(1, abi.F_RH + m))) < 1e-12
     qq = o.get_state()["q"].reshape(-1, 5)
     assert np.allclose(qq[:, 1:4], q[:, 1:4], atol=1e-12)
+
+
+def test_linear_velocity_residual_is_exact(oracle_mod):
+    """On an affine grid (constant metrics) a linear velocity field u = u0 + G x
+    with uniform pressure and q = q^n = q^{n-1} has the residual
+      rh(1)   = (div u) / J                     (rhs_flux_sans_convec: central
+                                                 differences of U/J,
+                                                 src/rhs_flux_sans_convec.F90:124-133)
+      rh(m+1) = (u . grad) u_m / J, m = 1..3    (rhs_convec_quick: QUICK,
+                                                 (3, 3, -7, 1)/8 with the
+                                                 U+/U- split, adds +fv,
+                                                 src/rhs_convec_quick.F90:90-198)
+    exactly: QUICK and the central differences reproduce the index derivative
+    of a linear field, the viscous terms and the pressure terms vanish, and so
+    do the BDF2 terms.  cfl1 = vnn1 = 0 makes dtau = 0, so the DAF update is
+    zero and the recalculated residual is that of the field as set.  Checked
+    on nodes 4..n-3, whose stencils do not reach the boundary nodes that
+    bcond_fm rewrites."""
+    n = 17
+    case, X, Y, Z = _cartesian(n)
+    case.cfl1 = case.vnn1 = 0.0
+    A = np.array([[2.0, 0.3, 0.1], [0.2, 1.5, -0.4], [0.0, 0.25, 3.0]])
+    P = np.stack([X, Y, Z], -1) @ A.T
+    o = oracle_mod.OracleSolver(case)
+    o.set_grid(P[..., 0].reshape(-1), P[..., 1].reshape(-1), P[..., 2].reshape(-1))
+    G = np.array([[0.3, -0.2, 0.1], [0.15, 0.05, -0.25], [-0.1, 0.2, 0.12]])
+    centre = A @ np.full(3, 0.5)
+    u0 = np.array([0.05, -0.03, 0.02]) - G @ centre
+    U = u0 + P @ G.T                              # (n, n, n, 3): every component changes sign
+    inner = (slice(3, n - 3),) * 3                # inside the checked nodes (both QUICK branches)
+    assert all((U[inner][..., c] > 0).any() and (U[inner][..., c] < 0).any() for c in range(3))
+    q = np.zeros((n, n, n, 5))
+    q[..., 0] = 0.1
+    q[..., 1:4] = U
+    o.set_state(q.reshape(-1), q.reshape(-1), q.reshape(-1))
+    o.solver_daf(1, 1, 1)
+    aj = o.get_field(1, abi.F_AJ).reshape(n, n, n)
+    want = [np.trace(G) / aj] + [np.einsum("kjic,c->kji", U, G[m]) / aj for m in range(3)]
+    for m in range(4):
+        got = o.get_field(1, abi.F_RH + m).reshape(n, n, n)
+        scale = np.abs(want[m][inner]).max()
+        assert np.abs(got[inner] - want[m][inner]).max() <= 1e-12 * scale, m
+    assert np.array_equal(o.get_state()["q"].reshape(n, n, n, 5)[inner][..., 1:4], U[inner])
+
+
+def test_quadratic_velocity_residual_is_exact(oracle_mod):
+    """QUICK is exact up to quadratics ((3, 3, -7, 1)/8 of i^2 is 2i), and so
+    are the central and face differences of the viscous and pressure terms.
+    On an affine grid quadratic velocity and pressure fields therefore have
+      rh(1)   = (div u) / J
+      rh(m+1) = [(u . grad) u_m + d_m p - nu (lap u_m + d_m div u)] / J,
+    the viscous term in the full-stress form nu div(grad u + grad u^T) that
+    rhs_viscous's face fluxes build (the a . (du/dx) terms beside the
+    c11, c12, c13 ones, src/rhs_viscous.F90:126-162).  A Laplacian-only
+    viscous term would miss by nu d_m div u / J, 1.4e-5 to 2.1e-4 here, against
+    a tolerance of 1e-12 of each field's largest value.  Same set-up as the
+    linear case (dtau = 0, which also zeroes the pressure dissipation
+    diss(1); nodes 4..n-3)."""
+    n = 17
+    case, X, Y, Z = _cartesian(n)
+    case.cfl1 = case.vnn1 = 0.0
+    case.ren = 10.0
+    A = np.array([[2.0, 0.3, 0.1], [0.2, 1.5, -0.4], [0.0, 0.25, 3.0]])
+    P = np.stack([X, Y, Z], -1) @ A.T
+    o = oracle_mod.OracleSolver(case)
+    o.set_grid(P[..., 0].reshape(-1), P[..., 1].reshape(-1), P[..., 2].reshape(-1))
+    rng = np.random.default_rng(3)
+    G = rng.normal(0.0, 0.2, (3, 3))
+    H = rng.normal(0.0, 0.1, (3, 3, 3))
+    H = 0.5 * (H + H.transpose(0, 2, 1))       # u_m = ... + sum_ab H[m, a, b] D_a D_b
+    D = P - A @ np.full(3, 0.5)
+    U = np.array([0.05, -0.03, 0.02]) + D @ G.T + np.einsum("mab,...a,...b->...m", H, D, D)
+    gp = np.array([0.2, -0.1, 0.05])
+    Kp = np.array([[0.1, 0.02, -0.03], [0.02, -0.05, 0.01], [-0.03, 0.01, 0.08]])
+    q = np.zeros((n, n, n, 5))
+    q[..., 0] = 0.1 + D @ gp + np.einsum("ab,...a,...b->...", Kp, D, D)
+    q[..., 1:4] = U
+    o.set_state(q.reshape(-1), q.reshape(-1), q.reshape(-1))
+    o.solver_daf(1, 1, 1)
+    aj = o.get_field(1, abi.F_AJ).reshape(n, n, n)
+    dp = gp + 2.0 * D @ Kp                                      # dp / dx_m (rhs_flux_sans_convec)
+    grad = G + 2.0 * np.einsum("mcb,...b->...mc", H, D)          # du_m / dx_c
+    div = np.einsum("...mm->...", grad)
+    conv = np.einsum("...c,...mc->...m", U, grad)
+    lap = 2.0 * np.einsum("mcc->m", H)
+    graddiv = 2.0 * np.einsum("ccm->m", H)
+    nu = 1.0 / case.ren
+    inner = (slice(3, n - 3),) * 3
+    want = [div / aj] + [(conv[..., m] + dp[..., m] - nu * (lap[m] + graddiv[m])) / aj for m in range(3)]
+    assert np.abs(nu * graddiv).max() > 1e-6
+    for m in range(4):
+        got = o.get_field(1, abi.F_RH + m).reshape(n, n, n)
+        scale = np.abs(want[m][inner]).max()
+        assert np.abs(got[inner] - want[m][inner]).max() <= 1e-12 * scale, m
 
 
 def test_prolongation_of_linear_correction_is_exact(oracle_mod):
