@@ -10,6 +10,7 @@ mathematical identities of the routines it restates:
   * a linear velocity field on an affine grid has the exact convective and
     divergence residual (QUICK and the central differences are exact on it)
   * so does a quadratic one, with the full-stress viscous term
+  * the SA eddy viscosity nu_t = nu_tilde f_v1 and the nu_tilde floor
   * prolongation of a linear coarse correction is exact on interior nodes
   * the FP32 mirror stays within FP32 round-off of the FP64 oracle
 """
@@ -219,6 +220,36 @@ def test_quadratic_velocity_residual_is_exact(oracle_mod):
         got = o.get_field(1, abi.F_RH + m).reshape(n, n, n)
         scale = np.abs(want[m][inner]).max()
         assert np.abs(got[inner] - want[m][inner]).max() <= 1e-12 * scale, m
+
+
+def test_sa_eddy_viscosity_closure(oracle_mod):
+    """With a zero turbulence time step (cfl2 = vnn2 = 0: dtev = 0), des_eddy
+    changes no interior nu_tilde except by the floor, and leaves
+      nu_t = nu_tilde f_v1,  f_v1 = chi^3 / (chi^3 + 357.911),
+      chi = nu_tilde Re,  nu_tilde >= 1e-7
+    on every interior node (rhs_sa_bcond, src/rhs_sa_bcond.F90:282-286; cv1^3
+    from src/des_eddy.F90:72).  nu_tilde spans 1e-9..1e-1, across the floor
+    and the range where f_v1 turns from chi^3 / cv1^3 to one."""
+    case, grid, state = cases.channel(im=17, jm=17, km=17, seed=0, itmax=2)
+    case.cfl2 = case.vnn2 = 0.0
+    o = oracle_mod.OracleSolver(case)
+    o.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
+    q = state["q"].reshape(-1, 5).copy()
+    nt = 10.0 ** np.random.default_rng(0).uniform(-9.0, -1.0, size=q.shape[0])
+    q[:, 4] = nt
+    o.set_state(q.reshape(-1), q.reshape(-1), q.reshape(-1), state["nut"])
+    o.des_eddy()
+    inner = np.zeros((17, 17, 17), bool)
+    inner[1:-1, 1:-1, 1:-1] = True
+    inner = inner.reshape(-1)
+    floor = np.maximum(1e-7, nt)[inner]
+    assert (nt[inner] < 1e-7).any()
+    q5 = o.get_state()["q"].reshape(-1, 5)[inner, 4]
+    assert np.array_equal(q5, floor)
+    chi3 = (floor * case.ren) ** 3
+    want = floor * (chi3 / (chi3 + 357.911))
+    nut = o.get_field(1, abi.F_NUT)[inner]
+    assert np.abs(nut - want).max() <= 1e-14 * np.abs(want).max()
 
 
 def test_prolongation_of_linear_correction_is_exact(oracle_mod):
