@@ -11,6 +11,7 @@ mathematical identities of the routines it restates:
     divergence residual (QUICK and the central differences are exact on it)
   * so does a quadratic one, with the full-stress viscous term
   * the SA eddy viscosity nu_t = nu_tilde f_v1 and the nu_tilde floor
+  * the convergence norm of mg_residual over the interior nodes
   * prolongation of a linear coarse correction is exact on interior nodes
   * the FP32 mirror stays within FP32 round-off of the FP64 oracle
 """
@@ -250,6 +251,26 @@ def test_sa_eddy_viscosity_closure(oracle_mod):
     want = floor * (chi3 / (chi3 + 357.911))
     nut = o.get_field(1, abi.F_NUT)[inner]
     assert np.abs(nut - want).max() <= 1e-14 * np.abs(want).max()
+
+
+def test_residual_norm_definition(oracle_mod):
+    """mg_residual (src/mg_residual.F90:32-84): per field, log10 of the sum of
+    |q - qold_mg| over the interior nodes divided by (im-2)(jm-2)(km-2);
+    boundary nodes do not count."""
+    case, grid, state = cases.cavity(n=17, seed=4)
+    o = oracle_mod.OracleSolver(case)
+    o.set_grid(grid["x"], grid["y"], grid["z"])
+    rng = np.random.default_rng(5)
+    N = 17 ** 3
+    q = rng.normal(size=(N, 5))
+    qold = rng.normal(size=(N, 5))
+    o.set_state(q.reshape(-1))
+    for m in range(5):
+        o.set_field(1, abi.F_QOLD + m, qold[:, m])
+    got = o.mg_residual(1)
+    d = np.abs(q - qold).reshape(17, 17, 17, 5)[1:-1, 1:-1, 1:-1]
+    want = np.log10(d.reshape(-1, 5).sum(axis=0) / 15 ** 3)
+    assert np.allclose(got, want, rtol=0, atol=1e-13)
 
 
 def test_prolongation_of_linear_correction_is_exact(oracle_mod):
