@@ -10,6 +10,7 @@ mathematical identities of the routines it restates:
   * a linear velocity field on an affine grid has the exact convective and
     divergence residual (QUICK and the central differences are exact on it)
   * so does a quadratic one, with the full-stress viscous term
+  * the BDF2 time derivative of a flow uniform in space
   * the SA eddy viscosity nu_t = nu_tilde f_v1 and the nu_tilde floor
   * the convergence norm of mg_residual over the interior nodes
   * prolongation of a linear coarse correction is exact on interior nodes
@@ -251,6 +252,36 @@ def test_sa_eddy_viscosity_closure(oracle_mod):
     want = floor * (chi3 / (chi3 + 357.911))
     nut = o.get_field(1, abi.F_NUT)[inner]
     assert np.abs(nut - want).max() <= 1e-14 * np.abs(want).max()
+
+
+def test_bdf2_term_of_a_uniform_accelerating_flow(oracle_mod):
+    """A flow uniform in space that changes linearly in time, q^{n-1} = a - 2 b dt,
+    q^n = a - b dt, q = a: every spatial term vanishes and the residual is the
+    BDF2 time derivative (3 q - 4 q^n + q^{n-1}) / (2 dt J) = b / J
+    (rhs_unst_visc_diss, src/rhs_unst_visc_diss.F90:35-50, e_source = 1),
+    which pins its coefficients, sign and scale; rh(1) = 0."""
+    n = 17
+    case, X, Y, Z = _cartesian(n)
+    case.cfl1 = case.vnn1 = 0.0
+    for b in range(6):
+        case.btype[b] = abi.BC_FREESTREAM   # the extrapolation keeps a uniform field uniform
+    A = np.array([[2.0, 0.3, 0.1], [0.2, 1.5, -0.4], [0.0, 0.25, 3.0]])
+    P = np.stack([X, Y, Z], -1) @ A.T
+    o = oracle_mod.OracleSolver(case)
+    o.set_grid(P[..., 0].reshape(-1), P[..., 1].reshape(-1), P[..., 2].reshape(-1))
+    a_ = np.array([0.1, 0.7, -0.2, 0.4, 0.0])
+    b_ = np.array([0.0, 0.3, 0.5, -0.25, 0.0])
+    dt = case.delti
+    Q = lambda v: np.broadcast_to(v, (n ** 3, 5)).reshape(-1).copy()
+    o.set_state(Q(a_), Q(a_ - b_ * dt), Q(a_ - 2.0 * b_ * dt))
+    o.solver_daf(1, 1, 1)
+    aj = o.get_field(1, abi.F_AJ).reshape(n, n, n)
+    inner = (slice(1, n - 1),) * 3
+    assert np.abs(o.get_field(1, abi.F_RH).reshape(n, n, n)[inner]).max() < 1e-12
+    for m in range(1, 4):
+        got = o.get_field(1, abi.F_RH + m).reshape(n, n, n)[inner]
+        want = b_[m] / aj[inner]
+        assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max(), m
 
 
 def test_residual_norm_definition(oracle_mod):
