@@ -13,6 +13,7 @@ mathematical identities of the routines it restates:
   * the BDF2 time derivative of a flow uniform in space
   * the SA eddy viscosity nu_t = nu_tilde f_v1 and the nu_tilde floor
   * the convergence norm of mg_residual over the interior nodes
+  * bcond_fm's extrapolation, wall and symmetry rows and the pressure fix
   * prolongation of a linear coarse correction is exact on interior nodes
   * the FP32 mirror stays within FP32 round-off of the FP64 oracle
 """
@@ -282,6 +283,48 @@ def test_bdf2_term_of_a_uniform_accelerating_flow(oracle_mod):
         got = o.get_field(1, abi.F_RH + m).reshape(n, n, n)[inner]
         want = b_[m] / aj[inner]
         assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max(), m
+
+
+def test_boundary_extrapolation_and_walls(oracle_mod):
+    """bcond_fm (src/bcond_fm.F90:80-310) with the coefficients of
+    src/init.F90:482-509 on the face nodes away from edges: an extrapolating
+    face (btype 3) sets q_b = 4/3 q_1 - 1/3 q_2 (a zero normal derivative to
+    second order: exact for a quadratic with zero slope at the face), a wall
+    (btype 1) sets u = v = w = 0 and extrapolates p, a symmetry plane (btype 2)
+    zeroes its bdir component only; then p(ifix, jfix, kfix) is subtracted
+    from p everywhere (src/bcond_fm.F90:316-322)."""
+    n = 17
+    case, X, Y, Z = _cartesian(n)
+    bt = [abi.BC_FREESTREAM, abi.BC_WALL, abi.BC_SYMMETRY, abi.BC_FREESTREAM, abi.BC_WALL, abi.BC_SYMMETRY]
+    for b in range(6):
+        case.btype[b] = bt[b]
+    case.ifix, case.jfix, case.kfix = 5, 6, 7
+    o = oracle_mod.OracleSolver(case)
+    o.set_grid(X.reshape(-1), Y.reshape(-1), Z.reshape(-1))
+    q = np.random.default_rng(6).normal(size=(n, n, n, 5))
+    o.set_state(q.reshape(-1))
+    o.bcond_fm()
+    got = o.get_state()["q"].reshape(n, n, n, 5)
+    pfix = q[case.kfix - 1, case.jfix - 1, case.ifix - 1, 0]
+    mid = slice(1, n - 1)
+    # faces in the reference's order: i = 1, i = im, j = 1, j = jm, k = 1, k = km
+    faces = [lambda a: a[mid, mid, 0], lambda a: a[mid, mid, -1], lambda a: a[mid, 0, mid],
+             lambda a: a[mid, -1, mid], lambda a: a[0, mid, mid], lambda a: a[-1, mid, mid]]
+    inner1 = [lambda a: a[mid, mid, 1], lambda a: a[mid, mid, -2], lambda a: a[mid, 1, mid],
+              lambda a: a[mid, -2, mid], lambda a: a[1, mid, mid], lambda a: a[-2, mid, mid]]
+    inner2 = [lambda a: a[mid, mid, 2], lambda a: a[mid, mid, -3], lambda a: a[mid, 2, mid],
+              lambda a: a[mid, -3, mid], lambda a: a[2, mid, mid], lambda a: a[-3, mid, mid]]
+    for b in range(6):
+        g, q1, q2 = faces[b](got), inner1[b](q), inner2[b](q)
+        ext = 4.0 / 3.0 * q1 - 1.0 / 3.0 * q2
+        assert np.allclose(g[..., 0], ext[..., 0] - pfix, rtol=0, atol=1e-14), b
+        for m in (1, 2, 3):
+            if bt[b] == abi.BC_WALL or (bt[b] == abi.BC_SYMMETRY and case.bdir[b] == m):
+                want = np.zeros_like(ext[..., m])
+            else:
+                want = ext[..., m]
+            assert np.allclose(g[..., m], want, rtol=0, atol=1e-14), (b, m)
+    assert np.allclose(got[1:-1, 1:-1, 1:-1, 0], q[1:-1, 1:-1, 1:-1, 0] - pfix, rtol=0, atol=1e-15)
 
 
 def test_residual_norm_definition(oracle_mod):
