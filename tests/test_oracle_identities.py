@@ -13,6 +13,7 @@ mathematical identities of the routines it restates:
   * the BDF2 time derivative of a flow uniform in space
   * the SA eddy viscosity nu_t = nu_tilde f_v1 and the nu_tilde floor
   * the convergence norm of mg_residual over the interior nodes
+  * the local pseudo-time step of rhs_daf_dtau on a curvilinear grid
   * bcond_fm's extrapolation, wall and symmetry rows and the pressure fix
   * prolongation of a linear coarse correction is exact on interior nodes
   * the FP32 mirror stays within FP32 round-off of the FP64 oracle
@@ -325,6 +326,30 @@ def test_boundary_extrapolation_and_walls(oracle_mod):
                 want = ext[..., m]
             assert np.allclose(g[..., m], want, rtol=0, atol=1e-14), (b, m)
     assert np.allclose(got[1:-1, 1:-1, 1:-1, 0], q[1:-1, 1:-1, 1:-1, 0] - pfix, rtol=0, atol=1e-15)
+
+
+def test_local_pseudo_time_step(oracle_mod):
+    """rhs_daf_dtau (src/rhs_daf_dtau.F90:30-84) on a curvilinear grid with an
+    eddy viscosity: per node, with g_d = |grad xi_d|^2,
+      dtau = min_d min( cfl1 / sqrt(g_d) / dxi_d,
+                        vnn1 / (1/Re + nu_t) / dxi_d^2 / g_d ),
+    the convective and viscous limits of the three directions."""
+    case, grid, state = cases.channel(im=17, jm=17, km=17, seed=1, itmax=2)
+    o = oracle_mod.OracleSolver(case)
+    o.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
+    o.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
+    o.solver_daf(1, 0, 1)
+    nut = o.get_field(1, abi.F_NUT)
+    assert np.ptp(nut) > 0
+    ret = 1.0 / case.ren + nut
+    lim = []
+    for f in (abi.F_CSI, abi.F_ETA, abi.F_ZET):     # dc = de = dz = 1 on the fine level
+        g = sum(o.get_field(1, f + c) ** 2 for c in range(3))
+        lim += [case.cfl1 / np.sqrt(g), case.vnn1 / ret / g]
+    want = np.minimum.reduce(lim)
+    got = o.get_field(1, abi.F_DTAU)
+    assert np.abs(got - want).max() <= 1e-14 * np.abs(want).max()
+    assert len(set(np.argmin(np.stack(lim), axis=0).tolist())) > 1   # more than one limit is active
 
 
 def test_residual_norm_definition(oracle_mod):
