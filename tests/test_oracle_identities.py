@@ -10,6 +10,8 @@ mathematical identities of the routines it restates:
   * a linear velocity field on an affine grid has the exact convective and
     divergence residual (QUICK and the central differences are exact on it)
   * so does a quadratic one, with the full-stress viscous term
+  * on a coarse level the convection is first-order upwind, whose error on a
+    quadratic field is known exactly
   * the BDF2 time derivative of a flow uniform in space
   * the SA eddy viscosity nu_t = nu_tilde f_v1 and the nu_tilde floor
   * the convergence norm of mg_residual over the interior nodes
@@ -254,6 +256,60 @@ def test_sa_eddy_viscosity_closure(oracle_mod):
     want = floor * (chi3 / (chi3 + 357.911))
     nut = o.get_field(1, abi.F_NUT)[inner]
     assert np.abs(nut - want).max() <= 1e-14 * np.abs(want).max()
+
+
+def test_coarse_levels_convect_first_order_upwind(oracle_mod):
+    """On coarse levels the convection is first-order upwind
+    (decide_upwind = 1, src/rhs_convec_quick.F90:90-161): for a quadratic
+    field its error is exactly -1/2 dxi |U/J| times the second difference
+    along each direction, so the level-2 residual of the quadratic case equals
+      [(u . grad) u_m - nu (lap u_m + d_m div u)] / J
+        - sum_d 1/2 dxi_d |U_d / J| (q_{I+1} - 2 q_I + q_{I-1})_d,
+    with dxi = 1/2 there.  The FAS forcing pk is zero and itr = 2, so rhs_pk
+    only adds it (src/rhs_pk.F90:35-67)."""
+    n, nc = 17, 9
+    case, X, Y, Z = _cartesian(n)
+    case.cfl1 = case.vnn1 = 0.0
+    case.ren = 10.0
+    A = np.array([[2.0, 0.3, 0.1], [0.2, 1.5, -0.4], [0.0, 0.25, 3.0]])
+    P = np.stack([X, Y, Z], -1) @ A.T
+    o = oracle_mod.OracleSolver(case)
+    o.set_grid(P[..., 0].reshape(-1), P[..., 1].reshape(-1), P[..., 2].reshape(-1))
+    rng = np.random.default_rng(3)
+    G = rng.normal(0.0, 0.2, (3, 3))
+    H = rng.normal(0.0, 0.1, (3, 3, 3))
+    H = 0.5 * (H + H.transpose(0, 2, 1))
+    D = P[::2, ::2, ::2] - A @ np.full(3, 0.5)     # the coarse nodes (injection)
+    U = np.array([0.05, -0.03, 0.02]) + D @ G.T + np.einsum("mab,...a,...b->...m", H, D, D)
+    qc = np.zeros((nc, nc, nc, 5))
+    qc[..., 0] = 0.1
+    qc[..., 1:4] = U
+    for m in range(5):
+        for f in (abi.F_Q, abi.F_QN, abi.F_QNM1, abi.F_QOLD):
+            o.set_field(2, f + m, qc[..., m].reshape(-1))
+    for m in range(4):
+        o.set_field(2, abi.F_PK + m, np.zeros(nc ** 3))
+    o.solver_daf(2, 1, 2)
+    aj = o.get_field(2, abi.F_AJ).reshape(nc, nc, nc)
+    met = [np.stack([o.get_field(2, f + c).reshape(nc, nc, nc) for c in range(3)], -1)
+           for f in (abi.F_CSI, abi.F_ETA, abi.F_ZET)]
+    grad = G + 2.0 * np.einsum("mcb,...b->...mc", H, D)
+    div = np.einsum("...mm->...", grad)
+    conv = np.einsum("...c,...mc->...m", U, grad)
+    lap = 2.0 * np.einsum("mcc->m", H)
+    graddiv = 2.0 * np.einsum("ccm->m", H)
+    nu, dxi = 1.0 / case.ren, 0.5
+    inner = (slice(2, nc - 2),) * 3
+    got = o.get_field(2, abi.F_RH).reshape(nc, nc, nc)
+    assert np.abs(got - div / aj)[inner].max() <= 1e-12 * np.abs(div / aj)[inner].max()
+    for m in range(3):
+        want = (conv[..., m] - nu * (lap[m] + graddiv[m])) / aj
+        for d, ax in enumerate((2, 1, 0)):            # xi along i (last axis), eta along j, zeta along k
+            Ud = np.einsum("...c,...c->...", met[d], U) / aj
+            q = U[..., m]
+            want = want - 0.5 * dxi * np.abs(Ud) * (np.roll(q, -1, ax) - 2.0 * q + np.roll(q, 1, ax))
+        got = o.get_field(2, abi.F_RH + 1 + m).reshape(nc, nc, nc)
+        assert np.abs(got - want)[inner].max() <= 1e-12 * np.abs(want[inner]).max(), m
 
 
 def test_bdf2_term_of_a_uniform_accelerating_flow(oracle_mod):
