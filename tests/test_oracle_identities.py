@@ -1,4 +1,6 @@
 """Known-answer checks that pin the CPU oracle without reference output.
+The check_* functions take the solver class, so that the same identities run
+on the GPU path too (tests/test_gpu_identities.py).
 
 The reference ships no tests or golden data, so the restatement is pinned by
 mathematical identities of the routines it restates:
@@ -116,12 +118,12 @@ def test_affine_metrics_exact(oracle_mod):
     assert np.allclose(aj, 1.0 / np.linalg.det(A * h), rtol=1e-12)
 
 
-def test_uniform_flow_has_zero_residual(oracle_mod):
+def check_uniform_flow_has_zero_residual(make):
     n = 17
     case, X, Y, Z = _cartesian(n)
     for b in range(6):
         case.btype[b] = abi.BC_FREESTREAM   # first-order extrapolation keeps a uniform field
-    o = oracle_mod.OracleSolver(case)
+    o = make(case)
     o.set_grid(X.reshape(-1), Y.reshape(-1), Z.reshape(-1))
     q = np.zeros((n ** 3, 5))
     q[:, 1], q[:, 2], q[:, 3] = 0.7, -0.2, 0.4
@@ -134,7 +136,11 @@ def test_uniform_flow_has_zero_residual(oracle_mod):
     assert np.allclose(qq[:, 1:4], q[:, 1:4], atol=1e-12)
 
 
-def test_linear_velocity_residual_is_exact(oracle_mod):
+def test_uniform_flow_has_zero_residual(oracle_mod):
+    check_uniform_flow_has_zero_residual(oracle_mod.OracleSolver)
+
+
+def check_linear_velocity_residual_is_exact(make):
     """On an affine grid (constant metrics) a linear velocity field u = u0 + G x
     with uniform pressure and q = q^n = q^{n-1} has the residual
       rh(1)   = (div u) / J                     (rhs_flux_sans_convec: central
@@ -155,7 +161,7 @@ def test_linear_velocity_residual_is_exact(oracle_mod):
     case.cfl1 = case.vnn1 = 0.0
     A = np.array([[2.0, 0.3, 0.1], [0.2, 1.5, -0.4], [0.0, 0.25, 3.0]])
     P = np.stack([X, Y, Z], -1) @ A.T
-    o = oracle_mod.OracleSolver(case)
+    o = make(case)
     o.set_grid(P[..., 0].reshape(-1), P[..., 1].reshape(-1), P[..., 2].reshape(-1))
     G = np.array([[0.3, -0.2, 0.1], [0.15, 0.05, -0.25], [-0.1, 0.2, 0.12]])
     centre = A @ np.full(3, 0.5)
@@ -177,7 +183,11 @@ def test_linear_velocity_residual_is_exact(oracle_mod):
     assert np.array_equal(o.get_state()["q"].reshape(n, n, n, 5)[inner][..., 1:4], U[inner])
 
 
-def test_quadratic_velocity_residual_is_exact(oracle_mod):
+def test_linear_velocity_residual_is_exact(oracle_mod):
+    check_linear_velocity_residual_is_exact(oracle_mod.OracleSolver)
+
+
+def check_quadratic_velocity_residual_is_exact(make):
     """QUICK is exact up to quadratics ((3, 3, -7, 1)/8 of i^2 is 2i), and so
     are the central and face differences of the viscous and pressure terms.
     On an affine grid quadratic velocity and pressure fields therefore have
@@ -196,7 +206,7 @@ def test_quadratic_velocity_residual_is_exact(oracle_mod):
     case.ren = 10.0
     A = np.array([[2.0, 0.3, 0.1], [0.2, 1.5, -0.4], [0.0, 0.25, 3.0]])
     P = np.stack([X, Y, Z], -1) @ A.T
-    o = oracle_mod.OracleSolver(case)
+    o = make(case)
     o.set_grid(P[..., 0].reshape(-1), P[..., 1].reshape(-1), P[..., 2].reshape(-1))
     rng = np.random.default_rng(3)
     G = rng.normal(0.0, 0.2, (3, 3))
@@ -228,7 +238,11 @@ def test_quadratic_velocity_residual_is_exact(oracle_mod):
         assert np.abs(got[inner] - want[m][inner]).max() <= 1e-12 * scale, m
 
 
-def test_sa_eddy_viscosity_closure(oracle_mod):
+def test_quadratic_velocity_residual_is_exact(oracle_mod):
+    check_quadratic_velocity_residual_is_exact(oracle_mod.OracleSolver)
+
+
+def check_sa_eddy_viscosity_closure(make):
     """With a zero turbulence time step (cfl2 = vnn2 = 0: dtev = 0), des_eddy
     changes no interior nu_tilde except by the floor, and leaves
       nu_t = nu_tilde f_v1,  f_v1 = chi^3 / (chi^3 + 357.911),
@@ -238,7 +252,7 @@ def test_sa_eddy_viscosity_closure(oracle_mod):
     and the range where f_v1 turns from chi^3 / cv1^3 to one."""
     case, grid, state = cases.channel(im=17, jm=17, km=17, seed=0, itmax=2)
     case.cfl2 = case.vnn2 = 0.0
-    o = oracle_mod.OracleSolver(case)
+    o = make(case)
     o.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
     q = state["q"].reshape(-1, 5).copy()
     nt = 10.0 ** np.random.default_rng(0).uniform(-9.0, -1.0, size=q.shape[0])
@@ -258,7 +272,11 @@ def test_sa_eddy_viscosity_closure(oracle_mod):
     assert np.abs(nut - want).max() <= 1e-14 * np.abs(want).max()
 
 
-def test_coarse_levels_convect_first_order_upwind(oracle_mod):
+def test_sa_eddy_viscosity_closure(oracle_mod):
+    check_sa_eddy_viscosity_closure(oracle_mod.OracleSolver)
+
+
+def check_coarse_levels_convect_first_order_upwind(make):
     """On coarse levels the convection is first-order upwind
     (decide_upwind = 1, src/rhs_convec_quick.F90:90-161): for a quadratic
     field its error is exactly -1/2 dxi |U/J| times the second difference
@@ -273,7 +291,7 @@ def test_coarse_levels_convect_first_order_upwind(oracle_mod):
     case.ren = 10.0
     A = np.array([[2.0, 0.3, 0.1], [0.2, 1.5, -0.4], [0.0, 0.25, 3.0]])
     P = np.stack([X, Y, Z], -1) @ A.T
-    o = oracle_mod.OracleSolver(case)
+    o = make(case)
     o.set_grid(P[..., 0].reshape(-1), P[..., 1].reshape(-1), P[..., 2].reshape(-1))
     rng = np.random.default_rng(3)
     G = rng.normal(0.0, 0.2, (3, 3))
@@ -312,7 +330,11 @@ def test_coarse_levels_convect_first_order_upwind(oracle_mod):
         assert np.abs(got - want)[inner].max() <= 1e-12 * np.abs(want[inner]).max(), m
 
 
-def test_bdf2_term_of_a_uniform_accelerating_flow(oracle_mod):
+def test_coarse_levels_convect_first_order_upwind(oracle_mod):
+    check_coarse_levels_convect_first_order_upwind(oracle_mod.OracleSolver)
+
+
+def check_bdf2_term_of_a_uniform_accelerating_flow(make):
     """A flow uniform in space that changes linearly in time, q^{n-1} = a - 2 b dt,
     q^n = a - b dt, q = a: every spatial term vanishes and the residual is the
     BDF2 time derivative (3 q - 4 q^n + q^{n-1}) / (2 dt J) = b / J
@@ -325,7 +347,7 @@ def test_bdf2_term_of_a_uniform_accelerating_flow(oracle_mod):
         case.btype[b] = abi.BC_FREESTREAM   # the extrapolation keeps a uniform field uniform
     A = np.array([[2.0, 0.3, 0.1], [0.2, 1.5, -0.4], [0.0, 0.25, 3.0]])
     P = np.stack([X, Y, Z], -1) @ A.T
-    o = oracle_mod.OracleSolver(case)
+    o = make(case)
     o.set_grid(P[..., 0].reshape(-1), P[..., 1].reshape(-1), P[..., 2].reshape(-1))
     a_ = np.array([0.1, 0.7, -0.2, 0.4, 0.0])
     b_ = np.array([0.0, 0.3, 0.5, -0.25, 0.0])
@@ -342,7 +364,11 @@ def test_bdf2_term_of_a_uniform_accelerating_flow(oracle_mod):
         assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max(), m
 
 
-def test_boundary_extrapolation_and_walls(oracle_mod):
+def test_bdf2_term_of_a_uniform_accelerating_flow(oracle_mod):
+    check_bdf2_term_of_a_uniform_accelerating_flow(oracle_mod.OracleSolver)
+
+
+def check_boundary_extrapolation_and_walls(make):
     """bcond_fm (src/bcond_fm.F90:80-310) with the coefficients of
     src/init.F90:482-509 on the face nodes away from edges: an extrapolating
     face (btype 3) sets q_b = 4/3 q_1 - 1/3 q_2 (a zero normal derivative to
@@ -356,7 +382,7 @@ def test_boundary_extrapolation_and_walls(oracle_mod):
     for b in range(6):
         case.btype[b] = bt[b]
     case.ifix, case.jfix, case.kfix = 5, 6, 7
-    o = oracle_mod.OracleSolver(case)
+    o = make(case)
     o.set_grid(X.reshape(-1), Y.reshape(-1), Z.reshape(-1))
     q = np.random.default_rng(6).normal(size=(n, n, n, 5))
     o.set_state(q.reshape(-1))
@@ -384,14 +410,18 @@ def test_boundary_extrapolation_and_walls(oracle_mod):
     assert np.allclose(got[1:-1, 1:-1, 1:-1, 0], q[1:-1, 1:-1, 1:-1, 0] - pfix, rtol=0, atol=1e-15)
 
 
-def test_local_pseudo_time_step(oracle_mod):
+def test_boundary_extrapolation_and_walls(oracle_mod):
+    check_boundary_extrapolation_and_walls(oracle_mod.OracleSolver)
+
+
+def check_local_pseudo_time_step(make):
     """rhs_daf_dtau (src/rhs_daf_dtau.F90:30-84) on a curvilinear grid with an
     eddy viscosity: per node, with g_d = |grad xi_d|^2,
       dtau = min_d min( cfl1 / sqrt(g_d) / dxi_d,
                         vnn1 / (1/Re + nu_t) / dxi_d^2 / g_d ),
     the convective and viscous limits of the three directions."""
     case, grid, state = cases.channel(im=17, jm=17, km=17, seed=1, itmax=2)
-    o = oracle_mod.OracleSolver(case)
+    o = make(case)
     o.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
     o.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
     o.solver_daf(1, 0, 1)
@@ -408,12 +438,16 @@ def test_local_pseudo_time_step(oracle_mod):
     assert len(set(np.argmin(np.stack(lim), axis=0).tolist())) > 1   # more than one limit is active
 
 
-def test_residual_norm_definition(oracle_mod):
+def test_local_pseudo_time_step(oracle_mod):
+    check_local_pseudo_time_step(oracle_mod.OracleSolver)
+
+
+def check_residual_norm_definition(make):
     """mg_residual (src/mg_residual.F90:32-84): per field, log10 of the sum of
     |q - qold_mg| over the interior nodes divided by (im-2)(jm-2)(km-2);
     boundary nodes do not count."""
     case, grid, state = cases.cavity(n=17, seed=4)
-    o = oracle_mod.OracleSolver(case)
+    o = make(case)
     o.set_grid(grid["x"], grid["y"], grid["z"])
     rng = np.random.default_rng(5)
     N = 17 ** 3
@@ -428,10 +462,14 @@ def test_residual_norm_definition(oracle_mod):
     assert np.allclose(got, want, rtol=0, atol=1e-13)
 
 
-def test_prolongation_of_linear_correction_is_exact(oracle_mod):
+def test_residual_norm_definition(oracle_mod):
+    check_residual_norm_definition(oracle_mod.OracleSolver)
+
+
+def check_prolongation_of_linear_correction_is_exact(make):
     case, grid, state = cases.cavity(n=17, seed=1)
     case.ep[1][0] = case.ep[1][1] = case.ep[1][2] = 0.0   # no smoothing: pure interpolation
-    o = oracle_mod.OracleSolver(case)
+    o = make(case)
     o.set_grid(grid["x"], grid["y"], grid["z"])
     o.set_state(state["q"])
     c = np.arange(9, dtype=float)
@@ -448,6 +486,10 @@ def test_prolongation_of_linear_correction_is_exact(oracle_mod):
     got = (o.get_field(1, abi.F_Q + 1) - q0).reshape(17, 17, 17)
     assert np.allclose(got[1:-1, 1:-1, 1:-1], want[1:-1, 1:-1, 1:-1], atol=1e-15)
     assert np.all(got[0] == 0)
+
+
+def test_prolongation_of_linear_correction_is_exact(oracle_mod):
+    check_prolongation_of_linear_correction_is_exact(oracle_mod.OracleSolver)
 
 
 def test_fp32_mirror_tracks_fp64(oracle_mod):
