@@ -105,6 +105,10 @@ def build_case(name, precision, predictor, model="kw", small=False):
     elif name == "channel":
         case, grid, state = cases.channel()
         desc = "SA RANS channel Re_tau=395, 129x97x65 tanh-stretched, periodic i/k, 3-level FAS"
+    elif name == "ogrid":
+        case, grid, state = cases.ogrid()
+        desc = ("SA-DES cylinder O-grid 257x129x65 (radial geometric stretching to 20D, span pi D), Re=3900, "
+                "dt=0.005 D/U, impulsive start, 3-level FAS")
     else:
         raise SystemExit("unknown case " + name)
     case.it_min = CRITERION["it_min"]
@@ -609,6 +613,50 @@ def run_extras(barrier, max_over_ranks):
     return out
 
 
+def run_guesses(args):
+    """The initial guesses of a physical step on one workload (MIXED, each step
+    to the convergence criterion): q^n (the reference's), linear
+    extrapolation, the learned guess with the library's defaults (no field
+    corrected), and the learned guess correcting p and nu_tilde (mask 17).
+    Each runs from the same seeded start on its own context; steps after the
+    first --warmup are reported (pseudo-iterations and device seconds)."""
+    from desalm.solver import DesalmError, Solver
+
+    def noop():
+        pass
+    res = {"section": "initial_guesses", "criterion": dict(CRITERION), "steps": args.guesses,
+           "reported_from_step": args.warmup + 1}
+    for name, pred, mask in (("qn", abi.PRED_QN, None), ("linear", abi.PRED_LINEAR, None),
+                             ("learned", abi.PRED_LEARNED, None), ("learned_p_nut", abi.PRED_LEARNED, 17)):
+        case, grid, state, omega, spec, rate, desc = build_case(args.case, abi.MIXED, pred, args.model)
+        res["workload"] = desc
+        S = Solver(case)
+        S.set_grid(grid["x"], grid["y"], grid["z"], grid.get("wd"))
+        S.set_state(state["q"], state["qn"], state["qnm1"], state["nut"])
+        if omega is not None:
+            S.set_omega(omega["omega"], omega["omega_n"], omega["omega_nm1"])
+        if mask is not None:
+            S.lp_fields(mask)
+        its, secs, failed, reps = [], [], None, None
+        for k in range(args.guesses):
+            try:
+                sec, reps, _ = timed(S, 1, S.mg_driver, noop, lambda x: x)
+            except DesalmError as e:   # e.g. a non-finite norm: the step's failure is the result
+                failed = {"step": k + 1, "error": str(e)}
+                break
+            its.append(reps[0]["iterations"])
+            secs.append(sec)
+        w = args.warmup
+        res[name] = {"iterations_per_step": its,
+                     "mean_iterations": float(np.mean(its[w:])) if len(its) > w else None,
+                     "s_per_step": float(np.mean(secs[w:])) if len(secs) > w else None,
+                     "ended_by_last": which_test(reps[0]) if reps else None, "failed": failed}
+        if pred == abi.PRED_LEARNED:
+            res[name]["network"] = S.lp_report()
+        S.close()
+    return res
+
+
 def _oracle_solver(case_name, model, real_bytes, predictor):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
@@ -704,7 +752,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--case", default="turbine", choices=["turbine", "cavity", "channel"])
+    ap.add_argument("--case", default="turbine", choices=["turbine", "cavity", "channel", "ogrid"])
     ap.add_argument("--model", default="kw", choices=["kw", "sa"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
@@ -714,7 +762,13 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--learned", action="store_true", help="with --ncu-workload: learned-guess steps")
     ap.add_argument("--small", action="store_true", help="with --ncu-workload: the turbine box at 193x97x97")
+    ap.add_argument("--guesses", type=int, default=0, metavar="STEPS",
+                    help="instead of the bench line: the initial guesses on --case (MIXED), each from the seeded "
+                         "start for STEPS physical steps, the first --warmup of them untimed")
     args = ap.parse_args()
+    if args.guesses:
+        print(json.dumps(run_guesses(args)))
+        return
     if args.ncu_workload:
         ncu_workload(args.case, abi.MIXED if args.precision == "mixed" else abi.FP64, args.model, args.learned,
                      args.small)
