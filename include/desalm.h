@@ -599,7 +599,9 @@ int  desalm_rfg_set(desalm_ctx* ctx, const desalm_rfg* rfg);
  * stream.  Call it before desalm_mg_driver / desalm_begin_step, as
  * src/main.F90:60 does; the step then shifts the plane into q^n like the rest
  * of q, and when the guess is extrapolated or learned, forces the plane again
- * for the same time after the guess, so the step holds the forced values. */
+ * for the same time after the guess, so the step holds the forced values.
+ * A desalm_set_state between the two calls replaces the forced plane like the
+ * rest of q; the extrapolated or learned guess still forces it again. */
 int  desalm_rfg_inlet(desalm_ctx* ctx, double time);
 
 /* Self-test of the device watchdog: a kernel waits, through the same bounded
