@@ -21,7 +21,31 @@ from desalm import abi, cases  # noqa: E402
 import oracle  # noqa: E402
 
 
+def run_rfg():
+    """The random flow generator's oracle: mode tables of a seed and the
+    inflow plane of a small wake box with per-node anisotropic tensors."""
+    import rfg_oracle
+    case, grid, state = cases.wake(im=9, jm=13, km=11, turbulence=0, seed=5)
+    tab = rfg_oracle.modes(200, 77)
+    spec = cases.rfg_inflow(case, tables=tab)
+    rng = np.random.default_rng(78)
+    uij = np.zeros((case.km, case.jm, 6))
+    for k in range(case.km):
+        for j in range(case.jm):
+            B = rng.normal(size=(3, 3))
+            R = (B @ B.T + 0.5 * np.eye(3)) * 1e-3
+            uij[k, j] = (R[0, 0], R[0, 1], R[0, 2], R[1, 1], R[1, 2], R[2, 2])
+    spec["uij"] = uij
+    spec["t_ts"] = rng.uniform(0.1, 0.5, size=(case.km, case.jm))
+    spec["t_ls"] = rng.uniform(0.1, 0.4, size=(case.km, case.jm))
+    q = state["q"].reshape(case.km, case.jm, case.im, 5).copy()
+    q = rfg_oracle.inlet_forcing(q, grid, (case.im, case.jm, case.km), 0.3, spec)
+    return {"p": tab["p"], "q": tab["q"], "k": tab["k"], "omega": tab["omega"], "plane": q[1:-1, 1:-1, 0, 1:4]}
+
+
 def run(name):
+    if name == "rfg":
+        return run_rfg()
     if name == "cavity17":
         case, grid, state = cases.cavity(n=17, seed=123, itmax=5)
     else:
@@ -43,7 +67,7 @@ def run(name):
 
 
 def main():
-    for name in ("cavity17", "channel17"):
+    for name in ("cavity17", "channel17", "rfg"):
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **run(name))
         print("wrote", name)
 

@@ -8,7 +8,7 @@ import pytest
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
-@pytest.mark.parametrize("name", ["cavity17", "channel17"])
+@pytest.mark.parametrize("name", ["cavity17", "channel17", "rfg"])
 def test_oracle_matches_golden(name, oracle_mod):
     import importlib.util
     spec = importlib.util.spec_from_file_location("make_golden", os.path.join(HERE, "golden", "make_golden.py"))
